@@ -1,0 +1,168 @@
+/*
+ * si3d_gpu.h — C ABI of the B200 (sm_100a) implementation of pSi3D's per-timestep
+ * semi-implicit core: momentum explicit terms + per-column tridiagonals, free-surface (zeta)
+ * assembly, the MIC-preconditioned conjugate-gradient zeta solve, velocities/continuity,
+ * active-scalar transport and the leapfrog-trapezoidal bookkeeping.
+ *
+ * The reference calls these stages from Fortran (si3d.f90:324-458 -> fd,
+ * si3d_procedures.f90:382-575).  A Fortran host binds this header through ISO_C_BINDING
+ * (module si3d_gpu_iface in si3d_b200/fortran/); every scalar is passed by value or by
+ * pointer, every array is a plain pointer to host memory laid out exactly as the reference's
+ * arrays: 3-D fields (km1, lm1) column-major with k fastest, 2-D fields of length lm1, all
+ * column indices 1-based with lm1 = lm + 1 the dry sentinel.
+ *
+ * Ownership: the caller owns every host array; the library copies what it needs and never
+ * retains host pointers.  The library owns the device state of a handle (one CUDA stream,
+ * device buffers, captured graphs).  Calls are synchronous: on return the device state is
+ * updated (or the host outputs are valid).  Handles are independent; one handle must not be
+ * used from two threads at once.
+ *
+ * Errors: every entry point returns an int.  0 = success.  The zeta solve reports NSPCG's own
+ * codes (1 = itmax reached, 2 = tolerance clamped, 3/4 = eigenvalue estimate halted,
+ * -6 = pAp <= 0, -7 = (r,z) <= 0); library errors are <= -100 (see SI3D_E*).  The library never
+ * traps, never exits and never waits without a bound.
+ */
+#ifndef SI3D_GPU_H
+#define SI3D_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* library error codes */
+#define SI3D_OK 0
+#define SI3D_ECUDA (-100)     /* a CUDA runtime call failed */
+#define SI3D_EDIMS (-101)     /* bad dimensions or arguments */
+#define SI3D_EHANDLE (-102)   /* unknown handle */
+#define SI3D_ENAME (-103)     /* unknown field name */
+#define SI3D_ENAN (-104)      /* non-finite value detected */
+#define SI3D_ETIMEOUT (-105)  /* a bounded device wait gave up */
+#define SI3D_ENOMEM (-106)    /* device allocation failed */
+#define SI3D_ENODEV (-107)    /* no CUDA device / not sm_100 */
+
+/* precision forms */
+#define SI3D_FP64 0       /* plain FP64 everywhere */
+#define SI3D_MIXED_IR 1   /* FP32 SpMV + MIC inside an FP64 iterative-refinement loop */
+
+/* zeta-solve orderings */
+#define SI3D_ORDER_REDBLACK 1   /* NSPCG iperm=1 red-black MIC (the GPU form) */
+
+/* initial guess for the zeta solve */
+#define SI3D_X0_PREV 0      /* sp, as the reference (si3d_procedures.f90:1970) */
+#define SI3D_X0_ZERO 1
+#define SI3D_X0_LEARNED 2   /* sp + the learned increment (si3d_gpu_set_warmstart) */
+
+/* Grid description produced by the host's `bathy` (si3d_utils.f90:595-892). */
+typedef struct si3d_grid {
+  int im1, jm1;            /* (i,j) extents including the fictitious border */
+  int km1;                 /* number of levels incl. fictitious top and bottom layers */
+  int k1;                  /* first real layer (2) */
+  int lm;                  /* number of wet columns */
+  const int* l2i;          /* [lm]   i of column l (1-based) */
+  const int* l2j;          /* [lm]   j of column l */
+  const int* lEC;          /* [lm]   east / west / north / south neighbour, lm+1 if dry */
+  const int* lWC;
+  const int* lNC;
+  const int* lSC;
+  const int* kmz;          /* [lm+1] bottom layer index; kmz[lm] = km1 */
+  const double* hhs;       /* [lm+1] depth at zeta points */
+  const double* hhu;       /* [lm+1] depth at u points */
+  const double* hhv;       /* [lm+1] depth at v points */
+  const double* zlevel;    /* [km1]  depth of the top of each layer (-100 above the surface) */
+} si3d_grid;
+
+/* Run parameters read by the host's `input` (si3d_utils.f90:21-315) plus the solver overlay. */
+typedef struct si3d_params {
+  double dt, dx, dy;
+  double Av0, Dv0, Ax0, Ay0, f, theta, cd, cw, beta;
+  int iadv, itrmom, ihd, ibc, isal, itrap, niter, ismooth;
+  /* zeta solve: NSPCG stopping test (2 or 5), tolerance, itmax, machine precision srelpr */
+  int pcg_test;
+  double pcg_tol;
+  int pcg_itmax;
+  double srelpr;
+  int ordering;            /* SI3D_ORDER_REDBLACK */
+  int x0_mode;             /* SI3D_X0_* */
+  int precision;           /* SI3D_FP64 or SI3D_MIXED_IR */
+} si3d_params;
+
+/* Per-call statistics (one entry per zeta solve inside the call). */
+typedef struct si3d_step_stats {
+  int nsolves;             /* zeta solves performed by the call */
+  int iters[24];           /* PCG iterations of each solve */
+  double relres[24];       /* final stopping-test value of each solve */
+  int ier[24];             /* NSPCG-style code of each solve */
+  int total_iters;
+  double ms_total;         /* device time of the call */
+  double ms_pcg;           /* device time spent in the zeta solves */
+} si3d_step_stats;
+
+/* Replaces the reference's allocation + init hand-off: uploads maps and parameters and
+ * allocates the device state (zero-initialised; the host then sets the initial fields).
+ * Reference interface replaced: the state set-up done by bathy/init before the time loop
+ * (si3d.f90:56-68) feeding fd (si3d_procedures.f90:382). */
+int si3d_gpu_init(const si3d_grid* grid, const si3d_params* params, int device, int* handle);
+
+/* Copy one reference array between host and device.  3-D names: uh uhp uhpp up upp hu hup hupp
+ * agx arx vh vhp vhpp vp vpp hv hvp hvpp agy ary h hp hpp sal salp salpp rhop Av Dv wp
+ * HeatSource Bth2 Bth3 Bth4 ((km1, lm1) column-major).  2-D names: s sp spp eagx earx eagy eary
+ * sx sy dd qq rr uair vair cdw (lm1).  Replaces the Fortran module arrays of si3d_types.f90:117-164. */
+int si3d_gpu_set_field(int handle, const char* name, const double* host);
+int si3d_gpu_get_field(int handle, const char* name, double* host);
+/* Integer column arrays k1z k1u k1v (lm1 entries). */
+int si3d_gpu_set_ifield(int handle, const char* name, const int* host);
+int si3d_gpu_get_ifield(int handle, const char* name, int* host);
+
+/* Density anomaly rhop = densty_s(salp, 4e-5, z) - 1000 at every column (sentinel included) and
+ * level k1..km1 from the uploaded salp and hp, as InitializeScalarFields does after reading the
+ * initial profile (si3d_procedures.f90:363-373). */
+int si3d_gpu_density(int handle);
+
+/* One call of fd (si3d_procedures.f90:382-575): surfbc CASE 0, exmom+matmom (x, y), matcon,
+ * SolverSparse (NSPCG mic1+cg replacement), vel + continuity(1), exsal + imsal, vel2.
+ * Replaces CALL fd(...) at si3d.f90:353 and si3d.f90:373. */
+int si3d_gpu_fd(int handle, int n, int istep, int lastiter, si3d_step_stats* stats);
+/* settrap (si3d_procedures.f90:3418), settrap2 (:3944), save (:3621); replace the calls at
+ * si3d.f90:365, :383, :393. */
+int si3d_gpu_settrap(int handle);
+int si3d_gpu_settrap2(int handle);
+int si3d_gpu_save(int handle, int istep);
+/* One whole time step n of the loop body si3d.f90:324-458 (leapfrog, settrap, niter
+ * trapezoidal iterations with settrap2, save); stats cover every solve of the step. */
+int si3d_gpu_step(int handle, int n, si3d_step_stats* stats);
+
+/* One routine of fd or of the step bookkeeping, for stage-by-stage unit tests: "momentum"
+ * (exmom + matmom + trid, x then y), "matcon", "solve" (SolverSparse incl. slayer_h), "vel"
+ * (vel + continuity(1)), "scalar" (exsal + imsal), "vel2", "settrap", "settrap2", "save". */
+int si3d_gpu_stage(int handle, const char* stage, int istep, si3d_step_stats* stats);
+
+/* Learned warm start: the increment added to sp for the next solve(s) when x0_mode is
+ * SI3D_X0_LEARNED (lm1 entries, host or device pointer flagged by `on_device`). */
+int si3d_gpu_set_warmstart(int handle, const double* dzeta, int on_device);
+
+/* Standalone replacement of CALL nspcg(mic1, cg, ...) (si3d_procedures.f90:1999-2000) on
+ * host Purdue arrays: coef (lm x 5, column-major: diagonal, W, S, N, E), jcoef (1-based,
+ * 0 = no entry), rhs (lm), zeta (lm; in: x0, out: solution).  The matrix must have the
+ * 5-point structure SolverSparse builds (jcoef columns = l, lWC, lSC, lNC, lEC).
+ * Outputs: iterations, final stopping-test value, emin/emax estimates. */
+int si3d_gpu_solve_zeta(int lm, const double* coeffA, const int* jcoefA, const double* rhs, double* zeta,
+                        int pcg_test, double pcg_tol, int pcg_itmax, double srelpr, int precision,
+                        int* iters, double* stptst, double* emin, double* emax);
+
+/* Batched tridiagonal solves with two right-hand sides sharing one factorisation, as trid
+ * (si3d_procedures.f90:3210-3289): for each of `nsys` systems of size `n` (column-major
+ * blocks a/b/c/g/r/ag/ar of n x nsys) solve [a b c] ag = g and [a b c] ar = r.  Host arrays. */
+int si3d_gpu_column_tridiag(int n, int nsys, const double* a, const double* b, const double* c,
+                            const double* g, const double* r, double* ag, double* ar);
+
+/* Wait for the handle's stream. */
+int si3d_gpu_sync(int handle);
+/* Human-readable text for an error code. */
+const char* si3d_gpu_strerror(int code);
+/* Free the device state of a handle. */
+void si3d_gpu_finalize(int handle);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SI3D_GPU_H */

@@ -1,0 +1,408 @@
+// Host side above the C ABI (include/si3d_host.h): the reference's input readers and set-up
+// restated in C++, and the time loop driving si3d_gpu_step.
+//
+// Readers: `input` (si3d_utils.f90:21-315, fixed-column records '(14X,G20.2)'), `bathy`
+// (:595-892, header '(37X,I5,6X,I5,8X,I5//)', rows '(5X,ncolsG5.0)' in decimetres),
+// InitializeScalarFields' file branch (si3d_procedures.f90:293-318, rows '(10X,G11.5)').
+// Set-up: ZGridDimensions (si3d_utils.f90:362-379), the l ordering and neighbour maps
+// (:781-806), kmz/hhs/hhu/hhv (:812-880), `init` (si3d_procedures.f90:23-181) and
+// InitializeTurbulenceModel CASE(0) (si3d_mixing.f90:650-671).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../../include/si3d_host.h"
+
+namespace {
+
+struct Records {
+  std::vector<std::string> rows;
+  size_t at = 0;
+  bool load(const std::string& path) {
+    std::ifstream in(path);
+    if (!in) return false;
+    for (std::string s; std::getline(in, s);) {
+      if (!s.empty() && s.back() == '\r') s.pop_back();
+      rows.push_back(s);
+    }
+    return true;
+  }
+  bool more() const { return at < rows.size(); }
+  std::string take() { return at < rows.size() ? rows[at++] : (at++, std::string()); }
+  void skip(int n) { at += n; }
+};
+
+// Value of a fixed-width numeric field (blanks ignored, empty = 0, D exponents allowed).
+bool numeric(const std::string& row, size_t col, size_t width, double& v) {
+  std::string t;
+  for (size_t i = col; i < std::min(row.size(), col + width); ++i) {
+    char ch = row[i];
+    if (ch == ' ' || ch == '\t') continue;
+    t.push_back(ch == 'd' || ch == 'D' ? 'e' : ch);
+  }
+  if (t.empty()) { v = 0; return true; }
+  char* e = nullptr;
+  v = std::strtod(t.c_str(), &e);
+  return e && *e == 0;
+}
+
+struct HostModel {
+  std::string err;
+  si3d_solver_opts opt{};
+  // input parameters
+  double xl = 0, yl = 0, zl = 0, tl = 0, idx = 0, idy = 0, idz = 0, dzmin = 0, datadj = 0, zetainit = 0, idt = 0;
+  double beta = 0, Av0 = 0, Dv0 = 0, Ax0 = 0, Ay0 = 0, f = 0, theta = 1, cd = 0, dtsurfbc = 0, cw = 0, wa = 0, phi = 0;
+  int ibathyf = 0, itrap = 1, niter = 2, ismooth = 0, iturb = 0, iadv = 1, itrmom = 1, ihd = 1, ibc = 1, isal = 1,
+      itrsca = 0, ifsurfbc = 0, icw = 0, nopen = 0, ntr = 0, iopss = 0, iox = 0, nxNBO = 0;
+  // grid
+  int im = 0, im1 = 0, jm = 0, jm1 = 0, km = 0, km1 = 0, k1 = 2, lm = 0, lm1 = 0, nts = 0;
+  std::vector<double> zlevel, hhs, hhu, hhv;
+  std::vector<int> l2i, l2j, lEC, lWC, lNC, lSC, kmz;
+  std::vector<unsigned char> wet;  // (i,j) mask, j fastest per i (the l traversal order)
+  std::vector<int> ij2l;
+  // initial state
+  std::vector<double> s0, hp0, hup0, hvp0, salp0, Av0f, Dv0f, uair, vair, cdw;
+  std::vector<int> k1z0, k1u0, k1v0;
+  // run
+  int gpu = -1, n = 0;
+  bool W(int i, int j) const { return wet[(size_t)(i - 1) * jm1 + (j - 1)] != 0; }
+  int L(int i, int j) const { return ij2l[(size_t)(i - 1) * jm1 + (j - 1)]; }
+  double zlv(int k) const { return zlevel[k - 1]; }
+  size_t I3(int k, int l) const { return (size_t)(l - 1) * km1 + (k - 1); }
+};
+
+std::mutex g_mu;
+std::vector<std::unique_ptr<HostModel>> g_models;
+
+HostModel* model(int h) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return (h >= 0 && h < (int)g_models.size()) ? g_models[h].get() : nullptr;
+}
+
+bool read_parameters(HostModel& M, const std::string& dir) {
+  Records R;
+  if (!R.load(dir + "/si3d_inp.txt")) { M.err = "cannot open si3d_inp.txt"; return false; }
+  bool ok = true;
+  auto g = [&](double& v) { ok = ok && numeric(R.take(), 14, 20, v); };
+  auto gi = [&](int& v) { double x = 0; ok = ok && numeric(R.take(), 14, 20, x); v = (int)std::lround(x); };
+  int dummy = 0;
+  R.skip(2);                                     // title block
+  R.skip(3); gi(dummy); gi(dummy); gi(dummy); gi(dummy);
+  R.skip(3);
+  g(M.xl); g(M.yl); g(M.zl); g(M.tl); g(M.idx); g(M.idy); g(M.idz); g(M.dzmin); g(M.datadj); g(M.zetainit);
+  g(M.idt); gi(M.ibathyf);
+  R.skip(3);
+  gi(M.itrap); gi(M.niter); gi(M.ismooth); g(M.beta); gi(M.iturb); g(M.Av0); g(M.Dv0); gi(M.iadv); gi(M.itrmom);
+  gi(M.ihd); g(M.Ax0); g(M.Ay0); g(M.f); g(M.theta); gi(M.ibc); gi(M.isal); gi(M.itrsca); g(M.cd); gi(M.ifsurfbc);
+  g(M.dtsurfbc); gi(M.icw); g(M.cw); g(M.wa); g(M.phi); gi(dummy); gi(dummy);
+  R.skip(3); gi(dummy); gi(dummy); R.skip(2);    // ipt, nnodes, node lists
+  R.skip(3); gi(dummy); gi(dummy); gi(dummy); R.skip(1);   // iop, itspfh, n_planes, planes
+  R.skip(3); gi(M.iox);
+  R.skip(3); gi(dummy); gi(dummy); gi(dummy);    // ipxml, itspf, iTurbVars
+  R.skip(3); gi(M.nopen); R.skip(7);
+  R.skip(3); gi(M.nxNBO); R.skip(7);
+  R.skip(3); gi(M.ntr); R.skip(5);
+  R.skip(3); gi(M.iopss);
+  if (!ok) { M.err = "si3d_inp.txt: unreadable record"; return false; }
+  if (M.iox || M.nopen || M.nxNBO || M.ntr || M.iopss || M.ifsurfbc || M.iturb || M.ihd > 1 || M.ibathyf < 0 ||
+      M.ismooth || M.itrmom != 1) {
+    M.err = "si3d_inp.txt selects an option outside the semi-implicit core (open boundaries, tracers, point "
+            "sources, heat budget, turbulence closure, Smagorinsky, smoothing, non-centred advection or "
+            "variable layers)";
+    return false;
+  }
+  M.im = (int)std::lround(M.xl / M.idx) + 1; M.im1 = M.im + 1;
+  M.jm = (int)std::lround(M.yl / M.idy) + 1; M.jm1 = M.jm + 1;
+  M.nts = (int)(M.tl / M.idt + .5);
+  M.km = (int)std::ceil(M.zl / M.idz) + 1;
+  M.km1 = M.km + 1;
+  M.zlevel.assign(M.km1, 0.0);
+  M.zlevel[M.k1 - 1] = 0.0;
+  for (int k = M.k1 + 1; k <= M.km1; ++k) M.zlevel[k - 1] = M.zlevel[k - 2] + M.idz;
+  M.zlevel[0] = -100.;
+  M.zlevel[M.k1 - 1] = -100.;
+  return true;
+}
+
+bool read_bathymetry(HostModel& M, const std::string& dir) {
+  Records R;
+  if (!R.load(dir + "/si3d_bathy")) { M.err = "cannot open si3d_bathy"; return false; }
+  const std::string head = R.take();
+  double a = 0, b = 0, c = 0;
+  if (!numeric(head, 37, 5, a) || !numeric(head, 48, 5, b) || !numeric(head, 61, 5, c) || c < 1) {
+    M.err = "si3d_bathy: bad header"; return false;
+  }
+  R.skip(2);
+  const int imm = (int)a, jmm = (int)b, ncols = (int)c;
+  if (M.im != imm + 1 || M.jm != jmm + 1) { M.err = "si3d_bathy header disagrees with si3d_inp.txt"; return false; }
+  // depths at zeta points, decimetres, blocks of ncols i-columns, rows j = jm .. 2
+  std::vector<double> dep((size_t)M.im1 * M.jm1, 0.0);
+  auto D = [&](int i, int j) -> double& { return dep[(size_t)(i - 1) * M.jm1 + (j - 1)]; };
+  for (int ia = 2; ia <= M.im; ia += ncols) {
+    const int ib = std::min(ia + ncols - 1, M.im);
+    for (int j = M.jm; j >= 2; --j) {
+      if (!R.more()) { M.err = "si3d_bathy: truncated"; return false; }
+      const std::string row = R.take();
+      for (int i = ia; i <= ib; ++i)
+        if (!numeric(row, 5 + 5 * (i - ia), 5, D(i, j))) { M.err = "si3d_bathy: bad depth"; return false; }
+    }
+  }
+  M.wet.assign((size_t)M.im1 * M.jm1, 0);
+  M.ij2l.assign((size_t)M.im1 * M.jm1, 0);
+  int l = 0;
+  for (int i = 1; i <= M.im1; ++i)
+    for (int j = 1; j <= M.jm1; ++j) {
+      const bool border = (i == 1 || i == M.im1 || j == 1 || j == M.jm1);
+      const double h4 = border ? 0.0 : D(i, j) * 0.1 + M.datadj;
+      D(i, j) = h4;
+      if (h4 > 0.0) { M.wet[(size_t)(i - 1) * M.jm1 + (j - 1)] = 1; ++l; }
+    }
+  M.lm = l; M.lm1 = l + 1;
+  const int lm1 = M.lm1;
+  for (auto& v : M.ij2l) v = lm1;
+  M.l2i.assign(lm1, 0); M.l2j.assign(lm1, 0);
+  l = 0;
+  for (int i = 1; i <= M.im1; ++i)
+    for (int j = 1; j <= M.jm1; ++j)
+      if (M.W(i, j)) { ++l; M.l2i[l - 1] = i; M.l2j[l - 1] = j; M.ij2l[(size_t)(i - 1) * M.jm1 + (j - 1)] = l; }
+  M.lEC.assign(lm1, lm1); M.lWC.assign(lm1, lm1); M.lNC.assign(lm1, lm1); M.lSC.assign(lm1, lm1);
+  for (int q = 1; q <= M.lm; ++q) {
+    const int i = M.l2i[q - 1], j = M.l2j[q - 1];
+    M.lEC[q - 1] = M.L(i + 1, j); M.lWC[q - 1] = M.L(i - 1, j);
+    M.lNC[q - 1] = M.L(i, j + 1); M.lSC[q - 1] = M.L(i, j - 1);
+  }
+  M.kmz.assign(lm1, 0); M.hhs.assign(lm1, 0.0);
+  for (int q = 1; q <= M.lm; ++q) {
+    const double hs1 = D(M.l2i[q - 1], M.l2j[q - 1]);
+    int kk = (int)std::floor(hs1 / M.idz);
+    if ((hs1 - kk * M.idz) > M.dzmin) { kk += 1; M.hhs[q - 1] = hs1; }
+    else M.hhs[q - 1] = kk * M.idz;
+    M.kmz[q - 1] = kk + 1;
+    if (M.kmz[q - 1] > M.km) { M.err = "bathymetry deeper than zl"; return false; }
+    if (M.kmz[q - 1] < M.k1) { M.err = "a wet cell shallower than dzmin has no layer"; return false; }
+  }
+  M.kmz[lm1 - 1] = M.km1;
+  M.hhu.assign(lm1, 0.0); M.hhv.assign(lm1, 0.0);
+  for (int q = 1; q <= M.lm; ++q) {
+    if (M.lEC[q - 1] != lm1) M.hhu[q - 1] = std::min(M.hhs[M.lEC[q - 1] - 1], M.hhs[q - 1]);
+    if (M.lNC[q - 1] != lm1) M.hhv[q - 1] = std::min(M.hhs[M.lNC[q - 1] - 1], M.hhs[q - 1]);
+  }
+  return true;
+}
+
+bool read_profile(HostModel& M, const std::string& dir, std::vector<double>& prof) {
+  Records R;
+  if (!R.load(dir + "/si3d_init.txt")) { M.err = "cannot open si3d_init.txt"; return false; }
+  R.skip(7);
+  prof.assign(M.km1, 0.0);
+  for (int k = 0; k < M.km1; ++k) {
+    if (!R.more()) { M.err = "si3d_init.txt: truncated"; return false; }
+    if (!numeric(R.take(), 10, 11, prof[k])) { M.err = "si3d_init.txt: bad value"; return false; }
+  }
+  return true;
+}
+
+bool read_wind(HostModel& M, const std::string& dir) {
+  const int lm1 = M.lm1;
+  M.uair.assign(lm1, 0.0); M.vair.assign(lm1, 0.0); M.cdw.assign(lm1, 0.0);
+  const double pi = 3.1415926535897932;
+  for (int q = 0; q < M.lm; ++q) {   // surfbc CASE(0) (si3d_boundaryconditions.f90:4508-4514)
+    M.uair[q] = -M.wa * std::sin(pi * M.phi / 180.);
+    M.vair[q] = -M.wa * std::cos(pi * M.phi / 180.);
+    M.cdw[q] = M.cw;
+  }
+  FILE* fp = std::fopen((dir + "/si3d_wind_override.bin").c_str(), "rb");
+  if (!fp) return true;
+  int32_t hd[2] = {0, 0};
+  const size_t n2 = (size_t)M.im1 * M.jm1;
+  std::vector<double> u(n2), v(n2);
+  bool ok = std::fread(hd, 4, 2, fp) == 2 && hd[0] == M.im1 && hd[1] == M.jm1 && std::fread(u.data(), 8, n2, fp) == n2 &&
+            std::fread(v.data(), 8, n2, fp) == n2;
+  std::fclose(fp);
+  if (!ok) { M.err = "si3d_wind_override.bin: size mismatch"; return false; }
+  for (int q = 0; q < M.lm; ++q) {
+    const size_t c = (size_t)(M.l2i[q] - 1) * M.jm1 + (M.l2j[q] - 1);
+    M.uair[q] = u[c]; M.vair[q] = v[c];
+  }
+  return true;
+}
+
+// init (si3d_procedures.f90:23-181), testcase 3 -> CASE DEFAULT, plus the scalar profile and the
+// constant eddy coefficients.
+void initial_state(HostModel& M, const std::vector<double>& prof) {
+  const int lm1 = M.lm1, km1 = M.km1, k1 = M.k1;
+  const size_t n3 = (size_t)km1 * lm1;
+  M.s0.assign(lm1, M.zetainit);
+  M.hp0.assign(n3, 0.0); M.hup0.assign(n3, 0.0); M.hvp0.assign(n3, 0.0);
+  M.k1z0.assign(lm1, km1); M.k1u0.assign(lm1, km1); M.k1v0.assign(lm1, km1);
+  for (int l = 1; l <= M.lm; ++l) {
+    const int kms = M.kmz[l - 1];
+    int first = 0;
+    for (int k = k1; k <= kms; ++k) {
+      double v = std::min(M.zlv(k + 1), M.hhs[l - 1]) - std::max(M.zlv(k), -M.s0[l - 1]);
+      if (v > 0.0) { if (!first) { first = 1; M.k1z0[l - 1] = k; } }
+      else v = 0.0;
+      M.hp0[M.I3(k, l)] = v;
+    }
+    M.hp0[M.I3(kms + 1, l)] = 0.5;   // sed_h (si3d_types.f90:420)
+    if (M.k1z0[l - 1] == km1) M.s0[l - 1] = -M.hhs[l - 1] + 0.0;
+    const int lE = M.lEC[l - 1], lN = M.lNC[l - 1];
+    if (lE != lm1) {
+      const int kmx = std::min(kms, M.kmz[lE - 1]);
+      first = 0;
+      for (int k = k1; k <= kmx; ++k) {
+        double v = std::min(M.zlv(k + 1), M.hhu[l - 1]) - std::max(M.zlv(k), -(M.s0[l - 1] + M.s0[lE - 1]) / 2.);
+        if (v > 0.0) { if (!first) { first = 1; M.k1u0[l - 1] = k; } }
+        else v = 0.0;
+        M.hup0[M.I3(k, l)] = v;
+      }
+    }
+    if (lN != lm1) {
+      const int kmy = std::min(kms, M.kmz[lN - 1]);
+      first = 0;
+      for (int k = k1; k <= kmy; ++k) {
+        double v = std::min(M.zlv(k + 1), M.hhv[l - 1]) - std::max(M.zlv(k), -(M.s0[l - 1] + M.s0[lN - 1]) / 2.);
+        if (v > 0.0) { if (!first) { first = 1; M.k1v0[l - 1] = k; } }
+        else v = 0.0;
+        M.hvp0[M.I3(k, l)] = v;
+      }
+    }
+  }
+  M.salp0.assign(n3, 0.0);
+  for (int l = 1; l <= lm1; ++l)
+    for (int k = 1; k <= km1; ++k) M.salp0[M.I3(k, l)] = prof[k - 1];
+  M.Av0f.assign(n3, 0.0); M.Dv0f.assign(n3, 0.0);
+  for (int l = 1; l <= M.lm; ++l) {
+    const int kms = M.kmz[l - 1], k1s = M.k1z0[l - 1];
+    for (int k = k1s + 1; k <= kms; ++k) { M.Av0f[M.I3(k, l)] = M.Av0; M.Dv0f[M.I3(k, l)] = M.Dv0; }
+    // Av(k1s) and Av(kms+1) stay zero (si3d_mixing.f90:661-669)
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int si3d_host_open(const char* run_dir, const si3d_solver_opts* opts, int* hm, char* err, int errlen) {
+  auto M = std::make_unique<HostModel>();
+  if (opts) M->opt = *opts;
+  else { M->opt.pcg_test = 5; M->opt.pcg_tol = 1e-12; M->opt.pcg_itmax = 200; M->opt.srelpr = 2.220446049250313e-16; }
+  const std::string dir = run_dir ? run_dir : ".";
+  std::vector<double> prof;
+  bool ok = read_parameters(*M, dir) && read_bathymetry(*M, dir) && read_profile(*M, dir, prof) && read_wind(*M, dir);
+  if (!ok) {
+    if (err && errlen > 0) { std::strncpy(err, M->err.c_str(), errlen - 1); err[errlen - 1] = 0; }
+    return SI3D_EDIMS;
+  }
+  initial_state(*M, prof);
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_models.push_back(std::move(M));
+  *hm = (int)g_models.size() - 1;
+  return 0;
+}
+
+int si3d_host_dims(int h, int* dims) {
+  HostModel* M = model(h);
+  if (!M) return SI3D_EHANDLE;
+  dims[0] = M->im1; dims[1] = M->jm1; dims[2] = M->km1; dims[3] = M->lm; dims[4] = M->km; dims[5] = M->nts;
+  return 0;
+}
+
+int si3d_host_get_map(int h, const char* name, int* out) {
+  HostModel* M = model(h);
+  if (!M) return SI3D_EHANDLE;
+  const std::string n = name ? name : "";
+  const std::vector<int>* v = n == "l2i" ? &M->l2i : n == "l2j" ? &M->l2j : n == "lEC" ? &M->lEC : n == "lWC" ? &M->lWC
+                            : n == "lNC" ? &M->lNC : n == "lSC" ? &M->lSC : n == "kmz" ? &M->kmz : nullptr;
+  if (!v) return SI3D_ENAME;
+  std::memcpy(out, v->data(), sizeof(int) * v->size());
+  return 0;
+}
+
+int si3d_host_get_zlevel(int h, double* out) {
+  HostModel* M = model(h);
+  if (!M) return SI3D_EHANDLE;
+  std::memcpy(out, M->zlevel.data(), sizeof(double) * M->zlevel.size());
+  return 0;
+}
+
+int si3d_host_attach_gpu(int h, int device, int* gpu_handle) {
+  HostModel* M = model(h);
+  if (!M) return SI3D_EHANDLE;
+  si3d_grid g{};
+  g.im1 = M->im1; g.jm1 = M->jm1; g.km1 = M->km1; g.k1 = M->k1; g.lm = M->lm;
+  g.l2i = M->l2i.data(); g.l2j = M->l2j.data();
+  g.lEC = M->lEC.data(); g.lWC = M->lWC.data(); g.lNC = M->lNC.data(); g.lSC = M->lSC.data();
+  g.kmz = M->kmz.data(); g.hhs = M->hhs.data(); g.hhu = M->hhu.data(); g.hhv = M->hhv.data();
+  g.zlevel = M->zlevel.data();
+  si3d_params p{};
+  p.dt = M->idt; p.dx = M->idx; p.dy = M->idy;
+  p.Av0 = M->Av0; p.Dv0 = M->Dv0; p.Ax0 = M->Ax0; p.Ay0 = M->Ay0; p.f = M->f; p.theta = M->theta; p.cd = M->cd;
+  p.cw = M->cw; p.beta = M->beta;
+  p.iadv = M->iadv; p.itrmom = M->itrmom; p.ihd = M->ihd; p.ibc = M->ibc; p.isal = M->isal; p.itrap = M->itrap;
+  p.niter = M->niter; p.ismooth = M->ismooth;
+  p.pcg_test = M->opt.pcg_test; p.pcg_tol = M->opt.pcg_tol; p.pcg_itmax = M->opt.pcg_itmax; p.srelpr = M->opt.srelpr;
+  p.ordering = SI3D_ORDER_REDBLACK; p.x0_mode = M->opt.x0_mode; p.precision = M->opt.precision;
+  int gh = -1;
+  int rc = si3d_gpu_init(&g, &p, device, &gh);
+  if (rc) return rc;
+  // initial fields (init: s = sp = spp; hpp = hp = h; k1 indices; sal = salp = salpp; Av/Dv)
+  const char* same_s[] = {"s", "sp", "spp"};
+  for (const char* nm : same_s) if ((rc = si3d_gpu_set_field(gh, nm, M->s0.data()))) return rc;
+  const char* same_h[] = {"h", "hp", "hpp"};
+  for (const char* nm : same_h) if ((rc = si3d_gpu_set_field(gh, nm, M->hp0.data()))) return rc;
+  const char* same_hu[] = {"hu", "hup", "hupp"};
+  for (const char* nm : same_hu) if ((rc = si3d_gpu_set_field(gh, nm, M->hup0.data()))) return rc;
+  const char* same_hv[] = {"hv", "hvp", "hvpp"};
+  for (const char* nm : same_hv) if ((rc = si3d_gpu_set_field(gh, nm, M->hvp0.data()))) return rc;
+  const char* same_t[] = {"sal", "salp", "salpp"};
+  for (const char* nm : same_t) if ((rc = si3d_gpu_set_field(gh, nm, M->salp0.data()))) return rc;
+  if ((rc = si3d_gpu_set_field(gh, "Av", M->Av0f.data()))) return rc;
+  if ((rc = si3d_gpu_set_field(gh, "Dv", M->Dv0f.data()))) return rc;
+  if ((rc = si3d_gpu_set_field(gh, "uair", M->uair.data()))) return rc;
+  if ((rc = si3d_gpu_set_field(gh, "vair", M->vair.data()))) return rc;
+  if ((rc = si3d_gpu_set_field(gh, "cdw", M->cdw.data()))) return rc;
+  std::vector<double> one(M->lm1, 1.0);
+  if ((rc = si3d_gpu_set_field(gh, "rr", one.data()))) return rc;
+  if ((rc = si3d_gpu_set_ifield(gh, "k1z", M->k1z0.data()))) return rc;
+  if ((rc = si3d_gpu_set_ifield(gh, "k1u", M->k1u0.data()))) return rc;
+  if ((rc = si3d_gpu_set_ifield(gh, "k1v", M->k1v0.data()))) return rc;
+  if ((rc = si3d_gpu_density(gh))) return rc;   // rhop from the initial profile (:363-373)
+  M->gpu = gh;
+  M->n = 0;
+  if (gpu_handle) *gpu_handle = gh;
+  return 0;
+}
+
+int si3d_host_run(int h, int nsteps, si3d_step_stats* stats) {
+  HostModel* M = model(h);
+  if (!M) return SI3D_EHANDLE;
+  if (M->gpu < 0) return SI3D_EHANDLE;
+  for (int s = 0; s < nsteps; ++s) {
+    const int n = M->n + 1;
+    const int rc = si3d_gpu_step(M->gpu, n, stats ? &stats[s] : nullptr);
+    if (rc) return rc;
+    M->n = n;
+  }
+  return 0;
+}
+
+int si3d_host_step_count(int h) {
+  HostModel* M = model(h);
+  return M ? M->n : SI3D_EHANDLE;
+}
+
+void si3d_host_close(int h) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (h < 0 || h >= (int)g_models.size() || !g_models[h]) return;
+  if (g_models[h]->gpu >= 0) si3d_gpu_finalize(g_models[h]->gpu);
+  g_models[h].reset();
+}
+
+}  // extern "C"

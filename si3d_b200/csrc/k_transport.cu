@@ -1,0 +1,586 @@
+// Column kernels after the zeta solve and the leapfrog-trapezoidal bookkeeping.
+//
+// slayer_h (si3d_procedures.f90:2070-2175), vel + continuity(1) (:2430-2567, :2653-2707),
+// exsal (:2827-3076) + imsal/trid1 (:3079-3207, :3292-3352), vel2/layer_h (:2570-2631,
+// :2181-2231), settrap (:3418-3618), settrap2 (:3944-4087), save (:3621-3941) with layer_hp2
+// (:2238-2292), TopLayerIndexp2 (:2368-2427), continuity(2) and densty_s.
+//
+// Every kernel gives one thread one water column and walks the layers; a warp covers 32
+// consecutive columns so each per-layer access of a layer-major field is coalesced.  Arrays that
+// the reference keeps across calls with partial rewrites (the thread-private flux arrays Bth2,
+// Bth3, Bth4, and uh/vh/h above the surface) are kept as persistent device fields and written
+// exactly where the reference writes them.
+#include "common.cuh"
+#include "kernels.h"
+
+namespace si3d {
+
+namespace {
+
+constexpr int TB = 128;
+
+__device__ __forceinline__ bool ewet(const Dev& d, int l) { return NB(d.g.lEC, l) != d.g.lm1; }
+__device__ __forceinline__ bool nwet(const Dev& d, int l) { return NB(d.g.lNC, l) != d.g.lm1; }
+
+// layer_hp2 for column l (the version that recomputes hp/hup/hvp from sp)
+__device__ void layer_hp2_col(const Dev& d, int l) {
+  const int kms = NB(d.g.kmz, l);
+  const double spl = d.s.sp[l - 1];
+  const double hhs = d.g.hhs[l - 1];
+  for (int k = d.g.k1; k <= kms; ++k) {
+    double v = fmin(zl(d, k + 1), hhs) - fmax(zl(d, k), -spl);
+    if (v <= HMIN) v = ZERO;
+    d.f.hp[IX(d, k, l)] = v;
+  }
+  if (ewet(d, l)) {
+    const int lE = NB(d.g.lEC, l);
+    const int kmx = min(kms, NB(d.g.kmz, lE));
+    const double sm = fmax(spl, d.s.sp[lE - 1]);
+    const double hhu = d.g.hhu[l - 1];
+    for (int k = d.g.k1; k <= kmx; ++k) {
+      double v = fmin(zl(d, k + 1), hhu) - fmax(zl(d, k), -sm);
+      if (v <= HMIN) v = ZERO;
+      d.f.hup[IX(d, k, l)] = v;
+    }
+  }
+  if (nwet(d, l)) {
+    const int lN = NB(d.g.lNC, l);
+    const int kmy = min(kms, NB(d.g.kmz, lN));
+    const double sm = fmax(spl, d.s.sp[lN - 1]);
+    const double hhv = d.g.hhv[l - 1];
+    for (int k = d.g.k1; k <= kmy; ++k) {
+      double v = fmin(zl(d, k + 1), hhv) - fmax(zl(d, k), -sm);
+      if (v <= HMIN) v = ZERO;
+      d.f.hvp[IX(d, k, l)] = v;
+    }
+  }
+}
+
+// TopLayerIndexp2 for column l
+__device__ void top_index_col(const Dev& d, int l) {
+  const int km1 = d.g.km1, kms = NB(d.g.kmz, l);
+  int kz = km1, ku = km1, kv = km1;
+  for (int k = d.g.k1; k <= kms; ++k) if (d.f.hp[IX(d, k, l)] > ZERO) { kz = k; break; }
+  if (ewet(d, l)) {
+    const int kmx = min(kms, NB(d.g.kmz, NB(d.g.lEC, l)));
+    for (int k = d.g.k1; k <= kmx; ++k) if (d.f.hup[IX(d, k, l)] > ZERO) { ku = k; break; }
+  }
+  if (nwet(d, l)) {
+    const int kmy = min(kms, NB(d.g.kmz, NB(d.g.lNC, l)));
+    for (int k = d.g.k1; k <= kmy; ++k) if (d.f.hvp[IX(d, k, l)] > ZERO) { kv = k; break; }
+  }
+  d.s.k1z[l - 1] = kz; d.s.k1u[l - 1] = ku; d.s.k1v[l - 1] = kv;
+}
+
+// ------------------------------------------------------------- slayer_h
+__global__ void k_slayer_h(Dev d) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const int km1 = d.g.km1;
+  const int kz = d.s.k1z[l - 1], ku = d.s.k1u[l - 1], kv = d.s.k1v[l - 1];
+  double* h = d.f.h; double* hu = d.f.hu; double* hv = d.f.hv;
+  const double* hp = d.f.hp; const double* hup = d.f.hup; const double* hvp = d.f.hvp;
+  for (int k = 1; k <= kz - 1; ++k) h[IX(d, k, l)] = hp[IX(d, k, l)];
+  for (int k = 1; k <= ku - 1; ++k) hu[IX(d, k, l)] = hup[IX(d, k, l)];
+  for (int k = 1; k <= kv - 1; ++k) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
+  for (int k = kz + 2; k <= km1; ++k) h[IX(d, k, l)] = hp[IX(d, k, l)];
+  for (int k = ku + 1; k <= km1; ++k) hu[IX(d, k, l)] = hup[IX(d, k, l)];
+  for (int k = kv + 2; k <= km1; ++k) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
+  // Surface layers.  A column whose surface index has reached the bottom level (every layer
+  // dry) is left untouched: the reference would read zlevel past km1 there.
+  const double sl = d.s.s[l - 1];
+  int k = kz;
+  if (k < km1) {
+    double haux = fmin(zl(d, k + 1), d.g.hhs[l - 1]) + sl;
+    if (haux <= HMIN) {
+      h[IX(d, k, l)] = ZERO;
+      k = k + 1;
+      if (k < km1) {
+        haux = fmin(zl(d, k + 1), d.g.hhs[l - 1]) + sl;
+        h[IX(d, k, l)] = (haux <= HMIN) ? ZERO : haux;
+      }
+    } else h[IX(d, k, l)] = haux;
+  }
+  if (ewet(d, l)) {
+    if (ku < km1) {
+      const double sm = fmax(sl, d.s.s[NB(d.g.lEC, l) - 1]);
+      const double haux = fmin(zl(d, ku + 1), d.g.hhu[l - 1]) + sm;
+      // on drying the reference recomputes the same layer (k is reset to k1u, :2136)
+      hu[IX(d, ku, l)] = (haux <= HMIN) ? ZERO : haux;
+    }
+  } else {
+    for (int kk = ku; kk <= ku + 1 && kk <= km1; ++kk) hu[IX(d, kk, l)] = hup[IX(d, kk, l)];
+  }
+  if (nwet(d, l)) {
+    const double sm = fmax(sl, d.s.s[NB(d.g.lNC, l) - 1]);
+    k = kv;
+    if (k < km1) {
+      double haux = fmin(zl(d, k + 1), d.g.hhv[l - 1]) + sm;
+      if (haux <= HMIN) {
+        hv[IX(d, k, l)] = ZERO;
+        k = k + 1;
+        if (k < km1) {
+          haux = fmin(zl(d, k + 1), d.g.hhv[l - 1]) + sm;
+          hv[IX(d, k, l)] = (haux <= HMIN) ? ZERO : haux;
+        }
+      } else hv[IX(d, k, l)] = haux;
+    }
+  } else {
+    for (int kk = kv; kk <= kv + 1 && kk <= km1; ++kk) hv[IX(d, kk, l)] = hvp[IX(d, kk, l)];
+  }
+}
+
+// ------------------------------------------------------------- vel (uh, vh, k1u, k1v)
+template <int IEQ>
+__global__ void k_vel_uv(Dev d, const int* __restrict__ cols, int ncols) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ncols) return;
+  const int l = cols[t];
+  const bool X = IEQ == 1;
+  const int lO = X ? NB(d.g.lEC, l) : NB(d.g.lNC, l);
+  const int kmx = min(NB(d.g.kmz, lO), NB(d.g.kmz, l));
+  int* k1 = X ? d.s.k1u : d.s.k1v;
+  const int k0 = k1[l - 1];
+  const double gth = (X ? d.p.gdtdx : d.p.gdtdy) * d.tz;
+  const double c = gth * 1000. * (d.s.s[lO - 1] - d.s.s[l - 1]);
+  double* uv = X ? d.f.uh : d.f.vh;
+  const double* ag = X ? d.f.agx : d.f.agy;
+  const double* ar = X ? d.f.arx : d.f.ary;
+  for (int k = k0; k <= kmx; ++k) uv[IX(d, k, l)] = ag[IX(d, k, l)] - c * ar[IX(d, k, l)];
+  const double* huv = X ? d.f.hu : d.f.hv;
+  // (a face column with every layer dry, k0 = km1, is never reached: the reference would write
+  //  past the last level there)
+  if (k0 < d.g.km1 && huv[IX(d, k0, l)] <= ZERO) {
+    uv[IX(d, k0 + 1, l)] = uv[IX(d, k0, l)] + uv[IX(d, k0 + 1, l)];
+    uv[IX(d, k0, l)] = 0.0;
+    k1[l - 1] = k0 + 1;
+  }
+}
+
+// continuity(1) and the surface-index update at the end of vel
+__global__ void k_cont1(Dev d) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
+  const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l);
+  if (k1s <= kms) {
+    double* wp = d.f.wp;
+    for (int k = 1; k <= d.g.km1; ++k) wp[IX(d, k, l)] = 0.0;
+    double w = 0.0;
+    for (int k = kms; k >= k1s; --k) {
+      w = w - (d.f.uh[IX(d, k, l)] - d.f.uh[IX(d, k, lW)] + d.f.uhpp[IX(d, k, l)] - d.f.uhpp[IX(d, k, lW)]) / d.p.twodx -
+          (d.f.vh[IX(d, k, l)] - d.f.vh[IX(d, k, lS)] + d.f.vhpp[IX(d, k, l)] - d.f.vhpp[IX(d, k, lS)]) / d.p.twody;
+      wp[IX(d, k, l)] = w;
+    }
+    double ws = wp[IX(d, k1s, l)];
+    for (int k = d.g.k1; k <= k1s - 1; ++k)
+      ws = ws - (d.f.uh[IX(d, k, l)] - d.f.uh[IX(d, k, lW)] + d.f.uhpp[IX(d, k, l)] - d.f.uhpp[IX(d, k, lW)]) / d.p.twodx -
+           (d.f.vh[IX(d, k, l)] - d.f.vh[IX(d, k, lS)] + d.f.vhpp[IX(d, k, l)] - d.f.vhpp[IX(d, k, lS)]) / d.p.twody;
+    wp[IX(d, k1s, l)] = ws;
+  }
+  if (d.f.h[IX(d, k1s, l)] <= ZERO) d.s.k1z[l - 1] = min(k1s + 1, d.g.km1);
+}
+
+// continuity(2): wp from uhp/vhp
+__global__ void k_cont2(Dev d) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
+  if (k1s > kms) return;
+  const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l);
+  double* wp = d.f.wp;
+  for (int k = 1; k <= d.g.km1; ++k) wp[IX(d, k, l)] = 0.0;
+  double w = 0.0;
+  for (int k = kms; k >= k1s; --k) {
+    w = w - (d.f.uhp[IX(d, k, l)] - d.f.uhp[IX(d, k, lW)]) / d.p.dx - (d.f.vhp[IX(d, k, l)] - d.f.vhp[IX(d, k, lS)]) / d.p.dy;
+    wp[IX(d, k, l)] = w;
+  }
+  double ws = wp[IX(d, k1s, l)];
+  for (int k = d.g.k1; k <= k1s - 1; ++k)
+    ws = ws - (d.f.uhp[IX(d, k, l)] - d.f.uhp[IX(d, k, lW)]) / d.p.dx - (d.f.vhp[IX(d, k, l)] - d.f.vhp[IX(d, k, lS)]) / d.p.dy;
+  wp[IX(d, k1s, l)] = ws;
+}
+
+// ------------------------------------------------------------- exsal fluxes
+// Roe's superbee limiter (the reference always uses it, :2931-2934); cf0 is the default C_f.
+__device__ __forceinline__ double superbee(double s1, double s2, double s3, double s4, double vel, double cf0) {
+  double C_f = cf0;
+  if (s3 - s2 != 0) {
+    const bool down = copysign(1.0, vel) > 0;  // gamma1 = -SIGN(1, vel)
+    const double ratio = down ? (s2 - s1) / (s3 - s2) : (s4 - s3) / (s3 - s2);
+    C_f = fmax(fmax(0., fmin(1., 2. * ratio)), fmin(2., ratio));
+  }
+  return C_f;
+}
+
+__global__ void k_exsal_flux(Dev d) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
+  const int lE = NB(d.g.lEC, l), lW = NB(d.g.lWC, l), lN = NB(d.g.lNC, l), lS = NB(d.g.lSC, l);
+  const int lEE = NB(d.g.lEC, lE), lNN = NB(d.g.lNC, lN);
+  const double twodt1 = d.p.twodt * d.tz;
+  const double* sp = d.f.salpp;
+  const double* hpp = d.f.hpp;
+  const double* hp = d.f.hp;
+  for (int k = k1s; k <= kms; ++k) {
+    const size_t ik = IX(d, k, l);
+    // EW
+    if (d.f.hup[ik] > ZERO) {
+      const double vel = (d.f.uhpp[ik] + d.f.uh[ik]) / 2.;
+      const double s2 = sp[ik], s3 = sp[IX(d, k, lE)];
+      const double s1 = (hpp[IX(d, k, lW)] <= ZERO) ? s2 : sp[IX(d, k, lW)];
+      const double s4 = (hpp[IX(d, k, lEE)] <= ZERO) ? s3 : sp[IX(d, k, lEE)];
+      const double C_f = superbee(s1, s2, s3, s4, vel, 0.0);
+      d.f.Bth2[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / d.p.dx * C_f) * (s3 - s2) / 2.;
+    } else d.f.Bth2[ik] = 0.0;
+    // NS
+    if (d.f.hvp[ik] > ZERO) {
+      const double vel = (d.f.vhpp[ik] + d.f.vh[ik]) / 2.;
+      const double s2 = sp[ik], s3 = sp[IX(d, k, lN)];
+      const double s1 = (hpp[IX(d, k, lS)] <= ZERO) ? s2 : sp[IX(d, k, lS)];
+      const double s4 = (hpp[IX(d, k, lNN)] <= ZERO) ? s3 : sp[IX(d, k, lNN)];
+      const double C_f = superbee(s1, s2, s3, s4, vel, 0.0);
+      d.f.Bth4[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / d.p.dy * C_f) * (s3 - s2) / 2.;
+    } else d.f.Bth4[ik] = 0.0;
+    // UD (hp(1, l) is never positive, so k-2 >= 1 whenever this branch is taken)
+    if (hp[IX(d, k - 1, l)] > ZERO) {
+      double vel = d.f.wp[ik];
+      if (k == k1s) vel = 0.0;
+      const double s2 = sp[ik], s3 = sp[IX(d, k - 1, l)];
+      const double s4 = (k - 2 < 1 || hpp[IX(d, k - 2, l)] <= ZERO) ? s3 : sp[IX(d, k - 2, l)];
+      const double s1 = (hpp[IX(d, k + 1, l)] <= ZERO) ? s2 : sp[IX(d, k + 1, l)];
+      const double C_f = superbee(s1, s2, s3, s4, vel, 1.0);
+      const double delz = (hp[ik] + hp[IX(d, k - 1, l)]) / 2.;
+      d.f.Bth3[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / delz * C_f) * (s3 - s2) / 2.;
+    } else d.f.Bth3[ik] = 0.0;
+  }
+}
+
+// Horizontal-diffusion coefficient Bhaxpp/Bhaypp of column m at layer k (:2867-2877).
+__device__ __forceinline__ double bha(const Dev& d, const double* hvpp, double A, int m, int k) {
+  if (m == d.g.lm1 || k < d.g.k1 || k > NB(d.g.kmz, m)) return 0.0;
+  return A * hvpp[IX(d, k, m)];
+}
+
+// exsal's divergence (Bex) fused with imsal's vertical-diffusion tridiagonal solve.
+__global__ void k_exsal_imsal(Dev d) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
+  const int nw = kms - k1s + 1;
+  if (nw < 1) return;
+  const int lE = NB(d.g.lEC, l), lW = NB(d.g.lWC, l), lN = NB(d.g.lNC, l), lS = NB(d.g.lSC, l);
+  const double twodt1 = d.p.twodt * d.tz;
+  const double* sp = d.f.salpp;
+  double* sal = d.f.sal;
+  double* esc = d.scr;
+  auto bex = [&](int k) -> double {
+    const size_t ik = IX(d, k, l);
+    const double spc = sp[ik];
+    double v = d.f.hpp[ik] * spc / twodt1 - (d.f.Bth2[ik] - d.f.Bth2[IX(d, k, lW)]) / d.p.dx -
+               (d.f.Bth4[ik] - d.f.Bth4[IX(d, k, lS)]) / d.p.dy - (d.f.Bth3[ik] - d.f.Bth3[IX(d, k + 1, l)]);
+    if (d.p.ihd > 0) {
+      const double hd = (bha(d, d.f.hupp, d.p.Ax0, l, k) * (sp[IX(d, k, lE)] - spc) -
+                         bha(d, d.f.hupp, d.p.Ax0, lW, k) * (spc - sp[IX(d, k, lW)])) / d.p.dxdx +
+                        (bha(d, d.f.hvpp, d.p.Ay0, l, k) * (sp[IX(d, k, lN)] - spc) -
+                         bha(d, d.f.hvpp, d.p.Ay0, lS, k) * (spc - sp[IX(d, k, lS)])) / d.p.dydy;
+      v = v + hd;
+    }
+    return v;
+  };
+  // layer thickness at time n with the surface corrections (:3128-3132)
+  auto hn = [&](int k) -> double {
+    if (k == k1s) return twodt1 * d.f.wp[IX(d, k1s, l)] + d.f.hpp[IX(d, k1s, l)];
+    if (k == k1s + 1 && d.f.hpp[IX(d, k1s, l)] <= ZERO) return d.f.hpp[IX(d, k1s + 1, l)];
+    return d.f.h[IX(d, k, l)];
+  };
+  if (nw == 1) {
+    const double a2 = hn(k1s) / twodt1;
+    const double ds = bex(k1s) + d.f.HeatSource[IX(d, k1s, l)];
+    double v = ds / a2;
+    if (d.f.h[IX(d, k1s, l)] < 1.E-2) v = sp[IX(d, k1s, l)];
+    sal[IX(d, k1s, l)] = v;
+    return;
+  }
+  // trid1 forward sweep: e in scratch, f in sal
+  double hn_k = hn(k1s), e_prev = 0, f_prev = 0;
+  for (int k = k1s; k <= kms; ++k) {
+    const double hn_kp = (k < kms) ? hn(k + 1) : 0.0;
+    const double a3 = (k < kms) ? -d.f.Dv[IX(d, k + 1, l)] / (hn_k + hn_kp) * 2. : 0.0;
+    double a1 = 0.0;
+    if (k > k1s) {
+      const double hn_km = hn(k - 1);
+      a1 = -d.f.Dv[IX(d, k, l)] / (hn_km + hn_k) * 2.;
+    }
+    const double a2 = hn_k / twodt1 - a1 - a3;
+    const double ds = bex(k) + d.f.HeatSource[IX(d, k, l)];
+    const int kk = k - k1s + 1;
+    if (kk == 1) {
+      e_prev = -a3 / a2;
+      f_prev = ds / a2;
+      esc[IX(d, k, l)] = e_prev;
+      sal[IX(d, k, l)] = f_prev;
+    } else if (kk < nw) {
+      const double den = a2 + a1 * e_prev;
+      const double e = -a3 / den;
+      const double f = (ds - a1 * f_prev) / den;
+      esc[IX(d, k, l)] = e;
+      sal[IX(d, k, l)] = f;
+      e_prev = e; f_prev = f;
+    } else {
+      sal[IX(d, k, l)] = (ds - a1 * f_prev) / (a2 + a1 * e_prev);
+    }
+    hn_k = hn_kp;
+  }
+  double nxt = sal[IX(d, kms, l)];
+  for (int k = kms - 1; k >= k1s; --k) {
+    nxt = esc[IX(d, k, l)] * nxt + sal[IX(d, k, l)];
+    sal[IX(d, k, l)] = nxt;
+  }
+  const double top = sal[IX(d, k1s, l)];
+  for (int k = d.g.k1; k <= k1s - 1; ++k) sal[IX(d, k, l)] = top;
+  sal[IX(d, kms + 1, l)] = sal[IX(d, kms, l)];
+}
+
+// ------------------------------------------------------------- vel2 (layer_h + wetting)
+__global__ void k_vel2(Dev d) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const int kms = NB(d.g.kmz, l);
+  const double sl = d.s.s[l - 1];
+  for (int k = d.g.k1; k <= kms; ++k) {
+    double v = fmin(zl(d, k + 1), d.g.hhs[l - 1]) - fmax(zl(d, k), -sl);
+    if (v <= HMIN) v = ZERO;
+    d.f.h[IX(d, k, l)] = v;
+  }
+  if (ewet(d, l)) {
+    const int lE = NB(d.g.lEC, l);
+    const int kmx = min(kms, NB(d.g.kmz, lE));
+    const double sm = fmax(sl, d.s.s[lE - 1]);
+    for (int k = d.g.k1; k <= kmx; ++k) {
+      double v = fmin(zl(d, k + 1), d.g.hhu[l - 1]) - fmax(zl(d, k), -sm);
+      if (v <= HMIN) v = ZERO;
+      d.f.hu[IX(d, k, l)] = v;
+    }
+  }
+  if (nwet(d, l)) {
+    const int lN = NB(d.g.lNC, l);
+    const int kmy = min(kms, NB(d.g.kmz, lN));
+    const double sm = fmax(sl, d.s.s[lN - 1]);
+    for (int k = d.g.k1; k <= kmy; ++k) {
+      double v = fmin(zl(d, k + 1), d.g.hhv[l - 1]) - fmax(zl(d, k), -sm);
+      if (v <= HMIN) v = ZERO;
+      d.f.hv[IX(d, k, l)] = v;
+    }
+  }
+  if (ewet(d, l)) {
+    const int k = d.s.k1u[l - 1];
+    const double hkm = d.f.hu[IX(d, k - 1, l)];
+    if (hkm > ZERO) {
+      const double hk = d.f.hu[IX(d, k, l)];
+      const double ut = d.f.uh[IX(d, k, l)] / (hk + hkm);
+      d.f.uh[IX(d, k, l)] = ut * hk;
+      d.f.uh[IX(d, k - 1, l)] = ut * hkm;
+    }
+  }
+  if (nwet(d, l)) {
+    const int k = d.s.k1v[l - 1];
+    const double hkm = d.f.hv[IX(d, k - 1, l)];
+    if (hkm > ZERO) {
+      const double hk = d.f.hv[IX(d, k, l)];
+      const double vt = d.f.vh[IX(d, k, l)] / (hk + hkm);
+      d.f.vh[IX(d, k, l)] = vt * hk;
+      d.f.vh[IX(d, k - 1, l)] = vt * hkm;
+    }
+  }
+}
+
+// ------------------------------------------------------------- settrap / settrap2 / save
+// zeta at n+1/2 (settrap: rotate n -> n-1 first; settrap2: recompute only)
+__global__ void k_half_zeta(Dev d, int rotate) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  if (rotate) {
+    d.s.spp[l - 1] = d.s.sp[l - 1];
+    for (int k = 1; k <= d.g.km1; ++k) {
+      const size_t ik = IX(d, k, l);
+      d.f.hpp[ik] = d.f.hp[ik]; d.f.hupp[ik] = d.f.hup[ik]; d.f.hvpp[ik] = d.f.hvp[ik];
+    }
+  }
+  d.s.sp[l - 1] = 0.5 * (d.s.s[l - 1] + d.s.spp[l - 1]);
+}
+
+// velocity averaging to n+1/2 with the wet/dry surface corrections (:3481-3543, :4011-4079)
+__device__ void half_velocities(const Dev& d, int l, bool rotate) {
+  if (ewet(d, l)) {
+    const int kmx = min(NB(d.g.kmz, l), NB(d.g.kmz, NB(d.g.lEC, l)));
+    for (int k = d.g.k1; k <= kmx; ++k) {
+      const size_t ik = IX(d, k, l);
+      if (rotate) { d.f.uhpp[ik] = d.f.uhp[ik]; d.f.upp[ik] = d.f.up[ik]; }
+      const double hup = d.f.hup[ik];
+      if (hup > ZERO) { const double v = 0.5 * (d.f.uh[ik] + d.f.uhpp[ik]); d.f.uhp[ik] = v; d.f.up[ik] = v / hup; }
+      else { d.f.uhp[ik] = 0.0; d.f.up[ik] = 0.0; }
+    }
+    const int k = d.s.k1u[l - 1];
+    const size_t ik = IX(d, k, l);
+    if (d.f.hu[IX(d, k - 1, l)] > ZERO) {
+      d.f.uhp[ik] = d.f.uhp[ik] + d.f.uh[IX(d, k - 1, l)] / 2.;
+      d.f.up[ik] = d.f.uhp[ik] / d.f.hup[ik];
+    }
+    if (d.f.hupp[IX(d, k - 1, l)] > ZERO) {
+      d.f.uhp[ik] = d.f.uhp[ik] + d.f.uhpp[IX(d, k - 1, l)] / 2.;
+      d.f.up[ik] = d.f.uhp[ik] / d.f.hup[ik];
+    }
+  }
+  if (nwet(d, l)) {
+    const int kmy = min(NB(d.g.kmz, l), NB(d.g.kmz, NB(d.g.lNC, l)));
+    for (int k = d.g.k1; k <= kmy; ++k) {
+      const size_t ik = IX(d, k, l);
+      if (rotate) { d.f.vhpp[ik] = d.f.vhp[ik]; d.f.vpp[ik] = d.f.vp[ik]; }
+      const double hvp = d.f.hvp[ik];
+      if (hvp > ZERO) { const double v = 0.5 * (d.f.vh[ik] + d.f.vhpp[ik]); d.f.vhp[ik] = v; d.f.vp[ik] = v / hvp; }
+      else { d.f.vhp[ik] = 0.0; d.f.vp[ik] = 0.0; }
+    }
+    const int k = d.s.k1v[l - 1];
+    const size_t ik = IX(d, k, l);
+    if (d.f.hv[IX(d, k - 1, l)] > ZERO) {
+      d.f.vhp[ik] = d.f.vhp[ik] + d.f.vh[IX(d, k - 1, l)] / 2.;
+      d.f.vp[ik] = d.f.vhp[ik] / d.f.hvp[ik];
+    }
+    if (d.f.hvpp[IX(d, k - 1, l)] > ZERO) {
+      d.f.vhp[ik] = d.f.vhp[ik] + d.f.vhpp[IX(d, k - 1, l)] / 2.;
+      d.f.vp[ik] = d.f.vhp[ik] / d.f.hvp[ik];
+    }
+  }
+}
+
+// settrap / settrap2 body after the zeta update: layer_hp2, TopLayerIndexp2, scalars at n+1/2
+// with densty_s, velocities at n+1/2.
+__global__ void k_half_level(Dev d, int rotate) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  layer_hp2_col(d, l);
+  top_index_col(d, l);
+  const int kms = NB(d.g.kmz, l);
+  for (int k = d.g.k1; k <= kms; ++k) {
+    const size_t ik = IX(d, k, l);
+    const double z = zmid(d, k, d.f.hp[ik]);
+    if (rotate) d.f.salpp[ik] = d.f.salp[ik];
+    const double sp = (d.f.sal[ik] + d.f.salpp[ik]) / 2.;
+    d.f.salp[ik] = sp;
+    d.f.rhop[ik] = densty_s(sp, 0.00004, z) - 1000.;
+  }
+  half_velocities(d, l, rotate != 0);
+}
+
+// save (istep = 2 after a trapezoidal step, 1 after a leapfrog step)
+__global__ void k_save(Dev d, int istep) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  if (istep == 1) d.s.spp[l - 1] = d.s.sp[l - 1];
+  d.s.sp[l - 1] = d.s.s[l - 1];
+  for (int k = 1; k <= d.g.km1; ++k) {
+    const size_t ik = IX(d, k, l);
+    if (istep == 1) { d.f.hpp[ik] = d.f.hp[ik]; d.f.hupp[ik] = d.f.hup[ik]; d.f.hvpp[ik] = d.f.hvp[ik]; }
+    d.f.hp[ik] = d.f.h[ik]; d.f.hup[ik] = d.f.hu[ik]; d.f.hvp[ik] = d.f.hv[ik];
+  }
+  top_index_col(d, l);
+  for (int k = d.g.k1; k <= d.g.km; ++k) {
+    const size_t ik = IX(d, k, l);
+    const double z = zmid(d, k, d.f.hp[ik]);
+    if (istep == 1) d.f.salpp[ik] = d.f.salp[ik];
+    d.f.salp[ik] = d.f.sal[ik];
+    d.f.rhop[ik] = densty_s(d.f.salp[ik], 0.00004, z) - 1000.;
+    if (istep == 1) {
+      d.f.uhpp[ik] = d.f.uhp[ik]; d.f.vhpp[ik] = d.f.vhp[ik]; d.f.upp[ik] = d.f.up[ik]; d.f.vpp[ik] = d.f.vp[ik];
+    }
+    const double hup = d.f.hup[ik];
+    if (hup > ZERO) { const double v = d.f.uh[ik]; d.f.uhp[ik] = v; d.f.up[ik] = v / hup; }
+    else { d.f.uhp[ik] = 0.0; d.f.up[ik] = 0.0; }
+    const double hvp = d.f.hvp[ik];
+    if (hvp > ZERO) { const double v = d.f.vh[ik]; d.f.vhp[ik] = v; d.f.vp[ik] = v / hvp; }
+    else { d.f.vhp[ik] = 0.0; d.f.vp[ik] = 0.0; }
+  }
+}
+
+// Initial density anomaly on every column incl. the sentinel (si3d_procedures.f90:363-373)
+__global__ void k_density_init(Dev d) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm1) return;
+  for (int k = d.g.k1; k <= d.g.km1; ++k) {
+    const size_t ik = IX(d, k, l);
+    d.f.rhop[ik] = densty_s(d.f.salp[ik], 0.00004, zmid(d, k, d.f.hp[ik])) - 1000.;
+  }
+}
+
+// Batched two-right-hand-side Thomas solver (trid) for the C-ABI unit entry point.
+__global__ void k_column_tridiag(int n, int nsys, const double* a, const double* b, const double* c,
+                                 const double* g, const double* r, double* ag, double* ar, double* c1) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= nsys) return;
+  // element k of system s at k*nsys + s (layer-major, coalesced); the host transposes
+  double cp = 0, dp = 0, ep = 0;
+  for (int k = 0; k < n; ++k) {
+    const size_t i = (size_t)k * nsys + s;
+    double cv, dv, ev;
+    if (k == 0) { cv = c[i] / b[i]; dv = g[i] / b[i]; ev = r[i] / b[i]; }
+    else {
+      const double den = b[i] - a[i] * cp;
+      cv = c[i] / den; dv = (g[i] - a[i] * dp) / den; ev = (r[i] - a[i] * ep) / den;
+    }
+    c1[i] = cv; ag[i] = dv; ar[i] = ev;
+    cp = cv; dp = dv; ep = ev;
+  }
+  for (int k = n - 2; k >= 0; --k) {
+    const size_t i = (size_t)k * nsys + s;
+    dp = ag[i] - c1[i] * dp;
+    ep = ar[i] - c1[i] * ep;
+    ag[i] = dp; ar[i] = ep;
+  }
+}
+
+}  // namespace
+
+static inline int grid_of(int n) { return (n + TB - 1) / TB; }
+
+void launch_slayer_h(const Dev& d, cudaStream_t st) { k_slayer_h<<<grid_of(d.g.lm), TB, 0, st>>>(d); }
+
+void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cudaStream_t st) {
+  if (nce > 0) k_vel_uv<1><<<grid_of(nce), TB, 0, st>>>(d, ce, nce);
+  if (ncn > 0) k_vel_uv<2><<<grid_of(ncn), TB, 0, st>>>(d, cn, ncn);
+  k_cont1<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+}
+
+void launch_exsal_imsal(const Dev& d, cudaStream_t st) {
+  k_exsal_flux<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+  k_exsal_imsal<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+}
+
+void launch_vel2(const Dev& d, cudaStream_t st) { k_vel2<<<grid_of(d.g.lm), TB, 0, st>>>(d); }
+
+void launch_settrap(const Dev& d, cudaStream_t st) {
+  k_half_zeta<<<grid_of(d.g.lm), TB, 0, st>>>(d, 1);
+  k_half_level<<<grid_of(d.g.lm), TB, 0, st>>>(d, 1);
+  k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+}
+
+void launch_settrap2(const Dev& d, cudaStream_t st) {
+  k_half_zeta<<<grid_of(d.g.lm), TB, 0, st>>>(d, 0);
+  k_half_level<<<grid_of(d.g.lm), TB, 0, st>>>(d, 0);
+  k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+}
+
+void launch_save(const Dev& d, int istep, cudaStream_t st) {
+  k_save<<<grid_of(d.g.lm), TB, 0, st>>>(d, istep);
+  k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+}
+
+void launch_density_init(const Dev& d, cudaStream_t st) { k_density_init<<<grid_of(d.g.lm1), TB, 0, st>>>(d); }
+
+void launch_column_tridiag(int n, int nsys, const double* a, const double* b, const double* c, const double* g,
+                           const double* r, double* ag, double* ar, double* scratch, cudaStream_t st) {
+  k_column_tridiag<<<grid_of(nsys), TB, 0, st>>>(n, nsys, a, b, c, g, r, ag, ar, scratch);
+}
+
+}  // namespace si3d

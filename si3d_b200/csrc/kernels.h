@@ -1,0 +1,50 @@
+// Declarations shared by the stage kernels and the C-ABI orchestration (si3d_gpu.cu).
+#pragma once
+#include "common.cuh"
+
+namespace si3d {
+
+// One colour of the red-black ordered zeta system (see k_zeta.cu).
+struct PcgColor {
+  int n;                 // nodes of this colour; arrays hold n + 1 entries (entry n = 0)
+  const int* l;          // [n] reference column index (1-based)
+  const int4* nbr;       // [n] W, S, N, E as indices into the other colour (absent -> other.n)
+  double *sx, *sy, *rhs, *u, *r, *z, *p, *q, *dinv, *diag, *rs;
+};
+
+// Device-resident CG scalars (NSPCG common blocks itcom1/itcom3 that itcg and pstops use).
+struct PcgScal {
+  double alpha, beta, alphao, rzdot, dkm1, pap, bnorm, stptst, zeta, srelpr, udnm, emin, emax;
+  int in, itmax, ntest, done, ier, q1, hist_cap, negpiv;
+  unsigned int cnt[4];
+};
+
+struct PcgDev {
+  PcgColor R, B;
+  PcgScal* sc;
+  double *part0, *part1, *part2, *part3;
+  double *hist_alpha, *hist_beta;
+};
+
+void launch_momentum(const Dev& d, int ieq, const int* cols, int ncols, cudaStream_t st);
+void launch_matcon(const Dev& d, cudaStream_t st);
+
+void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, int* negpiv, cudaStream_t st);
+void pcg_iteration(const PcgDev& P, cudaStream_t st);
+void pcg_finish(const Dev& d, const PcgDev& P, cudaStream_t st);
+int pcg_max_blocks(int nR, int nB);
+
+void launch_slayer_h(const Dev& d, cudaStream_t st);
+void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cudaStream_t st);
+void launch_exsal_imsal(const Dev& d, cudaStream_t st);
+void launch_vel2(const Dev& d, cudaStream_t st);
+void launch_settrap(const Dev& d, cudaStream_t st);
+void launch_settrap2(const Dev& d, cudaStream_t st);
+void launch_save(const Dev& d, int istep, cudaStream_t st);
+
+void launch_density_init(const Dev& d, cudaStream_t st);
+
+void launch_column_tridiag(int n, int nsys, const double* a, const double* b, const double* c, const double* g,
+                           const double* r, double* ag, double* ar, double* scratch, cudaStream_t st);
+
+}  // namespace si3d

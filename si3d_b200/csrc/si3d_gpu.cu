@@ -1,0 +1,858 @@
+// C-ABI implementation (include/si3d_gpu.h): handle management, device state, layout
+// transposes at the boundary, and the stage sequence of fd / settrap / settrap2 / save.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/si3d_gpu.h"
+#include "common.cuh"
+#include "kernels.h"
+
+using namespace si3d;
+
+namespace {
+
+#define CK(x)                                     \
+  do {                                            \
+    cudaError_t e_ = (x);                         \
+    if (e_ != cudaSuccess) return cuda_fail(e_);  \
+  } while (0)
+
+thread_local std::string g_last_cuda;
+int cuda_fail(cudaError_t e) {
+  g_last_cuda = cudaGetErrorString(e);
+  return SI3D_ECUDA;
+}
+
+// ---------------------------------------------------------------------------- layout kernels
+// (km1, lm1) column-major  <->  layer-major with pitch P
+__global__ void k_colmajor_to_layer(const double* __restrict__ src, double* __restrict__ dst, int km1, int lm1, int P) {
+  __shared__ double tile[32][33];
+  const int l0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int l = l0 + r, k = k0 + threadIdx.x;
+    if (l < lm1 && k < km1) tile[r][threadIdx.x] = src[(size_t)l * km1 + k];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int k = k0 + r, l = l0 + threadIdx.x;
+    if (l < lm1 && k < km1) dst[(size_t)k * P + l] = tile[threadIdx.x][r];
+  }
+}
+
+__global__ void k_layer_to_colmajor(const double* __restrict__ src, double* __restrict__ dst, int km1, int lm1, int P) {
+  __shared__ double tile[32][33];
+  const int l0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int k = k0 + r, l = l0 + threadIdx.x;
+    if (l < lm1 && k < km1) tile[r][threadIdx.x] = src[(size_t)k * P + l];
+  }
+  __syncthreads();
+  for (int r = threadIdx.y; r < 32; r += 8) {
+    const int l = l0 + r, k = k0 + threadIdx.x;
+    if (l < lm1 && k < km1) dst[(size_t)l * km1 + k] = tile[threadIdx.x][r];
+  }
+}
+
+// ---------------------------------------------------------------------------- handle context
+struct Ctx {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  Dev d{};
+  si3d_params prm{};
+  int lm = 0, lm1 = 0, km1 = 0, P = 0;
+  std::vector<void*> allocs;
+  // face-column lists (id_columnCE / id_columnCN)
+  int* ce = nullptr;
+  int* cn = nullptr;
+  int nce = 0, ncn = 0;
+  // red-black zeta system
+  PcgDev pcg{};
+  PcgScal* h_sc = nullptr;  // pinned
+  double* h_hist = nullptr; // pinned, 2 x itmax
+  int last_iters = 8;
+  double* dz = nullptr;     // learned warm-start increment (device, lm1)
+  bool dz_set = false;
+  double* staging = nullptr;  // device staging for transposes (km1 * lm1)
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
+  ~Ctx() {
+    if (st) cudaStreamSynchronize(st);
+    for (void* p : allocs) cudaFree(p);
+    if (h_sc) cudaFreeHost(h_sc);
+    if (h_hist) cudaFreeHost(h_hist);
+    for (cudaEvent_t e : {ev0, ev1, evp0, evp1}) if (e) cudaEventDestroy(e);
+    if (st) cudaStreamDestroy(st);
+  }
+  template <class T>
+  int alloc(T** p, size_t n) {
+    void* q = nullptr;
+    cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) { g_last_cuda = cudaGetErrorString(e); return SI3D_ENOMEM; }
+    allocs.push_back(q);
+    e = cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T));
+    if (e != cudaSuccess) { g_last_cuda = cudaGetErrorString(e); return SI3D_ECUDA; }
+    *p = static_cast<T*>(q);
+    return 0;
+  }
+};
+
+std::mutex g_mu;
+std::vector<Ctx*> g_ctx;
+
+Ctx* get(int h) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (h < 0 || h >= (int)g_ctx.size()) return nullptr;
+  return g_ctx[h];
+}
+
+double* f3ptr(Ctx* c, const std::string& n) {
+  Fields3& f = c->d.f;
+  static const std::map<std::string, double* Fields3::*> t = {
+      {"uh", &Fields3::uh},     {"uhp", &Fields3::uhp},   {"uhpp", &Fields3::uhpp}, {"up", &Fields3::up},
+      {"upp", &Fields3::upp},   {"hu", &Fields3::hu},     {"hup", &Fields3::hup},   {"hupp", &Fields3::hupp},
+      {"agx", &Fields3::agx},   {"arx", &Fields3::arx},   {"vh", &Fields3::vh},     {"vhp", &Fields3::vhp},
+      {"vhpp", &Fields3::vhpp}, {"vp", &Fields3::vp},     {"vpp", &Fields3::vpp},   {"hv", &Fields3::hv},
+      {"hvp", &Fields3::hvp},   {"hvpp", &Fields3::hvpp}, {"agy", &Fields3::agy},   {"ary", &Fields3::ary},
+      {"h", &Fields3::h},       {"hp", &Fields3::hp},     {"hpp", &Fields3::hpp},   {"sal", &Fields3::sal},
+      {"salp", &Fields3::salp}, {"salpp", &Fields3::salpp}, {"rhop", &Fields3::rhop}, {"Av", &Fields3::Av},
+      {"Dv", &Fields3::Dv},     {"wp", &Fields3::wp},     {"HeatSource", &Fields3::HeatSource},
+      {"Bth2", &Fields3::Bth2}, {"Bth3", &Fields3::Bth3}, {"Bth4", &Fields3::Bth4}};
+  auto it = t.find(n);
+  return it == t.end() ? nullptr : f.*(it->second);
+}
+
+double* f2ptr(Ctx* c, const std::string& n) {
+  Fields2& s = c->d.s;
+  static const std::map<std::string, double* Fields2::*> t = {
+      {"s", &Fields2::s},       {"sp", &Fields2::sp},     {"spp", &Fields2::spp},   {"eagx", &Fields2::eagx},
+      {"earx", &Fields2::earx}, {"eagy", &Fields2::eagy}, {"eary", &Fields2::eary}, {"sx", &Fields2::sx},
+      {"sy", &Fields2::sy},     {"dd", &Fields2::dd},     {"qq", &Fields2::qq},     {"rr", &Fields2::rr},
+      {"uair", &Fields2::uair}, {"vair", &Fields2::vair}, {"cdw", &Fields2::cdw}};
+  auto it = t.find(n);
+  return it == t.end() ? nullptr : s.*(it->second);
+}
+
+int* iptr(Ctx* c, const std::string& n) {
+  if (n == "k1z") return c->d.s.k1z;
+  if (n == "k1u") return c->d.s.k1u;
+  if (n == "k1v") return c->d.s.k1v;
+  return nullptr;
+}
+
+// Red-black colouring of the wet-column graph, as prbndx does it (nspcg.f:25337-25460): the
+// lowest unlabelled column of each connected component is red and colours alternate.
+void colour_columns(int lm, const int* lEC, const int* lWC, const int* lNC, const int* lSC, std::vector<int>& col) {
+  const int lm1 = lm + 1;
+  col.assign(lm, 0);
+  std::vector<int> stack;
+  stack.reserve(lm);
+  for (int first = 1; first <= lm; ++first) {
+    if (col[first - 1]) continue;
+    col[first - 1] = 1;
+    stack.clear();
+    stack.push_back(first);
+    for (size_t nx = 0; nx < stack.size(); ++nx) {
+      const int k = stack[nx];
+      const int nb[4] = {lWC[k - 1], lSC[k - 1], lNC[k - 1], lEC[k - 1]};
+      for (int m : nb) {
+        if (m == lm1) continue;
+        if (!col[m - 1]) { col[m - 1] = 3 - col[k - 1]; stack.push_back(m); }
+      }
+    }
+  }
+}
+
+int build_pcg(Ctx* c, const si3d_grid* g) {
+  const int lm = g->lm, lm1 = lm + 1;
+  std::vector<int> col;
+  colour_columns(lm, g->lEC, g->lWC, g->lNC, g->lSC, col);
+  std::vector<int> idx(lm + 2, -1), lr, lb;
+  for (int l = 1; l <= lm; ++l) {
+    if (col[l - 1] == 1) { idx[l] = (int)lr.size(); lr.push_back(l); }
+    else { idx[l] = (int)lb.size(); lb.push_back(l); }
+  }
+  const int nR = (int)lr.size(), nB = (int)lb.size();
+  auto nbrs = [&](const std::vector<int>& L, int nother) {
+    std::vector<int4> v(L.size());
+    for (size_t i = 0; i < L.size(); ++i) {
+      const int l = L[i];
+      auto m = [&](int q) { return q == lm1 ? nother : idx[q]; };
+      v[i] = make_int4(m(g->lWC[l - 1]), m(g->lSC[l - 1]), m(g->lNC[l - 1]), m(g->lEC[l - 1]));
+    }
+    return v;
+  };
+  std::vector<int4> nbR = nbrs(lr, nB), nbB = nbrs(lb, nR);
+  // a neighbour must carry the other colour (5-point graphs are bipartite)
+  for (int l = 1; l <= lm; ++l) {
+    const int nb[4] = {g->lWC[l - 1], g->lSC[l - 1], g->lNC[l - 1], g->lEC[l - 1]};
+    for (int m : nb) if (m != lm1 && col[m - 1] == col[l - 1]) return SI3D_EDIMS;
+  }
+  PcgDev& P = c->pcg;
+  int rc = 0;
+  for (int which = 0; which < 2 && !rc; ++which) {
+    PcgColor& C = which ? P.B : P.R;
+    const std::vector<int>& L = which ? lb : lr;
+    const std::vector<int4>& NBv = which ? nbB : nbR;
+    C.n = (int)L.size();
+    int* dl = nullptr;
+    int4* dn = nullptr;
+    rc |= c->alloc(&dl, L.size());
+    rc |= c->alloc(&dn, L.size());
+    if (rc) break;
+    if (!L.empty()) {
+      CK(cudaMemcpy(dl, L.data(), L.size() * sizeof(int), cudaMemcpyHostToDevice));
+      CK(cudaMemcpy(dn, NBv.data(), NBv.size() * sizeof(int4), cudaMemcpyHostToDevice));
+    }
+    C.l = dl;
+    C.nbr = dn;
+    const size_t n1 = L.size() + 1;
+    for (double** p : {&C.sx, &C.sy, &C.rhs, &C.u, &C.r, &C.z, &C.p, &C.q, &C.dinv, &C.diag, &C.rs})
+      rc |= c->alloc(p, n1);
+  }
+  if (rc) return rc;
+  const int nblk = pcg_max_blocks(nR, nB);
+  for (double** p : {&P.part0, &P.part1, &P.part2, &P.part3}) rc |= c->alloc(p, nblk);
+  rc |= c->alloc(&P.sc, 1);
+  const int cap = std::max(c->prm.pcg_itmax, 1) + 1;
+  rc |= c->alloc(&P.hist_alpha, cap);
+  rc |= c->alloc(&P.hist_beta, cap);
+  if (rc) return rc;
+  CK(cudaMallocHost(&c->h_sc, sizeof(PcgScal)));
+  CK(cudaMallocHost(&c->h_hist, sizeof(double) * 2 * cap));
+  return 0;
+}
+
+// chgcon/eigvss/zbrent/determ (nspcg.f:16499-16620, :17201, :32976, :16926) evaluated after the
+// solve from the recorded alpha/beta sequence: with stopping test 5 the estimates do not feed
+// back into the iteration, so they are reported rather than computed on the critical path.
+double determ(int n, const std::vector<double>& tri, double x) {
+  auto T = [&](int r, int cc) { return tri[(size_t)(cc - 1) * 2 + (r - 1)]; };
+  double d2 = T(1, n) - x;
+  double d1 = d2 * (T(1, n - 1) - x) - T(2, n);
+  for (int l = n - 1; l >= 2; --l) { const double d3 = d2; d2 = d1; d1 = (T(1, l - 1) - x) * d2 - d3 * T(2, l); }
+  return d1;
+}
+
+void zbrent(int n, const std::vector<double>& tri, int nsig, double& aa, double& bb, int maxfn, int& ier) {
+  double a = aa, b = bb, t = std::pow(0.1, nsig), fa = determ(n, tri, a), fb = determ(n, tri, b);
+  double c = 0, fc = 0, d = 0, e = 0, s = b, p, q, r, rm, tol, temp;
+  int ic = 2;
+  if (fa * fb > 0.0) { ier = 4; return; }
+  for (;;) {
+    c = a; fc = fa; d = b - c; e = d;
+    for (;;) {
+      if (std::fabs(fc) < std::fabs(fb)) { a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
+      tol = t * std::max(std::fabs(b), 0.1);
+      rm = (c - b) / 2.0;
+      if (std::fabs(fb) <= 0.0 || std::fabs(c - b) <= tol) { aa = c; bb = b; return; }
+      if (ic >= maxfn) { ier = 3; aa = c; bb = b; return; }
+      bool bisect = std::fabs(e) < tol || std::fabs(fa) <= std::fabs(fb);
+      if (!bisect) {
+        s = fb / fa;
+        if (a == c) { p = (c - b) * s; q = 1.0 - s; }
+        else {
+          q = fa / fc; r = fb / fc;
+          const double rone = r - 1.0;
+          p = s * ((c - b) * q * (q - r) - (b - a) * rone);
+          q = (q - 1.0) * rone * (s - 1.0);
+        }
+        if (p > 0.0) q = -q;
+        if (p < 0.0) p = -p;
+        s = e; e = d;
+        if (p + p >= 3.0 * rm * q || p + p >= std::fabs(s * q)) bisect = true;
+        else d = p / q;
+      }
+      if (bisect) { e = rm; d = e; }
+      a = b; fa = fb; temp = d;
+      if (std::fabs(temp) <= tol / 2.0) temp = std::copysign(tol / 2.0, rm);
+      b = b + temp; s = b; fb = determ(n, tri, s); ic = ic + 1;
+      if (!(fb * fc <= 0.0)) break;
+    }
+  }
+}
+
+void eigen_estimates(const double* al, const double* be, int n, double zeta, int itmax, double& emin, double& emax) {
+  emax = 2.0; emin = 1.0;
+  bool maxadp = true, minadp = true;
+  std::vector<double> tri((size_t)2 * (n + 2), 0.0);
+  auto T = [&](int r, int cc) -> double& { return tri[(size_t)(cc - 1) * 2 + (r - 1)]; };
+  double tl1 = 0, tl2 = 0, bl1 = 0, bl2 = 0, alphao = 0;
+  int ier = 0;
+  const int nsig = std::max((int)(-std::log10(std::fabs(zeta))), 4), maxfn = std::max(itmax, 50);
+  for (int ip = 0; ip < n; ++ip) {
+    const double alpha = al[ip], beta = be[ip];
+    if (ip == 0) { T(1, 1) = 1.0 / alpha; T(2, 1) = 0.0; emax = emin = 1.0 / alpha; alphao = alpha; continue; }
+    const double t1 = 1.0 / alpha + beta / alphao, t2 = beta / (alphao * alphao), tsqr = std::sqrt(t2);
+    T(1, ip + 1) = t1; T(2, ip + 1) = t2;
+    if (ip == 1) {
+      tl1 = T(1, 1) + tsqr; tl2 = t1 + tsqr; bl1 = T(1, 1) - tsqr; bl2 = t1 - tsqr;
+      const double t3 = T(1, 1) + t1, t4 = std::sqrt((t1 - T(1, 1)) * (t1 - T(1, 1)) + 4.0 * t2);
+      if (maxadp) emax = (t3 + t4) / 2.0;
+      if (minadp) emin = (t3 - t4) / 2.0;
+      alphao = alpha;
+      continue;
+    }
+    if (maxadp) {
+      tl1 = std::max(tl1, tl2 + tsqr); tl2 = t1 + tsqr;
+      double a = emax, b = std::max(tl1, tl2);
+      const double emaxo = emax;
+      zbrent(ip + 1, tri, nsig, a, b, maxfn, ier);
+      if (ier != 3 && ier != 4) { emax = std::min(a, b); if (std::fabs(emax - emaxo) < emax * zeta) maxadp = false; }
+      else maxadp = false;
+    }
+    if (minadp) {
+      bl1 = std::min(bl1, bl2 - tsqr); bl2 = t1 - tsqr;
+      double a = std::max(0.0, std::min(bl1, bl2)), b = emin;
+      const double emino = emin;
+      zbrent(ip + 1, tri, nsig, a, b, maxfn, ier);
+      if (ier != 3 && ier != 4) { emin = std::max(a, b); if (std::fabs(emin - emino) < emin * zeta) minadp = false; }
+      else minadp = false;
+    }
+    alphao = alpha;
+    if (!maxadp && !minadp) break;
+  }
+}
+
+// One zeta solve on the device (SolverSparse's call of nspcg, si3d_procedures.f90:1986-2003).
+int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
+  const si3d_params& p = c->prm;
+  PcgScal init{};
+  init.zeta = p.pcg_tol;
+  init.srelpr = p.srelpr;
+  int ier = 0;
+  if (init.zeta < 500.0 * init.srelpr) { ier = 2; init.zeta = 500.0 * init.srelpr; }  // echall clamp
+  init.itmax = p.pcg_itmax;
+  init.ntest = p.pcg_test;
+  init.emax = 2.0; init.emin = 1.0; init.udnm = 1.0;
+  init.hist_cap = p.pcg_itmax + 1;
+  *c->h_sc = init;
+  CK(cudaMemcpyAsync(c->pcg.sc, c->h_sc, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
+  const int x0 = (p.x0_mode == SI3D_X0_LEARNED && !c->dz_set) ? SI3D_X0_PREV : p.x0_mode;
+  pcg_setup(c->d, c->pcg, x0, c->dz, &c->pcg.sc->negpiv, c->st);
+  CK(cudaGetLastError());
+  // run iterations in batches; every kernel returns at once after convergence
+  int batch = std::max(1, std::min(c->last_iters - 1, 256));
+  int launched = 0;
+  for (;;) {
+    for (int i = 0; i < batch; ++i) pcg_iteration(c->pcg, c->st);
+    launched += batch;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (c->h_sc->done) break;
+    if (launched > p.pcg_itmax + 8) return SI3D_ETIMEOUT;  // cannot happen: itcg stops at itmax
+    batch = 4;
+  }
+  pcg_finish(c->d, c->pcg, c->st);
+  CK(cudaGetLastError());
+  const PcgScal& S = *c->h_sc;
+  if (S.negpiv & 2) ier = -12;
+  else if (S.ier != 0) ier = S.ier;
+  else if ((S.negpiv & 1) && ier == 0) ier = 5;
+  *iters = S.in;
+  *relres = S.stptst;
+  *ier_out = ier;
+  c->last_iters = std::max(S.in, 1);
+  return 0;
+}
+
+int fd_impl(Ctx* c, int istep, si3d_step_stats* st) {
+  Dev& d = c->d;
+  d.tz = 1.0 / istep;
+  // surfbc CASE(0) is a constant per-column wind set by the host (uair/vair/cdw fields)
+  launch_momentum(d, 1, c->ce, c->nce, c->st);
+  launch_momentum(d, 2, c->cn, c->ncn, c->st);
+  launch_matcon(d, c->st);
+  CK(cudaGetLastError());
+  if (st) CK(cudaEventRecord(c->evp0, c->st));
+  int iters = 0, ier = 0;
+  double rr = 0;
+  int rc = solve(c, &iters, &rr, &ier);
+  if (rc) return rc;
+  if (st) CK(cudaEventRecord(c->evp1, c->st));
+  if (st) {
+    if (st->nsolves < 24) {
+      st->iters[st->nsolves] = iters; st->relres[st->nsolves] = rr; st->ier[st->nsolves] = ier;
+    }
+    st->nsolves++;
+    st->total_iters += iters;
+  }
+  if (ier < 0) return ier;
+  launch_slayer_h(d, c->st);
+  launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st);
+  if (c->prm.isal != 0) launch_exsal_imsal(d, c->st);
+  launch_vel2(d, c->st);
+  CK(cudaGetLastError());
+  if (st) {
+    CK(cudaEventSynchronize(c->evp1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->evp0, c->evp1));
+    st->ms_pcg += ms;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* si3d_gpu_strerror(int code) {
+  switch (code) {
+    case SI3D_OK: return "ok";
+    case 1: return "zeta solve: itmax reached";
+    case 2: return "zeta solve: tolerance clamped to 500*srelpr";
+    case 3: return "zeta solve: eigenvalue estimate did not converge";
+    case 4: return "zeta solve: eigenvalue bracket failed";
+    case 5: return "zeta solve: negative pivot in the MIC factorisation";
+    case -6: return "zeta solve: (p, Ap) <= 0";
+    case -7: return "zeta solve: (r, z) <= 0";
+    case -12: return "zeta solve: zero pivot in the MIC factorisation";
+    case SI3D_ECUDA: return g_last_cuda.empty() ? "CUDA error" : g_last_cuda.c_str();
+    case SI3D_EDIMS: return "bad dimensions or arguments";
+    case SI3D_EHANDLE: return "unknown handle";
+    case SI3D_ENAME: return "unknown field name";
+    case SI3D_ENAN: return "non-finite value";
+    case SI3D_ETIMEOUT: return "bounded device wait gave up";
+    case SI3D_ENOMEM: return "device allocation failed";
+    case SI3D_ENODEV: return "no sm_100 CUDA device";
+    default: return "unknown error";
+  }
+}
+
+int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* handle) {
+  if (!g || !prm || !handle) return SI3D_EDIMS;
+  if (g->lm < 1 || g->km1 < 3 || g->km1 > SI3D_MAXK || g->k1 != 2) return SI3D_EDIMS;
+  if (prm->itrmom != 1 || prm->ihd > 1 || prm->pcg_itmax < 1 || (prm->pcg_test != 5 && prm->pcg_test != 2))
+    return SI3D_EDIMS;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device) return SI3D_ENODEV;
+  cudaDeviceProp pr;
+  CK(cudaGetDeviceProperties(&pr, device));
+  if (pr.major < 10) return SI3D_ENODEV;
+  CK(cudaSetDevice(device));
+  Ctx* c = new Ctx();
+  c->device = device;
+  c->prm = *prm;
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return SI3D_ECUDA; }
+  for (cudaEvent_t* e : {&c->ev0, &c->ev1, &c->evp0, &c->evp1}) cudaEventCreate(e);
+  const int lm = g->lm, lm1 = lm + 1, km1 = g->km1;
+  const int P = (lm1 + 31) / 32 * 32;
+  c->lm = lm; c->lm1 = lm1; c->km1 = km1; c->P = P;
+  Dev& d = c->d;
+  d.g.lm = lm; d.g.lm1 = lm1; d.g.km1 = km1; d.g.km = km1 - 1; d.g.k1 = g->k1; d.g.P = P;
+  int rc = 0;
+  // maps, padded to P; the sentinel column lm1 points to itself
+  auto up_int = [&](const int* src, int nsrc, int fill) -> const int* {
+    std::vector<int> v(P, fill);
+    for (int i = 0; i < nsrc; ++i) v[i] = src[i];
+    int* p = nullptr;
+    rc |= c->alloc(&p, P);
+    if (!rc) cudaMemcpy(p, v.data(), P * sizeof(int), cudaMemcpyHostToDevice);
+    return p;
+  };
+  auto up_dbl = [&](const double* src, int nsrc) -> const double* {
+    std::vector<double> v(P, 0.0);
+    for (int i = 0; i < nsrc; ++i) v[i] = src[i];
+    double* p = nullptr;
+    rc |= c->alloc(&p, P);
+    if (!rc) cudaMemcpy(p, v.data(), P * sizeof(double), cudaMemcpyHostToDevice);
+    return p;
+  };
+  d.g.lEC = up_int(g->lEC, lm, lm1);
+  d.g.lWC = up_int(g->lWC, lm, lm1);
+  d.g.lNC = up_int(g->lNC, lm, lm1);
+  d.g.lSC = up_int(g->lSC, lm, lm1);
+  d.g.kmz = up_int(g->kmz, lm1, km1);
+  d.g.hhs = up_dbl(g->hhs, lm1);
+  d.g.hhu = up_dbl(g->hhu, lm1);
+  d.g.hhv = up_dbl(g->hhv, lm1);
+  {
+    double* z = nullptr;
+    rc |= c->alloc(&z, km1);
+    if (!rc) cudaMemcpy(z, g->zlevel, km1 * sizeof(double), cudaMemcpyHostToDevice);
+    d.g.zlevel = z;
+  }
+  // parameters (si3d_utils.f90:291-306)
+  Params& p = d.p;
+  p.dt = prm->dt; p.dx = prm->dx; p.dy = prm->dy; p.twodt = 2. * p.dt; p.dtdx = p.dt / p.dx; p.dtdy = p.dt / p.dy;
+  p.gdtdx = G_GRAV * p.dtdx; p.gdtdy = G_GRAV * p.dtdy; p.gdt2dx2 = p.gdtdx * p.dtdx; p.gdt2dy2 = p.gdtdy * p.dtdy;
+  p.twodx = 2. * p.dx; p.twody = 2. * p.dy; p.fourdx = 2. * p.twodx; p.fourdy = 2. * p.twody;
+  p.dxdx = p.dx * p.dx; p.dydy = p.dy * p.dy;
+  p.Av0 = prm->Av0; p.Dv0 = prm->Dv0; p.Ax0 = prm->Ax0; p.Ay0 = prm->Ay0; p.f = prm->f; p.theta = prm->theta;
+  p.cd = prm->cd; p.cw = prm->cw;
+  p.iadv = prm->iadv; p.itrmom = prm->itrmom; p.ihd = prm->ihd; p.ibc = prm->ibc; p.isal = prm->isal;
+  // state
+  const size_t n3 = (size_t)km1 * P;
+  Fields3& f = d.f;
+  for (double** q : {&f.uh, &f.uhp, &f.uhpp, &f.up, &f.upp, &f.hu, &f.hup, &f.hupp, &f.agx, &f.arx, &f.vh, &f.vhp,
+                     &f.vhpp, &f.vp, &f.vpp, &f.hv, &f.hvp, &f.hvpp, &f.agy, &f.ary, &f.h, &f.hp, &f.hpp, &f.sal,
+                     &f.salp, &f.salpp, &f.rhop, &f.Av, &f.Dv, &f.wp, &f.HeatSource, &f.Bth2, &f.Bth3, &f.Bth4})
+    rc |= c->alloc(q, n3);
+  Fields2& s = d.s;
+  for (double** q : {&s.s, &s.sp, &s.spp, &s.eagx, &s.earx, &s.eagy, &s.eary, &s.sx, &s.sy, &s.dd, &s.qq, &s.rr,
+                     &s.uair, &s.vair, &s.cdw})
+    rc |= c->alloc(q, P);
+  for (int** q : {&s.k1z, &s.k1u, &s.k1v}) rc |= c->alloc(q, P);
+  rc |= c->alloc(&d.scr, n3);
+  rc |= c->alloc(&c->staging, (size_t)km1 * lm1);
+  rc |= c->alloc(&c->dz, P);
+  if (rc) { delete c; return rc; }
+  // face-column lists
+  std::vector<int> ce, cn;
+  for (int l = 1; l <= lm; ++l) {
+    if (g->lEC[l - 1] != lm1) ce.push_back(l);
+    if (g->lNC[l - 1] != lm1) cn.push_back(l);
+  }
+  c->nce = (int)ce.size(); c->ncn = (int)cn.size();
+  rc |= c->alloc(&c->ce, ce.size());
+  rc |= c->alloc(&c->cn, cn.size());
+  if (rc) { delete c; return rc; }
+  if (!ce.empty()) cudaMemcpy(c->ce, ce.data(), ce.size() * sizeof(int), cudaMemcpyHostToDevice);
+  if (!cn.empty()) cudaMemcpy(c->cn, cn.data(), cn.size() * sizeof(int), cudaMemcpyHostToDevice);
+  rc = build_pcg(c, g);
+  if (rc) { delete c; return rc; }
+  if (cudaDeviceSynchronize() != cudaSuccess) { delete c; return SI3D_ECUDA; }
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_ctx.push_back(c);
+  *handle = (int)g_ctx.size() - 1;
+  return 0;
+}
+
+void si3d_gpu_finalize(int h) {
+  Ctx* c = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (h < 0 || h >= (int)g_ctx.size()) return;
+    c = g_ctx[h];
+    g_ctx[h] = nullptr;
+  }
+  if (c) { cudaSetDevice(c->device); delete c; }
+}
+
+int si3d_gpu_set_field(int h, const char* name, const double* host) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (!name || !host) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  if (double* dst = f3ptr(c, name)) {
+    CK(cudaMemcpyAsync(c->staging, host, sizeof(double) * c->km1 * c->lm1, cudaMemcpyHostToDevice, c->st));
+    dim3 b(32, 8), gr((c->lm1 + 31) / 32, (c->km1 + 31) / 32);
+    k_colmajor_to_layer<<<gr, b, 0, c->st>>>(c->staging, dst, c->km1, c->lm1, c->P);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+  }
+  if (double* dst = f2ptr(c, name)) {
+    CK(cudaMemcpyAsync(dst, host, sizeof(double) * c->lm1, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+  }
+  return SI3D_ENAME;
+}
+
+int si3d_gpu_get_field(int h, const char* name, double* host) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (!name || !host) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  if (double* src = f3ptr(c, name)) {
+    dim3 b(32, 8), gr((c->lm1 + 31) / 32, (c->km1 + 31) / 32);
+    k_layer_to_colmajor<<<gr, b, 0, c->st>>>(src, c->staging, c->km1, c->lm1, c->P);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(host, c->staging, sizeof(double) * c->km1 * c->lm1, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+  }
+  if (double* src = f2ptr(c, name)) {
+    CK(cudaMemcpyAsync(host, src, sizeof(double) * c->lm1, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return 0;
+  }
+  return SI3D_ENAME;
+}
+
+int si3d_gpu_set_ifield(int h, const char* name, const int* host) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  int* dst = name ? iptr(c, name) : nullptr;
+  if (!dst) return SI3D_ENAME;
+  if (!host) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(dst, host, sizeof(int) * c->lm1, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_get_ifield(int h, const char* name, int* host) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  int* src = name ? iptr(c, name) : nullptr;
+  if (!src) return SI3D_ENAME;
+  if (!host) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  CK(cudaMemcpyAsync(host, src, sizeof(int) * c->lm1, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_set_warmstart(int h, const double* dz, int on_device) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  CK(cudaSetDevice(c->device));
+  if (!dz) { c->dz_set = false; return 0; }
+  CK(cudaMemcpyAsync(c->dz, dz, sizeof(double) * c->lm1, on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice,
+                     c->st));
+  CK(cudaStreamSynchronize(c->st));
+  c->dz_set = true;
+  return 0;
+}
+
+int si3d_gpu_fd(int h, int n, int istep, int lastiter, si3d_step_stats* st) {
+  (void)n; (void)lastiter;
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (istep != 1 && istep != 2) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  if (st) { std::memset(st, 0, sizeof(*st)); CK(cudaEventRecord(c->ev0, c->st)); }
+  int rc = fd_impl(c, istep, st);
+  if (rc) return rc;
+  if (st) {
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    st->ms_total = ms;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_density(int h) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  CK(cudaSetDevice(c->device));
+  launch_density_init(c->d, c->st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_stage(int h, const char* stage, int istep, si3d_step_stats* st) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (!stage || (istep != 1 && istep != 2)) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  if (st) std::memset(st, 0, sizeof(*st));
+  const std::string s = stage;
+  Dev& d = c->d;
+  d.tz = 1.0 / istep;
+  if (s == "momentum") { launch_momentum(d, 1, c->ce, c->nce, c->st); launch_momentum(d, 2, c->cn, c->ncn, c->st); }
+  else if (s == "matcon") launch_matcon(d, c->st);
+  else if (s == "solve") {
+    int it = 0, ier = 0;
+    double rr = 0;
+    const int rc = solve(c, &it, &rr, &ier);
+    if (rc) return rc;
+    if (st) { st->nsolves = 1; st->iters[0] = it; st->relres[0] = rr; st->ier[0] = ier; st->total_iters = it; }
+    if (ier < 0) return ier;
+    launch_slayer_h(d, c->st);
+  } else if (s == "vel") launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st);
+  else if (s == "scalar") launch_exsal_imsal(d, c->st);
+  else if (s == "vel2") launch_vel2(d, c->st);
+  else if (s == "settrap") launch_settrap(d, c->st);
+  else if (s == "settrap2") launch_settrap2(d, c->st);
+  else if (s == "save") launch_save(d, istep, c->st);
+  else return SI3D_ENAME;
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_settrap(int h) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  CK(cudaSetDevice(c->device));
+  launch_settrap(c->d, c->st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_settrap2(int h) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  CK(cudaSetDevice(c->device));
+  launch_settrap2(c->d, c->st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_save(int h, int istep) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (istep != 1 && istep != 2) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  launch_save(c->d, istep, c->st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+// Loop body of si3d.f90:324-458 for step n (outputs omitted).
+int si3d_gpu_step(int h, int n, si3d_step_stats* st) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  CK(cudaSetDevice(c->device));
+  if (st) { std::memset(st, 0, sizeof(*st)); CK(cudaEventRecord(c->ev0, c->st)); }
+  const si3d_params& p = c->prm;
+  int niter1 = p.niter;
+  int rc = 0;
+  if (n == 1) {
+    niter1 = std::max(2, p.niter);
+  } else {
+    rc = fd_impl(c, 1, st);
+    if (rc) return rc;
+    if (p.itrap == 0 || (n % std::max(p.itrap, 1)) != 0) {
+      launch_save(c->d, 1, c->st);
+      goto done;
+    }
+    launch_settrap(c->d, c->st);
+  }
+  for (int it = 1; it <= niter1; ++it) {
+    rc = fd_impl(c, 2, st);
+    if (rc) return rc;
+    if (it < niter1) launch_settrap2(c->d, c->st);
+    if (it > 20) break;
+  }
+  launch_save(c->d, 2, c->st);
+done:
+  CK(cudaGetLastError());
+  if (st) {
+    CK(cudaEventRecord(c->ev1, c->st));
+    CK(cudaEventSynchronize(c->ev1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+    st->ms_total = ms;
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_sync(int h) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_solve_zeta(int lm, const double* coef, const int* jcoef, const double* rhs, double* zeta, int pcg_test,
+                        double pcg_tol, int pcg_itmax, double srelpr, int precision, int* iters, double* stptst,
+                        double* emin, double* emax) {
+  if (lm < 1 || !coef || !jcoef || !rhs || !zeta || pcg_itmax < 1 || (pcg_test != 5 && pcg_test != 2))
+    return SI3D_EDIMS;
+  if (precision != SI3D_FP64) return SI3D_EDIMS;
+  // Recover the grid graph and sx/sy from the SolverSparse structure:
+  // coef = [rr, -sx(lW), -sy(lS), -sy(l), -sx(l)], jcoef = [l, lWC, lSC, lNC, lEC] (0 = dry).
+  const int lm1 = lm + 1;
+  std::vector<int> E(lm), W(lm), N(lm), S(lm);
+  std::vector<double> sx(lm1, 0.0), sy(lm1, 0.0), qq(lm1, 0.0), sp(lm1, 0.0);
+  for (int m = 0; m < lm; ++m) {
+    auto J = [&](int cidx) { const int v = jcoef[(size_t)cidx * lm + m]; return v <= 0 ? lm1 : v; };
+    if (jcoef[m] != m + 1) return SI3D_EDIMS;
+    W[m] = J(1); S[m] = J(2); N[m] = J(3); E[m] = J(4);
+    sx[m] = -coef[(size_t)4 * lm + m];
+    sy[m] = -coef[(size_t)3 * lm + m];
+    qq[m] = rhs[m];
+    sp[m] = zeta[m];
+  }
+  for (int m = 0; m < lm; ++m) {
+    const double sxw = W[m] == lm1 ? 0.0 : sx[W[m] - 1], sys = S[m] == lm1 ? 0.0 : sy[S[m] - 1];
+    if (-coef[(size_t)1 * lm + m] != sxw || -coef[(size_t)2 * lm + m] != sys) return SI3D_EDIMS;
+    if (coef[m] != 1 + sx[m] + sxw + sy[m] + sys) return SI3D_EDIMS;
+    if (E[m] != lm1 && W[E[m] - 1] != m + 1) return SI3D_EDIMS;
+    if (N[m] != lm1 && S[N[m] - 1] != m + 1) return SI3D_EDIMS;
+  }
+  si3d_grid g{};
+  std::vector<int> kmz(lm1, 3), l2(lm, 1);
+  std::vector<double> hh(lm1, 1.0), zlv = {-100., -100., 1.0};
+  g.im1 = 1; g.jm1 = 1; g.km1 = 3; g.k1 = 2; g.lm = lm;
+  g.l2i = l2.data(); g.l2j = l2.data(); g.lEC = E.data(); g.lWC = W.data(); g.lNC = N.data(); g.lSC = S.data();
+  g.kmz = kmz.data(); g.hhs = hh.data(); g.hhu = hh.data(); g.hhv = hh.data(); g.zlevel = zlv.data();
+  si3d_params prm{};
+  prm.dt = 1; prm.dx = 1; prm.dy = 1; prm.theta = 1; prm.itrmom = 1; prm.ihd = 1;
+  prm.pcg_test = pcg_test; prm.pcg_tol = pcg_tol; prm.pcg_itmax = pcg_itmax; prm.srelpr = srelpr;
+  prm.ordering = SI3D_ORDER_REDBLACK; prm.x0_mode = SI3D_X0_PREV; prm.precision = precision;
+  int hdl = -1;
+  int rc = si3d_gpu_init(&g, &prm, 0, &hdl);
+  if (rc) return rc;
+  Ctx* c = get(hdl);
+  int ier = 0, it = 0;
+  double rr = 0;
+  rc = si3d_gpu_set_field(hdl, "sx", sx.data());
+  if (!rc) rc = si3d_gpu_set_field(hdl, "sy", sy.data());
+  if (!rc) rc = si3d_gpu_set_field(hdl, "qq", qq.data());
+  if (!rc) rc = si3d_gpu_set_field(hdl, "sp", sp.data());
+  if (!rc) rc = solve(c, &it, &rr, &ier);
+  std::vector<double> s(lm1);
+  if (!rc) rc = si3d_gpu_get_field(hdl, "s", s.data());
+  if (!rc) {
+    for (int m = 0; m < lm; ++m) zeta[m] = s[m];
+    *iters = it; *stptst = rr;
+    std::vector<double> al(std::max(it, 1)), be(std::max(it, 1));
+    if (it > 0) {
+      cudaMemcpy(al.data(), c->pcg.hist_alpha, sizeof(double) * it, cudaMemcpyDeviceToHost);
+      cudaMemcpy(be.data(), c->pcg.hist_beta, sizeof(double) * it, cudaMemcpyDeviceToHost);
+    }
+    double zt = pcg_tol < 500.0 * srelpr ? 500.0 * srelpr : pcg_tol;
+    double e0 = 1.0, e1 = 2.0;
+    if (it > 0) eigen_estimates(al.data(), be.data(), it, zt, pcg_itmax, e0, e1);
+    if (emin) *emin = e0;
+    if (emax) *emax = e1;
+  }
+  si3d_gpu_finalize(hdl);
+  return rc ? rc : ier;
+}
+
+int si3d_gpu_column_tridiag(int n, int nsys, const double* a, const double* b, const double* c, const double* g,
+                            const double* r, double* ag, double* ar) {
+  if (n < 1 || nsys < 1 || !a || !b || !c || !g || !r || !ag || !ar) return SI3D_EDIMS;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SI3D_ENODEV;
+  const size_t N = (size_t)n * nsys;
+  std::vector<double> host(N);
+  double* dbuf = nullptr;
+  CK(cudaMalloc(&dbuf, 8 * N * sizeof(double)));
+  double* D[8];
+  for (int i = 0; i < 8; ++i) D[i] = dbuf + i * N;
+  // host blocks are n x nsys column-major (system-contiguous); the device wants k-major
+  auto up = [&](const double* src, double* dst) {
+    for (int s = 0; s < nsys; ++s)
+      for (int k = 0; k < n; ++k) host[(size_t)k * nsys + s] = src[(size_t)s * n + k];
+    return cudaMemcpy(dst, host.data(), N * sizeof(double), cudaMemcpyHostToDevice);
+  };
+  cudaError_t e = cudaSuccess;
+  const double* srcs[5] = {a, b, c, g, r};
+  for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = up(srcs[i], D[i]);
+  if (e == cudaSuccess) {
+    launch_column_tridiag(n, nsys, D[0], D[1], D[2], D[3], D[4], D[5], D[6], D[7], 0);
+    e = cudaGetLastError();
+  }
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+    e = cudaMemcpy(host.data(), D[5 + i], N * sizeof(double), cudaMemcpyDeviceToHost);
+    double* out = i ? ar : ag;
+    for (int s = 0; s < nsys && e == cudaSuccess; ++s)
+      for (int k = 0; k < n; ++k) out[(size_t)s * n + k] = host[(size_t)k * nsys + s];
+  }
+  cudaFree(dbuf);
+  if (e != cudaSuccess) return cuda_fail(e);
+  return 0;
+}
+
+}  // extern "C"
