@@ -1,0 +1,326 @@
+#!/usr/bin/env python
+"""Benchmark of the GPU semi-implicit core on the 2000 x 1000 x 60 workload.
+
+One step = one whole time step of si3d.f90:324-458 (leapfrog fd, settrap, two trapezoidal fd
+iterations with settrap2, save): momentum tridiagonals, zeta assembly, three MIC-PCG zeta solves at
+relative residual 1e-12, velocities, scalar transport and the time-level bookkeeping, all on one
+B200 with the state resident in HBM.  Prints one JSON line.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload c2]
+
+N > 1 (launched under torchrun) runs independent replicas of the basin, one per GPU: the
+single-basin path is not sharded (replicas only), so per-GPU work is fixed as N grows.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "s/timestep & PCG iters/step at 2000×1000×60: learned+mixed vs plain FP64, same tol"
+
+# Algorithmic bytes (compulsory FP64 streams per unit) of the stages, the frozen byte model:
+# 3-D stages count streams per wet 3-D cell N3, 2-D stages per wet column lm, one CG iteration 18
+# streams per unknown.
+STAGE_STREAMS = {"momentum_x": (14, "N3"), "momentum_y": (14, "N3"), "matcon": (14, "lm"), "pcg_iter": (18, "lm"),
+                 "vel": (9, "N3"), "scalar": (16, "N3"), "vel2": (3, "N3"), "settrap": (15, "N3"),
+                 "settrap2": (9, "N3"), "save": (15, "N3")}
+
+
+def _dist():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class Clocks:
+    """nvidia-smi sampler over the timed region."""
+
+    def __init__(self, device: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={device}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self) -> dict:
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            d = json.load(fh)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_table():
+    p = os.path.join(ROOT, "profiles", "traffic_per_launch.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return json.load(fh)
+    return {}
+
+
+def workload_dir(name: str, rank: int) -> str:
+    from si3d_b200 import synth
+    d = os.path.join(tempfile.gettempdir(), f"si3d_bench_{name}_r{rank}")
+    marker = os.path.join(d, ".complete")
+    if not os.path.exists(marker):
+        synth.make(name, d)
+        open(marker, "w").close()
+    return d
+
+
+def counts(run_dir: str):
+    """lm and N3 (wet 3-D cells) of a run directory, from the host set-up."""
+    from si3d_b200 import native
+    import ctypes as C
+    import numpy as np
+    h = native.host()
+    hm = C.c_int(-1)
+    err = C.create_string_buffer(256)
+    native.check(h.si3d_host_open(run_dir.encode(), None, C.byref(hm), err, 256))
+    dims = (C.c_int * 6)()
+    h.si3d_host_dims(hm.value, dims)
+    lm = dims[3]
+    kmz = np.empty(lm + 1, dtype=np.int32)
+    h.si3d_host_get_map(hm.value, b"kmz", native.ptr(kmz))
+    h.si3d_host_close(hm.value)
+    n3 = int((kmz[:lm] - 1).sum())
+    return lm, n3
+
+
+def cpu_sample(name: str, threads: int) -> dict:
+    """The CPU restatement of the reference timed on a window of the workload (same layers,
+    bathymetry and forcing generators), extrapolated linearly in wet 3-D cells."""
+    from si3d_b200 import synth
+    from oracle import pyoracle
+    full = synth.config(name)
+    sub = synth.config(name)
+    # central window of the basin, 1/100 of the cells
+    wx, wy = max(full.nx // 10, 16), max(full.ny // 10, 16)
+    x0, y0 = (full.nx - wx) // 2, (full.ny - wy) // 2
+    sub.nx, sub.ny = wx, wy
+    sub.depth = full.depth[x0:x0 + wx, y0:y0 + wy].copy()
+    if full.uair is not None:
+        sub.uair = full.uair[x0:x0 + wx, y0:y0 + wy].copy()
+        sub.vair = full.vair[x0:x0 + wx, y0:y0 + wy].copy()
+    d = os.path.join(tempfile.gettempdir(), f"si3d_cpu_window_{name}")
+    synth.write_run(sub, d)
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    pyoracle.build()
+    o = pyoracle.OracleRun(d, ordering=1, pcg_itmax=2000)
+    o.run(1)                      # first step: trapezoidal start
+    t0 = time.perf_counter()
+    nsteps = 0
+    while True:
+        o.run(1)
+        nsteps += 1
+        if time.perf_counter() - t0 > 10.0 or nsteps >= 20:
+            break
+    dt = (time.perf_counter() - t0) / nsteps
+    lm_w, n3_w = counts(d)
+    return {"window_s_per_step": dt, "window": f"{wx}x{wy} cells of {name}", "lm": lm_w, "n3": n3_w,
+            "steps": nsteps, "iters_per_step": sum(s["iters"] for s in o.solves()[-3 * nsteps:]) / nsteps}
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", default="c2")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--itmax", type=int, default=2000)
+    args = ap.parse_args()
+    ws, rank, local = _dist()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        threads = os.cpu_count() or 1
+        lm_full, n3_full = counts(workload_dir(args.workload, 0))
+        smp = cpu_sample(args.workload, threads)
+        v = smp["window_s_per_step"] * n3_full / smp["n3"]
+        line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "s/timestep", "n_gpus": args.gpus,
+                "steps": smp["steps"], "warmup": 1, "ms_per_step": v * 1e3, "higher_is_better": False,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": f"{args.workload} 2000x1000x60 closed basin, plain FP64, PCG test 5 at 1e-12"},
+                "cpu_baseline": {"value": v, "unit": "s/timestep", "cores": 1, "kind": "port",
+                                 "sample": f"{smp['steps']} steps of a {smp['window']} window, extrapolated by wet "
+                                           f"3-D cells ({smp['n3']} -> {n3_full}); the zeta solve is serial as in "
+                                           f"the reference"},
+                "e2e": {"value": v, "unit": "s/timestep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import ctypes as C
+    import numpy as np
+    import torch
+    from si3d_b200 import build as sbuild
+    from si3d_b200 import native
+    from si3d_b200.model import GpuRun
+
+    pg = None
+    if ws > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+        pg = dist
+    device = local if ws > 1 else 0
+    torch.cuda.set_device(device)
+    sbuild.build_all()
+    run_dir = workload_dir(args.workload, rank)
+    lm, n3 = counts(run_dir)
+    run = GpuRun(run_dir, device=device, pcg_itmax=args.itmax)
+    run.run(args.warmup)
+
+    def barrier():
+        torch.cuda.synchronize(device)
+        native.check(native.gpu().si3d_gpu_sync(run.gh))
+        if pg is not None:
+            pg.barrier()
+
+    # ---------------------------------------------------------------- timed device run
+    barrier()
+    launches0, _ = run.counters()
+    clocks = Clocks(device)
+    t_wall = time.perf_counter()
+    stats = run.run(args.steps)
+    barrier()
+    t_wall = time.perf_counter() - t_wall
+    clk = clocks.stop()
+    launches1, _ = run.counters()
+    dev_ms = sum(s.ms_total for s in stats)
+    pcg_ms = sum(s.ms_pcg for s in stats)
+    iters = sum(s.total_iters for s in stats)
+    s_per_step = dev_ms / 1e3 / args.steps
+    if pg is not None:
+        t = torch.tensor([s_per_step], device=f"cuda:{device}", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        s_per_step = float(t.item())
+
+    # ---------------------------------------------------------------- per-stage profile (2 steps)
+    run.profile(True)
+    run.run(2)
+    _, prof = run.counters()
+    run.profile(False)
+    stage_ms = {k: v for k, v in prof.items() if v[1] > 0}
+    dominant = max(stage_ms, key=lambda k: stage_ms[k][0])
+    peak, peak_kind = measured_peaks()
+    roof = None
+    if dominant in STAGE_STREAMS:
+        streams, unit = STAGE_STREAMS[dominant]
+        units = n3 if unit == "N3" else lm
+        per_call_ms = stage_ms[dominant][0] / stage_ms[dominant][1]
+        alg_bytes = streams * 8 * units
+        achieved = alg_bytes / (per_call_ms * 1e-3) / 1e9
+        tr = traffic_table().get(dominant)
+        traffic = None
+        if tr and tr.get("workload") == args.workload:
+            traffic = tr.get("bytes_per_call")
+        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": traffic, "kernel": dominant, "algorithmic_bytes_per_call": alg_bytes,
+                "ms_per_call": per_call_ms, "peak_kind": peak_kind}
+
+    # ---------------------------------------------------------------- end to end through the C ABI
+    # per step: upload the surface forcing (uair, vair, cdw) from pinned host memory, advance one
+    # step, read zeta back
+    g = native.gpu()
+    forcing = {k: torch.from_numpy(run.get(k)).pin_memory() for k in ("uair", "vair", "cdw")}
+    zeta = torch.empty(run.lm1, dtype=torch.float64).pin_memory()
+    barrier()
+    t_e2e = time.perf_counter()
+    for _ in range(args.steps):
+        for k, v in forcing.items():
+            native.check(g.si3d_gpu_set_field(run.gh, k.encode(), C.c_void_p(v.data_ptr())))
+        native.check(native.host().si3d_host_run(run.hm, 1, None))
+        native.check(g.si3d_gpu_get_field(run.gh, b"s", C.c_void_p(zeta.data_ptr())))
+    barrier()
+    e2e = (time.perf_counter() - t_e2e) / args.steps
+    if pg is not None:
+        t = torch.tensor([e2e], device=f"cuda:{device}", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e = float(t.item())
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        smp = cpu_sample(args.workload, 1)
+        v = smp["window_s_per_step"] * n3 / smp["n3"]
+        cpu = {"value": v, "unit": "s/timestep", "cores": 1, "kind": "port",
+               "sample": f"{smp['steps']} steps of a {smp['window']} window (plain FP64, red-black MIC-PCG at 1e-12), "
+                         f"extrapolated by wet 3-D cells ({smp['n3']} -> {n3})"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": s_per_step, "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": s_per_step * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"{args.workload}: 2000x1000 cells x 60 layers, seeded random bathymetry and wind "
+                                   f"stress, dt 30 s, itrap=1 niter=2, plain FP64, MIC-PCG test 5 at 1e-12",
+                       "form": "plain_fp64", "lm": lm, "n3": n3, "parallelism": f"replicas x{ws}",
+                       "l2": "state (~25 GB) far larger than L2; no flush needed"},
+            "pcg_iters_per_step": iters / args.steps, "pcg_s_per_step": pcg_ms / 1e3 / args.steps,
+            "wall_s_per_step": t_wall / args.steps,
+            "stage_ms_per_step": {k: v[0] / 2 for k, v in stage_ms.items()},
+            "roofline": roof, "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "s/timestep", "h2d_bytes_per_step": 3 * run.lm1 * 8,
+                    "d2h_bytes_per_step": run.lm1 * 8},
+            "gpu_launches": int(launches1 - launches0), "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    run.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

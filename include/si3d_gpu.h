@@ -155,6 +155,15 @@ int si3d_gpu_solve_zeta(int lm, const double* coeffA, const int* jcoefA, const d
 int si3d_gpu_column_tridiag(int n, int nsys, const double* a, const double* b, const double* c,
                             const double* g, const double* r, double* ag, double* ar);
 
+/* Instrumentation.  si3d_gpu_profile(h, 1) makes every stage record CUDA events on the handle's
+ * stream and wait for them (stage boundaries become synchronisation points); counters returns the
+ * number of kernels the handle has launched and, per stage, the accumulated device milliseconds
+ * and call counts (the zeta-solve iteration stage counts iterations).  Stage order: momentum x,
+ * momentum y, matcon, pcg setup, pcg iterations, pcg finish, slayer_h, vel, scalar, vel2,
+ * settrap, settrap2, save.  Returns the number of stages. */
+int si3d_gpu_profile(int handle, int enable);
+int si3d_gpu_counters(int handle, long long* launches, double* stage_ms, long long* stage_n);
+
 /* Wait for the handle's stream. */
 int si3d_gpu_sync(int handle);
 /* Human-readable text for an error code. */

@@ -76,6 +76,12 @@ struct Ctx {
   PcgScal* h_sc = nullptr;  // pinned
   double* h_hist = nullptr; // pinned, 2 x itmax
   int last_iters = 8;
+  // instrumentation: kernel-launch count and (optionally) per-stage device time
+  long long launches = 0;
+  bool prof = false;
+  double prof_ms[16] = {0};
+  long long prof_n[16] = {0};
+  cudaEvent_t pe0 = nullptr, pe1 = nullptr;
   double* dz = nullptr;     // learned warm-start increment (device, lm1)
   bool dz_set = false;
   double* staging = nullptr;  // device staging for transposes (km1 * lm1)
@@ -85,7 +91,7 @@ struct Ctx {
     for (void* p : allocs) cudaFree(p);
     if (h_sc) cudaFreeHost(h_sc);
     if (h_hist) cudaFreeHost(h_hist);
-    for (cudaEvent_t e : {ev0, ev1, evp0, evp1}) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {ev0, ev1, evp0, evp1, pe0, pe1}) if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
   }
   template <class T>
@@ -108,6 +114,30 @@ Ctx* get(int h) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (h < 0 || h >= (int)g_ctx.size()) return nullptr;
   return g_ctx[h];
+}
+
+// Stage ids for the per-stage device timers.
+enum { ST_MOMX, ST_MOMY, ST_MATCON, ST_PCG_SETUP, ST_PCG_ITER, ST_PCG_FINISH, ST_SLAYER, ST_VEL, ST_SCALAR, ST_VEL2,
+       ST_SETTRAP, ST_SETTRAP2, ST_SAVE, ST_COUNT };
+
+// Run `f` (which enqueues `nk` kernels) as one timed stage.
+template <class F>
+int stage(Ctx* c, int id, int nk, F&& f) {
+  if (c->prof) cudaEventRecord(c->pe0, c->st);
+  f();
+  c->launches += nk;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_fail(e);
+  if (c->prof) {
+    cudaEventRecord(c->pe1, c->st);
+    e = cudaEventSynchronize(c->pe1);
+    if (e != cudaSuccess) return cuda_fail(e);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->pe0, c->pe1);
+    c->prof_ms[id] += ms;
+    c->prof_n[id] += 1;
+  }
+  return 0;
 }
 
 double* f3ptr(Ctx* c, const std::string& n) {
@@ -333,14 +363,16 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   *c->h_sc = init;
   CK(cudaMemcpyAsync(c->pcg.sc, c->h_sc, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
   const int x0 = (p.x0_mode == SI3D_X0_LEARNED && !c->dz_set) ? SI3D_X0_PREV : p.x0_mode;
-  pcg_setup(c->d, c->pcg, x0, c->dz, &c->pcg.sc->negpiv, c->st);
-  CK(cudaGetLastError());
+  int rc0 = stage(c, ST_PCG_SETUP, 7, [&] { pcg_setup(c->d, c->pcg, x0, c->dz, &c->pcg.sc->negpiv, c->st); });
+  if (rc0) return rc0;
+  if (c->prof) CK(cudaEventRecord(c->pe0, c->st));
   // run iterations in batches; every kernel returns at once after convergence
   int batch = std::max(1, std::min(c->last_iters - 1, 256));
   int launched = 0;
   for (;;) {
     for (int i = 0; i < batch; ++i) pcg_iteration(c->pcg, c->st);
     launched += batch;
+    c->launches += 4LL * batch;
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -348,8 +380,16 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
     if (launched > p.pcg_itmax + 8) return SI3D_ETIMEOUT;  // cannot happen: itcg stops at itmax
     batch = 4;
   }
-  pcg_finish(c->d, c->pcg, c->st);
-  CK(cudaGetLastError());
+  if (c->prof) {
+    CK(cudaEventRecord(c->pe1, c->st));
+    CK(cudaEventSynchronize(c->pe1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->pe0, c->pe1);
+    c->prof_ms[ST_PCG_ITER] += ms;
+    c->prof_n[ST_PCG_ITER] += c->h_sc->in;
+  }
+  rc0 = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, c->st); });
+  if (rc0) return rc0;
   const PcgScal& S = *c->h_sc;
   if (S.negpiv & 2) ier = -12;
   else if (S.ier != 0) ier = S.ier;
@@ -365,14 +405,14 @@ int fd_impl(Ctx* c, int istep, si3d_step_stats* st) {
   Dev& d = c->d;
   d.tz = 1.0 / istep;
   // surfbc CASE(0) is a constant per-column wind set by the host (uair/vair/cdw fields)
-  launch_momentum(d, 1, c->ce, c->nce, c->st);
-  launch_momentum(d, 2, c->cn, c->ncn, c->st);
-  launch_matcon(d, c->st);
-  CK(cudaGetLastError());
+  int rc = stage(c, ST_MOMX, 1, [&] { launch_momentum(d, 1, c->ce, c->nce, c->st); });
+  if (!rc) rc = stage(c, ST_MOMY, 1, [&] { launch_momentum(d, 2, c->cn, c->ncn, c->st); });
+  if (!rc) rc = stage(c, ST_MATCON, 1, [&] { launch_matcon(d, c->st); });
+  if (rc) return rc;
   if (st) CK(cudaEventRecord(c->evp0, c->st));
   int iters = 0, ier = 0;
   double rr = 0;
-  int rc = solve(c, &iters, &rr, &ier);
+  rc = solve(c, &iters, &rr, &ier);
   if (rc) return rc;
   if (st) CK(cudaEventRecord(c->evp1, c->st));
   if (st) {
@@ -383,11 +423,11 @@ int fd_impl(Ctx* c, int istep, si3d_step_stats* st) {
     st->total_iters += iters;
   }
   if (ier < 0) return ier;
-  launch_slayer_h(d, c->st);
-  launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st);
-  if (c->prm.isal != 0) launch_exsal_imsal(d, c->st);
-  launch_vel2(d, c->st);
-  CK(cudaGetLastError());
+  rc = stage(c, ST_SLAYER, 1, [&] { launch_slayer_h(d, c->st); });
+  if (!rc) rc = stage(c, ST_VEL, 3, [&] { launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st); });
+  if (!rc && c->prm.isal != 0) rc = stage(c, ST_SCALAR, 2, [&] { launch_exsal_imsal(d, c->st); });
+  if (!rc) rc = stage(c, ST_VEL2, 1, [&] { launch_vel2(d, c->st); });
+  if (rc) return rc;
   if (st) {
     CK(cudaEventSynchronize(c->evp1));
     float ms = 0;
@@ -439,7 +479,7 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
   c->device = device;
   c->prm = *prm;
   if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess) { delete c; return SI3D_ECUDA; }
-  for (cudaEvent_t* e : {&c->ev0, &c->ev1, &c->evp0, &c->evp1}) cudaEventCreate(e);
+  for (cudaEvent_t* e : {&c->ev0, &c->ev1, &c->evp0, &c->evp1, &c->pe0, &c->pe1}) cudaEventCreate(e);
   const int lm = g->lm, lm1 = lm + 1, km1 = g->km1;
   const int P = (lm1 + 31) / 32 * 32;
   c->lm = lm; c->lm1 = lm1; c->km1 = km1; c->P = P;
@@ -719,18 +759,24 @@ int si3d_gpu_step(int h, int n, si3d_step_stats* st) {
     rc = fd_impl(c, 1, st);
     if (rc) return rc;
     if (p.itrap == 0 || (n % std::max(p.itrap, 1)) != 0) {
-      launch_save(c->d, 1, c->st);
+      rc = stage(c, ST_SAVE, 2, [&] { launch_save(c->d, 1, c->st); });
+      if (rc) return rc;
       goto done;
     }
-    launch_settrap(c->d, c->st);
+    rc = stage(c, ST_SETTRAP, 3, [&] { launch_settrap(c->d, c->st); });
+    if (rc) return rc;
   }
   for (int it = 1; it <= niter1; ++it) {
     rc = fd_impl(c, 2, st);
     if (rc) return rc;
-    if (it < niter1) launch_settrap2(c->d, c->st);
+    if (it < niter1) {
+      rc = stage(c, ST_SETTRAP2, 3, [&] { launch_settrap2(c->d, c->st); });
+      if (rc) return rc;
+    }
     if (it > 20) break;
   }
-  launch_save(c->d, 2, c->st);
+  rc = stage(c, ST_SAVE, 2, [&] { launch_save(c->d, 2, c->st); });
+  if (rc) return rc;
 done:
   CK(cudaGetLastError());
   if (st) {
@@ -742,6 +788,25 @@ done:
   }
   CK(cudaStreamSynchronize(c->st));
   return 0;
+}
+
+int si3d_gpu_profile(int h, int enable) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  c->prof = enable != 0;
+  for (int i = 0; i < 16; ++i) { c->prof_ms[i] = 0; c->prof_n[i] = 0; }
+  return 0;
+}
+
+int si3d_gpu_counters(int h, long long* launches, double* stage_ms, long long* stage_n) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (launches) *launches = c->launches;
+  for (int i = 0; i < ST_COUNT; ++i) {
+    if (stage_ms) stage_ms[i] = c->prof_ms[i];
+    if (stage_n) stage_n[i] = c->prof_n[i];
+  }
+  return ST_COUNT;
 }
 
 int si3d_gpu_sync(int h) {

@@ -53,6 +53,16 @@ class GpuRun:
         check(self.g.si3d_gpu_stage(self.gh, name.encode(), istep, C.byref(st)))
         return st
 
+    def profile(self, enable: bool) -> None:
+        check(self.g.si3d_gpu_profile(self.gh, 1 if enable else 0))
+
+    def counters(self):
+        n = C.c_longlong(0)
+        ms = np.zeros(16)
+        cnt = np.zeros(16, dtype=np.int64)
+        k = check(self.g.si3d_gpu_counters(self.gh, C.byref(n), native.ptr(ms), native.ptr(cnt)))
+        return n.value, {native.STAGES[i]: (float(ms[i]), int(cnt[i])) for i in range(k)}
+
     @property
     def n(self) -> int:
         return self.h.si3d_host_step_count(self.hm)

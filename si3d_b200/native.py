@@ -70,6 +70,8 @@ GPU_SYMBOLS = {
                                       C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "si3d_gpu_column_tridiag": (C.c_int, [C.c_int, C.c_int] + [C.c_void_p] * 7),
+    "si3d_gpu_profile": (C.c_int, [C.c_int, C.c_int]),
+    "si3d_gpu_counters": (C.c_int, [C.c_int, C.POINTER(C.c_longlong), C.c_void_p, C.c_void_p]),
     "si3d_gpu_sync": (C.c_int, [C.c_int]),
     "si3d_gpu_strerror": (C.c_char_p, [C.c_int]),
     "si3d_gpu_finalize": (None, [C.c_int]),
@@ -85,6 +87,9 @@ HOST_SYMBOLS = {
     "si3d_host_step_count": (C.c_int, [C.c_int]),
     "si3d_host_close": (None, [C.c_int]),
 }
+
+STAGES = ("momentum_x", "momentum_y", "matcon", "pcg_setup", "pcg_iter", "pcg_finish", "slayer_h", "vel",
+          "scalar", "vel2", "settrap", "settrap2", "save")
 
 _gpu = None
 _host = None
