@@ -1,0 +1,129 @@
+!*************************************************************************
+                          MODULE si3d_gpu_iface
+!*************************************************************************
+!
+!  ISO_C_BINDING interface to the B200 semi-implicit core (include/si3d_gpu.h).
+!  Every routine returns an INTEGER(C_INT) status: 0 = ok, NSPCG codes for the
+!  zeta solve (1, 2, -6, -7, ...), <= -100 for library errors.
+!  Arrays are passed as assumed-size (*) actual arguments with the layout the
+!  si3d module arrays already have: (km1, lm1) column-major, lm1 sentinel.
+!
+!-------------------------------------------------------------------------
+   USE ISO_C_BINDING
+   IMPLICIT NONE
+
+   TYPE, BIND(C) :: si3d_grid_t
+      INTEGER(C_INT) :: im1, jm1, km1, k1, lm
+      TYPE(C_PTR)    :: l2i, l2j, lEC, lWC, lNC, lSC, kmz
+      TYPE(C_PTR)    :: hhs, hhu, hhv, zlevel
+   END TYPE si3d_grid_t
+
+   TYPE, BIND(C) :: si3d_params_t
+      REAL(C_DOUBLE) :: dt, dx, dy
+      REAL(C_DOUBLE) :: Av0, Dv0, Ax0, Ay0, f, theta, cd, cw, beta
+      INTEGER(C_INT) :: iadv, itrmom, ihd, ibc, isal, itrap, niter, ismooth
+      INTEGER(C_INT) :: pcg_test
+      REAL(C_DOUBLE) :: pcg_tol
+      INTEGER(C_INT) :: pcg_itmax
+      REAL(C_DOUBLE) :: srelpr
+      INTEGER(C_INT) :: ordering, x0_mode, precision
+   END TYPE si3d_params_t
+
+   TYPE, BIND(C) :: si3d_step_stats_t
+      INTEGER(C_INT) :: nsolves
+      INTEGER(C_INT) :: iters(24)
+      REAL(C_DOUBLE) :: relres(24)
+      INTEGER(C_INT) :: ier(24)
+      INTEGER(C_INT) :: total_iters
+      REAL(C_DOUBLE) :: ms_total, ms_pcg
+   END TYPE si3d_step_stats_t
+
+   INTERFACE
+      INTEGER(C_INT) FUNCTION si3d_gpu_init(grid, params, device, handle) BIND(C, NAME="si3d_gpu_init")
+         IMPORT :: C_INT, si3d_grid_t, si3d_params_t
+         TYPE(si3d_grid_t), INTENT(IN)   :: grid
+         TYPE(si3d_params_t), INTENT(IN) :: params
+         INTEGER(C_INT), VALUE           :: device
+         INTEGER(C_INT), INTENT(OUT)     :: handle
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_set_field(handle, name, host) BIND(C, NAME="si3d_gpu_set_field")
+         IMPORT :: C_INT, C_CHAR, C_DOUBLE
+         INTEGER(C_INT), VALUE              :: handle
+         CHARACTER(KIND=C_CHAR), INTENT(IN) :: name(*)
+         REAL(C_DOUBLE), INTENT(IN)         :: host(*)
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_get_field(handle, name, host) BIND(C, NAME="si3d_gpu_get_field")
+         IMPORT :: C_INT, C_CHAR, C_DOUBLE
+         INTEGER(C_INT), VALUE              :: handle
+         CHARACTER(KIND=C_CHAR), INTENT(IN) :: name(*)
+         REAL(C_DOUBLE), INTENT(OUT)        :: host(*)
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_set_ifield(handle, name, host) BIND(C, NAME="si3d_gpu_set_ifield")
+         IMPORT :: C_INT, C_CHAR
+         INTEGER(C_INT), VALUE              :: handle
+         CHARACTER(KIND=C_CHAR), INTENT(IN) :: name(*)
+         INTEGER(C_INT), INTENT(IN)         :: host(*)
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_get_ifield(handle, name, host) BIND(C, NAME="si3d_gpu_get_ifield")
+         IMPORT :: C_INT, C_CHAR
+         INTEGER(C_INT), VALUE              :: handle
+         CHARACTER(KIND=C_CHAR), INTENT(IN) :: name(*)
+         INTEGER(C_INT), INTENT(OUT)        :: host(*)
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_density(handle) BIND(C, NAME="si3d_gpu_density")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE :: handle
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_fd(handle, n, istep, lastiter, stats) BIND(C, NAME="si3d_gpu_fd")
+         IMPORT :: C_INT, si3d_step_stats_t
+         INTEGER(C_INT), VALUE                  :: handle, n, istep, lastiter
+         TYPE(si3d_step_stats_t), INTENT(OUT)   :: stats
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_settrap(handle) BIND(C, NAME="si3d_gpu_settrap")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE :: handle
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_settrap2(handle) BIND(C, NAME="si3d_gpu_settrap2")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE :: handle
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_save(handle, istep) BIND(C, NAME="si3d_gpu_save")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE :: handle, istep
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_step(handle, n, stats) BIND(C, NAME="si3d_gpu_step")
+         IMPORT :: C_INT, si3d_step_stats_t
+         INTEGER(C_INT), VALUE                :: handle, n
+         TYPE(si3d_step_stats_t), INTENT(OUT) :: stats
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_solve_zeta(lm, coeffA, jcoefA, rhs, zeta, pcg_test, pcg_tol, pcg_itmax, &
+                                                  srelpr, precision, iters, stptst, emin, emax)            &
+                                                  BIND(C, NAME="si3d_gpu_solve_zeta")
+         IMPORT :: C_INT, C_DOUBLE
+         INTEGER(C_INT), VALUE         :: lm, pcg_test, pcg_itmax, precision
+         REAL(C_DOUBLE), VALUE         :: pcg_tol, srelpr
+         REAL(C_DOUBLE), INTENT(IN)    :: coeffA(*), rhs(*)
+         INTEGER(C_INT), INTENT(IN)    :: jcoefA(*)
+         REAL(C_DOUBLE), INTENT(INOUT) :: zeta(*)
+         INTEGER(C_INT), INTENT(OUT)   :: iters
+         REAL(C_DOUBLE), INTENT(OUT)   :: stptst, emin, emax
+      END FUNCTION
+
+      SUBROUTINE si3d_gpu_finalize(handle) BIND(C, NAME="si3d_gpu_finalize")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE :: handle
+      END SUBROUTINE
+   END INTERFACE
+
+END MODULE si3d_gpu_iface

@@ -111,11 +111,13 @@ def config(name: str, nsteps: Optional[int] = None, seed_offset: int = 0) -> Bas
         nx, ny, dx = 100, 50, 100.0
         return Basin("c0", nx, ny, dx, dx, bowl_bathymetry(nx, ny, dx, dx), 20, 1.0, 60.0, nsteps or 1000,
                      dzmin=0.05, wa=float(wind_speed_for_stress(0.1)), phi=270.0)
-    if name in ("c1", "c2", "t1"):
+    if name in ("c1", "c2", "t1", "m1"):
         if name == "c1":
             nx, ny, dx, nl, ddz, steps, sb, sw = 1000, 500, 50.0, 40, 1.5, 1000, 1001, 1002
         elif name == "c2":
             nx, ny, dx, nl, ddz, steps, sb, sw = 2000, 1000, 50.0, 60, 1.0, 500, 2001, 2002
+        elif name == "m1":  # medium basin for profiler captures (c2 generators, ~1.5 GB state)
+            nx, ny, dx, nl, ddz, steps, sb, sw = 600, 300, 50.0, 60, 1.0, 50, 2001, 2002
         else:  # small random basin for fast parity tests
             nx, ny, dx, nl, ddz, steps, sb, sw = 96, 64, 50.0, 12, 5.0, 50, 3001, 3002
         sb += seed_offset
