@@ -39,6 +39,7 @@ extern "C" {
 #define SI3D_ETIMEOUT (-105)  /* a bounded device wait gave up */
 #define SI3D_ENOMEM (-106)    /* device allocation failed */
 #define SI3D_ENODEV (-107)    /* no CUDA device / not sm_100 */
+#define SI3D_ECAPACITY (-108) /* problem larger than the fixed scratch of an allocation-free call */
 
 /* precision forms */
 #define SI3D_FP64 0       /* plain FP64 everywhere */
@@ -163,6 +164,20 @@ int si3d_gpu_column_tridiag(int n, int nsys, const double* a, const double* b, c
  * settrap, settrap2, save.  Returns the number of stages. */
 int si3d_gpu_profile(int handle, int enable);
 int si3d_gpu_counters(int handle, long long* launches, double* stage_ms, long long* stage_n);
+
+/* Allocation-free form of si3d_gpu_column_tridiag, for callers that cannot call cudaMalloc (a
+ * model coupled into a framework that owns the device allocator, or a loop that must not allocate
+ * once running).  No counterpart in the reference.  Inputs and outputs are the caller's DEVICE
+ * buffers in layer-major order (element k of system s at k*nsys + s); the sweep's scratch is a
+ * fixed array inside the library, so n*nsys must not exceed SI3D_NOALLOC_MAX_ELEMS (larger
+ * problems return SI3D_ECAPACITY without touching the GPU).  The library image keeps that 8 MiB
+ * array on every GPU that loads it until the process exits.  The first call on a device looks the
+ * array's address up (make it before any stream capture).  All calls share the array, so calls
+ * whose kernels overlap on one GPU race.  Work is queued on `stream` (a cudaStream_t, NULL = the
+ * default stream) and the call returns after that stream has finished it. */
+#define SI3D_NOALLOC_MAX_ELEMS (1 << 20)
+int si3d_gpu_column_tridiag_noalloc(int n, int nsys, const double* a, const double* b, const double* c,
+                                   const double* g, const double* r, double* ag, double* ar, void* stream);
 
 /* Wait for the handle's stream. */
 int si3d_gpu_sync(int handle);

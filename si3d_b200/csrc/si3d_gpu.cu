@@ -460,6 +460,7 @@ const char* si3d_gpu_strerror(int code) {
     case SI3D_ETIMEOUT: return "bounded device wait gave up";
     case SI3D_ENOMEM: return "device allocation failed";
     case SI3D_ENODEV: return "no sm_100 CUDA device";
+    case SI3D_ECAPACITY: return "problem exceeds the fixed scratch of the allocation-free entry point";
     default: return "unknown error";
   }
 }

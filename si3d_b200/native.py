@@ -70,6 +70,7 @@ GPU_SYMBOLS = {
                                       C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "si3d_gpu_column_tridiag": (C.c_int, [C.c_int, C.c_int] + [C.c_void_p] * 7),
+    "si3d_gpu_column_tridiag_noalloc": (C.c_int, [C.c_int, C.c_int] + [C.c_void_p] * 8),
     "si3d_gpu_profile": (C.c_int, [C.c_int, C.c_int]),
     "si3d_gpu_counters": (C.c_int, [C.c_int, C.POINTER(C.c_longlong), C.c_void_p, C.c_void_p]),
     "si3d_gpu_sync": (C.c_int, [C.c_int]),
