@@ -218,76 +218,87 @@ def main() -> int:
     sbuild.build_all()
     run_dir = workload_dir(args.workload, rank)
     lm, n3 = counts(run_dir)
-    run = GpuRun(run_dir, device=device, pcg_itmax=args.itmax)
-    run.run(args.warmup)
-
-    def barrier():
-        torch.cuda.synchronize(device)
-        native.check(native.gpu().si3d_gpu_sync(run.gh))
-        if pg is not None:
-            pg.barrier()
-
-    # ---------------------------------------------------------------- timed device run
-    barrier()
-    launches0, _ = run.counters()
-    clocks = Clocks(device)
-    t_wall = time.perf_counter()
-    stats = run.run(args.steps)
-    barrier()
-    t_wall = time.perf_counter() - t_wall
-    clk = clocks.stop()
-    launches1, _ = run.counters()
-    dev_ms = sum(s.ms_total for s in stats)
-    pcg_ms = sum(s.ms_pcg for s in stats)
-    iters = sum(s.total_iters for s in stats)
-    s_per_step = dev_ms / 1e3 / args.steps
-    if pg is not None:
-        t = torch.tensor([s_per_step], device=f"cuda:{device}", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        s_per_step = float(t.item())
-
-    # ---------------------------------------------------------------- per-stage profile (2 steps)
-    run.profile(True)
-    run.run(2)
-    _, prof = run.counters()
-    run.profile(False)
-    stage_ms = {k: v for k, v in prof.items() if v[1] > 0}
-    dominant = max(stage_ms, key=lambda k: stage_ms[k][0])
     peak, peak_kind = measured_peaks()
-    roof = None
-    if dominant in STAGE_STREAMS:
-        streams, unit = STAGE_STREAMS[dominant]
-        units = n3 if unit == "N3" else lm
-        per_call_ms = stage_ms[dominant][0] / stage_ms[dominant][1]
-        alg_bytes = streams * 8 * units
-        achieved = alg_bytes / (per_call_ms * 1e-3) / 1e9
-        tr = traffic_table().get(dominant)
-        traffic = None
-        if tr and tr.get("workload") == args.workload:
-            traffic = tr.get("bytes_per_call")
-        roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": traffic, "kernel": dominant, "algorithmic_bytes_per_call": alg_bytes,
-                "ms_per_call": per_call_ms, "peak_kind": peak_kind}
-
-    # ---------------------------------------------------------------- end to end through the C ABI
-    # per step: upload the surface forcing (uair, vair, cdw) from pinned host memory, advance one
-    # step, read zeta back
     g = native.gpu()
-    forcing = {k: torch.from_numpy(run.get(k)).pin_memory() for k in ("uair", "vair", "cdw")}
-    zeta = torch.empty(run.lm1, dtype=torch.float64).pin_memory()
-    barrier()
-    t_e2e = time.perf_counter()
-    for _ in range(args.steps):
-        for k, v in forcing.items():
-            native.check(g.si3d_gpu_set_field(run.gh, k.encode(), C.c_void_p(v.data_ptr())))
-        native.check(native.host().si3d_host_run(run.hm, 1, None))
-        native.check(g.si3d_gpu_get_field(run.gh, b"s", C.c_void_p(zeta.data_ptr())))
-    barrier()
-    e2e = (time.perf_counter() - t_e2e) / args.steps
-    if pg is not None:
-        t = torch.tensor([e2e], device=f"cuda:{device}", dtype=torch.float64)
+
+    def reduce_max(x):
+        if pg is None:
+            return x
+        t = torch.tensor([x], device=f"cuda:{device}", dtype=torch.float64)
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e = float(t.item())
+        return float(t.item())
+
+    def measure(form: str, precision: int, headline: bool) -> dict:
+        run = GpuRun(run_dir, device=device, pcg_itmax=args.itmax, precision=precision)
+        run.run(args.warmup)
+
+        def barrier():
+            torch.cuda.synchronize(device)
+            native.check(g.si3d_gpu_sync(run.gh))
+            if pg is not None:
+                pg.barrier()
+
+        # ------------------------------------------------------------ timed device run
+        barrier()
+        launches0, _ = run.counters()
+        clocks = Clocks(device) if headline else None
+        t_wall = time.perf_counter()
+        stats = run.run(args.steps)
+        barrier()
+        t_wall = time.perf_counter() - t_wall
+        clk = clocks.stop() if clocks else None
+        launches1, _ = run.counters()
+        out = {"s_per_step": reduce_max(sum(s.ms_total for s in stats) / 1e3 / args.steps),
+               "pcg_s_per_step": sum(s.ms_pcg for s in stats) / 1e3 / args.steps,
+               "pcg_iters_per_step": sum(s.total_iters for s in stats) / args.steps,
+               "max_relres": max(max(s.relres[i] for i in range(s.nsolves)) for s in stats),
+               "wall_s_per_step": t_wall / args.steps, "gpu_launches": int(launches1 - launches0), "clocks": clk}
+        # ------------------------------------------------------------ per-stage profile (2 steps)
+        run.profile(True)
+        run.run(2)
+        _, prof = run.counters()
+        run.profile(False)
+        stage_ms = {k: v for k, v in prof.items() if v[1] > 0}
+        out["stage_ms_per_step"] = {k: v[0] / 2 for k, v in stage_ms.items()}
+        dominant = max(stage_ms, key=lambda k: stage_ms[k][0])
+        if dominant in STAGE_STREAMS:
+            streams, unit = STAGE_STREAMS[dominant]
+            units = n3 if unit == "N3" else lm
+            word = 4 if (dominant == "pcg_iter" and precision == native.SI3D_MIXED_IR) else 8
+            per_call_ms = stage_ms[dominant][0] / stage_ms[dominant][1]
+            alg_bytes = streams * word * units
+            achieved = alg_bytes / (per_call_ms * 1e-3) / 1e9
+            tr = traffic_table().get(f"{dominant}:{form}")
+            traffic = tr.get("bytes_per_call") if tr and tr.get("workload") == args.workload else None
+            out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                               "frac": achieved / peak, "traffic": traffic, "kernel": dominant,
+                               "algorithmic_bytes_per_call": alg_bytes, "ms_per_call": per_call_ms,
+                               "peak_kind": peak_kind}
+        if headline:
+            # -------------------------------------------------------- end to end through the C ABI
+            # per step: upload the surface forcing (uair, vair, cdw) from pinned host memory,
+            # advance one step, read zeta back
+            forcing = {k: torch.from_numpy(run.get(k)).pin_memory() for k in ("uair", "vair", "cdw")}
+            zeta = torch.empty(run.lm1, dtype=torch.float64).pin_memory()
+            barrier()
+            t_e2e = time.perf_counter()
+            for _ in range(args.steps):
+                for k, v in forcing.items():
+                    native.check(g.si3d_gpu_set_field(run.gh, k.encode(), C.c_void_p(v.data_ptr())))
+                native.check(native.host().si3d_host_run(run.hm, 1, None))
+                native.check(g.si3d_gpu_get_field(run.gh, b"s", C.c_void_p(zeta.data_ptr())))
+            barrier()
+            out["e2e"] = {"value": reduce_max((time.perf_counter() - t_e2e) / args.steps), "unit": "s/timestep",
+                          "h2d_bytes_per_step": 3 * run.lm1 * 8, "d2h_bytes_per_step": run.lm1 * 8}
+        run.close()
+        return out
+
+    forms = [("plain_fp64", native.SI3D_FP64), ("mixed_ir", native.SI3D_MIXED_IR)]
+    res = {}
+    for i, (form, prec) in enumerate(forms):
+        res[form] = measure(form, prec, headline=(i == len(forms) - 1))
+    head_form = forms[-1][0]
+    head = res[head_form]
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -298,24 +309,24 @@ def main() -> int:
                          f"extrapolated by wet 3-D cells ({smp['n3']} -> {n3})"}
 
     if rank == 0:
+        plain = res["plain_fp64"]
         line = {
-            "metric": METRIC, "value": s_per_step, "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": s_per_step * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "metric": METRIC, "value": head["s_per_step"], "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": head["s_per_step"] * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (fp32 inner solves)" if head_form != "plain_fp64"
+            else "f64", "data": "synthetic",
             "config": {"workload": f"{args.workload}: 2000x1000 cells x 60 layers, seeded random bathymetry and wind "
-                                   f"stress, dt 30 s, itrap=1 niter=2, plain FP64, MIC-PCG test 5 at 1e-12",
-                       "form": "plain_fp64", "lm": lm, "n3": n3, "parallelism": f"replicas x{ws}",
+                                   f"stress, dt 30 s, itrap=1 niter=2, zeta solve to relative residual 1e-12 (test 5)",
+                       "form": head_form, "lm": lm, "n3": n3, "parallelism": f"replicas x{ws}",
                        "l2": "state (~25 GB) far larger than L2; no flush needed"},
-            "pcg_iters_per_step": iters / args.steps, "pcg_s_per_step": pcg_ms / 1e3 / args.steps,
-            "wall_s_per_step": t_wall / args.steps,
-            "stage_ms_per_step": {k: v[0] / 2 for k, v in stage_ms.items()},
-            "roofline": roof, "cpu_baseline": cpu,
-            "e2e": {"value": e2e, "unit": "s/timestep", "h2d_bytes_per_step": 3 * run.lm1 * 8,
-                    "d2h_bytes_per_step": run.lm1 * 8},
-            "gpu_launches": int(launches1 - launches0), "clocks": clk,
+            "pcg_iters_per_step": head["pcg_iters_per_step"], "pcg_s_per_step": head["pcg_s_per_step"],
+            "speedup_vs_plain_fp64": plain["s_per_step"] / head["s_per_step"],
+            "pcg_speedup_vs_plain_fp64": plain["pcg_s_per_step"] / head["pcg_s_per_step"],
+            "forms": {k: {kk: vv for kk, vv in v.items() if kk not in ("clocks", "e2e")} for k, v in res.items()},
+            "roofline": head.get("roofline"), "cpu_baseline": cpu, "e2e": head["e2e"],
+            "gpu_launches": head["gpu_launches"], "clocks": head["clocks"],
         }
         print(json.dumps(line), flush=True)
-    run.close()
     if pg is not None:
         pg.barrier()
         pg.destroy_process_group()

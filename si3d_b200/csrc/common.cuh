@@ -51,7 +51,9 @@ struct Dev {
   double tz;
 };
 
-__device__ __forceinline__ size_t IX(const Dev& d, int k, int l) { return (size_t)(k - 1) * d.g.P + (l - 1); }
+// 32-bit element index: si3d_gpu_init rejects grids with km1 * P >= 2^31, so the product cannot
+// overflow, and 32-bit address arithmetic costs half the instructions of 64-bit.
+__device__ __forceinline__ int IX(const Dev& d, int k, int l) { return (k - 1) * d.g.P + (l - 1); }
 __device__ __forceinline__ double zl(const Dev& d, int k) { return d.g.zlevel[k - 1]; }
 __device__ __forceinline__ int NB(const int* a, int l) { return a[l - 1]; }
 

@@ -22,6 +22,19 @@ constexpr int TB = 128;
 __device__ __forceinline__ bool ewet(const Dev& d, int l) { return NB(d.g.lEC, l) != d.g.lm1; }
 __device__ __forceinline__ bool nwet(const Dev& d, int l) { return NB(d.g.lNC, l) != d.g.lm1; }
 
+// Deepest level of column l whose values can change.  Below kmz+1 the reference keeps
+// h = hp = hpp = 0, wp = 0 and sal/salp/salpp/rhop at their initial values, and below the face
+// depth min(kmz(l), kmz(lE)) it keeps hu = hup = hupp = uh-derived fields = 0 (a closed face keeps
+// them 0 everywhere); its full-column loops rewrite those levels with identical values, so the
+// loops below stop at these limits and the state stays bit-identical.
+__device__ __forceinline__ int zlim(const Dev& d, int l) { return NB(d.g.kmz, l) + 1; }
+__device__ __forceinline__ int ulim(const Dev& d, int l) {
+  return ewet(d, l) ? min(NB(d.g.kmz, l), NB(d.g.kmz, NB(d.g.lEC, l))) : 0;
+}
+__device__ __forceinline__ int vlim(const Dev& d, int l) {
+  return nwet(d, l) ? min(NB(d.g.kmz, l), NB(d.g.kmz, NB(d.g.lNC, l))) : 0;
+}
+
 // layer_hp2 for column l (the version that recomputes hp/hup/hvp from sp)
 __device__ void layer_hp2_col(const Dev& d, int l) {
   const int kms = NB(d.g.kmz, l);
@@ -80,12 +93,13 @@ __global__ void k_slayer_h(Dev d) {
   const int kz = d.s.k1z[l - 1], ku = d.s.k1u[l - 1], kv = d.s.k1v[l - 1];
   double* h = d.f.h; double* hu = d.f.hu; double* hv = d.f.hv;
   const double* hp = d.f.hp; const double* hup = d.f.hup; const double* hvp = d.f.hvp;
-  for (int k = 1; k <= kz - 1; ++k) h[IX(d, k, l)] = hp[IX(d, k, l)];
-  for (int k = 1; k <= ku - 1; ++k) hu[IX(d, k, l)] = hup[IX(d, k, l)];
-  for (int k = 1; k <= kv - 1; ++k) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
-  for (int k = kz + 2; k <= km1; ++k) h[IX(d, k, l)] = hp[IX(d, k, l)];
-  for (int k = ku + 1; k <= km1; ++k) hu[IX(d, k, l)] = hup[IX(d, k, l)];
-  for (int k = kv + 2; k <= km1; ++k) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
+  const int zL = zlim(d, l), uL = ulim(d, l), vL = vlim(d, l);
+  for (int k = 1; k <= min(kz - 1, zL); ++k) h[IX(d, k, l)] = hp[IX(d, k, l)];
+  for (int k = 1; k <= min(ku - 1, uL); ++k) hu[IX(d, k, l)] = hup[IX(d, k, l)];
+  for (int k = 1; k <= min(kv - 1, vL); ++k) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
+  for (int k = kz + 2; k <= zL; ++k) h[IX(d, k, l)] = hp[IX(d, k, l)];
+  for (int k = ku + 1; k <= uL; ++k) hu[IX(d, k, l)] = hup[IX(d, k, l)];
+  for (int k = kv + 2; k <= vL; ++k) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
   // Surface layers.  A column whose surface index has reached the bottom level (every layer
   // dry) is left untouched: the reference would read zlevel past km1 there.
   const double sl = d.s.s[l - 1];
@@ -108,9 +122,7 @@ __global__ void k_slayer_h(Dev d) {
       // on drying the reference recomputes the same layer (k is reset to k1u, :2136)
       hu[IX(d, ku, l)] = (haux <= HMIN) ? ZERO : haux;
     }
-  } else {
-    for (int kk = ku; kk <= ku + 1 && kk <= km1; ++kk) hu[IX(d, kk, l)] = hup[IX(d, kk, l)];
-  }
+  }  // a closed east face keeps hu = hup = 0 (the reference's copy of hup(k1u:k1u+1) is a no-op)
   if (nwet(d, l)) {
     const double sm = fmax(sl, d.s.s[NB(d.g.lNC, l) - 1]);
     k = kv;
@@ -125,9 +137,7 @@ __global__ void k_slayer_h(Dev d) {
         }
       } else hv[IX(d, k, l)] = haux;
     }
-  } else {
-    for (int kk = kv; kk <= kv + 1 && kk <= km1; ++kk) hv[IX(d, kk, l)] = hvp[IX(d, kk, l)];
-  }
+  }  // a closed north face keeps hv = hvp = 0
 }
 
 // ------------------------------------------------------------- vel (uh, vh, k1u, k1v)
@@ -165,7 +175,7 @@ __global__ void k_cont1(Dev d) {
   const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l);
   if (k1s <= kms) {
     double* wp = d.f.wp;
-    for (int k = 1; k <= d.g.km1; ++k) wp[IX(d, k, l)] = 0.0;
+    for (int k = 1; k < k1s; ++k) wp[IX(d, k, l)] = 0.0;   // wp below kms is never non-zero
     double w = 0.0;
     for (int k = kms; k >= k1s; --k) {
       w = w - (d.f.uh[IX(d, k, l)] - d.f.uh[IX(d, k, lW)] + d.f.uhpp[IX(d, k, l)] - d.f.uhpp[IX(d, k, lW)]) / d.p.twodx -
@@ -189,7 +199,7 @@ __global__ void k_cont2(Dev d) {
   if (k1s > kms) return;
   const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l);
   double* wp = d.f.wp;
-  for (int k = 1; k <= d.g.km1; ++k) wp[IX(d, k, l)] = 0.0;
+  for (int k = 1; k < k1s; ++k) wp[IX(d, k, l)] = 0.0;   // wp below kms is never non-zero
   double w = 0.0;
   for (int k = kms; k >= k1s; --k) {
     w = w - (d.f.uhp[IX(d, k, l)] - d.f.uhp[IX(d, k, lW)]) / d.p.dx - (d.f.vhp[IX(d, k, l)] - d.f.vhp[IX(d, k, lS)]) / d.p.dy;
@@ -224,7 +234,7 @@ __global__ void k_exsal_flux(Dev d) {
   const double* hpp = d.f.hpp;
   const double* hp = d.f.hp;
   for (int k = k1s; k <= kms; ++k) {
-    const size_t ik = IX(d, k, l);
+    const int ik = IX(d, k, l);
     // EW
     if (d.f.hup[ik] > ZERO) {
       const double vel = (d.f.uhpp[ik] + d.f.uh[ik]) / 2.;
@@ -276,7 +286,7 @@ __global__ void k_exsal_imsal(Dev d) {
   double* sal = d.f.sal;
   double* esc = d.scr;
   auto bex = [&](int k) -> double {
-    const size_t ik = IX(d, k, l);
+    const int ik = IX(d, k, l);
     const double spc = sp[ik];
     double v = d.f.hpp[ik] * spc / twodt1 - (d.f.Bth2[ik] - d.f.Bth2[IX(d, k, lW)]) / d.p.dx -
                (d.f.Bth4[ik] - d.f.Bth4[IX(d, k, lS)]) / d.p.dy - (d.f.Bth3[ik] - d.f.Bth3[IX(d, k + 1, l)]);
@@ -403,10 +413,10 @@ __global__ void k_half_zeta(Dev d, int rotate) {
   if (l > d.g.lm) return;
   if (rotate) {
     d.s.spp[l - 1] = d.s.sp[l - 1];
-    for (int k = 1; k <= d.g.km1; ++k) {
-      const size_t ik = IX(d, k, l);
-      d.f.hpp[ik] = d.f.hp[ik]; d.f.hupp[ik] = d.f.hup[ik]; d.f.hvpp[ik] = d.f.hvp[ik];
-    }
+    const int zL = zlim(d, l), uL = ulim(d, l), vL = vlim(d, l);
+    for (int k = 1; k <= zL; ++k) d.f.hpp[IX(d, k, l)] = d.f.hp[IX(d, k, l)];
+    for (int k = 1; k <= uL; ++k) d.f.hupp[IX(d, k, l)] = d.f.hup[IX(d, k, l)];
+    for (int k = 1; k <= vL; ++k) d.f.hvpp[IX(d, k, l)] = d.f.hvp[IX(d, k, l)];
   }
   d.s.sp[l - 1] = 0.5 * (d.s.s[l - 1] + d.s.spp[l - 1]);
 }
@@ -416,14 +426,14 @@ __device__ void half_velocities(const Dev& d, int l, bool rotate) {
   if (ewet(d, l)) {
     const int kmx = min(NB(d.g.kmz, l), NB(d.g.kmz, NB(d.g.lEC, l)));
     for (int k = d.g.k1; k <= kmx; ++k) {
-      const size_t ik = IX(d, k, l);
+      const int ik = IX(d, k, l);
       if (rotate) { d.f.uhpp[ik] = d.f.uhp[ik]; d.f.upp[ik] = d.f.up[ik]; }
       const double hup = d.f.hup[ik];
       if (hup > ZERO) { const double v = 0.5 * (d.f.uh[ik] + d.f.uhpp[ik]); d.f.uhp[ik] = v; d.f.up[ik] = v / hup; }
       else { d.f.uhp[ik] = 0.0; d.f.up[ik] = 0.0; }
     }
     const int k = d.s.k1u[l - 1];
-    const size_t ik = IX(d, k, l);
+    const int ik = IX(d, k, l);
     if (d.f.hu[IX(d, k - 1, l)] > ZERO) {
       d.f.uhp[ik] = d.f.uhp[ik] + d.f.uh[IX(d, k - 1, l)] / 2.;
       d.f.up[ik] = d.f.uhp[ik] / d.f.hup[ik];
@@ -436,14 +446,14 @@ __device__ void half_velocities(const Dev& d, int l, bool rotate) {
   if (nwet(d, l)) {
     const int kmy = min(NB(d.g.kmz, l), NB(d.g.kmz, NB(d.g.lNC, l)));
     for (int k = d.g.k1; k <= kmy; ++k) {
-      const size_t ik = IX(d, k, l);
+      const int ik = IX(d, k, l);
       if (rotate) { d.f.vhpp[ik] = d.f.vhp[ik]; d.f.vpp[ik] = d.f.vp[ik]; }
       const double hvp = d.f.hvp[ik];
       if (hvp > ZERO) { const double v = 0.5 * (d.f.vh[ik] + d.f.vhpp[ik]); d.f.vhp[ik] = v; d.f.vp[ik] = v / hvp; }
       else { d.f.vhp[ik] = 0.0; d.f.vp[ik] = 0.0; }
     }
     const int k = d.s.k1v[l - 1];
-    const size_t ik = IX(d, k, l);
+    const int ik = IX(d, k, l);
     if (d.f.hv[IX(d, k - 1, l)] > ZERO) {
       d.f.vhp[ik] = d.f.vhp[ik] + d.f.vh[IX(d, k - 1, l)] / 2.;
       d.f.vp[ik] = d.f.vhp[ik] / d.f.hvp[ik];
@@ -464,7 +474,7 @@ __global__ void k_half_level(Dev d, int rotate) {
   top_index_col(d, l);
   const int kms = NB(d.g.kmz, l);
   for (int k = d.g.k1; k <= kms; ++k) {
-    const size_t ik = IX(d, k, l);
+    const int ik = IX(d, k, l);
     const double z = zmid(d, k, d.f.hp[ik]);
     if (rotate) d.f.salpp[ik] = d.f.salp[ik];
     const double sp = (d.f.sal[ik] + d.f.salpp[ik]) / 2.;
@@ -480,24 +490,40 @@ __global__ void k_save(Dev d, int istep) {
   if (l > d.g.lm) return;
   if (istep == 1) d.s.spp[l - 1] = d.s.sp[l - 1];
   d.s.sp[l - 1] = d.s.s[l - 1];
-  for (int k = 1; k <= d.g.km1; ++k) {
-    const size_t ik = IX(d, k, l);
-    if (istep == 1) { d.f.hpp[ik] = d.f.hp[ik]; d.f.hupp[ik] = d.f.hup[ik]; d.f.hvpp[ik] = d.f.hvp[ik]; }
-    d.f.hp[ik] = d.f.h[ik]; d.f.hup[ik] = d.f.hu[ik]; d.f.hvp[ik] = d.f.hv[ik];
+  const int zL = zlim(d, l), uL = ulim(d, l), vL = vlim(d, l);
+  for (int k = 1; k <= zL; ++k) {
+    const int ik = IX(d, k, l);
+    if (istep == 1) d.f.hpp[ik] = d.f.hp[ik];
+    d.f.hp[ik] = d.f.h[ik];
+  }
+  for (int k = 1; k <= uL; ++k) {
+    const int ik = IX(d, k, l);
+    if (istep == 1) d.f.hupp[ik] = d.f.hup[ik];
+    d.f.hup[ik] = d.f.hu[ik];
+  }
+  for (int k = 1; k <= vL; ++k) {
+    const int ik = IX(d, k, l);
+    if (istep == 1) d.f.hvpp[ik] = d.f.hvp[ik];
+    d.f.hvp[ik] = d.f.hv[ik];
   }
   top_index_col(d, l);
-  for (int k = d.g.k1; k <= d.g.km; ++k) {
-    const size_t ik = IX(d, k, l);
+  for (int k = d.g.k1; k <= min(d.g.km, zL); ++k) {
+    const int ik = IX(d, k, l);
     const double z = zmid(d, k, d.f.hp[ik]);
     if (istep == 1) d.f.salpp[ik] = d.f.salp[ik];
     d.f.salp[ik] = d.f.sal[ik];
     d.f.rhop[ik] = densty_s(d.f.salp[ik], 0.00004, z) - 1000.;
-    if (istep == 1) {
-      d.f.uhpp[ik] = d.f.uhp[ik]; d.f.vhpp[ik] = d.f.vhp[ik]; d.f.upp[ik] = d.f.up[ik]; d.f.vpp[ik] = d.f.vp[ik];
-    }
+  }
+  for (int k = d.g.k1; k <= uL; ++k) {
+    const int ik = IX(d, k, l);
+    if (istep == 1) { d.f.uhpp[ik] = d.f.uhp[ik]; d.f.upp[ik] = d.f.up[ik]; }
     const double hup = d.f.hup[ik];
     if (hup > ZERO) { const double v = d.f.uh[ik]; d.f.uhp[ik] = v; d.f.up[ik] = v / hup; }
     else { d.f.uhp[ik] = 0.0; d.f.up[ik] = 0.0; }
+  }
+  for (int k = d.g.k1; k <= vL; ++k) {
+    const int ik = IX(d, k, l);
+    if (istep == 1) { d.f.vhpp[ik] = d.f.vhp[ik]; d.f.vpp[ik] = d.f.vp[ik]; }
     const double hvp = d.f.hvp[ik];
     if (hvp > ZERO) { const double v = d.f.vh[ik]; d.f.vhp[ik] = v; d.f.vp[ik] = v / hvp; }
     else { d.f.vhp[ik] = 0.0; d.f.vp[ik] = 0.0; }
@@ -509,7 +535,7 @@ __global__ void k_density_init(Dev d) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (l > d.g.lm1) return;
   for (int k = d.g.k1; k <= d.g.km1; ++k) {
-    const size_t ik = IX(d, k, l);
+    const int ik = IX(d, k, l);
     d.f.rhop[ik] = densty_s(d.f.salp[ik], 0.00004, zmid(d, k, d.f.hp[ik])) - 1000.;
   }
 }

@@ -21,6 +21,8 @@
 // use fixed-order block partials reduced by the last block to finish (no spin-waits), so results
 // are deterministic.  Scalars stay on the device; every kernel returns at once when `done` is set,
 // which lets the host run batches of iterations without a round trip per iteration.
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -117,7 +119,8 @@ __global__ void k_pcg_gather(Dev d, PcgDev P, int color, int x0_mode, const doub
   const PcgColor& C = color ? P.B : P.R;
   if (i > C.n) return;
   if (i == C.n) {  // the permanent zero slot
-    C.sx[i] = 0.0; C.sy[i] = 0.0; C.u[i] = 0.0; C.r[i] = 0.0; C.z[i] = 0.0; C.p[i] = 0.0; C.q[i] = 0.0;
+    C.sx[i] = 0.0; C.sy[i] = 0.0; C.u[i] = 0.0; C.r[i] = 0.0; C.z[i] = 0.0; C.p[i] = 0.0; C.p2[i] = 0.0;
+    C.q[i] = 0.0;
     C.rhs[i] = 0.0; C.dinv[i] = 0.0;
     return;
   }
@@ -128,7 +131,7 @@ __global__ void k_pcg_gather(Dev d, PcgDev P, int color, int x0_mode, const doub
   double x0 = (x0_mode == 1) ? 0.0 : d.s.sp[l - 1];
   if (x0_mode == 2 && dz) x0 = x0 + dz[l - 1];
   C.u[i] = x0;
-  C.z[i] = 0.0; C.p[i] = 0.0; C.q[i] = 0.0;
+  C.z[i] = 0.0; C.p[i] = 0.0; C.p2[i] = 0.0; C.q[i] = 0.0;
 }
 
 // Red pivots are the diagonal itself (no lower neighbours in red-black order).
@@ -200,36 +203,49 @@ __global__ void k_pcg_bnorm(PcgDev P) {
   }
 }
 
-// Black half of z = M^-1 r, fused with u += alpha p and r -= alpha q.
-__global__ void __launch_bounds__(PB) k_pcg_black_solve(PcgDev P) {
+// Each thread of the iteration kernels handles NPT nodes of one colour (node = block base +
+// r * PB + thread, so every r-slice is a coalesced access and the NPT slices are independent
+// loads in flight).  Fewer, fuller blocks keep the last-block reductions short.
+constexpr int NPT = 4;
+
+// Black half of z = M^-1 r, fused with u += alpha p and r -= alpha q (itcg :9031, :9088).
+// `par` selects the current p buffer (p is double-buffered across iterations).
+template <typename T>
+__global__ void __launch_bounds__(PB) k_pcg_black_solve(PcgDevT<T> P, int par) {
   __shared__ double sh[32];
   if (P.sc->done) return;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const PcgColor &R = P.R, &B = P.B;
-  const double alpha = P.sc->alpha;
+  const PcgColorT<T> &R = P.R, &B = P.B;
+  const T* __restrict__ Bp = par ? B.p2 : B.p;
+  const T alpha = (T)P.sc->alpha;
   double rr = 0, rz = 0, uu = 0, zz = 0;
-  if (j < B.n) {
-    const int4 nb = B.nbr[j];
-    const double uj = B.u[j] + alpha * B.p[j];
-    const double rj = B.r[j] - alpha * B.q[j];
-    B.u[j] = uj;
-    B.r[j] = rj;
-    // icfstp: the red rows scatter into this black row in l order W, S, N, E
-    const int ks[4] = {nb.x, nb.y, nb.z, nb.w};
-    const double t[4] = {-R.sx[nb.x], -R.sy[nb.y], -B.sy[j], -B.sx[j]};
-    double x = rj;
-    for (int c = 0; c < 4; ++c) {
-      const int k = ks[c];
-      const double rk = R.r[k] - alpha * R.q[k];
-      const double xfk = rk * R.dinv[k];
-      x = x - t[c] * xfk;
+#pragma unroll
+  for (int q = 0; q < NPT; ++q) {
+    const int j = blockIdx.x * (PB * NPT) + q * PB + threadIdx.x;
+    if (j < B.n) {
+      const int4 nb = B.nbr[j];
+      const T uj = B.u[j] + alpha * Bp[j];
+      const T rj = B.r[j] - alpha * B.q[j];
+      B.u[j] = uj;
+      B.r[j] = rj;
+      // icfstp: the red rows scatter into this black row in l order W, S, N, E
+      const int ks[4] = {nb.x, nb.y, nb.z, nb.w};
+      const T t[4] = {-R.sx[nb.x], -R.sy[nb.y], -B.sy[j], -B.sx[j]};
+      T x = rj;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int k = ks[c];
+        const T rk = R.r[k] - alpha * R.q[k];
+        const T xfk = rk * R.dinv[k];
+        x = x - t[c] * xfk;
+      }
+      const T dj = B.dinv[j];
+      x = x * dj;                // icfstp: x(i) = x(i)*d(i)
+      x = x / dj;                // icsp:   x(i) = x(i)/d(i)
+      const T zj = x * dj;  // icbsp on a row with no upper entries
+      B.z[j] = zj;
+      rr += (double)rj * (double)rj; rz += (double)rj * (double)zj; uu += (double)uj * (double)uj;
+      zz += (double)zj * (double)zj;
     }
-    const double dj = B.dinv[j];
-    x = x * dj;          // icfstp: x(i) = x(i)*d(i)
-    x = x / dj;          // icsp:   x(i) = x(i)/d(i)
-    const double zj = x * dj;  // icbsp on a row with no upper entries
-    B.z[j] = zj;
-    rr = rj * rj; rz = rj * zj; uu = uj * uj; zz = zj * zj;
   }
   double s;
   s = block_sum(rr, sh); if (threadIdx.x == 0) P.part0[blockIdx.x] = s;
@@ -241,30 +257,36 @@ __global__ void __launch_bounds__(PB) k_pcg_black_solve(PcgDev P) {
 }
 
 // Red half of z = M^-1 r (+ u/r updates), then the (r,z) reduction, the stopping test and beta.
-__global__ void __launch_bounds__(PB) k_pcg_red_solve(PcgDev P, int nblk_black) {
+template <typename T>
+__global__ void __launch_bounds__(PB) k_pcg_red_solve(PcgDevT<T> P, int par, int nblk_black) {
   __shared__ double sh[32];
   if (P.sc->done) return;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const PcgColor &R = P.R, &B = P.B;
-  const double alpha = P.sc->alpha;
+  const PcgColorT<T> &R = P.R, &B = P.B;
+  const T* __restrict__ Rp = par ? R.p2 : R.p;
+  const T alpha = (T)P.sc->alpha;
   double rr = 0, rz = 0, uu = 0, zz = 0;
-  if (k < R.n) {
-    const int4 nb = R.nbr[k];
-    const double uk = R.u[k] + alpha * R.p[k];
-    const double rk = R.r[k] - alpha * R.q[k];
-    R.u[k] = uk;
-    R.r[k] = rk;
-    const double dk = R.dinv[k];
-    double x = rk * dk;   // icfstp
-    x = x / dk;           // icsp
-    // icbsp: sum = x - t(k,W) z_W - t(k,S) z_S - t(k,N) z_N - t(k,E) z_E
-    x = x - (-B.sx[nb.x]) * B.z[nb.x];
-    x = x - (-B.sy[nb.y]) * B.z[nb.y];
-    x = x - (-R.sy[k]) * B.z[nb.z];
-    x = x - (-R.sx[k]) * B.z[nb.w];
-    const double zk = x * dk;
-    R.z[k] = zk;
-    rr = rk * rk; rz = rk * zk; uu = uk * uk; zz = zk * zk;
+#pragma unroll
+  for (int q = 0; q < NPT; ++q) {
+    const int k = blockIdx.x * (PB * NPT) + q * PB + threadIdx.x;
+    if (k < R.n) {
+      const int4 nb = R.nbr[k];
+      const T uk = R.u[k] + alpha * Rp[k];
+      const T rk = R.r[k] - alpha * R.q[k];
+      R.u[k] = uk;
+      R.r[k] = rk;
+      const T dk = R.dinv[k];
+      T x = rk * dk;   // icfstp
+      x = x / dk;           // icsp
+      // icbsp: sum = x - t(k,W) z_W - t(k,S) z_S - t(k,N) z_N - t(k,E) z_E
+      x = x - (-B.sx[nb.x]) * B.z[nb.x];
+      x = x - (-B.sy[nb.y]) * B.z[nb.y];
+      x = x - (-R.sy[k]) * B.z[nb.z];
+      x = x - (-R.sx[k]) * B.z[nb.w];
+      const T zk = x * dk;
+      R.z[k] = zk;
+      rr += (double)rk * (double)rk; rz += (double)rk * (double)zk; uu += (double)uk * (double)uk;
+      zz += (double)zk * (double)zk;
+    }
   }
   const int off = nblk_black;
   double s;
@@ -323,62 +345,49 @@ __global__ void __launch_bounds__(PB) k_pcg_red_solve(PcgDev P, int nblk_black) 
   if (S->in != 0) S->beta = S->rzdot / S->dkm1;
 }
 
-// p = z + beta p and q = A p on the black nodes (red neighbours' new p formed on the fly).
-__global__ void __launch_bounds__(PB) k_pcg_black_apply(PcgDev P) {
+// p = z + beta p and q = A p on both colours in one launch (blocks [0, nblk_red) take red
+// nodes, the rest black).  The other colour's new p is formed on the fly from its z and old p,
+// with the same expression, so both colours see identical values; p is double-buffered.
+// Then (p,q), alpha and the iteration count (itcg :9064-9086).
+template <typename T>
+__global__ void __launch_bounds__(PB) k_pcg_apply(PcgDevT<T> P, int par, int nblk_red) {
   __shared__ double sh[32];
   if (P.sc->done) return;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  const PcgColor &R = P.R, &B = P.B;
-  const double beta = P.sc->beta;
+  const bool red = blockIdx.x < (unsigned)nblk_red;
+  const PcgColorT<T>& C = red ? P.R : P.B;
+  const PcgColorT<T>& O = red ? P.B : P.R;
+  const T* __restrict__ Cp = par ? C.p2 : C.p;
+  const T* __restrict__ Op = par ? O.p2 : O.p;
+  T* __restrict__ Cn = par ? C.p : C.p2;
+  const int blk = red ? blockIdx.x : blockIdx.x - nblk_red;
+  const T beta = (T)P.sc->beta;
   double pq = 0;
-  if (j < B.n) {
-    const int4 nb = B.nbr[j];
-    const double pj = B.z[j] + beta * B.p[j];
-    const double pW = R.z[nb.x] + beta * R.p[nb.x];
-    const double pS = R.z[nb.y] + beta * R.p[nb.y];
-    const double pN = R.z[nb.z] + beta * R.p[nb.z];
-    const double pE = R.z[nb.w] + beta * R.p[nb.w];
-    const double sxW = R.sx[nb.x], syS = R.sy[nb.y];
-    const double diag = 1 + B.sx[j] + sxW + B.sy[j] + syS;
-    double y = diag * pj;
-    y = y + (-sxW) * pW;
-    y = y + (-syS) * pS;
-    y = y + (-B.sy[j]) * pN;
-    y = y + (-B.sx[j]) * pE;
-    B.p[j] = pj;
-    B.q[j] = y;
-    pq = pj * y;
+#pragma unroll
+  for (int q = 0; q < NPT; ++q) {
+    const int i = blk * (PB * NPT) + q * PB + threadIdx.x;
+    if (i < C.n) {
+      const int4 nb = C.nbr[i];
+      const T pi = C.z[i] + beta * Cp[i];
+      const T pW = O.z[nb.x] + beta * Op[nb.x];
+      const T pS = O.z[nb.y] + beta * Op[nb.y];
+      const T pN = O.z[nb.z] + beta * Op[nb.z];
+      const T pE = O.z[nb.w] + beta * Op[nb.w];
+      const T sxW = O.sx[nb.x], syS = O.sy[nb.y];
+      const T diag = (T)1 + C.sx[i] + sxW + C.sy[i] + syS;
+      T y = diag * pi;
+      y = y + (-sxW) * pW;
+      y = y + (-syS) * pS;
+      y = y + (-C.sy[i]) * pN;
+      y = y + (-C.sx[i]) * pE;
+      Cn[i] = pi;
+      C.q[i] = y;
+      pq += (double)pi * (double)y;
+    }
   }
   const double s = block_sum(pq, sh);
   if (threadIdx.x == 0) P.part0[blockIdx.x] = s;
-}
-
-// p = z + beta p and q = A p on the red nodes, then (p,q), alpha and the iteration count.
-__global__ void __launch_bounds__(PB) k_pcg_red_apply(PcgDev P, int nblk_black) {
-  __shared__ double sh[32];
-  if (P.sc->done) return;
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
-  const PcgColor &R = P.R, &B = P.B;
-  const double beta = P.sc->beta;
-  double pq = 0;
-  if (k < R.n) {
-    const int4 nb = R.nbr[k];
-    const double pk = R.z[k] + beta * R.p[k];
-    const double sxW = B.sx[nb.x], syS = B.sy[nb.y];
-    const double diag = 1 + R.sx[k] + sxW + R.sy[k] + syS;
-    double y = diag * pk;
-    y = y + (-sxW) * B.p[nb.x];
-    y = y + (-syS) * B.p[nb.y];
-    y = y + (-R.sy[k]) * B.p[nb.z];
-    y = y + (-R.sx[k]) * B.p[nb.w];
-    R.p[k] = pk;
-    R.q[k] = y;
-    pq = pk * y;
-  }
-  const double s = block_sum(pq, sh);
-  if (threadIdx.x == 0) P.part0[nblk_black + blockIdx.x] = s;
   if (!last_block(&P.sc->cnt[1])) return;
-  const double pap = reduce_partials(P.part0, nblk_black + gridDim.x, sh);
+  const double pap = reduce_partials(P.part0, gridDim.x, sh);
   if (threadIdx.x != 0) return;
   PcgScal* S = P.sc;
   S->alphao = S->alpha;
@@ -408,14 +417,20 @@ void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, int
   k_pcg_bnorm<<<(nR + nB + PB - 1) / PB, PB, 0, st>>>(P);
 }
 
-void pcg_iteration(const PcgDev& P, cudaStream_t st) {
+void pcg_iteration(const PcgDev& P, int par, cudaStream_t st) {
   const int nR = P.R.n, nB = P.B.n;
-  const int gB = (nB + PB - 1) / PB, gR = (nR + PB - 1) / PB;
-  const int gBb = gB > 0 ? gB : 1, gRr = gR > 0 ? gR : 1;
-  k_pcg_black_solve<<<gBb, PB, 0, st>>>(P);
-  k_pcg_red_solve<<<gRr, PB, 0, st>>>(P, gBb);
-  k_pcg_black_apply<<<gBb, PB, 0, st>>>(P);
-  k_pcg_red_apply<<<gRr, PB, 0, st>>>(P, gBb);
+  const int gB = std::max((nB + PB * NPT - 1) / (PB * NPT), 1), gR = std::max((nR + PB * NPT - 1) / (PB * NPT), 1);
+  k_pcg_black_solve<double><<<gB, PB, 0, st>>>(P, par);
+  k_pcg_red_solve<double><<<gR, PB, 0, st>>>(P, par, gB);
+  k_pcg_apply<double><<<gR + gB, PB, 0, st>>>(P, par, gR);
+}
+
+void pcg_iteration_f(const PcgDevF& F, int par, cudaStream_t st) {
+  const int nR = F.R.n, nB = F.B.n;
+  const int gB = std::max((nB + PB * NPT - 1) / (PB * NPT), 1), gR = std::max((nR + PB * NPT - 1) / (PB * NPT), 1);
+  k_pcg_black_solve<float><<<gB, PB, 0, st>>>(F, par);
+  k_pcg_red_solve<float><<<gR, PB, 0, st>>>(F, par, gB);
+  k_pcg_apply<float><<<gR + gB, PB, 0, st>>>(F, par, gR);
 }
 
 void pcg_finish(const Dev& d, const PcgDev& P, cudaStream_t st) {
@@ -424,8 +439,66 @@ void pcg_finish(const Dev& d, const PcgDev& P, cudaStream_t st) {
   if (nB > 0) k_pcg_scatter<<<(nB + PB - 1) / PB, PB, 0, st>>>(d, P, 1);
 }
 
+// ------------------------------------------------------------------ iterative refinement
+// FP64 residual of the current FP64 iterate and ||r||^2 (into sc->stptst, fixed-order sum).
+__global__ void k_ir_norm(PcgDev P) {
+  __shared__ double sh[32];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nR = P.R.n, nB = P.B.n;
+  double v = 0;
+  if (i < nR) v = P.R.r[i] * P.R.r[i];
+  else if (i < nR + nB) v = P.B.r[i - nR] * P.B.r[i - nR];
+  const double bs = block_sum(v, sh);
+  if (threadIdx.x == 0) P.part0[blockIdx.x] = bs;
+  if (last_block(&P.sc->cnt[3])) {
+    const double tot = reduce_partials(P.part0, gridDim.x, sh);
+    if (threadIdx.x == 0) P.sc->stptst = tot;
+  }
+}
+
+// Inner FP32 system for the correction e: A e = r with e0 = 0.  Coefficients and the FP64 MIC
+// pivots are rounded to FP32; the inner stopping test (test 5 on the inner residual) uses
+// bnorm = ||r||.
+__global__ void k_ir_inner_setup(PcgDev P, PcgDevF F, int color) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const PcgColor& C = color ? P.B : P.R;
+  const PcgColorT<float>& G = color ? F.B : F.R;
+  if (i > C.n) return;
+  G.sx[i] = (float)C.sx[i];
+  G.sy[i] = (float)C.sy[i];
+  G.dinv[i] = (float)C.dinv[i];
+  G.r[i] = (float)C.r[i];
+  G.u[i] = 0.f; G.z[i] = 0.f; G.p[i] = 0.f; G.p2[i] = 0.f; G.q[i] = 0.f;
+}
+
+// u += e in FP64 (the zeta update is kept in double precision).
+__global__ void k_ir_correct(PcgDev P, PcgDevF F, int color) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const PcgColor& C = color ? P.B : P.R;
+  const PcgColorT<float>& G = color ? F.B : F.R;
+  if (i >= C.n) return;
+  C.u[i] = C.u[i] + (double)G.u[i];
+}
+
+void ir_residual(const PcgDev& P, cudaStream_t st) {
+  const int nR = P.R.n, nB = P.B.n;
+  if (nR > 0) k_pcg_resid0<<<(nR + PB - 1) / PB, PB, 0, st>>>(P, 0);
+  if (nB > 0) k_pcg_resid0<<<(nB + PB - 1) / PB, PB, 0, st>>>(P, 1);
+  k_ir_norm<<<(nR + nB + PB - 1) / PB, PB, 0, st>>>(P);
+}
+
+void ir_inner_setup(const PcgDev& P, const PcgDevF& F, cudaStream_t st) {
+  k_ir_inner_setup<<<(P.R.n + 1 + PB - 1) / PB, PB, 0, st>>>(P, F, 0);
+  k_ir_inner_setup<<<(P.B.n + 1 + PB - 1) / PB, PB, 0, st>>>(P, F, 1);
+}
+
+void ir_correct(const PcgDev& P, const PcgDevF& F, cudaStream_t st) {
+  if (P.R.n > 0) k_ir_correct<<<(P.R.n + PB - 1) / PB, PB, 0, st>>>(P, F, 0);
+  if (P.B.n > 0) k_ir_correct<<<(P.B.n + PB - 1) / PB, PB, 0, st>>>(P, F, 1);
+}
+
 int pcg_max_blocks(int nR, int nB) {
-  return (nR + PB - 1) / PB + (nB + PB - 1) / PB + 2;
+  return (nR + PB - 1) / PB + (nB + PB - 1) / PB + 2;   // also covers the setup kernels' grids
 }
 
 }  // namespace si3d

@@ -4,13 +4,16 @@
 
 namespace si3d {
 
-// One colour of the red-black ordered zeta system (see k_zeta.cu).
-struct PcgColor {
+// One colour of the red-black ordered zeta system (see k_zeta.cu), with vectors and coefficients
+// of type T (double for the plain solve, float for the inner solve of iterative refinement).
+template <typename T>
+struct PcgColorT {
   int n;                 // nodes of this colour; arrays hold n + 1 entries (entry n = 0)
   const int* l;          // [n] reference column index (1-based)
   const int4* nbr;       // [n] W, S, N, E as indices into the other colour (absent -> other.n)
-  double *sx, *sy, *rhs, *u, *r, *z, *p, *q, *dinv, *diag, *rs;
+  T *sx, *sy, *rhs, *u, *r, *z, *p, *p2, *q, *dinv, *diag, *rs;   // p/p2: double-buffered search direction
 };
+using PcgColor = PcgColorT<double>;
 
 // Device-resident CG scalars (NSPCG common blocks itcom1/itcom3 that itcg and pstops use).
 struct PcgScal {
@@ -19,20 +22,30 @@ struct PcgScal {
   unsigned int cnt[4];
 };
 
-struct PcgDev {
-  PcgColor R, B;
+template <typename T>
+struct PcgDevT {
+  PcgColorT<T> R, B;
   PcgScal* sc;
   double *part0, *part1, *part2, *part3;
   double *hist_alpha, *hist_beta;
 };
+using PcgDev = PcgDevT<double>;
+using PcgDevF = PcgDevT<float>;
 
 void launch_momentum(const Dev& d, int ieq, const int* cols, int ncols, cudaStream_t st);
 void launch_matcon(const Dev& d, cudaStream_t st);
 
 void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, int* negpiv, cudaStream_t st);
-void pcg_iteration(const PcgDev& P, cudaStream_t st);
+void pcg_iteration(const PcgDev& P, int par, cudaStream_t st);
 void pcg_finish(const Dev& d, const PcgDev& P, cudaStream_t st);
 int pcg_max_blocks(int nR, int nB);
+// Iterative refinement: FP64 residual r = rhs - A u and its squared norm into P.sc->stptst
+// (the host compares it with bnorm); FP32 inner-system set-up from the FP64 residual; the
+// FP32 iteration; the FP64 correction u += e.
+void ir_residual(const PcgDev& P, cudaStream_t st);
+void ir_inner_setup(const PcgDev& P, const PcgDevF& F, cudaStream_t st);
+void pcg_iteration_f(const PcgDevF& F, int par, cudaStream_t st);
+void ir_correct(const PcgDev& P, const PcgDevF& F, cudaStream_t st);
 
 void launch_slayer_h(const Dev& d, cudaStream_t st);
 void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cudaStream_t st);

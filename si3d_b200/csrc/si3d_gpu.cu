@@ -73,6 +73,10 @@ struct Ctx {
   int nce = 0, ncn = 0;
   // red-black zeta system
   PcgDev pcg{};
+  PcgDevF pcgf{};            // FP32 inner system of iterative refinement
+  PcgScal* h_scf = nullptr;  // pinned
+  int last_inner = 8;
+  long long ir_outer = 0;
   PcgScal* h_sc = nullptr;  // pinned
   double* h_hist = nullptr; // pinned, 2 x itmax
   int last_iters = 8;
@@ -90,6 +94,7 @@ struct Ctx {
     if (st) cudaStreamSynchronize(st);
     for (void* p : allocs) cudaFree(p);
     if (h_sc) cudaFreeHost(h_sc);
+    if (h_scf) cudaFreeHost(h_scf);
     if (h_hist) cudaFreeHost(h_hist);
     for (cudaEvent_t e : {ev0, ev1, evp0, evp1, pe0, pe1}) if (e) cudaEventDestroy(e);
     if (st) cudaStreamDestroy(st);
@@ -241,7 +246,7 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
     C.l = dl;
     C.nbr = dn;
     const size_t n1 = L.size() + 1;
-    for (double** p : {&C.sx, &C.sy, &C.rhs, &C.u, &C.r, &C.z, &C.p, &C.q, &C.dinv, &C.diag, &C.rs})
+    for (double** p : {&C.sx, &C.sy, &C.rhs, &C.u, &C.r, &C.z, &C.p, &C.p2, &C.q, &C.dinv, &C.diag, &C.rs})
       rc |= c->alloc(p, n1);
   }
   if (rc) return rc;
@@ -254,6 +259,21 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
   if (rc) return rc;
   CK(cudaMallocHost(&c->h_sc, sizeof(PcgScal)));
   CK(cudaMallocHost(&c->h_hist, sizeof(double) * 2 * cap));
+  // FP32 copy of the system for the inner solves of iterative refinement (shares the node lists,
+  // neighbour indices and reduction buffers with the FP64 system)
+  PcgDevF& F = c->pcgf;
+  for (int which = 0; which < 2 && !rc; ++which) {
+    PcgColorT<float>& G = which ? F.B : F.R;
+    const PcgColor& C = which ? P.B : P.R;
+    G.n = C.n; G.l = C.l; G.nbr = C.nbr;
+    G.rhs = G.diag = G.rs = nullptr;
+    for (float** q : {&G.sx, &G.sy, &G.u, &G.r, &G.z, &G.p, &G.p2, &G.q, &G.dinv}) rc |= c->alloc(q, (size_t)C.n + 1);
+  }
+  rc |= c->alloc(&F.sc, 1);
+  if (rc) return rc;
+  F.part0 = P.part0; F.part1 = P.part1; F.part2 = P.part2; F.part3 = P.part3;
+  F.hist_alpha = P.hist_alpha; F.hist_beta = P.hist_beta;
+  CK(cudaMallocHost(&c->h_scf, sizeof(PcgScal)));
   return 0;
 }
 
@@ -348,6 +368,74 @@ void eigen_estimates(const double* al, const double* be, int n, double zeta, int
   }
 }
 
+// Runs CG iterations in batches until the device-side `done` flag is set.  Every kernel of an
+// iteration returns at once after convergence, so a batch may overshoot without changing the
+// result; the host reads the scalars back once per batch.
+template <class F>
+int iterate(Ctx* c, PcgScal* dsc, PcgScal* hsc, int itmax, int predicted, F&& launch_one) {
+  int batch = std::max(1, std::min(predicted - 1, 256));
+  int launched = 0;
+  for (;;) {
+    for (int i = 0; i < batch; ++i) launch_one((launched + i) & 1);
+    launched += batch;
+    c->launches += 3LL * batch;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(hsc, dsc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (hsc->done) return 0;
+    if (launched > itmax + 8) return SI3D_ETIMEOUT;  // cannot happen: itcg stops at itmax
+    batch = 4;
+  }
+}
+
+// Mixed precision: FP32 MIC-PCG corrections inside an FP64 iterative-refinement loop.  The
+// residual r = b - A u, its norm, the stopping test (test 5 at the caller's tolerance) and the
+// update u += e are FP64; each inner solve runs the red-black MIC-PCG on FP32 copies of the
+// coefficients, pivots and residual (dot products still accumulate in FP64) until its own
+// residual has dropped by max(1e-5, what the outer test still needs).
+int refine(Ctx* c, int* total_inner) {
+  const si3d_params& p = c->prm;
+  const double zeta = std::max(p.pcg_tol, 500.0 * p.srelpr);
+  PcgScal& H = *c->h_sc;
+  int outer = 0, inner_total = 0;
+  const int max_outer = 40;
+  for (;;) {
+    ir_residual(c->pcg, c->st);
+    c->launches += 3;
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const double rn = std::sqrt(H.stptst), bn = H.bnorm;
+    H.stptst = rn / bn;
+    if (rn < bn * zeta) break;
+    if (outer >= max_outer) { H.ier = 1; break; }
+    ir_inner_setup(c->pcg, c->pcgf, c->st);
+    c->launches += 2;
+    PcgScal fi{};
+    fi.zeta = std::max(1e-5, 0.5 * zeta * bn / rn);
+    fi.srelpr = 2.220446049250313e-16;
+    fi.itmax = p.pcg_itmax;
+    fi.ntest = 5;
+    fi.bnorm = rn;
+    fi.emax = 2.0; fi.emin = 1.0; fi.udnm = 1.0;
+    fi.hist_cap = 0;
+    *c->h_scf = fi;
+    CK(cudaMemcpyAsync(c->pcgf.sc, c->h_scf, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
+    int rci = iterate(c, c->pcgf.sc, c->h_scf, p.pcg_itmax, c->last_inner,
+                      [&](int par) { pcg_iteration_f(c->pcgf, par, c->st); });
+    if (rci) return rci;
+    const int its = c->h_scf->in;
+    inner_total += its;
+    c->last_inner = std::max(its, 1);
+    ir_correct(c->pcg, c->pcgf, c->st);
+    c->launches += 2;
+    ++outer;
+  }
+  c->ir_outer += outer;
+  *total_inner = inner_total;
+  return 0;
+}
+
 // One zeta solve on the device (SolverSparse's call of nspcg, si3d_procedures.f90:1986-2003).
 int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   const si3d_params& p = c->prm;
@@ -366,19 +454,17 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   int rc0 = stage(c, ST_PCG_SETUP, 7, [&] { pcg_setup(c->d, c->pcg, x0, c->dz, &c->pcg.sc->negpiv, c->st); });
   if (rc0) return rc0;
   if (c->prof) CK(cudaEventRecord(c->pe0, c->st));
-  // run iterations in batches; every kernel returns at once after convergence
-  int batch = std::max(1, std::min(c->last_iters - 1, 256));
-  int launched = 0;
-  for (;;) {
-    for (int i = 0; i < batch; ++i) pcg_iteration(c->pcg, c->st);
-    launched += batch;
-    c->launches += 4LL * batch;
-    CK(cudaGetLastError());
-    CK(cudaMemcpyAsync(c->h_sc, c->pcg.sc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
-    CK(cudaStreamSynchronize(c->st));
-    if (c->h_sc->done) break;
-    if (launched > p.pcg_itmax + 8) return SI3D_ETIMEOUT;  // cannot happen: itcg stops at itmax
-    batch = 4;
+  int total_iters = 0;
+  if (p.precision == SI3D_MIXED_IR) {
+    int rcir = refine(c, &total_iters);
+    if (rcir) return rcir;
+  } else {
+    // run iterations in batches; every kernel returns at once after convergence
+    int rci = iterate(c, c->pcg.sc, c->h_sc, p.pcg_itmax, c->last_iters,
+                      [&](int par) { pcg_iteration(c->pcg, par, c->st); });
+    if (rci) return rci;
+    total_iters = c->h_sc->in;
+    c->last_iters = std::max(total_iters, 1);
   }
   if (c->prof) {
     CK(cudaEventRecord(c->pe1, c->st));
@@ -386,7 +472,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
     float ms = 0;
     cudaEventElapsedTime(&ms, c->pe0, c->pe1);
     c->prof_ms[ST_PCG_ITER] += ms;
-    c->prof_n[ST_PCG_ITER] += c->h_sc->in;
+    c->prof_n[ST_PCG_ITER] += total_iters;
   }
   rc0 = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, c->st); });
   if (rc0) return rc0;
@@ -394,10 +480,9 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   if (S.negpiv & 2) ier = -12;
   else if (S.ier != 0) ier = S.ier;
   else if ((S.negpiv & 1) && ier == 0) ier = 5;
-  *iters = S.in;
+  *iters = total_iters;
   *relres = S.stptst;
   *ier_out = ier;
-  c->last_iters = std::max(S.in, 1);
   return 0;
 }
 
@@ -483,6 +568,7 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
   for (cudaEvent_t* e : {&c->ev0, &c->ev1, &c->evp0, &c->evp1, &c->pe0, &c->pe1}) cudaEventCreate(e);
   const int lm = g->lm, lm1 = lm + 1, km1 = g->km1;
   const int P = (lm1 + 31) / 32 * 32;
+  if ((long long)km1 * P >= (1LL << 31)) { delete c; return SI3D_EDIMS; }   // 32-bit device indexing
   c->lm = lm; c->lm1 = lm1; c->km1 = km1; c->P = P;
   Dev& d = c->d;
   d.g.lm = lm; d.g.lm1 = lm1; d.g.km1 = km1; d.g.km = km1 - 1; d.g.k1 = g->k1; d.g.P = P;
@@ -823,7 +909,7 @@ int si3d_gpu_solve_zeta(int lm, const double* coef, const int* jcoef, const doub
                         double* emin, double* emax) {
   if (lm < 1 || !coef || !jcoef || !rhs || !zeta || pcg_itmax < 1 || (pcg_test != 5 && pcg_test != 2))
     return SI3D_EDIMS;
-  if (precision != SI3D_FP64) return SI3D_EDIMS;
+  if (precision != SI3D_FP64 && precision != SI3D_MIXED_IR) return SI3D_EDIMS;
   // Recover the grid graph and sx/sy from the SolverSparse structure:
   // coef = [rr, -sx(lW), -sy(lS), -sy(l), -sx(l)], jcoef = [l, lWC, lSC, lNC, lEC] (0 = dry).
   const int lm1 = lm + 1;

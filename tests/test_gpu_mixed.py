@@ -1,0 +1,47 @@
+"""Mixed-precision form: FP32 MIC-PCG inner solves inside FP64 iterative refinement, through the
+C ABI, against the FP64 oracle.  The stopping test stays test 5 at 1e-12 on the FP64 residual."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name,steps", [("t1", 30), ("c0", 30)])
+def test_mixed_ir_matches_fp64_oracle(run_dirs, oracle_lib, native_libs, name, steps):
+    from si3d_b200 import native
+    from si3d_b200.model import GpuRun
+    o = oracle_lib.OracleRun(run_dirs[name], ordering=1, pcg_itmax=2000)
+    g = GpuRun(run_dirs[name], pcg_itmax=2000, precision=native.SI3D_MIXED_IR)
+    o.run(steps)
+    st = g.run(steps)
+    relres = [s.relres[i] for s in st for i in range(s.nsolves)]
+    assert max(relres) < 1e-12, max(relres)
+    assert all(s.ier[i] == 0 for s in st for i in range(s.nsolves))
+    ds = np.abs(o.get("s") - g.get("s")).max()
+    assert ds <= 1e-9, f"max |dzeta| {ds:.3e} m"
+    for f, tol in (("uh", 1e-8), ("vh", 1e-8), ("sal", 1e-10)):
+        a, b = o.get(f), g.get(f)
+        err = np.abs(a - b).max() / max(np.abs(a).max(), 1e-300)
+        assert err <= tol, f"{name}:{f} rel err {err:.3e}"
+
+
+def test_mixed_standalone_solve(run_dirs, oracle_lib, native_libs):
+    from si3d_b200 import native
+    from si3d_b200.model import solve_zeta
+    o = oracle_lib.OracleRun(run_dirs["t1"], ordering=1)
+    o.run(2)
+    o.stage("momentum", 1)
+    o.stage("matcon", 1)
+    lm, lm1 = o.lm, o.lm1
+    lEC, lWC, lNC, lSC = (o.geti(n) for n in ("lEC", "lWC", "lNC", "lSC"))
+    sx, sy, rr, qq, sp = (o.get(n) for n in ("sx", "sy", "rr", "qq", "sp"))
+    m = np.arange(lm)
+    coef = np.stack([rr[m], -sx[lWC[m] - 1], -sy[lSC[m] - 1], -sy[m], -sx[m]], axis=1)
+    jco = np.zeros((lm, 5), dtype=np.int32)
+    jco[:, 0] = m + 1
+    for c, nb in ((1, lWC), (2, lSC), (3, lNC), (4, lEC)):
+        jco[:, c] = np.where(nb[m] == lm1, 0, nb[m])
+    x_o, r_o = oracle_lib.pcg(coef, jco, qq[:lm], sp[:lm], ordering=0, itmax=2000)
+    x_g, r_g = solve_zeta(coef, jco, qq[:lm], sp[:lm], itmax=2000, precision=native.SI3D_MIXED_IR)
+    assert r_g["stptst"] < 1e-12
+    assert np.abs(x_g - x_o).max() <= 1e-10 * max(np.abs(x_o).max(), 1e-3)
