@@ -221,12 +221,10 @@ def main() -> int:
     peak, peak_kind = measured_peaks()
     g = native.gpu()
 
+    from si3d_b200 import replicas
+
     def reduce_max(x):
-        if pg is None:
-            return x
-        t = torch.tensor([x], device=f"cuda:{device}", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(x, pg, device=f"cuda:{device}")
 
     def measure(form: str, precision: int, headline: bool) -> dict:
         run = GpuRun(run_dir, device=device, pcg_itmax=args.itmax, precision=precision)

@@ -56,6 +56,7 @@ class Basin:
     Ay0: float = 1.0
     f: float = 1e-4
     niter: int = 2
+    ibc: int = 1                 # baroclinic pressure term on/off
     seeds: dict = dataclasses.field(default_factory=dict)
 
     @property
@@ -156,7 +157,7 @@ def write_inp(b: Basin, path: str) -> None:
     L += [sep, "Parameters controlling solution algorithm", sep]
     for lab, val in [("itrap", 1), ("niter", b.niter), ("smooth", 0), ("beta", 0.05), ("iturb", 0),
                      ("az0", b.Av0), ("dz0", b.Dv0), ("iadv", 1), ("itrmom", 1), ("ihd", 1), ("ax0", b.Ax0),
-                     ("ay0", b.Ay0), ("f", b.f), ("theta", 1.0), ("ibc", 1), ("isal", 1), ("itrsch", 4),
+                     ("ay0", b.Ay0), ("f", b.f), ("theta", 1.0), ("ibc", b.ibc), ("isal", 1), ("itrsch", 4),
                      ("cd", b.cd), ("ifsbc", 0), ("dtsbc", 3600.0), ("icw", 0), ("cw", b.cw), ("ws", b.wa),
                      ("phi", b.phi), ("idbg", 0), ("nth", 1)]:
         L.append(_rec(lab, val))

@@ -1,0 +1,64 @@
+"""Regenerates the committed fixtures in this folder from the CPU oracle.
+
+The reference ships no golden data for its semi-implicit core, so these fixtures are the oracle's
+own outputs on small seeded inputs: they pin the oracle against accidental change (CPU tests) and
+let the GPU tests check the CUDA path against stored numbers without running the oracle.
+
+  python tests/golden/make_golden.py
+"""
+import dataclasses
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import pyoracle  # noqa: E402
+from si3d_b200 import synth  # noqa: E402
+
+STEPS = 10
+FIELDS_2D = ("s",)
+FIELDS_3D = ("uh", "vh", "sal", "wp")
+
+
+def run_fixture(name: str, steps: int = STEPS, fields_3d=FIELDS_3D):
+    """Oracle state of workload `name` after `steps` steps (plain FP64, red-black MIC-PCG at
+    test 5, 1e-12) plus the per-solve iteration log."""
+    d = os.path.join(tempfile.mkdtemp(), name)
+    synth.make(name, d)
+    o = pyoracle.OracleRun(d, ordering=1, pcg_itmax=2000)
+    o.run(steps)
+    out = {f: o.get(f)[:o.lm].copy() for f in FIELDS_2D}
+    for f in fields_3d:
+        out[f] = o.get(f)[:, :o.lm].copy()
+    sv = o.solves()
+    out["iters"] = np.array([s["iters"] for s in sv], dtype=np.int32)
+    out["stptst"] = np.array([s["stptst"] for s in sv])
+    out["steps"] = np.int32(steps)
+    return out
+
+
+def pcg_fixture():
+    """A seeded SPD 5-point system (SolverSparse's Purdue form) and its oracle solution."""
+    sys.path.insert(0, os.path.dirname(HERE))
+    from test_oracle_kat import _five_point_system
+    coef, jcoef, A = _five_point_system(48, 32, seed=2024)
+    b = A @ np.random.default_rng(2025).standard_normal(A.shape[0])
+    x0 = np.zeros_like(b)
+    x, info = pyoracle.pcg(coef, jcoef, b, x0, pcg_test=5, tol=1e-12, itmax=500, ordering=1)
+    return dict(coef=coef, jcoef=jcoef, rhs=b, x=x, iters=np.int32(info["iters"]), stptst=info["stptst"])
+
+
+def main():
+    pyoracle.build()
+    np.savez_compressed(os.path.join(HERE, f"t0_oracle_{STEPS}steps.npz"), **run_fixture("t0"))
+    np.savez_compressed(os.path.join(HERE, f"t1_oracle_{STEPS}steps.npz"), **run_fixture("t1", fields_3d=()))
+    np.savez_compressed(os.path.join(HERE, "pcg_48x32.npz"), **pcg_fixture())
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,95 @@
+"""The native host set-up (reading the reference's input files and building the grid maps) against
+the oracle's restatement of input/ZGridDimensions/bathy (si3d_utils.f90:21-382, 595-892), and its
+error paths.  CPU only."""
+import ctypes as C
+import os
+import shutil
+
+import numpy as np
+import pytest
+
+from si3d_b200 import synth
+
+MAPS = ("l2i", "l2j", "lEC", "lWC", "lNC", "lSC", "kmz")
+
+
+def _open(native, run_dir):
+    h = native.host()
+    hm = C.c_int(-1)
+    err = C.create_string_buffer(512)
+    rc = h.si3d_host_open(run_dir.encode(), None, C.byref(hm), err, 512)
+    return rc, hm.value, err.value.decode()
+
+
+@pytest.mark.parametrize("name", ["t0", "t1", "c0"])
+def test_maps_match_oracle(native_libs, oracle_lib, run_dirs, name):
+    rc, hm, err = _open(native_libs, run_dirs[name])
+    assert rc == 0, err
+    h = native_libs.host()
+    try:
+        dims = (C.c_int * 6)()
+        h.si3d_host_dims(hm, dims)
+        o = oracle_lib.OracleRun(run_dirs[name])
+        assert (dims[0], dims[1], dims[2], dims[3]) == (o.im1, o.jm1, o.km1, o.lm)
+        for m in MAPS:
+            a = np.empty(o.lm1, dtype=np.int32)
+            assert h.si3d_host_get_map(hm, m.encode(), native_libs.ptr(a)) == 0
+            np.testing.assert_array_equal(a, o.geti(m), err_msg=m)
+        z = np.empty(o.km1)
+        h.si3d_host_get_zlevel(hm, native_libs.ptr(z))
+        np.testing.assert_array_equal(z, o.zlevel())
+        assert h.si3d_host_get_map(hm, b"nope", native_libs.ptr(np.empty(o.lm1, dtype=np.int32))) == -103
+    finally:
+        h.si3d_host_close(hm)
+
+
+def _copy(src, dst):
+    shutil.copytree(src, dst)
+    return dst
+
+
+def test_missing_file(native_libs, tmp_path):
+    rc, _, err = _open(native_libs, str(tmp_path))
+    assert rc == -101 and "si3d_inp.txt" in err
+
+
+def test_truncated_bathymetry(native_libs, run_dirs, tmp_path):
+    d = _copy(run_dirs["t0"], str(tmp_path / "trunc"))
+    p = os.path.join(d, "si3d_bathy")
+    lines = open(p).read().splitlines()
+    open(p, "w").write("\n".join(lines[: len(lines) // 2]) + "\n")
+    rc, _, err = _open(native_libs, d)
+    assert rc == -101 and "truncated" in err
+
+
+def test_truncated_profile(native_libs, run_dirs, tmp_path):
+    d = _copy(run_dirs["t0"], str(tmp_path / "prof"))
+    p = os.path.join(d, "si3d_init.txt")
+    lines = open(p).read().splitlines()
+    open(p, "w").write("\n".join(lines[:-2]) + "\n")
+    rc, _, err = _open(native_libs, d)
+    assert rc == -101 and "si3d_init.txt" in err
+
+
+@pytest.mark.parametrize("label,value", [("nopen", 1), ("ntr", 2), ("iturb", 1)])
+def test_options_outside_the_core_are_refused(native_libs, run_dirs, tmp_path, label, value):
+    """Open boundaries, tracers and turbulence closures are not part of the semi-implicit core;
+    a run that selects them is refused rather than silently run without them."""
+    d = _copy(run_dirs["t0"], str(tmp_path / f"opt_{label}"))
+    p = os.path.join(d, "si3d_inp.txt")
+    lines = open(p).read().splitlines()
+    rec = synth._rec(label, 0)
+    i = lines.index(rec)
+    lines[i] = synth._rec(label, value)
+    open(p, "w").write("\n".join(lines) + "\n")
+    rc, _, err = _open(native_libs, d)
+    assert rc == -101 and "outside the semi-implicit core" in err
+
+
+def test_wind_override_size_mismatch(native_libs, run_dirs, tmp_path):
+    d = _copy(run_dirs["t1"], str(tmp_path / "wind"))
+    p = os.path.join(d, "si3d_wind_override.bin")
+    data = open(p, "rb").read()
+    open(p, "wb").write(data[:-8])
+    rc, _, err = _open(native_libs, d)
+    assert rc == -101 and "size mismatch" in err
