@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "_lib")
 
-CUDA_SOURCES = ["si3d_gpu.cu", "k_momentum.cu", "k_zeta.cu", "k_transport.cu", "noalloc.cu"]
+CUDA_SOURCES = ["si3d_gpu.cu", "k_momentum.cu", "k_zeta.cu", "k_pcg_persistent.cu", "k_transport.cu", "noalloc.cu"]
 CUDA_DEPS = CUDA_SOURCES + ["common.cuh", "kernels.h"]
 HOST_SOURCES = [os.path.join("host", "si3d_host.cpp")]
 

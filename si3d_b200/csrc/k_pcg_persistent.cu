@@ -1,0 +1,315 @@
+// Whole CG solve in one cooperative launch.
+//
+// The arithmetic of an iteration is that of the three-kernel form in k_zeta.cu (black half of
+// M^-1 fused with u += alpha p and r -= alpha q; red half; p = z + beta p and q = A p on both
+// colours), node for node, but all iterations run inside one kernel whose blocks are co-resident
+// (cudaLaunchCooperativeKernel guarantees it), separated by grid barriers.  That removes the
+// launch gaps, the host round trips that poll for convergence and the single-block reduction
+// tails.  After a barrier every block sums the block partials itself, in the same fixed order,
+// so every block computes the same alpha, beta and stopping decision without another
+// synchronisation; block 0 publishes the final scalars.
+//
+// Every barrier wait is bounded: after kSpinLimit polls a block records SI3D_ETIMEOUT as the
+// solve's ier, raises the barrier's abort flag and returns; the other blocks see the flag at
+// their next wait and return too, so the kernel always ends.
+#include <algorithm>
+
+#include "../../include/si3d_gpu.h"
+#include "common.cuh"
+#include "kernels.h"
+
+namespace si3d {
+
+namespace {
+
+constexpr int QB = 256;                       // threads per block
+constexpr long long kSpinLimit = 1LL << 26;   // polls (>= 32 ns each) before a wait gives up: > 2 s
+
+__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
+  unsigned int v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Block-wide sums of NV values at once (fixed order); the totals are returned in v[] in every
+// thread.  sh holds 8 * NV + NV doubles.
+template <int NV>
+__device__ __forceinline__ void bsum(double (&v)[NV], double* sh) {
+#pragma unroll
+  for (int i = 0; i < NV; ++i)
+    for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
+  if (ln == 0) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) sh[i * 8 + w] = v[i];
+  }
+  __syncthreads();
+  if (threadIdx.x < NV) {
+    double t = 0;
+#pragma unroll
+    for (int q = 0; q < QB / 32; ++q) t += sh[threadIdx.x * 8 + q];
+    sh[8 * NV + threadIdx.x] = t;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < NV; ++i) v[i] = sh[8 * NV + i];
+  __syncthreads();
+}
+
+// Totals of NV partial arrays (n entries each, arrays `stride` apart), in every thread.
+template <int NV>
+__device__ __forceinline__ void all_partials(const double* part, int n, int stride, double (&v)[NV], double* sh) {
+#pragma unroll
+  for (int i = 0; i < NV; ++i) v[i] = 0;
+  for (int j = threadIdx.x; j < n; j += QB) {
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] += __ldcg(part + i * stride + j);
+  }
+  bsum<NV>(v, sh);
+}
+
+// Counting grid barrier with a bounded wait.  Returns false (in every thread of the block) once
+// any block has given up.
+__device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, int* s_flag) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int ok = 1;
+    const unsigned int gen = ld_acquire(&bar->gen);
+    __threadfence();
+    const unsigned int arrived = atomicAdd(&bar->count, 1u);
+    if (arrived == gridDim.x - 1) {
+      atomicExch(&bar->count, 0u);
+      __threadfence();
+      atomicAdd(&bar->gen, 1u);
+    } else {
+      long long spins = 0;
+      while (ld_acquire(&bar->gen) == gen) {
+        if (++spins > kSpinLimit || ld_acquire(&bar->abort) != 0u) { ok = 0; break; }
+        __nanosleep(32);
+      }
+    }
+    if (!ok && atomicExch(&bar->abort, 1u) == 0u) {
+      sc->ier = SI3D_ETIMEOUT;
+      sc->done = 1;
+    }
+    __threadfence();
+    *s_flag = ok;
+  }
+  __syncthreads();
+  return *s_flag != 0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(QB) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
+  __shared__ double sh[8 * 4 + 4];
+  __shared__ int s_flag;
+  const PcgColorT<T> &R = P.R, &B = P.B;
+  PcgScal* SC = P.sc;
+  const int nb = gridDim.x;
+  const int stride = nb * QB;
+  const int g0 = blockIdx.x * QB + threadIdx.x;
+  // partial sums: (r,r) in part0, (r,z) in part1, (u,u) in part2, (z,z) in part3, black blocks at
+  // [0, nb) and red blocks at [nb, 2 nb); (p,q) at part0 + 2 nb.  The four arrays are equally
+  // spaced (part_n apart in one allocation).
+  double* const pq_part = P.part0 + 2 * nb;
+  const int pstride = P.part_n;
+  // private copies of the CG scalars, identical in every block
+  double alpha = SC->alpha, beta = SC->beta, rzdot = SC->rzdot, dkm1 = SC->dkm1, udnm = SC->udnm;
+  const double zeta = SC->zeta, srelpr = SC->srelpr, bnorm = SC->bnorm, emin = SC->emin;
+  int in = SC->in, q1 = SC->q1, ier = 0, par = 0;
+  const int itmax = SC->itmax, ntest = SC->ntest, hist_cap = SC->hist_cap;
+  double stptst = SC->stptst;
+  const bool t2 = (ntest == 2);
+  bool run = SC->done == 0;
+  while (run) {
+    const T* __restrict__ Bp = par ? B.p2 : B.p;
+    const T* __restrict__ Rp = par ? R.p2 : R.p;
+    const T a = (T)alpha;
+    // ---- black nodes: u += alpha p, r -= alpha q, black half of M^-1 (icfstp/icsp/icbsp)
+    double v[4] = {0, 0, 0, 0};
+    for (int j = g0; j < B.n; j += stride) {
+      const int4 q4 = B.nbr[j];
+      const T uj = B.u[j] + a * Bp[j];
+      const T rj = B.r[j] - a * B.q[j];
+      B.u[j] = uj;
+      B.r[j] = rj;
+      const int ks[4] = {q4.x, q4.y, q4.z, q4.w};
+      const T t[4] = {-R.sx[q4.x], -R.sy[q4.y], -B.sy[j], -B.sx[j]};
+      T x = rj;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int k = ks[c];
+        const T rk = R.r[k] - a * R.q[k];
+        const T xfk = rk * R.dinv[k];
+        x = x - t[c] * xfk;
+      }
+      const T dj = B.dinv[j];
+      x = x * dj;
+      x = x / dj;
+      const T zj = x * dj;
+      B.z[j] = zj;
+      v[0] += (double)rj * (double)rj; v[1] += (double)rj * (double)zj;
+      v[2] += (double)uj * (double)uj; v[3] += (double)zj * (double)zj;
+    }
+    if (t2) {
+      bsum<4>(v, sh);
+      if (threadIdx.x == 0)
+        for (int i = 0; i < 4; ++i) P.part0[i * pstride + blockIdx.x] = v[i];
+    } else {
+      double w2[2] = {v[0], v[1]};
+      bsum<2>(w2, sh);
+      if (threadIdx.x == 0) { P.part0[blockIdx.x] = w2[0]; P.part0[pstride + blockIdx.x] = w2[1]; }
+    }
+    if (!grid_barrier(bar, SC, &s_flag)) return;
+    // ---- red nodes: u/r updates, red half of M^-1
+    v[0] = v[1] = v[2] = v[3] = 0;
+    for (int k = g0; k < R.n; k += stride) {
+      const int4 q4 = R.nbr[k];
+      const T uk = R.u[k] + a * Rp[k];
+      const T rk = R.r[k] - a * R.q[k];
+      R.u[k] = uk;
+      R.r[k] = rk;
+      const T dk = R.dinv[k];
+      T x = rk * dk;
+      x = x / dk;
+      x = x - (-B.sx[q4.x]) * B.z[q4.x];
+      x = x - (-B.sy[q4.y]) * B.z[q4.y];
+      x = x - (-R.sy[k]) * B.z[q4.z];
+      x = x - (-R.sx[k]) * B.z[q4.w];
+      const T zk = x * dk;
+      R.z[k] = zk;
+      v[0] += (double)rk * (double)rk; v[1] += (double)rk * (double)zk;
+      v[2] += (double)uk * (double)uk; v[3] += (double)zk * (double)zk;
+    }
+    if (t2) {
+      bsum<4>(v, sh);
+      if (threadIdx.x == 0)
+        for (int i = 0; i < 4; ++i) P.part0[i * pstride + nb + blockIdx.x] = v[i];
+    } else {
+      double w2[2] = {v[0], v[1]};
+      bsum<2>(w2, sh);
+      if (threadIdx.x == 0) { P.part0[nb + blockIdx.x] = w2[0]; P.part0[pstride + nb + blockIdx.x] = w2[1]; }
+    }
+    if (!grid_barrier(bar, SC, &s_flag)) return;
+    // ---- every block: (r,r), (r,z) [, (u,u), (z,z)], the stopping test (pstops) and beta
+    double rrt, rzt, uut = 0, zzt = 0;
+    if (t2) {
+      double w4[4];
+      all_partials<4>(P.part0, 2 * nb, pstride, w4, sh);
+      rrt = w4[0]; rzt = w4[1]; uut = w4[2]; zzt = w4[3];
+    } else {
+      double w2[2];
+      all_partials<2>(P.part0, 2 * nb, pstride, w2, sh);
+      rrt = w2[0]; rzt = w2[1];
+    }
+    dkm1 = rzdot;
+    rzdot = rzt;
+    if (!(rzt > 0.0)) { ier = -7; break; }
+    const double tiny = 500.0 * srelpr;
+    bool halt;
+    if (ntest == 5) {
+      const double tl = sqrt(rrt);
+      stptst = tl / bnorm;
+      halt = tl < bnorm * zeta;
+    } else {
+      if (in < 1) {
+        q1 = 0;
+        udnm = 1.0;
+        stptst = sqrt(rzt);
+        halt = stptst < tiny;
+      } else {
+        if (!q1 && !((in > 5) && (in % 5 != 0))) {
+          const double uold = udnm;
+          udnm = sqrt(uut);
+          if (udnm < tiny) udnm = 1.0;
+          if ((in > 5) && (fabs(udnm - uold) < udnm * zeta)) q1 = 1;
+        }
+        const double eminl = emin < tiny ? tiny : emin;
+        const double tl = sqrt(zzt), tr = udnm * eminl;
+        stptst = tl / tr;
+        halt = tl < tr * zeta;
+      }
+    }
+    if (halt) break;
+    if (!(in < itmax)) { ier = 1; break; }
+    if (in != 0) beta = rzdot / dkm1;
+    // ---- p = z + beta p and q = A p on both colours (the new p goes to the other buffer)
+    const T bt = (T)beta;
+    double pq[1] = {0};
+#pragma unroll
+    for (int side = 0; side < 2; ++side) {
+      const PcgColorT<T>& C = side ? B : R;
+      const PcgColorT<T>& O = side ? R : B;
+      const T* __restrict__ Cp = par ? C.p2 : C.p;
+      const T* __restrict__ Op = par ? O.p2 : O.p;
+      T* __restrict__ Cn = par ? C.p : C.p2;
+      for (int i = g0; i < C.n; i += stride) {
+        const int4 q4 = C.nbr[i];
+        const T pi = C.z[i] + bt * Cp[i];
+        const T pW = O.z[q4.x] + bt * Op[q4.x];
+        const T pS = O.z[q4.y] + bt * Op[q4.y];
+        const T pN = O.z[q4.z] + bt * Op[q4.z];
+        const T pE = O.z[q4.w] + bt * Op[q4.w];
+        const T sxW = O.sx[q4.x], syS = O.sy[q4.y];
+        const T diag = (T)1 + C.sx[i] + sxW + C.sy[i] + syS;
+        T y = diag * pi;
+        y = y + (-sxW) * pW;
+        y = y + (-syS) * pS;
+        y = y + (-C.sy[i]) * pN;
+        y = y + (-C.sx[i]) * pE;
+        Cn[i] = pi;
+        C.q[i] = y;
+        pq[0] += (double)pi * (double)y;
+      }
+    }
+    bsum<1>(pq, sh);
+    if (threadIdx.x == 0) pq_part[blockIdx.x] = pq[0];
+    if (!grid_barrier(bar, SC, &s_flag)) return;
+    double pap[1];
+    all_partials<1>(pq_part, nb, 0, pap, sh);
+    alpha = rzdot / pap[0];
+    if (!(pap[0] > 0.0)) { ier = -6; break; }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && in < hist_cap) { P.hist_alpha[in] = alpha; P.hist_beta[in] = beta; }
+    in += 1;
+    par ^= 1;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    SC->alpha = alpha; SC->beta = beta; SC->rzdot = rzdot; SC->dkm1 = dkm1; SC->udnm = udnm; SC->q1 = q1;
+    SC->in = in; SC->stptst = stptst;
+    if (ier) SC->ier = ier;
+    SC->done = 1;
+  }
+}
+
+template <typename T>
+int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, cudaStream_t st) {
+  if (cudaMemsetAsync(bar, 0, sizeof(GridBar), st) != cudaSuccess) return -1;
+  PcgDevT<T> Pc = P;
+  void* args[] = {(void*)&Pc, (void*)&bar};
+  return cudaLaunchCooperativeKernel((const void*)k_pcg_loop<T>, dim3(nblocks), dim3(QB), args, 0, st) == cudaSuccess
+             ? 0
+             : -1;
+}
+
+}  // namespace
+
+int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm) {
+  int sms = 0, occ_d = 0, occ_f = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_pcg_loop<double>, QB, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_pcg_loop<float>, QB, 0);
+  int per_sm = std::min(occ_d, occ_f);
+  if (max_per_sm > 0) per_sm = std::min(per_sm, max_per_sm);
+  const int need = (std::max(nR, nB) + QB - 1) / QB;
+  return std::max(1, std::min(sms * std::max(per_sm, 1), need));
+}
+
+int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, cudaStream_t st) {
+  return launch_loop<double>(P, bar, nblocks, st);
+}
+
+int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st) {
+  return launch_loop<float>(F, bar, nblocks, st);
+}
+
+}  // namespace si3d

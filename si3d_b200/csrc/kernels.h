@@ -26,7 +26,8 @@ template <typename T>
 struct PcgDevT {
   PcgColorT<T> R, B;
   PcgScal* sc;
-  double *part0, *part1, *part2, *part3;
+  double *part0, *part1, *part2, *part3;   // block partials, part_n entries each, contiguous
+  int part_n;
   double *hist_alpha, *hist_beta;
 };
 using PcgDev = PcgDevT<double>;
@@ -46,6 +47,15 @@ void ir_residual(const PcgDev& P, cudaStream_t st);
 void ir_inner_setup(const PcgDev& P, const PcgDevF& F, cudaStream_t st);
 void pcg_iteration_f(const PcgDevF& F, int par, cudaStream_t st);
 void ir_correct(const PcgDev& P, const PcgDevF& F, cudaStream_t st);
+
+// Whole solve in one cooperative launch (k_pcg_persistent.cu).  The barrier state is reset by
+// every launch.
+struct GridBar {
+  unsigned int count, gen, abort, pad;
+};
+int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm);
+int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, cudaStream_t st);
+int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st);
 
 void launch_slayer_h(const Dev& d, cudaStream_t st);
 void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cudaStream_t st);

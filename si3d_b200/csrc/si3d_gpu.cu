@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -80,6 +81,10 @@ struct Ctx {
   PcgScal* h_sc = nullptr;  // pinned
   double* h_hist = nullptr; // pinned, 2 x itmax
   int last_iters = 8;
+  // whole-solve cooperative kernel (k_pcg_persistent.cu); false -> one launch per phase
+  bool persistent = true;
+  int loop_blocks = 0;
+  GridBar* bar = nullptr;
   // instrumentation: kernel-launch count and (optionally) per-stage device time
   long long launches = 0;
   bool prof = false;
@@ -250,8 +255,18 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
       rc |= c->alloc(p, n1);
   }
   if (rc) return rc;
-  const int nblk = pcg_max_blocks(nR, nB);
-  for (double** p : {&P.part0, &P.part1, &P.part2, &P.part3}) rc |= c->alloc(p, nblk);
+  // SI3D_PCG_BLOCKS_PER_SM caps the resident blocks per SM of the cooperative solve (tuning)
+  const char* bps = std::getenv("SI3D_PCG_BLOCKS_PER_SM");
+  c->loop_blocks = pcg_loop_blocks(c->device, nR, nB, bps ? std::atoi(bps) : 0);
+  const char* pers = std::getenv("SI3D_PCG_PERSISTENT");
+  c->persistent = !(pers && pers[0] == '0');
+  const int nblk = std::max(pcg_max_blocks(nR, nB), 3 * c->loop_blocks);
+  double* parts = nullptr;
+  rc |= c->alloc(&parts, 4 * (size_t)nblk);
+  rc |= c->alloc(&c->bar, 1);
+  if (rc) return rc;
+  P.part0 = parts; P.part1 = parts + nblk; P.part2 = parts + 2 * nblk; P.part3 = parts + 3 * nblk;
+  P.part_n = nblk;
   rc |= c->alloc(&P.sc, 1);
   const int cap = std::max(c->prm.pcg_itmax, 1) + 1;
   rc |= c->alloc(&P.hist_alpha, cap);
@@ -271,7 +286,7 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
   }
   rc |= c->alloc(&F.sc, 1);
   if (rc) return rc;
-  F.part0 = P.part0; F.part1 = P.part1; F.part2 = P.part2; F.part3 = P.part3;
+  F.part0 = P.part0; F.part1 = P.part1; F.part2 = P.part2; F.part3 = P.part3; F.part_n = P.part_n;
   F.hist_alpha = P.hist_alpha; F.hist_beta = P.hist_beta;
   CK(cudaMallocHost(&c->h_scf, sizeof(PcgScal)));
   return 0;
@@ -371,8 +386,15 @@ void eigen_estimates(const double* al, const double* be, int n, double zeta, int
 // Runs CG iterations in batches until the device-side `done` flag is set.  Every kernel of an
 // iteration returns at once after convergence, so a batch may overshoot without changing the
 // result; the host reads the scalars back once per batch.
-template <class F>
-int iterate(Ctx* c, PcgScal* dsc, PcgScal* hsc, int itmax, int predicted, F&& launch_one) {
+template <class F, class G>
+int iterate(Ctx* c, PcgScal* dsc, PcgScal* hsc, int itmax, int predicted, F&& launch_one, G&& launch_loop) {
+  if (c->persistent) {
+    if (launch_loop() != 0) { g_last_cuda = cudaGetErrorString(cudaGetLastError()); return SI3D_ECUDA; }
+    c->launches += 1;
+    CK(cudaMemcpyAsync(hsc, dsc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    return hsc->done ? 0 : SI3D_ETIMEOUT;
+  }
   int batch = std::max(1, std::min(predicted - 1, 256));
   int launched = 0;
   for (;;) {
@@ -422,7 +444,8 @@ int refine(Ctx* c, int* total_inner) {
     *c->h_scf = fi;
     CK(cudaMemcpyAsync(c->pcgf.sc, c->h_scf, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
     int rci = iterate(c, c->pcgf.sc, c->h_scf, p.pcg_itmax, c->last_inner,
-                      [&](int par) { pcg_iteration_f(c->pcgf, par, c->st); });
+                      [&](int par) { pcg_iteration_f(c->pcgf, par, c->st); },
+                      [&] { return pcg_loop_f(c->pcgf, c->bar, c->loop_blocks, c->st); });
     if (rci) return rci;
     const int its = c->h_scf->in;
     inner_total += its;
@@ -461,7 +484,8 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   } else {
     // run iterations in batches; every kernel returns at once after convergence
     int rci = iterate(c, c->pcg.sc, c->h_sc, p.pcg_itmax, c->last_iters,
-                      [&](int par) { pcg_iteration(c->pcg, par, c->st); });
+                      [&](int par) { pcg_iteration(c->pcg, par, c->st); },
+                      [&] { return pcg_loop(c->pcg, c->bar, c->loop_blocks, c->st); });
     if (rci) return rci;
     total_iters = c->h_sc->in;
     c->last_iters = std::max(total_iters, 1);
