@@ -85,6 +85,7 @@ struct Ctx {
   bool persistent = true;
   int loop_blocks = 0;
   GridBar* bar = nullptr;
+  bool log_solves = false;   // SI3D_LOG_SOLVES=1: per-solve iteration counts on stderr
   // instrumentation: kernel-launch count and (optionally) per-stage device time
   long long launches = 0;
   bool prof = false;
@@ -260,6 +261,8 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
   c->loop_blocks = pcg_loop_blocks(c->device, nR, nB, bps ? std::atoi(bps) : 0);
   const char* pers = std::getenv("SI3D_PCG_PERSISTENT");
   c->persistent = !(pers && pers[0] == '0');
+  const char* lg = std::getenv("SI3D_LOG_SOLVES");
+  c->log_solves = lg && lg[0] == '1';
   const int nblk = std::max(pcg_max_blocks(nR, nB), 3 * c->loop_blocks);
   double* parts = nullptr;
   rc |= c->alloc(&parts, 4 * (size_t)nblk);
@@ -448,6 +451,7 @@ int refine(Ctx* c, int* total_inner) {
                       [&] { return pcg_loop_f(c->pcgf, c->bar, c->loop_blocks, c->st); });
     if (rci) return rci;
     const int its = c->h_scf->in;
+    if (c->log_solves) std::fprintf(stderr, "si3d: inner FP32 solve %d: %d iterations\n", outer + 1, its);
     inner_total += its;
     c->last_inner = std::max(its, 1);
     ir_correct(c->pcg, c->pcgf, c->st);
@@ -489,6 +493,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
     if (rci) return rci;
     total_iters = c->h_sc->in;
     c->last_iters = std::max(total_iters, 1);
+    if (c->log_solves) std::fprintf(stderr, "si3d: FP64 solve: %d iterations\n", total_iters);
   }
   if (c->prof) {
     CK(cudaEventRecord(c->pe1, c->st));

@@ -107,18 +107,22 @@ def bowl_bathymetry(nx, ny, dx, dy, hmax=20.0) -> np.ndarray:
 
 
 def config(name: str, nsteps: Optional[int] = None, seed_offset: int = 0) -> Basin:
-    """The benchmark/parity workloads by name: c0, c1, c2, or the small test basins t0/t1."""
+    """The benchmark/parity workloads by name: c0, c1, c2, the small test basins t0/t1, and the
+    profiler cases m1 (600 x 300 x 60 with c2's generators) and p2 (c2's 2000 x 1000 grid with 6
+    layers of 10 m: a zeta system of c2's size with a ~3 GB 3-D state)."""
     if name == "c0":
         nx, ny, dx = 100, 50, 100.0
         return Basin("c0", nx, ny, dx, dx, bowl_bathymetry(nx, ny, dx, dx), 20, 1.0, 60.0, nsteps or 1000,
                      dzmin=0.05, wa=float(wind_speed_for_stress(0.1)), phi=270.0)
-    if name in ("c1", "c2", "t1", "m1"):
+    if name in ("c1", "c2", "t1", "m1", "p2"):
         if name == "c1":
             nx, ny, dx, nl, ddz, steps, sb, sw = 1000, 500, 50.0, 40, 1.5, 1000, 1001, 1002
         elif name == "c2":
             nx, ny, dx, nl, ddz, steps, sb, sw = 2000, 1000, 50.0, 60, 1.0, 500, 2001, 2002
         elif name == "m1":  # medium basin for profiler captures (c2 generators, ~1.5 GB state)
             nx, ny, dx, nl, ddz, steps, sb, sw = 600, 300, 50.0, 60, 1.0, 50, 2001, 2002
+        elif name == "p2":  # zeta-solve captures: c2's grid, seeds and wet mask, 6 layers of 10 m
+            nx, ny, dx, nl, ddz, steps, sb, sw = 2000, 1000, 50.0, 6, 10.0, 50, 2001, 2002
         else:  # small random basin for fast parity tests
             nx, ny, dx, nl, ddz, steps, sb, sw = 96, 64, 50.0, 12, 5.0, 50, 3001, 3002
         sb += seed_offset
