@@ -175,8 +175,9 @@ def main() -> int:
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--itmax", type=int, default=2000)
-    ap.add_argument("--forms", default="plain_fp64,mixed_ir",
-                    help="comma-separated subset of plain_fp64,mixed_ir; the last one is the headline")
+    ap.add_argument("--forms", default="",
+                    help="comma-separated subset of plain_fp64,mixed_ir,learned_fp64,learned_mixed (the last one is "
+                         "the headline); default: all forms, the learned ones when trained parameters exist")
     args = ap.parse_args()
     ws, rank, local = _dist()
     if args.warmup < 3:
@@ -228,8 +229,10 @@ def main() -> int:
     def reduce_max(x):
         return replicas.max_over_ranks(x, pg, device=f"cuda:{device}")
 
-    def measure(form: str, precision: int, headline: bool) -> dict:
-        run = GpuRun(run_dir, device=device, pcg_itmax=args.itmax, precision=precision)
+    def measure(form: str, precision: int, x0_mode: int, params, headline: bool) -> dict:
+        run = GpuRun(run_dir, device=device, pcg_itmax=args.itmax, precision=precision, x0_mode=x0_mode)
+        if params is not None:
+            run.set_net(params)
         run.run(args.warmup)
 
         def barrier():
@@ -260,6 +263,7 @@ def main() -> int:
         run.profile(False)
         stage_ms = {k: v for k, v in prof.items() if v[1] > 0}
         out["stage_ms_per_step"] = {k: v[0] / 2 for k, v in stage_ms.items()}
+        out["zeta"] = run.get("s")[:run.lm].copy()   # after warmup + steps + 2 steps, the same in every form
         dominant = max(stage_ms, key=lambda k: stage_ms[k][0])
         if dominant in STAGE_STREAMS:
             streams, unit = STAGE_STREAMS[dominant]
@@ -293,13 +297,25 @@ def main() -> int:
         run.close()
         return out
 
-    known = {"plain_fp64": native.SI3D_FP64, "mixed_ir": native.SI3D_MIXED_IR}
-    forms = [(f, known[f]) for f in args.forms.split(",")]
+    from si3d_b200 import learn
+    params = learn.load_params() if os.path.exists(learn.DEFAULT_PARAMS) else None
+    known = {"plain_fp64": (native.SI3D_FP64, native.SI3D_X0_PREV, None),
+             "mixed_ir": (native.SI3D_MIXED_IR, native.SI3D_X0_PREV, None),
+             "learned_fp64": (native.SI3D_FP64, native.SI3D_X0_LEARNED, params),
+             "learned_mixed": (native.SI3D_MIXED_IR, native.SI3D_X0_LEARNED, params)}
+    names = args.forms.split(",") if args.forms else (
+        ["plain_fp64", "mixed_ir"] + (["learned_fp64", "learned_mixed"] if params is not None else []))
+    forms = [(f, *known[f]) for f in names]
+    if any(f.startswith("learned") for f in names) and params is None:
+        raise SystemExit("learned forms need " + learn.DEFAULT_PARAMS)
     res = {}
-    for i, (form, prec) in enumerate(forms):
-        res[form] = measure(form, prec, headline=(i == len(forms) - 1))
+    for i, (form, prec, x0, prm) in enumerate(forms):
+        res[form] = measure(form, prec, x0, prm, headline=(i == len(forms) - 1))
     head_form = forms[-1][0]
     head = res[head_form]
+    if "plain_fp64" in res:
+        for k, v in res.items():
+            v["max_dzeta_vs_plain_fp64_m"] = float(np.abs(v["zeta"] - res["plain_fp64"]["zeta"]).max())
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
@@ -314,8 +330,9 @@ def main() -> int:
         line = {
             "metric": METRIC, "value": head["s_per_step"], "unit": "s/timestep", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": head["s_per_step"] * 1e3, "higher_is_better": False,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (fp32 inner solves)" if head_form != "plain_fp64"
-            else "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"plain_fp64": "f64", "mixed_ir": "f64 (fp32 inner solves)", "learned_fp64": "f64 (bf16 guess net)",
+                      "learned_mixed": "f64 (fp32 inner solves, bf16 guess net)"}[head_form], "data": "synthetic",
             "config": {"workload": f"{args.workload}: 2000x1000 cells x 60 layers, seeded random bathymetry and wind "
                                    f"stress, dt 30 s, itrap=1 niter=2, zeta solve to relative residual 1e-12 (test 5)",
                        "form": head_form, "lm": lm, "n3": n3, "parallelism": f"replicas x{ws}",
@@ -323,7 +340,7 @@ def main() -> int:
             "pcg_iters_per_step": head["pcg_iters_per_step"], "pcg_s_per_step": head["pcg_s_per_step"],
             "speedup_vs_plain_fp64": plain["s_per_step"] / head["s_per_step"],
             "pcg_speedup_vs_plain_fp64": plain["pcg_s_per_step"] / head["pcg_s_per_step"],
-            "forms": {k: {kk: vv for kk, vv in v.items() if kk not in ("clocks", "e2e")} for k, v in res.items()},
+            "forms": {k: {kk: vv for kk, vv in v.items() if kk not in ("clocks", "e2e", "zeta")} for k, v in res.items()},
             "roofline": head.get("roofline"), "cpu_baseline": cpu, "e2e": head["e2e"],
             "gpu_launches": head["gpu_launches"], "clocks": head["clocks"],
         }

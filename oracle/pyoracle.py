@@ -50,6 +50,10 @@ def lib():
         L.orc_trid1.argtypes = [C.c_int] + [C.c_void_p] * 3
         L.orc_densty.restype = C.c_double
         L.orc_densty.argtypes = [C.c_double, C.c_double, C.c_double]
+        L.orc_net_nparam.restype = C.c_int
+        L.orc_net_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p]
+        L.orc_net_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                   C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -177,3 +181,33 @@ def trid1(a, b, c, d):
 
 def densty(t, s, z) -> float:
     return lib().orc_densty(t, s, z)
+
+
+# ---------------------------------------------------------------------------- learned initial guess
+def net_nparam() -> int:
+    return lib().orc_net_nparam()
+
+
+def net_forward(params, feat, *, bf16: bool = True) -> np.ndarray:
+    """Network output [B][H][W] for feat [B][H][W][4] (include/si3d_learn.h layout)."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    f = np.ascontiguousarray(feat, dtype=np.float32)
+    B, H, W, _ = f.shape
+    out = np.empty((B, H, W))
+    if lib().orc_net_forward(_p(p), _p(f), B, H, W, int(bf16), _p(out)) != 0:
+        raise ValueError("bad shape")
+    return out
+
+
+def net_grad(params, feat, target, mask, *, bf16: bool = True):
+    """(loss, d loss / d params) of the masked mean-square error."""
+    p = np.ascontiguousarray(params, dtype=np.float32)
+    f = np.ascontiguousarray(feat, dtype=np.float32)
+    t = np.ascontiguousarray(target, dtype=np.float32)
+    m = np.ascontiguousarray(mask, dtype=np.float32)
+    B, H, W, _ = f.shape
+    g = np.empty(net_nparam())
+    loss = C.c_double(0)
+    if lib().orc_net_grad(_p(p), _p(f), _p(t), _p(m), B, H, W, int(bf16), _p(g), C.byref(loss)) != 0:
+        raise ValueError("bad shape")
+    return loss.value, g

@@ -17,8 +17,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "_lib")
 
-CUDA_SOURCES = ["si3d_gpu.cu", "k_momentum.cu", "k_zeta.cu", "k_pcg_persistent.cu", "k_transport.cu", "noalloc.cu"]
-CUDA_DEPS = CUDA_SOURCES + ["common.cuh", "kernels.h"]
+CUDA_SOURCES = ["si3d_gpu.cu", "k_momentum.cu", "k_zeta.cu", "k_pcg_persistent.cu", "k_transport.cu", "k_learn.cu",
+                "noalloc.cu"]
+CUDA_DEPS = CUDA_SOURCES + ["common.cuh", "kernels.h", "learn.h"]
 HOST_SOURCES = [os.path.join("host", "si3d_host.cpp")]
 
 NVCC_FLAGS = [
@@ -55,7 +56,8 @@ def _run(cmd: list[str], cwd: str) -> None:
 def build_gpu(force: bool = False) -> str:
     os.makedirs(LIB, exist_ok=True)
     out = os.path.join(LIB, "libsi3d_gpu.so")
-    deps = [os.path.join(CSRC, f) for f in CUDA_DEPS] + [os.path.join(ROOT, "include", "si3d_gpu.h")]
+    deps = [os.path.join(CSRC, f) for f in CUDA_DEPS] + [os.path.join(ROOT, "include", h)
+                                                          for h in ("si3d_gpu.h", "si3d_learn.h")]
     if force or _stale(out, deps):
         _run([_nvcc(), *NVCC_FLAGS, "-o", out, *CUDA_SOURCES], CSRC)
     return out

@@ -1,0 +1,631 @@
+// Learned initial guess for the zeta solve: network kernels (inference and training) and the
+// solver-side feature / scatter / record kernels.  Network shape and parameter layout are fixed by
+// include/si3d_learn.h.
+//
+// Tiling: every kernel works on 8 x 16 pixel tiles of a channels-last image with a one-pixel halo
+// staged in shared memory.  The four 32 -> 32 convolutions run on the tensor cores as an implicit
+// GEMM (M = 16 pixels of a tile row, N = 8 output channels, K = 16 input channels of one tap;
+// 9 taps x 2 channel halves = 18 K-steps), BF16 operands with FP32 accumulation
+// (mma.sync m16n8k16); the same kernel with tap-flipped, channel-transposed weights gives the
+// data gradient.  The 4 -> 32 stem, the 32 -> 1 head and the weight gradients are small and run on
+// the FP32 cores, accumulating in a fixed order.
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <algorithm>
+
+#include "../../include/si3d_gpu.h"
+#include "../../include/si3d_learn.h"
+#include "common.cuh"
+#include "learn.h"
+
+namespace si3d {
+namespace learn {
+
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int C = SI3D_NET_C;
+constexpr int TH = 8, TW = 16, TP = TH * TW;   // pixel tile
+constexpr int HT = TH + 2, WT = TW + 2;        // tile with halo
+constexpr int XS = 40;                         // shared-memory pixel stride of 32-channel tiles (bf16)
+constexpr int OFF_STEM_B = 9 * 4 * C;
+constexpr int OFF_BLK = OFF_STEM_B + C;
+constexpr int BLK_SZ = 9 * C * C + C;
+constexpr int OFF_HEAD_W = OFF_BLK + SI3D_NET_BLOCKS * BLK_SZ;
+constexpr int OFF_HEAD_B = OFF_HEAD_W + 9 * C;
+static_assert(OFF_HEAD_B + 1 == SI3D_NET_NPARAM, "parameter layout");
+constexpr int WG_BLOCKS = 296;                 // weight-gradient partial sums (2 per SM)
+
+__device__ __forceinline__ float bfr(float x) { return __bfloat162float(__float2bfloat16_rn(x)); }
+
+struct TileIdx {
+  int b, i0, j0;
+};
+__device__ __forceinline__ TileIdx tile_of(int t, int H, int W) {
+  const int nj = (W + TW - 1) / TW, ni = (H + TH - 1) / TH;
+  TileIdx r;
+  r.b = t / (ni * nj);
+  const int rem = t % (ni * nj);
+  r.i0 = (rem / nj) * TH;
+  r.j0 = (rem % nj) * TW;
+  return r;
+}
+
+// ------------------------------------------------------------------ weights
+// Block weights to the tensor-core layout [tap][n][k] (bf16): forward n = cout, k = cin;
+// data gradient n = cin, k = cout with the tap mirrored.  Stem/head weights rounded to bf16 values.
+__global__ void k_prep(const float* __restrict__ prm, bf16* __restrict__ wfwd, bf16* __restrict__ wbwd,
+                       float* __restrict__ stem, float* __restrict__ head) {
+  const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+  const int nb = SI3D_NET_BLOCKS * 9 * C * C;
+  if (tid < nb) {
+    const int blk = tid / (9 * C * C), r = tid % (9 * C * C);
+    const int t = r / (C * C), n = (r / C) % C, k = r % C;
+    const float* W = prm + OFF_BLK + blk * BLK_SZ;
+    wfwd[tid] = __float2bfloat16_rn(W[(t * C + k) * C + n]);          // W[t][cin=k][cout=n]
+    wbwd[tid] = __float2bfloat16_rn(W[((8 - t) * C + n) * C + k]);    // W[8-t][cin=n][cout=k]
+  }
+  if (tid < 9 * 4 * C) stem[tid] = bfr(prm[tid]);
+  if (tid < C) stem[9 * 4 * C + tid] = prm[OFF_STEM_B + tid];
+  if (tid < 9 * C) head[tid] = bfr(prm[OFF_HEAD_W + tid]);
+  if (tid == 0) head[9 * C] = prm[OFF_HEAD_B];
+}
+
+// ------------------------------------------------------------------ stem: 4 -> 32, FP32 cores
+__global__ void __launch_bounds__(TP) k_stem(const float* __restrict__ feat, const float* __restrict__ w, int H, int W,
+                                             bf16* __restrict__ X, float* __restrict__ Y) {
+  __shared__ float sF[HT * WT * 4];
+  __shared__ float sW[9 * 4 * C + C];
+  const int b = blockIdx.z, i0 = blockIdx.y * TH, j0 = blockIdx.x * TW;
+  for (int r = threadIdx.x; r < 9 * 4 * C + C; r += TP) sW[r] = w[r];
+  for (int r = threadIdx.x; r < HT * WT; r += TP) {
+    const int gi = i0 + r / WT - 1, gj = j0 + r % WT - 1;
+    float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (gi >= 0 && gi < H && gj >= 0 && gj < W) v = *reinterpret_cast<const float4*>(feat + (((size_t)b * H + gi) * W + gj) * 4);
+    sF[r * 4 + 0] = bfr(v.x); sF[r * 4 + 1] = bfr(v.y); sF[r * 4 + 2] = bfr(v.z); sF[r * 4 + 3] = bfr(v.w);
+  }
+  __syncthreads();
+  const int ti = threadIdx.x / TW, tj = threadIdx.x % TW;
+  const int gi = i0 + ti, gj = j0 + tj;
+  if (gi >= H || gj >= W) return;
+  float acc[C];
+#pragma unroll
+  for (int co = 0; co < C; ++co) acc[co] = 0.f;
+  for (int t = 0; t < 9; ++t) {
+    const int pi = ti + 1 + t / 3 - 1, pj = tj + 1 + t % 3 - 1;
+#pragma unroll
+    for (int ci = 0; ci < 4; ++ci) {
+      const float v = sF[(pi * WT + pj) * 4 + ci];
+#pragma unroll
+      for (int co = 0; co < C; ++co) acc[co] = acc[co] + v * sW[(t * 4 + ci) * C + co];
+    }
+  }
+  const size_t p = ((size_t)b * H + gi) * W + gj;
+#pragma unroll
+  for (int co = 0; co < C; co += 2) {
+    const float y0 = acc[co] + sW[9 * 4 * C + co], y1 = acc[co + 1] + sW[9 * 4 * C + co + 1];
+    if (Y) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
+    *reinterpret_cast<__nv_bfloat162*>(X + p * C + co) = __floats2bfloat162_rn(fmaxf(y0, 0.f), fmaxf(y1, 0.f));
+  }
+}
+
+// ------------------------------------------------------------------ 32 -> 32 conv on the tensor cores
+__device__ __forceinline__ void mma_bf16(float* c, uint32_t a0, uint32_t a1, uint32_t a2, uint32_t a3, uint32_t b0,
+                                         uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a0), "r"(a1), "r"(a2), "r"(a3), "r"(b0), "r"(b1));
+}
+
+enum { CONV_FWD = 0, CONV_BWD = 1 };
+
+// out[p][n] = sum_{tap, k} in[p + off(tap)][k] * Wk[tap][n][k].
+// CONV_FWD: y = out + bias; X_out = bf16(X_in + ReLU(y)); Y (optional) = y.
+// CONV_BWD: G_out = G_in + out.
+template <int MODE>
+__global__ void __launch_bounds__(128) k_conv32(const bf16* __restrict__ Xin, const bf16* __restrict__ Wk,
+                                                const float* __restrict__ bias, int H, int W, bf16* __restrict__ Xout,
+                                                float* __restrict__ Y, const float* __restrict__ Gin,
+                                                float* __restrict__ Gout) {
+  __shared__ __align__(16) bf16 sX[HT * WT * XS];
+  __shared__ __align__(16) bf16 sW[9 * C * XS];
+  const int b = blockIdx.z, i0 = blockIdx.y * TH, j0 = blockIdx.x * TW;
+  for (int r = threadIdx.x; r < 9 * C * 4; r += 128) {
+    const int row = r >> 2, part = r & 3;
+    *reinterpret_cast<uint4*>(&sW[row * XS + part * 8]) = *reinterpret_cast<const uint4*>(&Wk[row * C + part * 8]);
+  }
+  for (int r = threadIdx.x; r < HT * WT * 4; r += 128) {
+    const int pix = r >> 2, part = r & 3;
+    const int gi = i0 + pix / WT - 1, gj = j0 + pix % WT - 1;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (gi >= 0 && gi < H && gj >= 0 && gj < W)
+      v = *reinterpret_cast<const uint4*>(&Xin[(((size_t)b * H + gi) * W + gj) * C + part * 8]);
+    *reinterpret_cast<uint4*>(&sX[pix * XS + part * 8]) = v;
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+  float acc[2][4][4];
+#pragma unroll
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int nt = 0; nt < 4; ++nt)
+#pragma unroll
+      for (int e = 0; e < 4; ++e) acc[r][nt][e] = 0.f;
+#pragma unroll 1
+  for (int t = 0; t < 9; ++t) {
+    const int di = t / 3 - 1, dj = t % 3 - 1;
+#pragma unroll
+    for (int cb = 0; cb < 2; ++cb) {
+      uint32_t bq[4][2];
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const bf16* wp = &sW[(t * C + nt * 8 + g) * XS + cb * 16 + q * 2];
+        bq[nt][0] = *reinterpret_cast<const uint32_t*>(wp);
+        bq[nt][1] = *reinterpret_cast<const uint32_t*>(wp + 8);
+      }
+#pragma unroll
+      for (int r = 0; r < 2; ++r) {
+        const int ty = warp * 2 + r;
+        const bf16* xp = &sX[((ty + 1 + di) * WT + (g + 1 + dj)) * XS + cb * 16 + q * 2];
+        const uint32_t a0 = *reinterpret_cast<const uint32_t*>(xp);
+        const uint32_t a1 = *reinterpret_cast<const uint32_t*>(xp + 8 * XS);
+        const uint32_t a2 = *reinterpret_cast<const uint32_t*>(xp + 8);
+        const uint32_t a3 = *reinterpret_cast<const uint32_t*>(xp + 8 * XS + 8);
+#pragma unroll
+        for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[r][nt], a0, a1, a2, a3, bq[nt][0], bq[nt][1]);
+      }
+    }
+  }
+#pragma unroll
+  for (int r = 0; r < 2; ++r) {
+    const int ty = warp * 2 + r, gi = i0 + ty;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+      const int tj = g + 8 * half, gj = j0 + tj;
+      if (gi >= H || gj >= W) continue;
+      const size_t p = ((size_t)b * H + gi) * W + gj;
+#pragma unroll
+      for (int nt = 0; nt < 4; ++nt) {
+        const int co = nt * 8 + 2 * q;
+        const float v0 = acc[r][nt][2 * half], v1 = acc[r][nt][2 * half + 1];
+        if (MODE == CONV_FWD) {
+          const float y0 = v0 + bias[co], y1 = v1 + bias[co + 1];
+          const bf16* xc = &sX[((ty + 1) * WT + tj + 1) * XS + co];
+          const float x0 = __bfloat162float(xc[0]), x1 = __bfloat162float(xc[1]);
+          if (Y) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
+          *reinterpret_cast<__nv_bfloat162*>(Xout + p * C + co) =
+              __floats2bfloat162_rn(x0 + fmaxf(y0, 0.f), x1 + fmaxf(y1, 0.f));
+        } else {
+          const float2 gi2 = *reinterpret_cast<const float2*>(Gin + p * C + co);
+          *reinterpret_cast<float2*>(Gout + p * C + co) = make_float2(gi2.x + v0, gi2.y + v1);
+        }
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ head: 32 -> 1, FP32 cores
+__global__ void __launch_bounds__(TP) k_head(const bf16* __restrict__ X, const float* __restrict__ w, int H, int W,
+                                             float* __restrict__ out) {
+  __shared__ __align__(16) bf16 sX[HT * WT * XS];
+  __shared__ float sW[9 * C + 1];
+  const int b = blockIdx.z, i0 = blockIdx.y * TH, j0 = blockIdx.x * TW;
+  for (int r = threadIdx.x; r < 9 * C + 1; r += TP) sW[r] = w[r];
+  for (int r = threadIdx.x; r < HT * WT * 4; r += TP) {
+    const int pix = r >> 2, part = r & 3;
+    const int gi = i0 + pix / WT - 1, gj = j0 + pix % WT - 1;
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (gi >= 0 && gi < H && gj >= 0 && gj < W)
+      v = *reinterpret_cast<const uint4*>(&X[(((size_t)b * H + gi) * W + gj) * C + part * 8]);
+    *reinterpret_cast<uint4*>(&sX[pix * XS + part * 8]) = v;
+  }
+  __syncthreads();
+  const int ti = threadIdx.x / TW, tj = threadIdx.x % TW;
+  const int gi = i0 + ti, gj = j0 + tj;
+  if (gi >= H || gj >= W) return;
+  float acc = 0.f;
+  for (int t = 0; t < 9; ++t) {
+    const bf16* xp = &sX[((ti + t / 3) * WT + tj + t % 3) * XS];
+#pragma unroll
+    for (int ci = 0; ci < C; ++ci) acc = acc + __bfloat162float(xp[ci]) * sW[t * C + ci];
+  }
+  out[((size_t)b * H + gi) * W + gj] = acc + sW[9 * C];
+}
+
+// ------------------------------------------------------------------ backward pieces
+// G4[p][ci] = sum_tap gout[p - off(tap)] * wh[tap][ci]
+__global__ void __launch_bounds__(TP) k_head_bwd(const float* __restrict__ gout, const float* __restrict__ w, int H,
+                                                 int W, float* __restrict__ G) {
+  __shared__ float sG[HT * WT];
+  __shared__ float sW[9 * C];
+  const int b = blockIdx.z, i0 = blockIdx.y * TH, j0 = blockIdx.x * TW;
+  for (int r = threadIdx.x; r < 9 * C; r += TP) sW[r] = w[r];
+  for (int r = threadIdx.x; r < HT * WT; r += TP) {
+    const int gi = i0 + r / WT - 1, gj = j0 + r % WT - 1;
+    sG[r] = (gi >= 0 && gi < H && gj >= 0 && gj < W) ? gout[((size_t)b * H + gi) * W + gj] : 0.f;
+  }
+  __syncthreads();
+  const int ti = threadIdx.x / TW, tj = threadIdx.x % TW;
+  const int gi = i0 + ti, gj = j0 + tj;
+  if (gi >= H || gj >= W) return;
+  const size_t p = ((size_t)b * H + gi) * W + gj;
+  for (int ci = 0; ci < C; ++ci) {
+    float acc = 0.f;
+    for (int t = 0; t < 9; ++t) {
+      const int tm = 8 - t;   // gout at p + off(8 - t) = p - off(t)
+      acc = acc + sG[(ti + 1 + tm / 3 - 1) * WT + tj + 1 + tm % 3 - 1] * sW[t * C + ci];
+    }
+    G[p * C + ci] = acc;
+  }
+}
+
+// DY = G * (Y > 0) in FP32 and a BF16 copy for the tensor-core data gradient.
+__global__ void k_relu_bwd(const float* __restrict__ G, const float* __restrict__ Y, float* __restrict__ DY,
+                           bf16* __restrict__ DYb, size_t n) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float v = Y[i] > 0.f ? G[i] : 0.f;
+  DY[i] = v;
+  if (DYb) DYb[i] = __float2bfloat16_rn(v);
+}
+
+template <typename XT>
+__device__ __forceinline__ float ld_as_float(const XT* p);
+template <>
+__device__ __forceinline__ float ld_as_float<float>(const float* p) { return bfr(*p); }
+template <>
+__device__ __forceinline__ float ld_as_float<bf16>(const bf16* p) { return __bfloat162float(*p); }
+
+// Weight gradient partials: part[blk][(tap * CIN + ci) * COUT + co] = sum over the block's tiles of
+// X[p + off(tap)][ci] * DY[p][co], and part[blk][9 * CIN * COUT + co] = sum DY[p][co].  Thread
+// (rg, co) owns output channel co and the (tap, ci) rows rg, rg + NRG, ...; pixels are the outer loop,
+// so each step reads one DY value and broadcasts X across the warp.
+template <int CIN, int COUT, typename XT>
+__global__ void __launch_bounds__(256) k_wgrad(const XT* __restrict__ X, const float* __restrict__ DY, int B, int H,
+                                               int W, float* __restrict__ part) {
+  constexpr int R = 9 * CIN;
+  constexpr int NRG = 256 / COUT;
+  constexpr int PER = (R + NRG - 1) / NRG;
+  constexpr int NOUT = R * COUT + COUT;
+  __shared__ float sX[HT * WT * CIN];
+  __shared__ float sD[TP * COUT];
+  const int co = threadIdx.x % COUT, rg = threadIdx.x / COUT;
+  float acc[PER];
+  float accb = 0.f;
+#pragma unroll
+  for (int m = 0; m < PER; ++m) acc[m] = 0.f;
+  const int ntiles = B * ((H + TH - 1) / TH) * ((W + TW - 1) / TW);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const TileIdx T = tile_of(tile, H, W);
+    __syncthreads();
+    for (int r = threadIdx.x; r < HT * WT * CIN; r += 256) {
+      const int pix = r / CIN, ci = r % CIN;
+      const int gi = T.i0 + pix / WT - 1, gj = T.j0 + pix % WT - 1;
+      sX[r] = (gi >= 0 && gi < H && gj >= 0 && gj < W) ? ld_as_float<XT>(X + (((size_t)T.b * H + gi) * W + gj) * CIN + ci)
+                                                       : 0.f;
+    }
+    for (int r = threadIdx.x; r < TP * COUT; r += 256) {
+      const int pix = r / COUT, c = r % COUT;
+      const int gi = T.i0 + pix / TW, gj = T.j0 + pix % TW;
+      sD[r] = (gi < H && gj < W) ? DY[(((size_t)T.b * H + gi) * W + gj) * COUT + c] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int pix = 0; pix < TP; ++pix) {
+      const float dv = sD[pix * COUT + co];
+      const int base = ((pix / TW) * WT + pix % TW) * CIN;
+      if (rg == 0) accb = accb + dv;
+#pragma unroll
+      for (int m = 0; m < PER; ++m) {
+        const int r = rg + NRG * m;
+        if (r < R) {
+          const int t = r / CIN, ci = r % CIN;
+          acc[m] = acc[m] + sX[base + ((t / 3) * WT + t % 3) * CIN + ci] * dv;
+        }
+      }
+    }
+  }
+  float* o = part + (size_t)blockIdx.x * NOUT;
+#pragma unroll
+  for (int m = 0; m < PER; ++m) {
+    const int r = rg + NRG * m;
+    if (r < R) o[r * COUT + co] = acc[m];
+  }
+  if (rg == 0) o[R * COUT + co] = accb;
+}
+
+// grad[off + o] = sum_blk part[blk][o] (fixed order); the weight part [9][CIN][COUT] first, then
+// the COUT bias entries.
+__global__ void k_wgrad_reduce(const float* __restrict__ part, int nblk, int nout, float* __restrict__ grad) {
+  const int o = blockIdx.x * blockDim.x + threadIdx.x;
+  if (o >= nout) return;
+  float s = 0.f;
+  for (int b = 0; b < nblk; ++b) s = s + part[(size_t)b * nout + o];
+  grad[o] = s;
+}
+
+// ------------------------------------------------------------------ loss and optimiser
+__global__ void k_loss_part(const float* __restrict__ out, const float* __restrict__ t, const float* __restrict__ mask,
+                            int n, float* __restrict__ part) {
+  __shared__ float s1[256], s2[256];
+  float a = 0.f, m = 0.f;
+  for (int i = blockIdx.x * 256 + threadIdx.x; i < n; i += gridDim.x * 256) {
+    if (mask[i] > 0.f) {
+      const float d = out[i] - t[i];
+      a = a + d * d;
+      m = m + 1.f;
+    }
+  }
+  s1[threadIdx.x] = a;
+  s2[threadIdx.x] = m;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) { s1[threadIdx.x] += s1[threadIdx.x + o]; s2[threadIdx.x] += s2[threadIdx.x + o]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { part[2 * blockIdx.x] = s1[0]; part[2 * blockIdx.x + 1] = s2[0]; }
+}
+
+__global__ void k_loss_final(const float* __restrict__ part, int nblk, float* __restrict__ loss) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  float a = 0.f, m = 0.f;
+  for (int b = 0; b < nblk; ++b) { a = a + part[2 * b]; m = m + part[2 * b + 1]; }
+  loss[0] = m > 0.f ? a / m : 0.f;
+  loss[1] = m;
+}
+
+__global__ void k_loss_grad(const float* __restrict__ out, const float* __restrict__ t, const float* __restrict__ mask,
+                            int n, const float* __restrict__ loss, float* __restrict__ gout) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float m = loss[1];
+  gout[i] = (mask[i] > 0.f && m > 0.f) ? 2.f * (out[i] - t[i]) / m : 0.f;
+}
+
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m, float* __restrict__ v,
+                       int n, float lr, float b1, float b2, float eps, float c1, float c2) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float gi = g[i];
+  const float mi = b1 * m[i] + (1.f - b1) * gi;
+  const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+  m[i] = mi;
+  v[i] = vi;
+  p[i] = p[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+}
+
+// ------------------------------------------------------------------ solver-side kernels
+// r0 = qq - A sp for every wet column (SolverSparse's matrix: diagonal rr, off-diagonals -sx_W,
+// -sy_S, -sy, -sx) and block partial sums of r0^2.
+__global__ void k_feat_resid(Dev d, double* __restrict__ r0, double* __restrict__ part) {
+  __shared__ double sh[256];
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  double v = 0.0;
+  if (l <= d.g.lm) {
+    const int lE = NB(d.g.lEC, l), lW = NB(d.g.lWC, l), lN = NB(d.g.lNC, l), lS = NB(d.g.lSC, l);
+    const double* sp = d.s.sp;
+    const double ax = d.s.rr[l - 1] * sp[l - 1] - d.s.sx[lW - 1] * sp[lW - 1] - d.s.sy[lS - 1] * sp[lS - 1] -
+                      d.s.sy[l - 1] * sp[lN - 1] - d.s.sx[l - 1] * sp[lE - 1];
+    const double r = d.s.qq[l - 1] - ax;
+    r0[l - 1] = r;
+    v = r * r;
+  }
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
+}
+
+__global__ void k_feat_sigma(const double* __restrict__ part, int nblk, int lm, double* __restrict__ sigma) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += part[b];
+  sigma[0] = lm > 0 ? sqrt(s / lm) : 0.0;
+}
+
+__global__ void k_feat_write(Dev d, const int* __restrict__ pix, const double* __restrict__ r0,
+                             const double* __restrict__ sigma, float* __restrict__ feat) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const double s = sigma[0];
+  const double inv = s > 0.0 ? 1.0 / s : 0.0;
+  float4 f;
+  f.x = (float)(r0[l - 1] * inv);
+  f.y = (float)((d.s.sp[l - 1] - d.s.spp[l - 1]) * inv);
+  f.z = (float)(d.g.hhs[l - 1] / 30.0);
+  f.w = 1.f;
+  *reinterpret_cast<float4*>(feat + (size_t)pix[l - 1] * 4) = f;
+}
+
+__global__ void k_feat_scatter(int lm, const int* __restrict__ pix, const float* __restrict__ out,
+                               const double* __restrict__ sigma, double* __restrict__ dz) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > lm) return;
+  const double s = sigma[0];
+  dz[l - 1] = s > 0.0 ? s * (double)out[pix[l - 1]] : 0.0;
+}
+
+__global__ void k_record(Dev d, const int* __restrict__ pix, const float* __restrict__ feat,
+                         const double* __restrict__ sigma, float* __restrict__ rec) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const size_t p = (size_t)pix[l - 1];
+  const float4 f = *reinterpret_cast<const float4*>(feat + p * 4);
+  const double s = sigma[0];
+  float* o = rec + p * 5;
+  o[0] = f.x; o[1] = f.y; o[2] = f.z; o[3] = f.w;
+  o[4] = s > 0.0 ? (float)((d.s.s[l - 1] - d.s.sp[l - 1]) / s) : 0.f;
+}
+
+dim3 tiles(int B, int H, int W) { return dim3((W + TW - 1) / TW, (H + TH - 1) / TH, B); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------- host side
+size_t Workspace::bytes(int B, int H, int W, bool training) {
+  const size_t P = (size_t)B * H * W;
+  size_t s = 0;
+  auto add = [&](size_t n) { s += (n + 255) / 256 * 256; };
+  add(2 * SI3D_NET_BLOCKS * 9 * C * C * sizeof(bf16));   // wfwd, wbwd
+  add((9 * 4 * C + C) * sizeof(float));
+  add((9 * C + 1) * sizeof(float));
+  const int nx = training ? SI3D_NET_BLOCKS + 1 : 2;
+  for (int i = 0; i < nx; ++i) add(P * C * sizeof(bf16));
+  if (training) {
+    for (int i = 0; i < SI3D_NET_BLOCKS + 1; ++i) add(P * C * sizeof(float));   // y0..y4
+    for (int i = 0; i < 3; ++i) add(P * C * sizeof(float));                     // G, G', DY
+    add(P * C * sizeof(bf16));                                                   // DYb
+    add((size_t)WG_BLOCKS * (9 * C * C + C) * sizeof(float));                    // weight-gradient partials
+  }
+  return s;
+}
+
+bool Workspace::carve(void* base, size_t avail, int B, int H, int W, bool training) {
+  if (!base || avail < bytes(B, H, W, training)) return false;
+  const size_t P = (size_t)B * H * W;
+  char* q = static_cast<char*>(base);
+  auto take = [&](size_t n) { void* r = q; q += (n + 255) / 256 * 256; return r; };
+  wfwd = static_cast<bf16*>(take(SI3D_NET_BLOCKS * 9 * C * C * sizeof(bf16) * 2));
+  wbwd = wfwd + SI3D_NET_BLOCKS * 9 * C * C;
+  stem = static_cast<float*>(take((9 * 4 * C + C) * sizeof(float)));
+  head = static_cast<float*>(take((9 * C + 1) * sizeof(float)));
+  const int nx = training ? SI3D_NET_BLOCKS + 1 : 2;
+  for (int i = 0; i < SI3D_NET_BLOCKS + 1; ++i) x[i] = nullptr;
+  for (int i = 0; i < nx; ++i) x[i] = static_cast<bf16*>(take(P * C * sizeof(bf16)));
+  for (int i = 0; i < SI3D_NET_BLOCKS + 1; ++i) y[i] = nullptr;
+  G0 = G1 = DY = nullptr;
+  DYb = nullptr;
+  part = nullptr;
+  if (training) {
+    for (int i = 0; i < SI3D_NET_BLOCKS + 1; ++i) y[i] = static_cast<float*>(take(P * C * sizeof(float)));
+    G0 = static_cast<float*>(take(P * C * sizeof(float)));
+    G1 = static_cast<float*>(take(P * C * sizeof(float)));
+    DY = static_cast<float*>(take(P * C * sizeof(float)));
+    DYb = static_cast<bf16*>(take(P * C * sizeof(bf16)));
+    part = static_cast<float*>(take((size_t)WG_BLOCKS * (9 * C * C + C) * sizeof(float)));
+  }
+  this->training = training;
+  return true;
+}
+
+void prepare(const Workspace& ws, const float* params, cudaStream_t st) {
+  const int n = SI3D_NET_BLOCKS * 9 * C * C;
+  k_prep<<<(n + 255) / 256, 256, 0, st>>>(params, ws.wfwd, ws.wbwd, ws.stem, ws.head);
+}
+
+void forward(const Workspace& ws, const float* params, const float* feat, int B, int H, int W, float* out,
+             cudaStream_t st) {
+  const float* bias0 = params + OFF_BLK + 9 * C * C;
+  const dim3 grid = tiles(B, H, W);
+  k_stem<<<grid, TP, 0, st>>>(feat, ws.stem, H, W, ws.x[0], ws.training ? ws.y[0] : nullptr);
+  for (int k = 0; k < SI3D_NET_BLOCKS; ++k) {
+    const bf16* xin = ws.training ? ws.x[k] : ws.x[k & 1];
+    bf16* xout = ws.training ? ws.x[k + 1] : ws.x[(k + 1) & 1];
+    k_conv32<CONV_FWD><<<grid, 128, 0, st>>>(xin, ws.wfwd + (size_t)k * 9 * C * C, bias0 + (size_t)k * BLK_SZ, H, W,
+                                             xout, ws.training ? ws.y[k + 1] : nullptr, nullptr, nullptr);
+  }
+  const bf16* xl = ws.training ? ws.x[SI3D_NET_BLOCKS] : ws.x[SI3D_NET_BLOCKS & 1];
+  k_head<<<grid, TP, 0, st>>>(xl, ws.head, H, W, out);
+}
+
+void backward(const Workspace& ws, const float* feat, const float* gout, int B, int H, int W, float* grad,
+              cudaStream_t st) {
+  const dim3 grid = tiles(B, H, W);
+  const size_t n = (size_t)B * H * W * C;
+  const int eb = (int)((n + 255) / 256);
+  // head
+  k_wgrad<C, 1, bf16><<<WG_BLOCKS, 256, 0, st>>>(ws.x[SI3D_NET_BLOCKS], gout, B, H, W, ws.part);
+  k_wgrad_reduce<<<(9 * C + 1 + 255) / 256, 256, 0, st>>>(ws.part, WG_BLOCKS, 9 * C + 1, grad + OFF_HEAD_W);
+  k_head_bwd<<<grid, TP, 0, st>>>(gout, ws.head, H, W, ws.G0);
+  float* G = ws.G0;
+  float* Gn = ws.G1;
+  for (int k = SI3D_NET_BLOCKS - 1; k >= 0; --k) {
+    k_relu_bwd<<<eb, 256, 0, st>>>(G, ws.y[k + 1], ws.DY, ws.DYb, n);
+    k_wgrad<C, C, bf16><<<WG_BLOCKS, 256, 0, st>>>(ws.x[k], ws.DY, B, H, W, ws.part);
+    k_wgrad_reduce<<<(BLK_SZ + 255) / 256, 256, 0, st>>>(ws.part, WG_BLOCKS, BLK_SZ, grad + OFF_BLK + k * BLK_SZ);
+    k_conv32<CONV_BWD><<<grid, 128, 0, st>>>(ws.DYb, ws.wbwd + (size_t)k * 9 * C * C, nullptr, H, W, nullptr, nullptr,
+                                             G, Gn);
+    std::swap(G, Gn);
+  }
+  k_relu_bwd<<<eb, 256, 0, st>>>(G, ws.y[0], ws.DY, nullptr, n);
+  k_wgrad<4, C, float><<<WG_BLOCKS, 256, 0, st>>>(feat, ws.DY, B, H, W, ws.part);
+  k_wgrad_reduce<<<(9 * 4 * C + C + 255) / 256, 256, 0, st>>>(ws.part, WG_BLOCKS, 9 * 4 * C + C, grad);
+}
+
+void features(const Dev& d, const int* pix, double* r0, double* part, double* sigma, float* feat, cudaStream_t st) {
+  const int nb = (d.g.lm + 255) / 256;
+  k_feat_resid<<<nb, 256, 0, st>>>(d, r0, part);
+  k_feat_sigma<<<1, 32, 0, st>>>(part, nb, d.g.lm, sigma);
+  k_feat_write<<<nb, 256, 0, st>>>(d, pix, r0, sigma, feat);
+}
+
+void scatter(int lm, const int* pix, const float* out, const double* sigma, double* dz, cudaStream_t st) {
+  k_feat_scatter<<<(lm + 255) / 256, 256, 0, st>>>(lm, pix, out, sigma, dz);
+}
+
+void record(const Dev& d, const int* pix, const float* feat, const double* sigma, float* rec, cudaStream_t st) {
+  k_record<<<(d.g.lm + 255) / 256, 256, 0, st>>>(d, pix, feat, sigma, rec);
+}
+
+int feature_partials(int lm) { return (lm + 255) / 256; }
+
+}  // namespace learn
+}  // namespace si3d
+
+// ---------------------------------------------------------------------------- C ABI (training)
+using si3d::learn::Workspace;
+
+extern "C" {
+
+size_t si3d_net_workspace_bytes(int B, int H, int W) {
+  if (B < 1 || H < 1 || W < 1) return 0;
+  return Workspace::bytes(B, H, W, true);
+}
+
+int si3d_net_forward(const float* params, const float* feat, int B, int H, int W, float* out, void* ws_ptr,
+                     size_t ws_bytes) {
+  if (!params || !feat || !out || B < 1 || H < 1 || W < 1) return SI3D_EDIMS;
+  Workspace ws;
+  if (!ws.carve(ws_ptr, ws_bytes, B, H, W, true)) return SI3D_EDIMS;
+  si3d::learn::prepare(ws, params, 0);
+  si3d::learn::forward(ws, params, feat, B, H, W, out, 0);
+  return cudaGetLastError() == cudaSuccess ? SI3D_OK : SI3D_ECUDA;
+}
+
+int si3d_net_loss(const float* out, const float* target, const float* mask, int n, float* gout, float* loss_dev) {
+  if (!out || !target || !mask || !gout || !loss_dev || n < 1) return SI3D_EDIMS;
+  constexpr int NB = 148;
+  float* part = loss_dev + 2;   // the caller's loss buffer holds 2 + 2 * 148 floats
+  si3d::learn::k_loss_part<<<NB, 256>>>(out, target, mask, n, part);
+  si3d::learn::k_loss_final<<<1, 32>>>(part, NB, loss_dev);
+  si3d::learn::k_loss_grad<<<(n + 255) / 256, 256>>>(out, target, mask, n, loss_dev, gout);
+  return cudaGetLastError() == cudaSuccess ? SI3D_OK : SI3D_ECUDA;
+}
+
+int si3d_net_backward(const float* params, const float* feat, const float* gout, int B, int H, int W, float* grad,
+                      void* ws_ptr, size_t ws_bytes) {
+  if (!params || !feat || !gout || !grad || B < 1 || H < 1 || W < 1) return SI3D_EDIMS;
+  Workspace ws;
+  if (!ws.carve(ws_ptr, ws_bytes, B, H, W, true)) return SI3D_EDIMS;
+  si3d::learn::backward(ws, feat, gout, B, H, W, grad, 0);
+  return cudaGetLastError() == cudaSuccess ? SI3D_OK : SI3D_ECUDA;
+}
+
+int si3d_net_adam(float* params, const float* grad, float* m, float* v, int n, float lr, float beta1, float beta2,
+                  float eps, int t) {
+  if (!params || !grad || !m || !v || n < 1 || t < 1) return SI3D_EDIMS;
+  const float c1 = 1.f - powf(beta1, (float)t), c2 = 1.f - powf(beta2, (float)t);
+  si3d::learn::k_adam<<<(n + 255) / 256, 256>>>(params, grad, m, v, n, lr, beta1, beta2, eps, c1, c2);
+  return cudaGetLastError() == cudaSuccess ? SI3D_OK : SI3D_ECUDA;
+}
+
+int si3d_net_sync(void) { return cudaDeviceSynchronize() == cudaSuccess ? SI3D_OK : SI3D_ECUDA; }
+
+}  // extern "C"

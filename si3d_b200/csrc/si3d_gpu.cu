@@ -11,8 +11,10 @@
 #include <vector>
 
 #include "../../include/si3d_gpu.h"
+#include "../../include/si3d_learn.h"
 #include "common.cuh"
 #include "kernels.h"
+#include "learn.h"
 
 using namespace si3d;
 
@@ -94,6 +96,18 @@ struct Ctx {
   cudaEvent_t pe0 = nullptr, pe1 = nullptr;
   double* dz = nullptr;     // learned warm-start increment (device, lm1)
   bool dz_set = false;
+  // learned initial guess: pixel of every wet column in the (im1, jm1) image, network state,
+  // features of the current solve, optional training record
+  int im1 = 1, jm1 = 1;
+  int* pix = nullptr;
+  bool net_loaded = false;
+  float* net_params = nullptr;
+  void* net_mem = nullptr;
+  learn::Workspace net_ws;
+  float *feat = nullptr, *net_out = nullptr;
+  double *r0 = nullptr, *fpart = nullptr, *sigma = nullptr;
+  float* rec_buf = nullptr;
+  int rec_slots = 0, rec_count = 0;
   double* staging = nullptr;  // device staging for transposes (km1 * lm1)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
   ~Ctx() {
@@ -129,7 +143,7 @@ Ctx* get(int h) {
 
 // Stage ids for the per-stage device timers.
 enum { ST_MOMX, ST_MOMY, ST_MATCON, ST_PCG_SETUP, ST_PCG_ITER, ST_PCG_FINISH, ST_SLAYER, ST_VEL, ST_SCALAR, ST_VEL2,
-       ST_SETTRAP, ST_SETTRAP2, ST_SAVE, ST_COUNT };
+       ST_SETTRAP, ST_SETTRAP2, ST_SAVE, ST_LEARN, ST_COUNT };
 
 // Run `f` (which enqueues `nk` kernels) as one timed stage.
 template <class F>
@@ -477,6 +491,19 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   init.hist_cap = p.pcg_itmax + 1;
   *c->h_sc = init;
   CK(cudaMemcpyAsync(c->pcg.sc, c->h_sc, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
+  const bool use_net = p.x0_mode == SI3D_X0_LEARNED && c->net_loaded;
+  if (use_net || c->rec_buf) {
+    // features of this system; with the network loaded, the predicted increment into dz
+    int rcl = stage(c, ST_LEARN, use_net ? 9 : 3, [&] {
+      learn::features(c->d, c->pix, c->r0, c->fpart, c->sigma, c->feat, c->st);
+      if (use_net) {
+        learn::forward(c->net_ws, c->net_params, c->feat, 1, c->im1, c->jm1, c->net_out, c->st);
+        learn::scatter(c->lm, c->pix, c->net_out, c->sigma, c->dz, c->st);
+      }
+    });
+    if (rcl) return rcl;
+    if (use_net) c->dz_set = true;
+  }
   const int x0 = (p.x0_mode == SI3D_X0_LEARNED && !c->dz_set) ? SI3D_X0_PREV : p.x0_mode;
   int rc0 = stage(c, ST_PCG_SETUP, 7, [&] { pcg_setup(c->d, c->pcg, x0, c->dz, &c->pcg.sc->negpiv, c->st); });
   if (rc0) return rc0;
@@ -505,6 +532,12 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   }
   rc0 = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, c->st); });
   if (rc0) return rc0;
+  if (c->rec_buf) {
+    float* slot = c->rec_buf + (size_t)(c->rec_count % c->rec_slots) * c->im1 * c->jm1 * 5;
+    learn::record(c->d, c->pix, c->feat, c->sigma, slot, c->st);
+    CK(cudaGetLastError());
+    c->rec_count++;
+  }
   const PcgScal& S = *c->h_sc;
   if (S.negpiv & 2) ier = -12;
   else if (S.ier != 0) ier = S.ier;
@@ -657,6 +690,23 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
   rc |= c->alloc(&d.scr, n3);
   rc |= c->alloc(&c->staging, (size_t)km1 * lm1);
   rc |= c->alloc(&c->dz, P);
+  // pixel (i - 1) * jm1 + (j - 1) of every wet column in the (im1, jm1) image of the learned
+  // initial guess (only when the maps describe a real grid)
+  c->im1 = std::max(g->im1, 1);
+  c->jm1 = std::max(g->jm1, 1);
+  if (!rc && g->l2i && g->l2j) {
+    std::vector<int> px(lm);
+    bool ok = true;
+    for (int l = 0; l < lm; ++l) {
+      const int i = g->l2i[l] - 1, j = g->l2j[l] - 1;
+      if (i < 0 || i >= c->im1 || j < 0 || j >= c->jm1) ok = false;
+      px[l] = i * c->jm1 + j;
+    }
+    if (ok) {
+      rc |= c->alloc(&c->pix, lm);
+      if (!rc) cudaMemcpy(c->pix, px.data(), sizeof(int) * lm, cudaMemcpyHostToDevice);
+    }
+  }
   if (rc) { delete c; return rc; }
   // face-column lists
   std::vector<int> ce, cn;
@@ -766,6 +816,64 @@ int si3d_gpu_set_warmstart(int h, const double* dz, int on_device) {
   CK(cudaStreamSynchronize(c->st));
   c->dz_set = true;
   return 0;
+}
+
+// Buffers of the learned initial guess that both inference and recording use.
+static int ensure_learn(Ctx* c) {
+  if (c->feat) return 0;
+  if (!c->pix) return SI3D_EDIMS;
+  const size_t npx = (size_t)c->im1 * c->jm1;
+  int rc = c->alloc(&c->feat, npx * 4);
+  rc |= c->alloc(&c->net_out, npx);
+  rc |= c->alloc(&c->r0, c->lm);
+  rc |= c->alloc(&c->fpart, learn::feature_partials(c->lm));
+  rc |= c->alloc(&c->sigma, 1);
+  return rc;
+}
+
+int si3d_learn_set_params(int h, const float* params) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  CK(cudaSetDevice(c->device));
+  if (!params) { c->net_loaded = false; c->dz_set = false; return 0; }
+  int rc = ensure_learn(c);
+  if (rc) return rc;
+  if (!c->net_params) {
+    const size_t wsb = learn::Workspace::bytes(1, c->im1, c->jm1, false);
+    char* mem = nullptr;
+    rc |= c->alloc(&c->net_params, SI3D_NET_NPARAM);
+    rc |= c->alloc(&mem, wsb);
+    if (rc) return rc;
+    c->net_mem = mem;
+    if (!c->net_ws.carve(mem, wsb, 1, c->im1, c->jm1, false)) return SI3D_EDIMS;
+  }
+  CK(cudaMemcpyAsync(c->net_params, params, sizeof(float) * SI3D_NET_NPARAM, cudaMemcpyHostToDevice, c->st));
+  learn::prepare(c->net_ws, c->net_params, c->st);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  c->net_loaded = true;
+  return 0;
+}
+
+int si3d_learn_record(int h, float* dev_buf, int nslots, int* hh, int* ww) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (dev_buf && nslots < 1) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  const int rc = ensure_learn(c);
+  if (rc) return rc;
+  c->rec_buf = dev_buf;
+  c->rec_slots = dev_buf ? nslots : 0;
+  c->rec_count = 0;
+  if (hh) *hh = c->im1;
+  if (ww) *ww = c->jm1;
+  return 0;
+}
+
+int si3d_learn_recorded(int h) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  return c->rec_count;
 }
 
 int si3d_gpu_fd(int h, int n, int istep, int lastiter, si3d_step_stats* st) {

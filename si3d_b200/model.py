@@ -102,6 +102,14 @@ class GpuRun:
         a = np.ascontiguousarray(dz, dtype=np.float64)
         check(self.g.si3d_gpu_set_warmstart(self.gh, native.ptr(a), 0))
 
+    def set_net(self, params: Optional[np.ndarray]) -> None:
+        """Load the learned initial guess network (include/si3d_learn.h); None unloads it."""
+        if params is None:
+            check(self.g.si3d_learn_set_params(self.gh, None))
+            return
+        a = np.ascontiguousarray(params, dtype=np.float32)
+        check(self.g.si3d_learn_set_params(self.gh, native.ptr(a)))
+
     def close(self) -> None:
         if getattr(self, "hm", None) is not None:
             self.h.si3d_host_close(self.hm)

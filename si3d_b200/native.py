@@ -76,7 +76,22 @@ GPU_SYMBOLS = {
     "si3d_gpu_sync": (C.c_int, [C.c_int]),
     "si3d_gpu_strerror": (C.c_char_p, [C.c_int]),
     "si3d_gpu_finalize": (None, [C.c_int]),
+    # learned initial guess (include/si3d_learn.h)
+    "si3d_learn_set_params": (C.c_int, [C.c_int, C.c_void_p]),
+    "si3d_learn_record": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
+    "si3d_learn_recorded": (C.c_int, [C.c_int]),
+    "si3d_net_workspace_bytes": (C.c_size_t, [C.c_int, C.c_int, C.c_int]),
+    "si3d_net_forward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                   C.c_size_t]),
+    "si3d_net_loss": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]),
+    "si3d_net_backward": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                                    C.c_void_p, C.c_size_t]),
+    "si3d_net_adam": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_float, C.c_float,
+                                C.c_float, C.c_float, C.c_int]),
+    "si3d_net_sync": (C.c_int, []),
 }
+NET_NPARAM = 9 * 4 * 32 + 32 + 4 * (9 * 32 * 32 + 32) + 9 * 32 + 1
+NET_LOSS_FLOATS = 2 + 2 * 148
 
 HOST_SYMBOLS = {
     "si3d_host_open": (C.c_int, [C.c_char_p, C.POINTER(SolverOpts), C.POINTER(C.c_int), C.c_char_p, C.c_int]),
@@ -90,7 +105,7 @@ HOST_SYMBOLS = {
 }
 
 STAGES = ("momentum_x", "momentum_y", "matcon", "pcg_setup", "pcg_iter", "pcg_finish", "slayer_h", "vel",
-          "scalar", "vel2", "settrap", "settrap2", "save")
+          "scalar", "vel2", "settrap", "settrap2", "save", "learn")
 
 _gpu = None
 _host = None

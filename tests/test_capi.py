@@ -10,7 +10,7 @@ import pytest
 
 from conftest import HAS_GPU, ROOT
 
-DECL = re.compile(r"^\s*(?:const\s+)?(?:int|void|char|double)\s*\*?\s*(si3d_\w+)\s*\(", re.M)
+DECL = re.compile(r"^\s*(?:const\s+)?(?:int|void|char|double|size_t)\s*\*?\s*(si3d_\w+)\s*\(", re.M)
 
 
 def _declared(header: str):
@@ -27,7 +27,8 @@ def test_headers_declare_the_boundary():
     assert "si3d_host_open" in host and "si3d_host_run" in host
 
 
-@pytest.mark.parametrize("header,lib", [("si3d_gpu.h", "libsi3d_gpu.so"), ("si3d_host.h", "libsi3d_host.so")])
+@pytest.mark.parametrize("header,lib", [("si3d_gpu.h", "libsi3d_gpu.so"), ("si3d_learn.h", "libsi3d_gpu.so"),
+                                        ("si3d_host.h", "libsi3d_host.so")])
 def test_library_exports_every_declared_symbol(native_libs, header, lib):
     native_libs.gpu()   # the host library resolves CUDA-core symbols from it
     so = C.CDLL(os.path.join(ROOT, "si3d_b200", "_lib", lib))
@@ -37,6 +38,7 @@ def test_library_exports_every_declared_symbol(native_libs, header, lib):
 
 def test_python_bindings_cover_the_headers(native_libs):
     gpu = set(_declared(os.path.join(ROOT, "include", "si3d_gpu.h")))
+    gpu |= set(_declared(os.path.join(ROOT, "include", "si3d_learn.h")))
     host = set(_declared(os.path.join(ROOT, "include", "si3d_host.h")))
     assert gpu == set(native_libs.GPU_SYMBOLS)
     assert host == set(native_libs.HOST_SYMBOLS)
