@@ -186,6 +186,24 @@ const char* si3d_gpu_strerror(int code);
 /* Free the device state of a handle. */
 void si3d_gpu_finalize(int handle);
 
+/* ---------------------------------------------------------------- ensembles
+ * No counterpart in the reference (one si3d process runs one basin).  Several handles (basins of
+ * any size) advance in lock step: every member's time step is enqueued on its own stream without
+ * host synchronisation (each zeta solve is one cooperative launch that iterates to convergence on the
+ * device), and one ensemble step (n >= 2) is captured once into one CUDA graph - a fork on a master
+ * stream, one branch per member, a join - then replayed, one graph launch per step.  Members must be
+ * FP64 handles on one device with the cooperative solve enabled, and must outlive the ensemble. */
+#define SI3D_ENS_MAXSOLVES 4
+int si3d_ens_create(const int* handles, int n, int* ens);
+/* Time steps n0 .. n0 + nsteps - 1 of every member.  Optional outputs per step: iters/ier
+ * [nsteps][n][SI3D_ENS_MAXSOLVES] for each zeta solve (-1 / 0 past a member's solves and for the
+ * start-up step n = 1, which runs member by member), ms[nsteps] device time of the whole ensemble step.
+ * Returns the first negative solver ier met (the reference stops there). */
+int si3d_ens_step(int ens, int n0, int nsteps, int* iters, int* ier, double* ms);
+/* Nodes of the captured step graph (0 before the first step n >= 2). */
+int si3d_ens_nodes(int ens);
+void si3d_ens_destroy(int ens);
+
 #ifdef __cplusplus
 }
 #endif

@@ -17,6 +17,8 @@
 // Only agx/arx (ag/ar) and eagx/earx are written to HBM; ex is never stored.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "kernels.h"
 
@@ -278,17 +280,26 @@ __global__ void __launch_bounds__(MT, 3) k_momentum(Dev d, const int* __restrict
 
 }  // namespace
 
+// The dynamic shared-memory limit is a property of the kernel, shared by every handle: it only ever
+// grows, to the largest tile any handle has needed (handles with different layer counts coexist).
+int momentum_init(int km1) {
+  static std::mutex mu;
+  static int granted = 0;
+  const int smem = (int)((size_t)NARR * km1 * MC * sizeof(double));
+  std::lock_guard<std::mutex> lk(mu);
+  if (smem <= granted) return 0;
+  if (cudaFuncSetAttribute(k_momentum<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1;
+  if (cudaFuncSetAttribute(k_momentum<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess) return -1;
+  granted = smem;
+  return 0;
+}
+
 void launch_momentum(const Dev& d, int ieq, const int* cols, int ncols, cudaStream_t st) {
   if (ncols <= 0) return;
   const size_t smem = (size_t)NARR * d.g.km1 * MC * sizeof(double);
   const int G = (ncols + MC - 1) / MC;
-  if (ieq == 1) {
-    cudaFuncSetAttribute(k_momentum<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_momentum<1><<<G, MT, smem, st>>>(d, cols, ncols);
-  } else {
-    cudaFuncSetAttribute(k_momentum<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_momentum<2><<<G, MT, smem, st>>>(d, cols, ncols);
-  }
+  if (ieq == 1) k_momentum<1><<<G, MT, smem, st>>>(d, cols, ncols);
+  else k_momentum<2><<<G, MT, smem, st>>>(d, cols, ncols);
 }
 
 }  // namespace si3d

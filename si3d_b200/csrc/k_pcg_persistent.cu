@@ -281,14 +281,22 @@ __global__ void __launch_bounds__(QB) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
   }
 }
 
+// Cooperative launch (all blocks co-resident) through cudaLaunchKernelEx, which stream capture
+// records as a cooperative kernel node.
 template <typename T>
 int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, cudaStream_t st) {
   if (cudaMemsetAsync(bar, 0, sizeof(GridBar), st) != cudaSuccess) return -1;
-  PcgDevT<T> Pc = P;
-  void* args[] = {(void*)&Pc, (void*)&bar};
-  return cudaLaunchCooperativeKernel((const void*)k_pcg_loop<T>, dim3(nblocks), dim3(QB), args, 0, st) == cudaSuccess
-             ? 0
-             : -1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nblocks);
+  cfg.blockDim = dim3(QB);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_pcg_loop<T>, P, bar) == cudaSuccess ? 0 : -1;
 }
 
 }  // namespace

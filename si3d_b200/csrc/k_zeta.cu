@@ -433,6 +433,27 @@ void pcg_iteration_f(const PcgDevF& F, int par, cudaStream_t st) {
   k_pcg_apply<float><<<gR + gB, PB, 0, st>>>(F, par, gR);
 }
 
+__global__ void k_pcg_init(PcgScal* sc, PcgScal init) { *sc = init; }
+
+// Per-solve statistics into device memory (iterations, NSPCG-style ier, stopping-test value), the
+// same mapping the host applies after a synchronous solve.
+__global__ void k_pcg_stats(const PcgScal* sc, int ier0, int* iters_ier, double* relres, int slot) {
+  const PcgScal& S = *sc;
+  int ier = ier0;
+  if (S.negpiv & 2) ier = -12;
+  else if (S.ier != 0) ier = S.ier;
+  else if ((S.negpiv & 1) && ier == 0) ier = 5;
+  iters_ier[2 * slot] = S.in;
+  iters_ier[2 * slot + 1] = ier;
+  relres[slot] = S.stptst;
+}
+
+void pcg_init_scalars(PcgScal* sc, const PcgScal& init, cudaStream_t st) { k_pcg_init<<<1, 1, 0, st>>>(sc, init); }
+
+void pcg_record_stats(const PcgScal* sc, int ier0, int* iters_ier, double* relres, int slot, cudaStream_t st) {
+  k_pcg_stats<<<1, 1, 0, st>>>(sc, ier0, iters_ier, relres, slot);
+}
+
 void pcg_finish(const Dev& d, const PcgDev& P, cudaStream_t st) {
   const int nR = P.R.n, nB = P.B.n;
   if (nR > 0) k_pcg_scatter<<<(nR + PB - 1) / PB, PB, 0, st>>>(d, P, 0);

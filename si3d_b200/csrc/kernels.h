@@ -33,12 +33,16 @@ struct PcgDevT {
 using PcgDev = PcgDevT<double>;
 using PcgDevF = PcgDevT<float>;
 
+int momentum_init(int km1);   // once per handle: the dynamic shared memory the momentum kernel needs
 void launch_momentum(const Dev& d, int ieq, const int* cols, int ncols, cudaStream_t st);
 void launch_matcon(const Dev& d, cudaStream_t st);
 
 void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, int* negpiv, cudaStream_t st);
 void pcg_iteration(const PcgDev& P, int par, cudaStream_t st);
 void pcg_finish(const Dev& d, const PcgDev& P, cudaStream_t st);
+// Graph-capturable solve pieces: scalars initialised by a kernel, statistics kept on the device.
+void pcg_init_scalars(PcgScal* sc, const PcgScal& init, cudaStream_t st);
+void pcg_record_stats(const PcgScal* sc, int ier0, int* iters_ier, double* relres, int slot, cudaStream_t st);
 int pcg_max_blocks(int nR, int nB);
 // Iterative refinement: FP64 residual r = rhs - A u and its squared norm into P.sc->stptst
 // (the host compares it with bnorm); FP32 inner-system set-up from the FP64 residual; the

@@ -6,6 +6,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -20,15 +21,16 @@ using namespace si3d;
 
 namespace {
 
-#define CK(x)                                     \
-  do {                                            \
-    cudaError_t e_ = (x);                         \
-    if (e_ != cudaSuccess) return cuda_fail(e_);  \
+#define CK(x)                                                 \
+  do {                                                        \
+    cudaError_t e_ = (x);                                     \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #x, __LINE__); \
   } while (0)
 
 thread_local std::string g_last_cuda;
-int cuda_fail(cudaError_t e) {
+int cuda_fail(cudaError_t e, const char* what = nullptr, int line = 0) {
   g_last_cuda = cudaGetErrorString(e);
+  if (what) g_last_cuda += std::string(" [") + what + ", si3d_gpu.cu:" + std::to_string(line) + "]";
   return SI3D_ECUDA;
 }
 
@@ -108,6 +110,12 @@ struct Ctx {
   double *r0 = nullptr, *fpart = nullptr, *sigma = nullptr;
   float* rec_buf = nullptr;
   int rec_slots = 0, rec_count = 0;
+  // graph-capturable stepping (ensembles): no host synchronisation inside a step; every solve
+  // writes (iterations, ier) and its stopping-test value into device slots
+  bool graph_mode = false;
+  int solve_slot = 0;
+  int* d_stats_ii = nullptr;     // [24][2]
+  double* d_stats_rr = nullptr;  // [24]
   double* staging = nullptr;  // device staging for transposes (km1 * lm1)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
   ~Ctx() {
@@ -406,7 +414,7 @@ void eigen_estimates(const double* al, const double* be, int n, double zeta, int
 template <class F, class G>
 int iterate(Ctx* c, PcgScal* dsc, PcgScal* hsc, int itmax, int predicted, F&& launch_one, G&& launch_loop) {
   if (c->persistent) {
-    if (launch_loop() != 0) { g_last_cuda = cudaGetErrorString(cudaGetLastError()); return SI3D_ECUDA; }
+    if (launch_loop() != 0) return cuda_fail(cudaGetLastError(), "pcg_loop", __LINE__);
     c->launches += 1;
     CK(cudaMemcpyAsync(hsc, dsc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -489,8 +497,15 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   init.ntest = p.pcg_test;
   init.emax = 2.0; init.emin = 1.0; init.udnm = 1.0;
   init.hist_cap = p.pcg_itmax + 1;
-  *c->h_sc = init;
-  CK(cudaMemcpyAsync(c->pcg.sc, c->h_sc, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
+  if (c->graph_mode) {
+    // the scalars are set by a kernel (a host copy would capture a host buffer that later solves reuse)
+    if (p.precision != SI3D_FP64 || !c->persistent || c->rec_buf) return SI3D_EDIMS;
+    pcg_init_scalars(c->pcg.sc, init, c->st);
+    c->launches += 1;
+  } else {
+    *c->h_sc = init;
+    CK(cudaMemcpyAsync(c->pcg.sc, c->h_sc, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
+  }
   const bool use_net = p.x0_mode == SI3D_X0_LEARNED && c->net_loaded;
   if (use_net || c->rec_buf) {
     // features of this system; with the network loaded, the predicted increment into dz
@@ -507,6 +522,19 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   const int x0 = (p.x0_mode == SI3D_X0_LEARNED && !c->dz_set) ? SI3D_X0_PREV : p.x0_mode;
   int rc0 = stage(c, ST_PCG_SETUP, 7, [&] { pcg_setup(c->d, c->pcg, x0, c->dz, &c->pcg.sc->negpiv, c->st); });
   if (rc0) return rc0;
+  if (c->graph_mode) {
+    if (pcg_loop(c->pcg, c->bar, c->loop_blocks, c->st) != 0) return cuda_fail(cudaGetLastError(), "pcg_loop", __LINE__);
+    c->launches += 1;
+    rc0 = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, c->st); });
+    if (rc0) return rc0;
+    pcg_record_stats(c->pcg.sc, ier, c->d_stats_ii, c->d_stats_rr, std::min(c->solve_slot, 23), c->st);
+    c->launches += 1;
+    c->solve_slot++;
+    *iters = 0;
+    *relres = 0.0;
+    *ier_out = 0;
+    return 0;
+  }
   if (c->prof) CK(cudaEventRecord(c->pe0, c->st));
   int total_iters = 0;
   if (p.precision == SI3D_MIXED_IR) {
@@ -690,6 +718,9 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
   rc |= c->alloc(&d.scr, n3);
   rc |= c->alloc(&c->staging, (size_t)km1 * lm1);
   rc |= c->alloc(&c->dz, P);
+  rc |= c->alloc(&c->d_stats_ii, 48);
+  rc |= c->alloc(&c->d_stats_rr, 24);
+  if (!rc && momentum_init(km1) != 0) { g_last_cuda = "momentum kernel shared-memory attribute"; rc = SI3D_ECUDA; }
   // pixel (i - 1) * jm1 + (j - 1) of every wet column in the (im1, jm1) image of the learned
   // initial guess (only when the maps describe a real grid)
   c->im1 = std::max(g->im1, 1);
@@ -969,10 +1000,9 @@ int si3d_gpu_save(int h, int istep) {
 }
 
 // Loop body of si3d.f90:324-458 for step n (outputs omitted).
-int si3d_gpu_step(int h, int n, si3d_step_stats* st) {
-  Ctx* c = get(h);
-  if (!c) return SI3D_EHANDLE;
-  CK(cudaSetDevice(c->device));
+// The stage sequence of one time step n (si3d.f90:324-458): leapfrog fd, settrap, niter
+// trapezoidal fd/settrap2 iterations, save.  Enqueues only; the caller synchronises.
+static int step_impl(Ctx* c, int n, si3d_step_stats* st) {
   if (st) { std::memset(st, 0, sizeof(*st)); CK(cudaEventRecord(c->ev0, c->st)); }
   const si3d_params& p = c->prm;
   int niter1 = p.niter;
@@ -1010,8 +1040,169 @@ done:
     CK(cudaEventElapsedTime(&ms, c->ev0, c->ev1));
     st->ms_total = ms;
   }
+  return 0;
+}
+
+int si3d_gpu_step(int h, int n, si3d_step_stats* st) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  CK(cudaSetDevice(c->device));
+  const int rc = step_impl(c, n, st);
+  if (rc) return rc;
   CK(cudaStreamSynchronize(c->st));
   return 0;
+}
+
+// ---------------------------------------------------------------------------- ensembles
+struct Ens {
+  int device = 0;
+  std::vector<int> hs;
+  std::vector<int> nsolves;          // solves per step of each member (from the capture)
+  cudaStream_t master = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  size_t nodes = 0;
+  std::vector<cudaEvent_t> joins;
+  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  ~Ens() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (cudaEvent_t e : joins) cudaEventDestroy(e);
+    for (cudaEvent_t e : {fork, t0, t1}) if (e) cudaEventDestroy(e);
+    if (master) cudaStreamDestroy(master);
+  }
+};
+std::vector<Ens*> g_ens;
+
+Ens* get_ens(int e) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (e < 0 || e >= (int)g_ens.size()) return nullptr;
+  return g_ens[e];
+}
+
+int si3d_ens_create(const int* handles, int n, int* ens) {
+  if (!handles || n < 1 || !ens) return SI3D_EDIMS;
+  auto E = std::make_unique<Ens>();
+  for (int i = 0; i < n; ++i) {
+    Ctx* c = get(handles[i]);
+    if (!c) return SI3D_EHANDLE;
+    if (i == 0) E->device = c->device;
+    if (c->device != E->device || c->prm.precision != SI3D_FP64 || !c->persistent) return SI3D_EDIMS;
+    for (int j = 0; j < i; ++j)
+      if (handles[j] == handles[i]) return SI3D_EDIMS;
+    E->hs.push_back(handles[i]);
+  }
+  CK(cudaSetDevice(E->device));
+  CK(cudaStreamCreateWithFlags(&E->master, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&E->fork, &E->t0, &E->t1}) CK(cudaEventCreate(e));
+  E->joins.resize(n);
+  for (auto& e : E->joins) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  std::lock_guard<std::mutex> lk(g_mu);
+  g_ens.push_back(E.release());
+  *ens = (int)g_ens.size() - 1;
+  return 0;
+}
+
+// Capture one step (n >= 2) of every member into one graph: a fork on the master stream, each
+// member's step on its own stream, a join back.
+static int ens_capture(Ens* E) {
+  CK(cudaStreamBeginCapture(E->master, cudaStreamCaptureModeThreadLocal));
+  int rc = 0;
+  cudaError_t e = cudaEventRecord(E->fork, E->master);
+  E->nsolves.assign(E->hs.size(), 0);
+  for (size_t i = 0; i < E->hs.size() && !rc && e == cudaSuccess; ++i) {
+    Ctx* c = get(E->hs[i]);
+    e = cudaStreamWaitEvent(c->st, E->fork, 0);
+    if (e != cudaSuccess) break;
+    c->graph_mode = true;
+    c->solve_slot = 0;
+    const bool prof = c->prof;
+    c->prof = false;
+    rc = step_impl(c, 2, nullptr);
+    c->prof = prof;
+    c->graph_mode = false;
+    E->nsolves[i] = std::min(c->solve_slot, 24);
+    if (!rc) e = cudaEventRecord(E->joins[i], c->st);
+    if (!rc && e == cudaSuccess) e = cudaStreamWaitEvent(E->master, E->joins[i], 0);
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(E->master, &g);
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(e); }
+  if (e2 != cudaSuccess) return cuda_fail(e2);
+  E->graph = g;
+  CK(cudaGraphGetNodes(g, nullptr, &E->nodes));
+  CK(cudaGraphInstantiate(&E->exec, g, 0));
+  return 0;
+}
+
+int si3d_ens_step(int ens, int n0, int nsteps, int* iters, int* ier, double* ms) {
+  Ens* E = get_ens(ens);
+  if (!E) return SI3D_EHANDLE;
+  if (n0 < 1 || nsteps < 0) return SI3D_EDIMS;
+  CK(cudaSetDevice(E->device));
+  const int m = (int)E->hs.size();
+  for (int s = 0; s < nsteps; ++s) {
+    const int n = n0 + s;
+    if (iters) for (int i = 0; i < m * SI3D_ENS_MAXSOLVES; ++i) iters[(size_t)s * m * SI3D_ENS_MAXSOLVES + i] = -1;
+    if (ier) for (int i = 0; i < m * SI3D_ENS_MAXSOLVES; ++i) ier[(size_t)s * m * SI3D_ENS_MAXSOLVES + i] = 0;
+    if (n == 1) {   // the start-up step has its own sequence; run it member by member
+      CK(cudaEventRecord(E->t0, E->master));
+      for (int i = 0; i < m; ++i) {
+        Ctx* c = get(E->hs[i]);
+        CK(cudaStreamWaitEvent(c->st, E->t0, 0));
+        const int rc = step_impl(c, 1, nullptr);
+        if (rc) return rc;
+        CK(cudaEventRecord(E->joins[i], c->st));
+        CK(cudaStreamWaitEvent(E->master, E->joins[i], 0));
+      }
+      CK(cudaEventRecord(E->t1, E->master));
+    } else {
+      if (!E->exec) {
+        const int rc = ens_capture(E);
+        if (rc) return rc;
+      }
+      CK(cudaEventRecord(E->t0, E->master));
+      CK(cudaGraphLaunch(E->exec, E->master));
+      CK(cudaEventRecord(E->t1, E->master));
+    }
+    CK(cudaStreamSynchronize(E->master));
+    if (ms) {
+      float t = 0;
+      CK(cudaEventElapsedTime(&t, E->t0, E->t1));
+      ms[s] = t;
+    }
+    if (n > 1 && (iters || ier)) {
+      for (int i = 0; i < m; ++i) {
+        Ctx* c = get(E->hs[i]);
+        int buf[48];
+        CK(cudaMemcpy(buf, c->d_stats_ii, sizeof(buf), cudaMemcpyDeviceToHost));
+        for (int k = 0; k < std::min(E->nsolves[i], SI3D_ENS_MAXSOLVES); ++k) {
+          const size_t o = ((size_t)s * m + i) * SI3D_ENS_MAXSOLVES + k;
+          if (iters) iters[o] = buf[2 * k];
+          if (ier) ier[o] = buf[2 * k + 1];
+        }
+        for (int k = 0; k < E->nsolves[i]; ++k)
+          if (buf[2 * k + 1] < 0) return buf[2 * k + 1];   // the reference stops on ier < 0
+      }
+    }
+  }
+  return 0;
+}
+
+int si3d_ens_nodes(int ens) {
+  Ens* E = get_ens(ens);
+  if (!E) return SI3D_EHANDLE;
+  return (int)E->nodes;
+}
+
+void si3d_ens_destroy(int ens) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (ens < 0 || ens >= (int)g_ens.size() || !g_ens[ens]) return;
+  cudaSetDevice(g_ens[ens]->device);
+  cudaStreamSynchronize(g_ens[ens]->master);
+  delete g_ens[ens];
+  g_ens[ens] = nullptr;
 }
 
 int si3d_gpu_profile(int h, int enable) {

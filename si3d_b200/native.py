@@ -76,6 +76,10 @@ GPU_SYMBOLS = {
     "si3d_gpu_sync": (C.c_int, [C.c_int]),
     "si3d_gpu_strerror": (C.c_char_p, [C.c_int]),
     "si3d_gpu_finalize": (None, [C.c_int]),
+    "si3d_ens_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
+    "si3d_ens_step": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
+    "si3d_ens_nodes": (C.c_int, [C.c_int]),
+    "si3d_ens_destroy": (None, [C.c_int]),
     # learned initial guess (include/si3d_learn.h)
     "si3d_learn_set_params": (C.c_int, [C.c_int, C.c_void_p]),
     "si3d_learn_record": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]),
@@ -90,6 +94,7 @@ GPU_SYMBOLS = {
                                 C.c_float, C.c_float, C.c_int]),
     "si3d_net_sync": (C.c_int, []),
 }
+ENS_MAXSOLVES = 4
 NET_NPARAM = 9 * 4 * 32 + 32 + 4 * (9 * 32 * 32 + 32) + 9 * 32 + 1
 NET_LOSS_FLOATS = 2 + 2 * 148
 
