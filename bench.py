@@ -189,7 +189,7 @@ def bench_ensemble(args, ws: int, rank: int, device: int, pg) -> int:
     dirs = ensemble.write([members[i] for i in chosen], root)
     lm = [counts(d) for d in dirs]
     t_setup = time.perf_counter()
-    ens = ensemble.Ensemble(dirs, device=device, pcg_itmax=args.itmax)
+    ens = ensemble.Ensemble(dirs, device=device, pcg_itmax=args.itmax, autotune=True)
     t_setup = time.perf_counter() - t_setup
     try:
         ens.step(args.warmup)
@@ -300,7 +300,8 @@ def main() -> int:
         return replicas.max_over_ranks(x, pg, device=f"cuda:{device}")
 
     def measure(form: str, precision: int, x0_mode: int, params, headline: bool) -> dict:
-        run = GpuRun(run_dir, device=device, pcg_itmax=args.itmax, precision=precision, x0_mode=x0_mode)
+        run = GpuRun(run_dir, device=device, pcg_itmax=args.itmax, precision=precision, x0_mode=x0_mode,
+                     autotune=True)
         if params is not None:
             run.set_net(params)
         run.run(args.warmup)
@@ -321,7 +322,7 @@ def main() -> int:
         t_wall = time.perf_counter() - t_wall
         clk = clocks.stop() if clocks else None
         launches1, _ = run.counters()
-        out = {"s_per_step": reduce_max(sum(s.ms_total for s in stats) / 1e3 / args.steps),
+        out = {"s_per_step": reduce_max(sum(s.ms_total for s in stats) / 1e3 / args.steps), "launch_shapes": run.tune,
                "pcg_s_per_step": sum(s.ms_pcg for s in stats) / 1e3 / args.steps,
                "pcg_iters_per_step": sum(s.total_iters for s in stats) / args.steps,
                "max_relres": max(max(s.relres[i] for i in range(s.nsolves)) for s in stats),

@@ -179,6 +179,16 @@ int si3d_gpu_counters(int handle, long long* launches, double* stage_ms, long lo
 int si3d_gpu_column_tridiag_noalloc(int n, int nsys, const double* a, const double* b, const double* c,
                                    const double* g, const double* r, double* ag, double* ar, void* stream);
 
+/* Autotuner (no reference counterpart): times every candidate launch shape of the momentum and
+ * scalar-transport stages on this handle's current state and keeps the fastest - layer lanes per
+ * column of the cell-parallel kernels (2, 4, 8) and threads per block of the column-sequential
+ * kernels (64, 128, 256).  The fields those stages write are restored afterwards, so the state is
+ * unchanged; shapes never change results.  `reps` timed launches per candidate; the choice
+ * {mom_lanes, mom_threads, scalar_lanes, scalar_threads} is returned through `choice` (optional). */
+int si3d_gpu_autotune(int handle, int reps, int* choice);
+/* Apply a launch-shape choice (e.g. a cached autotuner result). */
+int si3d_gpu_set_tune(int handle, const int* choice);
+
 /* Wait for the handle's stream. */
 int si3d_gpu_sync(int handle);
 /* Human-readable text for an error code. */

@@ -223,17 +223,23 @@ __device__ __forceinline__ double superbee(double s1, double s2, double s3, doub
   return C_f;
 }
 
-__global__ void k_exsal_flux(Dev d) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+// Cell-parallel kernels use blocks of 32 consecutive columns x CLN layer lanes: a warp reads one
+// layer of 32 consecutive columns (coalesced) and each thread takes layers k0 + lane, k0 + lane + CLN...
+
+// exsal's three limited fluxes per cell (:2895-3013), into the persistent Bth2/Bth4/Bth3 fields.
+template <int CLN>
+__global__ void __launch_bounds__(32 * CLN) k_exsal_flux(Dev d) {
+  const int l = blockIdx.x * 32 + threadIdx.x + 1;
   if (l > d.g.lm) return;
   const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
+  if (k1s + (int)threadIdx.y > kms) return;
   const int lE = NB(d.g.lEC, l), lW = NB(d.g.lWC, l), lN = NB(d.g.lNC, l), lS = NB(d.g.lSC, l);
   const int lEE = NB(d.g.lEC, lE), lNN = NB(d.g.lNC, lN);
   const double twodt1 = d.p.twodt * d.tz;
   const double* sp = d.f.salpp;
   const double* hpp = d.f.hpp;
   const double* hp = d.f.hp;
-  for (int k = k1s; k <= kms; ++k) {
+  for (int k = k1s + threadIdx.y; k <= kms; k += CLN) {
     const int ik = IX(d, k, l);
     // EW
     if (d.f.hup[ik] > ZERO) {
@@ -273,19 +279,18 @@ __device__ __forceinline__ double bha(const Dev& d, const double* hvpp, double A
   return A * hvpp[IX(d, k, m)];
 }
 
-// exsal's divergence (Bex) fused with imsal's vertical-diffusion tridiagonal solve.
-__global__ void k_exsal_imsal(Dev d) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+// exsal's divergence Bex plus the heat source (imsal's right-hand side ds, :3059-3065, :3113) per
+// cell, staged in sal (which imsal then overwrites with the solution in place).
+template <int CLN>
+__global__ void __launch_bounds__(32 * CLN) k_exsal_rhs(Dev d) {
+  const int l = blockIdx.x * 32 + threadIdx.x + 1;
   if (l > d.g.lm) return;
   const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
-  const int nw = kms - k1s + 1;
-  if (nw < 1) return;
+  if (k1s + (int)threadIdx.y > kms) return;
   const int lE = NB(d.g.lEC, l), lW = NB(d.g.lWC, l), lN = NB(d.g.lNC, l), lS = NB(d.g.lSC, l);
   const double twodt1 = d.p.twodt * d.tz;
   const double* sp = d.f.salpp;
-  double* sal = d.f.sal;
-  double* esc = d.scr;
-  auto bex = [&](int k) -> double {
+  for (int k = k1s + threadIdx.y; k <= kms; k += CLN) {
     const int ik = IX(d, k, l);
     const double spc = sp[ik];
     double v = d.f.hpp[ik] * spc / twodt1 - (d.f.Bth2[ik] - d.f.Bth2[IX(d, k, lW)]) / d.p.dx -
@@ -297,50 +302,69 @@ __global__ void k_exsal_imsal(Dev d) {
                          bha(d, d.f.hvpp, d.p.Ay0, lS, k) * (spc - sp[IX(d, k, lS)])) / d.p.dydy;
       v = v + hd;
     }
-    return v;
-  };
+    d.f.sal[ik] = v + d.f.HeatSource[ik];
+  }
+}
+
+// imsal's vertical-diffusion tridiagonal solve per column (trid1), right-hand side read from sal.
+template <int NTB>
+__global__ void __launch_bounds__(NTB) k_imsal(Dev d) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
+  const int nw = kms - k1s + 1;
+  if (nw < 1) return;
+  const int P = d.g.P;
+  const double twodt1 = d.p.twodt * d.tz;
+  const double* __restrict__ sp = d.f.salpp;
+  const double* __restrict__ h = d.f.h;
+  const double* __restrict__ Dv = d.f.Dv;
+  double* __restrict__ sal = d.f.sal;
+  double* __restrict__ esc = d.scr;
   // layer thickness at time n with the surface corrections (:3128-3132)
+  const double hpp_k1 = d.f.hpp[IX(d, k1s, l)];
   auto hn = [&](int k) -> double {
-    if (k == k1s) return twodt1 * d.f.wp[IX(d, k1s, l)] + d.f.hpp[IX(d, k1s, l)];
-    if (k == k1s + 1 && d.f.hpp[IX(d, k1s, l)] <= ZERO) return d.f.hpp[IX(d, k1s + 1, l)];
-    return d.f.h[IX(d, k, l)];
+    if (k == k1s) return twodt1 * d.f.wp[IX(d, k1s, l)] + hpp_k1;
+    if (k == k1s + 1 && hpp_k1 <= ZERO) return d.f.hpp[IX(d, k1s + 1, l)];
+    return h[IX(d, k, l)];
   };
   if (nw == 1) {
     const double a2 = hn(k1s) / twodt1;
-    const double ds = bex(k1s) + d.f.HeatSource[IX(d, k1s, l)];
+    const double ds = sal[IX(d, k1s, l)];
     double v = ds / a2;
-    if (d.f.h[IX(d, k1s, l)] < 1.E-2) v = sp[IX(d, k1s, l)];
+    if (h[IX(d, k1s, l)] < 1.E-2) v = sp[IX(d, k1s, l)];
     sal[IX(d, k1s, l)] = v;
     return;
   }
-  // trid1 forward sweep: e in scratch, f in sal
-  double hn_k = hn(k1s), e_prev = 0, f_prev = 0;
-  for (int k = k1s; k <= kms; ++k) {
+  // trid1 forward sweep: e in scratch, f in sal; inputs loaded one layer ahead
+  double hn_k = hn(k1s), hn_km = 0.0, e_prev = 0, f_prev = 0;
+  int ik = IX(d, k1s, l);
+  double n_ds = sal[ik], n_dv = Dv[ik], n_dvp = Dv[ik + P];
+  for (int k = k1s; k <= kms; ++k, ik += P) {
+    const double ds = n_ds, dvk = n_dv, dvkp = n_dvp;
+    if (k < kms) { n_ds = sal[ik + P]; n_dv = Dv[ik + P]; n_dvp = Dv[ik + 2 * P]; }
     const double hn_kp = (k < kms) ? hn(k + 1) : 0.0;
-    const double a3 = (k < kms) ? -d.f.Dv[IX(d, k + 1, l)] / (hn_k + hn_kp) * 2. : 0.0;
+    const double a3 = (k < kms) ? -dvkp / (hn_k + hn_kp) * 2. : 0.0;
     double a1 = 0.0;
-    if (k > k1s) {
-      const double hn_km = hn(k - 1);
-      a1 = -d.f.Dv[IX(d, k, l)] / (hn_km + hn_k) * 2.;
-    }
+    if (k > k1s) a1 = -dvk / (hn_km + hn_k) * 2.;
     const double a2 = hn_k / twodt1 - a1 - a3;
-    const double ds = bex(k) + d.f.HeatSource[IX(d, k, l)];
     const int kk = k - k1s + 1;
     if (kk == 1) {
       e_prev = -a3 / a2;
       f_prev = ds / a2;
-      esc[IX(d, k, l)] = e_prev;
-      sal[IX(d, k, l)] = f_prev;
+      esc[ik] = e_prev;
+      sal[ik] = f_prev;
     } else if (kk < nw) {
       const double den = a2 + a1 * e_prev;
       const double e = -a3 / den;
       const double f = (ds - a1 * f_prev) / den;
-      esc[IX(d, k, l)] = e;
-      sal[IX(d, k, l)] = f;
+      esc[ik] = e;
+      sal[ik] = f;
       e_prev = e; f_prev = f;
     } else {
-      sal[IX(d, k, l)] = (ds - a1 * f_prev) / (a2 + a1 * e_prev);
+      sal[ik] = (ds - a1 * f_prev) / (a2 + a1 * e_prev);
     }
+    hn_km = hn_k;
     hn_k = hn_kp;
   }
   double nxt = sal[IX(d, kms, l)];
@@ -578,9 +602,18 @@ void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cu
   k_cont1<<<grid_of(d.g.lm), TB, 0, st>>>(d);
 }
 
-void launch_exsal_imsal(const Dev& d, cudaStream_t st) {
-  k_exsal_flux<<<grid_of(d.g.lm), TB, 0, st>>>(d);
-  k_exsal_imsal<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+void launch_exsal_imsal(const Dev& d, const Tune& tu, cudaStream_t st) {
+  const int cg = (d.g.lm + 31) / 32;
+  switch (tu.sal_cl) {
+    case 2: k_exsal_flux<2><<<cg, dim3(32, 2), 0, st>>>(d); k_exsal_rhs<2><<<cg, dim3(32, 2), 0, st>>>(d); break;
+    case 4: k_exsal_flux<4><<<cg, dim3(32, 4), 0, st>>>(d); k_exsal_rhs<4><<<cg, dim3(32, 4), 0, st>>>(d); break;
+    default: k_exsal_flux<8><<<cg, dim3(32, 8), 0, st>>>(d); k_exsal_rhs<8><<<cg, dim3(32, 8), 0, st>>>(d); break;
+  }
+  switch (tu.sal_nt) {
+    case 64: k_imsal<64><<<(d.g.lm + 63) / 64, 64, 0, st>>>(d); break;
+    case 256: k_imsal<256><<<(d.g.lm + 255) / 256, 256, 0, st>>>(d); break;
+    default: k_imsal<128><<<(d.g.lm + 127) / 128, 128, 0, st>>>(d); break;
+  }
 }
 
 void launch_vel2(const Dev& d, cudaStream_t st) { k_vel2<<<grid_of(d.g.lm), TB, 0, st>>>(d); }

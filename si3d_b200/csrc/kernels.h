@@ -33,8 +33,15 @@ struct PcgDevT {
 using PcgDev = PcgDevT<double>;
 using PcgDevF = PcgDevT<float>;
 
-int momentum_init(int km1);   // once per handle: the dynamic shared memory the momentum kernel needs
-void launch_momentum(const Dev& d, int ieq, const int* cols, int ncols, cudaStream_t st);
+// Launch shapes of the column stages that the autotuner picks per handle (results do not depend on
+// them): layer lanes per column of the cell-parallel kernels (2, 4, 8) and threads per block of the
+// column-sequential kernels (64, 128, 256).
+struct Tune {
+  int mom_cl = 8, mom_nt = 128, sal_cl = 8, sal_nt = 128;
+};
+
+int momentum_init(int km1);
+void launch_momentum(const Dev& d, int ieq, const int* cols, int ncols, const Tune& tu, cudaStream_t st);
 void launch_matcon(const Dev& d, cudaStream_t st);
 
 void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, int* negpiv, cudaStream_t st);
@@ -63,7 +70,7 @@ int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st);
 
 void launch_slayer_h(const Dev& d, cudaStream_t st);
 void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cudaStream_t st);
-void launch_exsal_imsal(const Dev& d, cudaStream_t st);
+void launch_exsal_imsal(const Dev& d, const Tune& tu, cudaStream_t st);
 void launch_vel2(const Dev& d, cudaStream_t st);
 void launch_settrap(const Dev& d, cudaStream_t st);
 void launch_settrap2(const Dev& d, cudaStream_t st);

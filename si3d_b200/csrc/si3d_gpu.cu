@@ -112,6 +112,7 @@ struct Ctx {
   int rec_slots = 0, rec_count = 0;
   // graph-capturable stepping (ensembles): no host synchronisation inside a step; every solve
   // writes (iterations, ier) and its stopping-test value into device slots
+  Tune tune;                     // launch shapes of the column stages (autotuned)
   bool graph_mode = false;
   int solve_slot = 0;
   int* d_stats_ii = nullptr;     // [24][2]
@@ -580,8 +581,8 @@ int fd_impl(Ctx* c, int istep, si3d_step_stats* st) {
   Dev& d = c->d;
   d.tz = 1.0 / istep;
   // surfbc CASE(0) is a constant per-column wind set by the host (uair/vair/cdw fields)
-  int rc = stage(c, ST_MOMX, 1, [&] { launch_momentum(d, 1, c->ce, c->nce, c->st); });
-  if (!rc) rc = stage(c, ST_MOMY, 1, [&] { launch_momentum(d, 2, c->cn, c->ncn, c->st); });
+  int rc = stage(c, ST_MOMX, 2, [&] { launch_momentum(d, 1, c->ce, c->nce, c->tune, c->st); });
+  if (!rc) rc = stage(c, ST_MOMY, 2, [&] { launch_momentum(d, 2, c->cn, c->ncn, c->tune, c->st); });
   if (!rc) rc = stage(c, ST_MATCON, 1, [&] { launch_matcon(d, c->st); });
   if (rc) return rc;
   if (st) CK(cudaEventRecord(c->evp0, c->st));
@@ -600,7 +601,7 @@ int fd_impl(Ctx* c, int istep, si3d_step_stats* st) {
   if (ier < 0) return ier;
   rc = stage(c, ST_SLAYER, 1, [&] { launch_slayer_h(d, c->st); });
   if (!rc) rc = stage(c, ST_VEL, 3, [&] { launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st); });
-  if (!rc && c->prm.isal != 0) rc = stage(c, ST_SCALAR, 2, [&] { launch_exsal_imsal(d, c->st); });
+  if (!rc && c->prm.isal != 0) rc = stage(c, ST_SCALAR, 3, [&] { launch_exsal_imsal(d, c->tune, c->st); });
   if (!rc) rc = stage(c, ST_VEL2, 1, [&] { launch_vel2(d, c->st); });
   if (rc) return rc;
   if (st) {
@@ -946,7 +947,7 @@ int si3d_gpu_stage(int h, const char* stage, int istep, si3d_step_stats* st) {
   const std::string s = stage;
   Dev& d = c->d;
   d.tz = 1.0 / istep;
-  if (s == "momentum") { launch_momentum(d, 1, c->ce, c->nce, c->st); launch_momentum(d, 2, c->cn, c->ncn, c->st); }
+  if (s == "momentum") { launch_momentum(d, 1, c->ce, c->nce, c->tune, c->st); launch_momentum(d, 2, c->cn, c->ncn, c->tune, c->st); }
   else if (s == "matcon") launch_matcon(d, c->st);
   else if (s == "solve") {
     int it = 0, ier = 0;
@@ -957,7 +958,7 @@ int si3d_gpu_stage(int h, const char* stage, int istep, si3d_step_stats* st) {
     if (ier < 0) return ier;
     launch_slayer_h(d, c->st);
   } else if (s == "vel") launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st);
-  else if (s == "scalar") launch_exsal_imsal(d, c->st);
+  else if (s == "scalar") launch_exsal_imsal(d, c->tune, c->st);
   else if (s == "vel2") launch_vel2(d, c->st);
   else if (s == "settrap") launch_settrap(d, c->st);
   else if (s == "settrap2") launch_settrap2(d, c->st);
@@ -1050,6 +1051,107 @@ int si3d_gpu_step(int h, int n, si3d_step_stats* st) {
   const int rc = step_impl(c, n, st);
   if (rc) return rc;
   CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+// ---------------------------------------------------------------------------- autotuner
+// Picks the launch shapes of the momentum and scalar-transport stages for this handle's grid by
+// timing every candidate on the handle's current state.  The fields those stages write are saved
+// first (device copy when memory allows, else host) and restored afterwards, so the model state is
+// bit-identical before and after; the shapes never change results.
+static int time_stage(Ctx* c, int which, int reps, float* best) {
+  Dev& d = c->d;
+  auto run = [&] {
+    if (which == 0) {
+      launch_momentum(d, 1, c->ce, c->nce, c->tune, c->st);
+      launch_momentum(d, 2, c->cn, c->ncn, c->tune, c->st);
+    } else {
+      launch_exsal_imsal(d, c->tune, c->st);
+    }
+  };
+  run();   // warm-up
+  CK(cudaGetLastError());
+  CK(cudaEventRecord(c->pe0, c->st));
+  for (int r = 0; r < reps; ++r) run();
+  CK(cudaEventRecord(c->pe1, c->st));
+  CK(cudaEventSynchronize(c->pe1));
+  CK(cudaGetLastError());
+  float ms = 0;
+  CK(cudaEventElapsedTime(&ms, c->pe0, c->pe1));
+  *best = ms / reps;
+  return 0;
+}
+
+int si3d_gpu_autotune(int h, int reps, int* choice) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (reps < 1) reps = 3;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->st));
+  Dev& d = c->d;
+  const size_t n3 = (size_t)c->km1 * c->P, n2 = (size_t)c->P;
+  std::vector<std::pair<double*, size_t>> keep = {
+      {d.f.agx, n3}, {d.f.arx, n3}, {d.f.agy, n3}, {d.f.ary, n3}, {d.scr, n3}, {d.f.Bth2, n3},
+      {d.f.Bth3, n3}, {d.f.Bth4, n3}, {d.f.sal, n3}, {d.s.eagx, n2}, {d.s.earx, n2}, {d.s.eagy, n2},
+      {d.s.eary, n2}};
+  size_t total = 0;
+  for (auto& k : keep) total += k.second;
+  size_t free_b = 0, tot_b = 0;
+  CK(cudaMemGetInfo(&free_b, &tot_b));
+  double* dev_copy = nullptr;
+  std::vector<double> host_copy;
+  if (free_b > total * sizeof(double) + (size_t(2) << 30) &&
+      cudaMalloc(&dev_copy, total * sizeof(double)) == cudaSuccess) {
+    size_t o = 0;
+    for (auto& k : keep) { CK(cudaMemcpy(dev_copy + o, k.first, k.second * sizeof(double), cudaMemcpyDeviceToDevice)); o += k.second; }
+  } else {
+    cudaGetLastError();
+    host_copy.resize(total);
+    size_t o = 0;
+    for (auto& k : keep) { CK(cudaMemcpy(host_copy.data() + o, k.first, k.second * sizeof(double), cudaMemcpyDeviceToHost)); o += k.second; }
+  }
+  int rc = 0;
+  auto pick = [&](int which, int* knob, std::initializer_list<int> cands) {
+    int best_v = *knob;
+    float best_t = 1e30f;
+    for (int v : cands) {
+      if (rc) return;
+      *knob = v;
+      float t = 0;
+      rc = time_stage(c, which, reps, &t);
+      if (!rc && t < best_t) { best_t = t; best_v = v; }
+    }
+    *knob = best_v;
+  };
+  Tune& tu = c->tune;
+  pick(0, &tu.mom_cl, {2, 4, 8});
+  pick(0, &tu.mom_nt, {64, 128, 256});
+  if (c->prm.isal != 0) {
+    pick(1, &tu.sal_cl, {2, 4, 8});
+    pick(1, &tu.sal_nt, {64, 128, 256});
+  }
+  // restore the state the timing runs overwrote
+  size_t o = 0;
+  for (auto& k : keep) {
+    const cudaError_t e = dev_copy ? cudaMemcpy(k.first, dev_copy + o, k.second * sizeof(double), cudaMemcpyDeviceToDevice)
+                                   : cudaMemcpy(k.first, host_copy.data() + o, k.second * sizeof(double),
+                                                cudaMemcpyHostToDevice);
+    if (e != cudaSuccess && !rc) rc = cuda_fail(e);
+    o += k.second;
+  }
+  if (dev_copy) cudaFree(dev_copy);
+  if (rc) return rc;
+  if (choice) { choice[0] = tu.mom_cl; choice[1] = tu.mom_nt; choice[2] = tu.sal_cl; choice[3] = tu.sal_nt; }
+  return 0;
+}
+
+int si3d_gpu_set_tune(int h, const int* choice) {
+  Ctx* c = get(h);
+  if (!c || !choice) return c ? SI3D_EDIMS : SI3D_EHANDLE;
+  auto ok_cl = [](int v) { return v == 2 || v == 4 || v == 8; };
+  auto ok_nt = [](int v) { return v == 64 || v == 128 || v == 256; };
+  if (!ok_cl(choice[0]) || !ok_nt(choice[1]) || !ok_cl(choice[2]) || !ok_nt(choice[3])) return SI3D_EDIMS;
+  c->tune.mom_cl = choice[0]; c->tune.mom_nt = choice[1]; c->tune.sal_cl = choice[2]; c->tune.sal_nt = choice[3];
   return 0;
 }
 

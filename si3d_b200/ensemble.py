@@ -64,9 +64,10 @@ def write(members: Sequence[synth.Basin], root: str) -> List[str]:
 class Ensemble:
     """Members opened from run directories (host set-up + GPU state each) and one si3d_ens handle."""
 
-    def __init__(self, run_dirs: Sequence[str], *, device: int = 0, pcg_itmax: int = 2000):
+    def __init__(self, run_dirs: Sequence[str], *, device: int = 0, pcg_itmax: int = 2000, autotune: bool = False):
         from .model import GpuRun
-        self.runs = [GpuRun(d, device=device, pcg_itmax=pcg_itmax) for d in run_dirs]
+        # each member is autotuned on its own grid before the step graph captures its launch shapes
+        self.runs = [GpuRun(d, device=device, pcg_itmax=pcg_itmax, autotune=autotune) for d in run_dirs]
         self.g = native.gpu()
         hs = (C.c_int * len(self.runs))(*[r.gh for r in self.runs])
         e = C.c_int(-1)

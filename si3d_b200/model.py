@@ -21,7 +21,7 @@ class GpuRun:
 
     def __init__(self, run_dir: str, *, device: int = 0, pcg_test: int = 5, pcg_tol: float = 1e-12,
                  pcg_itmax: int = 200, srelpr: float = 2.220446049250313e-16, x0_mode: int = native.SI3D_X0_PREV,
-                 precision: int = native.SI3D_FP64):
+                 precision: int = native.SI3D_FP64, autotune: bool = False):
         self.h = native.host()
         self.g = native.gpu()
         opts = SolverOpts(pcg_test, pcg_tol, pcg_itmax, srelpr, x0_mode, precision)
@@ -39,6 +39,9 @@ class GpuRun:
         check(self.h.si3d_host_attach_gpu(self.hm, device, C.byref(gh)))
         self.gh = gh.value
         self.stats: list[StepStats] = []
+        self.tune: Optional[tuple] = None
+        if autotune:
+            self.autotune()
 
     # ------------------------------------------------------------------ stepping
     def run(self, nsteps: int) -> list[StepStats]:
@@ -101,6 +104,19 @@ class GpuRun:
             return
         a = np.ascontiguousarray(dz, dtype=np.float64)
         check(self.g.si3d_gpu_set_warmstart(self.gh, native.ptr(a), 0))
+
+    def autotune(self, reps: int = 3) -> tuple:
+        """Pick the fastest launch shapes of the column stages on the current state (which is left
+        unchanged); returns (momentum lanes, momentum threads, scalar lanes, scalar threads)."""
+        ch = np.zeros(4, dtype=np.int32)
+        check(self.g.si3d_gpu_autotune(self.gh, reps, native.ptr(ch)))
+        self.tune = tuple(int(x) for x in ch)
+        return self.tune
+
+    def set_tune(self, choice) -> None:
+        ch = np.ascontiguousarray(choice, dtype=np.int32)
+        check(self.g.si3d_gpu_set_tune(self.gh, native.ptr(ch)))
+        self.tune = tuple(int(x) for x in ch)
 
     def set_net(self, params: Optional[np.ndarray]) -> None:
         """Load the learned initial guess network (include/si3d_learn.h); None unloads it."""

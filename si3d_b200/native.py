@@ -76,6 +76,8 @@ GPU_SYMBOLS = {
     "si3d_gpu_sync": (C.c_int, [C.c_int]),
     "si3d_gpu_strerror": (C.c_char_p, [C.c_int]),
     "si3d_gpu_finalize": (None, [C.c_int]),
+    "si3d_gpu_autotune": (C.c_int, [C.c_int, C.c_int, C.c_void_p]),
+    "si3d_gpu_set_tune": (C.c_int, [C.c_int, C.c_void_p]),
     "si3d_ens_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "si3d_ens_step": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "si3d_ens_nodes": (C.c_int, [C.c_int]),

@@ -54,3 +54,31 @@ def test_graph_is_captured_once(native_libs, small_members):
         assert ens.nodes() == n1 > 0
     finally:
         ens.close()
+
+
+def test_autotune_leaves_the_state_unchanged(native_libs, run_dirs):
+    """The autotuner times candidate launch shapes on the live state and restores it: the run that
+    continues after tuning is bit-identical to one that never tuned."""
+    from si3d_b200.model import GpuRun
+    names = ("s", "uh", "vh", "sal", "agx", "ary", "Bth2", "Bth3", "eagx")
+    a = GpuRun(run_dirs["t1"], pcg_itmax=2000)
+    b = GpuRun(run_dirs["t1"], pcg_itmax=2000)
+    try:
+        a.run(3)
+        b.run(3)
+        before = {n: b.get(n).copy() for n in names}
+        choice = b.autotune(reps=2)
+        assert choice[0] in (2, 4, 8) and choice[1] in (64, 128, 256)
+        for n in names:
+            np.testing.assert_array_equal(b.get(n), before[n], err_msg=n)
+        a.run(3)
+        b.run(3)
+        for n in names:
+            np.testing.assert_array_equal(a.get(n), b.get(n), err_msg=n)
+        b.set_tune((2, 64, 4, 256))
+        a.run(2)
+        b.run(2)
+        np.testing.assert_array_equal(a.get("sal"), b.get("sal"))
+    finally:
+        a.close()
+        b.close()
