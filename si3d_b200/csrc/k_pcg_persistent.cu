@@ -100,7 +100,7 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, int* s_f
 }
 
 template <typename T>
-__global__ void __launch_bounds__(QB) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
+__global__ void __launch_bounds__(QB, 3) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
   __shared__ double sh[8 * 4 + 4];
   __shared__ int s_flag;
   const PcgColorT<T> &R = P.R, &B = P.B;
@@ -126,13 +126,15 @@ __global__ void __launch_bounds__(QB) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
     const T* __restrict__ Rp = par ? R.p2 : R.p;
     const T a = (T)alpha;
     // ---- black nodes: u += alpha p, r -= alpha q, black half of M^-1 (icfstp/icsp/icbsp)
+    // (neighbour indices are loaded one node ahead and every store follows all of a node's loads,
+    // so a node costs one memory round trip)
     double v[4] = {0, 0, 0, 0};
+    int4 q4n = (g0 < B.n) ? B.nbr[g0] : make_int4(0, 0, 0, 0);
     for (int j = g0; j < B.n; j += stride) {
-      const int4 q4 = B.nbr[j];
+      const int4 q4 = q4n;
+      if (j + stride < B.n) q4n = B.nbr[j + stride];
       const T uj = B.u[j] + a * Bp[j];
       const T rj = B.r[j] - a * B.q[j];
-      B.u[j] = uj;
-      B.r[j] = rj;
       const int ks[4] = {q4.x, q4.y, q4.z, q4.w};
       const T t[4] = {-R.sx[q4.x], -R.sy[q4.y], -B.sy[j], -B.sx[j]};
       T x = rj;
@@ -147,6 +149,8 @@ __global__ void __launch_bounds__(QB) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
       x = x * dj;
       x = x / dj;
       const T zj = x * dj;
+      B.u[j] = uj;
+      B.r[j] = rj;
       B.z[j] = zj;
       v[0] += (double)rj * (double)rj; v[1] += (double)rj * (double)zj;
       v[2] += (double)uj * (double)uj; v[3] += (double)zj * (double)zj;
@@ -163,12 +167,12 @@ __global__ void __launch_bounds__(QB) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
     if (!grid_barrier(bar, SC, &s_flag)) return;
     // ---- red nodes: u/r updates, red half of M^-1
     v[0] = v[1] = v[2] = v[3] = 0;
+    q4n = (g0 < R.n) ? R.nbr[g0] : make_int4(0, 0, 0, 0);
     for (int k = g0; k < R.n; k += stride) {
-      const int4 q4 = R.nbr[k];
+      const int4 q4 = q4n;
+      if (k + stride < R.n) q4n = R.nbr[k + stride];
       const T uk = R.u[k] + a * Rp[k];
       const T rk = R.r[k] - a * R.q[k];
-      R.u[k] = uk;
-      R.r[k] = rk;
       const T dk = R.dinv[k];
       T x = rk * dk;
       x = x / dk;
@@ -177,6 +181,8 @@ __global__ void __launch_bounds__(QB) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
       x = x - (-R.sy[k]) * B.z[q4.z];
       x = x - (-R.sx[k]) * B.z[q4.w];
       const T zk = x * dk;
+      R.u[k] = uk;
+      R.r[k] = rk;
       R.z[k] = zk;
       v[0] += (double)rk * (double)rk; v[1] += (double)rk * (double)zk;
       v[2] += (double)uk * (double)uk; v[3] += (double)zk * (double)zk;
@@ -243,8 +249,10 @@ __global__ void __launch_bounds__(QB) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
       const T* __restrict__ Cp = par ? C.p2 : C.p;
       const T* __restrict__ Op = par ? O.p2 : O.p;
       T* __restrict__ Cn = par ? C.p : C.p2;
+      int4 q4n3 = (g0 < C.n) ? C.nbr[g0] : make_int4(0, 0, 0, 0);
       for (int i = g0; i < C.n; i += stride) {
-        const int4 q4 = C.nbr[i];
+        const int4 q4 = q4n3;
+        if (i + stride < C.n) q4n3 = C.nbr[i + stride];
         const T pi = C.z[i] + bt * Cp[i];
         const T pW = O.z[q4.x] + bt * Op[q4.x];
         const T pS = O.z[q4.y] + bt * Op[q4.y];
@@ -301,12 +309,12 @@ int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, cudaStream_t st)
 
 }  // namespace
 
-int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm) {
-  int sms = 0, occ_d = 0, occ_f = 0;
+int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32) {
+  int sms = 0, occ = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_d, k_pcg_loop<double>, QB, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, k_pcg_loop<float>, QB, 0);
-  int per_sm = std::min(occ_d, occ_f);
+  if (fp32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<float>, QB, 0);
+  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<double>, QB, 0);
+  int per_sm = occ;
   if (max_per_sm > 0) per_sm = std::min(per_sm, max_per_sm);
   const int need = (std::max(nR, nB) + QB - 1) / QB;
   return std::max(1, std::min(sms * std::max(per_sm, 1), need));

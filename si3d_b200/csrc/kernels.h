@@ -64,7 +64,7 @@ void ir_correct(const PcgDev& P, const PcgDevF& F, cudaStream_t st);
 struct GridBar {
   unsigned int count, gen, abort, pad;
 };
-int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm);
+int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32);
 int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, cudaStream_t st);
 int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st);
 

@@ -87,7 +87,7 @@ struct Ctx {
   int last_iters = 8;
   // whole-solve cooperative kernel (k_pcg_persistent.cu); false -> one launch per phase
   bool persistent = true;
-  int loop_blocks = 0;
+  int loop_blocks = 0, loop_blocks_f = 0;   // FP64 / FP32 grids of the cooperative solve
   GridBar* bar = nullptr;
   bool log_solves = false;   // SI3D_LOG_SOLVES=1: per-solve iteration counts on stderr
   // instrumentation: kernel-launch count and (optionally) per-stage device time
@@ -281,12 +281,13 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
   if (rc) return rc;
   // SI3D_PCG_BLOCKS_PER_SM caps the resident blocks per SM of the cooperative solve (tuning)
   const char* bps = std::getenv("SI3D_PCG_BLOCKS_PER_SM");
-  c->loop_blocks = pcg_loop_blocks(c->device, nR, nB, bps ? std::atoi(bps) : 0);
+  c->loop_blocks = pcg_loop_blocks(c->device, nR, nB, bps ? std::atoi(bps) : 0, false);
+  c->loop_blocks_f = pcg_loop_blocks(c->device, nR, nB, bps ? std::atoi(bps) : 0, true);
   const char* pers = std::getenv("SI3D_PCG_PERSISTENT");
   c->persistent = !(pers && pers[0] == '0');
   const char* lg = std::getenv("SI3D_LOG_SOLVES");
   c->log_solves = lg && lg[0] == '1';
-  const int nblk = std::max(pcg_max_blocks(nR, nB), 3 * c->loop_blocks);
+  const int nblk = std::max(pcg_max_blocks(nR, nB), 3 * std::max(c->loop_blocks, c->loop_blocks_f));
   double* parts = nullptr;
   rc |= c->alloc(&parts, 4 * (size_t)nblk);
   rc |= c->alloc(&c->bar, 1);
@@ -471,7 +472,7 @@ int refine(Ctx* c, int* total_inner) {
     CK(cudaMemcpyAsync(c->pcgf.sc, c->h_scf, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
     int rci = iterate(c, c->pcgf.sc, c->h_scf, p.pcg_itmax, c->last_inner,
                       [&](int par) { pcg_iteration_f(c->pcgf, par, c->st); },
-                      [&] { return pcg_loop_f(c->pcgf, c->bar, c->loop_blocks, c->st); });
+                      [&] { return pcg_loop_f(c->pcgf, c->bar, c->loop_blocks_f, c->st); });
     if (rci) return rci;
     const int its = c->h_scf->in;
     if (c->log_solves) std::fprintf(stderr, "si3d: inner FP32 solve %d: %d iterations\n", outer + 1, its);
