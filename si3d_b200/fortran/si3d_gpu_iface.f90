@@ -124,6 +124,46 @@
          IMPORT :: C_INT
          INTEGER(C_INT), VALUE :: handle
       END SUBROUTINE
+
+      ! launch-shape autotuner: choice = (momentum lanes, momentum threads, scalar lanes, scalar threads)
+      INTEGER(C_INT) FUNCTION si3d_gpu_autotune(handle, reps, choice) BIND(C, NAME="si3d_gpu_autotune")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE       :: handle, reps
+         INTEGER(C_INT), INTENT(OUT) :: choice(4)
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_set_tune(handle, choice) BIND(C, NAME="si3d_gpu_set_tune")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE      :: handle
+         INTEGER(C_INT), INTENT(IN) :: choice(4)
+      END FUNCTION
+
+      ! ensembles: several handles advanced in lock step, one CUDA graph launch per step
+      INTEGER(C_INT) FUNCTION si3d_ens_create(handles, n, ens) BIND(C, NAME="si3d_ens_create")
+         IMPORT :: C_INT
+         INTEGER(C_INT), INTENT(IN)  :: handles(*)
+         INTEGER(C_INT), VALUE       :: n
+         INTEGER(C_INT), INTENT(OUT) :: ens
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_ens_step(ens, n0, nsteps, iters, ier, ms) BIND(C, NAME="si3d_ens_step")
+         IMPORT :: C_INT, C_DOUBLE
+         INTEGER(C_INT), VALUE       :: ens, n0, nsteps
+         INTEGER(C_INT), INTENT(OUT) :: iters(*), ier(*)
+         REAL(C_DOUBLE), INTENT(OUT) :: ms(*)
+      END FUNCTION
+
+      SUBROUTINE si3d_ens_destroy(ens) BIND(C, NAME="si3d_ens_destroy")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE :: ens
+      END SUBROUTINE
+
+      ! learned initial guess (include/si3d_learn.h): SI3D_NET_NPARAM FP32 parameters
+      INTEGER(C_INT) FUNCTION si3d_learn_set_params(handle, params) BIND(C, NAME="si3d_learn_set_params")
+         IMPORT :: C_INT, C_FLOAT
+         INTEGER(C_INT), VALUE     :: handle
+         REAL(C_FLOAT), INTENT(IN) :: params(*)
+      END FUNCTION
    END INTERFACE
 
 END MODULE si3d_gpu_iface

@@ -51,6 +51,7 @@ def test_fortran_interface_binds_the_same_names():
     text = open(f90[0]).read()
     bound = set(re.findall(r'BIND\(C,\s*NAME="(si3d_\w+)"\)', text, re.I))
     declared = set(_declared(os.path.join(ROOT, "include", "si3d_gpu.h")))
+    declared |= set(_declared(os.path.join(ROOT, "include", "si3d_learn.h")))
     assert bound and bound <= declared
 
 
