@@ -11,7 +11,39 @@
 
 #include "oracle.hpp"
 
+#include <cstdlib>
+#include <thread>
+#include <vector>
+
 namespace orc {
+
+// Columns l = 1..lm in contiguous static chunks on SI3D_ORACLE_THREADS threads (default 1).  Like the
+// reference's OpenMP strip partition, every column's work only writes that column, so the results
+// do not depend on the thread count.
+static int oracle_threads() {
+  static const int n = [] {
+    const char* e = std::getenv("SI3D_ORACLE_THREADS");
+    const int v = e ? std::atoi(e) : 1;
+    return v < 1 ? 1 : v;
+  }();
+  return n;
+}
+
+template <class F>
+static void par_cols(int lm, F&& body) {
+  const int nt = std::min(oracle_threads(), lm);
+  if (nt <= 1) {
+    for (int l = 1; l <= lm; ++l) body(l);
+    return;
+  }
+  std::vector<std::thread> ts;
+  ts.reserve(nt);
+  for (int t = 0; t < nt; ++t) {
+    const int a = 1 + (int)((long long)lm * t / nt), b = (int)((long long)lm * (t + 1) / nt);
+    ts.emplace_back([&body, a, b] { for (int l = a; l <= b; ++l) body(l); });
+  }
+  for (auto& th : ts) th.join();
+}
 
 namespace {
 constexpr real ZERO = 0.0, HMIN = 0.0, g = 9.806, rhoair = 1.3;
@@ -92,11 +124,11 @@ namespace {
 
 // surfbc CASE(0) (si3d_boundaryconditions.f90:4508-4514), or the per-column override.
 void surfbc(Model& m) {
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     if (m.wind_override) { m.uair(l) = m.uair_ovr[l - 1]; m.vair(l) = m.vair_ovr[l - 1]; }
     else { m.uair(l) = -m.in.wa * std::sin(pi * m.in.phi / 180.); m.vair(l) = -m.in.wa * std::cos(pi * m.in.phi / 180.); }
     m.cdw(l) = m.in.cw;
-  }
+  });
 }
 
 // Coefficients haxpp/haypp/th/th1 as computed at the top of exmom (si3d_procedures.f90:623-681
@@ -110,14 +142,14 @@ void exmom(Model& m, int ieq, ExCoef& C) {
   F3 &haxpp = C.haxpp, &haypp = C.haypp, &th = C.th, &th1 = C.th1;
   if (ieq == 1) {
     for (int k = 1; k <= km1; ++k) { haxpp(k, lm1) = 0.0; haypp(k, lm1) = 0.0; }
-    for (int l = 1; l <= m.lm; ++l) {
+    par_cols(m.lm, [&](int l) {
       int kmx = std::min(m.kmz(m.lEC(l)), m.kmz(l)), k1x = m.k1u(l);
       for (int k = 1; k <= k1x - 1 && k <= km1; ++k) { haypp(k, l) = 0; haxpp(k, l) = 0; th(k, l) = 0; th1(k, l) = 0; }
       for (int k = kmx + 1; k <= km1; ++k) { haypp(k, l) = 0; haxpp(k, l) = 0; th(k, l) = 0; th1(k, l) = 0; }
       int i = m.l2i(l), j = m.l2j(l);
       if (!m.mask2d(i + 1, j)) {
         for (int k = k1x; k <= kmx; ++k) { haypp(k, l) = 0; haxpp(k, l) = 0; th(k, l) = 0; th1(k, l) = 0; }
-        continue;
+        return;
       }
       if (p.ihd == 1)
         for (int k = k1x; k <= kmx; ++k) {
@@ -130,16 +162,16 @@ void exmom(Model& m, int ieq, ExCoef& C) {
       }
       th(k1x, l) = 0.0; th1(k1x, l) = 0.0;
       th(kmx + 1, l) = 0.5; th1(kmx + 1, l) = 0.5;
-    }
-    for (int l = 1; l <= m.lm; ++l) {
+    });
+    par_cols(m.lm, [&](int l) {
       int kmx = std::min(m.kmz(m.lEC(l)), m.kmz(l)), k1x = m.k1u(l);
       for (int k = 1; k <= k1x - 1 && k <= km1; ++k) m.ex(k, l) = 0.0;
       for (int k = kmx + 1; k <= km1; ++k) m.ex(k, l) = 0.0;
       int i = m.l2i(l), j = m.l2j(l);
-      if (!m.mask2d(i + 1, j)) { for (int k = k1x; k <= kmx; ++k) m.ex(k, l) = 0.0; continue; }
+      if (!m.mask2d(i + 1, j)) { for (int k = k1x; k <= kmx; ++k) m.ex(k, l) = 0.0; return; }
       const int lE = m.lEC(l), lW = m.lWC(l), lN = m.lNC(l), lS = m.lSC(l), lSE = m.lSC(lE);
       for (int k = k1x; k <= kmx; ++k) {
-        if (m.hp(k, l) <= ZERO || m.hp(k, lE) <= ZERO) { m.ex(k, l) = m.uhpp(k, l); continue; }
+        if (m.hp(k, l) <= ZERO || m.hp(k, lE) <= ZERO) { m.ex(k, l) = m.uhpp(k, l); return; }
         real corx = 0.25 * p.f * (m.vhp(k, lE) + m.vhp(k, l) + m.vhp(k, lSE) + m.vhp(k, lS));
         real uE = m.uhp(k, lE) + m.uhp(k, l);
         real uW = m.uhp(k, l) + m.uhp(k, lW);
@@ -161,17 +193,17 @@ void exmom(Model& m, int ieq, ExCoef& C) {
                 (haxpp(k, l) * (m.upp(k, lE) - m.upp(k, l)) - haxpp(k, lW) * (m.upp(k, l) - m.upp(k, lW))) / m.dxdx;
         m.ex(k, l) = m.uhpp(k, l) - twodt1 * (advx * p.iadv - corx - hdx);
       }
-    }
+    });
   } else {
     for (int k = 1; k <= km1; ++k) { haxpp(k, lm1) = 0.0; haypp(k, lm1) = 0.0; }
-    for (int l = 1; l <= m.lm; ++l) {
+    par_cols(m.lm, [&](int l) {
       int kmy = std::min(m.kmz(m.lNC(l)), m.kmz(l)), k1y = m.k1v(l);
       for (int k = 1; k <= k1y - 1 && k <= km1; ++k) { haypp(k, l) = 0; haxpp(k, l) = 0; th(k, l) = 0; th1(k, l) = 0; }
       for (int k = kmy + 1; k <= km1; ++k) { haypp(k, l) = 0; haxpp(k, l) = 0; th(k, l) = 0; th1(k, l) = 0; }
       int i = m.l2i(l), j = m.l2j(l);
       if (!m.mask2d(i, j + 1)) {
         for (int k = k1y; k <= kmy; ++k) { haypp(k, l) = 0; haxpp(k, l) = 0; th(k, l) = 0; th1(k, l) = 0; }
-        continue;
+        return;
       }
       if (p.ihd == 1)
         for (int k = k1y; k <= kmy; ++k) {
@@ -184,15 +216,15 @@ void exmom(Model& m, int ieq, ExCoef& C) {
       }
       th(k1y, l) = 0.0; th1(k1y, l) = 0.0;
       th(kmy + 1, l) = 0.5; th1(kmy + 1, l) = 0.5;
-    }
-    for (int l = 1; l <= m.lm; ++l) {
+    });
+    par_cols(m.lm, [&](int l) {
       for (int k = 1; k <= km1; ++k) m.ex(k, l) = 0.0;
       int i = m.l2i(l), j = m.l2j(l);
-      if (!m.mask2d(i, j + 1)) continue;
+      if (!m.mask2d(i, j + 1)) return;
       int kmy = std::min(m.kmz(m.lNC(l)), m.kmz(l)), k1y = m.k1v(l);
       const int lE = m.lEC(l), lW = m.lWC(l), lN = m.lNC(l), lS = m.lSC(l), lNW = m.lWC(lN);
       for (int k = k1y; k <= kmy; ++k) {
-        if (m.hp(k, l) <= ZERO || m.hp(k, lN) <= ZERO) { m.ex(k, l) = m.vhpp(k, l); continue; }
+        if (m.hp(k, l) <= ZERO || m.hp(k, lN) <= ZERO) { m.ex(k, l) = m.vhpp(k, l); return; }
         real cory = 0.25 * p.f * (m.uhp(k, lN) + m.uhp(k, l) + m.uhp(k, lNW) + m.uhp(k, lW));
         real uE = m.uhp(k, lN) + m.uhp(k, l);
         real uW = m.uhp(k, lNW) + m.uhp(k, lW);
@@ -214,7 +246,7 @@ void exmom(Model& m, int ieq, ExCoef& C) {
                 (haxpp(k, l) * (m.vpp(k, lE) - m.vpp(k, l)) - haxpp(k, lW) * (m.vpp(k, l) - m.vpp(k, lW))) / m.dxdx;
         m.ex(k, l) = m.vhpp(k, l) - twodt1 * (advy * p.iadv + cory - hdy);
       }
-    }
+    });
   }
 }
 
@@ -264,22 +296,25 @@ void bclnc_km(Model& m, int l, int kb, int ieq, real& huvpdrho) {
 void matmom(Model& m, int ieq) {
   const int km1 = m.km1;
   const real twodt1 = m.twodt * m.tz, tz = m.tz, theta = m.in.theta;
-  std::vector<real> Avx(km1 + 2), rhopx(km1 + 2), hupdrho(km1 + 2), bclncx(km1 + 2), vdiffx(km1 + 2),
-      Avxdudz(km1 + 2), deltaz(km1 + 2), hh(km1 + 1), gg(km1 + 1), ag(km1 + 1), ar(km1 + 1), aa(3 * (km1 + 1));
-  auto AA = [&](int r, int k) -> real& { return aa[3 * (k - 1) + (r - 1)]; };
   const bool X = ieq == 1;
   F3 &huv = X ? m.hup : m.hvp;
   F3 &uvpp = X ? m.upp : m.vpp;
   F3 &agA = X ? m.agx : m.agy, &arA = X ? m.arx : m.ary;
   F1 &eag = X ? m.eagx : m.eagy, &ear = X ? m.earx : m.eary;
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
+    // per-thread column scratch (every entry a column reads is written for that column first)
+    thread_local std::vector<real> Avx, rhopx, hupdrho, bclncx, vdiffx, Avxdudz, deltaz, hh, gg, ag, ar, aa;
+    for (auto* v : {&Avx, &rhopx, &hupdrho, &bclncx, &vdiffx, &Avxdudz, &deltaz}) v->resize(km1 + 2);
+    for (auto* v : {&hh, &gg, &ag, &ar}) v->resize(km1 + 1);
+    aa.resize(3 * (km1 + 1));
+    auto AA = [&](int r, int k) -> real& { return aa[3 * (k - 1) + (r - 1)]; };
     int i = m.l2i(l), j = m.l2j(l);
-    if (X ? !m.mask2d(i + 1, j) : !m.mask2d(i, j + 1)) continue;   // id_columnCE / id_columnCN
+    if (X ? !m.mask2d(i + 1, j) : !m.mask2d(i, j + 1)) return;   // id_columnCE / id_columnCN
     const int lO = X ? m.lEC(l) : m.lNC(l);                         // the other side of the face
     int kmx = std::min(m.kmz(lO), m.kmz(l));
     int k1x = X ? m.k1u(l) : m.k1v(l);
     int nwlayers = (kmx - k1x) + 1;
-    if (nwlayers < 1) continue;
+    if (nwlayers < 1) return;
     std::fill(Avx.begin(), Avx.end(), 0.0);
     // x: k1x+1..kmx (:1269-1271); y: k1y..kmy (:1461-1463) — Avy(k1y) is never used.
     for (int k = (X ? k1x + 1 : k1x); k <= kmx; ++k) Avx[k] = 0.5 * (m.Av(k, lO) + m.Av(k, l));
@@ -364,7 +399,7 @@ void matmom(Model& m, int ieq) {
     for (int k = k1x; k <= kmx; ++k) se += ag[k];
     for (int k = k1x; k <= kmx; ++k) sr += ar[k];
     eag(l) = se; ear(l) = sr;
-  }
+  });
 }
 
 // matcon (si3d_procedures.f90:1749-1867)
@@ -374,15 +409,15 @@ void matcon(Model& m) {
              dt1 = m.dt * tz, rho4sx = 1000., rho4sy = 1000.;
   const int lm1 = m.lm1;
   m.sx(lm1) = 0.0; m.sy(lm1) = 0.0;
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int i = m.l2i(l), j = m.l2j(l);
     m.sx(l) = m.mask2d(i + 1, j) ? cx * rho4sx * m.earx(l) : 0.0;
-  }
-  for (int l = 1; l <= m.lm; ++l) {
+  });
+  par_cols(m.lm, [&](int l) {
     int i = m.l2i(l), j = m.l2j(l);
     m.sy(l) = m.mask2d(i, j + 1) ? cy * rho4sy * m.eary(l) : 0.0;
-  }
-  for (int l = 1; l <= m.lm; ++l) {
+  });
+  par_cols(m.lm, [&](int l) {
     int k1s = m.k1, kms = m.kmz(l);
     const int lW = m.lWC(l), lS = m.lSC(l);
     real sum = 0;
@@ -392,14 +427,14 @@ void matcon(Model& m) {
     // Beagx(lWCH(l)) with lWCH = Bend+1 -> lm1 (Beagx(Bend+1) = 0 from InitThreads and never written)
     m.qq(l) = m.spp(l) - dtdx1 * (m.eagx(l) - m.eagx(lW)) - dtdy1 * (m.eagy(l) - m.eagy(lS)) - m.dd(l);
     m.rr(l) = 1 + m.sx(l) + m.sx(lW) + m.sy(l) + m.sy(lS);
-  }
+  });
 }
 
 // slayer_h (si3d_procedures.f90:2070-2175)
 void slayer_h(Model& m) {
   const int km1 = m.km1, lm1 = m.lm1;
   for (int k = 1; k <= km1; ++k) { m.h(k, lm1) = m.hp(k, lm1); m.hu(k, lm1) = m.hup(k, lm1); m.hv(k, lm1) = m.hvp(k, lm1); }
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     const int kz = m.k1z(l), ku = m.k1u(l), kv = m.k1v(l);
     for (int k = 1; k <= kz - 1; ++k) m.h(k, l) = m.hp(k, l);
     for (int k = 1; k <= ku - 1; ++k) m.hu(k, l) = m.hup(k, l);
@@ -441,7 +476,7 @@ void slayer_h(Model& m) {
     } else {
       for (int kk = kv; kk <= kv + 1 && kk <= km1; ++kk) m.hv(kk, l) = m.hvp(kk, l);
     }
-  }
+  });
 }
 
 // SolverSparse (si3d_procedures.f90:1870-2065): ELLPACK assembly, NSPCG mic1+cg, s = zeta, slayer_h.
@@ -478,9 +513,9 @@ bool solver_sparse(Model& m) {
 // continuity (si3d_procedures.f90:2635-2824), cases 1 and 2 (no point sources).
 void continuity(Model& m, int ist) {
   const int km1 = m.km1;
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int kms = m.kmz(l), k1s = m.k1z(l);
-    if (k1s > kms) continue;
+    if (k1s > kms) return;
     const int lW = m.lWC(l), lS = m.lSC(l);
     for (int k = 1; k <= km1; ++k) m.wp(k, l) = 0.0;
     if (ist == 1) {
@@ -496,35 +531,35 @@ void continuity(Model& m, int ist) {
       for (int k = m.k1; k <= k1s - 1; ++k)
         m.wp(k1s, l) = m.wp(k1s, l) - (m.uhp(k, l) - m.uhp(k, lW)) / m.dx - (m.vhp(k, l) - m.vhp(k, lS)) / m.dy;
     }
-  }
+  });
 }
 
 // vel (si3d_procedures.f90:2430-2567)
 void vel(Model& m) {
   const real gthx1 = m.gdtdx * m.tz, gthy1 = m.gdtdy * m.tz, rho4cxx = 1000., rho4cyy = 1000.;
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int i = m.l2i(l), j = m.l2j(l);
-    if (!m.mask2d(i + 1, j)) continue;
+    if (!m.mask2d(i + 1, j)) return;
     int kmx = std::min(m.kmz(m.lEC(l)), m.kmz(l)), k0x = m.k1u(l);
     real cxx = gthx1 * rho4cxx * (m.s(m.lEC(l)) - m.s(l));
     for (int k = k0x; k <= kmx; ++k) m.uh(k, l) = m.agx(k, l) - cxx * m.arx(k, l);
     int k = k0x;
     if (m.hu(k, l) <= ZERO) { m.uh(k + 1, l) = m.uh(k, l) + m.uh(k + 1, l); m.uh(k, l) = 0.0; m.k1u(l) = k0x + 1; }
-  }
-  for (int l = 1; l <= m.lm; ++l) {
+  });
+  par_cols(m.lm, [&](int l) {
     int i = m.l2i(l), j = m.l2j(l);
-    if (!m.mask2d(i, j + 1)) continue;
+    if (!m.mask2d(i, j + 1)) return;
     int kmy = std::min(m.kmz(m.lNC(l)), m.kmz(l)), k0y = m.k1v(l);
     real cyy = gthy1 * rho4cyy * (m.s(m.lNC(l)) - m.s(l));
     for (int k = k0y; k <= kmy; ++k) m.vh(k, l) = m.agy(k, l) - cyy * m.ary(k, l);
     int k = k0y;
     if (m.hv(k, l) <= ZERO) { m.vh(k + 1, l) = m.vh(k, l) + m.vh(k + 1, l); m.vh(k, l) = 0.0; m.k1v(l) = k0y + 1; }
-  }
+  });
   continuity(m, 1);
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int k0s = m.k1z(l);
     if (m.h(k0s, l) <= ZERO) m.k1z(l) = std::min(k0s + 1, m.km1);
-  }
+  });
 }
 
 // exsal (si3d_procedures.f90:2827-3076): Superbee flux-limited advection (itrsca ignored).
@@ -533,12 +568,12 @@ void exsal(Model& m) {
   const real twodt1 = m.twodt * m.tz;
   const Inp& p = m.in;
   for (int k = 1; k <= km1; ++k) { m.Bhaxpp(k, lm1) = 0.0; m.Bhaypp(k, lm1) = 0.0; }
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int kms = m.kmz(l);
     for (int k = 1; k <= m.k1 - 1; ++k) { m.Bhaxpp(k, l) = 0.0; m.Bhaypp(k, l) = 0.0; }
     for (int k = kms + 1; k <= km1; ++k) { m.Bhaxpp(k, l) = 0.0; m.Bhaypp(k, l) = 0.0; }
     for (int k = m.k1; k <= kms; ++k) { m.Bhaxpp(k, l) = p.Ax0 * m.hupp(k, l); m.Bhaypp(k, l) = p.Ay0 * m.hvpp(k, l); }
-  }
+  });
   for (int k = 1; k <= km1; ++k) { m.Bth3(k, lm1) = 0; m.Bex(k, lm1) = 0.0; m.Bth4(k, lm1) = 0.0; m.Bth2(k, lm1) = 0.0; }
   auto limiter = [](real ss1, real ss2, real ss3, real ss4, real vel, real cf0) {
     real C_f = cf0;
@@ -550,7 +585,7 @@ void exsal(Model& m) {
     }
     return C_f;
   };
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int kms = m.kmz(l), k1s = m.k1z(l);
     const int lE = m.lEC(l), lW = m.lWC(l);
     for (int k = k1s; k <= kms; ++k) {
@@ -564,8 +599,8 @@ void exsal(Model& m) {
         m.Bth2(k, l) = vel / 2. * (ss3 + ss2) - ((1. - C_f) * std::fabs(vel) + vel * vel * twodt1 / m.dx * C_f) * (ss3 - ss2) / 2.;
       } else m.Bth2(k, l) = 0.0;
     }
-  }
-  for (int l = 1; l <= m.lm; ++l) {
+  });
+  par_cols(m.lm, [&](int l) {
     int kms = m.kmz(l), k1s = m.k1z(l);
     const int lN = m.lNC(l), lS = m.lSC(l);
     for (int k = k1s; k <= kms; ++k) {
@@ -588,8 +623,8 @@ void exsal(Model& m) {
         m.Bth3(k, l) = vel / 2. * (ss3 + ss2) - ((1. - C_f) * std::fabs(vel) + vel * vel * twodt1 / delz * C_f) * (ss3 - ss2) / 2.;
       } else m.Bth3(k, l) = 0.0;
     }
-  }
-  for (int l = 1; l <= m.lm; ++l) {
+  });
+  par_cols(m.lm, [&](int l) {
     int kms = m.kmz(l), k1s = m.k1z(l);
     const int lE = m.lEC(l), lW = m.lWC(l), lN = m.lNC(l), lS = m.lSC(l);
     for (int k = 1; k <= k1s - 1; ++k) m.Bex(k, l) = 0.0;
@@ -601,16 +636,18 @@ void exsal(Model& m) {
                     (m.Bth4(k, l) - m.Bth4(k, lS)) / m.dy - (m.Bth3(k, l) - m.Bth3(k + 1, l));
       if (p.ihd > 0) m.Bex(k, l) = m.Bex(k, l) + hd;
     }
-  }
+  });
 }
 
 // imsal (si3d_procedures.f90:3079-3207) + trid1
 void imsal(Model& m) {
   const int km1 = m.km1;
   const real twodt1 = m.twodt * m.tz;
-  std::vector<real> hn(km1 + 2), aa(3 * (km1 + 1)), dsal(km1 + 1), sal1(km1 + 1);
-  auto AA = [&](int r, int k) -> real& { return aa[3 * (k - 1) + (r - 1)]; };
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
+    // per-thread column scratch (every entry a column reads is written for that column first)
+    thread_local std::vector<real> hn, aa, dsal, sal1;
+    hn.resize(km1 + 2); aa.resize(3 * (km1 + 1)); dsal.resize(km1 + 1); sal1.resize(km1 + 1);
+    auto AA = [&](int r, int k) -> real& { return aa[3 * (k - 1) + (r - 1)]; };
     int kms = m.kmz(l), k1s = m.k1z(l), nwlayers = kms - k1s + 1;
     for (int k = k1s + 1; k <= kms; ++k) hn[k] = m.h(k, l);
     hn[k1s] = twodt1 * m.wp(k1s, l) + m.hpp(k1s, l);
@@ -632,12 +669,12 @@ void imsal(Model& m) {
       for (int k = m.k1; k <= k1s - 1; ++k) m.sal(k, l) = sal1[1];
       m.sal(kms + 1, l) = m.sal(kms, l);
     }
-  }
+  });
 }
 
 // layer_h (si3d_procedures.f90:2181-2231)
 void layer_h(Model& m) {
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int kms = m.kmz(l);
     for (int k = m.k1; k <= kms; ++k) {
       m.h(k, l) = std::min(m.zl(k + 1), m.hhs(l)) - std::max(m.zl(k), -m.s(l));
@@ -658,12 +695,12 @@ void layer_h(Model& m) {
         if (m.hv(k, l) <= HMIN) m.hv(k, l) = ZERO;
       }
     }
-  }
+  });
 }
 
 // layer_hp2 (si3d_procedures.f90:2238-2292)
 void layer_hp2(Model& m) {
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int i = m.l2i(l), j = m.l2j(l), kms = m.kmz(l);
     for (int k = m.k1; k <= kms; ++k) {
       m.hp(k, l) = std::min(m.zl(k + 1), m.hhs(l)) - std::max(m.zl(k), -m.sp(l));
@@ -683,12 +720,12 @@ void layer_hp2(Model& m) {
         if (m.hvp(k, l) <= HMIN) m.hvp(k, l) = ZERO;
       }
     }
-  }
+  });
 }
 
 // TopLayerIndexp2 (si3d_procedures.f90:2368-2427)
 void top_layer_index_p2(Model& m) {
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     m.k1z(l) = m.km1; m.k1u(l) = m.km1; m.k1v(l) = m.km1;
     int i = m.l2i(l), j = m.l2j(l), kms = m.kmz(l);
     for (int k = m.k1; k <= kms; ++k) if (m.hp(k, l) > ZERO) { m.k1z(l) = k; break; }
@@ -700,13 +737,13 @@ void top_layer_index_p2(Model& m) {
       int kmy = std::min(m.kmz(l), m.kmz(m.lNC(l)));
       for (int k = m.k1; k <= kmy; ++k) if (m.hvp(k, l) > ZERO) { m.k1v(l) = k; break; }
     }
-  }
+  });
 }
 
 // vel2 (si3d_procedures.f90:2570-2631)
 void vel2(Model& m) {
   layer_h(m);
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int i = m.l2i(l), j = m.l2j(l);
     if (m.mask2d(i + 1, j)) {
       int k = m.k1u(l);
@@ -724,7 +761,7 @@ void vel2(Model& m) {
         m.vh(k - 1, l) = vvtemp * m.hv(k - 1, l);
       }
     }
-  }
+  });
 }
 
 real zmid(const Model& m, int k, int l) {
@@ -734,7 +771,7 @@ real zmid(const Model& m, int k, int l) {
 // Velocity averaging to n+1/2 shared by settrap (:3481-3543) and settrap2 (:4011-4079);
 // settrap additionally rotates uhpp/upp first.
 void half_level_velocities(Model& m, bool rotate) {
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int i = m.l2i(l), j = m.l2j(l);
     if (m.mask2d(i + 1, j)) {
       int kmx = std::min(m.kmz(l), m.kmz(m.lEC(l)));
@@ -758,7 +795,7 @@ void half_level_velocities(Model& m, bool rotate) {
       if (m.hv(k - 1, l) > ZERO) { m.vhp(k, l) = m.vhp(k, l) + m.vh(k - 1, l) / 2.; m.vp(k, l) = m.vhp(k, l) / m.hvp(k, l); }
       if (m.hvpp(k - 1, l) > ZERO) { m.vhp(k, l) = m.vhp(k, l) + m.vhpp(k - 1, l) / 2.; m.vp(k, l) = m.vhp(k, l) / m.hvp(k, l); }
     }
-  }
+  });
 }
 
 // settrap (si3d_procedures.f90:3418-3618)
@@ -766,14 +803,14 @@ void settrap(Model& m) {
   const int km1 = m.km1, lm1 = m.lm1;
   m.spp(lm1) = m.sp(lm1);
   for (int k = 1; k <= km1; ++k) { m.hpp(k, lm1) = m.hp(k, lm1); m.hupp(k, lm1) = m.hup(k, lm1); m.hvpp(k, lm1) = m.hvp(k, lm1); }
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     m.spp(l) = m.sp(l);
     m.sp(l) = 0.5 * (m.s(l) + m.spp(l));
     for (int k = 1; k <= km1; ++k) { m.hpp(k, l) = m.hp(k, l); m.hupp(k, l) = m.hup(k, l); m.hvpp(k, l) = m.hvp(k, l); }
-  }
+  });
   layer_hp2(m);
   top_layer_index_p2(m);
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int kms = m.kmz(l);
     for (int k = m.k1; k <= kms; ++k) {
       real z = zmid(m, k, l);
@@ -781,7 +818,7 @@ void settrap(Model& m) {
       m.salp(k, l) = (m.sal(k, l) + m.salpp(k, l)) / 2.;
       m.rhop(k, l) = densty_s(m.salp(k, l), 0.00004, z) - 1000.;
     }
-  }
+  });
   half_level_velocities(m, true);
   continuity(m, 2);
 }
@@ -793,14 +830,14 @@ void settrap2(Model& m) {
   for (int l = 1; l <= m.lm; ++l) m.sp(l) = 0.5 * (m.s(l) + m.spp(l));
   layer_hp2(m);
   top_layer_index_p2(m);
-  for (int l = 1; l <= m.lm; ++l) {
+  par_cols(m.lm, [&](int l) {
     int kms = m.kmz(l);
     for (int k = m.k1; k <= kms; ++k) {
       real z = zmid(m, k, l);
       m.salp(k, l) = (m.sal(k, l) + m.salpp(k, l)) / 2.;
       m.rhop(k, l) = densty_s(m.salp(k, l), 0.00004, z) - 1000.;
     }
-  }
+  });
   half_level_velocities(m, false);
   continuity(m, 2);
 }
@@ -811,12 +848,12 @@ void save(Model& m, int istep) {
   if (istep == 2) {
     m.sp(lm1) = m.s(lm1);
     for (int k = 1; k <= km1; ++k) { m.hp(k, lm1) = m.h(k, lm1); m.hup(k, lm1) = m.hu(k, lm1); m.hvp(k, lm1) = m.hv(k, lm1); }
-    for (int l = 1; l <= m.lm; ++l) {
+    par_cols(m.lm, [&](int l) {
       m.sp(l) = m.s(l);
       for (int k = 1; k <= km1; ++k) { m.hp(k, l) = m.h(k, l); m.hup(k, l) = m.hu(k, l); m.hvp(k, l) = m.hv(k, l); }
-    }
+    });
     top_layer_index_p2(m);
-    for (int l = 1; l <= m.lm; ++l) {
+    par_cols(m.lm, [&](int l) {
       for (int k = m.k1; k <= m.km; ++k) {
         real z = zmid(m, k, l);
         m.salp(k, l) = m.sal(k, l);
@@ -830,7 +867,7 @@ void save(Model& m, int istep) {
         if (m.hvp(k, l) > ZERO) { m.vhp(k, l) = m.vh(k, l); m.vp(k, l) = m.vhp(k, l) / m.hvp(k, l); m.v(k, l) = m.vp(k, l); }
         else { m.vhp(k, l) = 0.0; m.vp(k, l) = 0.0; m.v(k, l) = 0.0; }
       }
-    }
+    });
     continuity(m, 2);
   } else {
     m.sp(lm1) = m.s(lm1);
@@ -838,15 +875,15 @@ void save(Model& m, int istep) {
       m.hp(k, lm1) = m.h(k, lm1); m.hup(k, lm1) = m.hu(k, lm1); m.hvp(k, lm1) = m.hv(k, lm1);
       m.hpp(k, lm1) = m.hp(k, lm1); m.hupp(k, lm1) = m.hup(k, lm1); m.hvpp(k, lm1) = m.hvp(k, lm1);
     }
-    for (int l = 1; l <= m.lm; ++l) {
+    par_cols(m.lm, [&](int l) {
       m.spp(l) = m.sp(l); m.sp(l) = m.s(l);
       for (int k = 1; k <= km1; ++k) {
         m.hpp(k, l) = m.hp(k, l); m.hupp(k, l) = m.hup(k, l); m.hvpp(k, l) = m.hvp(k, l);
         m.hp(k, l) = m.h(k, l); m.hup(k, l) = m.hu(k, l); m.hvp(k, l) = m.hv(k, l);
       }
-    }
+    });
     top_layer_index_p2(m);
-    for (int l = 1; l <= m.lm; ++l) {
+    par_cols(m.lm, [&](int l) {
       for (int k = m.k1; k <= m.km; ++k) {
         real z = zmid(m, k, l);
         m.salpp(k, l) = m.salp(k, l);
@@ -864,7 +901,7 @@ void save(Model& m, int istep) {
         if (m.hvp(k, l) > ZERO) { m.vhp(k, l) = m.vh(k, l); m.vp(k, l) = m.vhp(k, l) / m.hvp(k, l); m.v(k, l) = m.vp(k, l); }
         else { m.vhp(k, l) = 0.0; m.vp(k, l) = 0.0; m.v(k, l) = 0.0; }
       }
-    }
+    });
     continuity(m, 2);
   }
 }

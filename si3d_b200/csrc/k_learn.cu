@@ -423,11 +423,18 @@ __global__ void k_feat_resid(Dev d, double* __restrict__ r0, double* __restrict_
   if (threadIdx.x == 0) part[blockIdx.x] = sh[0];
 }
 
+// One block of 256 threads: strided partial sums, then a tree in shared memory (fixed order).
 __global__ void k_feat_sigma(const double* __restrict__ part, int nblk, int lm, double* __restrict__ sigma) {
-  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  __shared__ double sh[256];
   double s = 0.0;
-  for (int b = 0; b < nblk; ++b) s += part[b];
-  sigma[0] = lm > 0 ? sqrt(s / lm) : 0.0;
+  for (int b = threadIdx.x; b < nblk; b += 256) s += part[b];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) sigma[0] = lm > 0 ? sqrt(sh[0] / lm) : 0.0;
 }
 
 __global__ void k_feat_write(Dev d, const int* __restrict__ pix, const double* __restrict__ r0,
@@ -562,7 +569,7 @@ void backward(const Workspace& ws, const float* feat, const float* gout, int B, 
 void features(const Dev& d, const int* pix, double* r0, double* part, double* sigma, float* feat, cudaStream_t st) {
   const int nb = (d.g.lm + 255) / 256;
   k_feat_resid<<<nb, 256, 0, st>>>(d, r0, part);
-  k_feat_sigma<<<1, 32, 0, st>>>(part, nb, d.g.lm, sigma);
+  k_feat_sigma<<<1, 256, 0, st>>>(part, nb, d.g.lm, sigma);
   k_feat_write<<<nb, 256, 0, st>>>(d, pix, r0, sigma, feat);
 }
 

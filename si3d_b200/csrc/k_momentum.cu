@@ -57,7 +57,7 @@ __device__ __forceinline__ FaceCol face_col(const Dev& d, int l) {
 
 // ------------------------------------------------------------------ cell kernel
 template <int IEQ, int CL>
-__global__ void __launch_bounds__(CW * CL, 768 / (CW * CL)) k_mom_cells(Dev d, const int* __restrict__ cols, int ncols) {
+__global__ void __launch_bounds__(CW * CL, 1024 / (CW * CL)) k_mom_cells(Dev d, const int* __restrict__ cols, int ncols) {
   const int t = blockIdx.x * CW + threadIdx.x;
   if (t >= ncols) return;
   const Grid& g = d.g;
@@ -178,7 +178,7 @@ __global__ void __launch_bounds__(CW * CL, 768 / (CW * CL)) k_mom_cells(Dev d, c
 
 // ------------------------------------------------------------------ column kernel
 template <int IEQ, int NT>
-__global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const int* __restrict__ cols, int ncols) {
+__global__ void __launch_bounds__(NT, 1024 / NT) k_mom_columns(Dev d, const int* __restrict__ cols, int ncols) {
   const int t = blockIdx.x * NT + threadIdx.x;
   if (t >= ncols) return;
   const bool X = (IEQ == 1);

@@ -35,56 +35,6 @@ __device__ __forceinline__ int vlim(const Dev& d, int l) {
   return nwet(d, l) ? min(NB(d.g.kmz, l), NB(d.g.kmz, NB(d.g.lNC, l))) : 0;
 }
 
-// layer_hp2 for column l (the version that recomputes hp/hup/hvp from sp)
-__device__ void layer_hp2_col(const Dev& d, int l) {
-  const int kms = NB(d.g.kmz, l);
-  const double spl = d.s.sp[l - 1];
-  const double hhs = d.g.hhs[l - 1];
-  for (int k = d.g.k1; k <= kms; ++k) {
-    double v = fmin(zl(d, k + 1), hhs) - fmax(zl(d, k), -spl);
-    if (v <= HMIN) v = ZERO;
-    d.f.hp[IX(d, k, l)] = v;
-  }
-  if (ewet(d, l)) {
-    const int lE = NB(d.g.lEC, l);
-    const int kmx = min(kms, NB(d.g.kmz, lE));
-    const double sm = fmax(spl, d.s.sp[lE - 1]);
-    const double hhu = d.g.hhu[l - 1];
-    for (int k = d.g.k1; k <= kmx; ++k) {
-      double v = fmin(zl(d, k + 1), hhu) - fmax(zl(d, k), -sm);
-      if (v <= HMIN) v = ZERO;
-      d.f.hup[IX(d, k, l)] = v;
-    }
-  }
-  if (nwet(d, l)) {
-    const int lN = NB(d.g.lNC, l);
-    const int kmy = min(kms, NB(d.g.kmz, lN));
-    const double sm = fmax(spl, d.s.sp[lN - 1]);
-    const double hhv = d.g.hhv[l - 1];
-    for (int k = d.g.k1; k <= kmy; ++k) {
-      double v = fmin(zl(d, k + 1), hhv) - fmax(zl(d, k), -sm);
-      if (v <= HMIN) v = ZERO;
-      d.f.hvp[IX(d, k, l)] = v;
-    }
-  }
-}
-
-// TopLayerIndexp2 for column l
-__device__ void top_index_col(const Dev& d, int l) {
-  const int km1 = d.g.km1, kms = NB(d.g.kmz, l);
-  int kz = km1, ku = km1, kv = km1;
-  for (int k = d.g.k1; k <= kms; ++k) if (d.f.hp[IX(d, k, l)] > ZERO) { kz = k; break; }
-  if (ewet(d, l)) {
-    const int kmx = min(kms, NB(d.g.kmz, NB(d.g.lEC, l)));
-    for (int k = d.g.k1; k <= kmx; ++k) if (d.f.hup[IX(d, k, l)] > ZERO) { ku = k; break; }
-  }
-  if (nwet(d, l)) {
-    const int kmy = min(kms, NB(d.g.kmz, NB(d.g.lNC, l)));
-    for (int k = d.g.k1; k <= kmy; ++k) if (d.f.hvp[IX(d, k, l)] > ZERO) { kv = k; break; }
-  }
-  d.s.k1z[l - 1] = kz; d.s.k1u[l - 1] = ku; d.s.k1v[l - 1] = kv;
-}
-
 // ------------------------------------------------------------- slayer_h
 __global__ void k_slayer_h(Dev d) {
   const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
@@ -174,18 +124,23 @@ __global__ void k_cont1(Dev d) {
   const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
   const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l);
   if (k1s <= kms) {
-    double* wp = d.f.wp;
+    double* __restrict__ wp = d.f.wp;
+    const double* __restrict__ uh = d.f.uh;
+    const double* __restrict__ vh = d.f.vh;
+    const double* __restrict__ uhpp = d.f.uhpp;
+    const double* __restrict__ vhpp = d.f.vhpp;
     for (int k = 1; k < k1s; ++k) wp[IX(d, k, l)] = 0.0;   // wp below kms is never non-zero
     double w = 0.0;
+#pragma unroll 4
     for (int k = kms; k >= k1s; --k) {
-      w = w - (d.f.uh[IX(d, k, l)] - d.f.uh[IX(d, k, lW)] + d.f.uhpp[IX(d, k, l)] - d.f.uhpp[IX(d, k, lW)]) / d.p.twodx -
-          (d.f.vh[IX(d, k, l)] - d.f.vh[IX(d, k, lS)] + d.f.vhpp[IX(d, k, l)] - d.f.vhpp[IX(d, k, lS)]) / d.p.twody;
+      w = w - (uh[IX(d, k, l)] - uh[IX(d, k, lW)] + uhpp[IX(d, k, l)] - uhpp[IX(d, k, lW)]) / d.p.twodx -
+          (vh[IX(d, k, l)] - vh[IX(d, k, lS)] + vhpp[IX(d, k, l)] - vhpp[IX(d, k, lS)]) / d.p.twody;
       wp[IX(d, k, l)] = w;
     }
     double ws = wp[IX(d, k1s, l)];
     for (int k = d.g.k1; k <= k1s - 1; ++k)
-      ws = ws - (d.f.uh[IX(d, k, l)] - d.f.uh[IX(d, k, lW)] + d.f.uhpp[IX(d, k, l)] - d.f.uhpp[IX(d, k, lW)]) / d.p.twodx -
-           (d.f.vh[IX(d, k, l)] - d.f.vh[IX(d, k, lS)] + d.f.vhpp[IX(d, k, l)] - d.f.vhpp[IX(d, k, lS)]) / d.p.twody;
+      ws = ws - (uh[IX(d, k, l)] - uh[IX(d, k, lW)] + uhpp[IX(d, k, l)] - uhpp[IX(d, k, lW)]) / d.p.twodx -
+           (vh[IX(d, k, l)] - vh[IX(d, k, lS)] + vhpp[IX(d, k, l)] - vhpp[IX(d, k, lS)]) / d.p.twody;
     wp[IX(d, k1s, l)] = ws;
   }
   if (d.f.h[IX(d, k1s, l)] <= ZERO) d.s.k1z[l - 1] = min(k1s + 1, d.g.km1);
@@ -198,16 +153,19 @@ __global__ void k_cont2(Dev d) {
   const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
   if (k1s > kms) return;
   const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l);
-  double* wp = d.f.wp;
+  double* __restrict__ wp = d.f.wp;
+  const double* __restrict__ uhp = d.f.uhp;
+  const double* __restrict__ vhp = d.f.vhp;
   for (int k = 1; k < k1s; ++k) wp[IX(d, k, l)] = 0.0;   // wp below kms is never non-zero
   double w = 0.0;
+#pragma unroll 4
   for (int k = kms; k >= k1s; --k) {
-    w = w - (d.f.uhp[IX(d, k, l)] - d.f.uhp[IX(d, k, lW)]) / d.p.dx - (d.f.vhp[IX(d, k, l)] - d.f.vhp[IX(d, k, lS)]) / d.p.dy;
+    w = w - (uhp[IX(d, k, l)] - uhp[IX(d, k, lW)]) / d.p.dx - (vhp[IX(d, k, l)] - vhp[IX(d, k, lS)]) / d.p.dy;
     wp[IX(d, k, l)] = w;
   }
   double ws = wp[IX(d, k1s, l)];
   for (int k = d.g.k1; k <= k1s - 1; ++k)
-    ws = ws - (d.f.uhp[IX(d, k, l)] - d.f.uhp[IX(d, k, lW)]) / d.p.dx - (d.f.vhp[IX(d, k, l)] - d.f.vhp[IX(d, k, lS)]) / d.p.dy;
+    ws = ws - (uhp[IX(d, k, l)] - uhp[IX(d, k, lW)]) / d.p.dx - (vhp[IX(d, k, l)] - vhp[IX(d, k, lS)]) / d.p.dy;
   wp[IX(d, k1s, l)] = ws;
 }
 
@@ -445,17 +403,100 @@ __global__ void k_half_zeta(Dev d, int rotate) {
   d.s.sp[l - 1] = 0.5 * (d.s.s[l - 1] + d.s.spp[l - 1]);
 }
 
-// velocity averaging to n+1/2 with the wet/dry surface corrections (:3481-3543, :4011-4079)
-__device__ void half_velocities(const Dev& d, int l, bool rotate) {
-  if (ewet(d, l)) {
-    const int kmx = min(NB(d.g.kmz, l), NB(d.g.kmz, NB(d.g.lEC, l)));
-    for (int k = d.g.k1; k <= kmx; ++k) {
-      const int ik = IX(d, k, l);
-      if (rotate) { d.f.uhpp[ik] = d.f.uhp[ik]; d.f.upp[ik] = d.f.up[ik]; }
-      const double hup = d.f.hup[ik];
-      if (hup > ZERO) { const double v = 0.5 * (d.f.uh[ik] + d.f.uhpp[ik]); d.f.uhp[ik] = v; d.f.up[ik] = v / hup; }
-      else { d.f.uhp[ik] = 0.0; d.f.up[ik] = 0.0; }
+// settrap / settrap2 body after the zeta update (layer_hp2, TopLayerIndexp2, scalars at n+1/2 with
+// densty_s, velocities at n+1/2), cell-parallel: block = 32 columns x CLN layer lanes.  The first wet
+// layer of each column (TopLayerIndexp2) is the minimum over the lanes, reduced in shared memory;
+// the surface corrections at the new k1u/k1v run after a block barrier, once every layer's average
+// is in place.
+template <int CLN>
+__global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
+  __shared__ int s_first[3][CLN][32];
+  const int cx = threadIdx.x, ty = threadIdx.y;
+  const int l = blockIdx.x * 32 + cx + 1;
+  const bool act = l <= d.g.lm;
+  const int k1 = d.g.k1, km1 = d.g.km1;
+  int kms = 0, kmx = 0, kmy = 0;
+  bool ew = false, nw = false;
+  int fz = km1, fu = km1, fv = km1;
+  if (act) {
+    kms = NB(d.g.kmz, l);
+    const double spl = d.s.sp[l - 1];
+    const double hhs = d.g.hhs[l - 1];
+    for (int k = k1 + ty; k <= kms; k += CLN) {
+      double v = fmin(zl(d, k + 1), hhs) - fmax(zl(d, k), -spl);
+      if (v <= HMIN) v = ZERO;
+      d.f.hp[IX(d, k, l)] = v;
+      if (v > ZERO && k < fz) fz = k;
     }
+    ew = ewet(d, l);
+    if (ew) {
+      const int lE = NB(d.g.lEC, l);
+      kmx = min(kms, NB(d.g.kmz, lE));
+      const double sm = fmax(spl, d.s.sp[lE - 1]);
+      const double hhu = d.g.hhu[l - 1];
+      for (int k = k1 + ty; k <= kmx; k += CLN) {
+        double v = fmin(zl(d, k + 1), hhu) - fmax(zl(d, k), -sm);
+        if (v <= HMIN) v = ZERO;
+        d.f.hup[IX(d, k, l)] = v;
+        if (v > ZERO && k < fu) fu = k;
+      }
+    }
+    nw = nwet(d, l);
+    if (nw) {
+      const int lN = NB(d.g.lNC, l);
+      kmy = min(kms, NB(d.g.kmz, lN));
+      const double sm = fmax(spl, d.s.sp[lN - 1]);
+      const double hhv = d.g.hhv[l - 1];
+      for (int k = k1 + ty; k <= kmy; k += CLN) {
+        double v = fmin(zl(d, k + 1), hhv) - fmax(zl(d, k), -sm);
+        if (v <= HMIN) v = ZERO;
+        d.f.hvp[IX(d, k, l)] = v;
+        if (v > ZERO && k < fv) fv = k;
+      }
+    }
+  }
+  s_first[0][ty][cx] = fz; s_first[1][ty][cx] = fu; s_first[2][ty][cx] = fv;
+  __syncthreads();
+  if (act && ty == 0) {
+    int kz = km1, ku = km1, kv = km1;
+#pragma unroll
+    for (int q = 0; q < CLN; ++q) {
+      kz = min(kz, s_first[0][q][cx]); ku = min(ku, s_first[1][q][cx]); kv = min(kv, s_first[2][q][cx]);
+    }
+    d.s.k1z[l - 1] = kz; d.s.k1u[l - 1] = ku; d.s.k1v[l - 1] = kv;
+  }
+  if (act) {
+    for (int k = k1 + ty; k <= kms; k += CLN) {
+      const int ik = IX(d, k, l);
+      const double z = zmid(d, k, d.f.hp[ik]);
+      if (rotate) d.f.salpp[ik] = d.f.salp[ik];
+      const double sp = (d.f.sal[ik] + d.f.salpp[ik]) / 2.;
+      d.f.salp[ik] = sp;
+      d.f.rhop[ik] = densty_s(sp, 0.00004, z) - 1000.;
+    }
+    if (ew) {
+      for (int k = k1 + ty; k <= kmx; k += CLN) {
+        const int ik = IX(d, k, l);
+        if (rotate) { d.f.uhpp[ik] = d.f.uhp[ik]; d.f.upp[ik] = d.f.up[ik]; }
+        const double hup = d.f.hup[ik];
+        if (hup > ZERO) { const double v = 0.5 * (d.f.uh[ik] + d.f.uhpp[ik]); d.f.uhp[ik] = v; d.f.up[ik] = v / hup; }
+        else { d.f.uhp[ik] = 0.0; d.f.up[ik] = 0.0; }
+      }
+    }
+    if (nw) {
+      for (int k = k1 + ty; k <= kmy; k += CLN) {
+        const int ik = IX(d, k, l);
+        if (rotate) { d.f.vhpp[ik] = d.f.vhp[ik]; d.f.vpp[ik] = d.f.vp[ik]; }
+        const double hvp = d.f.hvp[ik];
+        if (hvp > ZERO) { const double v = 0.5 * (d.f.vh[ik] + d.f.vhpp[ik]); d.f.vhp[ik] = v; d.f.vp[ik] = v / hvp; }
+        else { d.f.vhp[ik] = 0.0; d.f.vp[ik] = 0.0; }
+      }
+    }
+  }
+  __syncthreads();
+  if (!act || ty != 0) return;
+  // surface corrections at the first wet face layer (:3503-3516 / :4033-4046)
+  if (ew) {
     const int k = d.s.k1u[l - 1];
     const int ik = IX(d, k, l);
     if (d.f.hu[IX(d, k - 1, l)] > ZERO) {
@@ -467,15 +508,7 @@ __device__ void half_velocities(const Dev& d, int l, bool rotate) {
       d.f.up[ik] = d.f.uhp[ik] / d.f.hup[ik];
     }
   }
-  if (nwet(d, l)) {
-    const int kmy = min(NB(d.g.kmz, l), NB(d.g.kmz, NB(d.g.lNC, l)));
-    for (int k = d.g.k1; k <= kmy; ++k) {
-      const int ik = IX(d, k, l);
-      if (rotate) { d.f.vhpp[ik] = d.f.vhp[ik]; d.f.vpp[ik] = d.f.vp[ik]; }
-      const double hvp = d.f.hvp[ik];
-      if (hvp > ZERO) { const double v = 0.5 * (d.f.vh[ik] + d.f.vhpp[ik]); d.f.vhp[ik] = v; d.f.vp[ik] = v / hvp; }
-      else { d.f.vhp[ik] = 0.0; d.f.vp[ik] = 0.0; }
-    }
+  if (nw) {
     const int k = d.s.k1v[l - 1];
     const int ik = IX(d, k, l);
     if (d.f.hv[IX(d, k - 1, l)] > ZERO) {
@@ -489,63 +522,74 @@ __device__ void half_velocities(const Dev& d, int l, bool rotate) {
   }
 }
 
-// settrap / settrap2 body after the zeta update: layer_hp2, TopLayerIndexp2, scalars at n+1/2
-// with densty_s, velocities at n+1/2.
-__global__ void k_half_level(Dev d, int rotate) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (l > d.g.lm) return;
-  layer_hp2_col(d, l);
-  top_index_col(d, l);
-  const int kms = NB(d.g.kmz, l);
-  for (int k = d.g.k1; k <= kms; ++k) {
-    const int ik = IX(d, k, l);
-    const double z = zmid(d, k, d.f.hp[ik]);
-    if (rotate) d.f.salpp[ik] = d.f.salp[ik];
-    const double sp = (d.f.sal[ik] + d.f.salpp[ik]) / 2.;
-    d.f.salp[ik] = sp;
-    d.f.rhop[ik] = densty_s(sp, 0.00004, z) - 1000.;
+// save (istep = 2 after a trapezoidal step, 1 after a leapfrog step), cell-parallel like
+// k_half_level; the new first wet layers are reduced over the lanes in shared memory.
+template <int CLN>
+__global__ void __launch_bounds__(32 * CLN) k_save(Dev d, int istep) {
+  __shared__ int s_first[3][CLN][32];
+  const int cx = threadIdx.x, ty = threadIdx.y;
+  const int l = blockIdx.x * 32 + cx + 1;
+  const bool act = l <= d.g.lm;
+  const int k1 = d.g.k1, km1 = d.g.km1;
+  int fz = km1, fu = km1, fv = km1;
+  int zL = 0, uL = 0, vL = 0, kms = 0;
+  if (act) {
+    if (ty == 0) {
+      if (istep == 1) d.s.spp[l - 1] = d.s.sp[l - 1];
+      d.s.sp[l - 1] = d.s.s[l - 1];
+    }
+    zL = zlim(d, l); uL = ulim(d, l); vL = vlim(d, l);
+    kms = NB(d.g.kmz, l);
+    const int kmx = ewet(d, l) ? min(kms, NB(d.g.kmz, NB(d.g.lEC, l))) : 0;
+    const int kmy = nwet(d, l) ? min(kms, NB(d.g.kmz, NB(d.g.lNC, l))) : 0;
+    for (int k = 1 + ty; k <= zL; k += CLN) {
+      const int ik = IX(d, k, l);
+      if (istep == 1) d.f.hpp[ik] = d.f.hp[ik];
+      const double v = d.f.h[ik];
+      d.f.hp[ik] = v;
+      if (k >= k1 && k <= kms && v > ZERO && k < fz) fz = k;
+    }
+    for (int k = 1 + ty; k <= uL; k += CLN) {
+      const int ik = IX(d, k, l);
+      if (istep == 1) d.f.hupp[ik] = d.f.hup[ik];
+      const double v = d.f.hu[ik];
+      d.f.hup[ik] = v;
+      if (k >= k1 && k <= kmx && v > ZERO && k < fu) fu = k;
+    }
+    for (int k = 1 + ty; k <= vL; k += CLN) {
+      const int ik = IX(d, k, l);
+      if (istep == 1) d.f.hvpp[ik] = d.f.hvp[ik];
+      const double v = d.f.hv[ik];
+      d.f.hvp[ik] = v;
+      if (k >= k1 && k <= kmy && v > ZERO && k < fv) fv = k;
+    }
   }
-  half_velocities(d, l, rotate != 0);
-}
-
-// save (istep = 2 after a trapezoidal step, 1 after a leapfrog step)
-__global__ void k_save(Dev d, int istep) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (l > d.g.lm) return;
-  if (istep == 1) d.s.spp[l - 1] = d.s.sp[l - 1];
-  d.s.sp[l - 1] = d.s.s[l - 1];
-  const int zL = zlim(d, l), uL = ulim(d, l), vL = vlim(d, l);
-  for (int k = 1; k <= zL; ++k) {
-    const int ik = IX(d, k, l);
-    if (istep == 1) d.f.hpp[ik] = d.f.hp[ik];
-    d.f.hp[ik] = d.f.h[ik];
+  s_first[0][ty][cx] = fz; s_first[1][ty][cx] = fu; s_first[2][ty][cx] = fv;
+  __syncthreads();
+  if (act && ty == 0) {
+    int kz = km1, ku = km1, kv = km1;
+#pragma unroll
+    for (int q = 0; q < CLN; ++q) {
+      kz = min(kz, s_first[0][q][cx]); ku = min(ku, s_first[1][q][cx]); kv = min(kv, s_first[2][q][cx]);
+    }
+    d.s.k1z[l - 1] = kz; d.s.k1u[l - 1] = ku; d.s.k1v[l - 1] = kv;
   }
-  for (int k = 1; k <= uL; ++k) {
-    const int ik = IX(d, k, l);
-    if (istep == 1) d.f.hupp[ik] = d.f.hup[ik];
-    d.f.hup[ik] = d.f.hu[ik];
-  }
-  for (int k = 1; k <= vL; ++k) {
-    const int ik = IX(d, k, l);
-    if (istep == 1) d.f.hvpp[ik] = d.f.hvp[ik];
-    d.f.hvp[ik] = d.f.hv[ik];
-  }
-  top_index_col(d, l);
-  for (int k = d.g.k1; k <= min(d.g.km, zL); ++k) {
+  if (!act) return;
+  for (int k = k1 + ty; k <= min(d.g.km, zL); k += CLN) {
     const int ik = IX(d, k, l);
     const double z = zmid(d, k, d.f.hp[ik]);
     if (istep == 1) d.f.salpp[ik] = d.f.salp[ik];
     d.f.salp[ik] = d.f.sal[ik];
     d.f.rhop[ik] = densty_s(d.f.salp[ik], 0.00004, z) - 1000.;
   }
-  for (int k = d.g.k1; k <= uL; ++k) {
+  for (int k = k1 + ty; k <= uL; k += CLN) {
     const int ik = IX(d, k, l);
     if (istep == 1) { d.f.uhpp[ik] = d.f.uhp[ik]; d.f.upp[ik] = d.f.up[ik]; }
     const double hup = d.f.hup[ik];
     if (hup > ZERO) { const double v = d.f.uh[ik]; d.f.uhp[ik] = v; d.f.up[ik] = v / hup; }
     else { d.f.uhp[ik] = 0.0; d.f.up[ik] = 0.0; }
   }
-  for (int k = d.g.k1; k <= vL; ++k) {
+  for (int k = k1 + ty; k <= vL; k += CLN) {
     const int ik = IX(d, k, l);
     if (istep == 1) { d.f.vhpp[ik] = d.f.vhp[ik]; d.f.vpp[ik] = d.f.vp[ik]; }
     const double hvp = d.f.hvp[ik];
@@ -618,20 +662,22 @@ void launch_exsal_imsal(const Dev& d, const Tune& tu, cudaStream_t st) {
 
 void launch_vel2(const Dev& d, cudaStream_t st) { k_vel2<<<grid_of(d.g.lm), TB, 0, st>>>(d); }
 
+constexpr int BK_LANES = 4;   // layer lanes of the cell-parallel bookkeeping kernels
+
 void launch_settrap(const Dev& d, cudaStream_t st) {
   k_half_zeta<<<grid_of(d.g.lm), TB, 0, st>>>(d, 1);
-  k_half_level<<<grid_of(d.g.lm), TB, 0, st>>>(d, 1);
+  k_half_level<BK_LANES><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d, 1);
   k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
 }
 
 void launch_settrap2(const Dev& d, cudaStream_t st) {
   k_half_zeta<<<grid_of(d.g.lm), TB, 0, st>>>(d, 0);
-  k_half_level<<<grid_of(d.g.lm), TB, 0, st>>>(d, 0);
+  k_half_level<BK_LANES><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d, 0);
   k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
 }
 
 void launch_save(const Dev& d, int istep, cudaStream_t st) {
-  k_save<<<grid_of(d.g.lm), TB, 0, st>>>(d, istep);
+  k_save<BK_LANES><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d, istep);
   k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
 }
 
