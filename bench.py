@@ -169,6 +169,16 @@ def cpu_sample(name: str, threads: int) -> dict:
             "steps": nsteps, "iters_per_step": sum(s["iters"] for s in o.solves()[-3 * nsteps:]) / nsteps}
 
 
+def step_roofline(form: dict, lm: int, n3: int, peak: float, peak_kind: str) -> dict:
+    """The whole plain FP64 step against the frozen byte model: per fd call 73 FP64 streams per wet
+    cell and 12 per column (3 fd calls per step), per CG iteration 18 streams per unknown, per solve
+    4 streams per unknown of set-up (3 solves per step)."""
+    alg = 3 * 8 * (73 * n3 + 12 * lm) + 8 * lm * (18 * form["pcg_iters_per_step"] + 3 * 4)
+    achieved = alg / form["s_per_step"] / 1e9
+    return {"bound": "hbm", "algorithmic_bytes_per_step": alg, "achieved": achieved, "peak": peak, "unit": "GB/s",
+            "frac": achieved / peak, "peak_kind": peak_kind}
+
+
 def bench_ensemble(args, ws: int, rank: int, device: int, pg) -> int:
     """c3: the seeded 64-basin ensemble, one CUDA graph launch per step.  With N ranks the members
     are partitioned across the GPUs by size (no collective on the data path); members that do not
@@ -418,6 +428,7 @@ def main() -> int:
             "pcg_speedup_vs_plain_fp64": plain["pcg_s_per_step"] / head["pcg_s_per_step"],
             "forms": {k: {kk: vv for kk, vv in v.items() if kk not in ("clocks", "e2e", "zeta")} for k, v in res.items()},
             "roofline": head.get("roofline"), "cpu_baseline": cpu, "e2e": head["e2e"],
+            "plain_step_roofline": step_roofline(plain, lm, n3, peak, peak_kind),
             "gpu_launches": head["gpu_launches"], "clocks": head["clocks"],
         }
         print(json.dumps(line), flush=True)
