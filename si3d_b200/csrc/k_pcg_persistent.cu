@@ -99,7 +99,139 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, int* s_f
   return *s_flag != 0;
 }
 
-template <typename T>
+// ---- adaptive eigenvalue estimates for stopping test 2: chgcon (nspcg.f:16499-16620), eigvss
+// (:17201-17240), zbrent (:32976-33160) and determ (:16926-16962), run by one thread after each new
+// alpha.  tri holds the Lanczos tridiagonal column by column: tri[2 (c - 1)] = T(1, c), tri[2 (c - 1) + 1]
+// = T(2, c).
+__device__ double lz_determ(int n, const double* tri, double x) {
+  auto T = [&](int r, int c) { return tri[(c - 1) * 2 + (r - 1)]; };
+  const int nm1 = n - 1;
+  double d2 = T(1, n) - x;
+  double d1 = d2 * (T(1, nm1) - x) - T(2, n);
+  if (n != 2) {
+    for (int l = nm1; l >= 2; --l) {
+      const double d3 = d2;
+      d2 = d1;
+      d1 = (T(1, l - 1) - x) * d2 - d3 * T(2, l);
+    }
+  }
+  return d1;
+}
+
+// Brent's root search on the determinant, in zbrent's own step order.
+__device__ void lz_zbrent(int n, const double* tri, double eps, int nsig, double& aa, double& bb, int maxfn, int& ier) {
+  double a = aa, b = bb;
+  const double t = pow(0.1, (double)nsig);
+  int ic = 2;
+  double fa = lz_determ(n, tri, a), fb = lz_determ(n, tri, b), fc = 0, c = 0, d = 0, e = 0, s = b;
+  double p, q, r, rone, tol, rm, temp;
+  if (fa * fb > 0.0) { ier = 4; aa = a; bb = b; return; }
+  for (;;) {
+    c = a; fc = fa; d = b - c; e = d;
+    for (;;) {
+      if (fabs(fc) < fabs(fb)) { a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
+      tol = t * fmax(fabs(b), 0.1);
+      rm = (c - b) / 2.0;
+      if (fabs(fb) <= eps || fabs(c - b) <= tol) { aa = c; bb = b; return; }
+      if (ic >= maxfn) { ier = 3; aa = c; bb = b; return; }
+      bool bisect = fabs(e) < tol || fabs(fa) <= fabs(fb);
+      if (!bisect) {
+        s = fb / fa;
+        if (a == c) {
+          p = (c - b) * s;
+          q = 1.0 - s;
+        } else {
+          q = fa / fc;
+          r = fb / fc;
+          rone = r - 1.0;
+          p = s * ((c - b) * q * (q - r) - (b - a) * rone);
+          q = (q - 1.0) * rone * (s - 1.0);
+        }
+        if (p > 0.0) q = -q;
+        if (p < 0.0) p = -p;
+        s = e;
+        e = d;
+        if (p + p >= 3.0 * rm * q || p + p >= fabs(s * q)) bisect = true;
+        else d = p / q;
+      }
+      if (bisect) { e = rm; d = e; }
+      a = b;
+      fa = fb;
+      temp = d;
+      if (fabs(temp) <= tol / 2.0) temp = copysign(tol / 2.0, rm);
+      b = b + temp;
+      s = b;
+      fb = lz_determ(n, tri, s);
+      ic = ic + 1;
+      if (!(fb * fc <= 0.0)) break;   // root no longer bracketed by (b, c): restart from (a, b)
+    }
+  }
+}
+
+__device__ double lz_eigvss(const double* tri, int n, double start, double end, int icode, double zeta, int itmax,
+                            int& ier) {
+  const int itmp = (int)(-log10(fabs(zeta)));
+  const int nsig = itmp > 4 ? itmp : 4;
+  const int maxfn = itmax > 50 ? itmax : 50;
+  double a = start, b = end;
+  lz_zbrent(n, tri, 0.0, nsig, a, b, maxfn, ier);
+  return icode == 1 ? fmax(a, b) : fmin(a, b);
+}
+
+// chgcon after iteration ip (alpha: this iteration's, alphao: the previous one's, beta: this
+// iteration's).  Updates S->emin/emax, the adaptivity flags and the bounds; sets S->chg_ier to 3/4
+// when the root search stops as zbrent's do.
+__device__ __noinline__ void lz_chgcon(PcgScal* S, double* tri, int ip, double alpha, double beta, double alphao) {
+  auto T = [&](int r, int c) -> double& { return tri[(c - 1) * 2 + (r - 1)]; };
+  if (ip == 0) {
+    const double end = 1.0 / alpha;
+    T(1, 1) = end; T(2, 1) = 0.0;
+    if (S->maxadp) S->emax = end;
+    if (S->minadp) S->emin = end;
+    return;
+  }
+  const double t1 = 1.0 / alpha + beta / alphao;
+  const double t2 = beta / (alphao * alphao);
+  const double tsqr = sqrt(t2);
+  T(1, ip + 1) = t1; T(2, ip + 1) = t2;
+  if (ip == 1) {
+    S->tl1 = T(1, 1) + tsqr; S->tl2 = t1 + tsqr;
+    S->bl1 = T(1, 1) - tsqr; S->bl2 = t1 - tsqr;
+    const double t3 = T(1, 1) + t1;
+    const double t4 = sqrt((t1 - T(1, 1)) * (t1 - T(1, 1)) + 4.0 * t2);
+    if (S->maxadp) S->emax = (t3 + t4) / 2.0;
+    if (S->minadp) S->emin = (t3 - t4) / 2.0;
+    return;
+  }
+  int ier = S->chg_ier;
+  if (S->maxadp) {
+    S->tl1 = fmax(S->tl1, S->tl2 + tsqr);
+    S->tl2 = t1 + tsqr;
+    const double emaxo = S->emax;
+    const double end = fmax(S->tl1, S->tl2);
+    const double e1 = lz_eigvss(tri, ip + 1, emaxo, end, 2, S->zeta, S->itmax, ier);
+    if (ier != 3 && ier != 4) {
+      S->emax = e1;
+      if (fabs(S->emax - emaxo) < S->emax * S->zeta) S->maxadp = 0;
+    } else S->maxadp = 0;
+  }
+  if (S->minadp) {
+    S->bl1 = fmin(S->bl1, S->bl2 - tsqr);
+    S->bl2 = t1 - tsqr;
+    const double start = fmax(0.0, fmin(S->bl1, S->bl2));
+    const double emino = S->emin;
+    const double e1 = lz_eigvss(tri, ip + 1, start, emino, 1, S->zeta, S->itmax, ier);
+    if (ier != 3 && ier != 4) {
+      S->emin = e1;
+      if (fabs(S->emin - emino) < S->emin * S->zeta) S->minadp = 0;
+    } else S->minadp = 0;
+  }
+  S->chg_ier = ier;
+}
+
+// TEST2: stopping test 2 with chgcon's adaptive emin (test 5 otherwise); a separate instantiation keeps
+// the test-5 loop free of the eigenvalue code.
+template <typename T, bool TEST2>
 __global__ void __launch_bounds__(QB, 3) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
   __shared__ double sh[8 * 4 + 4];
   __shared__ int s_flag;
@@ -117,9 +249,9 @@ __global__ void __launch_bounds__(QB, 3) k_pcg_loop(PcgDevT<T> P, GridBar* bar) 
   double alpha = SC->alpha, beta = SC->beta, rzdot = SC->rzdot, dkm1 = SC->dkm1, udnm = SC->udnm;
   const double zeta = SC->zeta, srelpr = SC->srelpr, bnorm = SC->bnorm, emin = SC->emin;
   int in = SC->in, q1 = SC->q1, ier = 0, par = 0;
-  const int itmax = SC->itmax, ntest = SC->ntest, hist_cap = SC->hist_cap;
+  const int itmax = SC->itmax, hist_cap = SC->hist_cap;
   double stptst = SC->stptst;
-  const bool t2 = (ntest == 2);
+  const bool t2 = TEST2;
   bool run = SC->done == 0;
   while (run) {
     const T* __restrict__ Bp = par ? B.p2 : B.p;
@@ -213,7 +345,7 @@ __global__ void __launch_bounds__(QB, 3) k_pcg_loop(PcgDevT<T> P, GridBar* bar) 
     if (!(rzt > 0.0)) { ier = -7; break; }
     const double tiny = 500.0 * srelpr;
     bool halt;
-    if (ntest == 5) {
+    if (!TEST2) {
       const double tl = sqrt(rrt);
       stptst = tl / bnorm;
       halt = tl < bnorm * zeta;
@@ -230,7 +362,8 @@ __global__ void __launch_bounds__(QB, 3) k_pcg_loop(PcgDevT<T> P, GridBar* bar) 
           if (udnm < tiny) udnm = 1.0;
           if ((in > 5) && (fabs(udnm - uold) < udnm * zeta)) q1 = 1;
         }
-        const double eminl = emin < tiny ? tiny : emin;
+        const double em = __ldcg(&SC->emin);   // chgcon's latest estimate (block 0, before the last barrier)
+        const double eminl = em < tiny ? tiny : em;
         const double tl = sqrt(zzt), tr = udnm * eminl;
         stptst = tl / tr;
         halt = tl < tr * zeta;
@@ -275,9 +408,12 @@ __global__ void __launch_bounds__(QB, 3) k_pcg_loop(PcgDevT<T> P, GridBar* bar) 
     if (!grid_barrier(bar, SC, &s_flag)) return;
     double pap[1];
     all_partials<1>(pq_part, nb, 0, pap, sh);
+    const double alpha_prev = alpha;
     alpha = rzdot / pap[0];
     if (!(pap[0] > 0.0)) { ier = -6; break; }
     if (blockIdx.x == 0 && threadIdx.x == 0 && in < hist_cap) { P.hist_alpha[in] = alpha; P.hist_beta[in] = beta; }
+    if (TEST2 && blockIdx.x == 0 && threadIdx.x == 0 && P.tri && (SC->maxadp || SC->minadp))
+      lz_chgcon(SC, P.tri, in, alpha, beta, alpha_prev);
     in += 1;
     par ^= 1;
   }
@@ -285,6 +421,7 @@ __global__ void __launch_bounds__(QB, 3) k_pcg_loop(PcgDevT<T> P, GridBar* bar) 
     SC->alpha = alpha; SC->beta = beta; SC->rzdot = rzdot; SC->dkm1 = dkm1; SC->udnm = udnm; SC->q1 = q1;
     SC->in = in; SC->stptst = stptst;
     if (ier) SC->ier = ier;
+    else if (SC->chg_ier) SC->ier = SC->chg_ier;
     SC->done = 1;
   }
 }
@@ -292,7 +429,7 @@ __global__ void __launch_bounds__(QB, 3) k_pcg_loop(PcgDevT<T> P, GridBar* bar) 
 // Cooperative launch (all blocks co-resident) through cudaLaunchKernelEx, which stream capture
 // records as a cooperative kernel node.
 template <typename T>
-int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, cudaStream_t st) {
+int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st) {
   if (cudaMemsetAsync(bar, 0, sizeof(GridBar), st) != cudaSuccess) return -1;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nblocks);
@@ -304,7 +441,9 @@ int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, cudaStream_t st)
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_pcg_loop<T>, P, bar) == cudaSuccess ? 0 : -1;
+  const cudaError_t e = test2 ? cudaLaunchKernelEx(&cfg, k_pcg_loop<T, true>, P, bar)
+                              : cudaLaunchKernelEx(&cfg, k_pcg_loop<T, false>, P, bar);
+  return e == cudaSuccess ? 0 : -1;
 }
 
 }  // namespace
@@ -312,20 +451,27 @@ int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, cudaStream_t st)
 int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32) {
   int sms = 0, occ = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  if (fp32) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<float>, QB, 0);
-  else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<double>, QB, 0);
+  int occ2 = 0;
+  if (fp32) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<float, false>, QB, 0);
+    occ2 = occ;
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<double, false>, QB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_pcg_loop<double, true>, QB, 0);
+  }
+  occ = std::min(occ, occ2);
   int per_sm = occ;
   if (max_per_sm > 0) per_sm = std::min(per_sm, max_per_sm);
   const int need = (std::max(nR, nB) + QB - 1) / QB;
   return std::max(1, std::min(sms * std::max(per_sm, 1), need));
 }
 
-int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, cudaStream_t st) {
-  return launch_loop<double>(P, bar, nblocks, st);
+int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st) {
+  return launch_loop<double>(P, bar, nblocks, test2, st);
 }
 
 int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st) {
-  return launch_loop<float>(F, bar, nblocks, st);
+  return launch_loop<float>(F, bar, nblocks, false, st);
 }
 
 }  // namespace si3d

@@ -20,6 +20,9 @@ struct PcgScal {
   double alpha, beta, alphao, rzdot, dkm1, pap, bnorm, stptst, zeta, srelpr, udnm, emin, emax;
   int in, itmax, ntest, done, ier, q1, hist_cap, negpiv;
   unsigned int cnt[4];
+  // adaptive eigenvalue estimates of stopping test 2 (chgcon, itcom2/itcom3 of NSPCG)
+  double tl1, tl2, bl1, bl2;
+  int maxadp, minadp, chg_ier;
 };
 
 template <typename T>
@@ -29,6 +32,7 @@ struct PcgDevT {
   double *part0, *part1, *part2, *part3;   // block partials, part_n entries each, contiguous
   int part_n;
   double *hist_alpha, *hist_beta;
+  double* tri;   // Lanczos tridiagonal of chgcon, 2 x (itmax + 2), column-major (test 2)
 };
 using PcgDev = PcgDevT<double>;
 using PcgDevF = PcgDevT<float>;
@@ -65,7 +69,7 @@ struct GridBar {
   unsigned int count, gen, abort, pad;
 };
 int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32);
-int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, cudaStream_t st);
+int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st);   // test2: stopping test 2
 int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st);
 
 void launch_slayer_h(const Dev& d, cudaStream_t st);

@@ -298,6 +298,7 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
   const int cap = std::max(c->prm.pcg_itmax, 1) + 1;
   rc |= c->alloc(&P.hist_alpha, cap);
   rc |= c->alloc(&P.hist_beta, cap);
+  rc |= c->alloc(&P.tri, 2 * (size_t)(cap + 1));
   if (rc) return rc;
   CK(cudaMallocHost(&c->h_sc, sizeof(PcgScal)));
   CK(cudaMallocHost(&c->h_hist, sizeof(double) * 2 * cap));
@@ -314,7 +315,7 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
   rc |= c->alloc(&F.sc, 1);
   if (rc) return rc;
   F.part0 = P.part0; F.part1 = P.part1; F.part2 = P.part2; F.part3 = P.part3; F.part_n = P.part_n;
-  F.hist_alpha = P.hist_alpha; F.hist_beta = P.hist_beta;
+  F.hist_alpha = P.hist_alpha; F.hist_beta = P.hist_beta; F.tri = nullptr;
   CK(cudaMallocHost(&c->h_scf, sizeof(PcgScal)));
   return 0;
 }
@@ -498,6 +499,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   init.itmax = p.pcg_itmax;
   init.ntest = p.pcg_test;
   init.emax = 2.0; init.emin = 1.0; init.udnm = 1.0;
+  init.maxadp = 1; init.minadp = 1;
   init.hist_cap = p.pcg_itmax + 1;
   if (c->graph_mode) {
     // the scalars are set by a kernel (a host copy would capture a host buffer that later solves reuse)
@@ -525,7 +527,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   int rc0 = stage(c, ST_PCG_SETUP, 7, [&] { pcg_setup(c->d, c->pcg, x0, c->dz, &c->pcg.sc->negpiv, c->st); });
   if (rc0) return rc0;
   if (c->graph_mode) {
-    if (pcg_loop(c->pcg, c->bar, c->loop_blocks, c->st) != 0) return cuda_fail(cudaGetLastError(), "pcg_loop", __LINE__);
+    if (pcg_loop(c->pcg, c->bar, c->loop_blocks, c->prm.pcg_test == 2, c->st) != 0) return cuda_fail(cudaGetLastError(), "pcg_loop", __LINE__);
     c->launches += 1;
     rc0 = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, c->st); });
     if (rc0) return rc0;
@@ -546,7 +548,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
     // run iterations in batches; every kernel returns at once after convergence
     int rci = iterate(c, c->pcg.sc, c->h_sc, p.pcg_itmax, c->last_iters,
                       [&](int par) { pcg_iteration(c->pcg, par, c->st); },
-                      [&] { return pcg_loop(c->pcg, c->bar, c->loop_blocks, c->st); });
+                      [&] { return pcg_loop(c->pcg, c->bar, c->loop_blocks, c->prm.pcg_test == 2, c->st); });
     if (rci) return rci;
     total_iters = c->h_sc->in;
     c->last_iters = std::max(total_iters, 1);
@@ -1395,7 +1397,8 @@ int si3d_gpu_solve_zeta(int lm, const double* coef, const int* jcoef, const doub
     }
     double zt = pcg_tol < 500.0 * srelpr ? 500.0 * srelpr : pcg_tol;
     double e0 = 1.0, e1 = 2.0;
-    if (it > 0) eigen_estimates(al.data(), be.data(), it, zt, pcg_itmax, e0, e1);
+    if (pcg_test == 2) { e0 = c->h_sc->emin; e1 = c->h_sc->emax; }   // adapted on the device during the solve
+    else if (it > 0) eigen_estimates(al.data(), be.data(), it, zt, pcg_itmax, e0, e1);
     if (emin) *emin = e0;
     if (emax) *emax = e1;
   }

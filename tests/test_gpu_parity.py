@@ -5,8 +5,12 @@ device) and run one routine on each side; the column stages must agree to the la
 few ulps, the zeta solve to its stopping tolerance.  Run tests advance whole time steps
 (si3d.f90:324-458) on both sides and compare every prognostic field.
 """
+import os
+
 import numpy as np
 import pytest
+
+from conftest import ROOT
 
 pytestmark = pytest.mark.gpu
 
@@ -138,3 +142,40 @@ def test_standalone_solve_matches_oracle(run_dirs, oracle_lib, native_libs):
     assert abs(r_g["iters"] - r_o["iters"]) <= 2
     assert np.abs(x_g - x_o).max() <= 1e-11 * max(np.abs(x_o).max(), 1e-3)
     assert r_g["stptst"] < 1e-12
+
+
+@pytest.mark.gpu
+def test_stopping_test_2_standalone_matches_oracle(native_libs, oracle_lib):
+    """Stopping test 2 (the reference's own setting, 1e-6) with chgcon's adaptive emin/emax on the
+    device: same iteration count, eigenvalue estimates and solution as the oracle's red-black MIC-PCG."""
+    from si3d_b200.model import solve_zeta
+    g = np.load(os.path.join(ROOT, "tests", "golden", "pcg_48x32.npz"))
+    x0 = np.zeros_like(g["rhs"])
+    x_o, r_o = oracle_lib.pcg(g["coef"], g["jcoef"], g["rhs"], x0, pcg_test=2, tol=1e-6, itmax=500, ordering=1)
+    x_g, r_g = solve_zeta(g["coef"], g["jcoef"], g["rhs"], x0, pcg_test=2, tol=1e-6, itmax=500)
+    assert r_o["ier"] == 0 and r_g["ier"] == 0
+    assert abs(r_g["iters"] - r_o["iters"]) <= 1
+    assert r_g["emin"] == pytest.approx(r_o["emin"], rel=1e-6)
+    assert r_g["emax"] == pytest.approx(r_o["emax"], rel=1e-6)
+    assert np.abs(x_g - x_o).max() <= 1e-6 * np.abs(x_o).max()
+
+
+@pytest.mark.gpu
+def test_stopping_test_2_steps_match_oracle(native_libs, oracle_lib, run_dirs):
+    """Whole time steps with stopping test 2 at 1e-6: per-solve iteration counts within one of the
+    oracle's and the surface elevation within the solve tolerance's reach."""
+    from si3d_b200.model import GpuRun
+    steps = 5
+    o = oracle_lib.OracleRun(run_dirs["t1"], pcg_test=2, pcg_tol=1e-6, pcg_itmax=200, ordering=1)
+    o.run(steps)
+    it_o = [s["iters"] for s in o.solves()]
+    run = GpuRun(run_dirs["t1"], pcg_test=2, pcg_tol=1e-6, pcg_itmax=200)
+    try:
+        st = run.run(steps)
+        it_g = [s.iters[i] for s in st for i in range(s.nsolves)]
+        assert len(it_g) == len(it_o)
+        assert max(abs(a - b) for a, b in zip(it_g, it_o)) <= 1
+        s_o = o.get("s")[:o.lm]
+        assert np.abs(run.get("s")[:run.lm] - s_o).max() <= 1e-6 * max(np.abs(s_o).max(), 1e-3)
+    finally:
+        run.close()
