@@ -41,43 +41,22 @@ struct FaceCol {
   int l, lE, lW, lN, lS, lO, kmx, k1x, lX2;
 };
 
-template <int IEQ>
-__device__ __forceinline__ FaceCol face_col(const Dev& d, int l) {
-  const Grid& g = d.g;
-  const bool X = (IEQ == 1);
-  FaceCol f;
-  f.l = l;
-  f.lE = NB(g.lEC, l); f.lW = NB(g.lWC, l); f.lN = NB(g.lNC, l); f.lS = NB(g.lSC, l);
-  f.lO = X ? f.lE : f.lN;
-  f.kmx = min(NB(g.kmz, f.lO), NB(g.kmz, l));
-  f.k1x = X ? NB(d.s.k1u, l) : NB(d.s.k1v, l);
-  f.lX2 = X ? NB(g.lSC, f.lE) : NB(g.lWC, f.lN);   // lSC(lEC(l)) / lWC(lNC(l))
-  return f;
-}
-
 // ------------------------------------------------------------------ cell kernel
 template <int IEQ, int CL>
-__global__ void __launch_bounds__(CW * CL, 1024 / (CW * CL)) k_mom_cells(Dev d, const int* __restrict__ cols, int ncols) {
+__global__ void __launch_bounds__(CW * CL, 1024 / (CW * CL)) k_mom_cells(Dev d, const FaceMeta* __restrict__ meta, int ncols) {
   const int t = blockIdx.x * CW + threadIdx.x;
   if (t >= ncols) return;
-  const Grid& g = d.g;
-  const int lm1 = g.lm1;
   const bool X = (IEQ == 1);
-  const FaceCol F = face_col<IEQ>(d, cols[t]);
-  const int l = F.l, lE = F.lE, lW = F.lW, lN = F.lN, lS = F.lS, lO = F.lO, kmx = F.kmx, k1x = F.k1x, lX2 = F.lX2;
+  const int4 ma = __ldg(&meta[t].a), mb = __ldg(&meta[t].b);
+  const int l = ma.x, lE = ma.y, lW = ma.z, lN = ma.w, lS = mb.x, lX2 = mb.y, kmx = mb.z;
+  const int lO = X ? lE : lN;
+  const int* k1f = X ? d.s.k1u : d.s.k1v;
+  const int k1x = NB(k1f, l);
   if (k1x + (int)threadIdx.y > kmx) return;
-  int mW_first = 0, mW_last = -1, mS_first = 0, mS_last = -1;
-  if (X) {
-    if (lW != lm1) { mW_first = NB(d.s.k1u, lW); mW_last = min(NB(g.kmz, l), NB(g.kmz, lW)); }
-    if (lS != lm1 && NB(g.lEC, lS) != lm1) {
-      mS_first = NB(d.s.k1u, lS); mS_last = min(NB(g.kmz, NB(g.lEC, lS)), NB(g.kmz, lS));
-    }
-  } else {
-    if (lS != lm1) { mS_first = NB(d.s.k1v, lS); mS_last = min(NB(g.kmz, l), NB(g.kmz, lS)); }
-    if (lW != lm1 && NB(g.lNC, lW) != lm1) {
-      mW_first = NB(d.s.k1v, lW); mW_last = min(NB(g.kmz, NB(g.lNC, lW)), NB(g.kmz, lW));
-    }
-  }
+  // west / south neighbouring faces' diffusion ranges (their first wet layers change per step)
+  const int mW_last = mb.w, mS_last = __ldg(&meta[t].c.x);
+  const int mW_first = mW_last >= 0 ? NB(k1f, lW) : 0;
+  const int mS_first = mS_last >= 0 ? NB(k1f, lS) : 0;
   const double* huv = X ? d.f.hup : d.f.hvp;
   const double* huvpp = X ? d.f.hupp : d.f.hvpp;
   const double* uvpp_h = X ? d.f.uhpp : d.f.vhpp;
@@ -178,11 +157,15 @@ __global__ void __launch_bounds__(CW * CL, 1024 / (CW * CL)) k_mom_cells(Dev d, 
 
 // ------------------------------------------------------------------ column kernel
 template <int IEQ, int NT>
-__global__ void __launch_bounds__(NT, 1024 / NT) k_mom_columns(Dev d, const int* __restrict__ cols, int ncols) {
+__global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceMeta* __restrict__ meta, int ncols) {
   const int t = blockIdx.x * NT + threadIdx.x;
   if (t >= ncols) return;
   const bool X = (IEQ == 1);
-  const FaceCol F = face_col<IEQ>(d, cols[t]);
+  const int4 ma = __ldg(&meta[t].a), mb = __ldg(&meta[t].b);
+  FaceCol F;
+  F.l = ma.x; F.lE = ma.y; F.lW = ma.z; F.lN = ma.w; F.lS = mb.x; F.lX2 = mb.y; F.kmx = mb.z;
+  F.lO = X ? F.lE : F.lN;
+  F.k1x = X ? NB(d.s.k1u, F.l) : NB(d.s.k1v, F.l);
   const int l = F.l, lE = F.lE, lW = F.lW, lN = F.lN, lS = F.lS, lO = F.lO, kmx = F.kmx, k1x = F.k1x, lX2 = F.lX2;
   const int nw = kmx - k1x + 1;
   if (nw < 1) return;
@@ -314,7 +297,7 @@ int momentum_init(int km1) {
 }
 
 template <int IEQ>
-void launch_dir(const Dev& d, const int* cols, int ncols, const Tune& tu, cudaStream_t st) {
+void launch_dir(const Dev& d, const FaceMeta* cols, int ncols, const Tune& tu, cudaStream_t st) {
   const int g1 = (ncols + CW - 1) / CW;
   switch (tu.mom_cl) {
     case 2: k_mom_cells<IEQ, 2><<<g1, dim3(CW, 2), 0, st>>>(d, cols, ncols); break;
@@ -328,7 +311,7 @@ void launch_dir(const Dev& d, const int* cols, int ncols, const Tune& tu, cudaSt
   }
 }
 
-void launch_momentum(const Dev& d, int ieq, const int* cols, int ncols, const Tune& tu, cudaStream_t st) {
+void launch_momentum(const Dev& d, int ieq, const FaceMeta* cols, int ncols, const Tune& tu, cudaStream_t st) {
   if (ncols <= 0) return;
   if (ieq == 1) launch_dir<1>(d, cols, ncols, tu, st);
   else launch_dir<2>(d, cols, ncols, tu, st);

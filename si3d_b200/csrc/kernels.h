@@ -44,8 +44,17 @@ struct Tune {
   int mom_cl = 8, mom_nt = 128, sal_cl = 8, sal_nt = 128;
 };
 
+// Static indices of one u (v) face column of the momentum stage, computed once from the grid maps
+// so that the kernels start from one coalesced load instead of a chain of dependent lookups:
+// a = (l, lE, lW, lN), b = (lS, lX2, kmx, mW_last), c = (mS_last, 0, 0, 0), where lX2 is lSC(lEC(l))
+// (lWC(lNC(l)) for v), kmx the face depth, and mW_last / mS_last the last layer of the west / south
+// neighbouring face's diffusion coefficient (-1 when that face contributes none).
+struct FaceMeta {
+  int4 a, b, c;
+};
+
 int momentum_init(int km1);
-void launch_momentum(const Dev& d, int ieq, const int* cols, int ncols, const Tune& tu, cudaStream_t st);
+void launch_momentum(const Dev& d, int ieq, const FaceMeta* meta, int ncols, const Tune& tu, cudaStream_t st);
 void launch_matcon(const Dev& d, cudaStream_t st);
 
 void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, int* negpiv, cudaStream_t st);

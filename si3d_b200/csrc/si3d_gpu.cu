@@ -76,6 +76,8 @@ struct Ctx {
   int* ce = nullptr;
   int* cn = nullptr;
   int nce = 0, ncn = 0;
+  FaceMeta* mce = nullptr;   // static indices of the u / v face columns (momentum stage)
+  FaceMeta* mcn = nullptr;
   // red-black zeta system
   PcgDev pcg{};
   PcgDevF pcgf{};            // FP32 inner system of iterative refinement
@@ -584,8 +586,8 @@ int fd_impl(Ctx* c, int istep, si3d_step_stats* st) {
   Dev& d = c->d;
   d.tz = 1.0 / istep;
   // surfbc CASE(0) is a constant per-column wind set by the host (uair/vair/cdw fields)
-  int rc = stage(c, ST_MOMX, 2, [&] { launch_momentum(d, 1, c->ce, c->nce, c->tune, c->st); });
-  if (!rc) rc = stage(c, ST_MOMY, 2, [&] { launch_momentum(d, 2, c->cn, c->ncn, c->tune, c->st); });
+  int rc = stage(c, ST_MOMX, 2, [&] { launch_momentum(d, 1, c->mce, c->nce, c->tune, c->st); });
+  if (!rc) rc = stage(c, ST_MOMY, 2, [&] { launch_momentum(d, 2, c->mcn, c->ncn, c->tune, c->st); });
   if (!rc) rc = stage(c, ST_MATCON, 1, [&] { launch_matcon(d, c->st); });
   if (rc) return rc;
   if (st) CK(cudaEventRecord(c->evp0, c->st));
@@ -755,6 +757,41 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
   if (rc) { delete c; return rc; }
   if (!ce.empty()) cudaMemcpy(c->ce, ce.data(), ce.size() * sizeof(int), cudaMemcpyHostToDevice);
   if (!cn.empty()) cudaMemcpy(c->cn, cn.data(), cn.size() * sizeof(int), cudaMemcpyHostToDevice);
+  {
+    // static per-face indices of the momentum stage (exmom/matmom neighbours and layer bounds)
+    auto kz = [&](int q) { return g->kmz[q - 1]; };
+    auto nbE = [&](int q) { return q == lm1 ? lm1 : g->lEC[q - 1]; };
+    auto nbW = [&](int q) { return q == lm1 ? lm1 : g->lWC[q - 1]; };
+    auto nbN = [&](int q) { return q == lm1 ? lm1 : g->lNC[q - 1]; };
+    auto nbS = [&](int q) { return q == lm1 ? lm1 : g->lSC[q - 1]; };
+    auto meta_of = [&](int l, bool X) {
+      const int lE = nbE(l), lW = nbW(l), lN = nbN(l), lS = nbS(l);
+      const int lO = X ? lE : lN;
+      const int lX2 = X ? nbS(lE) : nbW(lN);
+      const int kmx = std::min(kz(lO), kz(l));
+      int mW_last = -1, mS_last = -1;
+      if (X) {
+        if (lW != lm1) mW_last = std::min(kz(l), kz(lW));
+        if (lS != lm1 && nbE(lS) != lm1) mS_last = std::min(kz(nbE(lS)), kz(lS));
+      } else {
+        if (lS != lm1) mS_last = std::min(kz(l), kz(lS));
+        if (lW != lm1 && nbN(lW) != lm1) mW_last = std::min(kz(nbN(lW)), kz(lW));
+      }
+      FaceMeta m;
+      m.a = make_int4(l, lE, lW, lN);
+      m.b = make_int4(lS, lX2, kmx, mW_last);
+      m.c = make_int4(mS_last, 0, 0, 0);
+      return m;
+    };
+    std::vector<FaceMeta> me, mn;
+    for (int l : ce) me.push_back(meta_of(l, true));
+    for (int l : cn) mn.push_back(meta_of(l, false));
+    rc |= c->alloc(&c->mce, me.size());
+    rc |= c->alloc(&c->mcn, mn.size());
+    if (rc) { delete c; return rc; }
+    if (!me.empty()) cudaMemcpy(c->mce, me.data(), me.size() * sizeof(FaceMeta), cudaMemcpyHostToDevice);
+    if (!mn.empty()) cudaMemcpy(c->mcn, mn.data(), mn.size() * sizeof(FaceMeta), cudaMemcpyHostToDevice);
+  }
   rc = build_pcg(c, g);
   if (rc) { delete c; return rc; }
   if (cudaDeviceSynchronize() != cudaSuccess) { delete c; return SI3D_ECUDA; }
@@ -950,7 +987,7 @@ int si3d_gpu_stage(int h, const char* stage, int istep, si3d_step_stats* st) {
   const std::string s = stage;
   Dev& d = c->d;
   d.tz = 1.0 / istep;
-  if (s == "momentum") { launch_momentum(d, 1, c->ce, c->nce, c->tune, c->st); launch_momentum(d, 2, c->cn, c->ncn, c->tune, c->st); }
+  if (s == "momentum") { launch_momentum(d, 1, c->mce, c->nce, c->tune, c->st); launch_momentum(d, 2, c->mcn, c->ncn, c->tune, c->st); }
   else if (s == "matcon") launch_matcon(d, c->st);
   else if (s == "solve") {
     int it = 0, ier = 0;
@@ -1066,8 +1103,8 @@ static int time_stage(Ctx* c, int which, int reps, float* best) {
   Dev& d = c->d;
   auto run = [&] {
     if (which == 0) {
-      launch_momentum(d, 1, c->ce, c->nce, c->tune, c->st);
-      launch_momentum(d, 2, c->cn, c->ncn, c->tune, c->st);
+      launch_momentum(d, 1, c->mce, c->nce, c->tune, c->st);
+      launch_momentum(d, 2, c->mcn, c->ncn, c->tune, c->st);
     } else {
       launch_exsal_imsal(d, c->tune, c->st);
     }
