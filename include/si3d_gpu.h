@@ -44,6 +44,8 @@ extern "C" {
 /* precision forms */
 #define SI3D_FP64 0       /* plain FP64 everywhere */
 #define SI3D_MIXED_IR 1   /* FP32 SpMV + MIC inside an FP64 iterative-refinement loop */
+#define SI3D_MIXED_MG 2   /* FP32 SpMV + aggregation-multigrid V-cycle inside FP64 iterative
+                             refinement (needs the l2i/l2j maps of a plain (im1, jm1) grid) */
 
 /* zeta-solve orderings */
 #define SI3D_ORDER_REDBLACK 1   /* NSPCG iperm=1 red-black MIC (the GPU form) */
@@ -51,7 +53,15 @@ extern "C" {
 /* initial guess for the zeta solve */
 #define SI3D_X0_PREV 0      /* sp, as the reference (si3d_procedures.f90:1970) */
 #define SI3D_X0_ZERO 1
-#define SI3D_X0_LEARNED 2   /* sp + the learned increment (si3d_gpu_set_warmstart) */
+#define SI3D_X0_LEARNED 2   /* with a network loaded (si3d_learn_set_params): sp + the predicted
+                               increment for the leapfrog solve of a step, the latest solution for
+                               the trapezoidal solves after it; otherwise sp + the increment set by
+                               si3d_gpu_set_warmstart for every solve */
+#define SI3D_X0_LAST 3      /* s, the latest accepted solution: within a step the trapezoidal solves
+                               start from the previous solve's zeta(n+1) instead of the half level sp */
+#define SI3D_X0_HIST 4      /* s + the same solve's correction one step earlier (solve k of step n
+                               starts from s + (x_k(n-1) - s_k(n-1)), where s_k is the zeta solve k
+                               started from); the first step starts from s */
 
 /* Grid description produced by the host's `bathy` (si3d_utils.f90:595-892). */
 typedef struct si3d_grid {
@@ -84,7 +94,7 @@ typedef struct si3d_params {
   double srelpr;
   int ordering;            /* SI3D_ORDER_REDBLACK */
   int x0_mode;             /* SI3D_X0_* */
-  int precision;           /* SI3D_FP64 or SI3D_MIXED_IR */
+  int precision;           /* SI3D_FP64, SI3D_MIXED_IR or SI3D_MIXED_MG */
 } si3d_params;
 
 /* Per-call statistics (one entry per zeta solve inside the call). */

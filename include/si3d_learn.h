@@ -36,7 +36,9 @@ extern "C" {
 
 /* ---------------------------------------------------------------- use inside the time step */
 /* Load network parameters (host FP32, SI3D_NET_NPARAM values) into a solver handle.  With
- * x0_mode = SI3D_X0_LEARNED every zeta solve then starts from sp + prediction.  NULL unloads. */
+ * x0_mode = SI3D_X0_LEARNED the leapfrog solve of every step then starts from sp + prediction (the
+ * solve the network is trained on, where sp is the current zeta) and the trapezoidal solves after it
+ * from the latest solution.  NULL unloads. */
 int si3d_learn_set_params(int handle, const float* params_host);
 
 /* Record training examples: while `dev_buf` is non-NULL, every zeta solve writes one image

@@ -16,88 +16,14 @@
 
 #include "../../include/si3d_gpu.h"
 #include "common.cuh"
+#include "coop.cuh"
 #include "kernels.h"
 
 namespace si3d {
 
 namespace {
 
-constexpr int QB = 256;                       // threads per block
-constexpr long long kSpinLimit = 1LL << 26;   // polls (>= 32 ns each) before a wait gives up: > 2 s
-
-__device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
-  unsigned int v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Block-wide sums of NV values at once (fixed order); the totals are returned in v[] in every
-// thread.  sh holds 8 * NV + NV doubles.
-template <int NV>
-__device__ __forceinline__ void bsum(double (&v)[NV], double* sh) {
-#pragma unroll
-  for (int i = 0; i < NV; ++i)
-    for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
-  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
-  if (ln == 0) {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) sh[i * 8 + w] = v[i];
-  }
-  __syncthreads();
-  if (threadIdx.x < NV) {
-    double t = 0;
-#pragma unroll
-    for (int q = 0; q < QB / 32; ++q) t += sh[threadIdx.x * 8 + q];
-    sh[8 * NV + threadIdx.x] = t;
-  }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < NV; ++i) v[i] = sh[8 * NV + i];
-  __syncthreads();
-}
-
-// Totals of NV partial arrays (n entries each, arrays `stride` apart), in every thread.
-template <int NV>
-__device__ __forceinline__ void all_partials(const double* part, int n, int stride, double (&v)[NV], double* sh) {
-#pragma unroll
-  for (int i = 0; i < NV; ++i) v[i] = 0;
-  for (int j = threadIdx.x; j < n; j += QB) {
-#pragma unroll
-    for (int i = 0; i < NV; ++i) v[i] += __ldcg(part + i * stride + j);
-  }
-  bsum<NV>(v, sh);
-}
-
-// Counting grid barrier with a bounded wait.  Returns false (in every thread of the block) once
-// any block has given up.
-__device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, int* s_flag) {
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    int ok = 1;
-    const unsigned int gen = ld_acquire(&bar->gen);
-    __threadfence();
-    const unsigned int arrived = atomicAdd(&bar->count, 1u);
-    if (arrived == gridDim.x - 1) {
-      atomicExch(&bar->count, 0u);
-      __threadfence();
-      atomicAdd(&bar->gen, 1u);
-    } else {
-      long long spins = 0;
-      while (ld_acquire(&bar->gen) == gen) {
-        if (++spins > kSpinLimit || ld_acquire(&bar->abort) != 0u) { ok = 0; break; }
-        __nanosleep(32);
-      }
-    }
-    if (!ok && atomicExch(&bar->abort, 1u) == 0u) {
-      sc->ier = SI3D_ETIMEOUT;
-      sc->done = 1;
-    }
-    __threadfence();
-    *s_flag = ok;
-  }
-  __syncthreads();
-  return *s_flag != 0;
-}
+using namespace coop;
 
 // ---- adaptive eigenvalue estimates for stopping test 2: chgcon (nspcg.f:16499-16620), eigvss
 // (:17201-17240), zbrent (:32976-33160) and determ (:16926-16962), run by one thread after each new

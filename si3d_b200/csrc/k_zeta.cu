@@ -114,7 +114,8 @@ __device__ __forceinline__ bool last_block(unsigned int* counter) {
 }  // namespace
 
 // Gather the assembled system into colour order: sx, sy, rhs and the initial guess.
-__global__ void k_pcg_gather(Dev d, PcgDev P, int color, int x0_mode, const double* __restrict__ dz) {
+__global__ void k_pcg_gather(Dev d, PcgDev P, int color, int x0_mode, const double* __restrict__ dz,
+                             const double* __restrict__ hist) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const PcgColor& C = color ? P.B : P.R;
   if (i > C.n) return;
@@ -128,8 +129,15 @@ __global__ void k_pcg_gather(Dev d, PcgDev P, int color, int x0_mode, const doub
   C.sx[i] = d.s.sx[l - 1];
   C.sy[i] = d.s.sy[l - 1];
   C.rhs[i] = d.s.qq[l - 1];
-  double x0 = (x0_mode == 1) ? 0.0 : d.s.sp[l - 1];
-  if (x0_mode == 2 && dz) x0 = x0 + dz[l - 1];
+  // x0: sp (the reference), zero, sp + learned increment, s (the latest accepted solution),
+  // or s + this solve's correction one step earlier
+  double x0;
+  switch (x0_mode) {
+    case 1: x0 = 0.0; break;
+    case 3: x0 = d.s.s[l - 1]; break;
+    case 4: x0 = d.s.s[l - 1] + (hist ? hist[i] : 0.0); break;
+    default: x0 = d.s.sp[l - 1]; if (x0_mode == 2 && dz) x0 = x0 + dz[l - 1];
+  }
   C.u[i] = x0;
   C.z[i] = 0.0; C.p[i] = 0.0; C.p2[i] = 0.0; C.q[i] = 0.0;
 }
@@ -399,17 +407,23 @@ __global__ void __launch_bounds__(PB) k_pcg_apply(PcgDevT<T> P, int par, int nbl
 }
 
 // zeta back to column order: s(l) = zeta(l) (SolverSparse :2035-2040)
-__global__ void k_pcg_scatter(Dev d, PcgDev P, int color) {
+// With `hist`, also this solve's correction to the zeta it started from (s before the write), in
+// colour order, for the next step's guess of the same solve.
+__global__ void k_pcg_scatter(Dev d, PcgDev P, int color, double* __restrict__ hist) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const PcgColor& C = color ? P.B : P.R;
   if (i >= C.n) return;
-  d.s.s[C.l[i] - 1] = C.u[i];
+  const int l = C.l[i];
+  const double u = C.u[i];
+  if (hist) hist[i] = u - d.s.s[l - 1];
+  d.s.s[l - 1] = u;
 }
 
-void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, int* negpiv, cudaStream_t st) {
+void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, const double* hist, int* negpiv,
+               cudaStream_t st) {
   const int nR = P.R.n, nB = P.B.n;
-  k_pcg_gather<<<(nR + 1 + PB - 1) / PB, PB, 0, st>>>(d, P, 0, x0_mode, dz);
-  k_pcg_gather<<<(nB + 1 + PB - 1) / PB, PB, 0, st>>>(d, P, 1, x0_mode, dz);
+  k_pcg_gather<<<(nR + 1 + PB - 1) / PB, PB, 0, st>>>(d, P, 0, x0_mode, dz, hist);
+  k_pcg_gather<<<(nB + 1 + PB - 1) / PB, PB, 0, st>>>(d, P, 1, x0_mode, dz, hist ? hist + nR + 1 : nullptr);
   if (nR > 0) k_pcg_factor_red<<<(nR + PB - 1) / PB, PB, 0, st>>>(P);
   if (nB > 0) k_pcg_factor_black<<<(nB + PB - 1) / PB, PB, 0, st>>>(P, negpiv);
   if (nR > 0) k_pcg_resid0<<<(nR + PB - 1) / PB, PB, 0, st>>>(P, 0);
@@ -454,10 +468,10 @@ void pcg_record_stats(const PcgScal* sc, int ier0, int* iters_ier, double* relre
   k_pcg_stats<<<1, 1, 0, st>>>(sc, ier0, iters_ier, relres, slot);
 }
 
-void pcg_finish(const Dev& d, const PcgDev& P, cudaStream_t st) {
+void pcg_finish(const Dev& d, const PcgDev& P, double* hist, cudaStream_t st) {
   const int nR = P.R.n, nB = P.B.n;
-  if (nR > 0) k_pcg_scatter<<<(nR + PB - 1) / PB, PB, 0, st>>>(d, P, 0);
-  if (nB > 0) k_pcg_scatter<<<(nB + PB - 1) / PB, PB, 0, st>>>(d, P, 1);
+  if (nR > 0) k_pcg_scatter<<<(nR + PB - 1) / PB, PB, 0, st>>>(d, P, 0, hist);
+  if (nB > 0) k_pcg_scatter<<<(nB + PB - 1) / PB, PB, 0, st>>>(d, P, 1, hist ? hist + nR + 1 : nullptr);
 }
 
 // ------------------------------------------------------------------ iterative refinement

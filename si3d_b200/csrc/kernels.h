@@ -57,9 +57,10 @@ int momentum_init(int km1);
 void launch_momentum(const Dev& d, int ieq, const FaceMeta* meta, int ncols, const Tune& tu, cudaStream_t st);
 void launch_matcon(const Dev& d, cudaStream_t st);
 
-void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, int* negpiv, cudaStream_t st);
+void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, const double* hist, int* negpiv,
+               cudaStream_t st);
 void pcg_iteration(const PcgDev& P, int par, cudaStream_t st);
-void pcg_finish(const Dev& d, const PcgDev& P, cudaStream_t st);
+void pcg_finish(const Dev& d, const PcgDev& P, double* hist, cudaStream_t st);
 // Graph-capturable solve pieces: scalars initialised by a kernel, statistics kept on the device.
 void pcg_init_scalars(PcgScal* sc, const PcgScal& init, cudaStream_t st);
 void pcg_record_stats(const PcgScal* sc, int ier0, int* iters_ier, double* relres, int slot, cudaStream_t st);

@@ -1,0 +1,62 @@
+// Aggregation multigrid for the FP32 inner solves of iterative refinement (precision
+// SI3D_MIXED_MG).
+//
+// The zeta matrix is a mass term plus a graph Laplacian over the wet cells of the (im1, jm1)
+// grid: (A x)_l = m_l x_l + sum over the faces f of l of c_f (x_l - x_nbr).  Every level of the
+// hierarchy stores that form as an image: cell (r, c) of a rows x cols level at
+// (r + 1) * pitch + c + 1, with a zero frame (one ghost row/column before, two after) so that
+// stencils and 2 x 2 aggregates never test bounds.  Per cell: the mass, the face to the next
+// column (fc) and to the next row (fr), the inverse diagonal, the right-hand side b and the
+// iterate z.  Level 0 is the zeta system itself (row = i - 1, column = j - 1 of the wet column);
+// level k + 1 aggregates 2 x 2 cells of level k: masses add, the faces that cross between two
+// aggregates add and are scaled by one half (the scaled piecewise-constant coarse operator; the
+// unscaled Galerkin product over-weights the Laplacian of smooth modes by about two).  Land and
+// frame cells carry zero mass and faces and stay zero.
+//
+// The preconditioner is one symmetric V-cycle: red-black Gauss-Seidel (red then black) from a zero
+// guess on the way down, the residual summed over each aggregate, the coarsest level swept red,
+// black, red by one block, and on the way up the coarse correction enters through the black
+// half-sweep (black then red), so the cycle is a symmetric positive-definite operator and plain CG
+// applies.
+#pragma once
+#include "kernels.h"
+
+namespace si3d {
+
+constexpr int kMgMaxLevels = 10;
+constexpr int kMgCoarsest = 8192;   // cells of the coarsest level at most (one block sweeps it)
+// Levels at least: each level divides the face-to-mass ratio of the operator by four, and the
+// coarsest level, swept once, must be mass-dominated; 4 coarsenings bring the ratio of the 50 m,
+// 30 s, 60 m deep workloads (about 210 at the leapfrog solve) below one.
+constexpr int kMgMinLevels = 5;
+
+// x / d for 0 <= x < 2^31 as (x * m) >> p with p = 31 + ceil(log2 d), m = ceil(2^p / d).
+struct FastDiv {
+  unsigned long long m;
+  int p, d;
+};
+
+struct MgLevel {
+  int rows, cols, pitch, hw;   // hw = (cols + 1) / 2 cells of one colour per row (at most)
+  FastDiv div_cols, div_hw;
+  float *z, *b, *fc, *fr, *mass, *dinv;
+};
+
+struct MgDev {
+  int nlev = 0;
+  MgLevel lv[kMgMaxLevels];
+  float *u = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;   // level-0 CG vectors; lv[0].b is r
+  const int *pixR = nullptr, *pixB = nullptr;   // red / black node of the FP64 system -> level-0 offset
+  double* part = nullptr;   // block partials: (r, r) [nb], (r, z) black + red [2 nb], (p, q) [nb]
+  PcgScal* sc = nullptr;    // inner scalars: zeta, bnorm, itmax in; in, stptst, ier, done out
+};
+
+FastDiv fast_div(int d);
+size_t mg_level_elems(int rows, int cols);   // floats of one array of a rows x cols level
+int mg_loop_blocks(int device, int cells0, int max_per_sm);
+void mg_setup(const PcgDev& P, const MgDev& M, cudaStream_t st);        // coefficients of every level
+void mg_inner_setup(const PcgDev& P, const MgDev& M, cudaStream_t st);  // b = outer residual, u = 0
+int mg_loop(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st);
+void mg_correct(const PcgDev& P, const MgDev& M, cudaStream_t st);      // FP64 u += FP32 u
+
+}  // namespace si3d

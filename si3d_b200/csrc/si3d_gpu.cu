@@ -16,6 +16,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "learn.h"
+#include "mg.h"
 
 using namespace si3d;
 
@@ -65,6 +66,8 @@ __global__ void k_layer_to_colmajor(const double* __restrict__ src, double* __re
 }
 
 // ---------------------------------------------------------------------------- handle context
+constexpr int kHistSlots = 4;   // leapfrog, trapezoidal 1, 2, and all later trapezoidal solves
+
 struct Ctx {
   int device = 0;
   cudaStream_t st = nullptr;
@@ -81,6 +84,8 @@ struct Ctx {
   // red-black zeta system
   PcgDev pcg{};
   PcgDevF pcgf{};            // FP32 inner system of iterative refinement
+  MgDev mg{};                // aggregation hierarchy of the MG inner solves (precision SI3D_MIXED_MG)
+  int mg_blocks = 0;
   PcgScal* h_scf = nullptr;  // pinned
   int last_inner = 8;
   long long ir_outer = 0;
@@ -92,6 +97,11 @@ struct Ctx {
   int loop_blocks = 0, loop_blocks_f = 0;   // FP64 / FP32 grids of the cooperative solve
   GridBar* bar = nullptr;
   bool log_solves = false;   // SI3D_LOG_SOLVES=1: per-solve iteration counts on stderr
+  int cur_istep = 1;         // istep of the fd call in progress (1 = leapfrog, 2 = trapezoidal)
+  // solve slot within a step (0 = leapfrog, 1.. = trapezoidal iterations, clamped to kHistSlots - 1)
+  // and per slot the correction of that solve one step earlier, in colour order
+  int trap_solves = 0, hist_slot = 0;
+  double* hist = nullptr;
   // instrumentation: kernel-launch count and (optionally) per-stage device time
   long long launches = 0;
   bool prof = false;
@@ -233,6 +243,68 @@ void colour_columns(int lm, const int* lEC, const int* lWC, const int* lNC, cons
   }
 }
 
+// Aggregation hierarchy of the MG inner solves.  Level 0 is the (im1, jm1) image of the wet
+// columns, so the grid maps must describe that image: every neighbour one row (east / west) or one
+// column (north / south) away.  Levels halve both sides until one block can sweep the coarsest
+// and the coarsest is mass-dominated (kMgMinLevels).
+int build_mg(Ctx* c, const si3d_grid* g, const std::vector<int>& lr, const std::vector<int>& lb) {
+  const int lm = g->lm, lm1 = lm + 1;
+  if (!g->l2i || !g->l2j) return SI3D_EDIMS;
+  MgDev& M = c->mg;
+  int rows = c->im1, cols = c->jm1, rc = 0;
+  M.nlev = 0;
+  for (;;) {
+    MgLevel& L = M.lv[M.nlev++];
+    L.rows = rows;
+    L.cols = cols;
+    L.pitch = ((cols + 3 + 31) / 32) * 32;
+    L.hw = (cols + 1) / 2;
+    L.div_cols = fast_div(cols);
+    L.div_hw = fast_div(L.hw);
+    const size_t ne = mg_level_elems(rows, cols);
+    for (float** q : {&L.z, &L.b, &L.fc, &L.fr, &L.mass, &L.dinv}) rc |= c->alloc(q, ne);
+    if (rc) return rc;
+    if ((M.nlev >= kMgMinLevels && (long long)rows * cols <= kMgCoarsest) || M.nlev == kMgMaxLevels ||
+        (rows == 1 && cols == 1))
+      break;
+    rows = (rows + 1) / 2;
+    cols = (cols + 1) / 2;
+  }
+  const size_t n0 = mg_level_elems(c->im1, c->jm1);
+  for (float** q : {&M.u, &M.p0, &M.p1, &M.q}) rc |= c->alloc(q, n0);
+  if (rc) return rc;
+  const int pitch = M.lv[0].pitch;
+  std::vector<int> off(lm + 2, -1);
+  for (int l = 1; l <= lm; ++l) {
+    const int i = g->l2i[l - 1] - 1, j = g->l2j[l - 1] - 1;
+    if (i < 0 || i >= c->im1 || j < 0 || j >= c->jm1) return SI3D_EDIMS;
+    off[l] = (i + 1) * pitch + j + 1;
+  }
+  for (int l = 1; l <= lm; ++l) {
+    const int e = g->lEC[l - 1], w = g->lWC[l - 1], n = g->lNC[l - 1], s = g->lSC[l - 1];
+    if ((e != lm1 && off[e] != off[l] + pitch) || (w != lm1 && off[w] != off[l] - pitch) ||
+        (n != lm1 && off[n] != off[l] + 1) || (s != lm1 && off[s] != off[l] - 1))
+      return SI3D_EDIMS;
+  }
+  std::vector<int> pr(lr.size()), pb(lb.size());
+  for (size_t k = 0; k < lr.size(); ++k) pr[k] = off[lr[k]];
+  for (size_t k = 0; k < lb.size(); ++k) pb[k] = off[lb[k]];
+  int *dr = nullptr, *db = nullptr;
+  rc |= c->alloc(&dr, pr.size());
+  rc |= c->alloc(&db, pb.size());
+  if (rc) return rc;
+  if (!pr.empty()) CK(cudaMemcpy(dr, pr.data(), pr.size() * sizeof(int), cudaMemcpyHostToDevice));
+  if (!pb.empty()) CK(cudaMemcpy(db, pb.data(), pb.size() * sizeof(int), cudaMemcpyHostToDevice));
+  M.pixR = dr;
+  M.pixB = db;
+  // SI3D_MG_BLOCKS_PER_SM caps the resident blocks per SM of the MG solve (tuning)
+  const char* bps = std::getenv("SI3D_MG_BLOCKS_PER_SM");
+  c->mg_blocks = mg_loop_blocks(c->device, c->im1 * c->jm1, bps ? std::atoi(bps) : 0);
+  rc |= c->alloc(&M.part, 4 * (size_t)c->mg_blocks);
+  M.sc = c->pcgf.sc;
+  return rc;
+}
+
 int build_pcg(Ctx* c, const si3d_grid* g) {
   const int lm = g->lm, lm1 = lm + 1;
   std::vector<int> col;
@@ -319,6 +391,7 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
   F.part0 = P.part0; F.part1 = P.part1; F.part2 = P.part2; F.part3 = P.part3; F.part_n = P.part_n;
   F.hist_alpha = P.hist_alpha; F.hist_beta = P.hist_beta; F.tri = nullptr;
   CK(cudaMallocHost(&c->h_scf, sizeof(PcgScal)));
+  if (c->prm.precision == SI3D_MIXED_MG) return build_mg(c, g, lr, lb);
   return 0;
 }
 
@@ -444,13 +517,20 @@ int iterate(Ctx* c, PcgScal* dsc, PcgScal* hsc, int itmax, int predicted, F&& la
 // residual r = b - A u, its norm, the stopping test (test 5 at the caller's tolerance) and the
 // update u += e are FP64; each inner solve runs the red-black MIC-PCG on FP32 copies of the
 // coefficients, pivots and residual (dot products still accumulate in FP64) until its own
-// residual has dropped by max(1e-5, what the outer test still needs).
+// residual has dropped by max(1e-5, what the outer test still needs).  With precision
+// SI3D_MIXED_MG the inner solves are aggregation-multigrid preconditioned CG instead (k_mg.cu),
+// whose hierarchy is rebuilt from this solve's coefficients once before the first inner solve.
 int refine(Ctx* c, int* total_inner) {
   const si3d_params& p = c->prm;
   const double zeta = std::max(p.pcg_tol, 500.0 * p.srelpr);
+  const bool mg = p.precision == SI3D_MIXED_MG;
   PcgScal& H = *c->h_sc;
   int outer = 0, inner_total = 0;
   const int max_outer = 40;
+  if (mg) {
+    mg_setup(c->pcg, c->mg, c->st);
+    c->launches += 1 + c->mg.nlev;
+  }
   for (;;) {
     ir_residual(c->pcg, c->st);
     c->launches += 3;
@@ -461,7 +541,8 @@ int refine(Ctx* c, int* total_inner) {
     H.stptst = rn / bn;
     if (rn < bn * zeta) break;
     if (outer >= max_outer) { H.ier = 1; break; }
-    ir_inner_setup(c->pcg, c->pcgf, c->st);
+    if (mg) mg_inner_setup(c->pcg, c->mg, c->st);
+    else ir_inner_setup(c->pcg, c->pcgf, c->st);
     c->launches += 2;
     PcgScal fi{};
     fi.zeta = std::max(1e-5, 0.5 * zeta * bn / rn);
@@ -473,15 +554,26 @@ int refine(Ctx* c, int* total_inner) {
     fi.hist_cap = 0;
     *c->h_scf = fi;
     CK(cudaMemcpyAsync(c->pcgf.sc, c->h_scf, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
-    int rci = iterate(c, c->pcgf.sc, c->h_scf, p.pcg_itmax, c->last_inner,
-                      [&](int par) { pcg_iteration_f(c->pcgf, par, c->st); },
-                      [&] { return pcg_loop_f(c->pcgf, c->bar, c->loop_blocks_f, c->st); });
-    if (rci) return rci;
+    if (mg) {
+      if (mg_loop(c->mg, c->bar, c->mg_blocks, c->st) != 0) return cuda_fail(cudaGetLastError(), "mg_loop", __LINE__);
+      c->launches += 1;
+      CK(cudaMemcpyAsync(c->h_scf, c->pcgf.sc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      if (!c->h_scf->done || c->h_scf->ier == SI3D_ETIMEOUT) return SI3D_ETIMEOUT;
+      if (c->h_scf->ier < 0) { H.ier = c->h_scf->ier; break; }   // inner breakdown: report it
+    } else {
+      int rci = iterate(c, c->pcgf.sc, c->h_scf, p.pcg_itmax, c->last_inner,
+                        [&](int par) { pcg_iteration_f(c->pcgf, par, c->st); },
+                        [&] { return pcg_loop_f(c->pcgf, c->bar, c->loop_blocks_f, c->st); });
+      if (rci) return rci;
+    }
     const int its = c->h_scf->in;
-    if (c->log_solves) std::fprintf(stderr, "si3d: inner FP32 solve %d: %d iterations\n", outer + 1, its);
+    if (c->log_solves)
+      std::fprintf(stderr, "si3d: inner FP32 %s solve %d: %d iterations\n", mg ? "MG" : "MIC", outer + 1, its);
     inner_total += its;
     c->last_inner = std::max(its, 1);
-    ir_correct(c->pcg, c->pcgf, c->st);
+    if (mg) mg_correct(c->pcg, c->mg, c->st);
+    else ir_correct(c->pcg, c->pcgf, c->st);
     c->launches += 2;
     ++outer;
   }
@@ -512,7 +604,10 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
     *c->h_sc = init;
     CK(cudaMemcpyAsync(c->pcg.sc, c->h_sc, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
   }
-  const bool use_net = p.x0_mode == SI3D_X0_LEARNED && c->net_loaded;
+  // The learned guess predicts the leapfrog solve (istep 1) of a step, the solve it was trained on
+  // where sp is the current zeta; the trapezoidal solves that follow start from the latest solution.
+  const bool learned_step = p.x0_mode == SI3D_X0_LEARNED && c->cur_istep == 1;
+  const bool use_net = learned_step && c->net_loaded;
   if (use_net || c->rec_buf) {
     // features of this system; with the network loaded, the predicted increment into dz
     int rcl = stage(c, ST_LEARN, use_net ? 9 : 3, [&] {
@@ -525,13 +620,19 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
     if (rcl) return rcl;
     if (use_net) c->dz_set = true;
   }
-  const int x0 = (p.x0_mode == SI3D_X0_LEARNED && !c->dz_set) ? SI3D_X0_PREV : p.x0_mode;
-  int rc0 = stage(c, ST_PCG_SETUP, 7, [&] { pcg_setup(c->d, c->pcg, x0, c->dz, &c->pcg.sc->negpiv, c->st); });
+  int x0 = p.x0_mode;
+  if (p.x0_mode == SI3D_X0_LEARNED) {
+    if (!learned_step && c->net_loaded) x0 = SI3D_X0_LAST;
+    else if (!c->dz_set) x0 = SI3D_X0_PREV;
+  }
+  const bool use_hist = p.x0_mode == SI3D_X0_HIST;
+  double* hist = use_hist ? c->hist + (size_t)c->hist_slot * (c->pcg.R.n + c->pcg.B.n + 2) : nullptr;
+  int rc0 = stage(c, ST_PCG_SETUP, 7, [&] { pcg_setup(c->d, c->pcg, x0, c->dz, hist, &c->pcg.sc->negpiv, c->st); });
   if (rc0) return rc0;
   if (c->graph_mode) {
     if (pcg_loop(c->pcg, c->bar, c->loop_blocks, c->prm.pcg_test == 2, c->st) != 0) return cuda_fail(cudaGetLastError(), "pcg_loop", __LINE__);
     c->launches += 1;
-    rc0 = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, c->st); });
+    rc0 = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, hist, c->st); });
     if (rc0) return rc0;
     pcg_record_stats(c->pcg.sc, ier, c->d_stats_ii, c->d_stats_rr, std::min(c->solve_slot, 23), c->st);
     c->launches += 1;
@@ -543,7 +644,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   }
   if (c->prof) CK(cudaEventRecord(c->pe0, c->st));
   int total_iters = 0;
-  if (p.precision == SI3D_MIXED_IR) {
+  if (p.precision == SI3D_MIXED_IR || p.precision == SI3D_MIXED_MG) {
     int rcir = refine(c, &total_iters);
     if (rcir) return rcir;
   } else {
@@ -564,7 +665,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
     c->prof_ms[ST_PCG_ITER] += ms;
     c->prof_n[ST_PCG_ITER] += total_iters;
   }
-  rc0 = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, c->st); });
+  rc0 = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, hist, c->st); });
   if (rc0) return rc0;
   if (c->rec_buf) {
     float* slot = c->rec_buf + (size_t)(c->rec_count % c->rec_slots) * c->im1 * c->jm1 * 5;
@@ -585,6 +686,9 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
 int fd_impl(Ctx* c, int istep, si3d_step_stats* st) {
   Dev& d = c->d;
   d.tz = 1.0 / istep;
+  c->cur_istep = istep;
+  if (istep == 1) c->trap_solves = 0;
+  c->hist_slot = istep == 1 ? 0 : std::min(++c->trap_solves, kHistSlots - 1);
   // surfbc CASE(0) is a constant per-column wind set by the host (uair/vair/cdw fields)
   int rc = stage(c, ST_MOMX, 2, [&] { launch_momentum(d, 1, c->mce, c->nce, c->tune, c->st); });
   if (!rc) rc = stage(c, ST_MOMY, 2, [&] { launch_momentum(d, 2, c->mcn, c->ncn, c->tune, c->st); });
@@ -650,6 +754,9 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
   if (!g || !prm || !handle) return SI3D_EDIMS;
   if (g->lm < 1 || g->km1 < 3 || g->km1 > SI3D_MAXK || g->k1 != 2) return SI3D_EDIMS;
   if (prm->itrmom != 1 || prm->ihd > 1 || prm->pcg_itmax < 1 || (prm->pcg_test != 5 && prm->pcg_test != 2))
+    return SI3D_EDIMS;
+  if (prm->x0_mode < SI3D_X0_PREV || prm->x0_mode > SI3D_X0_HIST) return SI3D_EDIMS;
+  if (prm->precision != SI3D_FP64 && prm->precision != SI3D_MIXED_IR && prm->precision != SI3D_MIXED_MG)
     return SI3D_EDIMS;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device) return SI3D_ENODEV;
@@ -793,6 +900,7 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
     if (!mn.empty()) cudaMemcpy(c->mcn, mn.data(), mn.size() * sizeof(FaceMeta), cudaMemcpyHostToDevice);
   }
   rc = build_pcg(c, g);
+  if (!rc) rc = c->alloc(&c->hist, (size_t)kHistSlots * (c->pcg.R.n + c->pcg.B.n + 2));
   if (rc) { delete c; return rc; }
   if (cudaDeviceSynchronize() != cudaSuccess) { delete c; return SI3D_ECUDA; }
   std::lock_guard<std::mutex> lk(g_mu);
@@ -1035,6 +1143,7 @@ int si3d_gpu_save(int h, int istep) {
   if (istep != 1 && istep != 2) return SI3D_EDIMS;
   CK(cudaSetDevice(c->device));
   launch_save(c->d, istep, c->st);
+  c->trap_solves = 0;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
   return 0;
@@ -1044,6 +1153,7 @@ int si3d_gpu_save(int h, int istep) {
 // The stage sequence of one time step n (si3d.f90:324-458): leapfrog fd, settrap, niter
 // trapezoidal fd/settrap2 iterations, save.  Enqueues only; the caller synchronises.
 static int step_impl(Ctx* c, int n, si3d_step_stats* st) {
+  c->trap_solves = 0;
   if (st) { std::memset(st, 0, sizeof(*st)); CK(cudaEventRecord(c->ev0, c->st)); }
   const si3d_params& p = c->prm;
   int niter1 = p.niter;

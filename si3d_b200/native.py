@@ -14,8 +14,9 @@ _LIBDIR = os.path.join(_HERE, "_lib")
 
 SI3D_FP64 = 0
 SI3D_MIXED_IR = 1
+SI3D_MIXED_MG = 2
 SI3D_ORDER_REDBLACK = 1
-SI3D_X0_PREV, SI3D_X0_ZERO, SI3D_X0_LEARNED = 0, 1, 2
+SI3D_X0_PREV, SI3D_X0_ZERO, SI3D_X0_LEARNED, SI3D_X0_LAST, SI3D_X0_HIST = 0, 1, 2, 3, 4
 
 
 class Si3dError(RuntimeError):

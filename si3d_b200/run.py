@@ -22,7 +22,9 @@ def main(argv=None) -> int:
     src.add_argument("--run-dir")
     src.add_argument("--workload", help="synthetic workload name (c0, c1, c2, t0, t1, m1, p2)")
     ap.add_argument("--steps", type=int, default=1)
-    ap.add_argument("--precision", choices=["fp64", "mixed"], default="fp64")
+    ap.add_argument("--precision", choices=["fp64", "mixed", "mg"], default="fp64",
+                    help="fp64: plain FP64 MIC-PCG; mixed: FP32 MIC-PCG inside FP64 refinement; "
+                         "mg: FP32 multigrid-preconditioned CG inside FP64 refinement")
     ap.add_argument("--itmax", type=int, default=2000)
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args(argv)
@@ -37,7 +39,7 @@ def main(argv=None) -> int:
         if not os.path.exists(marker):
             synth.make(args.workload, run_dir)
             open(marker, "w").close()
-    prec = native.SI3D_MIXED_IR if args.precision == "mixed" else native.SI3D_FP64
+    prec = {"fp64": native.SI3D_FP64, "mixed": native.SI3D_MIXED_IR, "mg": native.SI3D_MIXED_MG}[args.precision]
     run = GpuRun(run_dir, device=args.device, pcg_itmax=args.itmax, precision=prec)
     try:
         for _ in range(args.steps):

@@ -135,12 +135,13 @@ def test_recorder_writes_features_and_target(native_libs, run_dirs, oracle_lib):
 
 
 def test_untrained_network_is_the_plain_guess(native_libs, run_dirs):
-    """The initialisation zeroes the head, so before training the learned guess equals sp and the
-    solve is the plain one, iteration for iteration."""
+    """The initialisation zeroes the head, so before training the learned guess is sp on the leapfrog
+    solves (where sp is the latest solution) and the latest solution on the others: the solves are
+    those of x0 = SI3D_X0_LAST, iteration for iteration."""
     from si3d_b200 import native
     from si3d_b200.learn import init_params, iterations
     d = run_dirs["t1"]
-    a = iterations(d, 4, params=None, x0_mode=native.SI3D_X0_PREV, precision=native.SI3D_FP64)
+    a = iterations(d, 4, params=None, x0_mode=native.SI3D_X0_LAST, precision=native.SI3D_FP64)
     b = iterations(d, 4, params=init_params(0), x0_mode=native.SI3D_X0_LEARNED, precision=native.SI3D_FP64)
     assert a["iters"] == b["iters"]
     assert np.abs(a["zeta"] - b["zeta"]).max() <= 1e-12

@@ -1,17 +1,19 @@
-"""Mixed-precision form: FP32 MIC-PCG inner solves inside FP64 iterative refinement, through the
-C ABI, against the FP64 oracle.  The stopping test stays test 5 at 1e-12 on the FP64 residual."""
+"""Mixed-precision forms: FP32 inner solves (MIC-PCG, or aggregation-multigrid PCG) inside FP64
+iterative refinement, through the C ABI, against the FP64 oracle.  The stopping test stays test 5 at
+1e-12 on the FP64 residual."""
 import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name,steps", [("t1", 30), ("c0", 30)])
-def test_mixed_ir_matches_fp64_oracle(run_dirs, oracle_lib, native_libs, name, steps):
+@pytest.mark.parametrize("precision", ["MIXED_IR", "MIXED_MG"])
+@pytest.mark.parametrize("name,steps", [("t0", 30), ("t1", 30), ("c0", 30)])
+def test_mixed_ir_matches_fp64_oracle(run_dirs, oracle_lib, native_libs, name, steps, precision):
     from si3d_b200 import native
     from si3d_b200.model import GpuRun
     o = oracle_lib.OracleRun(run_dirs[name], ordering=1, pcg_itmax=2000)
-    g = GpuRun(run_dirs[name], pcg_itmax=2000, precision=native.SI3D_MIXED_IR)
+    g = GpuRun(run_dirs[name], pcg_itmax=2000, precision=getattr(native, f"SI3D_{precision}"))
     o.run(steps)
     st = g.run(steps)
     relres = [s.relres[i] for s in st for i in range(s.nsolves)]
@@ -45,3 +47,31 @@ def test_mixed_standalone_solve(run_dirs, oracle_lib, native_libs):
     x_g, r_g = solve_zeta(coef, jco, qq[:lm], sp[:lm], itmax=2000, precision=native.SI3D_MIXED_IR)
     assert r_g["stptst"] < 1e-12
     assert np.abs(x_g - x_o).max() <= 1e-10 * max(np.abs(x_o).max(), 1e-3)
+
+
+def test_multigrid_inner_solves_need_few_iterations(run_dirs, native_libs):
+    """The multigrid V-cycle makes the inner iteration count nearly independent of the system: on
+    t1 every step's MG inner iterations stay below a quarter of the MIC inner iterations."""
+    from si3d_b200 import native
+    from si3d_b200.model import GpuRun
+    its = {}
+    for prec in ("MIXED_IR", "MIXED_MG"):
+        g = GpuRun(run_dirs["t1"], pcg_itmax=2000, precision=getattr(native, f"SI3D_{prec}"))
+        try:
+            st = g.run(10)
+            its[prec] = [s.total_iters for s in st]
+        finally:
+            g.close()
+    assert all(4 * m < i for m, i in zip(its["MIXED_MG"], its["MIXED_IR"])), its
+
+
+def test_multigrid_needs_the_grid_image():
+    """Without the (i, j) maps the hierarchy cannot be built: the standalone solve refuses the MG
+    form instead of falling back to another solver."""
+    import numpy as np
+    from si3d_b200 import native
+    from si3d_b200.model import solve_zeta
+    coef = np.array([[4.0, -1.0, 0, 0, 0], [4.0, 0, 0, 0, -1.0]])
+    jco = np.array([[1, 2, 0, 0, 0], [2, 0, 0, 0, 1]], dtype=np.int32)
+    with pytest.raises(Exception):
+        solve_zeta(coef, jco, np.ones(2), np.zeros(2), itmax=50, precision=native.SI3D_MIXED_MG)

@@ -179,3 +179,29 @@ def test_stopping_test_2_steps_match_oracle(native_libs, oracle_lib, run_dirs):
         assert np.abs(run.get("s")[:run.lm] - s_o).max() <= 1e-6 * max(np.abs(s_o).max(), 1e-3)
     finally:
         run.close()
+
+
+@pytest.mark.parametrize("x0", ["LAST", "HIST"])
+@pytest.mark.parametrize("precision", ["FP64", "MIXED_IR"])
+def test_initial_guess_modes_match_oracle(run_dirs, oracle_lib, native_libs, x0, precision):
+    """The initial guess changes where each CG solve starts, not the system it solves: 30 steps with
+    x0 = the latest solution (LAST) or the latest solution plus the same solve's correction one step
+    earlier (HIST) stay within the plain tolerances of the oracle's sp-started run."""
+    from si3d_b200 import native
+    from si3d_b200.model import GpuRun
+    o = oracle_lib.OracleRun(run_dirs["t1"], ordering=1, pcg_itmax=2000)
+    g = GpuRun(run_dirs["t1"], pcg_itmax=2000, x0_mode=getattr(native, f"SI3D_X0_{x0}"),
+               precision=getattr(native, f"SI3D_{precision}"))
+    try:
+        o.run(30)
+        st = g.run(30)
+        assert all(s.ier[i] == 0 for s in st for i in range(s.nsolves))
+        assert max(s.relres[i] for s in st for i in range(s.nsolves)) < 1e-12
+        ds = np.abs(o.get("s") - g.get("s")).max()
+        assert ds <= 1e-9, f"max |dzeta| {ds:.3e} m"
+        for f, tol in (("uh", 1e-8), ("vh", 1e-8), ("sal", 1e-10)):
+            a, b = o.get(f), g.get(f)
+            err = np.abs(a - b).max() / max(np.abs(a).max(), 1e-300)
+            assert err <= tol, f"{x0}/{precision}:{f} rel err {err:.3e}"
+    finally:
+        g.close()
