@@ -30,11 +30,11 @@ constexpr int CW = 32;   // face columns per block of the cell kernel (layer lan
 
 // Horizontal-diffusion coefficient of a neighbouring face column m at layer k
 // (haxpp/haypp as rebuilt by exmom each call, :623-681 / :962-1018): zero outside that
-// column's wet face layers or when its face is closed.
-__device__ __forceinline__ double face_coef(const Dev& d, const double* hpp3, double A, int m, int kfirst,
-                                            int klast, int other, int k) {
-  if (m == d.g.lm1 || k < kfirst || k > klast) return 0.0;
-  return A * fmin(hpp3[IX(d, k, other)], hpp3[IX(d, k, m)]);
+// column's wet face layers or when its face is closed.  The two depths are loaded by the caller
+// unconditionally (m = lm1 is the dry column, a valid address), so the test only selects.
+__device__ __forceinline__ double face_coef(const Dev& d, double A, double h_other, double h_m, int m, int kfirst,
+                                            int klast, int k) {
+  return (m == d.g.lm1 || k < kfirst || k > klast) ? 0.0 : A * fmin(h_other, h_m);
 }
 
 struct FaceCol {
@@ -43,7 +43,7 @@ struct FaceCol {
 
 // ------------------------------------------------------------------ cell kernel
 template <int IEQ, int CL>
-__global__ void __launch_bounds__(CW * CL, 1024 / (CW * CL)) k_mom_cells(Dev d, const FaceMeta* __restrict__ meta, int ncols) {
+__global__ void __launch_bounds__(CW * CL, 768 / (CW * CL)) k_mom_cells(Dev d, const FaceMeta* __restrict__ meta, int ncols) {
   const int t = blockIdx.x * CW + threadIdx.x;
   if (t >= ncols) return;
   const bool X = (IEQ == 1);
@@ -66,62 +66,73 @@ __global__ void __launch_bounds__(CW * CL, 1024 / (CW * CL)) k_mom_cells(Dev d, 
   double* arA = X ? d.f.arx : d.f.ary;
   const double twodt1 = d.p.twodt * d.tz;
   const double gdt = X ? d.p.gdtdx : d.p.gdtdy;
+  const double* __restrict__ vhp = d.f.vhp;
+  const double* __restrict__ uhp = d.f.uhp;
+  const double* __restrict__ wp = d.f.wp;
+  const double* __restrict__ hp3 = d.f.hp;
+  const int P = d.g.P;
+  const int dE = lE - l, dW = lW - l, dN = lN - l, dS = lS - l, dX2 = lX2 - l, dO = lO - l;
   for (int k = k1x + threadIdx.y; k <= kmx; k += CL) {
     const int ik = IX(d, k, l);
+    // every input of the explicit term is loaded before the dry-cell test, so a layer costs one
+    // memory round trip; the arithmetic below is the reference's, term by term
     const double hk = huv[ik];
-    const double hkm = huv[IX(d, k - 1, l)];
-    const double hkp = huv[IX(d, k + 1, l)];
-    // ---- explicit term (exmom)
+    const double hkm = huv[ik - P];
+    const double hkp = huv[ik + P];
+    const double hpl = hp3[ik], hpo = hp3[ik + dO];
+    double cor, uE, uW, vN, vS, wU, wD;
+    if (X) {
+      const double vE = vhp[ik + dE], vC = vhp[ik], vX = vhp[ik + dX2], vSS = vhp[ik + dS];
+      const double uEE = uhp[ik + dE], uC = uhp[ik], uWW = uhp[ik + dW];
+      cor = 0.25 * d.p.f * (vE + vC + vX + vSS);
+      uE = uEE + uC;
+      uW = uC + uWW;
+      vN = vE + vC;
+      vS = vX + vSS;
+      wU = wp[ik + dE] + wp[ik];
+      wD = wp[ik + P + dE] + wp[ik + P];
+    } else {
+      const double uN = uhp[ik + dN], uC = uhp[ik], uX = uhp[ik + dX2], uWW = uhp[ik + dW];
+      const double vNN = vhp[ik + dN], vC = vhp[ik], vSS = vhp[ik + dS];
+      cor = 0.25 * d.p.f * (uN + uC + uX + uWW);
+      uE = uN + uC;
+      uW = uX + uWW;
+      vN = vNN + vC;
+      vS = vC + vSS;
+      wU = wp[ik + dN] + wp[ik];
+      wD = wp[ik + P + dN] + wp[ik + P];
+    }
+    const double uc = uvp[ik];
+    const double uvE = uvp[ik + dE], uvW = uvp[ik + dW], uvN = uvp[ik + dN], uvS = uvp[ik + dS];
+    const double uvU = uvp[ik - P], uvD = uvp[ik + P];
+    const double own_pp = uvpp_h[ik];
+    double hd = 0.0;
+    if (d.p.ihd == 1) {
+      const double hppl = huvpp[ik], hppE = huvpp[ik + dE], hppN = huvpp[ik + dN];
+      const double hppW = huvpp[ik + dW], hppS = huvpp[ik + dS];
+      const double pc = uvpp[ik], pN = uvpp[ik + dN], pS = uvpp[ik + dS], pE = uvpp[ik + dE], pW = uvpp[ik + dW];
+      const double ax_l = d.p.Ax0 * fmin(hppE, hppl);
+      const double ay_l = d.p.Ay0 * fmin(hppN, hppl);
+      const double ax_w = face_coef(d, d.p.Ax0, hppl, hppW, lW, mW_first, mW_last, k);
+      const double ay_s = face_coef(d, d.p.Ay0, hppl, hppS, lS, mS_first, mS_last, k);
+      hd = (ay_l * (pN - pc) - ay_s * (pc - pS)) / d.p.dydy + (ax_l * (pE - pc) - ax_w * (pc - pW)) / d.p.dxdx;
+    }
     double ex;
-    const double hpl = d.f.hp[ik], hpo = d.f.hp[IX(d, k, lO)];
     if (hpl <= ZERO || hpo <= ZERO) {
-      ex = uvpp_h[ik];
+      ex = own_pp;
     } else {
       const double th_k = (k == k1x) ? 0.0 : hkm / (hkm + hk);
       const double th1_k = (k == k1x) ? 0.0 : 1. - th_k;
       const double th_kp = (k == kmx) ? 0.5 : hk / (hk + hkp);
       const double th1_kp = (k == kmx) ? 0.5 : 1. - th_kp;
-      double cor, uE, uW, vN, vS, wU, wD;
-      const double* vhp = d.f.vhp;
-      const double* uhp = d.f.uhp;
-      if (X) {
-        cor = 0.25 * d.p.f * (vhp[IX(d, k, lE)] + vhp[ik] + vhp[IX(d, k, lX2)] + vhp[IX(d, k, lS)]);
-        uE = uhp[IX(d, k, lE)] + uhp[ik];
-        uW = uhp[ik] + uhp[IX(d, k, lW)];
-        vN = vhp[IX(d, k, lE)] + vhp[ik];
-        vS = vhp[IX(d, k, lX2)] + vhp[IX(d, k, lS)];
-        wU = d.f.wp[IX(d, k, lE)] + d.f.wp[ik];
-        wD = d.f.wp[IX(d, k + 1, lE)] + d.f.wp[IX(d, k + 1, l)];
-      } else {
-        cor = 0.25 * d.p.f * (uhp[IX(d, k, lN)] + uhp[ik] + uhp[IX(d, k, lX2)] + uhp[IX(d, k, lW)]);
-        uE = uhp[IX(d, k, lN)] + uhp[ik];
-        uW = uhp[IX(d, k, lX2)] + uhp[IX(d, k, lW)];
-        vN = vhp[IX(d, k, lN)] + vhp[ik];
-        vS = vhp[ik] + vhp[IX(d, k, lS)];
-        wU = d.f.wp[IX(d, k, lN)] + d.f.wp[ik];
-        wD = d.f.wp[IX(d, k + 1, lN)] + d.f.wp[IX(d, k + 1, l)];
-      }
       if (k == k1x) wU = 0.0;
       if (k == kmx) wD = 0.0;
-      const double uc = uvp[ik];
-      const double scE = uvp[IX(d, k, lE)] + uc, scW = uvp[IX(d, k, lW)] + uc;
-      const double scN = uvp[IX(d, k, lN)] + uc, scS = uvp[IX(d, k, lS)] + uc;
+      const double scE = uvE + uc, scW = uvW + uc;
+      const double scN = uvN + uc, scS = uvS + uc;
       double adv = (uE * scE - uW * scW) / d.p.fourdx + (vN * scN - vS * scS) / d.p.fourdy;
-      adv = adv + (wU * (th_k * uc + th1_k * uvp[IX(d, k - 1, l)]) -
-                   wD * (th_kp * uvp[IX(d, k + 1, l)] + th1_kp * uc)) / 2.;
-      double hd = 0.0;
-      if (d.p.ihd == 1) {
-        const double hppl = huvpp[ik];
-        const double ax_l = d.p.Ax0 * fmin(huvpp[IX(d, k, lE)], hppl);
-        const double ay_l = d.p.Ay0 * fmin(huvpp[IX(d, k, lN)], hppl);
-        const double ax_w = face_coef(d, huvpp, d.p.Ax0, lW, mW_first, mW_last, l, k);
-        const double ay_s = face_coef(d, huvpp, d.p.Ay0, lS, mS_first, mS_last, l, k);
-        const double pc = uvpp[ik];
-        hd = (ay_l * (uvpp[IX(d, k, lN)] - pc) - ay_s * (pc - uvpp[IX(d, k, lS)])) / d.p.dydy +
-             (ax_l * (uvpp[IX(d, k, lE)] - pc) - ax_w * (pc - uvpp[IX(d, k, lW)])) / d.p.dxdx;
-      }
-      if (X) ex = uvpp_h[ik] - twodt1 * (adv * d.p.iadv - cor - hd);
-      else ex = uvpp_h[ik] - twodt1 * (adv * d.p.iadv + cor - hd);
+      adv = adv + (wU * (th_k * uc + th1_k * uvU) - wD * (th_kp * uvD + th1_kp * uc)) / 2.;
+      if (X) ex = own_pp - twodt1 * (adv * d.p.iadv - cor - hd);
+      else ex = own_pp - twodt1 * (adv * d.p.iadv + cor - hd);
     }
     // ---- baroclinic increment (:1283-1301 / :1475-1491), bottom layer via bclnc_km
     double hdrho = 0;

@@ -185,6 +185,9 @@ __device__ __forceinline__ double superbee(double s1, double s2, double s3, doub
 // layer of 32 consecutive columns (coalesced) and each thread takes layers k0 + lane, k0 + lane + CLN...
 
 // exsal's three limited fluxes per cell (:2895-3013), into the persistent Bth2/Bth4/Bth3 fields.
+// Every value a layer may need is loaded before any test (all addresses are valid: neighbours are
+// real columns or the dry column lm1, and layer k - 2 is clamped to 1), so a layer costs one memory
+// round trip; the tests then only select among loaded values, in the reference's arithmetic.
 template <int CLN>
 __global__ void __launch_bounds__(32 * CLN) k_exsal_flux(Dev d) {
   const int l = blockIdx.x * 32 + threadIdx.x + 1;
@@ -193,52 +196,70 @@ __global__ void __launch_bounds__(32 * CLN) k_exsal_flux(Dev d) {
   if (k1s + (int)threadIdx.y > kms) return;
   const int lE = NB(d.g.lEC, l), lW = NB(d.g.lWC, l), lN = NB(d.g.lNC, l), lS = NB(d.g.lSC, l);
   const int lEE = NB(d.g.lEC, lE), lNN = NB(d.g.lNC, lN);
+  const int P = d.g.P;
   const double twodt1 = d.p.twodt * d.tz;
-  const double* sp = d.f.salpp;
-  const double* hpp = d.f.hpp;
-  const double* hp = d.f.hp;
+  const double* __restrict__ sp = d.f.salpp;
+  const double* __restrict__ hpp = d.f.hpp;
+  const double* __restrict__ hp = d.f.hp;
+  const double* __restrict__ hup = d.f.hup;
+  const double* __restrict__ hvp = d.f.hvp;
+  const double* __restrict__ uhpp = d.f.uhpp;
+  const double* __restrict__ uh = d.f.uh;
+  const double* __restrict__ vhpp = d.f.vhpp;
+  const double* __restrict__ vh = d.f.vh;
+  const double* __restrict__ wp = d.f.wp;
+  double* __restrict__ B2 = d.f.Bth2;
+  double* __restrict__ B3 = d.f.Bth3;
+  double* __restrict__ B4 = d.f.Bth4;
+  const int dE = lE - l, dW = lW - l, dN = lN - l, dS = lS - l, dEE = lEE - l, dNN = lNN - l;
   for (int k = k1s + threadIdx.y; k <= kms; k += CLN) {
     const int ik = IX(d, k, l);
+    const int ik2 = IX(d, k - 2 < 1 ? 1 : k - 2, l);
+    // ---- all loads of this layer
+    const double hu = hup[ik], hv = hvp[ik], hpu = hp[ik - P], hpk = hp[ik];
+    const double uo = uhpp[ik], un = uh[ik], vo = vhpp[ik], vn = vh[ik], wk = wp[ik];
+    const double s2 = sp[ik], sE = sp[ik + dE], sW = sp[ik + dW], sEE = sp[ik + dEE];
+    const double sN = sp[ik + dN], sS = sp[ik + dS], sNN = sp[ik + dNN];
+    const double sU = sp[ik - P], sUU = sp[ik2], sD = sp[ik + P];
+    const double hW = hpp[ik + dW], hEE = hpp[ik + dEE], hS = hpp[ik + dS], hNN = hpp[ik + dNN];
+    const double hUU = hpp[ik2], hD = hpp[ik + P];
     // EW
-    if (d.f.hup[ik] > ZERO) {
-      const double vel = (d.f.uhpp[ik] + d.f.uh[ik]) / 2.;
-      const double s2 = sp[ik], s3 = sp[IX(d, k, lE)];
-      const double s1 = (hpp[IX(d, k, lW)] <= ZERO) ? s2 : sp[IX(d, k, lW)];
-      const double s4 = (hpp[IX(d, k, lEE)] <= ZERO) ? s3 : sp[IX(d, k, lEE)];
+    if (hu > ZERO) {
+      const double vel = (uo + un) / 2.;
+      const double s3 = sE;
+      const double s1 = (hW <= ZERO) ? s2 : sW;
+      const double s4 = (hEE <= ZERO) ? s3 : sEE;
       const double C_f = superbee(s1, s2, s3, s4, vel, 0.0);
-      d.f.Bth2[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / d.p.dx * C_f) * (s3 - s2) / 2.;
-    } else d.f.Bth2[ik] = 0.0;
+      B2[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / d.p.dx * C_f) * (s3 - s2) / 2.;
+    } else B2[ik] = 0.0;
     // NS
-    if (d.f.hvp[ik] > ZERO) {
-      const double vel = (d.f.vhpp[ik] + d.f.vh[ik]) / 2.;
-      const double s2 = sp[ik], s3 = sp[IX(d, k, lN)];
-      const double s1 = (hpp[IX(d, k, lS)] <= ZERO) ? s2 : sp[IX(d, k, lS)];
-      const double s4 = (hpp[IX(d, k, lNN)] <= ZERO) ? s3 : sp[IX(d, k, lNN)];
+    if (hv > ZERO) {
+      const double vel = (vo + vn) / 2.;
+      const double s3 = sN;
+      const double s1 = (hS <= ZERO) ? s2 : sS;
+      const double s4 = (hNN <= ZERO) ? s3 : sNN;
       const double C_f = superbee(s1, s2, s3, s4, vel, 0.0);
-      d.f.Bth4[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / d.p.dy * C_f) * (s3 - s2) / 2.;
-    } else d.f.Bth4[ik] = 0.0;
+      B4[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / d.p.dy * C_f) * (s3 - s2) / 2.;
+    } else B4[ik] = 0.0;
     // UD (hp(1, l) is never positive, so k-2 >= 1 whenever this branch is taken)
-    if (hp[IX(d, k - 1, l)] > ZERO) {
-      double vel = d.f.wp[ik];
+    if (hpu > ZERO) {
+      double vel = wk;
       if (k == k1s) vel = 0.0;
-      const double s2 = sp[ik], s3 = sp[IX(d, k - 1, l)];
-      const double s4 = (k - 2 < 1 || hpp[IX(d, k - 2, l)] <= ZERO) ? s3 : sp[IX(d, k - 2, l)];
-      const double s1 = (hpp[IX(d, k + 1, l)] <= ZERO) ? s2 : sp[IX(d, k + 1, l)];
+      const double s3 = sU;
+      const double s4 = (k - 2 < 1 || hUU <= ZERO) ? s3 : sUU;
+      const double s1 = (hD <= ZERO) ? s2 : sD;
       const double C_f = superbee(s1, s2, s3, s4, vel, 1.0);
-      const double delz = (hp[ik] + hp[IX(d, k - 1, l)]) / 2.;
-      d.f.Bth3[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / delz * C_f) * (s3 - s2) / 2.;
-    } else d.f.Bth3[ik] = 0.0;
+      const double delz = (hpk + hpu) / 2.;
+      B3[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / delz * C_f) * (s3 - s2) / 2.;
+    } else B3[ik] = 0.0;
   }
 }
 
-// Horizontal-diffusion coefficient Bhaxpp/Bhaypp of column m at layer k (:2867-2877).
-__device__ __forceinline__ double bha(const Dev& d, const double* hvpp, double A, int m, int k) {
-  if (m == d.g.lm1 || k < d.g.k1 || k > NB(d.g.kmz, m)) return 0.0;
-  return A * hvpp[IX(d, k, m)];
-}
-
 // exsal's divergence Bex plus the heat source (imsal's right-hand side ds, :3059-3065, :3113) per
-// cell, staged in sal (which imsal then overwrites with the solution in place).
+// cell, staged in sal (which imsal then overwrites with the solution in place).  The horizontal-
+// diffusion coefficients Bhaxpp/Bhaypp of a column m at layer k (:2867-2877) are A * hupp (hvpp)
+// inside m's wet layers [k1, kmz(m)] and zero elsewhere or for the dry column; as in the flux kernel
+// every value is loaded before the tests select among them.
 template <int CLN>
 __global__ void __launch_bounds__(32 * CLN) k_exsal_rhs(Dev d) {
   const int l = blockIdx.x * 32 + threadIdx.x + 1;
@@ -246,21 +267,41 @@ __global__ void __launch_bounds__(32 * CLN) k_exsal_rhs(Dev d) {
   const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
   if (k1s + (int)threadIdx.y > kms) return;
   const int lE = NB(d.g.lEC, l), lW = NB(d.g.lWC, l), lN = NB(d.g.lNC, l), lS = NB(d.g.lSC, l);
+  const int lm1 = d.g.lm1, k1 = d.g.k1;
+  const int kmW = NB(d.g.kmz, lW), kmS = NB(d.g.kmz, lS);
+  const int P = d.g.P;
   const double twodt1 = d.p.twodt * d.tz;
-  const double* sp = d.f.salpp;
+  const double* __restrict__ sp = d.f.salpp;
+  const double* __restrict__ hpp = d.f.hpp;
+  const double* __restrict__ B2 = d.f.Bth2;
+  const double* __restrict__ B3 = d.f.Bth3;
+  const double* __restrict__ B4 = d.f.Bth4;
+  const double* __restrict__ hupp = d.f.hupp;
+  const double* __restrict__ hvpp = d.f.hvpp;
+  const double* __restrict__ heat = d.f.HeatSource;
+  double* __restrict__ sal = d.f.sal;
+  const bool ihd = d.p.ihd > 0;
+  const int dE = lE - l, dW = lW - l, dN = lN - l, dS = lS - l;
   for (int k = k1s + threadIdx.y; k <= kms; k += CLN) {
     const int ik = IX(d, k, l);
-    const double spc = sp[ik];
-    double v = d.f.hpp[ik] * spc / twodt1 - (d.f.Bth2[ik] - d.f.Bth2[IX(d, k, lW)]) / d.p.dx -
-               (d.f.Bth4[ik] - d.f.Bth4[IX(d, k, lS)]) / d.p.dy - (d.f.Bth3[ik] - d.f.Bth3[IX(d, k + 1, l)]);
-    if (d.p.ihd > 0) {
-      const double hd = (bha(d, d.f.hupp, d.p.Ax0, l, k) * (sp[IX(d, k, lE)] - spc) -
-                         bha(d, d.f.hupp, d.p.Ax0, lW, k) * (spc - sp[IX(d, k, lW)])) / d.p.dxdx +
-                        (bha(d, d.f.hvpp, d.p.Ay0, l, k) * (sp[IX(d, k, lN)] - spc) -
-                         bha(d, d.f.hvpp, d.p.Ay0, lS, k) * (spc - sp[IX(d, k, lS)])) / d.p.dydy;
+    const double spc = sp[ik], hc = hpp[ik], b2 = B2[ik], b2W = B2[ik + dW], b4 = B4[ik], b4S = B4[ik + dS];
+    const double b3 = B3[ik], b3D = B3[ik + P], hs = heat[ik];
+    double sE = 0, sW = 0, sN = 0, sS = 0, axl = 0, axW = 0, ayl = 0, ayS = 0;
+    if (ihd) {
+      sE = sp[ik + dE]; sW = sp[ik + dW]; sN = sp[ik + dN]; sS = sp[ik + dS];
+      axl = hupp[ik]; axW = hupp[ik + dW]; ayl = hvpp[ik]; ayS = hvpp[ik + dS];
+    }
+    double v = hc * spc / twodt1 - (b2 - b2W) / d.p.dx - (b4 - b4S) / d.p.dy - (b3 - b3D);
+    if (ihd) {
+      const bool inl = k >= k1 && k <= kms;
+      const double bxl = inl ? d.p.Ax0 * axl : 0.0;
+      const double bxW = (lW != lm1 && k >= k1 && k <= kmW) ? d.p.Ax0 * axW : 0.0;
+      const double byl = inl ? d.p.Ay0 * ayl : 0.0;
+      const double byS = (lS != lm1 && k >= k1 && k <= kmS) ? d.p.Ay0 * ayS : 0.0;
+      const double hd = (bxl * (sE - spc) - bxW * (spc - sW)) / d.p.dxdx + (byl * (sN - spc) - byS * (spc - sS)) / d.p.dydy;
       v = v + hd;
     }
-    d.f.sal[ik] = v + d.f.HeatSource[ik];
+    sal[ik] = v + hs;
   }
 }
 
