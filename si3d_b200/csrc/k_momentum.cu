@@ -192,6 +192,7 @@ __global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceM
   const double gdt = X ? d.p.gdtdx : d.p.gdtdy;
   // depth-mean density (:1277 / :1470)
   double rsum = 0;
+#pragma unroll 4
   for (int k = k1x; k <= kmx; ++k) rsum += 1000 + d.f.rhop[IX(d, k, l)];
   const double rhopx = rsum / nw;
   const double ws0 = rhopx * gdt * (d.s.spp[lO - 1] - d.s.spp[l - 1]);
@@ -286,6 +287,7 @@ __global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceM
   }
   // back substitution, then the depth sums in ascending order
   double d2 = d1p, e2 = e1p;
+#pragma unroll 4
   for (int k = kmx - 1; k >= k1x; --k) {
     const int ik = IX(d, k, l);
     const double c = cc[ik];
@@ -294,7 +296,9 @@ __global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceM
     agA[ik] = d2; arA[ik] = e2;
   }
   double sg = 0, sr = 0;
+#pragma unroll 4
   for (int k = k1x; k <= kmx; ++k) sg += agA[IX(d, k, l)];
+#pragma unroll 4
   for (int k = k1x; k <= kmx; ++k) sr += arA[IX(d, k, l)];
   if (X) { d.s.eagx[l - 1] = sg; d.s.earx[l - 1] = sr; }
   else { d.s.eagy[l - 1] = sg; d.s.eary[l - 1] = sr; }

@@ -37,18 +37,30 @@ __device__ __forceinline__ int vlim(const Dev& d, int l) {
 
 // ------------------------------------------------------------- slayer_h
 __global__ void k_slayer_h(Dev d) {
+  double* __restrict__ f_h = d.f.h;
+  double* __restrict__ f_hp = d.f.hp;
+  double* __restrict__ f_hu = d.f.hu;
+  double* __restrict__ f_hup = d.f.hup;
+  double* __restrict__ f_hv = d.f.hv;
+  double* __restrict__ f_hvp = d.f.hvp;
   const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (l > d.g.lm) return;
   const int km1 = d.g.km1;
   const int kz = d.s.k1z[l - 1], ku = d.s.k1u[l - 1], kv = d.s.k1v[l - 1];
-  double* h = d.f.h; double* hu = d.f.hu; double* hv = d.f.hv;
-  const double* hp = d.f.hp; const double* hup = d.f.hup; const double* hvp = d.f.hvp;
+  double* __restrict__ h = f_h; double* __restrict__ hu = f_hu; double* __restrict__ hv = f_hv;
+  const double* __restrict__ hp = f_hp; const double* __restrict__ hup = f_hup; const double* __restrict__ hvp = f_hvp;
   const int zL = zlim(d, l), uL = ulim(d, l), vL = vlim(d, l);
+  #pragma unroll 4
   for (int k = 1; k <= min(kz - 1, zL); ++k) h[IX(d, k, l)] = hp[IX(d, k, l)];
+  #pragma unroll 4
   for (int k = 1; k <= min(ku - 1, uL); ++k) hu[IX(d, k, l)] = hup[IX(d, k, l)];
+  #pragma unroll 4
   for (int k = 1; k <= min(kv - 1, vL); ++k) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
+  #pragma unroll 4
   for (int k = kz + 2; k <= zL; ++k) h[IX(d, k, l)] = hp[IX(d, k, l)];
+  #pragma unroll 4
   for (int k = ku + 1; k <= uL; ++k) hu[IX(d, k, l)] = hup[IX(d, k, l)];
+  #pragma unroll 4
   for (int k = kv + 2; k <= vL; ++k) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
   // Surface layers.  A column whose surface index has reached the bottom level (every layer
   // dry) is left untouched: the reference would read zlevel past km1 there.
@@ -93,6 +105,14 @@ __global__ void k_slayer_h(Dev d) {
 // ------------------------------------------------------------- vel (uh, vh, k1u, k1v)
 template <int IEQ>
 __global__ void k_vel_uv(Dev d, const int* __restrict__ cols, int ncols) {
+  double* __restrict__ f_agx = d.f.agx;
+  double* __restrict__ f_agy = d.f.agy;
+  double* __restrict__ f_arx = d.f.arx;
+  double* __restrict__ f_ary = d.f.ary;
+  double* __restrict__ f_hu = d.f.hu;
+  double* __restrict__ f_hv = d.f.hv;
+  double* __restrict__ f_uh = d.f.uh;
+  double* __restrict__ f_vh = d.f.vh;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= ncols) return;
   const int l = cols[t];
@@ -103,11 +123,12 @@ __global__ void k_vel_uv(Dev d, const int* __restrict__ cols, int ncols) {
   const int k0 = k1[l - 1];
   const double gth = (X ? d.p.gdtdx : d.p.gdtdy) * d.tz;
   const double c = gth * 1000. * (d.s.s[lO - 1] - d.s.s[l - 1]);
-  double* uv = X ? d.f.uh : d.f.vh;
-  const double* ag = X ? d.f.agx : d.f.agy;
-  const double* ar = X ? d.f.arx : d.f.ary;
+  double* uv = X ? f_uh : f_vh;
+  const double* ag = X ? f_agx : f_agy;
+  const double* ar = X ? f_arx : f_ary;
+  #pragma unroll 4
   for (int k = k0; k <= kmx; ++k) uv[IX(d, k, l)] = ag[IX(d, k, l)] - c * ar[IX(d, k, l)];
-  const double* huv = X ? d.f.hu : d.f.hv;
+  const double* huv = X ? f_hu : f_hv;
   // (a face column with every layer dry, k0 = km1, is never reached: the reference would write
   //  past the last level there)
   if (k0 < d.g.km1 && huv[IX(d, k0, l)] <= ZERO) {
@@ -378,53 +399,61 @@ __global__ void __launch_bounds__(NTB) k_imsal(Dev d) {
 
 // ------------------------------------------------------------- vel2 (layer_h + wetting)
 __global__ void k_vel2(Dev d) {
+  double* __restrict__ f_h = d.f.h;
+  double* __restrict__ f_hu = d.f.hu;
+  double* __restrict__ f_hv = d.f.hv;
+  double* __restrict__ f_uh = d.f.uh;
+  double* __restrict__ f_vh = d.f.vh;
   const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (l > d.g.lm) return;
   const int kms = NB(d.g.kmz, l);
   const double sl = d.s.s[l - 1];
+  #pragma unroll 4
   for (int k = d.g.k1; k <= kms; ++k) {
     double v = fmin(zl(d, k + 1), d.g.hhs[l - 1]) - fmax(zl(d, k), -sl);
     if (v <= HMIN) v = ZERO;
-    d.f.h[IX(d, k, l)] = v;
+    f_h[IX(d, k, l)] = v;
   }
   if (ewet(d, l)) {
     const int lE = NB(d.g.lEC, l);
     const int kmx = min(kms, NB(d.g.kmz, lE));
     const double sm = fmax(sl, d.s.s[lE - 1]);
+    #pragma unroll 4
     for (int k = d.g.k1; k <= kmx; ++k) {
       double v = fmin(zl(d, k + 1), d.g.hhu[l - 1]) - fmax(zl(d, k), -sm);
       if (v <= HMIN) v = ZERO;
-      d.f.hu[IX(d, k, l)] = v;
+      f_hu[IX(d, k, l)] = v;
     }
   }
   if (nwet(d, l)) {
     const int lN = NB(d.g.lNC, l);
     const int kmy = min(kms, NB(d.g.kmz, lN));
     const double sm = fmax(sl, d.s.s[lN - 1]);
+    #pragma unroll 4
     for (int k = d.g.k1; k <= kmy; ++k) {
       double v = fmin(zl(d, k + 1), d.g.hhv[l - 1]) - fmax(zl(d, k), -sm);
       if (v <= HMIN) v = ZERO;
-      d.f.hv[IX(d, k, l)] = v;
+      f_hv[IX(d, k, l)] = v;
     }
   }
   if (ewet(d, l)) {
     const int k = d.s.k1u[l - 1];
-    const double hkm = d.f.hu[IX(d, k - 1, l)];
+    const double hkm = f_hu[IX(d, k - 1, l)];
     if (hkm > ZERO) {
-      const double hk = d.f.hu[IX(d, k, l)];
-      const double ut = d.f.uh[IX(d, k, l)] / (hk + hkm);
-      d.f.uh[IX(d, k, l)] = ut * hk;
-      d.f.uh[IX(d, k - 1, l)] = ut * hkm;
+      const double hk = f_hu[IX(d, k, l)];
+      const double ut = f_uh[IX(d, k, l)] / (hk + hkm);
+      f_uh[IX(d, k, l)] = ut * hk;
+      f_uh[IX(d, k - 1, l)] = ut * hkm;
     }
   }
   if (nwet(d, l)) {
     const int k = d.s.k1v[l - 1];
-    const double hkm = d.f.hv[IX(d, k - 1, l)];
+    const double hkm = f_hv[IX(d, k - 1, l)];
     if (hkm > ZERO) {
-      const double hk = d.f.hv[IX(d, k, l)];
-      const double vt = d.f.vh[IX(d, k, l)] / (hk + hkm);
-      d.f.vh[IX(d, k, l)] = vt * hk;
-      d.f.vh[IX(d, k - 1, l)] = vt * hkm;
+      const double hk = f_hv[IX(d, k, l)];
+      const double vt = f_vh[IX(d, k, l)] / (hk + hkm);
+      f_vh[IX(d, k, l)] = vt * hk;
+      f_vh[IX(d, k - 1, l)] = vt * hkm;
     }
   }
 }
@@ -432,14 +461,23 @@ __global__ void k_vel2(Dev d) {
 // ------------------------------------------------------------- settrap / settrap2 / save
 // zeta at n+1/2 (settrap: rotate n -> n-1 first; settrap2: recompute only)
 __global__ void k_half_zeta(Dev d, int rotate) {
+  double* __restrict__ f_hp = d.f.hp;
+  double* __restrict__ f_hpp = d.f.hpp;
+  double* __restrict__ f_hup = d.f.hup;
+  double* __restrict__ f_hupp = d.f.hupp;
+  double* __restrict__ f_hvp = d.f.hvp;
+  double* __restrict__ f_hvpp = d.f.hvpp;
   const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (l > d.g.lm) return;
   if (rotate) {
     d.s.spp[l - 1] = d.s.sp[l - 1];
     const int zL = zlim(d, l), uL = ulim(d, l), vL = vlim(d, l);
-    for (int k = 1; k <= zL; ++k) d.f.hpp[IX(d, k, l)] = d.f.hp[IX(d, k, l)];
-    for (int k = 1; k <= uL; ++k) d.f.hupp[IX(d, k, l)] = d.f.hup[IX(d, k, l)];
-    for (int k = 1; k <= vL; ++k) d.f.hvpp[IX(d, k, l)] = d.f.hvp[IX(d, k, l)];
+    #pragma unroll 4
+    for (int k = 1; k <= zL; ++k) f_hpp[IX(d, k, l)] = f_hp[IX(d, k, l)];
+    #pragma unroll 4
+    for (int k = 1; k <= uL; ++k) f_hupp[IX(d, k, l)] = f_hup[IX(d, k, l)];
+    #pragma unroll 4
+    for (int k = 1; k <= vL; ++k) f_hvpp[IX(d, k, l)] = f_hvp[IX(d, k, l)];
   }
   d.s.sp[l - 1] = 0.5 * (d.s.s[l - 1] + d.s.spp[l - 1]);
 }
@@ -451,6 +489,27 @@ __global__ void k_half_zeta(Dev d, int rotate) {
 // is in place.
 template <int CLN>
 __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
+  double* __restrict__ f_hp = d.f.hp;
+  double* __restrict__ f_hu = d.f.hu;
+  double* __restrict__ f_hup = d.f.hup;
+  double* __restrict__ f_hupp = d.f.hupp;
+  double* __restrict__ f_hv = d.f.hv;
+  double* __restrict__ f_hvp = d.f.hvp;
+  double* __restrict__ f_hvpp = d.f.hvpp;
+  double* __restrict__ f_rhop = d.f.rhop;
+  double* __restrict__ f_sal = d.f.sal;
+  double* __restrict__ f_salp = d.f.salp;
+  double* __restrict__ f_salpp = d.f.salpp;
+  double* __restrict__ f_uh = d.f.uh;
+  double* __restrict__ f_uhp = d.f.uhp;
+  double* __restrict__ f_uhpp = d.f.uhpp;
+  double* __restrict__ f_up = d.f.up;
+  double* __restrict__ f_upp = d.f.upp;
+  double* __restrict__ f_vh = d.f.vh;
+  double* __restrict__ f_vhp = d.f.vhp;
+  double* __restrict__ f_vhpp = d.f.vhpp;
+  double* __restrict__ f_vp = d.f.vp;
+  double* __restrict__ f_vpp = d.f.vpp;
   __shared__ int s_first[3][CLN][32];
   const int cx = threadIdx.x, ty = threadIdx.y;
   const int l = blockIdx.x * 32 + cx + 1;
@@ -463,10 +522,11 @@ __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
     kms = NB(d.g.kmz, l);
     const double spl = d.s.sp[l - 1];
     const double hhs = d.g.hhs[l - 1];
+    #pragma unroll 4
     for (int k = k1 + ty; k <= kms; k += CLN) {
       double v = fmin(zl(d, k + 1), hhs) - fmax(zl(d, k), -spl);
       if (v <= HMIN) v = ZERO;
-      d.f.hp[IX(d, k, l)] = v;
+      f_hp[IX(d, k, l)] = v;
       if (v > ZERO && k < fz) fz = k;
     }
     ew = ewet(d, l);
@@ -475,10 +535,11 @@ __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
       kmx = min(kms, NB(d.g.kmz, lE));
       const double sm = fmax(spl, d.s.sp[lE - 1]);
       const double hhu = d.g.hhu[l - 1];
+      #pragma unroll 4
       for (int k = k1 + ty; k <= kmx; k += CLN) {
         double v = fmin(zl(d, k + 1), hhu) - fmax(zl(d, k), -sm);
         if (v <= HMIN) v = ZERO;
-        d.f.hup[IX(d, k, l)] = v;
+        f_hup[IX(d, k, l)] = v;
         if (v > ZERO && k < fu) fu = k;
       }
     }
@@ -488,10 +549,11 @@ __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
       kmy = min(kms, NB(d.g.kmz, lN));
       const double sm = fmax(spl, d.s.sp[lN - 1]);
       const double hhv = d.g.hhv[l - 1];
+      #pragma unroll 4
       for (int k = k1 + ty; k <= kmy; k += CLN) {
         double v = fmin(zl(d, k + 1), hhv) - fmax(zl(d, k), -sm);
         if (v <= HMIN) v = ZERO;
-        d.f.hvp[IX(d, k, l)] = v;
+        f_hvp[IX(d, k, l)] = v;
         if (v > ZERO && k < fv) fv = k;
       }
     }
@@ -507,30 +569,33 @@ __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
     d.s.k1z[l - 1] = kz; d.s.k1u[l - 1] = ku; d.s.k1v[l - 1] = kv;
   }
   if (act) {
+    #pragma unroll 4
     for (int k = k1 + ty; k <= kms; k += CLN) {
       const int ik = IX(d, k, l);
-      const double z = zmid(d, k, d.f.hp[ik]);
-      if (rotate) d.f.salpp[ik] = d.f.salp[ik];
-      const double sp = (d.f.sal[ik] + d.f.salpp[ik]) / 2.;
-      d.f.salp[ik] = sp;
-      d.f.rhop[ik] = densty_s(sp, 0.00004, z) - 1000.;
+      const double z = zmid(d, k, f_hp[ik]);
+      if (rotate) f_salpp[ik] = f_salp[ik];
+      const double sp = (f_sal[ik] + f_salpp[ik]) / 2.;
+      f_salp[ik] = sp;
+      f_rhop[ik] = densty_s(sp, 0.00004, z) - 1000.;
     }
     if (ew) {
+      #pragma unroll 4
       for (int k = k1 + ty; k <= kmx; k += CLN) {
         const int ik = IX(d, k, l);
-        if (rotate) { d.f.uhpp[ik] = d.f.uhp[ik]; d.f.upp[ik] = d.f.up[ik]; }
-        const double hup = d.f.hup[ik];
-        if (hup > ZERO) { const double v = 0.5 * (d.f.uh[ik] + d.f.uhpp[ik]); d.f.uhp[ik] = v; d.f.up[ik] = v / hup; }
-        else { d.f.uhp[ik] = 0.0; d.f.up[ik] = 0.0; }
+        if (rotate) { f_uhpp[ik] = f_uhp[ik]; f_upp[ik] = f_up[ik]; }
+        const double hup = f_hup[ik];
+        if (hup > ZERO) { const double v = 0.5 * (f_uh[ik] + f_uhpp[ik]); f_uhp[ik] = v; f_up[ik] = v / hup; }
+        else { f_uhp[ik] = 0.0; f_up[ik] = 0.0; }
       }
     }
     if (nw) {
+      #pragma unroll 4
       for (int k = k1 + ty; k <= kmy; k += CLN) {
         const int ik = IX(d, k, l);
-        if (rotate) { d.f.vhpp[ik] = d.f.vhp[ik]; d.f.vpp[ik] = d.f.vp[ik]; }
-        const double hvp = d.f.hvp[ik];
-        if (hvp > ZERO) { const double v = 0.5 * (d.f.vh[ik] + d.f.vhpp[ik]); d.f.vhp[ik] = v; d.f.vp[ik] = v / hvp; }
-        else { d.f.vhp[ik] = 0.0; d.f.vp[ik] = 0.0; }
+        if (rotate) { f_vhpp[ik] = f_vhp[ik]; f_vpp[ik] = f_vp[ik]; }
+        const double hvp = f_hvp[ik];
+        if (hvp > ZERO) { const double v = 0.5 * (f_vh[ik] + f_vhpp[ik]); f_vhp[ik] = v; f_vp[ik] = v / hvp; }
+        else { f_vhp[ik] = 0.0; f_vp[ik] = 0.0; }
       }
     }
   }
@@ -540,25 +605,25 @@ __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
   if (ew) {
     const int k = d.s.k1u[l - 1];
     const int ik = IX(d, k, l);
-    if (d.f.hu[IX(d, k - 1, l)] > ZERO) {
-      d.f.uhp[ik] = d.f.uhp[ik] + d.f.uh[IX(d, k - 1, l)] / 2.;
-      d.f.up[ik] = d.f.uhp[ik] / d.f.hup[ik];
+    if (f_hu[IX(d, k - 1, l)] > ZERO) {
+      f_uhp[ik] = f_uhp[ik] + f_uh[IX(d, k - 1, l)] / 2.;
+      f_up[ik] = f_uhp[ik] / f_hup[ik];
     }
-    if (d.f.hupp[IX(d, k - 1, l)] > ZERO) {
-      d.f.uhp[ik] = d.f.uhp[ik] + d.f.uhpp[IX(d, k - 1, l)] / 2.;
-      d.f.up[ik] = d.f.uhp[ik] / d.f.hup[ik];
+    if (f_hupp[IX(d, k - 1, l)] > ZERO) {
+      f_uhp[ik] = f_uhp[ik] + f_uhpp[IX(d, k - 1, l)] / 2.;
+      f_up[ik] = f_uhp[ik] / f_hup[ik];
     }
   }
   if (nw) {
     const int k = d.s.k1v[l - 1];
     const int ik = IX(d, k, l);
-    if (d.f.hv[IX(d, k - 1, l)] > ZERO) {
-      d.f.vhp[ik] = d.f.vhp[ik] + d.f.vh[IX(d, k - 1, l)] / 2.;
-      d.f.vp[ik] = d.f.vhp[ik] / d.f.hvp[ik];
+    if (f_hv[IX(d, k - 1, l)] > ZERO) {
+      f_vhp[ik] = f_vhp[ik] + f_vh[IX(d, k - 1, l)] / 2.;
+      f_vp[ik] = f_vhp[ik] / f_hvp[ik];
     }
-    if (d.f.hvpp[IX(d, k - 1, l)] > ZERO) {
-      d.f.vhp[ik] = d.f.vhp[ik] + d.f.vhpp[IX(d, k - 1, l)] / 2.;
-      d.f.vp[ik] = d.f.vhp[ik] / d.f.hvp[ik];
+    if (f_hvpp[IX(d, k - 1, l)] > ZERO) {
+      f_vhp[ik] = f_vhp[ik] + f_vhpp[IX(d, k - 1, l)] / 2.;
+      f_vp[ik] = f_vhp[ik] / f_hvp[ik];
     }
   }
 }
@@ -567,6 +632,29 @@ __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
 // k_half_level; the new first wet layers are reduced over the lanes in shared memory.
 template <int CLN>
 __global__ void __launch_bounds__(32 * CLN) k_save(Dev d, int istep) {
+  double* __restrict__ f_h = d.f.h;
+  double* __restrict__ f_hp = d.f.hp;
+  double* __restrict__ f_hpp = d.f.hpp;
+  double* __restrict__ f_hu = d.f.hu;
+  double* __restrict__ f_hup = d.f.hup;
+  double* __restrict__ f_hupp = d.f.hupp;
+  double* __restrict__ f_hv = d.f.hv;
+  double* __restrict__ f_hvp = d.f.hvp;
+  double* __restrict__ f_hvpp = d.f.hvpp;
+  double* __restrict__ f_rhop = d.f.rhop;
+  double* __restrict__ f_sal = d.f.sal;
+  double* __restrict__ f_salp = d.f.salp;
+  double* __restrict__ f_salpp = d.f.salpp;
+  double* __restrict__ f_uh = d.f.uh;
+  double* __restrict__ f_uhp = d.f.uhp;
+  double* __restrict__ f_uhpp = d.f.uhpp;
+  double* __restrict__ f_up = d.f.up;
+  double* __restrict__ f_upp = d.f.upp;
+  double* __restrict__ f_vh = d.f.vh;
+  double* __restrict__ f_vhp = d.f.vhp;
+  double* __restrict__ f_vhpp = d.f.vhpp;
+  double* __restrict__ f_vp = d.f.vp;
+  double* __restrict__ f_vpp = d.f.vpp;
   __shared__ int s_first[3][CLN][32];
   const int cx = threadIdx.x, ty = threadIdx.y;
   const int l = blockIdx.x * 32 + cx + 1;
@@ -583,25 +671,28 @@ __global__ void __launch_bounds__(32 * CLN) k_save(Dev d, int istep) {
     kms = NB(d.g.kmz, l);
     const int kmx = ewet(d, l) ? min(kms, NB(d.g.kmz, NB(d.g.lEC, l))) : 0;
     const int kmy = nwet(d, l) ? min(kms, NB(d.g.kmz, NB(d.g.lNC, l))) : 0;
+    #pragma unroll 4
     for (int k = 1 + ty; k <= zL; k += CLN) {
       const int ik = IX(d, k, l);
-      if (istep == 1) d.f.hpp[ik] = d.f.hp[ik];
-      const double v = d.f.h[ik];
-      d.f.hp[ik] = v;
+      if (istep == 1) f_hpp[ik] = f_hp[ik];
+      const double v = f_h[ik];
+      f_hp[ik] = v;
       if (k >= k1 && k <= kms && v > ZERO && k < fz) fz = k;
     }
+    #pragma unroll 4
     for (int k = 1 + ty; k <= uL; k += CLN) {
       const int ik = IX(d, k, l);
-      if (istep == 1) d.f.hupp[ik] = d.f.hup[ik];
-      const double v = d.f.hu[ik];
-      d.f.hup[ik] = v;
+      if (istep == 1) f_hupp[ik] = f_hup[ik];
+      const double v = f_hu[ik];
+      f_hup[ik] = v;
       if (k >= k1 && k <= kmx && v > ZERO && k < fu) fu = k;
     }
+    #pragma unroll 4
     for (int k = 1 + ty; k <= vL; k += CLN) {
       const int ik = IX(d, k, l);
-      if (istep == 1) d.f.hvpp[ik] = d.f.hvp[ik];
-      const double v = d.f.hv[ik];
-      d.f.hvp[ik] = v;
+      if (istep == 1) f_hvpp[ik] = f_hvp[ik];
+      const double v = f_hv[ik];
+      f_hvp[ik] = v;
       if (k >= k1 && k <= kmy && v > ZERO && k < fv) fv = k;
     }
   }
@@ -616,26 +707,29 @@ __global__ void __launch_bounds__(32 * CLN) k_save(Dev d, int istep) {
     d.s.k1z[l - 1] = kz; d.s.k1u[l - 1] = ku; d.s.k1v[l - 1] = kv;
   }
   if (!act) return;
+  #pragma unroll 4
   for (int k = k1 + ty; k <= min(d.g.km, zL); k += CLN) {
     const int ik = IX(d, k, l);
-    const double z = zmid(d, k, d.f.hp[ik]);
-    if (istep == 1) d.f.salpp[ik] = d.f.salp[ik];
-    d.f.salp[ik] = d.f.sal[ik];
-    d.f.rhop[ik] = densty_s(d.f.salp[ik], 0.00004, z) - 1000.;
+    const double z = zmid(d, k, f_hp[ik]);
+    if (istep == 1) f_salpp[ik] = f_salp[ik];
+    f_salp[ik] = f_sal[ik];
+    f_rhop[ik] = densty_s(f_salp[ik], 0.00004, z) - 1000.;
   }
+  #pragma unroll 4
   for (int k = k1 + ty; k <= uL; k += CLN) {
     const int ik = IX(d, k, l);
-    if (istep == 1) { d.f.uhpp[ik] = d.f.uhp[ik]; d.f.upp[ik] = d.f.up[ik]; }
-    const double hup = d.f.hup[ik];
-    if (hup > ZERO) { const double v = d.f.uh[ik]; d.f.uhp[ik] = v; d.f.up[ik] = v / hup; }
-    else { d.f.uhp[ik] = 0.0; d.f.up[ik] = 0.0; }
+    if (istep == 1) { f_uhpp[ik] = f_uhp[ik]; f_upp[ik] = f_up[ik]; }
+    const double hup = f_hup[ik];
+    if (hup > ZERO) { const double v = f_uh[ik]; f_uhp[ik] = v; f_up[ik] = v / hup; }
+    else { f_uhp[ik] = 0.0; f_up[ik] = 0.0; }
   }
+  #pragma unroll 4
   for (int k = k1 + ty; k <= vL; k += CLN) {
     const int ik = IX(d, k, l);
-    if (istep == 1) { d.f.vhpp[ik] = d.f.vhp[ik]; d.f.vpp[ik] = d.f.vp[ik]; }
-    const double hvp = d.f.hvp[ik];
-    if (hvp > ZERO) { const double v = d.f.vh[ik]; d.f.vhp[ik] = v; d.f.vp[ik] = v / hvp; }
-    else { d.f.vhp[ik] = 0.0; d.f.vp[ik] = 0.0; }
+    if (istep == 1) { f_vhpp[ik] = f_vhp[ik]; f_vpp[ik] = f_vp[ik]; }
+    const double hvp = f_hvp[ik];
+    if (hvp > ZERO) { const double v = f_vh[ik]; f_vhp[ik] = v; f_vp[ik] = v / hvp; }
+    else { f_vhp[ik] = 0.0; f_vp[ik] = 0.0; }
   }
 }
 

@@ -30,6 +30,8 @@ namespace si3d {
 
 // ------------------------------------------------------------------ matcon
 __global__ void k_matcon(Dev d) {
+  double* __restrict__ f_uhpp = d.f.uhpp;
+  double* __restrict__ f_vhpp = d.f.vhpp;
   const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (l > d.g.lm) return;
   const double tz = d.tz;
@@ -53,9 +55,10 @@ __global__ void k_matcon(Dev d) {
   d.s.sy[l - 1] = syl;
   const int kms = NB(d.g.kmz, l);
   double sum = 0;
+  #pragma unroll 4
   for (int k = d.g.k1; k <= kms; ++k)
-    sum += (d.f.uhpp[IX(d, k, l)] - d.f.uhpp[IX(d, k, lW)]) / d.p.dx +
-           (d.f.vhpp[IX(d, k, l)] - d.f.vhpp[IX(d, k, lS)]) / d.p.dy;
+    sum += (f_uhpp[IX(d, k, l)] - f_uhpp[IX(d, k, lW)]) / d.p.dx +
+           (f_vhpp[IX(d, k, l)] - f_vhpp[IX(d, k, lS)]) / d.p.dy;
   const double ddv = dt1 * sum;
   d.s.dd[l - 1] = ddv;
   d.s.qq[l - 1] = d.s.spp[l - 1] - dtdx1 * (d.s.eagx[l - 1] - d.s.eagx[lW - 1]) -
