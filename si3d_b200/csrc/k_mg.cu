@@ -1,22 +1,28 @@
-// Aggregation-multigrid preconditioned CG for the FP32 inner solves of iterative refinement
-// (hierarchy and V-cycle: mg.h).  One cooperative launch runs a whole inner solve; its phases are
-// separated by grid barriers (coop.cuh) and every block reduces the block partials itself in the
-// same fixed order, so all blocks take the same alpha, beta and stopping decision.
+// Mixed-precision zeta solve with aggregation-multigrid preconditioned FP32 inner solves (hierarchy
+// and V-cycle: mg.h), the whole solve in one cooperative launch: FP64 iterative refinement around
+// FP32 MG-PCG.  Phases are separated by grid barriers (coop.cuh) and every block reduces the block
+// partials itself in the same fixed order, so all blocks take the same decisions.
 //
-// Phases of one iteration (a barrier after each):
-//   U       u += alpha p, r -= alpha q (from the second iteration on), (r, r), and the first
+// Outer (FP64) pass: u += e (from the second pass on; e is the FP32 correction), then the residual
+// r = b - A u and ||r|| (and ||b|| on the first pass); stop when ||r|| < ||b|| zeta (test 5);
+// otherwise the inner solve starts from e = 0 with right-hand side r rounded to FP32 and stops when
+// its residual has dropped by max(1e-5, what the outer test still needs).
+//
+// Inner (FP32 MG-PCG) iteration (a barrier after each phase):
+//   U       e += alpha p, r -= alpha q (from the second iteration on), (r, r), and the first
 //           (red) half-sweep of level 0 from z = 0, which is z = dinv r;
-//           the stopping test (test 5 on the inner residual) right after its barrier
+//           the stopping test on the inner residual right after its barrier
 //   down    per level k < L - 1: black half-sweep; residual summed over 2 x 2 aggregates into
 //           level k + 1's b, whose red cells get their first half-sweep z = dinv b
 //   coarse  black then red half-sweep of the coarsest level, by block 0 alone
 //   up      per level k = L - 2 .. 0: black half-sweep with the neighbours' values plus the coarse
 //           correction of their aggregate; red half-sweep; at level 0 both add to (r, z)
 //   PQ      beta, p = z + beta p and q = A p (neighbours' p formed on the fly), (p, q)
-// With L levels that is 4 L - 1 barriers an iteration.
+// With L levels that is 4 L - 1 barriers an inner iteration.
 #include <algorithm>
 
 #include "../../include/si3d_gpu.h"
+#include "common.cuh"
 #include "coop.cuh"
 #include "mg.h"
 
@@ -50,24 +56,49 @@ __device__ __forceinline__ int fdiv(const FastDiv& f, int x) {
 }
 
 // ---------------------------------------------------------------- per-solve setup
-// Level 0 from the FP64 red-black system: the faces the system couples, the diagonal it applies
-// (1 + sx + sx(W) + sy + sy(S)), and mass = diagonal - faces.
-__global__ void k_mg_coef0(PcgDev P, MgDev M, int color) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const PcgColor& C = color ? P.B : P.R;
-  const PcgColor& O = color ? P.R : P.B;
-  if (i >= C.n) return;
-  const int o = (color ? M.pixB : M.pixR)[i];
-  const int4 q = C.nbr[i];   // W, S, N, E in the other colour (absent: O.n, the zero slot)
-  const double sxi = C.sx[i], syi = C.sy[i], sxW = O.sx[q.x], syS = O.sy[q.y];
-  const double diag = 1.0 + sxi + sxW + syi + syS;
-  const double fN = (q.z != O.n) ? syi : 0.0;   // face to (i, j + 1): the next column
-  const double fE = (q.w != O.n) ? sxi : 0.0;   // face to (i + 1, j): the next row
+// Level 0 and the FP64 system from the assembled zeta system of wet column l (matcon's sx, sy, qq):
+// the faces the system couples, the diagonal it applies (1 + sx + sx(W) + sy + sy(S), as the red-black
+// system does), mass = diagonal - faces, and the initial guess (x0 modes of the red-black gather).
+__global__ void k_mg_setup(Dev d, MgDev M, int x0_mode, const double* __restrict__ dz,
+                           const double* __restrict__ hist) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const int lm1 = d.g.lm1;
+  const int o = M.pixL[l - 1];
+  const int lE = NB(d.g.lEC, l), lW = NB(d.g.lWC, l), lN = NB(d.g.lNC, l), lS = NB(d.g.lSC, l);
+  const double sxi = d.s.sx[l - 1], syi = d.s.sy[l - 1];
+  const double sxW = (lW != lm1) ? d.s.sx[lW - 1] : 0.0;
+  const double syS = (lS != lm1) ? d.s.sy[lS - 1] : 0.0;
+  const double diag = 1 + sxi + sxW + syi + syS;
+  const double fN = (lN != lm1) ? syi : 0.0;   // face to (i, j + 1): the next column
+  const double fE = (lE != lm1) ? sxi : 0.0;   // face to (i + 1, j): the next row
+  M.fc64[o] = fN;
+  M.fr64[o] = fE;
+  M.dg64[o] = diag;
+  M.b64[o] = d.s.qq[l - 1];
+  double x0;
+  switch (x0_mode) {
+    case 1: x0 = 0.0; break;
+    case 3: x0 = d.s.s[l - 1]; break;
+    case 4: x0 = d.s.s[l - 1] + (hist ? hist[l - 1] : 0.0); break;
+    default: x0 = d.s.sp[l - 1]; if (x0_mode == 2 && dz) x0 = x0 + dz[l - 1];
+  }
+  M.u64[o] = x0;
   const MgLevel& L = M.lv[0];
   L.fc[o] = (float)fN;
   L.fr[o] = (float)fE;
   L.mass[o] = (float)(diag - fN - fE - sxW - syS);
   L.dinv[o] = (float)(1.0 / diag);
+}
+
+// zeta back to the columns: s(l) = u; with `hist`, also this solve's correction to the zeta it
+// started from (s before the write), per column, for the next step's guess of the same solve.
+__global__ void k_mg_scatter(Dev d, MgDev M, double* __restrict__ hist) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const double u = M.u64[M.pixL[l - 1]];
+  if (hist) hist[l - 1] = u - d.s.s[l - 1];
+  d.s.s[l - 1] = u;
 }
 
 // Level k + 1 from level k: 2 x 2 aggregates (frame cells read as zero).
@@ -88,23 +119,6 @@ __global__ void k_mg_coarsen(MgLevel F, MgLevel G) {
   G.mass[O] = mass;
   const float diag = mass + fc + fr + fcW + frS;
   G.dinv[O] = diag > 0.f ? 1.f / diag : 0.f;
-}
-
-// Inner right-hand side: the FP64 outer residual rounded to FP32; the correction starts at zero.
-__global__ void k_mg_inner_setup(PcgDev P, MgDev M, int color) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const PcgColor& C = color ? P.B : P.R;
-  if (i >= C.n) return;
-  const int o = (color ? M.pixB : M.pixR)[i];
-  M.lv[0].b[o] = (float)C.r[i];
-  M.u[o] = 0.f;
-}
-
-__global__ void k_mg_correct(PcgDev P, MgDev M, int color) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const PcgColor& C = color ? P.B : P.R;
-  if (i >= C.n) return;
-  C.u[i] = C.u[i] + (double)M.u[(color ? M.pixB : M.pixR)[i]];
 }
 
 // ---------------------------------------------------------------- V-cycle pieces
@@ -189,22 +203,18 @@ __device__ __forceinline__ void restrict_residual(const MgLevel& F, const MgLeve
 }
 
 // ---------------------------------------------------------------- the inner solve
-__global__ void __launch_bounds__(QB, 2) k_mg_loop(MgDev M, GridBar* bar) {
-  __shared__ double sh[8 + 1];
-  __shared__ int s_flag;
-  __shared__ MgLevel s_lv[kMgMaxLevels];
-  const int nlev = M.nlev;
-  if (threadIdx.x < nlev) s_lv[threadIdx.x] = M.lv[threadIdx.x];
-  __syncthreads();
-  PcgScal* SC = M.sc;
+// FP32 MG-PCG on level 0 from e = 0 (M.u) with right-hand side r (level 0's b), until
+// ||r|| < bnorm * zeta or itmax iterations.  Returns false when a barrier gave up (the caller returns
+// at once); otherwise its = the iterations taken and ier = 0, 1 (itmax) or -6 / -7 (breakdown).
+__device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* bar, PcgScal* SC, int* s_flag,
+                       double* sh, double zeta, double bnorm, int itmax, int& its, int& ier) {
   const int nb = gridDim.x, stride = nb * QB, g0 = blockIdx.x * QB + threadIdx.x;
   double* const rr_part = M.part;
   double* const rz_part = M.part + nb;
   double* const pq_part = M.part + 3 * nb;
-  const double zeta = SC->zeta, bnorm = SC->bnorm;
-  const int itmax = SC->itmax;
-  double alpha = 0.0, beta = 0.0, rz_old = 1.0, stptst = 1.0;
-  int it = 0, ier = 0;
+  double alpha = 0.0, beta = 0.0, rz_old = 1.0;
+  int it = 0;
+  ier = 0;
   const MgLevel& L0 = s_lv[0];
   const int n0 = L0.rows * L0.cols, pt = L0.pitch;
   for (;;) {
@@ -246,21 +256,20 @@ __global__ void __launch_bounds__(QB, 2) k_mg_loop(MgDev M, GridBar* bar) {
       bsum<1>(w, sh);
       if (threadIdx.x == 0) rr_part[blockIdx.x] = w[0];
     }
-    if (!grid_barrier(bar, SC, &s_flag)) return;
+    if (!grid_barrier(bar, SC, s_flag)) return false;
     {
       double w[1];
       all_partials<1>(rr_part, nb, 0, w, sh);
       const double tl = sqrt(w[0]);
-      stptst = tl / bnorm;
       if (tl < bnorm * zeta) break;
       if (it >= itmax) { ier = 1; break; }
     }
     // ---- down: black half-sweep, restriction
     for (int k = 0; k < nlev - 1; ++k) {
       half_sweep<false, false>(s_lv[k], s_lv[k], 1, g0, stride);
-      if (!grid_barrier(bar, SC, &s_flag)) return;
+      if (!grid_barrier(bar, SC, s_flag)) return false;
       restrict_residual(s_lv[k], s_lv[k + 1], g0, stride);
-      if (!grid_barrier(bar, SC, &s_flag)) return;
+      if (!grid_barrier(bar, SC, s_flag)) return false;
     }
     // ---- coarsest level: black, red (one block)
     if (blockIdx.x == 0) {
@@ -269,7 +278,7 @@ __global__ void __launch_bounds__(QB, 2) k_mg_loop(MgDev M, GridBar* bar) {
       __syncthreads();
       half_sweep<false, false>(Lc, Lc, 0, threadIdx.x, QB);
     }
-    if (!grid_barrier(bar, SC, &s_flag)) return;
+    if (!grid_barrier(bar, SC, s_flag)) return false;
     // ---- up: black half-sweep with the coarse correction, red half-sweep; (r, z) at level 0
     for (int k = nlev - 2; k >= 0; --k) {
       if (k == 0) {
@@ -279,7 +288,7 @@ __global__ void __launch_bounds__(QB, 2) k_mg_loop(MgDev M, GridBar* bar) {
       } else {
         half_sweep<true, false>(s_lv[k], s_lv[k + 1], 1, g0, stride);
       }
-      if (!grid_barrier(bar, SC, &s_flag)) return;
+      if (!grid_barrier(bar, SC, s_flag)) return false;
       if (k == 0) {
         double w[1] = {half_sweep<false, true>(s_lv[0], s_lv[0], 0, g0, stride)};
         bsum<1>(w, sh);
@@ -287,7 +296,7 @@ __global__ void __launch_bounds__(QB, 2) k_mg_loop(MgDev M, GridBar* bar) {
       } else {
         half_sweep<false, false>(s_lv[k], s_lv[k], 0, g0, stride);
       }
-      if (!grid_barrier(bar, SC, &s_flag)) return;
+      if (!grid_barrier(bar, SC, s_flag)) return false;
     }
     {
       double w[1];
@@ -336,7 +345,7 @@ __global__ void __launch_bounds__(QB, 2) k_mg_loop(MgDev M, GridBar* bar) {
       bsum<1>(w, sh);
       if (threadIdx.x == 0) pq_part[blockIdx.x] = w[0];
     }
-    if (!grid_barrier(bar, SC, &s_flag)) return;
+    if (!grid_barrier(bar, SC, s_flag)) return false;
     {
       double w[1];
       all_partials<1>(pq_part, nb, 0, w, sh);
@@ -345,10 +354,93 @@ __global__ void __launch_bounds__(QB, 2) k_mg_loop(MgDev M, GridBar* bar) {
     }
     ++it;
   }
+  its = it;
+  return true;
+}
+
+// ---------------------------------------------------------------- the whole solve
+__global__ void __launch_bounds__(QB, 2) k_mg_solve(MgDev M, GridBar* bar) {
+  __shared__ double sh[8 * 2 + 2];
+  __shared__ int s_flag;
+  __shared__ MgLevel s_lv[kMgMaxLevels];
+  const int nlev = M.nlev;
+  if (threadIdx.x < nlev) s_lv[threadIdx.x] = M.lv[threadIdx.x];
+  __syncthreads();
+  PcgScal* SC = M.sc;
+  const int nb = gridDim.x, stride = nb * QB, g0 = blockIdx.x * QB + threadIdx.x;
+  double* const res_part = M.part + 4 * nb;   // (r, r) [nb], (b, b) [nb] of the FP64 system
+  const double zeta = SC->zeta, srelpr = SC->srelpr;
+  const int itmax = SC->itmax;
+  const MgLevel& L0 = s_lv[0];
+  const int n0 = L0.rows * L0.cols, pt = L0.pitch;
+  double bn = 1.0, stp = 1.0;
+  int outer = 0, total = 0, ier = 0;
+  for (;;) {
+    if (outer > 0) {
+      // ---- u += e (FP64)
+      for (int t = g0; t < n0; t += stride) {
+        const int r = fdiv(L0.div_cols, t), c = t - r * L0.cols;
+        const int o = (r + 1) * pt + c + 1;
+        M.u64[o] = M.u64[o] + (double)M.u[o];
+      }
+      if (!grid_barrier(bar, SC, &s_flag)) return;
+    }
+    // ---- r = b - A u (FP64), ||r||^2 (and ||b||^2 on the first pass); inner rhs r and e = 0
+    {
+      double v[2] = {0.0, 0.0};
+      for (int t0 = g0; t0 < n0; t0 += 2 * stride) {
+        int o[2];
+        bool ok[2];
+        double rv[2], bv[2];
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const int t = t0 + k * stride;
+          ok[k] = t < n0;
+          const int r = ok[k] ? fdiv(L0.div_cols, t) : 0;
+          const int c = ok[k] ? t - r * L0.cols : 0;
+          const int x = (r + 1) * pt + c + 1;
+          o[k] = x;
+          double y = M.dg64[x] * M.u64[x];
+          y = y + (-M.fr64[x - pt]) * M.u64[x - pt];
+          y = y + (-M.fc64[x - 1]) * M.u64[x - 1];
+          y = y + (-M.fc64[x]) * M.u64[x + 1];
+          y = y + (-M.fr64[x]) * M.u64[x + pt];
+          bv[k] = M.b64[x];
+          rv[k] = bv[k] - y;
+        }
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          if (!ok[k]) continue;
+          v[0] += rv[k] * rv[k];
+          v[1] += bv[k] * bv[k];
+          L0.b[o[k]] = (float)rv[k];
+          M.u[o[k]] = 0.f;
+        }
+      }
+      bsum<2>(v, sh);
+      if (threadIdx.x == 0) { res_part[blockIdx.x] = v[0]; res_part[nb + blockIdx.x] = v[1]; }
+    }
+    if (!grid_barrier(bar, SC, &s_flag)) return;
+    double w[2];
+    all_partials<2>(res_part, nb, nb, w, sh);
+    if (outer == 0) bn = fmax(sqrt(w[1]), srelpr);   // bnorm of stopping test 5 (nmcalc)
+    const double rn = sqrt(w[0]);
+    stp = rn / bn;
+    if (rn < bn * zeta) break;
+    if (outer >= kMgMaxOuter) { ier = 1; break; }
+    // ---- inner FP32 MG-PCG
+    int its = 0, iier = 0;
+    if (!mg_pcg(M, s_lv, nlev, bar, SC, &s_flag, sh, fmax(1e-5, 0.5 * zeta * bn / rn), rn, itmax, its, iier)) return;
+    total += its;
+    ++outer;
+    if (iier < 0) { ier = iier; break; }
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
-    SC->in = it;
-    SC->stptst = stptst;
+    SC->in = total;
+    SC->stptst = stp;
+    SC->bnorm = bn;
     SC->ier = ier;
+    SC->q1 = outer;
     SC->done = 1;
   }
 }
@@ -358,33 +450,22 @@ __global__ void __launch_bounds__(QB, 2) k_mg_loop(MgDev M, GridBar* bar) {
 int mg_loop_blocks(int device, int cells0, int max_per_sm) {
   int sms = 0, occ = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_loop, QB, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_solve, QB, 0);
   int per_sm = std::max(occ, 1);
   if (max_per_sm > 0) per_sm = std::min(per_sm, max_per_sm);
   const int need = std::max(1, (cells0 + QB - 1) / QB);
   return std::max(1, std::min(sms * per_sm, need));
 }
 
-void mg_setup(const PcgDev& P, const MgDev& M, cudaStream_t st) {
-  if (P.R.n > 0) k_mg_coef0<<<(P.R.n + PB - 1) / PB, PB, 0, st>>>(P, M, 0);
-  if (P.B.n > 0) k_mg_coef0<<<(P.B.n + PB - 1) / PB, PB, 0, st>>>(P, M, 1);
+void mg_setup(const Dev& d, const MgDev& M, int x0_mode, const double* dz, const double* hist, cudaStream_t st) {
+  k_mg_setup<<<(d.g.lm + PB - 1) / PB, PB, 0, st>>>(d, M, x0_mode, dz, hist);
   for (int k = 0; k + 1 < M.nlev; ++k) {
     const int n = M.lv[k + 1].rows * M.lv[k + 1].cols;
     k_mg_coarsen<<<(n + PB - 1) / PB, PB, 0, st>>>(M.lv[k], M.lv[k + 1]);
   }
 }
 
-void mg_inner_setup(const PcgDev& P, const MgDev& M, cudaStream_t st) {
-  if (P.R.n > 0) k_mg_inner_setup<<<(P.R.n + PB - 1) / PB, PB, 0, st>>>(P, M, 0);
-  if (P.B.n > 0) k_mg_inner_setup<<<(P.B.n + PB - 1) / PB, PB, 0, st>>>(P, M, 1);
-}
-
-void mg_correct(const PcgDev& P, const MgDev& M, cudaStream_t st) {
-  if (P.R.n > 0) k_mg_correct<<<(P.R.n + PB - 1) / PB, PB, 0, st>>>(P, M, 0);
-  if (P.B.n > 0) k_mg_correct<<<(P.B.n + PB - 1) / PB, PB, 0, st>>>(P, M, 1);
-}
-
-int mg_loop(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st) {
+int mg_solve(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st) {
   if (cudaMemsetAsync(bar, 0, sizeof(GridBar), st) != cudaSuccess) return -1;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nblocks);
@@ -396,7 +477,11 @@ int mg_loop(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st) {
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, k_mg_loop, M, bar) == cudaSuccess ? 0 : -1;
+  return cudaLaunchKernelEx(&cfg, k_mg_solve, M, bar) == cudaSuccess ? 0 : -1;
+}
+
+void mg_finish(const Dev& d, const MgDev& M, double* hist, cudaStream_t st) {
+  k_mg_scatter<<<(d.g.lm + PB - 1) / PB, PB, 0, st>>>(d, M, hist);
 }
 
 }  // namespace si3d

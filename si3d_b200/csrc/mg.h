@@ -42,21 +42,29 @@ struct MgLevel {
   float *z, *b, *fc, *fr, *mass, *dinv;
 };
 
+constexpr int kMgMaxOuter = 40;      // FP64 refinement passes at most (then ier = 1)
+
 struct MgDev {
   int nlev = 0;
   MgLevel lv[kMgMaxLevels];
-  float *u = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;   // level-0 CG vectors; lv[0].b is r
-  const int *pixR = nullptr, *pixB = nullptr;   // red / black node of the FP64 system -> level-0 offset
-  double* part = nullptr;   // block partials: (r, r) [nb], (r, z) black + red [2 nb], (p, q) [nb]
-  PcgScal* sc = nullptr;    // inner scalars: zeta, bnorm, itmax in; in, stptst, ier, done out
+  // level-0 FP32 CG vectors of the inner solve (e = u; lv[0].b is its residual)
+  float *u = nullptr, *p0 = nullptr, *p1 = nullptr, *q = nullptr;
+  // the FP64 system on the level-0 image: solution, right-hand side, faces and diagonal
+  double *u64 = nullptr, *b64 = nullptr, *fc64 = nullptr, *fr64 = nullptr, *dg64 = nullptr;
+  const int* pixL = nullptr;   // wet column l -> level-0 offset (index l - 1)
+  // block partials: (r, r) [nb], (r, z) black + red [2 nb], (p, q) [nb], FP64 (r, r) and (b, b) [2 nb]
+  double* part = nullptr;
+  // in: zeta (outer tolerance), srelpr, itmax (inner); out: in (inner iterations, all passes),
+  // stptst (outer), bnorm, ier, q1 (outer passes), done
+  PcgScal* sc = nullptr;
 };
 
 FastDiv fast_div(int d);
 size_t mg_level_elems(int rows, int cols);   // floats of one array of a rows x cols level
 int mg_loop_blocks(int device, int cells0, int max_per_sm);
-void mg_setup(const PcgDev& P, const MgDev& M, cudaStream_t st);        // coefficients of every level
-void mg_inner_setup(const PcgDev& P, const MgDev& M, cudaStream_t st);  // b = outer residual, u = 0
-int mg_loop(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st);
-void mg_correct(const PcgDev& P, const MgDev& M, cudaStream_t st);      // FP64 u += FP32 u
+// the FP64 system, level 0 and the coarser levels from matcon's sx, sy, qq and the initial guess
+void mg_setup(const Dev& d, const MgDev& M, int x0_mode, const double* dz, const double* hist, cudaStream_t st);
+int mg_solve(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st);     // the cooperative solve
+void mg_finish(const Dev& d, const MgDev& M, double* hist, cudaStream_t st);  // s(l) = u (and hist)
 
 }  // namespace si3d

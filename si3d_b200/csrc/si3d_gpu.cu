@@ -247,7 +247,7 @@ void colour_columns(int lm, const int* lEC, const int* lWC, const int* lNC, cons
 // columns, so the grid maps must describe that image: every neighbour one row (east / west) or one
 // column (north / south) away.  Levels halve both sides until one block can sweep the coarsest
 // and the coarsest is mass-dominated (kMgMinLevels).
-int build_mg(Ctx* c, const si3d_grid* g, const std::vector<int>& lr, const std::vector<int>& lb) {
+int build_mg(Ctx* c, const si3d_grid* g) {
   const int lm = g->lm, lm1 = lm + 1;
   if (!g->l2i || !g->l2j) return SI3D_EDIMS;
   MgDev& M = c->mg;
@@ -272,6 +272,7 @@ int build_mg(Ctx* c, const si3d_grid* g, const std::vector<int>& lr, const std::
   }
   const size_t n0 = mg_level_elems(c->im1, c->jm1);
   for (float** q : {&M.u, &M.p0, &M.p1, &M.q}) rc |= c->alloc(q, n0);
+  for (double** q : {&M.u64, &M.b64, &M.fc64, &M.fr64, &M.dg64}) rc |= c->alloc(q, n0);
   if (rc) return rc;
   const int pitch = M.lv[0].pitch;
   std::vector<int> off(lm + 2, -1);
@@ -286,22 +287,18 @@ int build_mg(Ctx* c, const si3d_grid* g, const std::vector<int>& lr, const std::
         (n != lm1 && off[n] != off[l] + 1) || (s != lm1 && off[s] != off[l] - 1))
       return SI3D_EDIMS;
   }
-  std::vector<int> pr(lr.size()), pb(lb.size());
-  for (size_t k = 0; k < lr.size(); ++k) pr[k] = off[lr[k]];
-  for (size_t k = 0; k < lb.size(); ++k) pb[k] = off[lb[k]];
-  int *dr = nullptr, *db = nullptr;
-  rc |= c->alloc(&dr, pr.size());
-  rc |= c->alloc(&db, pb.size());
+  int* dl = nullptr;
+  rc |= c->alloc(&dl, lm);
   if (rc) return rc;
-  if (!pr.empty()) CK(cudaMemcpy(dr, pr.data(), pr.size() * sizeof(int), cudaMemcpyHostToDevice));
-  if (!pb.empty()) CK(cudaMemcpy(db, pb.data(), pb.size() * sizeof(int), cudaMemcpyHostToDevice));
-  M.pixR = dr;
-  M.pixB = db;
+  CK(cudaMemcpy(dl, off.data() + 1, lm * sizeof(int), cudaMemcpyHostToDevice));
+  M.pixL = dl;
   // SI3D_MG_BLOCKS_PER_SM caps the resident blocks per SM of the MG solve (tuning)
   const char* bps = std::getenv("SI3D_MG_BLOCKS_PER_SM");
   c->mg_blocks = mg_loop_blocks(c->device, c->im1 * c->jm1, bps ? std::atoi(bps) : 0);
-  rc |= c->alloc(&M.part, 4 * (size_t)c->mg_blocks);
-  M.sc = c->pcgf.sc;
+  rc |= c->alloc(&M.part, 6 * (size_t)c->mg_blocks);
+  PcgScal* sc = nullptr;
+  rc |= c->alloc(&sc, 1);
+  M.sc = sc;
   return rc;
 }
 
@@ -391,7 +388,7 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
   F.part0 = P.part0; F.part1 = P.part1; F.part2 = P.part2; F.part3 = P.part3; F.part_n = P.part_n;
   F.hist_alpha = P.hist_alpha; F.hist_beta = P.hist_beta; F.tri = nullptr;
   CK(cudaMallocHost(&c->h_scf, sizeof(PcgScal)));
-  if (c->prm.precision == SI3D_MIXED_MG) return build_mg(c, g, lr, lb);
+  if (c->prm.precision == SI3D_MIXED_MG) return build_mg(c, g);
   return 0;
 }
 
@@ -517,20 +514,14 @@ int iterate(Ctx* c, PcgScal* dsc, PcgScal* hsc, int itmax, int predicted, F&& la
 // residual r = b - A u, its norm, the stopping test (test 5 at the caller's tolerance) and the
 // update u += e are FP64; each inner solve runs the red-black MIC-PCG on FP32 copies of the
 // coefficients, pivots and residual (dot products still accumulate in FP64) until its own
-// residual has dropped by max(1e-5, what the outer test still needs).  With precision
-// SI3D_MIXED_MG the inner solves are aggregation-multigrid preconditioned CG instead (k_mg.cu),
-// whose hierarchy is rebuilt from this solve's coefficients once before the first inner solve.
+// residual has dropped by max(1e-5, what the outer test still needs).  (Precision SI3D_MIXED_MG runs
+// the same refinement around multigrid-preconditioned inner solves on the device: solve_mg.)
 int refine(Ctx* c, int* total_inner) {
   const si3d_params& p = c->prm;
   const double zeta = std::max(p.pcg_tol, 500.0 * p.srelpr);
-  const bool mg = p.precision == SI3D_MIXED_MG;
   PcgScal& H = *c->h_sc;
   int outer = 0, inner_total = 0;
   const int max_outer = 40;
-  if (mg) {
-    mg_setup(c->pcg, c->mg, c->st);
-    c->launches += 1 + c->mg.nlev;
-  }
   for (;;) {
     ir_residual(c->pcg, c->st);
     c->launches += 3;
@@ -541,8 +532,7 @@ int refine(Ctx* c, int* total_inner) {
     H.stptst = rn / bn;
     if (rn < bn * zeta) break;
     if (outer >= max_outer) { H.ier = 1; break; }
-    if (mg) mg_inner_setup(c->pcg, c->mg, c->st);
-    else ir_inner_setup(c->pcg, c->pcgf, c->st);
+    ir_inner_setup(c->pcg, c->pcgf, c->st);
     c->launches += 2;
     PcgScal fi{};
     fi.zeta = std::max(1e-5, 0.5 * zeta * bn / rn);
@@ -554,31 +544,63 @@ int refine(Ctx* c, int* total_inner) {
     fi.hist_cap = 0;
     *c->h_scf = fi;
     CK(cudaMemcpyAsync(c->pcgf.sc, c->h_scf, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
-    if (mg) {
-      if (mg_loop(c->mg, c->bar, c->mg_blocks, c->st) != 0) return cuda_fail(cudaGetLastError(), "mg_loop", __LINE__);
-      c->launches += 1;
-      CK(cudaMemcpyAsync(c->h_scf, c->pcgf.sc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
-      CK(cudaStreamSynchronize(c->st));
-      if (!c->h_scf->done || c->h_scf->ier == SI3D_ETIMEOUT) return SI3D_ETIMEOUT;
-      if (c->h_scf->ier < 0) { H.ier = c->h_scf->ier; break; }   // inner breakdown: report it
-    } else {
-      int rci = iterate(c, c->pcgf.sc, c->h_scf, p.pcg_itmax, c->last_inner,
-                        [&](int par) { pcg_iteration_f(c->pcgf, par, c->st); },
-                        [&] { return pcg_loop_f(c->pcgf, c->bar, c->loop_blocks_f, c->st); });
-      if (rci) return rci;
-    }
+    int rci = iterate(c, c->pcgf.sc, c->h_scf, p.pcg_itmax, c->last_inner,
+                      [&](int par) { pcg_iteration_f(c->pcgf, par, c->st); },
+                      [&] { return pcg_loop_f(c->pcgf, c->bar, c->loop_blocks_f, c->st); });
+    if (rci) return rci;
     const int its = c->h_scf->in;
-    if (c->log_solves)
-      std::fprintf(stderr, "si3d: inner FP32 %s solve %d: %d iterations\n", mg ? "MG" : "MIC", outer + 1, its);
+    if (c->log_solves) std::fprintf(stderr, "si3d: inner FP32 MIC solve %d: %d iterations\n", outer + 1, its);
     inner_total += its;
     c->last_inner = std::max(its, 1);
-    if (mg) mg_correct(c->pcg, c->mg, c->st);
-    else ir_correct(c->pcg, c->pcgf, c->st);
+    ir_correct(c->pcg, c->pcgf, c->st);
     c->launches += 2;
     ++outer;
   }
   c->ir_outer += outer;
   *total_inner = inner_total;
+  return 0;
+}
+
+// The zeta solve of precision SI3D_MIXED_MG: FP64 refinement around FP32 multigrid-preconditioned CG,
+// all of it in one cooperative launch (k_mg.cu) on the grid image; the red-black system is not used.
+// `hist` holds per column (index l - 1) the correction of this solve one step earlier.
+int solve_mg(Ctx* c, const PcgScal& init, int x0, double* hist, int ier, int* iters, double* relres, int* ier_out) {
+  PcgScal& H = *c->h_sc;
+  H = PcgScal{};
+  H.zeta = init.zeta;
+  H.srelpr = init.srelpr;
+  H.itmax = init.itmax;
+  CK(cudaMemcpyAsync(c->mg.sc, c->h_sc, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
+  int rc = stage(c, ST_PCG_SETUP, c->mg.nlev, [&] { mg_setup(c->d, c->mg, x0, c->dz, hist, c->st); });
+  if (rc) return rc;
+  if (c->prof) CK(cudaEventRecord(c->pe0, c->st));
+  if (mg_solve(c->mg, c->bar, c->mg_blocks, c->st) != 0) return cuda_fail(cudaGetLastError(), "mg_solve", __LINE__);
+  c->launches += 1;
+  CK(cudaMemcpyAsync(c->h_sc, c->mg.sc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (!H.done || H.ier == SI3D_ETIMEOUT) return SI3D_ETIMEOUT;
+  if (c->prof) {
+    CK(cudaEventRecord(c->pe1, c->st));
+    CK(cudaEventSynchronize(c->pe1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->pe0, c->pe1);
+    c->prof_ms[ST_PCG_ITER] += ms;
+    c->prof_n[ST_PCG_ITER] += H.in;
+  }
+  c->ir_outer += H.q1;
+  if (c->log_solves) std::fprintf(stderr, "si3d: MG solve: %d inner iterations in %d passes\n", H.in, H.q1);
+  rc = stage(c, ST_PCG_FINISH, 1, [&] { mg_finish(c->d, c->mg, hist, c->st); });
+  if (rc) return rc;
+  if (c->rec_buf) {
+    float* slot = c->rec_buf + (size_t)(c->rec_count % c->rec_slots) * c->im1 * c->jm1 * 5;
+    learn::record(c->d, c->pix, c->feat, c->sigma, slot, c->st);
+    CK(cudaGetLastError());
+    c->rec_count++;
+  }
+  if (H.ier != 0) ier = H.ier;
+  *iters = H.in;
+  *relres = H.stptst;
+  *ier_out = ier;
   return 0;
 }
 
@@ -627,6 +649,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   }
   const bool use_hist = p.x0_mode == SI3D_X0_HIST;
   double* hist = use_hist ? c->hist + (size_t)c->hist_slot * (c->pcg.R.n + c->pcg.B.n + 2) : nullptr;
+  if (p.precision == SI3D_MIXED_MG) return solve_mg(c, init, x0, hist, ier, iters, relres, ier_out);
   int rc0 = stage(c, ST_PCG_SETUP, 7, [&] { pcg_setup(c->d, c->pcg, x0, c->dz, hist, &c->pcg.sc->negpiv, c->st); });
   if (rc0) return rc0;
   if (c->graph_mode) {
@@ -644,7 +667,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   }
   if (c->prof) CK(cudaEventRecord(c->pe0, c->st));
   int total_iters = 0;
-  if (p.precision == SI3D_MIXED_IR || p.precision == SI3D_MIXED_MG) {
+  if (p.precision == SI3D_MIXED_IR) {
     int rcir = refine(c, &total_iters);
     if (rcir) return rcir;
   } else {

@@ -27,6 +27,8 @@ def main(argv=None) -> int:
                          "mg: FP32 multigrid-preconditioned CG inside FP64 refinement")
     ap.add_argument("--itmax", type=int, default=2000)
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--autotune", action="store_true",
+                    help="pick the launch shapes of the column stages on the live state first")
     args = ap.parse_args(argv)
 
     from . import build, native, synth
@@ -40,7 +42,7 @@ def main(argv=None) -> int:
             synth.make(args.workload, run_dir)
             open(marker, "w").close()
     prec = {"fp64": native.SI3D_FP64, "mixed": native.SI3D_MIXED_IR, "mg": native.SI3D_MIXED_MG}[args.precision]
-    run = GpuRun(run_dir, device=args.device, pcg_itmax=args.itmax, precision=prec)
+    run = GpuRun(run_dir, device=args.device, pcg_itmax=args.itmax, precision=prec, autotune=args.autotune)
     try:
         for _ in range(args.steps):
             (s,) = run.run(1)
