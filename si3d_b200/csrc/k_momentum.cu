@@ -15,8 +15,10 @@
 //   coefficients and boundary terms (wind and bottom stress) and the Thomas sweeps with two
 //   right-hand sides - reading the staged ex/increment back and writing the final ag/ar.  The c'
 //   coefficients of the forward sweep go to the Thomas scratch array.
-// Both kernels evaluate the reference's expressions in its operation order, so ag, ar, eag and ear
-// are bit-identical to a single fused evaluation.
+// The cell kernel evaluates the reference's expressions in its operation order.  The column kernel
+// shares reciprocals between the tridiagonal coefficients (three divisions a layer instead of ten)
+// and sums the depth totals during the back substitution (bottom to top), so ag, ar, eag and ear
+// agree with the reference's arithmetic to a few units in the last place.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -234,31 +236,37 @@ __global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceM
   const int dO = (lO - l);   // column offset of the other face column
   int ik0 = IX(d, k1x, l);
   double n_hkp = huv[ik0 + P], n_upp1 = uvpp[ik0 + P], n_ex = agA[ik0], n_hdr = arA[ik0];
-  double n_avo = Av[ik0 + dO], n_avl = Av[ik0], n_avop = Av[ik0 + P + dO], n_avlp = Av[ik0 + P];
+  double n_avop = Av[ik0 + P + dO], n_avlp = Av[ik0 + P];
+  double avo = Av[ik0 + dO], avl = Av[ik0];   // Av of layer k (both columns); layer k + 1 is carried
+  // reciprocals shared between the coefficients: 1 / hk, 1 / hkm, 1 / (hkm + hk) (the previous
+  // layer's 1 / (hk + hkp)), and 1 / rhopx; three divisions a layer instead of ten
+  const double rrho = 1.0 / rhopx;
+  double rhk = 1.0 / hk, rhkm = 0.0, rkm = 0.0;
   for (int k = k1x; k <= kmx; ++k) {
     const int ik = IX(d, k, l);
     const double hkp = n_hkp, upp1 = n_upp1, ex = n_ex, hdr = n_hdr;
-    const double avo = n_avo, avl = n_avl, avop = n_avop, avlp = n_avlp;
+    const double avop = n_avop, avlp = n_avlp;
     if (k < kmx) {
       const int in = ik + P;
       n_hkp = huv[in + P]; n_upp1 = uvpp[in + P]; n_ex = agA[in]; n_hdr = arA[in];
-      n_avo = Av[in + dO]; n_avl = Av[in]; n_avop = Av[in + P + dO]; n_avlp = Av[in + P];
+      n_avop = Av[in + P + dO]; n_avlp = Av[in + P];
     }
+    const double rkp = 1.0 / (hk + hkp), rhkp = 1.0 / hkp;
     const double Avk = (k > k1x) ? 0.5 * (avo + avl) : 0.0;
     const double Avkp = (k < kmx) ? 0.5 * (avop + avlp) : 0.0;
     double vdiff = 0.0;
     if (nw >= 2) {
-      const double fk = (k > k1x) ? Avk * (upm - upk) / (hkm + hk) : 0.0;
-      const double fkp = (k < kmx) ? Avkp * (upk - upp1) / (hk + hkp) : 0.0;
+      const double fk = (k > k1x) ? Avk * (upm - upk) * rkm : 0.0;
+      const double fkp = (k < kmx) ? Avkp * (upk - upp1) * rkp : 0.0;
       vdiff = d.p.twodt * (fk - fkp) * 2. * (1. - theta);
     }
     double a1 = 0, a2, a3 = 0;
     if (nw == 1) {
       a2 = 1.0;
     } else {
-      if (k < kmx) a3 = -twodt1 * Avkp / (hkp * (hk + hkp)) * 2. * theta;
-      if (k > k1x) a1 = -twodt1 * Avk / (hkm * (hkm + hk)) * 2. * theta;
-      a2 = 1.0 - (hkm / hk) * a1 - (hkp / hk) * a3;
+      if (k < kmx) a3 = -twodt1 * Avkp * (rhkp * rkp) * 2. * theta;
+      if (k > k1x) a1 = -twodt1 * Avk * (rhkm * rkm) * 2. * theta;
+      a2 = 1.0 - (hkm * rhk) * a1 - (hkp * rhk) * a3;
     }
     if (d.p.ibc != 0) {
       if (k == k1x) bcl = hdr;
@@ -266,27 +274,31 @@ __global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceM
       else bcl = bcl + hdr_prev + hdr;
     }
     hdr_prev = hdr;
-    const double hh = hk / rhopx;
+    const double hh = hk * rrho;
     const double vtz = vdiff * tz;
     double gg = ex - hh * (bcl + ws0) * tz + vtz;
     if (k == k1x) { gg = gg + taus_g * twodt1; a2 = a2 + taus_a * twodt1; }
     if (k == kmx) a2 = a2 + taub * twodt1;
     double c1v, d1v, e1v;
     if (k == k1x) {
-      c1v = a3 / a2; d1v = gg / a2; e1v = hh / a2;
+      const double r = 1.0 / a2;
+      c1v = a3 * r; d1v = gg * r; e1v = hh * r;
     } else {
-      const double den = a2 - a1 * c1p;
-      c1v = a3 / den;
-      d1v = (gg - a1 * d1p) / den;
-      e1v = (hh - a1 * e1p) / den;
+      const double r = 1.0 / (a2 - a1 * c1p);
+      c1v = a3 * r;
+      d1v = (gg - a1 * d1p) * r;
+      e1v = (hh - a1 * e1p) * r;
     }
     cc[ik] = c1v; agA[ik] = d1v; arA[ik] = e1v;
     c1p = c1v; d1p = d1v; e1p = e1v;
     hkm = hk; hk = hkp;
     upm = upk; upk = upp1;
+    avo = avop; avl = avlp;
+    rhkm = rhk; rhk = rhkp; rkm = rkp;
   }
-  // back substitution, then the depth sums in ascending order
+  // back substitution, summing the depth totals on the way up
   double d2 = d1p, e2 = e1p;
+  double sg = d2, sr = e2;
 #pragma unroll 4
   for (int k = kmx - 1; k >= k1x; --k) {
     const int ik = IX(d, k, l);
@@ -294,12 +306,8 @@ __global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceM
     d2 = agA[ik] - c * d2;
     e2 = arA[ik] - c * e2;
     agA[ik] = d2; arA[ik] = e2;
+    sg += d2; sr += e2;
   }
-  double sg = 0, sr = 0;
-#pragma unroll 4
-  for (int k = k1x; k <= kmx; ++k) sg += agA[IX(d, k, l)];
-#pragma unroll 4
-  for (int k = k1x; k <= kmx; ++k) sr += arA[IX(d, k, l)];
   if (X) { d.s.eagx[l - 1] = sg; d.s.earx[l - 1] = sr; }
   else { d.s.eagy[l - 1] = sg; d.s.eary[l - 1] = sr; }
 }

@@ -356,38 +356,46 @@ __global__ void __launch_bounds__(NTB) k_imsal(Dev d) {
     sal[IX(d, k1s, l)] = v;
     return;
   }
-  // trid1 forward sweep: e in scratch, f in sal; inputs loaded one layer ahead
-  double hn_k = hn(k1s), hn_km = 0.0, e_prev = 0, f_prev = 0;
+  // trid1 forward sweep: e in scratch, f in sal; inputs (and the next layer's thickness) loaded one
+  // layer ahead; 1 / (hn(k) + hn(k+1)) is shared with the next layer's a1, so a layer takes two
+  // divisions
+  const double rt = 1.0 / twodt1;
+  double hn_k = hn(k1s), e_prev = 0, f_prev = 0, rkm = 0.0;
   int ik = IX(d, k1s, l);
-  double n_ds = sal[ik], n_dv = Dv[ik], n_dvp = Dv[ik + P];
+  double n_ds = sal[ik], n_dv = Dv[ik], n_dvp = Dv[ik + P], n_hn = hn(k1s + 1);
   for (int k = k1s; k <= kms; ++k, ik += P) {
-    const double ds = n_ds, dvk = n_dv, dvkp = n_dvp;
-    if (k < kms) { n_ds = sal[ik + P]; n_dv = Dv[ik + P]; n_dvp = Dv[ik + 2 * P]; }
-    const double hn_kp = (k < kms) ? hn(k + 1) : 0.0;
-    const double a3 = (k < kms) ? -dvkp / (hn_k + hn_kp) * 2. : 0.0;
+    const double ds = n_ds, dvk = n_dv, dvkp = n_dvp, hn_kp = (k < kms) ? n_hn : 0.0;
+    if (k < kms) {
+      n_ds = sal[ik + P]; n_dv = Dv[ik + P]; n_dvp = Dv[ik + 2 * P];
+      n_hn = (k + 1 < kms) ? hn(k + 2) : 0.0;
+    }
+    const double rkp = (k < kms) ? 1.0 / (hn_k + hn_kp) : 0.0;
+    const double a3 = (k < kms) ? -dvkp * rkp * 2. : 0.0;
     double a1 = 0.0;
-    if (k > k1s) a1 = -dvk / (hn_km + hn_k) * 2.;
-    const double a2 = hn_k / twodt1 - a1 - a3;
+    if (k > k1s) a1 = -dvk * rkm * 2.;
+    const double a2 = hn_k * rt - a1 - a3;
     const int kk = k - k1s + 1;
     if (kk == 1) {
-      e_prev = -a3 / a2;
-      f_prev = ds / a2;
+      const double r = 1.0 / a2;
+      e_prev = -a3 * r;
+      f_prev = ds * r;
       esc[ik] = e_prev;
       sal[ik] = f_prev;
-    } else if (kk < nw) {
-      const double den = a2 + a1 * e_prev;
-      const double e = -a3 / den;
-      const double f = (ds - a1 * f_prev) / den;
-      esc[ik] = e;
-      sal[ik] = f;
-      e_prev = e; f_prev = f;
     } else {
-      sal[ik] = (ds - a1 * f_prev) / (a2 + a1 * e_prev);
+      const double r = 1.0 / (a2 + a1 * e_prev);
+      const double f = (ds - a1 * f_prev) * r;
+      sal[ik] = f;
+      if (kk < nw) {
+        const double e = -a3 * r;
+        esc[ik] = e;
+        e_prev = e; f_prev = f;
+      }
     }
-    hn_km = hn_k;
     hn_k = hn_kp;
+    rkm = rkp;
   }
   double nxt = sal[IX(d, kms, l)];
+#pragma unroll 4
   for (int k = kms - 1; k >= k1s; --k) {
     nxt = esc[IX(d, k, l)] * nxt + sal[IX(d, k, l)];
     sal[IX(d, k, l)] = nxt;
