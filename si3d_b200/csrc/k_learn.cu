@@ -77,7 +77,7 @@ __global__ void k_prep(const float* __restrict__ prm, bf16* __restrict__ wfwd, b
 __global__ void __launch_bounds__(TP) k_stem(const float* __restrict__ feat, const float* __restrict__ w, int H, int W,
                                              bf16* __restrict__ X, float* __restrict__ Y) {
   __shared__ float sF[HT * WT * 4];
-  __shared__ float sW[9 * 4 * C + C];
+  __shared__ __align__(16) float sW[9 * 4 * C + C];
   const int b = blockIdx.z, i0 = blockIdx.y * TH, j0 = blockIdx.x * TW;
   for (int r = threadIdx.x; r < 9 * 4 * C + C; r += TP) sW[r] = w[r];
   for (int r = threadIdx.x; r < HT * WT; r += TP) {
@@ -98,8 +98,15 @@ __global__ void __launch_bounds__(TP) k_stem(const float* __restrict__ feat, con
 #pragma unroll
     for (int ci = 0; ci < 4; ++ci) {
       const float v = sF[(pi * WT + pj) * 4 + ci];
+      const float4* w4 = reinterpret_cast<const float4*>(&sW[(t * 4 + ci) * C]);
 #pragma unroll
-      for (int co = 0; co < C; ++co) acc[co] = acc[co] + v * sW[(t * 4 + ci) * C + co];
+      for (int q = 0; q < C / 4; ++q) {
+        const float4 w = w4[q];
+        acc[4 * q + 0] = __fmaf_rn(v, w.x, acc[4 * q + 0]);
+        acc[4 * q + 1] = __fmaf_rn(v, w.y, acc[4 * q + 1]);
+        acc[4 * q + 2] = __fmaf_rn(v, w.z, acc[4 * q + 2]);
+        acc[4 * q + 3] = __fmaf_rn(v, w.w, acc[4 * q + 3]);
+      }
     }
   }
   const size_t p = ((size_t)b * H + gi) * W + gj;
@@ -212,7 +219,7 @@ __global__ void __launch_bounds__(128) k_conv32(const bf16* __restrict__ Xin, co
 __global__ void __launch_bounds__(TP) k_head(const bf16* __restrict__ X, const float* __restrict__ w, int H, int W,
                                              float* __restrict__ out) {
   __shared__ __align__(16) bf16 sX[HT * WT * XS];
-  __shared__ float sW[9 * C + 1];
+  __shared__ __align__(16) float sW[9 * C + 1];
   const int b = blockIdx.z, i0 = blockIdx.y * TH, j0 = blockIdx.x * TW;
   for (int r = threadIdx.x; r < 9 * C + 1; r += TP) sW[r] = w[r];
   for (int r = threadIdx.x; r < HT * WT * 4; r += TP) {
@@ -229,9 +236,20 @@ __global__ void __launch_bounds__(TP) k_head(const bf16* __restrict__ X, const f
   if (gi >= H || gj >= W) return;
   float acc = 0.f;
   for (int t = 0; t < 9; ++t) {
-    const bf16* xp = &sX[((ti + t / 3) * WT + tj + t % 3) * XS];
+    const uint4* xp = reinterpret_cast<const uint4*>(&sX[((ti + t / 3) * WT + tj + t % 3) * XS]);
+    const float4* w4 = reinterpret_cast<const float4*>(&sW[t * C]);
 #pragma unroll
-    for (int ci = 0; ci < C; ++ci) acc = acc + __bfloat162float(xp[ci]) * sW[t * C + ci];
+    for (int q = 0; q < C / 8; ++q) {
+      const uint4 xv = xp[q];
+      const __nv_bfloat162* x2 = reinterpret_cast<const __nv_bfloat162*>(&xv);
+      const float4 wa = w4[2 * q], wb = w4[2 * q + 1];
+      const float2 f0 = __bfloat1622float2(x2[0]), f1 = __bfloat1622float2(x2[1]);
+      const float2 f2 = __bfloat1622float2(x2[2]), f3 = __bfloat1622float2(x2[3]);
+      acc = __fmaf_rn(f0.x, wa.x, acc); acc = __fmaf_rn(f0.y, wa.y, acc);
+      acc = __fmaf_rn(f1.x, wa.z, acc); acc = __fmaf_rn(f1.y, wa.w, acc);
+      acc = __fmaf_rn(f2.x, wb.x, acc); acc = __fmaf_rn(f2.y, wb.y, acc);
+      acc = __fmaf_rn(f3.x, wb.z, acc); acc = __fmaf_rn(f3.y, wb.w, acc);
+    }
   }
   out[((size_t)b * H + gi) * W + gj] = acc + sW[9 * C];
 }
