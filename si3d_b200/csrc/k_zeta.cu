@@ -54,11 +54,12 @@ __global__ void k_matcon(Dev d) {
   d.s.sx[l - 1] = sxl;
   d.s.sy[l - 1] = syl;
   const int kms = NB(d.g.kmz, l);
+  const double rdx = 1.0 / d.p.dx, rdy = 1.0 / d.p.dy;   // divisions by the grid constants as products
   double sum = 0;
   #pragma unroll 4
   for (int k = d.g.k1; k <= kms; ++k)
-    sum += (f_uhpp[IX(d, k, l)] - f_uhpp[IX(d, k, lW)]) / d.p.dx +
-           (f_vhpp[IX(d, k, l)] - f_vhpp[IX(d, k, lS)]) / d.p.dy;
+    sum += (f_uhpp[IX(d, k, l)] - f_uhpp[IX(d, k, lW)]) * rdx +
+           (f_vhpp[IX(d, k, l)] - f_vhpp[IX(d, k, lS)]) * rdy;
   const double ddv = dt1 * sum;
   d.s.dd[l - 1] = ddv;
   d.s.qq[l - 1] = d.s.spp[l - 1] - dtdx1 * (d.s.eagx[l - 1] - d.s.eagx[lW - 1]) -
