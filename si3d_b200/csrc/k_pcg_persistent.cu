@@ -158,7 +158,7 @@ __device__ __noinline__ void lz_chgcon(PcgScal* S, double* tri, int ip, double a
 // TEST2: stopping test 2 with chgcon's adaptive emin (test 5 otherwise); a separate instantiation keeps
 // the test-5 loop free of the eigenvalue code.
 template <typename T, bool TEST2>
-__global__ void __launch_bounds__(QB, 3) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
+__global__ void __launch_bounds__(QB, 4) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
   __shared__ double sh[8 * 4 + 4];
   __shared__ int s_flag;
   const PcgColorT<T> &R = P.R, &B = P.B;
