@@ -36,32 +36,36 @@ __device__ __forceinline__ int vlim(const Dev& d, int l) {
 }
 
 // ------------------------------------------------------------- slayer_h
-__global__ void k_slayer_h(Dev d) {
+template <int CLN>
+__global__ void __launch_bounds__(32 * CLN) k_slayer_h(Dev d) {
   double* __restrict__ f_h = d.f.h;
   double* __restrict__ f_hp = d.f.hp;
   double* __restrict__ f_hu = d.f.hu;
   double* __restrict__ f_hup = d.f.hup;
   double* __restrict__ f_hv = d.f.hv;
   double* __restrict__ f_hvp = d.f.hvp;
-  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  const int l = blockIdx.x * 32 + threadIdx.x + 1;
   if (l > d.g.lm) return;
+  const int ty = threadIdx.y;
   const int km1 = d.g.km1;
   const int kz = d.s.k1z[l - 1], ku = d.s.k1u[l - 1], kv = d.s.k1v[l - 1];
   double* __restrict__ h = f_h; double* __restrict__ hu = f_hu; double* __restrict__ hv = f_hv;
   const double* __restrict__ hp = f_hp; const double* __restrict__ hup = f_hup; const double* __restrict__ hvp = f_hvp;
   const int zL = zlim(d, l), uL = ulim(d, l), vL = vlim(d, l);
   #pragma unroll 4
-  for (int k = 1; k <= min(kz - 1, zL); ++k) h[IX(d, k, l)] = hp[IX(d, k, l)];
+  for (int k = 1 + ty; k <= min(kz - 1, zL); k += CLN) h[IX(d, k, l)] = hp[IX(d, k, l)];
   #pragma unroll 4
-  for (int k = 1; k <= min(ku - 1, uL); ++k) hu[IX(d, k, l)] = hup[IX(d, k, l)];
+  for (int k = 1 + ty; k <= min(ku - 1, uL); k += CLN) hu[IX(d, k, l)] = hup[IX(d, k, l)];
   #pragma unroll 4
-  for (int k = 1; k <= min(kv - 1, vL); ++k) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
+  for (int k = 1 + ty; k <= min(kv - 1, vL); k += CLN) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
   #pragma unroll 4
-  for (int k = kz + 2; k <= zL; ++k) h[IX(d, k, l)] = hp[IX(d, k, l)];
+  for (int k = kz + 2 + ty; k <= zL; k += CLN) h[IX(d, k, l)] = hp[IX(d, k, l)];
   #pragma unroll 4
-  for (int k = ku + 1; k <= uL; ++k) hu[IX(d, k, l)] = hup[IX(d, k, l)];
+  for (int k = ku + 1 + ty; k <= uL; k += CLN) hu[IX(d, k, l)] = hup[IX(d, k, l)];
   #pragma unroll 4
-  for (int k = kv + 2; k <= vL; ++k) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
+  for (int k = kv + 2 + ty; k <= vL; k += CLN) hv[IX(d, k, l)] = hvp[IX(d, k, l)];
+  // the copies above leave out the surface layers written below, so the lanes never overlap
+  if (ty != 0) return;
   // Surface layers.  A column whose surface index has reached the bottom level (every layer
   // dry) is left untouched: the reference would read zlevel past km1 there.
   const double sl = d.s.s[l - 1];
@@ -103,8 +107,8 @@ __global__ void k_slayer_h(Dev d) {
 }
 
 // ------------------------------------------------------------- vel (uh, vh, k1u, k1v)
-template <int IEQ>
-__global__ void k_vel_uv(Dev d, const int* __restrict__ cols, int ncols) {
+template <int IEQ, int CLN>
+__global__ void __launch_bounds__(32 * CLN) k_vel_uv(Dev d, const int* __restrict__ cols, int ncols) {
   double* __restrict__ f_agx = d.f.agx;
   double* __restrict__ f_agy = d.f.agy;
   double* __restrict__ f_arx = d.f.arx;
@@ -113,21 +117,26 @@ __global__ void k_vel_uv(Dev d, const int* __restrict__ cols, int ncols) {
   double* __restrict__ f_hv = d.f.hv;
   double* __restrict__ f_uh = d.f.uh;
   double* __restrict__ f_vh = d.f.vh;
-  const int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= ncols) return;
-  const int l = cols[t];
+  const int t = blockIdx.x * 32 + threadIdx.x, ty = threadIdx.y;
+  const bool act = t < ncols;
   const bool X = IEQ == 1;
-  const int lO = X ? NB(d.g.lEC, l) : NB(d.g.lNC, l);
-  const int kmx = min(NB(d.g.kmz, lO), NB(d.g.kmz, l));
+  int l = 0, k0 = 0;
   int* k1 = X ? d.s.k1u : d.s.k1v;
-  const int k0 = k1[l - 1];
-  const double gth = (X ? d.p.gdtdx : d.p.gdtdy) * d.tz;
-  const double c = gth * 1000. * (d.s.s[lO - 1] - d.s.s[l - 1]);
   double* uv = X ? f_uh : f_vh;
-  const double* ag = X ? f_agx : f_agy;
-  const double* ar = X ? f_arx : f_ary;
-  #pragma unroll 4
-  for (int k = k0; k <= kmx; ++k) uv[IX(d, k, l)] = ag[IX(d, k, l)] - c * ar[IX(d, k, l)];
+  if (act) {
+    l = cols[t];
+    const int lO = X ? NB(d.g.lEC, l) : NB(d.g.lNC, l);
+    const int kmx = min(NB(d.g.kmz, lO), NB(d.g.kmz, l));
+    k0 = k1[l - 1];
+    const double gth = (X ? d.p.gdtdx : d.p.gdtdy) * d.tz;
+    const double c = gth * 1000. * (d.s.s[lO - 1] - d.s.s[l - 1]);
+    const double* ag = X ? f_agx : f_agy;
+    const double* ar = X ? f_arx : f_ary;
+#pragma unroll 4
+    for (int k = k0 + ty; k <= kmx; k += CLN) uv[IX(d, k, l)] = ag[IX(d, k, l)] - c * ar[IX(d, k, l)];
+  }
+  __syncthreads();   // the surface correction reads layers written by other lanes
+  if (!act || ty != 0) return;
   const double* huv = X ? f_hu : f_hv;
   // (a face column with every layer dry, k0 = km1, is never reached: the reference would write
   //  past the last level there)
@@ -406,44 +415,49 @@ __global__ void __launch_bounds__(NTB) k_imsal(Dev d) {
 }
 
 // ------------------------------------------------------------- vel2 (layer_h + wetting)
-__global__ void k_vel2(Dev d) {
+template <int CLN>
+__global__ void __launch_bounds__(32 * CLN) k_vel2(Dev d) {
   double* __restrict__ f_h = d.f.h;
   double* __restrict__ f_hu = d.f.hu;
   double* __restrict__ f_hv = d.f.hv;
   double* __restrict__ f_uh = d.f.uh;
   double* __restrict__ f_vh = d.f.vh;
-  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (l > d.g.lm) return;
-  const int kms = NB(d.g.kmz, l);
-  const double sl = d.s.s[l - 1];
+  const int l = blockIdx.x * 32 + threadIdx.x + 1, ty = threadIdx.y;
+  const bool act = l <= d.g.lm;
+  if (act) {
+    const int kms = NB(d.g.kmz, l);
+    const double sl = d.s.s[l - 1];
+#pragma unroll 4
+    for (int k = d.g.k1 + ty; k <= kms; k += CLN) {
+      double v = fmin(zl(d, k + 1), d.g.hhs[l - 1]) - fmax(zl(d, k), -sl);
+      if (v <= HMIN) v = ZERO;
+      f_h[IX(d, k, l)] = v;
+    }
+    if (ewet(d, l)) {
+      const int lE = NB(d.g.lEC, l);
+      const int kmx = min(kms, NB(d.g.kmz, lE));
+      const double sm = fmax(sl, d.s.s[lE - 1]);
   #pragma unroll 4
-  for (int k = d.g.k1; k <= kms; ++k) {
-    double v = fmin(zl(d, k + 1), d.g.hhs[l - 1]) - fmax(zl(d, k), -sl);
-    if (v <= HMIN) v = ZERO;
-    f_h[IX(d, k, l)] = v;
-  }
-  if (ewet(d, l)) {
-    const int lE = NB(d.g.lEC, l);
-    const int kmx = min(kms, NB(d.g.kmz, lE));
-    const double sm = fmax(sl, d.s.s[lE - 1]);
-    #pragma unroll 4
-    for (int k = d.g.k1; k <= kmx; ++k) {
-      double v = fmin(zl(d, k + 1), d.g.hhu[l - 1]) - fmax(zl(d, k), -sm);
-      if (v <= HMIN) v = ZERO;
-      f_hu[IX(d, k, l)] = v;
+      for (int k = d.g.k1 + ty; k <= kmx; k += CLN) {
+        double v = fmin(zl(d, k + 1), d.g.hhu[l - 1]) - fmax(zl(d, k), -sm);
+        if (v <= HMIN) v = ZERO;
+        f_hu[IX(d, k, l)] = v;
+      }
+    }
+    if (nwet(d, l)) {
+      const int lN = NB(d.g.lNC, l);
+      const int kmy = min(kms, NB(d.g.kmz, lN));
+      const double sm = fmax(sl, d.s.s[lN - 1]);
+  #pragma unroll 4
+      for (int k = d.g.k1 + ty; k <= kmy; k += CLN) {
+        double v = fmin(zl(d, k + 1), d.g.hhv[l - 1]) - fmax(zl(d, k), -sm);
+        if (v <= HMIN) v = ZERO;
+        f_hv[IX(d, k, l)] = v;
+      }
     }
   }
-  if (nwet(d, l)) {
-    const int lN = NB(d.g.lNC, l);
-    const int kmy = min(kms, NB(d.g.kmz, lN));
-    const double sm = fmax(sl, d.s.s[lN - 1]);
-    #pragma unroll 4
-    for (int k = d.g.k1; k <= kmy; ++k) {
-      double v = fmin(zl(d, k + 1), d.g.hhv[l - 1]) - fmax(zl(d, k), -sm);
-      if (v <= HMIN) v = ZERO;
-      f_hv[IX(d, k, l)] = v;
-    }
-  }
+  __syncthreads();   // the surface corrections read layers written by other lanes
+  if (!act || ty != 0) return;
   if (ewet(d, l)) {
     const int k = d.s.k1u[l - 1];
     const double hkm = f_hu[IX(d, k - 1, l)];
@@ -781,11 +795,15 @@ __global__ void k_column_tridiag(int n, int nsys, const double* a, const double*
 
 static inline int grid_of(int n) { return (n + TB - 1) / TB; }
 
-void launch_slayer_h(const Dev& d, cudaStream_t st) { k_slayer_h<<<grid_of(d.g.lm), TB, 0, st>>>(d); }
+constexpr int BK_LANES = 4;   // layer lanes of the cell-parallel bookkeeping and velocity kernels
+
+void launch_slayer_h(const Dev& d, cudaStream_t st) {
+  k_slayer_h<BK_LANES><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
+}
 
 void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cudaStream_t st) {
-  if (nce > 0) k_vel_uv<1><<<grid_of(nce), TB, 0, st>>>(d, ce, nce);
-  if (ncn > 0) k_vel_uv<2><<<grid_of(ncn), TB, 0, st>>>(d, cn, ncn);
+  if (nce > 0) k_vel_uv<1, BK_LANES><<<(nce + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d, ce, nce);
+  if (ncn > 0) k_vel_uv<2, BK_LANES><<<(ncn + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d, cn, ncn);
   k_cont1<<<grid_of(d.g.lm), TB, 0, st>>>(d);
 }
 
@@ -803,9 +821,9 @@ void launch_exsal_imsal(const Dev& d, const Tune& tu, cudaStream_t st) {
   }
 }
 
-void launch_vel2(const Dev& d, cudaStream_t st) { k_vel2<<<grid_of(d.g.lm), TB, 0, st>>>(d); }
-
-constexpr int BK_LANES = 4;   // layer lanes of the cell-parallel bookkeeping kernels
+void launch_vel2(const Dev& d, cudaStream_t st) {
+  k_vel2<BK_LANES><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
+}
 
 void launch_settrap(const Dev& d, cudaStream_t st) {
   k_half_zeta<<<grid_of(d.g.lm), TB, 0, st>>>(d, 1);
