@@ -40,6 +40,11 @@ STAGE_STREAMS = {"momentum_x": (14, "N3"), "momentum_y": (14, "N3"), "matcon": (
 # levels (a third of level 0 together) not counted.
 MG_ITER_STREAMS = 15
 
+WORKLOAD_DESC = {
+    "c2": "c2: 2000x1000 cells x 60 layers, seeded random bathymetry and wind stress, dt 30 s, itrap=1 niter=2, "
+          "zeta solve to relative residual 1e-12 (test 5)",
+}
+
 
 def _dist():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
@@ -137,12 +142,13 @@ def counts(run_dir: str):
     return lm, n3
 
 
-def cpu_sample(name: str, threads: int) -> dict:
+def cpu_sample(name: str, threads: int, steps: int = 0, warmup: int = 0) -> dict:
     """The CPU restatement of the reference timed on a window of the workload (same layers,
     bathymetry and forcing generators), extrapolated linearly in wet 3-D cells.  The column stages
     run on `threads` host threads; the zeta solve is serial, as the reference runs it on thread 0.
     (Linear extrapolation understates the solve at full size, whose iteration count grows with the
-    domain.)"""
+    domain.)  With `steps`, exactly `warmup` untimed and `steps` timed window steps; otherwise up to
+    20 steps or 10 s."""
     from si3d_b200 import synth
     from oracle import pyoracle
     full = synth.config(name)
@@ -160,13 +166,13 @@ def cpu_sample(name: str, threads: int) -> dict:
     os.environ["SI3D_ORACLE_THREADS"] = str(threads)   # read once, at the oracle's first column loop
     pyoracle.build()
     o = pyoracle.OracleRun(d, ordering=1, pcg_itmax=2000)
-    o.run(1)                      # first step: trapezoidal start
+    o.run(1 + max(warmup, 0))    # first step: trapezoidal start
     t0 = time.perf_counter()
     nsteps = 0
     while True:
         o.run(1)
         nsteps += 1
-        if time.perf_counter() - t0 > 10.0 or nsteps >= 20:
+        if (steps > 0 and nsteps >= steps) or (steps <= 0 and (time.perf_counter() - t0 > 10.0 or nsteps >= 20)):
             break
     dt = (time.perf_counter() - t0) / nsteps
     lm_w, n3_w = counts(d)
@@ -275,12 +281,14 @@ def main() -> int:
             return 0
         threads = os.cpu_count() or 1
         lm_full, n3_full = counts(workload_dir(args.workload, 0))
-        smp = cpu_sample(args.workload, threads)
+        smp = cpu_sample(args.workload, threads, steps=args.steps, warmup=args.warmup)
         v = smp["window_s_per_step"] * n3_full / smp["n3"]
         line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "s/timestep", "n_gpus": args.gpus,
-                "steps": smp["steps"], "warmup": 1, "ms_per_step": v * 1e3, "higher_is_better": False,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": f"{args.workload} 2000x1000x60 closed basin, plain FP64, PCG test 5 at 1e-12"},
+                "config": {"workload": WORKLOAD_DESC.get(args.workload, args.workload), "form": "plain_fp64",
+                           "lm": lm_full, "n3": n3_full, "parallelism": "replicas x1",
+                           "l2": "host run; no GPU caches involved"},
                 "cpu_baseline": {"value": v, "unit": "s/timestep", "cores": threads, "kind": "port",
                                  "sample": f"{smp['steps']} steps of a {smp['window']} window, extrapolated by wet "
                                            f"3-D cells ({smp['n3']} -> {n3_full}); column stages on {threads} threads, "
@@ -434,8 +442,7 @@ def main() -> int:
                       "learned_mixed": "f64 (fp32 inner solves, bf16 guess net)",
                       "mg_mixed": "f64 (fp32 multigrid inner solves)",
                       "learned_mg": "f64 (fp32 multigrid inner solves, bf16 guess net)"}[head_form], "data": "synthetic",
-            "config": {"workload": f"{args.workload}: 2000x1000 cells x 60 layers, seeded random bathymetry and wind "
-                                   f"stress, dt 30 s, itrap=1 niter=2, zeta solve to relative residual 1e-12 (test 5)",
+            "config": {"workload": WORKLOAD_DESC.get(args.workload, args.workload),
                        "form": head_form, "lm": lm, "n3": n3, "parallelism": f"replicas x{ws}",
                        "l2": "state (~25 GB) far larger than L2; no flush needed"},
             "pcg_iters_per_step": head["pcg_iters_per_step"], "pcg_s_per_step": head["pcg_s_per_step"],
