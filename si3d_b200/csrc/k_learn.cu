@@ -133,82 +133,89 @@ enum { CONV_FWD = 0, CONV_BWD = 1 };
 // out[p][n] = sum_{tap, k} in[p + off(tap)][k] * Wk[tap][n][k].
 // CONV_FWD: y = out + bias; X_out = bf16(X_in + ReLU(y)); Y (optional) = y.
 // CONV_BWD: G_out = G_in + out.
+// Persistent blocks: the weights go to shared memory once per block, which then loops over 8 x 16
+// pixel tiles (tile = blockIdx.x, blockIdx.x + gridDim.x, ...).
 template <int MODE>
 __global__ void __launch_bounds__(128) k_conv32(const bf16* __restrict__ Xin, const bf16* __restrict__ Wk,
-                                                const float* __restrict__ bias, int H, int W, bf16* __restrict__ Xout,
-                                                float* __restrict__ Y, const float* __restrict__ Gin,
-                                                float* __restrict__ Gout) {
+                                                const float* __restrict__ bias, int B, int H, int W,
+                                                bf16* __restrict__ Xout, float* __restrict__ Y,
+                                                const float* __restrict__ Gin, float* __restrict__ Gout) {
   __shared__ __align__(16) bf16 sX[HT * WT * XS];
   __shared__ __align__(16) bf16 sW[9 * C * XS];
-  const int b = blockIdx.z, i0 = blockIdx.y * TH, j0 = blockIdx.x * TW;
   for (int r = threadIdx.x; r < 9 * C * 4; r += 128) {
     const int row = r >> 2, part = r & 3;
     *reinterpret_cast<uint4*>(&sW[row * XS + part * 8]) = *reinterpret_cast<const uint4*>(&Wk[row * C + part * 8]);
   }
-  for (int r = threadIdx.x; r < HT * WT * 4; r += 128) {
-    const int pix = r >> 2, part = r & 3;
-    const int gi = i0 + pix / WT - 1, gj = j0 + pix % WT - 1;
-    uint4 v = make_uint4(0u, 0u, 0u, 0u);
-    if (gi >= 0 && gi < H && gj >= 0 && gj < W)
-      v = *reinterpret_cast<const uint4*>(&Xin[(((size_t)b * H + gi) * W + gj) * C + part * 8]);
-    *reinterpret_cast<uint4*>(&sX[pix * XS + part * 8]) = v;
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-  float acc[2][4][4];
+  const int ntj = (W + TW - 1) / TW, nti = (H + TH - 1) / TH, ntiles = B * nti * ntj;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int b = tile / (nti * ntj), rem = tile - b * (nti * ntj);
+    const int i0 = (rem / ntj) * TH, j0 = (rem % ntj) * TW;
+    __syncthreads();   // the previous tile's readers of sX are done
+    for (int r = threadIdx.x; r < HT * WT * 4; r += 128) {
+      const int pix = r >> 2, part = r & 3;
+      const int gi = i0 + pix / WT - 1, gj = j0 + pix % WT - 1;
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (gi >= 0 && gi < H && gj >= 0 && gj < W)
+        v = *reinterpret_cast<const uint4*>(&Xin[(((size_t)b * H + gi) * W + gj) * C + part * 8]);
+      *reinterpret_cast<uint4*>(&sX[pix * XS + part * 8]) = v;
+    }
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    float acc[2][4][4];
 #pragma unroll
-  for (int r = 0; r < 2; ++r)
+    for (int r = 0; r < 2; ++r)
 #pragma unroll
-    for (int nt = 0; nt < 4; ++nt)
+      for (int nt = 0; nt < 4; ++nt)
 #pragma unroll
-      for (int e = 0; e < 4; ++e) acc[r][nt][e] = 0.f;
+        for (int e = 0; e < 4; ++e) acc[r][nt][e] = 0.f;
 #pragma unroll 1
-  for (int t = 0; t < 9; ++t) {
-    const int di = t / 3 - 1, dj = t % 3 - 1;
+    for (int t = 0; t < 9; ++t) {
+      const int di = t / 3 - 1, dj = t % 3 - 1;
 #pragma unroll
-    for (int cb = 0; cb < 2; ++cb) {
-      uint32_t bq[4][2];
+      for (int cb = 0; cb < 2; ++cb) {
+        uint32_t bq[4][2];
 #pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const bf16* wp = &sW[(t * C + nt * 8 + g) * XS + cb * 16 + q * 2];
-        bq[nt][0] = *reinterpret_cast<const uint32_t*>(wp);
-        bq[nt][1] = *reinterpret_cast<const uint32_t*>(wp + 8);
-      }
+        for (int nt = 0; nt < 4; ++nt) {
+          const bf16* wp = &sW[(t * C + nt * 8 + g) * XS + cb * 16 + q * 2];
+          bq[nt][0] = *reinterpret_cast<const uint32_t*>(wp);
+          bq[nt][1] = *reinterpret_cast<const uint32_t*>(wp + 8);
+        }
 #pragma unroll
-      for (int r = 0; r < 2; ++r) {
-        const int ty = warp * 2 + r;
-        const bf16* xp = &sX[((ty + 1 + di) * WT + (g + 1 + dj)) * XS + cb * 16 + q * 2];
-        const uint32_t a0 = *reinterpret_cast<const uint32_t*>(xp);
-        const uint32_t a1 = *reinterpret_cast<const uint32_t*>(xp + 8 * XS);
-        const uint32_t a2 = *reinterpret_cast<const uint32_t*>(xp + 8);
-        const uint32_t a3 = *reinterpret_cast<const uint32_t*>(xp + 8 * XS + 8);
+        for (int r = 0; r < 2; ++r) {
+          const int ty = warp * 2 + r;
+          const bf16* xp = &sX[((ty + 1 + di) * WT + (g + 1 + dj)) * XS + cb * 16 + q * 2];
+          const uint32_t a0 = *reinterpret_cast<const uint32_t*>(xp);
+          const uint32_t a1 = *reinterpret_cast<const uint32_t*>(xp + 8 * XS);
+          const uint32_t a2 = *reinterpret_cast<const uint32_t*>(xp + 8);
+          const uint32_t a3 = *reinterpret_cast<const uint32_t*>(xp + 8 * XS + 8);
 #pragma unroll
-        for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[r][nt], a0, a1, a2, a3, bq[nt][0], bq[nt][1]);
+          for (int nt = 0; nt < 4; ++nt) mma_bf16(acc[r][nt], a0, a1, a2, a3, bq[nt][0], bq[nt][1]);
+        }
       }
     }
-  }
 #pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int ty = warp * 2 + r, gi = i0 + ty;
+    for (int r = 0; r < 2; ++r) {
+      const int ty = warp * 2 + r, gi = i0 + ty;
 #pragma unroll
-    for (int half = 0; half < 2; ++half) {
-      const int tj = g + 8 * half, gj = j0 + tj;
-      if (gi >= H || gj >= W) continue;
-      const size_t p = ((size_t)b * H + gi) * W + gj;
+      for (int half = 0; half < 2; ++half) {
+        const int tj = g + 8 * half, gj = j0 + tj;
+        if (gi >= H || gj >= W) continue;
+        const size_t p = ((size_t)b * H + gi) * W + gj;
 #pragma unroll
-      for (int nt = 0; nt < 4; ++nt) {
-        const int co = nt * 8 + 2 * q;
-        const float v0 = acc[r][nt][2 * half], v1 = acc[r][nt][2 * half + 1];
-        if (MODE == CONV_FWD) {
-          const float y0 = v0 + bias[co], y1 = v1 + bias[co + 1];
-          const bf16* xc = &sX[((ty + 1) * WT + tj + 1) * XS + co];
-          const float x0 = __bfloat162float(xc[0]), x1 = __bfloat162float(xc[1]);
-          if (Y) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
-          *reinterpret_cast<__nv_bfloat162*>(Xout + p * C + co) =
-              __floats2bfloat162_rn(x0 + fmaxf(y0, 0.f), x1 + fmaxf(y1, 0.f));
-        } else {
-          const float2 gi2 = *reinterpret_cast<const float2*>(Gin + p * C + co);
-          *reinterpret_cast<float2*>(Gout + p * C + co) = make_float2(gi2.x + v0, gi2.y + v1);
+        for (int nt = 0; nt < 4; ++nt) {
+          const int co = nt * 8 + 2 * q;
+          const float v0 = acc[r][nt][2 * half], v1 = acc[r][nt][2 * half + 1];
+          if (MODE == CONV_FWD) {
+            const float y0 = v0 + bias[co], y1 = v1 + bias[co + 1];
+            const bf16* xc = &sX[((ty + 1) * WT + tj + 1) * XS + co];
+            const float x0 = __bfloat162float(xc[0]), x1 = __bfloat162float(xc[1]);
+            if (Y) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
+            *reinterpret_cast<__nv_bfloat162*>(Xout + p * C + co) =
+                __floats2bfloat162_rn(x0 + fmaxf(y0, 0.f), x1 + fmaxf(y1, 0.f));
+          } else {
+            const float2 gi2 = *reinterpret_cast<const float2*>(Gin + p * C + co);
+            *reinterpret_cast<float2*>(Gout + p * C + co) = make_float2(gi2.x + v0, gi2.y + v1);
+          }
         }
       }
     }
@@ -545,6 +552,17 @@ void prepare(const Workspace& ws, const float* params, cudaStream_t st) {
   k_prep<<<(n + 255) / 256, 256, 0, st>>>(params, ws.wfwd, ws.wbwd, ws.stem, ws.head);
 }
 
+// Persistent grid of the convolution: every resident block of the device, at most one per tile.
+template <int MODE>
+int conv_blocks(int B, int H, int W) {
+  int dev = 0, sms = 1, occ = 1;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv32<MODE>, 128, 0);
+  const long long ntiles = (long long)B * ((H + TH - 1) / TH) * ((W + TW - 1) / TW);
+  return (int)std::max(1LL, std::min(ntiles, (long long)sms * std::max(occ, 1)));
+}
+
 void forward(const Workspace& ws, const float* params, const float* feat, int B, int H, int W, float* out,
              cudaStream_t st) {
   const float* bias0 = params + OFF_BLK + 9 * C * C;
@@ -553,8 +571,9 @@ void forward(const Workspace& ws, const float* params, const float* feat, int B,
   for (int k = 0; k < SI3D_NET_BLOCKS; ++k) {
     const bf16* xin = ws.training ? ws.x[k] : ws.x[k & 1];
     bf16* xout = ws.training ? ws.x[k + 1] : ws.x[(k + 1) & 1];
-    k_conv32<CONV_FWD><<<grid, 128, 0, st>>>(xin, ws.wfwd + (size_t)k * 9 * C * C, bias0 + (size_t)k * BLK_SZ, H, W,
-                                             xout, ws.training ? ws.y[k + 1] : nullptr, nullptr, nullptr);
+    k_conv32<CONV_FWD><<<conv_blocks<CONV_FWD>(B, H, W), 128, 0, st>>>(
+        xin, ws.wfwd + (size_t)k * 9 * C * C, bias0 + (size_t)k * BLK_SZ, B, H, W, xout,
+        ws.training ? ws.y[k + 1] : nullptr, nullptr, nullptr);
   }
   const bf16* xl = ws.training ? ws.x[SI3D_NET_BLOCKS] : ws.x[SI3D_NET_BLOCKS & 1];
   k_head<<<grid, TP, 0, st>>>(xl, ws.head, H, W, out);
@@ -575,8 +594,8 @@ void backward(const Workspace& ws, const float* feat, const float* gout, int B, 
     k_relu_bwd<<<eb, 256, 0, st>>>(G, ws.y[k + 1], ws.DY, ws.DYb, n);
     k_wgrad<C, C, bf16><<<WG_BLOCKS, 256, 0, st>>>(ws.x[k], ws.DY, B, H, W, ws.part);
     k_wgrad_reduce<<<(BLK_SZ + 255) / 256, 256, 0, st>>>(ws.part, WG_BLOCKS, BLK_SZ, grad + OFF_BLK + k * BLK_SZ);
-    k_conv32<CONV_BWD><<<grid, 128, 0, st>>>(ws.DYb, ws.wbwd + (size_t)k * 9 * C * C, nullptr, H, W, nullptr, nullptr,
-                                             G, Gn);
+    k_conv32<CONV_BWD><<<conv_blocks<CONV_BWD>(B, H, W), 128, 0, st>>>(ws.DYb, ws.wbwd + (size_t)k * 9 * C * C, nullptr,
+                                                                       B, H, W, nullptr, nullptr, G, Gn);
     std::swap(G, Gn);
   }
   k_relu_bwd<<<eb, 256, 0, st>>>(G, ws.y[0], ws.DY, nullptr, n);
