@@ -147,6 +147,19 @@ def test_untrained_network_is_the_plain_guess(native_libs, run_dirs):
     assert np.abs(a["zeta"] - b["zeta"]).max() <= 1e-12
 
 
+def test_untrained_network_with_multigrid_solves(native_libs, run_dirs):
+    """The learned guess feeds the multigrid-mixed solve as well: an untrained network reproduces the
+    x0 = SI3D_X0_LAST multigrid run iteration for iteration, at the unchanged tolerance."""
+    from si3d_b200 import native
+    from si3d_b200.learn import init_params, iterations
+    d = run_dirs["t1"]
+    a = iterations(d, 4, params=None, x0_mode=native.SI3D_X0_LAST, precision=native.SI3D_MIXED_MG)
+    b = iterations(d, 4, params=init_params(0), x0_mode=native.SI3D_X0_LEARNED, precision=native.SI3D_MIXED_MG)
+    assert a["iters"] == b["iters"]
+    assert b["max_relres"] < 1e-12
+    assert np.abs(a["zeta"] - b["zeta"]).max() <= 1e-12
+
+
 PARAMS = os.path.join(ROOT, "si3d_b200", "weights", "zeta_increment_net.f32")
 
 

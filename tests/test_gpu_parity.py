@@ -182,7 +182,7 @@ def test_stopping_test_2_steps_match_oracle(native_libs, oracle_lib, run_dirs):
 
 
 @pytest.mark.parametrize("x0", ["LAST", "HIST"])
-@pytest.mark.parametrize("precision", ["FP64", "MIXED_IR"])
+@pytest.mark.parametrize("precision", ["FP64", "MIXED_IR", "MIXED_MG"])
 def test_initial_guess_modes_match_oracle(run_dirs, oracle_lib, native_libs, x0, precision):
     """The initial guess changes where each CG solve starts, not the system it solves: 30 steps with
     x0 = the latest solution (LAST) or the latest solution plus the same solve's correction one step
