@@ -30,6 +30,16 @@ namespace {
 
 constexpr int CW = 32;   // face columns per block of the cell kernel (layer lanes per column: CL)
 
+// 8-byte asynchronous global -> shared copy (cp.async, completion tracked per thread by commit
+// groups).
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned int s = static_cast<unsigned int>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // Horizontal-diffusion coefficient of a neighbouring face column m at layer k
 // (haxpp/haypp as rebuilt by exmom each call, :623-681 / :962-1018): zero outside that
 // column's wet face layers or when its face is closed.  The two depths are loaded by the caller
@@ -171,6 +181,8 @@ __global__ void __launch_bounds__(CW * CL, 768 / (CW * CL)) k_mom_cells(Dev d, c
 // ------------------------------------------------------------------ column kernel
 template <int IEQ, int NT>
 __global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceMeta* __restrict__ meta, int ncols) {
+  constexpr int RD = (NT >= 256) ? 3 : 4;   // layers in flight (static shared memory under 48 KB)
+  __shared__ double ring[RD][6][NT];        // [slot][input][thread]: a thread's slots are its own
   const int t = blockIdx.x * NT + threadIdx.x;
   if (t >= ncols) return;
   const bool X = (IEQ == 1);
@@ -228,29 +240,41 @@ __global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceM
   }
   const double taus_g = cwx / rhopx * (X ? d.s.uair[l - 1] : d.s.vair[l - 1]);
   const double taus_a = cwx / rhopx / huv[IX(d, k1x, l)];
-  // forward sweep of trid with the matmom coefficients; every per-layer input is loaded one layer
-  // ahead so the loads overlap the division chain of the sweep
+  // forward sweep of trid with the matmom coefficients.  Iteration k consumes huv, uvpp and Av (both
+  // columns) of layer k + 1 and the staged ex / increment of layer k; these six values are copied
+  // into this thread's slots of a shared-memory ring by cp.async, RD layers ahead, so the copies of
+  // several layers are in flight during the division chain without holding registers.
   double bcl = 0, c1p = 0, d1p = 0, e1p = 0, hdr_prev = 0;
   double hkm = huv[IX(d, k1x - 1, l)], hk = huv[IX(d, k1x, l)];
   double upm = uvpp[IX(d, k1x - 1, l)], upk = uvpp[IX(d, k1x, l)];
   const int dO = (lO - l);   // column offset of the other face column
-  int ik0 = IX(d, k1x, l);
-  double n_hkp = huv[ik0 + P], n_upp1 = uvpp[ik0 + P], n_ex = agA[ik0], n_hdr = arA[ik0];
-  double n_avop = Av[ik0 + P + dO], n_avlp = Av[ik0 + P];
+  const int ik0 = IX(d, k1x, l);
   double avo = Av[ik0 + dO], avl = Av[ik0];   // Av of layer k (both columns); layer k + 1 is carried
+  const int tid = threadIdx.x;
+  auto issue = [&](int kk, int slot) {   // the six inputs of iteration kk into ring slot `slot`
+    const int ikk = IX(d, kk, l);
+    cp_async8(&ring[slot][0][tid], &huv[ikk + P]);
+    cp_async8(&ring[slot][1][tid], &uvpp[ikk + P]);
+    cp_async8(&ring[slot][2][tid], &Av[ikk + P + dO]);
+    cp_async8(&ring[slot][3][tid], &Av[ikk + P]);
+    cp_async8(&ring[slot][4][tid], &agA[ikk]);
+    cp_async8(&ring[slot][5][tid], &arA[ikk]);
+  };
+#pragma unroll
+  for (int j = 0; j < RD; ++j) {   // one commit group per layer (empty past the bottom)
+    if (k1x + j <= kmx) issue(k1x + j, j);
+    cp_async_commit();
+  }
   // reciprocals shared between the coefficients: 1 / hk, 1 / hkm, 1 / (hkm + hk) (the previous
   // layer's 1 / (hk + hkp)), and 1 / rhopx; three divisions a layer instead of ten
   const double rrho = 1.0 / rhopx;
   double rhk = 1.0 / hk, rhkm = 0.0, rkm = 0.0;
-  for (int k = k1x; k <= kmx; ++k) {
+  for (int k = k1x, slot = 0; k <= kmx; ++k, slot = (slot + 1 == RD) ? 0 : slot + 1) {
     const int ik = IX(d, k, l);
-    const double hkp = n_hkp, upp1 = n_upp1, ex = n_ex, hdr = n_hdr;
-    const double avop = n_avop, avlp = n_avlp;
-    if (k < kmx) {
-      const int in = ik + P;
-      n_hkp = huv[in + P]; n_upp1 = uvpp[in + P]; n_ex = agA[in]; n_hdr = arA[in];
-      n_avop = Av[in + P + dO]; n_avlp = Av[in + P];
-    }
+    cp_async_wait<RD - 1>();   // layer k's group has landed (this thread's own copies)
+    const double hkp = ring[slot][0][tid], upp1 = ring[slot][1][tid];
+    const double avop = ring[slot][2][tid], avlp = ring[slot][3][tid];
+    const double ex = ring[slot][4][tid], hdr = ring[slot][5][tid];
     const double rkp = 1.0 / (hk + hkp), rhkp = 1.0 / hkp;
     const double Avk = (k > k1x) ? 0.5 * (avo + avl) : 0.0;
     const double Avkp = (k < kmx) ? 0.5 * (avop + avlp) : 0.0;
@@ -290,6 +314,9 @@ __global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceM
       e1v = (hh - a1 * e1p) * r;
     }
     cc[ik] = c1v; agA[ik] = d1v; arA[ik] = e1v;
+    // refill the slot with layer k + RD (its values are consumed: the stores above depend on them)
+    if (k + RD <= kmx) issue(k + RD, slot);
+    cp_async_commit();
     c1p = c1v; d1p = d1v; e1p = e1v;
     hkm = hk; hk = hkp;
     upm = upk; upk = upp1;
