@@ -92,6 +92,16 @@ __device__ __forceinline__ double densty_s(double t, double s, double z) {
   return rho;
 }
 
+// 8-byte asynchronous global -> shared copy (cp.async, completion tracked per thread by commit
+// groups).
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned int s = static_cast<unsigned int>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 __device__ __forceinline__ double zmid(const Dev& d, int k, double hpk) {
   const double z = zl(d, k);
   return (z == -100.) ? 0.5 * hpk : z + 0.5 * hpk;

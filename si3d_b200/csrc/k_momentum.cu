@@ -30,15 +30,6 @@ namespace {
 
 constexpr int CW = 32;   // face columns per block of the cell kernel (layer lanes per column: CL)
 
-// 8-byte asynchronous global -> shared copy (cp.async, completion tracked per thread by commit
-// groups).
-__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
-  const unsigned int s = static_cast<unsigned int>(__cvta_generic_to_shared(smem));
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Horizontal-diffusion coefficient of a neighbouring face column m at layer k
 // (haxpp/haypp as rebuilt by exmom each call, :623-681 / :962-1018): zero outside that

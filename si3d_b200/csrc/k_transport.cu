@@ -17,6 +17,7 @@ namespace si3d {
 
 namespace {
 
+
 constexpr int TB = 128;
 
 __device__ __forceinline__ bool ewet(const Dev& d, int l) { return NB(d.g.lEC, l) != d.g.lm1; }
@@ -338,6 +339,8 @@ __global__ void __launch_bounds__(32 * CLN) k_exsal_rhs(Dev d) {
 // imsal's vertical-diffusion tridiagonal solve per column (trid1), right-hand side read from sal.
 template <int NTB>
 __global__ void __launch_bounds__(NTB) k_imsal(Dev d) {
+  constexpr int RD = 4;                // layers in flight in the forward sweep
+  __shared__ double ring[RD][3][NTB];  // [slot][input][thread]: a thread's slots are its own
   const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (l > d.g.lm) return;
   const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
@@ -365,19 +368,29 @@ __global__ void __launch_bounds__(NTB) k_imsal(Dev d) {
     sal[IX(d, k1s, l)] = v;
     return;
   }
-  // trid1 forward sweep: e in scratch, f in sal; inputs (and the next layer's thickness) loaded one
-  // layer ahead; 1 / (hn(k) + hn(k+1)) is shared with the next layer's a1, so a layer takes two
-  // divisions
+  // trid1 forward sweep: e in scratch, f in sal.  Iteration k reads sal(k), Dv(k + 1) and h(k + 1);
+  // these are copied into this thread's slots of a shared-memory ring by cp.async, RD layers ahead.
+  // 1 / (hn(k) + hn(k+1)) is shared with the next layer's a1, so a layer takes two divisions.
   const double rt = 1.0 / twodt1;
-  double hn_k = hn(k1s), e_prev = 0, f_prev = 0, rkm = 0.0;
+  const int tid = threadIdx.x;
+  auto issue = [&](int kk, int slot) {
+    const int ikk = IX(d, kk, l);
+    cp_async8(&ring[slot][0][tid], &sal[ikk]);
+    cp_async8(&ring[slot][1][tid], &Dv[ikk + P]);
+    cp_async8(&ring[slot][2][tid], &h[ikk + P]);
+  };
+#pragma unroll
+  for (int j = 0; j < RD; ++j) {   // one commit group per layer (empty past the bottom)
+    if (k1s + j <= kms) issue(k1s + j, j);
+    cp_async_commit();
+  }
+  const double hn1 = hn(k1s + 1);  // the second layer's thickness carries the surface correction
+  double hn_k = hn(k1s), e_prev = 0, f_prev = 0, rkm = 0.0, dvk = Dv[IX(d, k1s, l)];
   int ik = IX(d, k1s, l);
-  double n_ds = sal[ik], n_dv = Dv[ik], n_dvp = Dv[ik + P], n_hn = hn(k1s + 1);
-  for (int k = k1s; k <= kms; ++k, ik += P) {
-    const double ds = n_ds, dvk = n_dv, dvkp = n_dvp, hn_kp = (k < kms) ? n_hn : 0.0;
-    if (k < kms) {
-      n_ds = sal[ik + P]; n_dv = Dv[ik + P]; n_dvp = Dv[ik + 2 * P];
-      n_hn = (k + 1 < kms) ? hn(k + 2) : 0.0;
-    }
+  for (int k = k1s, slot = 0; k <= kms; ++k, ik += P, slot = (slot + 1 == RD) ? 0 : slot + 1) {
+    cp_async_wait<RD - 1>();     // layer k's group has landed (this thread's own copies)
+    const double ds = ring[slot][0][tid], dvkp = ring[slot][1][tid];
+    const double hn_kp = (k < kms) ? ((k == k1s) ? hn1 : ring[slot][2][tid]) : 0.0;
     const double rkp = (k < kms) ? 1.0 / (hn_k + hn_kp) : 0.0;
     const double a3 = (k < kms) ? -dvkp * rkp * 2. : 0.0;
     double a1 = 0.0;
@@ -400,8 +413,12 @@ __global__ void __launch_bounds__(NTB) k_imsal(Dev d) {
         e_prev = e; f_prev = f;
       }
     }
+    // refill the slot with layer k + RD (its values are consumed: the stores above depend on them)
+    if (k + RD <= kms) issue(k + RD, slot);
+    cp_async_commit();
     hn_k = hn_kp;
     rkm = rkp;
+    dvk = dvkp;
   }
   double nxt = sal[IX(d, kms, l)];
 #pragma unroll 4
