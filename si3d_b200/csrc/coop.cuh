@@ -20,41 +20,42 @@ __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
   return v;
 }
 
-// Block-wide sums of NV values at once (fixed order); the totals are returned in v[] in every
-// thread.  sh holds 8 * NV + NV doubles.
-template <int NV>
+// Block-wide sums of NV values at once (fixed order) over blocks of BS threads; the totals are
+// returned in v[] in every thread.  sh holds (BS / 32) * NV + NV doubles.
+template <int NV, int BS = QB>
 __device__ __forceinline__ void bsum(double (&v)[NV], double* sh) {
+  constexpr int NW = BS / 32;
 #pragma unroll
   for (int i = 0; i < NV; ++i)
     for (int o = 16; o > 0; o >>= 1) v[i] += __shfl_down_sync(0xffffffffu, v[i], o);
   const int w = threadIdx.x >> 5, ln = threadIdx.x & 31;
   if (ln == 0) {
 #pragma unroll
-    for (int i = 0; i < NV; ++i) sh[i * 8 + w] = v[i];
+    for (int i = 0; i < NV; ++i) sh[i * NW + w] = v[i];
   }
   __syncthreads();
   if (threadIdx.x < NV) {
     double t = 0;
 #pragma unroll
-    for (int q = 0; q < QB / 32; ++q) t += sh[threadIdx.x * 8 + q];
-    sh[8 * NV + threadIdx.x] = t;
+    for (int q = 0; q < NW; ++q) t += sh[threadIdx.x * NW + q];
+    sh[NW * NV + threadIdx.x] = t;
   }
   __syncthreads();
 #pragma unroll
-  for (int i = 0; i < NV; ++i) v[i] = sh[8 * NV + i];
+  for (int i = 0; i < NV; ++i) v[i] = sh[NW * NV + i];
   __syncthreads();
 }
 
 // Totals of NV partial arrays (n entries each, arrays `stride` apart), in every thread.
-template <int NV>
+template <int NV, int BS = QB>
 __device__ __forceinline__ void all_partials(const double* part, int n, int stride, double (&v)[NV], double* sh) {
 #pragma unroll
   for (int i = 0; i < NV; ++i) v[i] = 0;
-  for (int j = threadIdx.x; j < n; j += QB) {
+  for (int j = threadIdx.x; j < n; j += BS) {
 #pragma unroll
     for (int i = 0; i < NV; ++i) v[i] += __ldcg(part + i * stride + j);
   }
-  bsum<NV>(v, sh);
+  bsum<NV, BS>(v, sh);
 }
 
 // Counting grid barrier with a bounded wait.  Returns false (in every thread of the block) once

@@ -50,6 +50,7 @@ using namespace coop;
 constexpr int PB = 256;               // threads per block of the setup kernels
 constexpr float kFaceScale = 0.5f;    // coarse faces: half the sum of the crossing fine faces
 constexpr int UN = 4;                 // cells a thread keeps in flight in the level loops
+constexpr int MQ = 512;               // threads per block of the cooperative solve (one block per SM)
 
 __device__ __forceinline__ int fdiv(const FastDiv& f, int x) {
   return (int)(((unsigned long long)(unsigned int)x * f.m) >> f.p);
@@ -208,7 +209,7 @@ __device__ __forceinline__ void restrict_residual(const MgLevel& F, const MgLeve
 // at once); otherwise its = the iterations taken and ier = 0, 1 (itmax) or -6 / -7 (breakdown).
 __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* bar, PcgScal* SC, int* s_flag,
                        double* sh, double zeta, double bnorm, int itmax, int& its, int& ier) {
-  const int nb = gridDim.x, stride = nb * QB, g0 = blockIdx.x * QB + threadIdx.x;
+  const int nb = gridDim.x, stride = nb * MQ, g0 = blockIdx.x * MQ + threadIdx.x;
   double* const rr_part = M.part;
   double* const rz_part = M.part + nb;
   double* const pq_part = M.part + 3 * nb;
@@ -253,13 +254,13 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
         }
       }
       double w[1] = {rr};
-      bsum<1>(w, sh);
+      bsum<1, MQ>(w, sh);
       if (threadIdx.x == 0) rr_part[blockIdx.x] = w[0];
     }
     if (!grid_barrier(bar, SC, s_flag)) return false;
     {
       double w[1];
-      all_partials<1>(rr_part, nb, 0, w, sh);
+      all_partials<1, MQ>(rr_part, nb, 0, w, sh);
       const double tl = sqrt(w[0]);
       if (tl < bnorm * zeta) break;
       if (it >= itmax) { ier = 1; break; }
@@ -274,16 +275,16 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
     // ---- coarsest level: black, red (one block)
     if (blockIdx.x == 0) {
       const MgLevel& Lc = s_lv[nlev - 1];
-      half_sweep<false, false>(Lc, Lc, 1, threadIdx.x, QB);
+      half_sweep<false, false>(Lc, Lc, 1, threadIdx.x, MQ);
       __syncthreads();
-      half_sweep<false, false>(Lc, Lc, 0, threadIdx.x, QB);
+      half_sweep<false, false>(Lc, Lc, 0, threadIdx.x, MQ);
     }
     if (!grid_barrier(bar, SC, s_flag)) return false;
     // ---- up: black half-sweep with the coarse correction, red half-sweep; (r, z) at level 0
     for (int k = nlev - 2; k >= 0; --k) {
       if (k == 0) {
         double w[1] = {half_sweep<true, true>(s_lv[0], s_lv[1], 1, g0, stride)};
-        bsum<1>(w, sh);
+        bsum<1, MQ>(w, sh);
         if (threadIdx.x == 0) rz_part[blockIdx.x] = w[0];
       } else {
         half_sweep<true, false>(s_lv[k], s_lv[k + 1], 1, g0, stride);
@@ -291,7 +292,7 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
       if (!grid_barrier(bar, SC, s_flag)) return false;
       if (k == 0) {
         double w[1] = {half_sweep<false, true>(s_lv[0], s_lv[0], 0, g0, stride)};
-        bsum<1>(w, sh);
+        bsum<1, MQ>(w, sh);
         if (threadIdx.x == 0) rz_part[nb + blockIdx.x] = w[0];
       } else {
         half_sweep<false, false>(s_lv[k], s_lv[k], 0, g0, stride);
@@ -300,7 +301,7 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
     }
     {
       double w[1];
-      all_partials<1>(rz_part, 2 * nb, 0, w, sh);
+      all_partials<1, MQ>(rz_part, 2 * nb, 0, w, sh);
       if (!(w[0] > 0.0)) { ier = -7; break; }
       beta = (it == 0) ? 0.0 : w[0] / rz_old;
       rz_old = w[0];
@@ -342,13 +343,13 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
         }
       }
       double w[1] = {pq};
-      bsum<1>(w, sh);
+      bsum<1, MQ>(w, sh);
       if (threadIdx.x == 0) pq_part[blockIdx.x] = w[0];
     }
     if (!grid_barrier(bar, SC, s_flag)) return false;
     {
       double w[1];
-      all_partials<1>(pq_part, nb, 0, w, sh);
+      all_partials<1, MQ>(pq_part, nb, 0, w, sh);
       if (!(w[0] > 0.0)) { ier = -6; break; }
       alpha = rz_old / w[0];
     }
@@ -359,15 +360,15 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
 }
 
 // ---------------------------------------------------------------- the whole solve
-__global__ void __launch_bounds__(QB, 2) k_mg_solve(MgDev M, GridBar* bar) {
-  __shared__ double sh[8 * 2 + 2];
+__global__ void __launch_bounds__(MQ, 1) k_mg_solve(MgDev M, GridBar* bar) {
+  __shared__ double sh[(MQ / 32) * 2 + 2];
   __shared__ int s_flag;
   __shared__ MgLevel s_lv[kMgMaxLevels];
   const int nlev = M.nlev;
   if (threadIdx.x < nlev) s_lv[threadIdx.x] = M.lv[threadIdx.x];
   __syncthreads();
   PcgScal* SC = M.sc;
-  const int nb = gridDim.x, stride = nb * QB, g0 = blockIdx.x * QB + threadIdx.x;
+  const int nb = gridDim.x, stride = nb * MQ, g0 = blockIdx.x * MQ + threadIdx.x;
   double* const res_part = M.part + 4 * nb;   // (r, r) [nb], (b, b) [nb] of the FP64 system
   const double zeta = SC->zeta, srelpr = SC->srelpr;
   const int itmax = SC->itmax;
@@ -417,12 +418,12 @@ __global__ void __launch_bounds__(QB, 2) k_mg_solve(MgDev M, GridBar* bar) {
           M.u[o[k]] = 0.f;
         }
       }
-      bsum<2>(v, sh);
+      bsum<2, MQ>(v, sh);
       if (threadIdx.x == 0) { res_part[blockIdx.x] = v[0]; res_part[nb + blockIdx.x] = v[1]; }
     }
     if (!grid_barrier(bar, SC, &s_flag)) return;
     double w[2];
-    all_partials<2>(res_part, nb, nb, w, sh);
+    all_partials<2, MQ>(res_part, nb, nb, w, sh);
     if (outer == 0) bn = fmax(sqrt(w[1]), srelpr);   // bnorm of stopping test 5 (nmcalc)
     const double rn = sqrt(w[0]);
     stp = rn / bn;
@@ -450,10 +451,10 @@ __global__ void __launch_bounds__(QB, 2) k_mg_solve(MgDev M, GridBar* bar) {
 int mg_loop_blocks(int device, int cells0, int max_per_sm) {
   int sms = 0, occ = 0;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_solve, QB, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mg_solve, MQ, 0);
   int per_sm = std::max(occ, 1);
   if (max_per_sm > 0) per_sm = std::min(per_sm, max_per_sm);
-  const int need = std::max(1, (cells0 + QB - 1) / QB);
+  const int need = std::max(1, (cells0 + MQ - 1) / MQ);
   return std::max(1, std::min(sms * per_sm, need));
 }
 
@@ -469,7 +470,7 @@ int mg_solve(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st) {
   if (cudaMemsetAsync(bar, 0, sizeof(GridBar), st) != cudaSuccess) return -1;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nblocks);
-  cfg.blockDim = dim3(QB);
+  cfg.blockDim = dim3(MQ);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
