@@ -25,6 +25,8 @@ namespace {
 
 using namespace coop;
 
+constexpr int PQB = 1024;   // threads per block of the cooperative solve (one block per SM)
+
 // ---- adaptive eigenvalue estimates for stopping test 2: chgcon (nspcg.f:16499-16620), eigvss
 // (:17201-17240), zbrent (:32976-33160) and determ (:16926-16962), run by one thread after each new
 // alpha.  tri holds the Lanczos tridiagonal column by column: tri[2 (c - 1)] = T(1, c), tri[2 (c - 1) + 1]
@@ -158,14 +160,14 @@ __device__ __noinline__ void lz_chgcon(PcgScal* S, double* tri, int ip, double a
 // TEST2: stopping test 2 with chgcon's adaptive emin (test 5 otherwise); a separate instantiation keeps
 // the test-5 loop free of the eigenvalue code.
 template <typename T, bool TEST2>
-__global__ void __launch_bounds__(QB, 4) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
-  __shared__ double sh[8 * 4 + 4];
+__global__ void __launch_bounds__(PQB, 1) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
+  __shared__ double sh[(PQB / 32) * 4 + 4];
   __shared__ int s_flag;
   const PcgColorT<T> &R = P.R, &B = P.B;
   PcgScal* SC = P.sc;
   const int nb = gridDim.x;
-  const int stride = nb * QB;
-  const int g0 = blockIdx.x * QB + threadIdx.x;
+  const int stride = nb * PQB;
+  const int g0 = blockIdx.x * PQB + threadIdx.x;
   // partial sums: (r,r) in part0, (r,z) in part1, (u,u) in part2, (z,z) in part3, black blocks at
   // [0, nb) and red blocks at [nb, 2 nb); (p,q) at part0 + 2 nb.  The four arrays are equally
   // spaced (part_n apart in one allocation).
@@ -214,12 +216,12 @@ __global__ void __launch_bounds__(QB, 4) k_pcg_loop(PcgDevT<T> P, GridBar* bar) 
       v[2] += (double)uj * (double)uj; v[3] += (double)zj * (double)zj;
     }
     if (t2) {
-      bsum<4>(v, sh);
+      bsum<4, PQB>(v, sh);
       if (threadIdx.x == 0)
         for (int i = 0; i < 4; ++i) P.part0[i * pstride + blockIdx.x] = v[i];
     } else {
       double w2[2] = {v[0], v[1]};
-      bsum<2>(w2, sh);
+      bsum<2, PQB>(w2, sh);
       if (threadIdx.x == 0) { P.part0[blockIdx.x] = w2[0]; P.part0[pstride + blockIdx.x] = w2[1]; }
     }
     if (!grid_barrier(bar, SC, &s_flag)) return;
@@ -246,12 +248,12 @@ __global__ void __launch_bounds__(QB, 4) k_pcg_loop(PcgDevT<T> P, GridBar* bar) 
       v[2] += (double)uk * (double)uk; v[3] += (double)zk * (double)zk;
     }
     if (t2) {
-      bsum<4>(v, sh);
+      bsum<4, PQB>(v, sh);
       if (threadIdx.x == 0)
         for (int i = 0; i < 4; ++i) P.part0[i * pstride + nb + blockIdx.x] = v[i];
     } else {
       double w2[2] = {v[0], v[1]};
-      bsum<2>(w2, sh);
+      bsum<2, PQB>(w2, sh);
       if (threadIdx.x == 0) { P.part0[nb + blockIdx.x] = w2[0]; P.part0[pstride + nb + blockIdx.x] = w2[1]; }
     }
     if (!grid_barrier(bar, SC, &s_flag)) return;
@@ -259,11 +261,11 @@ __global__ void __launch_bounds__(QB, 4) k_pcg_loop(PcgDevT<T> P, GridBar* bar) 
     double rrt, rzt, uut = 0, zzt = 0;
     if (t2) {
       double w4[4];
-      all_partials<4>(P.part0, 2 * nb, pstride, w4, sh);
+      all_partials<4, PQB>(P.part0, 2 * nb, pstride, w4, sh);
       rrt = w4[0]; rzt = w4[1]; uut = w4[2]; zzt = w4[3];
     } else {
       double w2[2];
-      all_partials<2>(P.part0, 2 * nb, pstride, w2, sh);
+      all_partials<2, PQB>(P.part0, 2 * nb, pstride, w2, sh);
       rrt = w2[0]; rzt = w2[1];
     }
     dkm1 = rzdot;
@@ -329,11 +331,11 @@ __global__ void __launch_bounds__(QB, 4) k_pcg_loop(PcgDevT<T> P, GridBar* bar) 
         pq[0] += (double)pi * (double)y;
       }
     }
-    bsum<1>(pq, sh);
+    bsum<1, PQB>(pq, sh);
     if (threadIdx.x == 0) pq_part[blockIdx.x] = pq[0];
     if (!grid_barrier(bar, SC, &s_flag)) return;
     double pap[1];
-    all_partials<1>(pq_part, nb, 0, pap, sh);
+    all_partials<1, PQB>(pq_part, nb, 0, pap, sh);
     const double alpha_prev = alpha;
     alpha = rzdot / pap[0];
     if (!(pap[0] > 0.0)) { ier = -6; break; }
@@ -359,7 +361,7 @@ int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, bool test2, cuda
   if (cudaMemsetAsync(bar, 0, sizeof(GridBar), st) != cudaSuccess) return -1;
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nblocks);
-  cfg.blockDim = dim3(QB);
+  cfg.blockDim = dim3(PQB);
   cfg.dynamicSmemBytes = 0;
   cfg.stream = st;
   cudaLaunchAttribute attr[1];
@@ -379,16 +381,16 @@ int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   int occ2 = 0;
   if (fp32) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<float, false>, QB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<float, false>, PQB, 0);
     occ2 = occ;
   } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<double, false>, QB, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_pcg_loop<double, true>, QB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<double, false>, PQB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_pcg_loop<double, true>, PQB, 0);
   }
   occ = std::min(occ, occ2);
   int per_sm = occ;
   if (max_per_sm > 0) per_sm = std::min(per_sm, max_per_sm);
-  const int need = (std::max(nR, nB) + QB - 1) / QB;
+  const int need = (std::max(nR, nB) + PQB - 1) / PQB;
   return std::max(1, std::min(sms * std::max(per_sm, 1), need));
 }
 
