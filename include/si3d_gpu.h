@@ -45,7 +45,8 @@ extern "C" {
 #define SI3D_FP64 0       /* plain FP64 everywhere */
 #define SI3D_MIXED_IR 1   /* FP32 SpMV + MIC inside an FP64 iterative-refinement loop */
 #define SI3D_MIXED_MG 2   /* FP32 SpMV + aggregation-multigrid V-cycle inside FP64 iterative
-                             refinement (needs the l2i/l2j maps of a plain (im1, jm1) grid) */
+                             refinement (needs the l2i/l2j maps of a plain (im1, jm1) grid);
+                             a project addition with no counterpart in the reference */
 
 /* zeta-solve orderings */
 #define SI3D_ORDER_REDBLACK 1   /* NSPCG iperm=1 red-black MIC (the GPU form) */
@@ -58,7 +59,8 @@ extern "C" {
                                the trapezoidal solves after it; otherwise sp + the increment set by
                                si3d_gpu_set_warmstart for every solve */
 #define SI3D_X0_LAST 3      /* s, the latest accepted solution: within a step the trapezoidal solves
-                               start from the previous solve's zeta(n+1) instead of the half level sp */
+                               start from the previous solve's zeta(n+1) instead of the half level sp
+                               (LAST and HIST are project additions, no counterpart in the reference) */
 #define SI3D_X0_HIST 4      /* s + the same solve's correction one step earlier (solve k of step n
                                starts from s + (x_k(n-1) - s_k(n-1)), where s_k is the zeta solve k
                                started from); the first step starts from s */
