@@ -75,3 +75,37 @@ def test_multigrid_needs_the_grid_image():
     jco = np.array([[1, 2, 0, 0, 0], [2, 0, 0, 0, 1]], dtype=np.int32)
     with pytest.raises(Exception):
         solve_zeta(coef, jco, np.ones(2), np.zeros(2), itmax=50, precision=native.SI3D_MIXED_MG)
+
+
+@pytest.mark.parametrize("istep", [1, 2])
+@pytest.mark.parametrize("name", ["t0", "t1", "c0"])
+def test_multigrid_solve_matches_restatement(run_dirs, oracle_lib, native_libs, name, istep):
+    """One MIXED_MG zeta solve against the numpy restatement of the same solve (same hierarchy,
+    half-sweeps, FP32 CG recurrences and FP64 refinement): the inner iteration totals agree up to
+    reduction-order rounding and both zeta meet the 1e-12 test."""
+    from oracle import mg_numpy
+    from si3d_b200 import native
+    from si3d_b200.model import GpuRun
+    from test_gpu_parity import STATE_2D, STATE_3D, STATE_I
+    o = oracle_lib.OracleRun(run_dirs[name], ordering=1, pcg_itmax=2000)
+    o.run(2)
+    o.stage("momentum", istep)
+    o.stage("matcon", istep)
+    g = GpuRun(run_dirs[name], pcg_itmax=2000, precision=native.SI3D_MIXED_MG)
+    try:
+        for f in STATE_3D:
+            g.set(f, o.get(f))
+        for f in STATE_2D:
+            g.set(f, o.get(f))
+        for f in STATE_I:
+            g.set(f, o.geti(f))
+        maps = [o.geti(n) for n in ("l2i", "l2j", "lEC", "lWC", "lNC", "lSC")]
+        sx, sy, qq, sp = (o.get(n) for n in ("sx", "sy", "qq", "sp"))
+        z, info = mg_numpy.solve(o.lm, *maps, sx, sy, qq, sp, o.im1, o.jm1)
+        st = g.stage("solve", istep)
+        assert st.nsolves == 1 and st.ier[0] == 0 and st.relres[0] < 1e-12
+        assert abs(st.iters[0] - info["iters"]) <= 2, (st.iters[0], info)
+        zg = g.get("s")[:o.lm]
+        assert np.abs(zg - z).max() <= 1e-10 * max(np.abs(z).max(), 1e-3)
+    finally:
+        g.close()
