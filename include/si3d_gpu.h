@@ -97,6 +97,8 @@ typedef struct si3d_params {
   int ordering;            /* SI3D_ORDER_REDBLACK */
   int x0_mode;             /* SI3D_X0_* */
   int precision;           /* SI3D_FP64, SI3D_MIXED_IR or SI3D_MIXED_MG */
+  int ntr;                 /* non-active tracers, 0..30 (ntrmax, si3d_types.f90:291); conservative
+                              tracers only (ecomod = 0, srcsnk00), advanced once per step by fd */
 } si3d_params;
 
 /* Per-call statistics (one entry per zeta solve inside the call). */
@@ -118,8 +120,10 @@ int si3d_gpu_init(const si3d_grid* grid, const si3d_params* params, int device, 
 
 /* Copy one reference array between host and device.  3-D names: uh uhp uhpp up upp hu hup hupp
  * agx arx vh vhp vhpp vp vpp hv hvp hvpp agy ary h hp hpp sal salp salpp rhop Av Dv wp
- * HeatSource Bth2 Bth3 Bth4 ((km1, lm1) column-major).  2-D names: s sp spp eagx earx eagy eary
- * sx sy dd qq rr uair vair cdw (lm1).  Replaces the Fortran module arrays of si3d_types.f90:117-164. */
+ * HeatSource Bth2 Bth3 Bth4 ((km1, lm1) column-major), and per tracer nt = 1..ntr the names
+ * "tracer<nt>" and "tracerpp<nt>" (tracer(:,:,nt), tracerpp(:,:,nt), si3d_utils.f90:571-574).
+ * 2-D names: s sp spp eagx earx eagy eary sx sy dd qq rr uair vair cdw (lm1).  Replaces the
+ * Fortran module arrays of si3d_types.f90:117-164. */
 int si3d_gpu_set_field(int handle, const char* name, const double* host);
 int si3d_gpu_get_field(int handle, const char* name, double* host);
 /* Integer column arrays k1z k1u k1v (lm1 entries). */
@@ -132,11 +136,12 @@ int si3d_gpu_get_ifield(int handle, const char* name, int* host);
 int si3d_gpu_density(int handle);
 
 /* One call of fd (si3d_procedures.f90:382-575): surfbc CASE 0, exmom+matmom (x, y), matcon,
- * SolverSparse (NSPCG mic1+cg replacement), vel + continuity(1), exsal + imsal, vel2.
+ * SolverSparse (NSPCG mic1+cg replacement), vel + continuity(1), exsal + imsal, and with
+ * ntr > 0, niter > 0 and lastiter = 1 exTracer + ImTracer for every tracer (:520-544), then vel2.
  * Replaces CALL fd(...) at si3d.f90:353 and si3d.f90:373. */
 int si3d_gpu_fd(int handle, int n, int istep, int lastiter, si3d_step_stats* stats);
-/* settrap (si3d_procedures.f90:3418), settrap2 (:3944), save (:3621); replace the calls at
- * si3d.f90:365, :383, :393. */
+/* settrap (si3d_procedures.f90:3418), settrap2 (:3944), save (:3621, which also sets
+ * tracerpp = tracer); replace the calls at si3d.f90:365, :383, :393. */
 int si3d_gpu_settrap(int handle);
 int si3d_gpu_settrap2(int handle);
 int si3d_gpu_save(int handle, int istep);
@@ -173,7 +178,7 @@ int si3d_gpu_column_tridiag(int n, int nsys, const double* a, const double* b, c
  * number of kernels the handle has launched and, per stage, the accumulated device milliseconds
  * and call counts (the zeta-solve iteration stage counts iterations).  Stage order: momentum x,
  * momentum y, matcon, pcg setup, pcg iterations, pcg finish, slayer_h, vel, scalar, vel2,
- * settrap, settrap2, save.  Returns the number of stages. */
+ * settrap, settrap2, save, learned guess, tracers.  Returns the number of stages. */
 int si3d_gpu_profile(int handle, int enable);
 int si3d_gpu_counters(int handle, long long* launches, double* stage_ms, long long* stage_n);
 

@@ -62,6 +62,8 @@ struct Inp {
   int idbg = 0, num_threads = 1;
   int ipt = 0, nnodes = 0, iop = 0, itspfh = 0, n_planes = 0, iox = 0, ipxml = 0, itspf = 0,
       iTurbVars = 0, nopen = 0, nxNBO = 0, ntr = 0, iopss = 0;
+  // tracer block (si3d_utils.f90:172-181), read when ntr > 0
+  int ecomod = 0, iotr = 0, itspftr = 0, ipwq = 0, nswq = 0;
 };
 
 struct F3 {  // (km1, lm1) column-major, 1-based
@@ -110,6 +112,8 @@ struct Model {
   // thread-private scratch that the reference keeps across calls (si3d.f90:299-316;
   // InitThreads si3d_procedures.f90:4838-4841 zero-initialises them)
   F3 Bth2, Bth3, Bth4, Bex, Bhaxpp, Bhaypp;
+  // non-active tracers (si3d_utils.f90:571-574): tracer and tracerpp per tracer, ntr of each
+  std::vector<F3> tracer, tracerpp;
   // per-column wind override (harness overlay; surfbc CASE 0 otherwise)
   bool wind_override = false;
   std::vector<real> uair_ovr, vair_ovr;  // l-indexed (1..lm)

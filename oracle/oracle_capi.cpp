@@ -1,5 +1,6 @@
 // C entry points of the CPU oracle, loaded by tests/ and bench.py through ctypes —
 // TEST INFRASTRUCTURE ONLY (see oracle.hpp).
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
@@ -23,7 +24,17 @@ F3* field3(Model& m, const std::string& n) {
       {"wp", &Model::wp},     {"Bth2", &Model::Bth2}, {"Bth3", &Model::Bth3}, {"Bth4", &Model::Bth4},
       {"Bex", &Model::Bex}};
   auto it = t.find(n);
-  return it == t.end() ? nullptr : &(m.*(it->second));
+  if (it != t.end()) return &(m.*(it->second));
+  // "tracer<nt>" and "tracerpp<nt>", nt = 1..ntr
+  for (auto [pre, vec] : {std::pair<const char*, std::vector<F3>*>{"tracerpp", &m.tracerpp},
+                          std::pair<const char*, std::vector<F3>*>{"tracer", &m.tracer}}) {
+    const size_t np = std::strlen(pre);
+    if (n.size() > np && n.compare(0, np, pre) == 0 && n.find_first_not_of("0123456789", np) == std::string::npos) {
+      const int nt = std::atoi(n.c_str() + np);
+      return (nt >= 1 && nt <= (int)vec->size()) ? &(*vec)[nt - 1] : nullptr;
+    }
+  }
+  return nullptr;
 }
 
 F1* field2(Model& m, const std::string& n) {
@@ -83,11 +94,11 @@ int orc_set_int(void* h, const char* name, const int* in) {
   return -1;
 }
 
-// im1, jm1, km1, lm, km, k1, nts, n
+// im1, jm1, km1, lm, km, k1, nts, n, ntr
 int orc_dims(void* h, int* out) {
   Model& m = *static_cast<Model*>(h);
   out[0] = m.im1; out[1] = m.jm1; out[2] = m.km1; out[3] = m.lm; out[4] = m.km; out[5] = m.k1;
-  out[6] = m.nts; out[7] = m.n;
+  out[6] = m.nts; out[7] = m.n; out[8] = m.in.ntr;
   return 0;
 }
 

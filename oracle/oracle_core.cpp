@@ -672,6 +672,125 @@ void imsal(Model& m) {
   });
 }
 
+// exTracer (si3d_procedures.f90:4090-4356) for tracer nt, ecomod = 0: the three flux loops of
+// exsal on tracerpp (no settling velocities: the suspended-sediment and water-quality species
+// indices are not set for conservative tracers, so vel = wp), Bex on the wet layers and on the
+// sediment layer kms + 1.  Bex and the flux arrays keep whatever an earlier routine left elsewhere.
+void extracer(Model& m, int nt) {
+  const int km1 = m.km1, lm1 = m.lm1;
+  const real twodt1 = m.twodt * m.tz;
+  const Inp& p = m.in;
+  const F3& c = m.tracerpp[nt - 1];
+  for (int k = 1; k <= km1; ++k) { m.Bhaxpp(k, lm1) = 0.0; m.Bhaypp(k, lm1) = 0.0; }
+  par_cols(m.lm, [&](int l) {
+    for (int k = m.k1; k <= m.kmz(l); ++k) { m.Bhaxpp(k, l) = p.Ax0 * m.hupp(k, l); m.Bhaypp(k, l) = p.Ay0 * m.hvpp(k, l); }
+  });
+  for (int k = 1; k <= km1; ++k) { m.Bth3(k, lm1) = 0.0; m.Bex(k, lm1) = 0.0; m.Bth2(k, lm1) = 0.0; m.Bth4(k, lm1) = 0.0; }
+  auto limiter = [](real ss1, real ss2, real ss3, real ss4, real vel, real cf0) {
+    real C_f = cf0;
+    const real ss[5] = {0, ss1, ss2, ss3, ss4};
+    int gamma1 = -(int)std::copysign(1.0, vel);
+    if (ss3 - ss2 != 0) {
+      real ratio = (ss[3 + gamma1] - ss[2 + gamma1]) / (ss3 - ss2);
+      C_f = std::max(std::max(0., std::min(1., 2. * ratio)), std::min(2., ratio));
+    }
+    return C_f;
+  };
+  par_cols(m.lm, [&](int l) {
+    const int kms = m.kmz(l), k1s = m.k1z(l), lE = m.lEC(l), lW = m.lWC(l), lEE = m.lEC(lE);
+    for (int k = k1s; k <= kms; ++k) {
+      if (m.hup(k, l) > ZERO) {
+        real vel = (m.uhpp(k, l) + m.uh(k, l)) / 2.;
+        real ss2 = c(k, l), ss3 = c(k, lE);
+        real ss1 = (m.hpp(k, lW) <= ZERO) ? ss2 : c(k, lW);
+        real ss4 = (m.hpp(k, lEE) <= ZERO) ? ss3 : c(k, lEE);
+        real C_f = limiter(ss1, ss2, ss3, ss4, vel, 0.0);
+        m.Bth2(k, l) = vel / 2. * (ss3 + ss2) - ((1. - C_f) * std::fabs(vel) + vel * vel * twodt1 / m.dx * C_f) * (ss3 - ss2) / 2.;
+      } else m.Bth2(k, l) = 0.0;
+    }
+  });
+  par_cols(m.lm, [&](int l) {
+    const int kms = m.kmz(l), k1s = m.k1z(l), lN = m.lNC(l), lS = m.lSC(l), lNN = m.lNC(lN);
+    for (int k = k1s; k <= kms; ++k) {
+      if (m.hvp(k, l) > ZERO) {
+        real vel = (m.vhpp(k, l) + m.vh(k, l)) / 2.;
+        real ss2 = c(k, l), ss3 = c(k, lN);
+        real ss1 = (m.hpp(k, lS) <= ZERO) ? ss2 : c(k, lS);
+        real ss4 = (m.hpp(k, lNN) <= ZERO) ? ss3 : c(k, lNN);
+        real C_f = limiter(ss1, ss2, ss3, ss4, vel, 0.0);
+        m.Bth4(k, l) = vel / 2. * (ss3 + ss2) - ((1. - C_f) * std::fabs(vel) + vel * vel * twodt1 / m.dy * C_f) * (ss3 - ss2) / 2.;
+      } else m.Bth4(k, l) = 0.0;
+      if (m.hp(k - 1, l) > ZERO) {
+        real vel = (k == k1s) ? 0.0 : m.wp(k, l);
+        real ss2 = c(k, l), ss3 = c(k - 1, l);
+        real ss4 = (m.hpp(k - 2, l) <= ZERO) ? ss3 : c(k - 2, l);
+        real ss1 = (m.hpp(k + 1, l) <= ZERO) ? ss2 : c(k + 1, l);
+        real C_f = limiter(ss1, ss2, ss3, ss4, vel, 1.0);
+        real delz = (m.hp(k, l) + m.hp(k - 1, l)) / 2.;
+        m.Bth3(k, l) = vel / 2. * (ss3 + ss2) - ((1. - C_f) * std::fabs(vel) + vel * vel * twodt1 / delz * C_f) * (ss3 - ss2) / 2.;
+      } else m.Bth3(k, l) = 0.0;
+    }
+  });
+  par_cols(m.lm, [&](int l) {
+    const int kms = m.kmz(l), k1s = m.k1z(l);
+    const int lE = m.lEC(l), lW = m.lWC(l), lN = m.lNC(l), lS = m.lSC(l);
+    for (int k = k1s; k <= kms; ++k) {
+      m.Bex(k, l) = m.hpp(k, l) * c(k, l) / twodt1 - (m.Bth2(k, l) - m.Bth2(k, lW)) / m.dx -
+                    (m.Bth4(k, l) - m.Bth4(k, lS)) / m.dy - (m.Bth3(k, l) - m.Bth3(k + 1, l));
+      if (p.ihd > 0) {
+        real hd = (m.Bhaxpp(k, l) * (c(k, lE) - c(k, l)) - m.Bhaxpp(k, lW) * (c(k, l) - c(k, lW))) / m.dxdx +
+                  (m.Bhaypp(k, l) * (c(k, lN) - c(k, l)) - m.Bhaypp(k, lS) * (c(k, l) - c(k, lS))) / m.dydy;
+        m.Bex(k, l) = m.Bex(k, l) + hd;
+      }
+    }
+    m.Bex(kms + 1, l) = m.hpp(kms + 1, l) * c(kms + 1, l) / twodt1;
+  });
+}
+
+// ImTracer (si3d_procedures.f90:4359-4487) for tracer nt with sourcesink = 0 (srcsnk00) and no
+// point sources: the implicit vertical diffusion per column (trid1), the sediment layer kms + 1,
+// and negative concentrations clipped to zero from layer k1 - 1 to kms + 1.
+void imtracer(Model& m, int nt) {
+  const int km1 = m.km1;
+  const real twodt1 = m.twodt * m.tz;
+  F3& t = m.tracer[nt - 1];
+  par_cols(m.lm, [&](int l) {
+    thread_local std::vector<real> hn, aa, ds, sal1;
+    hn.resize(km1 + 2); aa.resize(3 * (km1 + 1)); ds.resize(km1 + 1); sal1.resize(km1 + 1);
+    auto AA = [&](int r, int k) -> real& { return aa[3 * (k - 1) + (r - 1)]; };
+    const int kms = m.kmz(l), k1s = m.k1z(l), nwlayers = kms - k1s + 1;
+    for (int k = k1s + 1; k <= kms; ++k) hn[k] = m.h(k, l);
+    hn[k1s] = twodt1 * m.wp(k1s, l) + m.hpp(k1s, l);
+    if (m.hpp(k1s, l) <= ZERO) hn[k1s + 1] = m.hpp(k1s + 1, l);
+    if (nwlayers == 1) {
+      AA(2, k1s) = hn[k1s] / twodt1;
+      ds[k1s] = m.Bex(k1s, l) + 0.0;
+      t(k1s, l) = ds[k1s] / AA(2, k1s);
+    } else if (nwlayers >= 2) {
+      for (int k = k1s; k <= kms - 1; ++k) AA(3, k) = -m.Dv(k + 1, l) / (hn[k] + hn[k + 1]) * 2.;
+      AA(3, kms) = 0.0;
+      for (int k = k1s + 1; k <= kms; ++k) AA(1, k) = -m.Dv(k, l) / (hn[k - 1] + hn[k]) * 2.;
+      AA(1, k1s) = 0.0;
+      for (int k = k1s; k <= kms; ++k) AA(2, k) = hn[k] / twodt1 - AA(1, k) - AA(3, k);
+      for (int k = k1s; k <= kms; ++k) ds[k] = m.Bex(k, l) + 0.0;
+      trid1(aa.data(), ds.data() + 1, sal1.data() + 1, k1s, kms, nwlayers);
+      for (int k = k1s; k <= kms; ++k) t(k, l) = sal1[1 + k - k1s];
+      for (int k = m.k1; k <= k1s - 1; ++k) t(k, l) = sal1[1];
+      t(m.k1 - 1, l) = sal1[1];
+    }
+    hn[kms + 1] = m.hpp(kms + 1, l);
+    const real a2 = hn[kms + 1] / twodt1;
+    t(kms + 1, l) = (m.Bex(kms + 1, l) + 0.0) / a2;
+    for (int k = m.k1 - 1; k <= kms + 1; ++k)
+      if (t(k, l) < 0.0) t(k, l) = 0.0;
+  });
+}
+
+// fd's non-active scalar block (si3d_procedures.f90:520-544) for ecomod = 0 and nopen = 0.
+void tracers(Model& m) {
+  for (int nt = 1; nt <= m.in.ntr; ++nt) { extracer(m, nt); imtracer(m, nt); }
+}
+
 // layer_h (si3d_procedures.f90:2181-2231)
 void layer_h(Model& m) {
   par_cols(m.lm, [&](int l) {
@@ -904,6 +1023,8 @@ void save(Model& m, int istep) {
     });
     continuity(m, 2);
   }
+  // both branches end with tracerpp = tracer (:3771-3774, :3926-3929)
+  if (m.in.ntr > 0) m.tracerpp = m.tracer;
 }
 
 // fd (si3d_procedures.f90:382-575) for the hot-path configuration.
@@ -918,6 +1039,7 @@ bool fd(Model& m, ExCoef& C) {
   if (!solver_sparse(m)) return false;
   vel(m);
   if (m.in.isal != 0) { exsal(m); imsal(m); }
+  if (m.in.ntr > 0 && m.in.niter > 0 && m.lastiter == 1) tracers(m);
   vel2(m);
   if (m.in.ismooth >= 1 && m.istep == 1) { m.err = "ismooth>=1 is not on the hot path"; return false; }
   return true;
@@ -936,6 +1058,7 @@ bool run_stage(Model& m, const std::string& stage, int istep) {
   else if (stage == "solve") return solver_sparse(m);
   else if (stage == "vel") vel(m);
   else if (stage == "scalar") { exsal(m); imsal(m); }
+  else if (stage == "tracer") tracers(m);
   else if (stage == "vel2") vel2(m);
   else if (stage == "fd") return fd(m, C);
   else if (stage == "settrap") settrap(m);

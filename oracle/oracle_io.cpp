@@ -105,9 +105,16 @@ static bool read_inp(Model& m, const std::string& dir) {
   L.skip(3); ok &= rec_i(L, p.nxNBO);                                 // ioNBTOGGLE=1 block
   if (p.nxNBO != 0) { m.err = "nested-boundary output (nxNBO>0) is not supported"; return false; }
   L.skip(7);
-  L.skip(3); ok &= rec_i(L, p.ntr);                                   // :174-190
-  if (p.ntr != 0) { m.err = "non-active tracers (ntr>0) are outside the hot path"; return false; }
-  L.skip(5);
+  L.skip(3); ok &= rec_i(L, p.ntr);                                   // :172-190
+  if (p.ntr > 0) {
+    ok &= rec_i(L, p.ecomod); ok &= rec_i(L, p.iotr); ok &= rec_i(L, p.itspftr); ok &= rec_i(L, p.ipwq);
+    ok &= rec_i(L, p.nswq);
+    if (p.ntr > 30) { m.err = "ntr > ntrmax = 30 (si3d_types.f90:291)"; return false; }
+    // srcsnk00 (si3d_ecomod.f90:24-34): conservative tracers; the other models are not restated
+    if (p.ecomod != 0) { m.err = "only conservative tracers (ecomod=0) are restated"; return false; }
+  } else {
+    L.skip(5);
+  }
   L.skip(3); ok &= rec_i(L, p.iopss);                                 // :193-230
   if (p.iopss != 0) { m.err = "point sources (iopss>0) are outside the hot path"; return false; }
   if (!ok) { m.err = "si3d_inp.txt: bad record in output/boundary blocks"; return false; }
@@ -229,18 +236,24 @@ static bool read_bathy(Model& m, const std::string& dir) {
 }
 
 // si3d_init.txt, InitProc=4 file branch (si3d_procedures.f90:293-318)
+// Records '(10X, ntr+1 G11.5)': temperature, then one column per tracer; prof is (km1, ntr + 1)
+// with k fastest.
 static bool read_init_profile(Model& m, const std::string& dir, std::vector<real>& prof) {
   Lines L;
   if (!load_lines(dir + "/si3d_init.txt", L)) { m.err = "Error opening si3d_init.txt"; return false; }
   L.skip(5);   // '(////)'
   L.skip(1);   // tracer_line '(A)'
   L.skip(1);   // '(A)'
-  prof.assign(m.km1, 0.0);
+  const int nc = m.in.ntr + 1;
+  prof.assign((size_t)m.km1 * nc, 0.0);
   for (int k = 1; k <= m.km1; ++k) {
     if (L.eof()) { m.err = "si3d_init.txt: truncated"; return false; }
-    real v;
-    if (!parse_num(field(L.next(), 10, 11), v)) { m.err = "si3d_init.txt: bad value"; return false; }
-    prof[k - 1] = v;
+    const std::string line = L.next();
+    for (int c = 0; c < nc; ++c) {
+      real v;
+      if (!parse_num(field(line, 10 + 11 * c, 11), v)) { m.err = "si3d_init.txt: bad value"; return false; }
+      prof[(size_t)c * m.km1 + k - 1] = v;
+    }
   }
   return true;
 }
@@ -313,6 +326,16 @@ static void init_state(Model& m, const std::vector<real>& prof) {
   for (int l = 1; l <= lm1; ++l)
     for (int k = 1; k <= km1; ++k) m.salp(k, l) = prof[k - 1];
   m.sal = m.salp; m.salpp = m.salp;
+  // non-active tracers, ecomod >= 0 branch: tracer(k,:,nn) = column nn + 1 (:335-351); the
+  // sediment-layer values of the Hg and suspended-sediment species do not apply to ecomod = 0
+  m.tracer.assign(m.in.ntr, F3());
+  for (int nn = 1; nn <= m.in.ntr; ++nn) {
+    F3& t = m.tracer[nn - 1];
+    t.init(km1, lm1, 0.0);
+    for (int l = 1; l <= lm1; ++l)
+      for (int k = 1; k <= km1; ++k) t(k, l) = prof[(size_t)nn * km1 + k - 1];
+  }
+  m.tracerpp = m.tracer;
   for (int l = 1; l <= lm1; ++l)
     for (int k = k1; k <= km1; ++k) {
       real z = (m.zl(k) == -100.) ? 0.5 * m.hp(k, l) : m.zl(k) + 0.5 * m.hp(k, l);

@@ -77,9 +77,10 @@ class OracleRun:
         if not h:
             raise RuntimeError(f"oracle: {err.value.decode()}")
         self.h = C.c_void_p(h)
-        d = np.zeros(8, dtype=np.int32)
+        d = np.zeros(9, dtype=np.int32)
         L.orc_dims(self.h, _p(d))
         self.im1, self.jm1, self.km1, self.lm, self.km, self.k1, self.nts = (int(x) for x in d[:7])
+        self.ntr = int(d[8])
         self.lm1 = self.lm + 1
 
     def run(self, nsteps: int) -> None:
@@ -87,7 +88,7 @@ class OracleRun:
             raise RuntimeError(f"oracle: {lib().orc_error(self.h).decode()}")
 
     def get(self, name: str) -> np.ndarray:
-        if name in FIELDS_3D:
+        if name in FIELDS_3D or name.startswith("tracer"):
             a = np.empty((self.km1, self.lm1), order="F")
         else:
             a = np.empty(self.lm1)

@@ -102,6 +102,18 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
+// Roe's superbee limiter (the reference always uses it, si3d_procedures.f90:2931-2934 in exsal,
+// :4186-4190 in exTracer); cf0 is the default C_f.
+__device__ __forceinline__ double superbee(double s1, double s2, double s3, double s4, double vel, double cf0) {
+  double C_f = cf0;
+  if (s3 - s2 != 0) {
+    const bool down = copysign(1.0, vel) > 0;  // gamma1 = -SIGN(1, vel)
+    const double ratio = down ? (s2 - s1) / (s3 - s2) : (s4 - s3) / (s3 - s2);
+    C_f = fmax(fmax(0., fmin(1., 2. * ratio)), fmin(2., ratio));
+  }
+  return C_f;
+}
+
 __device__ __forceinline__ double zmid(const Dev& d, int k, double hpk) {
   const double z = zl(d, k);
   return (z == -100.) ? 0.5 * hpk : z + 0.5 * hpk;

@@ -59,7 +59,7 @@ struct HostModel {
   double xl = 0, yl = 0, zl = 0, tl = 0, idx = 0, idy = 0, idz = 0, dzmin = 0, datadj = 0, zetainit = 0, idt = 0;
   double beta = 0, Av0 = 0, Dv0 = 0, Ax0 = 0, Ay0 = 0, f = 0, theta = 1, cd = 0, dtsurfbc = 0, cw = 0, wa = 0, phi = 0;
   int ibathyf = 0, itrap = 1, niter = 2, ismooth = 0, iturb = 0, iadv = 1, itrmom = 1, ihd = 1, ibc = 1, isal = 1,
-      itrsca = 0, ifsurfbc = 0, icw = 0, nopen = 0, ntr = 0, iopss = 0, iox = 0, nxNBO = 0;
+      itrsca = 0, ifsurfbc = 0, icw = 0, nopen = 0, ntr = 0, iopss = 0, iox = 0, nxNBO = 0, ecomod = 0;
   // grid
   int im = 0, im1 = 0, jm = 0, jm1 = 0, km = 0, km1 = 0, k1 = 2, lm = 0, lm1 = 0, nts = 0;
   std::vector<double> zlevel, hhs, hhu, hhv;
@@ -68,6 +68,7 @@ struct HostModel {
   std::vector<int> ij2l;
   // initial state
   std::vector<double> s0, hp0, hup0, hvp0, salp0, Av0f, Dv0f, uair, vair, cdw;
+  std::vector<double> tracer0;   // ntr fields of (km1, lm1), column-major
   std::vector<int> k1z0, k1u0, k1v0;
   // run
   int gpu = -1, n = 0;
@@ -107,14 +108,21 @@ bool read_parameters(HostModel& M, const std::string& dir) {
   R.skip(3); gi(dummy); gi(dummy); gi(dummy);    // ipxml, itspf, iTurbVars
   R.skip(3); gi(M.nopen); R.skip(7);
   R.skip(3); gi(M.nxNBO); R.skip(7);
-  R.skip(3); gi(M.ntr); R.skip(5);
+  R.skip(3); gi(M.ntr);                          // tracer block (si3d_utils.f90:172-190)
+  if (M.ntr > 0) { gi(M.ecomod); gi(dummy); gi(dummy); gi(dummy); gi(dummy); }   // iotr itspftr ipwq nswq
+  else R.skip(5);
   R.skip(3); gi(M.iopss);
   if (!ok) { M.err = "si3d_inp.txt: unreadable record"; return false; }
-  if (M.iox || M.nopen || M.nxNBO || M.ntr || M.iopss || M.ifsurfbc || M.iturb || M.ihd > 1 || M.ibathyf < 0 ||
+  if (M.iox || M.nopen || M.nxNBO || M.iopss || M.ifsurfbc || M.iturb || M.ihd > 1 || M.ibathyf < 0 ||
       M.ismooth || M.itrmom != 1) {
-    M.err = "si3d_inp.txt selects an option outside the semi-implicit core (open boundaries, tracers, point "
+    M.err = "si3d_inp.txt selects an option outside the semi-implicit core (open boundaries, point "
             "sources, heat budget, turbulence closure, Smagorinsky, smoothing, non-centred advection or "
             "variable layers)";
+    return false;
+  }
+  if (M.ntr < 0 || M.ntr > 30 || (M.ntr > 0 && M.ecomod != 0)) {
+    M.err = "si3d_inp.txt: only 0..30 conservative tracers (ecomod = 0) are supported; water quality, "
+            "tracer clouds, size structure and sediment models are not";
     return false;
   }
   M.im = (int)std::lround(M.xl / M.idx) + 1; M.im1 = M.im + 1;
@@ -200,10 +208,15 @@ bool read_profile(HostModel& M, const std::string& dir, std::vector<double>& pro
   Records R;
   if (!R.load(dir + "/si3d_init.txt")) { M.err = "cannot open si3d_init.txt"; return false; }
   R.skip(7);
-  prof.assign(M.km1, 0.0);
+  // records '(10X, ntr+1 G11.5)' (si3d_procedures.f90:313-318): temperature, then one column per
+  // tracer; prof is (km1, ntr + 1) with k fastest
+  const int nc = M.ntr + 1;
+  prof.assign((size_t)M.km1 * nc, 0.0);
   for (int k = 0; k < M.km1; ++k) {
     if (!R.more()) { M.err = "si3d_init.txt: truncated"; return false; }
-    if (!numeric(R.take(), 10, 11, prof[k])) { M.err = "si3d_init.txt: bad value"; return false; }
+    const std::string rec = R.take();
+    for (int c = 0; c < nc; ++c)
+      if (!numeric(rec, 10 + 11 * c, 11, prof[(size_t)c * M.km1 + k])) { M.err = "si3d_init.txt: bad value"; return false; }
   }
   return true;
 }
@@ -277,6 +290,11 @@ void initial_state(HostModel& M, const std::vector<double>& prof) {
   M.salp0.assign(n3, 0.0);
   for (int l = 1; l <= lm1; ++l)
     for (int k = 1; k <= km1; ++k) M.salp0[M.I3(k, l)] = prof[k - 1];
+  // tracer(k, :, nn) = column nn + 1 for every column incl. lm1 (:335-351, ecomod = 0)
+  M.tracer0.assign(n3 * M.ntr, 0.0);
+  for (int nn = 1; nn <= M.ntr; ++nn)
+    for (int l = 1; l <= lm1; ++l)
+      for (int k = 1; k <= km1; ++k) M.tracer0[n3 * (nn - 1) + M.I3(k, l)] = prof[(size_t)nn * km1 + k - 1];
   M.Av0f.assign(n3, 0.0); M.Dv0f.assign(n3, 0.0);
   for (int l = 1; l <= M.lm; ++l) {
     const int kms = M.kmz[l - 1], k1s = M.k1z0[l - 1];
@@ -349,6 +367,7 @@ int si3d_host_attach_gpu(int h, int device, int* gpu_handle) {
   p.niter = M->niter; p.ismooth = M->ismooth;
   p.pcg_test = M->opt.pcg_test; p.pcg_tol = M->opt.pcg_tol; p.pcg_itmax = M->opt.pcg_itmax; p.srelpr = M->opt.srelpr;
   p.ordering = SI3D_ORDER_REDBLACK; p.x0_mode = M->opt.x0_mode; p.precision = M->opt.precision;
+  p.ntr = M->ntr;
   int gh = -1;
   int rc = si3d_gpu_init(&g, &p, device, &gh);
   if (rc) return rc;
@@ -363,6 +382,12 @@ int si3d_host_attach_gpu(int h, int device, int* gpu_handle) {
   for (const char* nm : same_hv) if ((rc = si3d_gpu_set_field(gh, nm, M->hvp0.data()))) return rc;
   const char* same_t[] = {"sal", "salp", "salpp"};
   for (const char* nm : same_t) if ((rc = si3d_gpu_set_field(gh, nm, M->salp0.data()))) return rc;
+  for (int nn = 1; nn <= M->ntr; ++nn) {   // tracerpp = tracer (:352)
+    const double* t0 = M->tracer0.data() + (size_t)(nn - 1) * M->km1 * M->lm1;
+    const std::string a = "tracer" + std::to_string(nn), b = "tracerpp" + std::to_string(nn);
+    if ((rc = si3d_gpu_set_field(gh, a.c_str(), t0))) return rc;
+    if ((rc = si3d_gpu_set_field(gh, b.c_str(), t0))) return rc;
+  }
   if ((rc = si3d_gpu_set_field(gh, "Av", M->Av0f.data()))) return rc;
   if ((rc = si3d_gpu_set_field(gh, "Dv", M->Dv0f.data()))) return rc;
   if ((rc = si3d_gpu_set_field(gh, "uair", M->uair.data()))) return rc;

@@ -201,26 +201,17 @@ __global__ void k_cont2(Dev d) {
 }
 
 // ------------------------------------------------------------- exsal fluxes
-// Roe's superbee limiter (the reference always uses it, :2931-2934); cf0 is the default C_f.
-__device__ __forceinline__ double superbee(double s1, double s2, double s3, double s4, double vel, double cf0) {
-  double C_f = cf0;
-  if (s3 - s2 != 0) {
-    const bool down = copysign(1.0, vel) > 0;  // gamma1 = -SIGN(1, vel)
-    const double ratio = down ? (s2 - s1) / (s3 - s2) : (s4 - s3) / (s3 - s2);
-    C_f = fmax(fmax(0., fmin(1., 2. * ratio)), fmin(2., ratio));
-  }
-  return C_f;
-}
 
 // Cell-parallel kernels use blocks of 32 consecutive columns x CLN layer lanes: a warp reads one
 // layer of 32 consecutive columns (coalesced) and each thread takes layers k0 + lane, k0 + lane + CLN...
 
-// exsal's three limited fluxes per cell (:2895-3013), into the persistent Bth2/Bth4/Bth3 fields.
+// exsal's three limited fluxes per cell (:2895-3013) of the scalar `sp` (salpp; exTracer's flux
+// loops, :4140-4330, run the same code on tracerpp), into the persistent Bth2/Bth4/Bth3 fields.
 // Every value a layer may need is loaded before any test (all addresses are valid: neighbours are
 // real columns or the dry column lm1, and layer k - 2 is clamped to 1), so a layer costs one memory
 // round trip; the tests then only select among loaded values, in the reference's arithmetic.
 template <int CLN>
-__global__ void __launch_bounds__(32 * CLN) k_exsal_flux(Dev d) {
+__global__ void __launch_bounds__(32 * CLN) k_exsal_flux(Dev d, const double* __restrict__ sp) {
   const int l = blockIdx.x * 32 + threadIdx.x + 1;
   if (l > d.g.lm) return;
   const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
@@ -229,7 +220,6 @@ __global__ void __launch_bounds__(32 * CLN) k_exsal_flux(Dev d) {
   const int lEE = NB(d.g.lEC, lE), lNN = NB(d.g.lNC, lN);
   const int P = d.g.P;
   const double twodt1 = d.p.twodt * d.tz;
-  const double* __restrict__ sp = d.f.salpp;
   const double* __restrict__ hpp = d.f.hpp;
   const double* __restrict__ hp = d.f.hp;
   const double* __restrict__ hup = d.f.hup;
@@ -826,15 +816,25 @@ void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cu
 
 void launch_exsal_imsal(const Dev& d, const Tune& tu, cudaStream_t st) {
   const int cg = (d.g.lm + 31) / 32;
+  const double* sp = d.f.salpp;
   switch (tu.sal_cl) {
-    case 2: k_exsal_flux<2><<<cg, dim3(32, 2), 0, st>>>(d); k_exsal_rhs<2><<<cg, dim3(32, 2), 0, st>>>(d); break;
-    case 4: k_exsal_flux<4><<<cg, dim3(32, 4), 0, st>>>(d); k_exsal_rhs<4><<<cg, dim3(32, 4), 0, st>>>(d); break;
-    default: k_exsal_flux<8><<<cg, dim3(32, 8), 0, st>>>(d); k_exsal_rhs<8><<<cg, dim3(32, 8), 0, st>>>(d); break;
+    case 2: k_exsal_flux<2><<<cg, dim3(32, 2), 0, st>>>(d, sp); k_exsal_rhs<2><<<cg, dim3(32, 2), 0, st>>>(d); break;
+    case 4: k_exsal_flux<4><<<cg, dim3(32, 4), 0, st>>>(d, sp); k_exsal_rhs<4><<<cg, dim3(32, 4), 0, st>>>(d); break;
+    default: k_exsal_flux<8><<<cg, dim3(32, 8), 0, st>>>(d, sp); k_exsal_rhs<8><<<cg, dim3(32, 8), 0, st>>>(d); break;
   }
   switch (tu.sal_nt) {
     case 64: k_imsal<64><<<(d.g.lm + 63) / 64, 64, 0, st>>>(d); break;
     case 256: k_imsal<256><<<(d.g.lm + 255) / 256, 256, 0, st>>>(d); break;
     default: k_imsal<128><<<(d.g.lm + 127) / 128, 128, 0, st>>>(d); break;
+  }
+}
+
+void launch_scalar_flux(const Dev& d, const double* cpp, const Tune& tu, cudaStream_t st) {
+  const int cg = (d.g.lm + 31) / 32;
+  switch (tu.sal_cl) {
+    case 2: k_exsal_flux<2><<<cg, dim3(32, 2), 0, st>>>(d, cpp); break;
+    case 4: k_exsal_flux<4><<<cg, dim3(32, 4), 0, st>>>(d, cpp); break;
+    default: k_exsal_flux<8><<<cg, dim3(32, 8), 0, st>>>(d, cpp); break;
   }
 }
 

@@ -130,6 +130,16 @@ struct Ctx {
   int* d_stats_ii = nullptr;     // [24][2]
   double* d_stats_rr = nullptr;  // [24]
   double* staging = nullptr;  // device staging for transposes (km1 * lm1)
+  // non-active tracers: two pools of ntr layer-major fields; tr_buf[tr_cur] holds tracer, the other
+  // tracerpp.  save makes tracerpp = tracer by swapping the pools; after it the tracer pool is not
+  // read (tr_alias: "tracer" reads resolve to tracerpp) until the next ImTracer rewrites every
+  // entry it may change.  Entries no routine writes (below kmz + 1, the dry column) are the same in
+  // both pools once tr_synced; a host write clears it and the next save copies instead of swapping.
+  double* tr_buf[2] = {nullptr, nullptr};
+  int tr_cur = 0;
+  bool tr_alias = true, tr_synced = true;
+  long long tr_stride = 0;
+  double* tr_scr = nullptr;   // elimination factors, one km1 x P field per tracer group
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
   ~Ctx() {
     if (st) cudaStreamSynchronize(st);
@@ -164,7 +174,7 @@ Ctx* get(int h) {
 
 // Stage ids for the per-stage device timers.
 enum { ST_MOMX, ST_MOMY, ST_MATCON, ST_PCG_SETUP, ST_PCG_ITER, ST_PCG_FINISH, ST_SLAYER, ST_VEL, ST_SCALAR, ST_VEL2,
-       ST_SETTRAP, ST_SETTRAP2, ST_SAVE, ST_LEARN, ST_COUNT };
+       ST_SETTRAP, ST_SETTRAP2, ST_SAVE, ST_LEARN, ST_TRACER, ST_COUNT };
 
 // Run `f` (which enqueues `nk` kernels) as one timed stage.
 template <class F>
@@ -200,6 +210,56 @@ double* f3ptr(Ctx* c, const std::string& n) {
       {"Bth2", &Fields3::Bth2}, {"Bth3", &Fields3::Bth3}, {"Bth4", &Fields3::Bth4}};
   auto it = t.find(n);
   return it == t.end() ? nullptr : f.*(it->second);
+}
+
+// "tracer<nt>" / "tracerpp<nt>", nt = 1..ntr: sets *pp and returns nt, else 0.
+int tracer_name(const Ctx* c, const std::string& n, bool* pp) {
+  for (const char* pre : {"tracerpp", "tracer"}) {
+    const size_t np = std::strlen(pre);
+    if (n.size() > np && n.compare(0, np, pre) == 0 && n.find_first_not_of("0123456789", np) == std::string::npos) {
+      const int nt = std::atoi(n.c_str() + np);
+      *pp = np == 8;
+      return (nt >= 1 && nt <= c->prm.ntr) ? nt : -1;
+    }
+  }
+  return 0;
+}
+
+double* tracer_pool(Ctx* c, bool pp) { return c->tr_buf[pp ? 1 - c->tr_cur : c->tr_cur]; }
+
+// Give the tracer pool its own copy of tracerpp before a host write to either field.
+int tracer_materialise(Ctx* c) {
+  if (!c->tr_alias) return 0;
+  const size_t bytes = sizeof(double) * (size_t)c->tr_stride * c->prm.ntr;
+  CK(cudaMemcpyAsync(tracer_pool(c, false), tracer_pool(c, true), bytes, cudaMemcpyDeviceToDevice, c->st));
+  c->tr_alias = false;
+  return 0;
+}
+
+// fd's tracer block (si3d_procedures.f90:520-544, ecomod = 0): every tracer's right-hand side and
+// column solve, then exsal's flux kernel on the last tracer so that the persistent flux arrays hold
+// what the reference's last exTracer leaves in them.
+void tracer_stage(Ctx* c) {
+  const int ntr = c->prm.ntr;
+  double* tr = tracer_pool(c, false);
+  const double* trpp = tracer_pool(c, true);
+  launch_tracers(c->d, trpp, tr, c->tr_alias ? trpp : tr, ntr, c->tr_stride, c->tr_scr, c->st);
+  launch_scalar_flux(c->d, trpp + (ntr - 1) * c->tr_stride, c->tune, c->st);
+  c->tr_alias = false;
+}
+
+// save's tracerpp = tracer (:3771-3774, :3926-3929).
+int tracer_save(Ctx* c) {
+  if (c->prm.ntr == 0 || c->tr_alias) return 0;
+  if (c->tr_synced) {
+    c->tr_cur = 1 - c->tr_cur;
+  } else {
+    const size_t bytes = sizeof(double) * (size_t)c->tr_stride * c->prm.ntr;
+    CK(cudaMemcpyAsync(tracer_pool(c, true), tracer_pool(c, false), bytes, cudaMemcpyDeviceToDevice, c->st));
+    c->tr_synced = true;
+  }
+  c->tr_alias = true;
+  return 0;
 }
 
 double* f2ptr(Ctx* c, const std::string& n) {
@@ -706,7 +766,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   return 0;
 }
 
-int fd_impl(Ctx* c, int istep, si3d_step_stats* st) {
+int fd_impl(Ctx* c, int istep, bool lastiter, si3d_step_stats* st) {
   Dev& d = c->d;
   d.tz = 1.0 / istep;
   c->cur_istep = istep;
@@ -734,6 +794,7 @@ int fd_impl(Ctx* c, int istep, si3d_step_stats* st) {
   rc = stage(c, ST_SLAYER, 1, [&] { launch_slayer_h(d, c->st); });
   if (!rc) rc = stage(c, ST_VEL, 3, [&] { launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st); });
   if (!rc && c->prm.isal != 0) rc = stage(c, ST_SCALAR, 3, [&] { launch_exsal_imsal(d, c->tune, c->st); });
+  if (!rc && c->prm.ntr > 0 && c->prm.niter > 0 && lastiter) rc = stage(c, ST_TRACER, 3, [&] { tracer_stage(c); });
   if (!rc) rc = stage(c, ST_VEL2, 1, [&] { launch_vel2(d, c->st); });
   if (rc) return rc;
   if (st) {
@@ -779,6 +840,14 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
   if (prm->itrmom != 1 || prm->ihd > 1 || prm->pcg_itmax < 1 || (prm->pcg_test != 5 && prm->pcg_test != 2))
     return SI3D_EDIMS;
   if (prm->x0_mode < SI3D_X0_PREV || prm->x0_mode > SI3D_X0_HIST) return SI3D_EDIMS;
+  if (prm->ntr < 0 || prm->ntr > 30) return SI3D_EDIMS;   // ntrmax (si3d_types.f90:291)
+  // every kernel indexes neighbours through the maps and layers down to kmz + 1: both are checked
+  // here once, so no device access can leave its field
+  for (int l = 0; l < g->lm; ++l) {
+    if (g->kmz[l] < g->k1 || g->kmz[l] > g->km1 - 1) return SI3D_EDIMS;
+    for (const int* m : {g->lEC, g->lWC, g->lNC, g->lSC})
+      if (m[l] < 1 || m[l] > g->lm + 1) return SI3D_EDIMS;
+  }
   if (prm->precision != SI3D_FP64 && prm->precision != SI3D_MIXED_IR && prm->precision != SI3D_MIXED_MG)
     return SI3D_EDIMS;
   int ndev = 0;
@@ -852,6 +921,12 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
     rc |= c->alloc(q, P);
   for (int** q : {&s.k1z, &s.k1u, &s.k1v}) rc |= c->alloc(q, P);
   rc |= c->alloc(&d.scr, n3);
+  if (prm->ntr > 0) {
+    c->tr_stride = (long long)n3;
+    rc |= c->alloc(&c->tr_buf[0], n3 * prm->ntr);
+    rc |= c->alloc(&c->tr_buf[1], n3 * prm->ntr);
+    rc |= c->alloc(&c->tr_scr, n3 * ((prm->ntr + kTracerGroup - 1) / kTracerGroup));
+  }
   rc |= c->alloc(&c->staging, (size_t)km1 * lm1);
   rc |= c->alloc(&c->dz, P);
   rc |= c->alloc(&c->d_stats_ii, 48);
@@ -948,7 +1023,18 @@ int si3d_gpu_set_field(int h, const char* name, const double* host) {
   if (!c) return SI3D_EHANDLE;
   if (!name || !host) return SI3D_EDIMS;
   CK(cudaSetDevice(c->device));
-  if (double* dst = f3ptr(c, name)) {
+  bool pp = false;
+  const int nt = tracer_name(c, name, &pp);
+  if (nt < 0) return SI3D_ENAME;
+  double* dst = nullptr;
+  if (nt > 0) {
+    if (int rc = tracer_materialise(c)) return rc;
+    c->tr_synced = false;
+    dst = tracer_pool(c, pp) + (nt - 1) * c->tr_stride;
+  } else {
+    dst = f3ptr(c, name);
+  }
+  if (dst) {
     CK(cudaMemcpyAsync(c->staging, host, sizeof(double) * c->km1 * c->lm1, cudaMemcpyHostToDevice, c->st));
     dim3 b(32, 8), gr((c->lm1 + 31) / 32, (c->km1 + 31) / 32);
     k_colmajor_to_layer<<<gr, b, 0, c->st>>>(c->staging, dst, c->km1, c->lm1, c->P);
@@ -969,7 +1055,11 @@ int si3d_gpu_get_field(int h, const char* name, double* host) {
   if (!c) return SI3D_EHANDLE;
   if (!name || !host) return SI3D_EDIMS;
   CK(cudaSetDevice(c->device));
-  if (double* src = f3ptr(c, name)) {
+  bool pp = false;
+  const int nt = tracer_name(c, name, &pp);
+  if (nt < 0) return SI3D_ENAME;
+  const double* src = nt > 0 ? tracer_pool(c, pp || c->tr_alias) + (nt - 1) * c->tr_stride : f3ptr(c, name);
+  if (src) {
     dim3 b(32, 8), gr((c->lm1 + 31) / 32, (c->km1 + 31) / 32);
     k_layer_to_colmajor<<<gr, b, 0, c->st>>>(src, c->staging, c->km1, c->lm1, c->P);
     CK(cudaGetLastError());
@@ -1080,13 +1170,13 @@ int si3d_learn_recorded(int h) {
 }
 
 int si3d_gpu_fd(int h, int n, int istep, int lastiter, si3d_step_stats* st) {
-  (void)n; (void)lastiter;
+  (void)n;
   Ctx* c = get(h);
   if (!c) return SI3D_EHANDLE;
   if (istep != 1 && istep != 2) return SI3D_EDIMS;
   CK(cudaSetDevice(c->device));
   if (st) { std::memset(st, 0, sizeof(*st)); CK(cudaEventRecord(c->ev0, c->st)); }
-  int rc = fd_impl(c, istep, st);
+  int rc = fd_impl(c, istep, lastiter != 0, st);
   if (rc) return rc;
   if (st) {
     CK(cudaEventRecord(c->ev1, c->st));
@@ -1130,10 +1220,11 @@ int si3d_gpu_stage(int h, const char* stage, int istep, si3d_step_stats* st) {
     launch_slayer_h(d, c->st);
   } else if (s == "vel") launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st);
   else if (s == "scalar") launch_exsal_imsal(d, c->tune, c->st);
+  else if (s == "tracer") { if (c->prm.ntr > 0) tracer_stage(c); }
   else if (s == "vel2") launch_vel2(d, c->st);
   else if (s == "settrap") launch_settrap(d, c->st);
   else if (s == "settrap2") launch_settrap2(d, c->st);
-  else if (s == "save") launch_save(d, istep, c->st);
+  else if (s == "save") { launch_save(d, istep, c->st); if (int rc = tracer_save(c)) return rc; }
   else return SI3D_ENAME;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
@@ -1166,6 +1257,7 @@ int si3d_gpu_save(int h, int istep) {
   if (istep != 1 && istep != 2) return SI3D_EDIMS;
   CK(cudaSetDevice(c->device));
   launch_save(c->d, istep, c->st);
+  if (int rc = tracer_save(c)) return rc;
   c->trap_solves = 0;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
@@ -1184,10 +1276,12 @@ static int step_impl(Ctx* c, int n, si3d_step_stats* st) {
   if (n == 1) {
     niter1 = std::max(2, p.niter);
   } else {
-    rc = fd_impl(c, 1, st);
+    const bool leapfrog_only = p.itrap == 0 || (n % std::max(p.itrap, 1)) != 0;
+    rc = fd_impl(c, 1, leapfrog_only, st);
     if (rc) return rc;
-    if (p.itrap == 0 || (n % std::max(p.itrap, 1)) != 0) {
+    if (leapfrog_only) {
       rc = stage(c, ST_SAVE, 2, [&] { launch_save(c->d, 1, c->st); });
+      if (!rc) rc = tracer_save(c);
       if (rc) return rc;
       goto done;
     }
@@ -1195,7 +1289,7 @@ static int step_impl(Ctx* c, int n, si3d_step_stats* st) {
     if (rc) return rc;
   }
   for (int it = 1; it <= niter1; ++it) {
-    rc = fd_impl(c, 2, st);
+    rc = fd_impl(c, 2, it == niter1, st);
     if (rc) return rc;
     if (it < niter1) {
       rc = stage(c, ST_SETTRAP2, 3, [&] { launch_settrap2(c->d, c->st); });
@@ -1204,6 +1298,7 @@ static int step_impl(Ctx* c, int n, si3d_step_stats* st) {
     if (it > 20) break;
   }
   rc = stage(c, ST_SAVE, 2, [&] { launch_save(c->d, 2, c->st); });
+  if (!rc) rc = tracer_save(c);
   if (rc) return rc;
 done:
   CK(cudaGetLastError());
@@ -1381,6 +1476,9 @@ int si3d_ens_create(const int* handles, int n, int* ens) {
 // Capture one step (n >= 2) of every member into one graph: a fork on the master stream, each
 // member's step on its own stream, a join back.
 static int ens_capture(Ens* E) {
+  // a captured step replays fixed pointers, while the two tracer pools change roles at every save
+  for (int h : E->hs)
+    if (get(h)->prm.ntr > 0) return SI3D_EDIMS;
   CK(cudaStreamBeginCapture(E->master, cudaStreamCaptureModeThreadLocal));
   int rc = 0;
   cudaError_t e = cudaEventRecord(E->fork, E->master);
@@ -1535,7 +1633,8 @@ int si3d_gpu_solve_zeta(int lm, const double* coef, const int* jcoef, const doub
     if (N[m] != lm1 && S[N[m] - 1] != m + 1) return SI3D_EDIMS;
   }
   si3d_grid g{};
-  std::vector<int> kmz(lm1, 3), l2(lm, 1);
+  std::vector<int> kmz(lm1, 2), l2(lm, 1);   // one layer (k1 = 2) per column; the sentinel at km1
+  kmz[lm] = 3;
   std::vector<double> hh(lm1, 1.0), zlv = {-100., -100., 1.0};
   g.im1 = 1; g.jm1 = 1; g.km1 = 3; g.k1 = 2; g.lm = lm;
   g.l2i = l2.data(); g.l2j = l2.data(); g.lEC = E.data(); g.lWC = W.data(); g.lNC = N.data(); g.lSC = S.data();

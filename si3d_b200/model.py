@@ -3,6 +3,7 @@ on the device through the C ABI, read fields back in the reference's (km1, lm1) 
 from __future__ import annotations
 
 import ctypes as C
+import re
 from typing import Optional
 
 import numpy as np
@@ -72,7 +73,7 @@ class GpuRun:
 
     # ------------------------------------------------------------------ fields
     def get(self, name: str) -> np.ndarray:
-        if name in FIELDS_3D:
+        if name in FIELDS_3D or re.fullmatch(r"tracer(pp)?[0-9]+", name):
             a = np.empty((self.km1, self.lm1), dtype=np.float64, order="F")
         elif name in FIELDS_2D:
             a = np.empty(self.lm1, dtype=np.float64)

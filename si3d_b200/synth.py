@@ -57,6 +57,7 @@ class Basin:
     f: float = 1e-4
     niter: int = 2
     ibc: int = 1                 # baroclinic pressure term on/off
+    ntr: int = 0                 # non-active (conservative) tracers, ecomod = 0
     seeds: dict = dataclasses.field(default_factory=dict)
 
     @property
@@ -176,7 +177,7 @@ def write_inp(b: Basin, path: str) -> None:
     L += [_rec(x, 0) for x in ("iside", "itype", "isbc", "jsbc", "iebc", "jebc")]
     L += [sep, "Open boundary conditions for nesting procedures", sep, _rec("nxBDO", 0)]
     L += [_rec(x, 0) for x in ("iob", "xxb", "iside", "isbc", "jsbc", "iebc", "jebc")]
-    L += [sep, "Specification for tracer simulation", sep, _rec("ntr", 0)]
+    L += [sep, "Specification for tracer simulation", sep, _rec("ntr", b.ntr)]
     L += [_rec(x, 0) for x in ("ecomod", "iotr", "itspftr", "ipwq", "nswq")]
     L += [sep, "Specification for oxygenation system simulations", sep, _rec("iopts", 0)]
     L += [_rec(x, 0) for x in ("Nodev", "iodt", "ipss", "jpss", "iodev")]
@@ -209,13 +210,35 @@ def layer_profile(b: Basin) -> np.ndarray:
     return t
 
 
+def tracer_profiles(b: Basin) -> np.ndarray:
+    """Initial tracer concentrations at levels k = 1..km1, shape (ntr, km1): tracer 1 is a step (1
+    above mid-depth, 0 below: a sharp front for the flux limiter), with three or more tracers the
+    last is uniform (0.5), and the others are Gaussian bands centred at evenly spaced depths."""
+    km = int(math.ceil(b.zl / b.ddz)) + 1
+    km1 = km + 1
+    k = np.arange(1, km1 + 1, dtype=np.float64)
+    out = np.zeros((b.ntr, km1))
+    for t in range(b.ntr):
+        if t == 0:
+            out[t] = np.where(k <= (km + 2) / 2, 1.0, 0.0)
+        elif t == b.ntr - 1 and b.ntr >= 3:
+            out[t] = 0.5
+        else:
+            kc = 2 + t * (km - 2) / b.ntr
+            w = max(1.0, (km - 2) / 8)
+            out[t] = np.exp(-((k - kc) / w) ** 2)
+    return np.round(out, 5)
+
+
 def write_init(b: Basin, path: str) -> None:
     t = layer_profile(b)
+    tr = tracer_profiles(b)
+    head = "         z          T" + "".join(f"{'C' + str(i + 1):>11}" for i in range(b.ntr))
     lines = ["Initial condition file for si3d model", f"synthetic {b.name}", "synthetic profile",
-             "Depths (m)   Temp (oC)", "Source: linear", "         z          T", "-" * 40]
+             "Depths (m)   Temp (oC)", "Source: linear", head, "-" * 40]
     for k, tv in enumerate(t, start=1):
         z = -(k - 1.5) * b.ddz
-        lines.append(f"{z:10.2f}{tv:11.5f}")
+        lines.append(f"{z:10.2f}{tv:11.5f}" + "".join(f"{tr[i, k - 1]:11.5f}" for i in range(b.ntr)))
     with open(path, "w") as fh:
         fh.write("\n".join(lines) + "\n")
 
@@ -245,7 +268,8 @@ def write_run(b: Basin, run_dir: str) -> str:
     return run_dir
 
 
-def make(name: str, run_dir: str, nsteps: Optional[int] = None, seed_offset: int = 0) -> Basin:
+def make(name: str, run_dir: str, nsteps: Optional[int] = None, seed_offset: int = 0, ntr: int = 0) -> Basin:
     b = config(name, nsteps, seed_offset)
+    b.ntr = ntr
     write_run(b, run_dir)
     return b

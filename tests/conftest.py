@@ -49,6 +49,19 @@ def native_libs():
 
 
 @pytest.fixture(scope="session")
+def tracer_dirs(tmp_path_factory):
+    """The small runs with three conservative tracers (a step, a Gaussian band, a uniform field)."""
+    from si3d_b200 import synth
+    base = tmp_path_factory.mktemp("tracer_runs")
+    out = {}
+    for name in ("t0", "t1", "c0"):
+        d = str(base / name)
+        synth.make(name, d, ntr=3)
+        out[name] = d
+    return out
+
+
+@pytest.fixture(scope="session")
 def run_dirs(tmp_path_factory):
     """Small reference-format runs shared by the tests."""
     from si3d_b200 import synth

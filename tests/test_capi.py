@@ -100,6 +100,23 @@ def test_bad_arguments_are_rejected(native_libs):
     assert g.si3d_gpu_sync(-1) == -102
 
 
+def test_maps_and_depths_out_of_range_are_rejected(native_libs):
+    """The kernels index neighbours through the maps and layers down to kmz + 1; maps outside
+    [1, lm + 1], a bottom layer outside [k1, km1 - 1] and more tracers than ntrmax are refused at
+    init, before any device work."""
+    g = native_libs.gpu()
+    h = C.c_int(-1)
+    for field, bad in (("kmz", [4, 3, 0]), ("kmz", [1, 3, 0]), ("lEC", [4, 3, 3]), ("lSC", [0, 3, 3])):
+        grid, prm, keep = _tiny_grid()
+        a = np.ascontiguousarray(bad, dtype=np.int32)
+        keep.append(a)
+        setattr(grid, field, a.ctypes.data_as(C.POINTER(C.c_int)))
+        assert g.si3d_gpu_init(C.byref(grid), C.byref(prm), 0, C.byref(h)) == -101, field
+    grid, prm, _keep = _tiny_grid()
+    prm.ntr = 31
+    assert g.si3d_gpu_init(C.byref(grid), C.byref(prm), 0, C.byref(h)) == -101
+
+
 @pytest.mark.skipif(HAS_GPU, reason="checks the no-device path")
 def test_no_device_fails_loudly(native_libs):
     """Without an sm_100 device the core returns SI3D_ENODEV instead of computing anything."""

@@ -71,10 +71,10 @@ def test_truncated_profile(native_libs, run_dirs, tmp_path):
     assert rc == -101 and "si3d_init.txt" in err
 
 
-@pytest.mark.parametrize("label,value", [("nopen", 1), ("ntr", 2), ("iturb", 1)])
+@pytest.mark.parametrize("label,value", [("nopen", 1), ("iturb", 1)])
 def test_options_outside_the_core_are_refused(native_libs, run_dirs, tmp_path, label, value):
-    """Open boundaries, tracers and turbulence closures are not part of the semi-implicit core;
-    a run that selects them is refused rather than silently run without them."""
+    """Open boundaries and turbulence closures are not part of the semi-implicit core; a run that
+    selects them is refused rather than silently run without them."""
     d = _copy(run_dirs["t0"], str(tmp_path / f"opt_{label}"))
     p = os.path.join(d, "si3d_inp.txt")
     lines = open(p).read().splitlines()
@@ -93,3 +93,45 @@ def test_wind_override_size_mismatch(native_libs, run_dirs, tmp_path):
     open(p, "wb").write(data[:-8])
     rc, _, err = _open(native_libs, d)
     assert rc == -101 and "size mismatch" in err
+
+
+def _set_records(path, values):
+    lines = open(path).read().splitlines()
+    for label, value in values:
+        lines[lines.index(synth._rec(label, 0))] = synth._rec(label, value)
+    open(path, "w").write("\n".join(lines) + "\n")
+
+
+def test_tracer_run_opens(native_libs, oracle_lib, tmp_path):
+    """Conservative tracers (ecomod = 0): the host and the oracle both read ntr and the extra
+    columns of si3d_init.txt."""
+    d = str(tmp_path / "tr")
+    synth.make("t0", d, ntr=3)
+    rc, hm, err = _open(native_libs, d)
+    assert rc == 0, err
+    native_libs.host().si3d_host_close(hm)
+    assert oracle_lib.OracleRun(d).ntr == 3
+
+
+def test_tracer_models_other_than_conservative_are_refused(native_libs, oracle_lib, tmp_path):
+    """Water quality, tracer clouds, size structure and sediment (ecomod != 0) are refused by the
+    host and by the oracle instead of being run as conservative tracers."""
+    d = str(tmp_path / "eco")
+    synth.make("t0", d, ntr=2)
+    _set_records(os.path.join(d, "si3d_inp.txt"), [("ecomod", 1)])
+    rc, _, err = _open(native_libs, d)
+    assert rc == -101 and "conservative" in err
+    with pytest.raises(RuntimeError, match="conservative"):
+        oracle_lib.OracleRun(d)
+
+
+def test_tracer_columns_missing_from_profile(native_libs, oracle_lib, run_dirs, tmp_path):
+    """ntr > 0 with a one-column si3d_init.txt: a formatted read pads the short records with blanks,
+    which read as zero, so the tracers start at zero (the host and the oracle both open the run)."""
+    d = _copy(run_dirs["t0"], str(tmp_path / "ntr_noprof"))
+    _set_records(os.path.join(d, "si3d_inp.txt"), [("ntr", 2)])
+    rc, hm, err = _open(native_libs, d)
+    assert rc == 0, err
+    native_libs.host().si3d_host_close(hm)
+    o = oracle_lib.OracleRun(d)
+    assert o.ntr == 2 and not o.get("tracer2").any()
