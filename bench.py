@@ -39,6 +39,12 @@ STAGE_STREAMS = {"momentum_x": (14, "N3"), "momentum_y": (14, "N3"), "matcon": (
 # column -- read e, r, p, q, z, the two faces, mass and 1/diag, write e, r, z, p, q -- the coarser
 # levels (a third of level 0 together) not counted.
 MG_ITER_STREAMS = 15
+# The tracer block of one fd call (exTracer + ImTracer for ntr conservative tracers), per wet 3-D
+# cell: shared streams read once for all tracers (hup, hvp, uhpp, uh, vhpp, vh, wp, hp, hpp, h,
+# Dv, hupp, hvpp) and the three flux arrays written, plus per tracer tracerpp read and tracer
+# written.
+TRACER_SHARED_STREAMS = 16
+TRACER_STREAMS_PER_TRACER = 2
 
 WORKLOAD_DESC = {
     "c2": "c2: 2000x1000 cells x 60 layers, seeded random bathymetry and wind stress, dt 30 s, itrap=1 niter=2, "
@@ -113,12 +119,12 @@ def traffic_table():
     return {}
 
 
-def workload_dir(name: str, rank: int) -> str:
+def workload_dir(name: str, rank: int, ntr: int = 0) -> str:
     from si3d_b200 import synth
-    d = os.path.join(tempfile.gettempdir(), f"si3d_bench_{name}_r{rank}")
+    d = os.path.join(tempfile.gettempdir(), f"si3d_bench_{name}_tr{ntr}_r{rank}")
     marker = os.path.join(d, ".complete")
     if not os.path.exists(marker):
-        synth.make(name, d)
+        synth.make(name, d, ntr=ntr)
         open(marker, "w").close()
     return d
 
@@ -142,7 +148,7 @@ def counts(run_dir: str):
     return lm, n3
 
 
-def cpu_sample(name: str, threads: int, steps: int = 0, warmup: int = 0) -> dict:
+def cpu_sample(name: str, threads: int, steps: int = 0, warmup: int = 0, ntr: int = 0) -> dict:
     """The CPU restatement of the reference timed on a window of the workload (same layers,
     bathymetry and forcing generators), extrapolated linearly in wet 3-D cells.  The column stages
     run on `threads` host threads; the zeta solve is serial, as the reference runs it on thread 0.
@@ -157,11 +163,12 @@ def cpu_sample(name: str, threads: int, steps: int = 0, warmup: int = 0) -> dict
     wx, wy = max(full.nx // 5, 16), max(full.ny // 5, 16)
     x0, y0 = (full.nx - wx) // 2, (full.ny - wy) // 2
     sub.nx, sub.ny = wx, wy
+    sub.ntr = ntr
     sub.depth = full.depth[x0:x0 + wx, y0:y0 + wy].copy()
     if full.uair is not None:
         sub.uair = full.uair[x0:x0 + wx, y0:y0 + wy].copy()
         sub.vair = full.vair[x0:x0 + wx, y0:y0 + wy].copy()
-    d = os.path.join(tempfile.gettempdir(), f"si3d_cpu_window_{name}")
+    d = os.path.join(tempfile.gettempdir(), f"si3d_cpu_window_{name}_tr{ntr}")
     synth.write_run(sub, d)
     os.environ["SI3D_ORACLE_THREADS"] = str(threads)   # read once, at the oracle's first column loop
     pyoracle.build()
@@ -267,6 +274,8 @@ def main() -> int:
     ap.add_argument("--workload", default="c2")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--itmax", type=int, default=2000)
+    ap.add_argument("--ntr", type=int, default=0,
+                    help="conservative tracers carried by the workload (0..30; the headline workload has none)")
     ap.add_argument("--forms", default="",
                     help="comma-separated subset of plain_fp64,mixed_ir,mixed_last,learned_fp64,learned_mixed (the last one "
                          "is the headline); default: plain_fp64,mixed_ir,mixed_last and learned_mixed when trained "
@@ -280,13 +289,14 @@ def main() -> int:
         if rank != 0:
             return 0
         threads = os.cpu_count() or 1
-        lm_full, n3_full = counts(workload_dir(args.workload, 0))
-        smp = cpu_sample(args.workload, threads, steps=args.steps, warmup=args.warmup)
+        lm_full, n3_full = counts(workload_dir(args.workload, 0, args.ntr))
+        smp = cpu_sample(args.workload, threads, steps=args.steps, warmup=args.warmup, ntr=args.ntr)
         v = smp["window_s_per_step"] * n3_full / smp["n3"]
         line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "s/timestep", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD_DESC.get(args.workload, args.workload), "form": "plain_fp64",
+                           "ntr": args.ntr,
                            "lm": lm_full, "n3": n3_full, "parallelism": "replicas x1",
                            "l2": "host run; no GPU caches involved"},
                 "cpu_baseline": {"value": v, "unit": "s/timestep", "cores": threads, "kind": "port",
@@ -316,7 +326,7 @@ def main() -> int:
     sbuild.build_all()
     if args.workload == "c3":
         return bench_ensemble(args, ws, rank, device, pg)
-    run_dir = workload_dir(args.workload, rank)
+    run_dir = workload_dir(args.workload, rank, args.ntr)
     lm, n3 = counts(run_dir)
     peak, peak_kind = measured_peaks()
     g = native.gpu()
@@ -362,6 +372,13 @@ def main() -> int:
         stage_ms = {k: v for k, v in prof.items() if v[1] > 0}
         out["stage_ms_per_step"] = {k: v[0] / 2 for k, v in stage_ms.items()}
         out["zeta"] = run.get("s")[:run.lm].copy()   # after warmup + steps + 2 steps, the same in every form
+        if "tracer" in stage_ms:
+            ms, calls = stage_ms["tracer"]
+            alg = 8 * n3 * (TRACER_SHARED_STREAMS + TRACER_STREAMS_PER_TRACER * args.ntr)
+            out["tracer_stage"] = {"ntr": args.ntr, "ms_per_call": ms / calls, "calls_per_step": calls / 2,
+                                   "ms_per_tracer": ms / calls / args.ntr, "algorithmic_bytes_per_call": alg,
+                                   "achieved": alg / (ms / calls * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
+                                   "frac": alg / (ms / calls * 1e-3) / 1e9 / peak, "peak_kind": peak_kind}
         dominant = max(stage_ms, key=lambda k: stage_ms[k][0])
         if dominant in STAGE_STREAMS:
             streams, unit = STAGE_STREAMS[dominant]
@@ -424,7 +441,7 @@ def main() -> int:
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        smp = cpu_sample(args.workload, threads)
+        smp = cpu_sample(args.workload, threads, ntr=args.ntr)
         v = smp["window_s_per_step"] * n3 / smp["n3"]
         cpu = {"value": v, "unit": "s/timestep", "cores": threads, "kind": "port",
                "sample": f"{smp['steps']} steps of a {smp['window']} window (plain FP64, red-black MIC-PCG at 1e-12), "
@@ -443,7 +460,7 @@ def main() -> int:
                       "mg_mixed": "f64 (fp32 multigrid inner solves)",
                       "learned_mg": "f64 (fp32 multigrid inner solves, bf16 guess net)"}[head_form], "data": "synthetic",
             "config": {"workload": WORKLOAD_DESC.get(args.workload, args.workload),
-                       "form": head_form, "lm": lm, "n3": n3, "parallelism": f"replicas x{ws}",
+                       "form": head_form, "ntr": args.ntr, "lm": lm, "n3": n3, "parallelism": f"replicas x{ws}",
                        "l2": "state (~25 GB) far larger than L2; no flush needed"},
             "pcg_iters_per_step": head["pcg_iters_per_step"], "pcg_s_per_step": head["pcg_s_per_step"],
             "speedup_vs_plain_fp64": plain["s_per_step"] / head["s_per_step"],

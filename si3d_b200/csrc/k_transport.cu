@@ -205,8 +205,8 @@ __global__ void k_cont2(Dev d) {
 // Cell-parallel kernels use blocks of 32 consecutive columns x CLN layer lanes: a warp reads one
 // layer of 32 consecutive columns (coalesced) and each thread takes layers k0 + lane, k0 + lane + CLN...
 
-// exsal's three limited fluxes per cell (:2895-3013) of the scalar `sp` (salpp; exTracer's flux
-// loops, :4140-4330, run the same code on tracerpp), into the persistent Bth2/Bth4/Bth3 fields.
+// exsal's three limited fluxes per cell (:2895-3013) of the scalar `sp` (salpp), into the
+// persistent Bth2/Bth4/Bth3 fields.
 // Every value a layer may need is loaded before any test (all addresses are valid: neighbours are
 // real columns or the dry column lm1, and layer k - 2 is clamped to 1), so a layer costs one memory
 // round trip; the tests then only select among loaded values, in the reference's arithmetic.
@@ -826,15 +826,6 @@ void launch_exsal_imsal(const Dev& d, const Tune& tu, cudaStream_t st) {
     case 64: k_imsal<64><<<(d.g.lm + 63) / 64, 64, 0, st>>>(d); break;
     case 256: k_imsal<256><<<(d.g.lm + 255) / 256, 256, 0, st>>>(d); break;
     default: k_imsal<128><<<(d.g.lm + 127) / 128, 128, 0, st>>>(d); break;
-  }
-}
-
-void launch_scalar_flux(const Dev& d, const double* cpp, const Tune& tu, cudaStream_t st) {
-  const int cg = (d.g.lm + 31) / 32;
-  switch (tu.sal_cl) {
-    case 2: k_exsal_flux<2><<<cg, dim3(32, 2), 0, st>>>(d, cpp); break;
-    case 4: k_exsal_flux<4><<<cg, dim3(32, 4), 0, st>>>(d, cpp); break;
-    default: k_exsal_flux<8><<<cg, dim3(32, 8), 0, st>>>(d, cpp); break;
   }
 }
 

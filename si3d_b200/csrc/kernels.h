@@ -85,16 +85,16 @@ int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st);
 void launch_slayer_h(const Dev& d, cudaStream_t st);
 void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cudaStream_t st);
 void launch_exsal_imsal(const Dev& d, const Tune& tu, cudaStream_t st);
-// exsal's flux kernel on any scalar (tracerpp of one tracer): the persistent Bth2/Bth3/Bth4
-void launch_scalar_flux(const Dev& d, const double* cpp, const Tune& tu, cudaStream_t st);
 // Non-active tracers (k_tracer.cu): exTracer + ImTracer for ntr tracers at once.  Tracer nt
-// (0-based) of a pool is the layer-major field at pool + nt * stride.  `cpp` holds tracerpp,
-// `tr` receives tracer, `cur` holds the tracer values that layers without a solve keep (the tracer
-// pool itself, or tracerpp when the two are known to be equal); `scr` has one km1 x P field per
-// group of kTracerGroup tracers.
+// (0-based) of a pool is the layer-major field at pool + nt * stride.  `cpp` holds tracerpp, `tr`
+// receives tracer; layers without a solve keep the tracer pool's values, or tracerpp's when
+// keep_pp (the two are then equal and the tracer pool is stale).  `fx` holds the face fluxes of
+// the tracers of one flux group but the last tracer (3 min(ntr - 1, kTracerFluxGroup) fields of
+// km1 x P); `scr` one km1 x P field per group of kTracerGroup tracers of the column solve.
 constexpr int kTracerGroup = 8;
-void launch_tracers(const Dev& d, const double* cpp, double* tr, const double* cur, int ntr, long long stride,
-                    double* scr, cudaStream_t st);
+constexpr int kTracerFluxGroup = 4;
+void launch_tracers(const Dev& d, const double* cpp, double* tr, bool keep_pp, int ntr, long long stride,
+                    double* fx, double* scr, cudaStream_t st);
 void launch_vel2(const Dev& d, cudaStream_t st);
 void launch_settrap(const Dev& d, cudaStream_t st);
 void launch_settrap2(const Dev& d, cudaStream_t st);

@@ -140,6 +140,7 @@ struct Ctx {
   bool tr_alias = true, tr_synced = true;
   long long tr_stride = 0;
   double* tr_scr = nullptr;   // elimination factors, one km1 x P field per tracer group
+  double* tr_fx = nullptr;    // face fluxes of one flux group (the last tracer's go to Bth2/3/4)
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
   ~Ctx() {
     if (st) cudaStreamSynchronize(st);
@@ -237,14 +238,11 @@ int tracer_materialise(Ctx* c) {
 }
 
 // fd's tracer block (si3d_procedures.f90:520-544, ecomod = 0): every tracer's right-hand side and
-// column solve, then exsal's flux kernel on the last tracer so that the persistent flux arrays hold
-// what the reference's last exTracer leaves in them.
+// column solve; the persistent flux arrays end as the reference's last exTracer leaves them.
 void tracer_stage(Ctx* c) {
-  const int ntr = c->prm.ntr;
   double* tr = tracer_pool(c, false);
   const double* trpp = tracer_pool(c, true);
-  launch_tracers(c->d, trpp, tr, c->tr_alias ? trpp : tr, ntr, c->tr_stride, c->tr_scr, c->st);
-  launch_scalar_flux(c->d, trpp + (ntr - 1) * c->tr_stride, c->tune, c->st);
+  launch_tracers(c->d, trpp, tr, c->tr_alias, c->prm.ntr, c->tr_stride, c->tr_fx, c->tr_scr, c->st);
   c->tr_alias = false;
 }
 
@@ -794,7 +792,8 @@ int fd_impl(Ctx* c, int istep, bool lastiter, si3d_step_stats* st) {
   rc = stage(c, ST_SLAYER, 1, [&] { launch_slayer_h(d, c->st); });
   if (!rc) rc = stage(c, ST_VEL, 3, [&] { launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st); });
   if (!rc && c->prm.isal != 0) rc = stage(c, ST_SCALAR, 3, [&] { launch_exsal_imsal(d, c->tune, c->st); });
-  if (!rc && c->prm.ntr > 0 && c->prm.niter > 0 && lastiter) rc = stage(c, ST_TRACER, 3, [&] { tracer_stage(c); });
+  if (!rc && c->prm.ntr > 0 && c->prm.niter > 0 && lastiter)
+    rc = stage(c, ST_TRACER, 2 * ((c->prm.ntr + kTracerFluxGroup - 1) / kTracerFluxGroup) + 1, [&] { tracer_stage(c); });
   if (!rc) rc = stage(c, ST_VEL2, 1, [&] { launch_vel2(d, c->st); });
   if (rc) return rc;
   if (st) {
@@ -926,6 +925,7 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
     rc |= c->alloc(&c->tr_buf[0], n3 * prm->ntr);
     rc |= c->alloc(&c->tr_buf[1], n3 * prm->ntr);
     rc |= c->alloc(&c->tr_scr, n3 * ((prm->ntr + kTracerGroup - 1) / kTracerGroup));
+    rc |= c->alloc(&c->tr_fx, n3 * 3 * std::min(std::max(prm->ntr - 1, 1), kTracerFluxGroup));
   }
   rc |= c->alloc(&c->staging, (size_t)km1 * lm1);
   rc |= c->alloc(&c->dz, P);
