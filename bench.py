@@ -380,7 +380,13 @@ def main() -> int:
                                    "achieved": alg / (ms / calls * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                                    "frac": alg / (ms / calls * 1e-3) / 1e9 / peak, "peak_kind": peak_kind}
         dominant = max(stage_ms, key=lambda k: stage_ms[k][0])
-        if dominant in STAGE_STREAMS:
+        if dominant == "tracer":
+            ts = out["tracer_stage"]
+            out["roofline"] = {"bound": "hbm", "achieved": ts["achieved"], "peak": peak, "unit": "GB/s",
+                               "frac": ts["frac"], "traffic": None, "kernel": "tracer",
+                               "algorithmic_bytes_per_call": ts["algorithmic_bytes_per_call"],
+                               "ms_per_call": ts["ms_per_call"], "peak_kind": peak_kind}
+        elif dominant in STAGE_STREAMS:
             streams, unit = STAGE_STREAMS[dominant]
             if dominant == "pcg_iter" and precision == native.SI3D_MIXED_MG:
                 streams = MG_ITER_STREAMS

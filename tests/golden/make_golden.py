@@ -25,15 +25,15 @@ FIELDS_2D = ("s",)
 FIELDS_3D = ("uh", "vh", "sal", "wp")
 
 
-def run_fixture(name: str, steps: int = STEPS, fields_3d=FIELDS_3D):
-    """Oracle state of workload `name` after `steps` steps (plain FP64, red-black MIC-PCG at
-    test 5, 1e-12) plus the per-solve iteration log."""
+def run_fixture(name: str, steps: int = STEPS, fields_3d=FIELDS_3D, ntr: int = 0):
+    """Oracle state of workload `name` (with `ntr` conservative tracers) after `steps` steps (plain
+    FP64, red-black MIC-PCG at test 5, 1e-12) plus the per-solve iteration log."""
     d = os.path.join(tempfile.mkdtemp(), name)
-    synth.make(name, d)
+    synth.make(name, d, ntr=ntr)
     o = pyoracle.OracleRun(d, ordering=1, pcg_itmax=2000)
     o.run(steps)
     out = {f: o.get(f)[:o.lm].copy() for f in FIELDS_2D}
-    for f in fields_3d:
+    for f in tuple(fields_3d) + tuple(f"tracer{t}" for t in range(1, ntr + 1)):
         out[f] = o.get(f)[:, :o.lm].copy()
     sv = o.solves()
     out["iters"] = np.array([s["iters"] for s in sv], dtype=np.int32)
@@ -58,6 +58,8 @@ def main():
     np.savez_compressed(os.path.join(HERE, f"t0_oracle_{STEPS}steps.npz"), **run_fixture("t0"))
     np.savez_compressed(os.path.join(HERE, f"t1_oracle_{STEPS}steps.npz"), **run_fixture("t1", fields_3d=()))
     np.savez_compressed(os.path.join(HERE, "pcg_48x32.npz"), **pcg_fixture())
+    np.savez_compressed(os.path.join(HERE, f"t0_tracers3_oracle_{STEPS}steps.npz"),
+                        **run_fixture("t0", fields_3d=(), ntr=3))
 
 
 if __name__ == "__main__":

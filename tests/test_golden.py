@@ -67,3 +67,29 @@ def test_gpu_standalone_solve_matches_fixture(native_libs):
     assert info["ier"] == 0 and info["stptst"] < 1e-12
     assert abs(info["iters"] - int(g["iters"])) <= 2
     assert np.abs(x - g["x"]).max() <= 1e-9 * np.abs(g["x"]).max()
+
+
+TRACERS = ("tracer1", "tracer2", "tracer3")
+
+
+def test_oracle_reproduces_tracer_fixture(oracle_lib, tracer_dirs):
+    g = _load("t0_tracers3_oracle_10steps.npz")
+    o = oracle_lib.OracleRun(tracer_dirs["t0"], ordering=1, pcg_itmax=2000)
+    o.run(int(g["steps"]))
+    for f in TRACERS:
+        np.testing.assert_allclose(o.get(f)[:, :o.lm], g[f], rtol=1e-12, atol=1e-15)
+
+
+@pytest.mark.gpu
+def test_gpu_matches_tracer_fixture(native_libs, tracer_dirs):
+    """Three conservative tracers after 10 steps on t0, against the stored oracle values."""
+    from si3d_b200.model import GpuRun
+    g = _load("t0_tracers3_oracle_10steps.npz")
+    run = GpuRun(tracer_dirs["t0"], pcg_itmax=2000)
+    try:
+        run.run(int(g["steps"]))
+        assert np.abs(run.get("s")[:run.lm] - g["s"]).max() <= 1e-10
+        for f in TRACERS:
+            assert np.abs(run.get(f)[:, :run.lm] - g[f]).max() <= 1e-9 * np.abs(g[f]).max(), f
+    finally:
+        run.close()
