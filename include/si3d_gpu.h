@@ -173,6 +173,27 @@ int si3d_gpu_solve_zeta(int lm, const double* coeffA, const int* jcoefA, const d
 int si3d_gpu_column_tridiag(int n, int nsys, const double* a, const double* b, const double* c,
                             const double* g, const double* r, double* ag, double* ar);
 
+/* Output frames of the reference's binary writers, packed on the device in the order of the
+ * record the reference writes and converted to 4-byte floats (the default-REAL build the readers
+ * expect); the caller adds the record framing and the time stamp.  Replaces the array packing of
+ * outp (si3d_utils.f90:2484-2602), outz (:2373-2481) and outh (:2142-2334).  kind:
+ *   SI3D_OUT_PTRACK  hp up vp wp salp at every layer k1..kmz+1 of every wet column (first frame:
+ *                    i j k before them)
+ *   SI3D_OUT_TRACER  tracer `arg` (1..ntr) at the same points (first frame: i j k before it)
+ *   SI3D_OUT_PLANE   layer `arg` of every column that reaches it (arg > km: each column's bottom
+ *                    layer): first frame i j u v w salp Av s, later frames face-averaged u v w,
+ *                    salp (-99 where dry), Av, s
+ * first != 0 selects the first frame's layout.  *count receives the number of floats; with host ==
+ * NULL the call only reports it.  SI3D_EDIMS when capacity < count or arg is out of range. */
+#define SI3D_OUT_PTRACK 1
+#define SI3D_OUT_TRACER 2
+#define SI3D_OUT_PLANE 3
+int si3d_gpu_output_frame(int handle, int kind, int arg, int first, float* host, long long capacity, long long* count);
+/* Page-locked host memory for output frames (the device-to-host copy then runs at full link
+ * bandwidth).  Project additions without a reference counterpart. */
+int si3d_gpu_host_alloc(long long bytes, void** ptr);
+int si3d_gpu_host_free(void* ptr);
+
 /* Instrumentation.  si3d_gpu_profile(h, 1) makes every stage record CUDA events on the handle's
  * stream and wait for them (stage boundaries become synchronisation points); counters returns the
  * number of kernels the handle has launched and, per stage, the accumulated device milliseconds

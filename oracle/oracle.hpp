@@ -17,6 +17,8 @@
 // manufactured PCG solutions, dense tridiagonal solves) under tests/.
 #pragma once
 #include <cstdint>
+#include <cstdio>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -64,6 +66,14 @@ struct Inp {
       iTurbVars = 0, nopen = 0, nxNBO = 0, ntr = 0, iopss = 0;
   // tracer block (si3d_utils.f90:172-181), read when ntr > 0
   int ecomod = 0, iotr = 0, itspftr = 0, ipwq = 0, nswq = 0;
+  std::vector<int> p_out;   // output planes (si3d_utils.f90:80-83)
+};
+
+// Calendar of compute_date (si3d_utils.f90:3546-3674); REAL variables as double.
+struct Date {
+  int iyr = 0, imon = 0, iday = 0, ihr = 0, iyrp = 0, imonp = 0, idayp = 0, ihrp = 0;
+  double isec = 0, isecp = 0, isec0 = 0;
+  int month[12] = {31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};   // SAVEd between calls
 };
 
 struct F3 {  // (km1, lm1) column-major, 1-based
@@ -114,6 +124,11 @@ struct Model {
   F3 Bth2, Bth3, Bth4, Bex, Bhaxpp, Bhaypp;
   // non-active tracers (si3d_utils.f90:571-574): tracer and tracerpp per tracer, ntr of each
   std::vector<F3> tracer, tracerpp;
+  // binary output files (outp, outz, outh) written into the run directory, and the date stamp
+  std::string dir;
+  Date date;
+  std::shared_ptr<FILE> f_ptrack;
+  std::vector<std::shared_ptr<FILE>> f_tracer, f_plane;
   // per-column wind override (harness overlay; surfbc CASE 0 otherwise)
   bool wind_override = false;
   std::vector<real> uair_ovr, vair_ovr;  // l-indexed (1..lm)
@@ -127,6 +142,8 @@ struct Model {
 
 // I/O and setup
 bool read_inputs(Model& m, const std::string& dir);  // input + ZGridDimensions + bathy + init
+void compute_date(Model& m, double itime_sec);
+bool write_outputs(Model& m, int n);   // outh, outz, outp as the time loop calls them for step n
 // time loop
 bool run_steps(Model& m, int nsteps);
 // one routine (momentum, matcon, solve, vel, scalar, vel2, fd, settrap, settrap2, save)

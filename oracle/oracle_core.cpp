@@ -1068,12 +1068,13 @@ bool run_stage(Model& m, const std::string& stage, int istep) {
   return true;
 }
 
-// Time loop si3d.f90:324-458 (outputs and logs omitted).
+// Time loop si3d.f90:324-458 (logs omitted; the binary outputs outh, outz and outp are written).
 bool run_steps(Model& m, int nsteps) {
   ExCoef C;
   C.haxpp.init(m.km1, m.lm1); C.haypp.init(m.km1, m.lm1); C.th.init(m.km1, m.lm1); C.th1.init(m.km1, m.lm1);
   for (int s = 0; s < nsteps; ++s) {
     m.n += 1;
+    compute_date(m, m.in.idt);   // si3d.f90:333
     int niter1 = m.in.niter;
     m.lastiter = 0;
     bool first = (m.n == 1);
@@ -1083,7 +1084,11 @@ bool run_steps(Model& m, int nsteps) {
       m.iter = 0;
       if (m.in.itrap == 0 || (m.n % std::max(m.in.itrap, 1)) != 0) m.lastiter = 1;
       if (!fd(m, C)) { m.failed = true; return false; }
-      if (m.in.itrap == 0 || (m.n % std::max(m.in.itrap, 1)) != 0) { save(m, m.istep); continue; }
+      if (m.in.itrap == 0 || (m.n % std::max(m.in.itrap, 1)) != 0) {
+        save(m, m.istep);
+        if (!write_outputs(m, m.n)) { m.failed = true; return false; }
+        continue;
+      }
       settrap(m);
     }
     m.istep = 2;
@@ -1095,6 +1100,7 @@ bool run_steps(Model& m, int nsteps) {
       if (it > 20) break;
     }
     save(m, m.istep);
+    if (!write_outputs(m, m.n)) { m.failed = true; return false; }
   }
   return true;
 }

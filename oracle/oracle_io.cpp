@@ -5,8 +5,10 @@
 // (:184-379, InitProc = 4 file branch), `InitializeTurbulenceModel` CASE(0)
 // (si3d_mixing.f90:650-671).  The readers follow the reference's fixed-column record
 // formats; only the records the hot-path configuration uses are interpreted.
+#include <cctype>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <sstream>
@@ -95,10 +97,23 @@ static bool read_inp(Model& m, const std::string& dir) {
   L.skip(3); ok &= rec_i(L, p.ipt); ok &= rec_i(L, p.nnodes);        // :56-69
   L.skip(2);                                                          // node lists or '(/)'
   L.skip(3); ok &= rec_i(L, p.iop); ok &= rec_i(L, p.itspfh); ok &= rec_i(L, p.n_planes);
-  L.skip(1);                                                          // planes record
+  {                                                                   // planes '(14X,20I)'
+    const std::string rec = field(L.next(), 14, 1000);
+    p.p_out.clear();
+    size_t i = 0;
+    while ((int)p.p_out.size() < p.n_planes) {
+      while (i < rec.size() && (rec[i] == ' ' || rec[i] == ',' || rec[i] == '\t')) ++i;
+      size_t j = i;
+      while (j < rec.size() && (std::isdigit((unsigned char)rec[j]) || rec[j] == '-')) ++j;
+      if (j == i) { m.err = "si3d_inp.txt: bad output plane list"; return false; }
+      p.p_out.push_back(std::atoi(rec.substr(i, j - i).c_str()));
+      i = j;
+    }
+  }
   L.skip(3); ok &= rec_i(L, p.iox);                                   // :91-93
   if (p.iox != 0) { m.err = "si3d_inp.txt: cross-section output (iox/=0) is not supported"; return false; }
   L.skip(3); ok &= rec_i(L, p.ipxml); ok &= rec_i(L, p.itspf); ok &= rec_i(L, p.iTurbVars);
+  if (p.ipxml > 0 && p.iTurbVars != 0) { m.err = "turbulence variables in the 3-D output need iturb > 0"; return false; }
   L.skip(3); ok &= rec_i(L, p.nopen);                                 // :125-145
   if (p.nopen != 0) { m.err = "open boundaries (nopen>0) are outside the hot path"; return false; }
   L.skip(7);
@@ -352,13 +367,16 @@ static void init_state(Model& m, const std::vector<real>& prof) {
 }
 
 bool read_inputs(Model& m, const std::string& dir) {
+  m.dir = dir;
   if (!read_inp(m, dir)) return false;
+  m.date.isec0 = (double)m.in.ihr0 / 100. * 3600.;   // si3d_utils.f90:310
+  compute_date(m, 0.0);                               // :43
   if (!read_bathy(m, dir)) return false;
   std::vector<real> prof;
   if (!read_init_profile(m, dir, prof)) return false;
   if (!read_wind_override(m, dir)) return false;
   init_state(m, prof);
-  return true;
+  return write_outputs(m, 0);   // initial frames (si3d.f90:89-100)
 }
 
 }  // namespace orc

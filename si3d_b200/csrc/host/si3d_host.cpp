@@ -8,7 +8,9 @@
 // (:781-806), kmz/hhs/hhu/hhv (:812-880), `init` (si3d_procedures.f90:23-181) and
 // InitializeTurbulenceModel CASE(0) (si3d_mixing.f90:650-671).
 #include <algorithm>
+#include <cctype>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
@@ -69,6 +71,21 @@ struct HostModel {
   // initial state
   std::vector<double> s0, hp0, hup0, hvp0, salp0, Av0f, Dv0f, uair, vair, cdw;
   std::vector<double> tracer0;   // ntr fields of (km1, lm1), column-major
+  // outputs (si3d_utils.f90:72-121, :172-181) and the date of compute_date (:3546-3674)
+  int iyr0 = 0, imon0 = 0, iday0 = 0, ihr0 = 0;
+  int iop = 0, itspfh = 0, n_planes = 0, ipxml = 0, itspf = 0, iTurbVars = 0, iotr = 0, itspftr = 0;
+  std::vector<int> p_out;
+  struct Date {
+    int iyr = 0, imon = 0, iday = 0, ihr = 0, iyrp = 0, imonp = 0, idayp = 0, ihrp = 0;
+    double isec = 0, isecp = 0, isec0 = 0;
+    int month[12] = {31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
+  } date;
+  std::string dir;
+  std::shared_ptr<FILE> f_ptrack;
+  std::vector<std::shared_ptr<FILE>> f_tracer, f_plane;
+  float* frame = nullptr;   // page-locked frame buffer
+  long long frame_cap = 0;
+  ~HostModel() { if (frame) si3d_gpu_host_free(frame); }
   std::vector<int> k1z0, k1u0, k1v0;
   // run
   int gpu = -1, n = 0;
@@ -94,7 +111,7 @@ bool read_parameters(HostModel& M, const std::string& dir) {
   auto gi = [&](int& v) { double x = 0; ok = ok && numeric(R.take(), 14, 20, x); v = (int)std::lround(x); };
   int dummy = 0;
   R.skip(2);                                     // title block
-  R.skip(3); gi(dummy); gi(dummy); gi(dummy); gi(dummy);
+  R.skip(3); gi(M.iyr0); gi(M.imon0); gi(M.iday0); gi(M.ihr0);
   R.skip(3);
   g(M.xl); g(M.yl); g(M.zl); g(M.tl); g(M.idx); g(M.idy); g(M.idz); g(M.dzmin); g(M.datadj); g(M.zetainit);
   g(M.idt); gi(M.ibathyf);
@@ -103,13 +120,26 @@ bool read_parameters(HostModel& M, const std::string& dir) {
   gi(M.ihd); g(M.Ax0); g(M.Ay0); g(M.f); g(M.theta); gi(M.ibc); gi(M.isal); gi(M.itrsca); g(M.cd); gi(M.ifsurfbc);
   g(M.dtsurfbc); gi(M.icw); g(M.cw); g(M.wa); g(M.phi); gi(dummy); gi(dummy);
   R.skip(3); gi(dummy); gi(dummy); R.skip(2);    // ipt, nnodes, node lists
-  R.skip(3); gi(dummy); gi(dummy); gi(dummy); R.skip(1);   // iop, itspfh, n_planes, planes
+  R.skip(3); gi(M.iop); gi(M.itspfh); gi(M.n_planes);
+  {   // planes '(14X,20I)'
+    const std::string rec = R.take();
+    M.p_out.clear();
+    size_t i = 14;
+    while ((int)M.p_out.size() < M.n_planes) {
+      while (i < rec.size() && (rec[i] == ' ' || rec[i] == ',' || rec[i] == '\t')) ++i;
+      size_t j = i;
+      while (j < rec.size() && (std::isdigit((unsigned char)rec[j]) || rec[j] == '-')) ++j;
+      if (j == i) { M.err = "si3d_inp.txt: bad output plane list"; return false; }
+      M.p_out.push_back(std::atoi(rec.substr(i, j - i).c_str()));
+      i = j;
+    }
+  }
   R.skip(3); gi(M.iox);
-  R.skip(3); gi(dummy); gi(dummy); gi(dummy);    // ipxml, itspf, iTurbVars
+  R.skip(3); gi(M.ipxml); gi(M.itspf); gi(M.iTurbVars);
   R.skip(3); gi(M.nopen); R.skip(7);
   R.skip(3); gi(M.nxNBO); R.skip(7);
   R.skip(3); gi(M.ntr);                          // tracer block (si3d_utils.f90:172-190)
-  if (M.ntr > 0) { gi(M.ecomod); gi(dummy); gi(dummy); gi(dummy); gi(dummy); }   // iotr itspftr ipwq nswq
+  if (M.ntr > 0) { gi(M.ecomod); gi(M.iotr); gi(M.itspftr); gi(dummy); gi(dummy); }   // ipwq nswq unused
   else R.skip(5);
   R.skip(3); gi(M.iopss);
   if (!ok) { M.err = "si3d_inp.txt: unreadable record"; return false; }
@@ -118,6 +148,10 @@ bool read_parameters(HostModel& M, const std::string& dir) {
     M.err = "si3d_inp.txt selects an option outside the semi-implicit core (open boundaries, point "
             "sources, heat budget, turbulence closure, Smagorinsky, smoothing, non-centred advection or "
             "variable layers)";
+    return false;
+  }
+  if (M.ipxml > 0 && M.iTurbVars != 0) {
+    M.err = "si3d_inp.txt: turbulence variables in the 3-D output need a turbulence closure (iturb > 0)";
     return false;
   }
   if (M.ntr < 0 || M.ntr > 30 || (M.ntr > 0 && M.ecomod != 0)) {
@@ -303,6 +337,143 @@ void initial_state(HostModel& M, const std::vector<double>& prof) {
   }
 }
 
+
+// compute_date (si3d_utils.f90:3546-3674): REAL variables as double, NINT rounding half away from
+// zero, the month table kept between calls as the reference's SAVEd local.
+void compute_date(HostModel& M, double itime_sec) {
+  HostModel::Date& D = M.date;
+  auto leap = [](int y) { return y % 4 == 0; };
+  if (itime_sec == 0) {
+    D.iyrp = M.iyr0; D.imonp = M.imon0; D.idayp = M.iday0; D.ihrp = M.ihr0; D.isecp = D.isec0;
+    D.iyr = M.iyr0; D.imon = M.imon0; D.iday = M.iday0; D.ihr = M.ihr0; D.isec = D.isec0;
+    if (leap(D.iyrp)) D.month[1] = 29;
+    return;
+  }
+  D.isecp += itime_sec;
+  if (D.isecp < 86400) {
+    D.isec = D.isecp;
+    D.ihrp = (int)std::lround(D.isec / 3600. * 100.);
+    D.ihr = D.ihrp;
+    return;
+  }
+  D.idayp = (int)(D.idayp + D.isecp / 86400);
+  D.isecp = std::fmod(D.isecp, 86400.);
+  D.isec = D.isecp;
+  D.ihrp = (int)std::lround(D.isec / 3600. * 100.);
+  D.ihr = D.ihrp;
+  if (D.imonp == 2) D.month[1] = leap(D.iyrp) ? 29 : 28;
+  if (D.idayp <= D.month[D.imonp - 1]) {
+    D.iday = D.idayp;
+    return;
+  }
+  const int months = (int)(itime_sec / 2500000 + 1);
+  for (int j = 1; j <= months; ++j) {
+    D.idayp -= D.month[D.imonp - 1];
+    if (++D.imonp == 13) {
+      D.imonp = 1;
+      ++D.iyrp;
+      D.month[1] = leap(D.iyrp) ? 29 : 28;
+    }
+    if (D.idayp <= D.month[D.imonp - 1]) {
+      D.iday = D.idayp;
+      break;
+    }
+  }
+  D.imon = D.imonp;
+  D.iyr = D.iyrp;
+}
+
+// Fortran unformatted sequential record: byte length, payload, byte length (4-byte integers).
+bool put_record(HostModel& M, FILE* f, const void* head, size_t nh, const void* body, size_t nb) {
+  const int32_t len = (int32_t)(nh + nb);
+  bool ok = std::fwrite(&len, 4, 1, f) == 1 && (nh == 0 || std::fwrite(head, 1, nh, f) == nh) &&
+            (nb == 0 || std::fwrite(body, 1, nb, f) == nb) && std::fwrite(&len, 4, 1, f) == 1;
+  ok = ok && std::fflush(f) == 0;
+  if (!ok) M.err = "output: write failed";
+  return ok;
+}
+
+std::shared_ptr<FILE> open_output(HostModel& M, const std::string& name) {
+  FILE* f = std::fopen((M.dir + "/" + name).c_str(), "wb");
+  if (!f) { M.err = "output: cannot open " + name; return nullptr; }
+  return std::shared_ptr<FILE>(f, [](FILE* q) { std::fclose(q); });
+}
+
+bool header_records(HostModel& M, FILE* f, int frames, long long points) {
+  const int32_t a = frames, b = (int32_t)points;
+  return put_record(M, f, &a, 4, nullptr, 0) && put_record(M, f, &b, 4, nullptr, 0);
+}
+
+// One frame: pack on the device into the page-locked buffer, then the record with the time stamp
+// n, year, month, day, hour (si3d_utils.f90:2540-2541).
+int frame_record(HostModel& M, FILE* f, int n, int kind, int arg) {
+  long long cnt = 0;
+  int rc = si3d_gpu_output_frame(M.gpu, kind, arg, n == 0, nullptr, 0, &cnt);
+  if (rc) return rc;
+  if (cnt > M.frame_cap) {
+    if (M.frame) si3d_gpu_host_free(M.frame);
+    M.frame = nullptr;
+    M.frame_cap = 0;
+    void* p = nullptr;
+    if ((rc = si3d_gpu_host_alloc(std::max<long long>(cnt, 1) * 4, &p))) return rc;
+    M.frame = static_cast<float*>(p);
+    M.frame_cap = cnt;
+  }
+  if ((rc = si3d_gpu_output_frame(M.gpu, kind, arg, n == 0, M.frame, M.frame_cap, &cnt))) return rc;
+  unsigned char head[20];
+  const int32_t iv[4] = {n, M.date.iyr, M.date.imon, M.date.iday};
+  const float hour = (float)M.date.ihr;
+  std::memcpy(head, iv, 16);
+  std::memcpy(head + 16, &hour, 4);
+  return put_record(M, f, head, 20, M.frame, (size_t)cnt * 4) ? 0 : SI3D_EDIMS;
+}
+
+// The output calls of the time loop (si3d.f90:430-438; with n = 0 the initial ones, :89-100):
+// outh (planes), outz (tracers), outp (ptrack file).  Files go to the run directory.
+int write_outputs(HostModel& M, int n) {
+  int rc = 0;
+  const int apxml = std::abs(M.ipxml);
+  if (M.iop > 0 && (n == 0 || (n >= M.itspfh && n % std::max(M.iop, 1) == 0))) {
+    if (n == 0) {
+      M.f_plane.clear();
+      for (int kp : M.p_out) {
+        if (kp < M.k1) { M.err = "output plane is not in the domain"; return SI3D_EDIMS; }
+        auto f = open_output(M, "plane_" + std::to_string(kp));
+        long long cnt = 0;
+        if (!f) return SI3D_EDIMS;
+        if ((rc = si3d_gpu_output_frame(M.gpu, SI3D_OUT_PLANE, kp, 1, nullptr, 0, &cnt))) return rc;
+        if (!header_records(M, f.get(), (M.nts - M.itspfh) / std::max(M.iop, 1), cnt / 8)) return SI3D_EDIMS;
+        M.f_plane.push_back(f);
+      }
+    }
+    for (size_t j = 0; j < M.p_out.size(); ++j)
+      if ((rc = frame_record(M, M.f_plane[j].get(), n, SI3D_OUT_PLANE, M.p_out[j]))) return rc;
+  }
+  long long pts = 0;
+  for (int l = 0; l < M.lm; ++l) pts += M.kmz[l] + 2 - M.k1;
+  if (M.iotr > 0 && M.ntr > 0 && (n == 0 || n % std::max(M.iotr, 1) == 0)) {
+    if (n == 0) {
+      M.f_tracer.clear();
+      for (int t = 1; t <= M.ntr; ++t) {
+        auto f = open_output(M, "tracer_" + std::to_string(t));
+        if (!f || !header_records(M, f.get(), (M.nts - M.itspftr) / std::max(M.iotr, 1), pts)) return SI3D_EDIMS;
+        M.f_tracer.push_back(f);
+      }
+    }
+    for (int t = 1; t <= M.ntr; ++t)
+      if ((rc = frame_record(M, M.f_tracer[t - 1].get(), n, SI3D_OUT_TRACER, t))) return rc;
+  }
+  if (M.ipxml > 0 && (n == 0 || (n >= M.itspf && n % std::max(apxml, 1) == 0))) {
+    if (n == 0) {
+      M.f_ptrack = open_output(M, "si3d_3D");
+      if (!M.f_ptrack || !header_records(M, M.f_ptrack.get(), (M.nts - M.itspf) / std::max(apxml, 1), pts))
+        return SI3D_EDIMS;
+    }
+    if ((rc = frame_record(M, M.f_ptrack.get(), n, SI3D_OUT_PTRACK, 0))) return rc;
+  }
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -319,6 +490,9 @@ int si3d_host_open(const char* run_dir, const si3d_solver_opts* opts, int* hm, c
     return SI3D_EDIMS;
   }
   initial_state(*M, prof);
+  M->dir = dir;
+  M->date.isec0 = (double)M->ihr0 / 100. * 3600.;   // si3d_utils.f90:310
+  compute_date(*M, 0.0);                              // :43
   std::lock_guard<std::mutex> lk(g_mu);
   g_models.push_back(std::move(M));
   *hm = (int)g_models.size() - 1;
@@ -401,6 +575,7 @@ int si3d_host_attach_gpu(int h, int device, int* gpu_handle) {
   if ((rc = si3d_gpu_density(gh))) return rc;   // rhop from the initial profile (:363-373)
   M->gpu = gh;
   M->n = 0;
+  if ((rc = write_outputs(*M, 0))) return rc;   // the initial frames (si3d.f90:89-100)
   if (gpu_handle) *gpu_handle = gh;
   return 0;
 }
@@ -411,9 +586,11 @@ int si3d_host_run(int h, int nsteps, si3d_step_stats* stats) {
   if (M->gpu < 0) return SI3D_EHANDLE;
   for (int s = 0; s < nsteps; ++s) {
     const int n = M->n + 1;
-    const int rc = si3d_gpu_step(M->gpu, n, stats ? &stats[s] : nullptr);
+    compute_date(*M, M->idt);   // si3d.f90:333
+    int rc = si3d_gpu_step(M->gpu, n, stats ? &stats[s] : nullptr);
     if (rc) return rc;
     M->n = n;
+    if ((rc = write_outputs(*M, n))) return rc;
   }
   return 0;
 }

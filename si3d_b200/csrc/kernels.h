@@ -102,6 +102,14 @@ void launch_save(const Dev& d, int istep, cudaStream_t st);
 
 void launch_density_init(const Dev& d, cudaStream_t st);
 
+// Output frames (k_output.cu): nf fields (layer-major FP64) at every point k1..kmz(l) + 1 of every
+// wet column, point offsets poff (lm + 1 entries), optionally preceded by the coordinates i, j, k,
+// as 4-byte floats into `out`; and one horizontal plane's frame over its column list.
+void launch_pack_points(const Dev& d, const double* const* fields, int nf, const int* poff, const int* l2i,
+                        const int* l2j, bool coords, float* out, cudaStream_t st);
+void launch_pack_plane(const Dev& d, const int* cols, int n, int kp, bool first, const int* l2i, const int* l2j,
+                       float* out, cudaStream_t st);
+
 void launch_column_tridiag(int n, int nsys, const double* a, const double* b, const double* c, const double* g,
                            const double* r, double* ag, double* ar, double* scratch, cudaStream_t st);
 

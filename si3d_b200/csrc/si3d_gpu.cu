@@ -141,6 +141,14 @@ struct Ctx {
   long long tr_stride = 0;
   double* tr_scr = nullptr;   // elimination factors, one km1 x P field per tracer group
   double* tr_fx = nullptr;    // face fluxes of one flux group (the last tracer's go to Bth2/3/4)
+  // output frames: column coordinates, point offsets of the 3-D frames, a device frame buffer and
+  // the column list of each output plane requested so far
+  int *d_l2i = nullptr, *d_l2j = nullptr, *poff = nullptr;
+  long long npoints = 0;
+  float* out_buf = nullptr;
+  long long out_cap = 0;
+  std::map<int, std::pair<int*, int>> planes;
+  std::vector<int> h_kmz;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
   ~Ctx() {
     if (st) cudaStreamSynchronize(st);
@@ -920,6 +928,20 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
     rc |= c->alloc(q, P);
   for (int** q : {&s.k1z, &s.k1u, &s.k1v}) rc |= c->alloc(q, P);
   rc |= c->alloc(&d.scr, n3);
+  {   // output frames: coordinates and point offsets (k1 .. kmz + 1 per wet column)
+    std::vector<int> off(lm + 1, 0);
+    c->h_kmz.assign(g->kmz, g->kmz + lm);
+    for (int l = 0; l < lm; ++l) off[l + 1] = off[l] + (g->kmz[l] + 2 - g->k1);
+    c->npoints = off[lm];
+    rc |= c->alloc(&c->poff, lm + 1);
+    rc |= c->alloc(&c->d_l2i, lm);
+    rc |= c->alloc(&c->d_l2j, lm);
+    if (!rc) {
+      cudaMemcpy(c->poff, off.data(), sizeof(int) * (lm + 1), cudaMemcpyHostToDevice);
+      cudaMemcpy(c->d_l2i, g->l2i, sizeof(int) * lm, cudaMemcpyHostToDevice);
+      cudaMemcpy(c->d_l2j, g->l2j, sizeof(int) * lm, cudaMemcpyHostToDevice);
+    }
+  }
   if (prm->ntr > 0) {
     c->tr_stride = (long long)n3;
     rc |= c->alloc(&c->tr_buf[0], n3 * prm->ntr);
@@ -1583,6 +1605,78 @@ int si3d_gpu_profile(int h, int enable) {
   if (!c) return SI3D_EHANDLE;
   c->prof = enable != 0;
   for (int i = 0; i < 16; ++i) { c->prof_ms[i] = 0; c->prof_n[i] = 0; }
+  return 0;
+}
+
+int si3d_gpu_output_frame(int h, int kind, int arg, int first, float* host, long long capacity, long long* count) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (!count) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  Dev& d = c->d;
+  const double* fields[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  int nf = 0;
+  std::pair<int*, int> plane{nullptr, 0};
+  long long n = 0;
+  switch (kind) {
+    case SI3D_OUT_PTRACK:
+      fields[0] = d.f.hp; fields[1] = d.f.up; fields[2] = d.f.vp; fields[3] = d.f.wp; fields[4] = d.f.salp;
+      nf = 5;
+      n = c->npoints * (nf + (first ? 3 : 0));
+      break;
+    case SI3D_OUT_TRACER:
+      if (arg < 1 || arg > c->prm.ntr) return SI3D_EDIMS;
+      fields[0] = tracer_pool(c, c->tr_alias) + (arg - 1) * c->tr_stride;
+      nf = 1;
+      n = c->npoints * (nf + (first ? 3 : 0));
+      break;
+    case SI3D_OUT_PLANE: {
+      if (arg < d.g.k1) return SI3D_EDIMS;   // "Output plane is not in DOMAIN" (si3d_utils.f90:2165)
+      auto it = c->planes.find(arg);
+      if (it == c->planes.end()) {   // CountPlaneCells (:2337-2368): kmz >= kp, or every column
+        std::vector<int> cols;
+        for (int l = 1; l <= c->lm; ++l)
+          if (arg > d.g.km || c->h_kmz[l - 1] >= arg) cols.push_back(l);
+        int* dc = nullptr;
+        if (c->alloc(&dc, cols.size())) return SI3D_ENOMEM;
+        if (!cols.empty()) CK(cudaMemcpy(dc, cols.data(), sizeof(int) * cols.size(), cudaMemcpyHostToDevice));
+        it = c->planes.emplace(arg, std::make_pair(dc, (int)cols.size())).first;
+      }
+      plane = it->second;
+      n = (long long)plane.second * (first ? 8 : 6);
+      break;
+    }
+    default: return SI3D_EDIMS;
+  }
+  *count = n;
+  if (!host) return 0;   // size query
+  if (capacity < n) return SI3D_EDIMS;
+  if (!c->out_buf) {   // the largest frame: the first ptrack frame, or a plane's
+    c->out_cap = std::max(c->npoints * 8, (long long)c->lm * 8);
+    if (c->alloc(&c->out_buf, c->out_cap)) return SI3D_ENOMEM;
+  }
+  if (n > c->out_cap) return SI3D_EDIMS;
+  if (kind == SI3D_OUT_PLANE)
+    launch_pack_plane(d, plane.first, plane.second, arg, first != 0, c->d_l2i, c->d_l2j, c->out_buf, c->st);
+  else
+    launch_pack_points(d, fields, nf, c->poff, c->d_l2i, c->d_l2j, first != 0, c->out_buf, c->st);
+  c->launches += 1;
+  CK(cudaGetLastError());
+  if (n > 0) CK(cudaMemcpyAsync(host, c->out_buf, sizeof(float) * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_host_alloc(long long bytes, void** ptr) {
+  if (!ptr || bytes <= 0) return SI3D_EDIMS;
+  *ptr = nullptr;
+  const cudaError_t e = cudaMallocHost(ptr, (size_t)bytes);
+  if (e != cudaSuccess) { g_last_cuda = cudaGetErrorString(e); *ptr = nullptr; return SI3D_ENOMEM; }
+  return 0;
+}
+
+int si3d_gpu_host_free(void* ptr) {
+  if (ptr && cudaFreeHost(ptr) != cudaSuccess) return SI3D_ECUDA;
   return 0;
 }
 

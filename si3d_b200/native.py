@@ -25,6 +25,9 @@ class Si3dError(RuntimeError):
         self.code = code
 
 
+SI3D_OUT_PTRACK, SI3D_OUT_TRACER, SI3D_OUT_PLANE = 1, 2, 3
+
+
 class Grid(C.Structure):
     _fields_ = [("im1", C.c_int), ("jm1", C.c_int), ("km1", C.c_int), ("k1", C.c_int), ("lm", C.c_int),
                 ("l2i", C.POINTER(C.c_int)), ("l2j", C.POINTER(C.c_int)), ("lEC", C.POINTER(C.c_int)),
@@ -74,6 +77,10 @@ GPU_SYMBOLS = {
     "si3d_gpu_column_tridiag_noalloc": (C.c_int, [C.c_int, C.c_int] + [C.c_void_p] * 8),
     "si3d_gpu_profile": (C.c_int, [C.c_int, C.c_int]),
     "si3d_gpu_counters": (C.c_int, [C.c_int, C.POINTER(C.c_longlong), C.c_void_p, C.c_void_p]),
+    "si3d_gpu_output_frame": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_longlong,
+                                        C.POINTER(C.c_longlong)]),
+    "si3d_gpu_host_alloc": (C.c_int, [C.c_longlong, C.POINTER(C.c_void_p)]),
+    "si3d_gpu_host_free": (C.c_int, [C.c_void_p]),
     "si3d_gpu_sync": (C.c_int, [C.c_int]),
     "si3d_gpu_strerror": (C.c_char_p, [C.c_int]),
     "si3d_gpu_finalize": (None, [C.c_int]),

@@ -58,6 +58,15 @@ class Basin:
     niter: int = 2
     ibc: int = 1                 # baroclinic pressure term on/off
     ntr: int = 0                 # non-active (conservative) tracers, ecomod = 0
+    # binary outputs: H-planes every iop steps from itspfh (outh), tracers every iotr steps (outz),
+    # the 3-D ptrack file every ipxml steps from itspf (outp); 0 = off
+    iop: int = 0
+    itspfh: int = 0
+    planes: tuple = ()
+    ipxml: int = 0
+    itspf: int = 0
+    iotr: int = 0
+    itspftr: int = 0
     seeds: dict = dataclasses.field(default_factory=dict)
 
     @property
@@ -168,17 +177,17 @@ def write_inp(b: Basin, path: str) -> None:
         L.append(_rec(lab, val))
     L += [sep, "Output specifications for time files", sep, _rec("ipt", 0), _rec("nnodes", 0),
           _rec("inodes", 0), _rec("jnodes", 0)]
-    L += [sep, "Output specifications for H-plane files", sep, _rec("iop", 0), _rec("itspfh", 0),
-          _rec("nplanes", 0), _rec("planes", 0)]
+    L += [sep, "Output specifications for H-plane files", sep, _rec("iop", b.iop), _rec("itspfh", b.itspfh),
+          _rec("nplanes", len(b.planes)), _rec("planes", " ".join(str(k) for k in b.planes) or 0)]
     L += [sep, "Output specifications for X-section files", sep, _rec("ixt", 0)]
-    L += [sep, "Output specifications for 3D space files", sep, _rec("ipxml", 0), _rec("itspf", 0),
+    L += [sep, "Output specifications for 3D space files", sep, _rec("ipxml", b.ipxml), _rec("itspf", b.itspf),
           _rec("iTurbVars", 0)]
     L += [sep, "Open boundary conditions specifications", sep, _rec("nopen", 0), _rec("dtopenbc", 360.0)]
     L += [_rec(x, 0) for x in ("iside", "itype", "isbc", "jsbc", "iebc", "jebc")]
     L += [sep, "Open boundary conditions for nesting procedures", sep, _rec("nxBDO", 0)]
     L += [_rec(x, 0) for x in ("iob", "xxb", "iside", "isbc", "jsbc", "iebc", "jebc")]
     L += [sep, "Specification for tracer simulation", sep, _rec("ntr", b.ntr)]
-    L += [_rec(x, 0) for x in ("ecomod", "iotr", "itspftr", "ipwq", "nswq")]
+    L += [_rec("ecomod", 0), _rec("iotr", b.iotr), _rec("itspftr", b.itspftr), _rec("ipwq", 0), _rec("nswq", 0)]
     L += [sep, "Specification for oxygenation system simulations", sep, _rec("iopts", 0)]
     L += [_rec(x, 0) for x in ("Nodev", "iodt", "ipss", "jpss", "iodev")]
     with open(path, "w") as fh:
@@ -268,8 +277,13 @@ def write_run(b: Basin, run_dir: str) -> str:
     return run_dir
 
 
-def make(name: str, run_dir: str, nsteps: Optional[int] = None, seed_offset: int = 0, ntr: int = 0) -> Basin:
+def make(name: str, run_dir: str, nsteps: Optional[int] = None, seed_offset: int = 0, ntr: int = 0,
+         outputs: Optional[dict] = None) -> Basin:
+    """Write workload `name` into run_dir; `outputs` sets the output records (iop, itspfh, planes,
+    ipxml, itspf, iotr, itspftr)."""
     b = config(name, nsteps, seed_offset)
     b.ntr = ntr
+    for k, v in (outputs or {}).items():
+        setattr(b, k, v)
     write_run(b, run_dir)
     return b
