@@ -189,6 +189,14 @@ int si3d_gpu_column_tridiag(int n, int nsys, const double* a, const double* b, c
 #define SI3D_OUT_TRACER 2
 #define SI3D_OUT_PLANE 3
 int si3d_gpu_output_frame(int handle, int kind, int arg, int first, float* host, long long capacity, long long* count);
+/* The same without waiting: the frame is packed on the handle's stream (in order with the time
+ * steps) and copied to `host` (page-locked) on a separate copy stream, overlapping the steps that
+ * follow; *ticket identifies the copy, and si3d_gpu_output_wait(handle, ticket) returns once it has
+ * landed.  At most 16 copies may be in flight per handle.  Project additions without a reference
+ * counterpart. */
+int si3d_gpu_output_frame_async(int handle, int kind, int arg, int first, float* host, long long capacity,
+                                long long* count, unsigned long long* ticket);
+int si3d_gpu_output_wait(int handle, unsigned long long ticket);
 /* Page-locked host memory for output frames (the device-to-host copy then runs at full link
  * bandwidth).  Project additions without a reference counterpart. */
 int si3d_gpu_host_alloc(long long bytes, void** ptr);

@@ -38,10 +38,14 @@ int si3d_host_dims(int hm, int* dims);
 int si3d_host_get_map(int hm, const char* name, int* out);
 /* zlevel (km1 entries). */
 int si3d_host_get_zlevel(int hm, double* out);
-/* Create the GPU state (si3d_gpu_init) and upload the initial fields. */
+/* Create the GPU state (si3d_gpu_init), upload the initial fields and write the initial output
+ * frames (si3d.f90:89-100). */
 int si3d_host_attach_gpu(int hm, int device, int* gpu_handle);
 /* Run `nsteps` time steps from the current step counter; per-step stats (optional, nsteps
- * entries). */
+ * entries).  The binary outputs the input file selects (outh planes, outz tracers, outp ptrack
+ * file: si3d.f90:430-438) are written into the run directory: frames are packed on the device and
+ * copied asynchronously, and a writer thread writes the records while the next steps run; every
+ * record is in its file when the call returns. */
 int si3d_host_run(int hm, int nsteps, si3d_step_stats* stats);
 /* Current time-step counter n. */
 int si3d_host_step_count(int hm);

@@ -14,8 +14,11 @@
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <condition_variable>
+#include <deque>
 #include <memory>
 #include <mutex>
+#include <thread>
 #include <string>
 #include <vector>
 
@@ -83,9 +86,32 @@ struct HostModel {
   std::string dir;
   std::shared_ptr<FILE> f_ptrack;
   std::vector<std::shared_ptr<FILE>> f_tracer, f_plane;
-  float* frame = nullptr;   // page-locked frame buffer
-  long long frame_cap = 0;
-  ~HostModel() { if (frame) si3d_gpu_host_free(frame); }
+  // frame writer: the main thread packs frames into page-locked buffers (asynchronous copies); a
+  // writer thread waits for each copy and writes its record, so file output overlaps the steps
+  struct Buf { float* p = nullptr; long long cap = 0; };
+  struct Job {
+    std::shared_ptr<FILE> f;
+    std::vector<unsigned char> head;   // record bytes before the frame (or the whole record)
+    Buf buf;
+    long long count = 0;
+    unsigned long long ticket = 0;
+  };
+  std::mutex wmu;
+  std::condition_variable wcv;
+  std::deque<Job> jobs;
+  std::vector<Buf> free_bufs;
+  int in_flight = 0;               // frames queued or being written
+  bool stop = false;
+  int werr = 0;                    // first writer error
+  std::thread writer;
+  ~HostModel() {
+    if (writer.joinable()) {
+      { std::lock_guard<std::mutex> lk(wmu); stop = true; }
+      wcv.notify_all();
+      writer.join();
+    }
+    for (Buf& b : free_bufs) si3d_gpu_host_free(b.p);
+  }
   std::vector<int> k1z0, k1u0, k1v0;
   // run
   int gpu = -1, n = 0;
@@ -399,33 +425,95 @@ std::shared_ptr<FILE> open_output(HostModel& M, const std::string& name) {
   return std::shared_ptr<FILE>(f, [](FILE* q) { std::fclose(q); });
 }
 
-bool header_records(HostModel& M, FILE* f, int frames, long long points) {
-  const int32_t a = frames, b = (int32_t)points;
-  return put_record(M, f, &a, 4, nullptr, 0) && put_record(M, f, &b, 4, nullptr, 0);
+constexpr int kMaxFramesInFlight = 4;
+
+void writer_loop(HostModel* M) {
+  for (;;) {
+    HostModel::Job j;
+    {
+      std::unique_lock<std::mutex> lk(M->wmu);
+      M->wcv.wait(lk, [&] { return M->stop || !M->jobs.empty(); });
+      if (M->jobs.empty()) return;
+      j = std::move(M->jobs.front());
+      M->jobs.pop_front();
+    }
+    int rc = j.ticket ? si3d_gpu_output_wait(M->gpu, j.ticket) : 0;
+    if (!rc && !put_record(*M, j.f.get(), j.head.data(), j.head.size(), j.buf.p, (size_t)j.count * 4)) rc = SI3D_EDIMS;
+    {
+      std::lock_guard<std::mutex> lk(M->wmu);
+      if (rc && !M->werr) M->werr = rc;
+      if (j.buf.p) M->free_bufs.push_back(j.buf);
+      --M->in_flight;
+    }
+    M->wcv.notify_all();
+  }
 }
 
-// One frame: pack on the device into the page-locked buffer, then the record with the time stamp
-// n, year, month, day, hour (si3d_utils.f90:2540-2541).
-int frame_record(HostModel& M, FILE* f, int n, int kind, int arg) {
+void enqueue(HostModel& M, HostModel::Job&& j) {
+  {
+    std::lock_guard<std::mutex> lk(M.wmu);
+    if (!M.writer.joinable()) M.writer = std::thread(writer_loop, &M);
+    ++M.in_flight;
+    M.jobs.push_back(std::move(j));
+  }
+  M.wcv.notify_all();
+}
+
+// Wait until every queued record is written; returns the writer's first error.
+int drain(HostModel& M) {
+  std::unique_lock<std::mutex> lk(M.wmu);
+  M.wcv.wait(lk, [&] { return M.in_flight == 0; });
+  return M.werr;
+}
+
+bool header_records(HostModel& M, const std::shared_ptr<FILE>& f, int frames, long long points) {
+  for (int32_t v : {(int32_t)frames, (int32_t)points}) {
+    HostModel::Job j;
+    j.f = f;
+    j.head.resize(4);
+    std::memcpy(j.head.data(), &v, 4);
+    enqueue(M, std::move(j));
+  }
+  return true;
+}
+
+// One frame: packed on the device and copied asynchronously into a page-locked buffer; the record
+// (time stamp n, year, month, day, hour, si3d_utils.f90:2540-2541, then the frame) is written by
+// the writer thread once the copy has landed.
+int frame_record(HostModel& M, const std::shared_ptr<FILE>& f, int n, int kind, int arg) {
   long long cnt = 0;
   int rc = si3d_gpu_output_frame(M.gpu, kind, arg, n == 0, nullptr, 0, &cnt);
   if (rc) return rc;
-  if (cnt > M.frame_cap) {
-    if (M.frame) si3d_gpu_host_free(M.frame);
-    M.frame = nullptr;
-    M.frame_cap = 0;
+  HostModel::Buf buf;
+  {
+    std::unique_lock<std::mutex> lk(M.wmu);
+    M.wcv.wait(lk, [&] { return M.in_flight < kMaxFramesInFlight; });
+    if (M.werr) return M.werr;
+    for (size_t i = 0; i < M.free_bufs.size(); ++i)
+      if (M.free_bufs[i].cap >= cnt) { buf = M.free_bufs[i]; M.free_bufs.erase(M.free_bufs.begin() + i); break; }
+  }
+  if (!buf.p) {
     void* p = nullptr;
     if ((rc = si3d_gpu_host_alloc(std::max<long long>(cnt, 1) * 4, &p))) return rc;
-    M.frame = static_cast<float*>(p);
-    M.frame_cap = cnt;
+    buf.p = static_cast<float*>(p);
+    buf.cap = std::max<long long>(cnt, 1);
   }
-  if ((rc = si3d_gpu_output_frame(M.gpu, kind, arg, n == 0, M.frame, M.frame_cap, &cnt))) return rc;
-  unsigned char head[20];
+  HostModel::Job j;
+  j.f = f;
+  j.buf = buf;
+  rc = si3d_gpu_output_frame_async(M.gpu, kind, arg, n == 0, buf.p, buf.cap, &j.count, &j.ticket);
+  if (rc) {
+    std::lock_guard<std::mutex> lk(M.wmu);
+    M.free_bufs.push_back(buf);
+    return rc;
+  }
+  j.head.resize(20);
   const int32_t iv[4] = {n, M.date.iyr, M.date.imon, M.date.iday};
   const float hour = (float)M.date.ihr;
-  std::memcpy(head, iv, 16);
-  std::memcpy(head + 16, &hour, 4);
-  return put_record(M, f, head, 20, M.frame, (size_t)cnt * 4) ? 0 : SI3D_EDIMS;
+  std::memcpy(j.head.data(), iv, 16);
+  std::memcpy(j.head.data() + 16, &hour, 4);
+  enqueue(M, std::move(j));
+  return 0;
 }
 
 // The output calls of the time loop (si3d.f90:430-438; with n = 0 the initial ones, :89-100):
@@ -442,12 +530,12 @@ int write_outputs(HostModel& M, int n) {
         long long cnt = 0;
         if (!f) return SI3D_EDIMS;
         if ((rc = si3d_gpu_output_frame(M.gpu, SI3D_OUT_PLANE, kp, 1, nullptr, 0, &cnt))) return rc;
-        if (!header_records(M, f.get(), (M.nts - M.itspfh) / std::max(M.iop, 1), cnt / 8)) return SI3D_EDIMS;
+        if (!header_records(M, f, (M.nts - M.itspfh) / std::max(M.iop, 1), cnt / 8)) return SI3D_EDIMS;
         M.f_plane.push_back(f);
       }
     }
     for (size_t j = 0; j < M.p_out.size(); ++j)
-      if ((rc = frame_record(M, M.f_plane[j].get(), n, SI3D_OUT_PLANE, M.p_out[j]))) return rc;
+      if ((rc = frame_record(M, M.f_plane[j], n, SI3D_OUT_PLANE, M.p_out[j]))) return rc;
   }
   long long pts = 0;
   for (int l = 0; l < M.lm; ++l) pts += M.kmz[l] + 2 - M.k1;
@@ -456,20 +544,20 @@ int write_outputs(HostModel& M, int n) {
       M.f_tracer.clear();
       for (int t = 1; t <= M.ntr; ++t) {
         auto f = open_output(M, "tracer_" + std::to_string(t));
-        if (!f || !header_records(M, f.get(), (M.nts - M.itspftr) / std::max(M.iotr, 1), pts)) return SI3D_EDIMS;
+        if (!f || !header_records(M, f, (M.nts - M.itspftr) / std::max(M.iotr, 1), pts)) return SI3D_EDIMS;
         M.f_tracer.push_back(f);
       }
     }
     for (int t = 1; t <= M.ntr; ++t)
-      if ((rc = frame_record(M, M.f_tracer[t - 1].get(), n, SI3D_OUT_TRACER, t))) return rc;
+      if ((rc = frame_record(M, M.f_tracer[t - 1], n, SI3D_OUT_TRACER, t))) return rc;
   }
   if (M.ipxml > 0 && (n == 0 || (n >= M.itspf && n % std::max(apxml, 1) == 0))) {
     if (n == 0) {
       M.f_ptrack = open_output(M, "si3d_3D");
-      if (!M.f_ptrack || !header_records(M, M.f_ptrack.get(), (M.nts - M.itspf) / std::max(apxml, 1), pts))
+      if (!M.f_ptrack || !header_records(M, M.f_ptrack, (M.nts - M.itspf) / std::max(apxml, 1), pts))
         return SI3D_EDIMS;
     }
-    if ((rc = frame_record(M, M.f_ptrack.get(), n, SI3D_OUT_PTRACK, 0))) return rc;
+    if ((rc = frame_record(M, M.f_ptrack, n, SI3D_OUT_PTRACK, 0))) return rc;
   }
   return 0;
 }
@@ -576,6 +664,7 @@ int si3d_host_attach_gpu(int h, int device, int* gpu_handle) {
   M->gpu = gh;
   M->n = 0;
   if ((rc = write_outputs(*M, 0))) return rc;   // the initial frames (si3d.f90:89-100)
+  if ((rc = drain(*M))) return rc;
   if (gpu_handle) *gpu_handle = gh;
   return 0;
 }
@@ -592,7 +681,7 @@ int si3d_host_run(int h, int nsteps, si3d_step_stats* stats) {
     M->n = n;
     if ((rc = write_outputs(*M, n))) return rc;
   }
-  return 0;
+  return drain(*M);   // every record of these steps is in its file when the call returns
 }
 
 int si3d_host_step_count(int h) {
@@ -603,6 +692,7 @@ int si3d_host_step_count(int h) {
 void si3d_host_close(int h) {
   std::lock_guard<std::mutex> lk(g_mu);
   if (h < 0 || h >= (int)g_models.size() || !g_models[h]) return;
+  drain(*g_models[h]);   // the writer still needs the device handle for its last copies
   if (g_models[h]->gpu >= 0) si3d_gpu_finalize(g_models[h]->gpu);
   g_models[h].reset();
 }

@@ -145,8 +145,13 @@ struct Ctx {
   // the column list of each output plane requested so far
   int *d_l2i = nullptr, *d_l2j = nullptr, *poff = nullptr;
   long long npoints = 0;
-  float* out_buf = nullptr;
+  float* out_buf[2] = {nullptr, nullptr};   // device frames, used in turn
   long long out_cap = 0;
+  int out_slot = 0;
+  cudaStream_t cst = nullptr;                 // device-to-host copies of frames
+  cudaEvent_t out_packed = nullptr, out_free[2] = {nullptr, nullptr};
+  cudaEvent_t out_done[16] = {};              // one per copy in flight (tickets), used in turn
+  int out_ev = 0;
   std::map<int, std::pair<int*, int>> planes;
   std::vector<int> h_kmz;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
@@ -156,7 +161,10 @@ struct Ctx {
     if (h_sc) cudaFreeHost(h_sc);
     if (h_scf) cudaFreeHost(h_scf);
     if (h_hist) cudaFreeHost(h_hist);
-    for (cudaEvent_t e : {ev0, ev1, evp0, evp1, pe0, pe1}) if (e) cudaEventDestroy(e);
+    if (cst) cudaStreamSynchronize(cst);
+    for (cudaEvent_t e : {ev0, ev1, evp0, evp1, pe0, pe1, out_packed, out_free[0], out_free[1]}) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : out_done) if (e) cudaEventDestroy(e);
+    if (cst) cudaStreamDestroy(cst);
     if (st) cudaStreamDestroy(st);
   }
   template <class T>
@@ -1608,7 +1616,14 @@ int si3d_gpu_profile(int h, int enable) {
   return 0;
 }
 
-int si3d_gpu_output_frame(int h, int kind, int arg, int first, float* host, long long capacity, long long* count) {
+}  // extern "C"
+
+namespace {
+
+// Pack one frame into the next device buffer (after its previous copy has left it) and copy it to
+// `host` on the copy stream; the returned event marks the copy's end.
+int output_frame_impl(int h, int kind, int arg, int first, float* host, long long capacity, long long* count,
+                      cudaEvent_t* done) {
   Ctx* c = get(h);
   if (!c) return SI3D_EHANDLE;
   if (!count) return SI3D_EDIMS;
@@ -1651,19 +1666,65 @@ int si3d_gpu_output_frame(int h, int kind, int arg, int first, float* host, long
   *count = n;
   if (!host) return 0;   // size query
   if (capacity < n) return SI3D_EDIMS;
-  if (!c->out_buf) {   // the largest frame: the first ptrack frame, or a plane's
+  if (!c->out_buf[0]) {   // the largest frame: the first ptrack frame, or a plane's
     c->out_cap = std::max(c->npoints * 8, (long long)c->lm * 8);
-    if (c->alloc(&c->out_buf, c->out_cap)) return SI3D_ENOMEM;
+    if (c->alloc(&c->out_buf[0], c->out_cap) || c->alloc(&c->out_buf[1], c->out_cap)) return SI3D_ENOMEM;
+    CK(cudaStreamCreateWithFlags(&c->cst, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&c->out_packed, cudaEventDisableTiming));
+    for (cudaEvent_t* e : {&c->out_free[0], &c->out_free[1]}) CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    for (cudaEvent_t& e : c->out_done) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    CK(cudaEventRecord(c->out_free[0], c->cst));
+    CK(cudaEventRecord(c->out_free[1], c->cst));
   }
   if (n > c->out_cap) return SI3D_EDIMS;
+  const int slot = c->out_slot;
+  c->out_slot ^= 1;
+  float* buf = c->out_buf[slot];
+  CK(cudaStreamWaitEvent(c->st, c->out_free[slot], 0));
   if (kind == SI3D_OUT_PLANE)
-    launch_pack_plane(d, plane.first, plane.second, arg, first != 0, c->d_l2i, c->d_l2j, c->out_buf, c->st);
+    launch_pack_plane(d, plane.first, plane.second, arg, first != 0, c->d_l2i, c->d_l2j, buf, c->st);
   else
-    launch_pack_points(d, fields, nf, c->poff, c->d_l2i, c->d_l2j, first != 0, c->out_buf, c->st);
+    launch_pack_points(d, fields, nf, c->poff, c->d_l2i, c->d_l2j, first != 0, buf, c->st);
   c->launches += 1;
   CK(cudaGetLastError());
-  if (n > 0) CK(cudaMemcpyAsync(host, c->out_buf, sizeof(float) * n, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
+  CK(cudaEventRecord(c->out_packed, c->st));
+  CK(cudaStreamWaitEvent(c->cst, c->out_packed, 0));
+  if (n > 0) CK(cudaMemcpyAsync(host, buf, sizeof(float) * n, cudaMemcpyDeviceToHost, c->cst));
+  CK(cudaEventRecord(c->out_free[slot], c->cst));
+  cudaEvent_t ev = c->out_done[c->out_ev];
+  c->out_ev = (c->out_ev + 1) % 16;
+  CK(cudaEventRecord(ev, c->cst));
+  *done = ev;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int si3d_gpu_output_frame(int h, int kind, int arg, int first, float* host, long long capacity, long long* count) {
+  cudaEvent_t done = nullptr;
+  const int rc = output_frame_impl(h, kind, arg, first, host, capacity, count, &done);
+  if (rc || !host) return rc;
+  CK(cudaEventSynchronize(done));
+  return 0;
+}
+
+int si3d_gpu_output_frame_async(int h, int kind, int arg, int first, float* host, long long capacity,
+                                long long* count, unsigned long long* ticket) {
+  if (!ticket) return SI3D_EDIMS;
+  cudaEvent_t done = nullptr;
+  const int rc = output_frame_impl(h, kind, arg, first, host, capacity, count, &done);
+  *ticket = reinterpret_cast<unsigned long long>(done);
+  return rc;
+}
+
+int si3d_gpu_output_wait(int h, unsigned long long ticket) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (!ticket) return 0;
+  CK(cudaSetDevice(c->device));
+  CK(cudaEventSynchronize(reinterpret_cast<cudaEvent_t>(ticket)));
   return 0;
 }
 

@@ -165,6 +165,15 @@
          INTEGER(C_INT), VALUE     :: handle
          REAL(C_FLOAT), INTENT(IN) :: params(*)
       END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_output_frame(handle, kind, arg, first, host, capacity, count) &
+            BIND(C, NAME="si3d_gpu_output_frame")
+         IMPORT :: C_INT, C_FLOAT, C_LONG_LONG
+         INTEGER(C_INT), VALUE            :: handle, kind, arg, first
+         REAL(C_FLOAT), INTENT(OUT)       :: host(*)
+         INTEGER(C_LONG_LONG), VALUE      :: capacity
+         INTEGER(C_LONG_LONG), INTENT(OUT) :: count
+      END FUNCTION
    END INTERFACE
 
 END MODULE si3d_gpu_iface

@@ -79,6 +79,9 @@ GPU_SYMBOLS = {
     "si3d_gpu_counters": (C.c_int, [C.c_int, C.POINTER(C.c_longlong), C.c_void_p, C.c_void_p]),
     "si3d_gpu_output_frame": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_longlong,
                                         C.POINTER(C.c_longlong)]),
+    "si3d_gpu_output_frame_async": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_longlong,
+                                              C.POINTER(C.c_longlong), C.POINTER(C.c_ulonglong)]),
+    "si3d_gpu_output_wait": (C.c_int, [C.c_int, C.c_ulonglong]),
     "si3d_gpu_host_alloc": (C.c_int, [C.c_longlong, C.POINTER(C.c_void_p)]),
     "si3d_gpu_host_free": (C.c_int, [C.c_void_p]),
     "si3d_gpu_sync": (C.c_int, [C.c_int]),
