@@ -99,6 +99,7 @@ typedef struct si3d_params {
   int precision;           /* SI3D_FP64, SI3D_MIXED_IR or SI3D_MIXED_MG */
   int ntr;                 /* non-active tracers, 0..30 (ntrmax, si3d_types.f90:291); conservative
                               tracers only (ecomod = 0, srcsnk00), advanced once per step by fd */
+  int iturb;               /* 0 constant eddy coefficients, 1 Mellor-Yamada 2.5 (si3d_mixing.f90:33-551) */
 } si3d_params;
 
 /* Per-call statistics (one entry per zeta solve inside the call). */
@@ -120,7 +121,8 @@ int si3d_gpu_init(const si3d_grid* grid, const si3d_params* params, int device, 
 
 /* Copy one reference array between host and device.  3-D names: uh uhp uhpp up upp hu hup hupp
  * agx arx vh vhp vhpp vp vpp hv hvp hvpp agy ary h hp hpp sal salp salpp rhop Av Dv wp
- * HeatSource Bth2 Bth3 Bth4 ((km1, lm1) column-major), and per tracer nt = 1..ntr the names
+ * HeatSource Bth2 Bth3 Bth4 ((km1, lm1) column-major); with iturb = 1 also q2 q2p q2pp q2l q2lp
+ * q2lpp u v; and per tracer nt = 1..ntr the names
  * "tracer<nt>" and "tracerpp<nt>" (tracer(:,:,nt), tracerpp(:,:,nt), si3d_utils.f90:571-574).
  * 2-D names: s sp spp eagx earx eagy eary sx sy dd qq rr uair vair cdw (lm1).  Replaces the
  * Fortran module arrays of si3d_types.f90:117-164. */

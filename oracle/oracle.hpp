@@ -122,6 +122,8 @@ struct Model {
   // thread-private scratch that the reference keeps across calls (si3d.f90:299-316;
   // InitThreads si3d_procedures.f90:4838-4841 zero-initialises them)
   F3 Bth2, Bth3, Bth4, Bex, Bhaxpp, Bhaypp;
+  // Mellor-Yamada 2.5 state (iturb = 1): 2 TKE and 2 TKE x length scale at n+1, n (or n+1/2), n-1
+  F3 q2, q2p, q2pp, q2l, q2lp, q2lpp;
   // non-active tracers (si3d_utils.f90:571-574): tracer and tracerpp per tracer, ntr of each
   std::vector<F3> tracer, tracerpp;
   // binary output files (outp, outz, outh) written into the run directory, and the date stamp
@@ -143,6 +145,12 @@ struct Model {
 // I/O and setup
 bool read_inputs(Model& m, const std::string& dir);  // input + ZGridDimensions + bathy + init
 void compute_date(Model& m, double itime_sec);
+// Mellor-Yamada 2.5 (oracle_turb.cpp)
+void init_turbulence(Model& m);
+void settrap_2eq(Model& m);
+void settrap2_2eq(Model& m);
+void save_2eq(Model& m, int istep);
+void update_mixing(Model& m, int istep);
 bool write_outputs(Model& m, int n);   // outh, outz, outp as the time loop calls them for step n
 // time loop
 bool run_steps(Model& m, int nsteps);

@@ -22,7 +22,8 @@ F3* field3(Model& m, const std::string& n) {
       {"hp", &Model::hp},     {"hpp", &Model::hpp},   {"sal", &Model::sal},   {"salp", &Model::salp},
       {"salpp", &Model::salpp}, {"rhop", &Model::rhop}, {"Av", &Model::Av},   {"Dv", &Model::Dv},
       {"wp", &Model::wp},     {"Bth2", &Model::Bth2}, {"Bth3", &Model::Bth3}, {"Bth4", &Model::Bth4},
-      {"Bex", &Model::Bex}};
+      {"Bex", &Model::Bex},   {"q2", &Model::q2},     {"q2p", &Model::q2p},   {"q2pp", &Model::q2pp},
+      {"q2l", &Model::q2l},   {"q2lp", &Model::q2lp}, {"q2lpp", &Model::q2lpp}};
   auto it = t.find(n);
   if (it != t.end()) return &(m.*(it->second));
   // "tracer<nt>" and "tracerpp<nt>", nt = 1..ntr

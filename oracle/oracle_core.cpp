@@ -940,6 +940,7 @@ void settrap(Model& m) {
   });
   half_level_velocities(m, true);
   continuity(m, 2);
+  if (m.in.iturb > 0) settrap_2eq(m);   // :3612
 }
 
 // settrap2 (si3d_procedures.f90:3944-4087)
@@ -959,6 +960,7 @@ void settrap2(Model& m) {
   });
   half_level_velocities(m, false);
   continuity(m, 2);
+  if (m.in.iturb > 0) settrap2_2eq(m);   // :4085
 }
 
 // save (si3d_procedures.f90:3621-3941)
@@ -1023,6 +1025,7 @@ void save(Model& m, int istep) {
     });
     continuity(m, 2);
   }
+  if (m.in.iturb > 0) save_2eq(m, istep);   // :3769, :3924
   // both branches end with tracerpp = tracer (:3771-3774, :3926-3929)
   if (m.in.ntr > 0) m.tracerpp = m.tracer;
 }
@@ -1042,6 +1045,7 @@ bool fd(Model& m, ExCoef& C) {
   if (m.in.ntr > 0 && m.in.niter > 0 && m.lastiter == 1) tracers(m);
   vel2(m);
   if (m.in.ismooth >= 1 && m.istep == 1) { m.err = "ismooth>=1 is not on the hot path"; return false; }
+  if (m.in.iturb == 1) update_mixing(m, m.istep);   // UpdateMixingCoefficients (:571)
   return true;
 }
 
@@ -1059,6 +1063,7 @@ bool run_stage(Model& m, const std::string& stage, int istep) {
   else if (stage == "vel") vel(m);
   else if (stage == "scalar") { exsal(m); imsal(m); }
   else if (stage == "tracer") tracers(m);
+  else if (stage == "turbulence") { if (m.in.iturb == 1) update_mixing(m, istep); }
   else if (stage == "vel2") vel2(m);
   else if (stage == "fd") return fd(m, C);
   else if (stage == "settrap") settrap(m);

@@ -134,7 +134,7 @@ static bool read_inp(Model& m, const std::string& dir) {
   if (p.iopss != 0) { m.err = "point sources (iopss>0) are outside the hot path"; return false; }
   if (!ok) { m.err = "si3d_inp.txt: bad record in output/boundary blocks"; return false; }
   if (p.ifsurfbc != 0) { m.err = "only ifsurfbc=0 (constant surface forcing) is on the hot path"; return false; }
-  if (p.iturb != 0) { m.err = "only iturb=0 (constant eddy coefficients) is on the hot path"; return false; }
+  if (p.iturb != 0 && p.iturb != 1) { m.err = "only iturb = 0 (constant) and 1 (Mellor-Yamada 2.5) are restated"; return false; }
   if (p.ihd > 1) { m.err = "Smagorinsky (ihd>1) is outside the hot path"; return false; }
   if (p.ibathyf < 0) { m.err = "variable layer files (ibathyf<0) are not supported by the oracle"; return false; }
 
@@ -356,7 +356,10 @@ static void init_state(Model& m, const std::vector<real>& prof) {
       real z = (m.zl(k) == -100.) ? 0.5 * m.hp(k, l) : m.zl(k) + 0.5 * m.hp(k, l);
       m.rhop(k, l) = densty_s(m.salp(k, l), 0.00004, z) - 1000.;
     }
-  // InitializeTurbulenceModel CASE(0) (si3d_mixing.f90:650-671)
+  // InitializeTurbulenceModel (si3d_mixing.f90:615-724): CASE(1) sets q2 and q2l and leaves the
+  // eddy coefficients at zero until the first fd; CASE(0) (:650-671) sets them
+  for (F3* a : {&m.q2, &m.q2p, &m.q2pp, &m.q2l, &m.q2lp, &m.q2lpp}) a->init(km1, lm1, 0.0);
+  if (m.in.iturb == 1) { init_turbulence(m); return; }
   for (int l = 1; l <= m.lm; ++l) {
     int kms = m.kmz(l), k1s = m.k1z(l);
     m.Av(k1s, l) = 0.0; m.Dv(k1s, l) = 0.0;

@@ -63,7 +63,7 @@ def _p(a):
 
 
 FIELDS_3D = ("uh uhp uhpp u up upp hu hup hupp ex agx arx vh vhp vhpp v vp vpp hv hvp hvpp agy ary h hp hpp sal salp "
-             "salpp rhop Av Dv wp Bth2 Bth3 Bth4 Bex").split()
+             "salpp rhop Av Dv wp Bth2 Bth3 Bth4 Bex q2 q2p q2pp q2l q2lp q2lpp").split()
 
 
 class OracleRun:

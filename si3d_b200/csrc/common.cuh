@@ -20,6 +20,9 @@ struct Fields3 {
   double *vh, *vhp, *vhpp, *vp, *vpp, *hv, *hvp, *hvpp, *agy, *ary;
   double *h, *hp, *hpp, *sal, *salp, *salpp, *rhop, *Av, *Dv, *wp, *HeatSource;
   double *Bth2, *Bth3, *Bth4;
+  // Mellor-Yamada 2.5 (iturb = 1 only, else null): q2, q2l at three time levels, and u, v as save
+  // leaves them
+  double *q2, *q2p, *q2pp, *q2l, *q2lp, *q2lpp, *u, *v;
 };
 
 struct Fields2 {

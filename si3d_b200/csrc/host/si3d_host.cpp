@@ -74,6 +74,7 @@ struct HostModel {
   // initial state
   std::vector<double> s0, hp0, hup0, hvp0, salp0, Av0f, Dv0f, uair, vair, cdw;
   std::vector<double> tracer0;   // ntr fields of (km1, lm1), column-major
+  std::vector<double> q2l0;      // iturb = 1: initial q2l (InitializeTurbulenceModel CASE(1))
   // outputs (si3d_utils.f90:72-121, :172-181) and the date of compute_date (:3546-3674)
   int iyr0 = 0, imon0 = 0, iday0 = 0, ihr0 = 0;
   int iop = 0, itspfh = 0, n_planes = 0, ipxml = 0, itspf = 0, iTurbVars = 0, iotr = 0, itspftr = 0;
@@ -169,7 +170,7 @@ bool read_parameters(HostModel& M, const std::string& dir) {
   else R.skip(5);
   R.skip(3); gi(M.iopss);
   if (!ok) { M.err = "si3d_inp.txt: unreadable record"; return false; }
-  if (M.iox || M.nopen || M.nxNBO || M.iopss || M.ifsurfbc || M.iturb || M.ihd > 1 || M.ibathyf < 0 ||
+  if (M.iox || M.nopen || M.nxNBO || M.iopss || M.ifsurfbc || (M.iturb != 0 && M.iturb != 1) || M.ihd > 1 || M.ibathyf < 0 ||
       M.ismooth || M.itrmom != 1) {
     M.err = "si3d_inp.txt selects an option outside the semi-implicit core (open boundaries, point "
             "sources, heat budget, turbulence closure, Smagorinsky, smoothing, non-centred advection or "
@@ -356,6 +357,26 @@ void initial_state(HostModel& M, const std::vector<double>& prof) {
     for (int l = 1; l <= lm1; ++l)
       for (int k = 1; k <= km1; ++k) M.tracer0[n3 * (nn - 1) + M.I3(k, l)] = prof[(size_t)nn * km1 + k - 1];
   M.Av0f.assign(n3, 0.0); M.Dv0f.assign(n3, 0.0);
+  if (M.iturb == 1) {
+    // InitializeTurbulenceModel CASE(1) (si3d_mixing.f90:679-719): q2 = q2_min everywhere, q2l
+    // = q2 times the mixing length kappa z sqrt(1 - z / htot) below each column's top layer (htot
+    // sums hp over every layer, the sediment layer included); the eddy coefficients stay zero
+    // until the first fd
+    M.q2l0.assign(n3, 0.0);
+    for (int l = 1; l <= M.lm; ++l) {
+      const int kms = M.kmz[l - 1], k1s = M.k1z0[l - 1];
+      double htot = 0.0;
+      for (int k = 1; k <= km1; ++k) htot += M.hp0[M.I3(k, l)];
+      if (kms <= k1s) continue;
+      double z0 = 0.0;
+      for (int k = k1s + 1; k <= kms; ++k) {
+        z0 = z0 + M.hp0[M.I3(k - 1, l)];
+        const double mixl = 0.41 * z0 * std::sqrt(std::max(1. - (z0 / htot), 0.0));
+        M.q2l0[M.I3(k, l)] = 2.e-6 * mixl;
+      }
+    }
+    return;
+  }
   for (int l = 1; l <= M.lm; ++l) {
     const int kms = M.kmz[l - 1], k1s = M.k1z0[l - 1];
     for (int k = k1s + 1; k <= kms; ++k) { M.Av0f[M.I3(k, l)] = M.Av0; M.Dv0f[M.I3(k, l)] = M.Dv0; }
@@ -630,6 +651,7 @@ int si3d_host_attach_gpu(int h, int device, int* gpu_handle) {
   p.pcg_test = M->opt.pcg_test; p.pcg_tol = M->opt.pcg_tol; p.pcg_itmax = M->opt.pcg_itmax; p.srelpr = M->opt.srelpr;
   p.ordering = SI3D_ORDER_REDBLACK; p.x0_mode = M->opt.x0_mode; p.precision = M->opt.precision;
   p.ntr = M->ntr;
+  p.iturb = M->iturb;
   int gh = -1;
   int rc = si3d_gpu_init(&g, &p, device, &gh);
   if (rc) return rc;
@@ -649,6 +671,11 @@ int si3d_host_attach_gpu(int h, int device, int* gpu_handle) {
     const std::string a = "tracer" + std::to_string(nn), b = "tracerpp" + std::to_string(nn);
     if ((rc = si3d_gpu_set_field(gh, a.c_str(), t0))) return rc;
     if ((rc = si3d_gpu_set_field(gh, b.c_str(), t0))) return rc;
+  }
+  if (M->iturb == 1) {
+    const std::vector<double> qmin((size_t)M->km1 * M->lm1, 2.e-6);
+    for (const char* nm : {"q2", "q2p", "q2pp"}) if ((rc = si3d_gpu_set_field(gh, nm, qmin.data()))) return rc;
+    for (const char* nm : {"q2l", "q2lp", "q2lpp"}) if ((rc = si3d_gpu_set_field(gh, nm, M->q2l0.data()))) return rc;
   }
   if ((rc = si3d_gpu_set_field(gh, "Av", M->Av0f.data()))) return rc;
   if ((rc = si3d_gpu_set_field(gh, "Dv", M->Dv0f.data()))) return rc;

@@ -102,6 +102,12 @@ void launch_save(const Dev& d, int istep, cudaStream_t st);
 
 void launch_density_init(const Dev& d, cudaStream_t st);
 
+// Mellor-Yamada 2.5 (k_turb.cu): the closure at the end of fd (scr4: four km1 x P scratch fields),
+// the half levels of settrap (mode 1) / settrap2 (mode 2), and save's time levels.
+void launch_turbulence(const Dev& d, double* scr4, cudaStream_t st);
+void launch_turb_half(const Dev& d, int mode, cudaStream_t st);
+void launch_turb_save(const Dev& d, int istep, cudaStream_t st);
+
 // Output frames (k_output.cu): nf fields (layer-major FP64) at every point k1..kmz(l) + 1 of every
 // wet column, point offsets poff (lm + 1 entries), optionally preceded by the coordinates i, j, k,
 // as 4-byte floats into `out`; and one horizontal plane's frame over its column list.

@@ -141,6 +141,7 @@ struct Ctx {
   long long tr_stride = 0;
   double* tr_scr = nullptr;   // elimination factors, one km1 x P field per tracer group
   double* tr_fx = nullptr;    // face fluxes of one flux group (the last tracer's go to Bth2/3/4)
+  double* turb_scr = nullptr; // Mellor-Yamada 2.5: four km1 x P scratch fields
   // output frames: column coordinates, point offsets of the 3-D frames, a device frame buffer and
   // the column list of each output plane requested so far
   int *d_l2i = nullptr, *d_l2j = nullptr, *poff = nullptr;
@@ -191,7 +192,7 @@ Ctx* get(int h) {
 
 // Stage ids for the per-stage device timers.
 enum { ST_MOMX, ST_MOMY, ST_MATCON, ST_PCG_SETUP, ST_PCG_ITER, ST_PCG_FINISH, ST_SLAYER, ST_VEL, ST_SCALAR, ST_VEL2,
-       ST_SETTRAP, ST_SETTRAP2, ST_SAVE, ST_LEARN, ST_TRACER, ST_COUNT };
+       ST_SETTRAP, ST_SETTRAP2, ST_SAVE, ST_LEARN, ST_TRACER, ST_TURB, ST_COUNT };
 
 // Run `f` (which enqueues `nk` kernels) as one timed stage.
 template <class F>
@@ -224,7 +225,9 @@ double* f3ptr(Ctx* c, const std::string& n) {
       {"h", &Fields3::h},       {"hp", &Fields3::hp},     {"hpp", &Fields3::hpp},   {"sal", &Fields3::sal},
       {"salp", &Fields3::salp}, {"salpp", &Fields3::salpp}, {"rhop", &Fields3::rhop}, {"Av", &Fields3::Av},
       {"Dv", &Fields3::Dv},     {"wp", &Fields3::wp},     {"HeatSource", &Fields3::HeatSource},
-      {"Bth2", &Fields3::Bth2}, {"Bth3", &Fields3::Bth3}, {"Bth4", &Fields3::Bth4}};
+      {"Bth2", &Fields3::Bth2}, {"Bth3", &Fields3::Bth3}, {"Bth4", &Fields3::Bth4},
+      {"q2", &Fields3::q2},     {"q2p", &Fields3::q2p},   {"q2pp", &Fields3::q2pp}, {"q2l", &Fields3::q2l},
+      {"q2lp", &Fields3::q2lp}, {"q2lpp", &Fields3::q2lpp}, {"u", &Fields3::u},      {"v", &Fields3::v}};
   auto it = t.find(n);
   return it == t.end() ? nullptr : f.*(it->second);
 }
@@ -274,6 +277,22 @@ int tracer_save(Ctx* c) {
   }
   c->tr_alias = true;
   return 0;
+}
+
+// settrap / settrap2 / save with the turbulence time levels (si3d_procedures.f90:3612, :4085,
+// :3769, :3924) and save's tracer hand-over.
+void settrap_all(Ctx* c) {
+  launch_settrap(c->d, c->st);
+  if (c->prm.iturb == 1) launch_turb_half(c->d, 1, c->st);
+}
+void settrap2_all(Ctx* c) {
+  launch_settrap2(c->d, c->st);
+  if (c->prm.iturb == 1) launch_turb_half(c->d, 2, c->st);
+}
+int save_all(Ctx* c, int istep) {
+  launch_save(c->d, istep, c->st);
+  if (c->prm.iturb == 1) launch_turb_save(c->d, istep, c->st);
+  return tracer_save(c);
 }
 
 double* f2ptr(Ctx* c, const std::string& n) {
@@ -811,6 +830,8 @@ int fd_impl(Ctx* c, int istep, bool lastiter, si3d_step_stats* st) {
   if (!rc && c->prm.ntr > 0 && c->prm.niter > 0 && lastiter)
     rc = stage(c, ST_TRACER, 2 * ((c->prm.ntr + kTracerFluxGroup - 1) / kTracerFluxGroup) + 1, [&] { tracer_stage(c); });
   if (!rc) rc = stage(c, ST_VEL2, 1, [&] { launch_vel2(d, c->st); });
+  // UpdateMixingCoefficients (si3d_procedures.f90:571)
+  if (!rc && c->prm.iturb == 1) rc = stage(c, ST_TURB, 1, [&] { launch_turbulence(d, c->turb_scr, c->st); });
   if (rc) return rc;
   if (st) {
     CK(cudaEventSynchronize(c->evp1));
@@ -856,6 +877,7 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
     return SI3D_EDIMS;
   if (prm->x0_mode < SI3D_X0_PREV || prm->x0_mode > SI3D_X0_HIST) return SI3D_EDIMS;
   if (prm->ntr < 0 || prm->ntr > 30) return SI3D_EDIMS;   // ntrmax (si3d_types.f90:291)
+  if (prm->iturb != 0 && prm->iturb != 1) return SI3D_EDIMS;
   // every kernel indexes neighbours through the maps and layers down to kmz + 1: both are checked
   // here once, so no device access can leave its field
   for (int l = 0; l < g->lm; ++l) {
@@ -936,6 +958,10 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
     rc |= c->alloc(q, P);
   for (int** q : {&s.k1z, &s.k1u, &s.k1v}) rc |= c->alloc(q, P);
   rc |= c->alloc(&d.scr, n3);
+  if (prm->iturb == 1) {
+    for (double** q : {&f.q2, &f.q2p, &f.q2pp, &f.q2l, &f.q2lp, &f.q2lpp, &f.u, &f.v}) rc |= c->alloc(q, n3);
+    rc |= c->alloc(&c->turb_scr, 4 * n3);
+  }
   {   // output frames: coordinates and point offsets (k1 .. kmz + 1 per wet column)
     std::vector<int> off(lm + 1, 0);
     c->h_kmz.assign(g->kmz, g->kmz + lm);
@@ -1251,10 +1277,11 @@ int si3d_gpu_stage(int h, const char* stage, int istep, si3d_step_stats* st) {
   } else if (s == "vel") launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st);
   else if (s == "scalar") launch_exsal_imsal(d, c->tune, c->st);
   else if (s == "tracer") { if (c->prm.ntr > 0) tracer_stage(c); }
+  else if (s == "turbulence") { if (c->prm.iturb == 1) launch_turbulence(d, c->turb_scr, c->st); }
   else if (s == "vel2") launch_vel2(d, c->st);
-  else if (s == "settrap") launch_settrap(d, c->st);
-  else if (s == "settrap2") launch_settrap2(d, c->st);
-  else if (s == "save") { launch_save(d, istep, c->st); if (int rc = tracer_save(c)) return rc; }
+  else if (s == "settrap") settrap_all(c);
+  else if (s == "settrap2") settrap2_all(c);
+  else if (s == "save") { if (int rc = save_all(c, istep)) return rc; }
   else return SI3D_ENAME;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
@@ -1265,7 +1292,7 @@ int si3d_gpu_settrap(int h) {
   Ctx* c = get(h);
   if (!c) return SI3D_EHANDLE;
   CK(cudaSetDevice(c->device));
-  launch_settrap(c->d, c->st);
+  settrap_all(c);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
   return 0;
@@ -1275,7 +1302,7 @@ int si3d_gpu_settrap2(int h) {
   Ctx* c = get(h);
   if (!c) return SI3D_EHANDLE;
   CK(cudaSetDevice(c->device));
-  launch_settrap2(c->d, c->st);
+  settrap2_all(c);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
   return 0;
@@ -1286,8 +1313,7 @@ int si3d_gpu_save(int h, int istep) {
   if (!c) return SI3D_EHANDLE;
   if (istep != 1 && istep != 2) return SI3D_EDIMS;
   CK(cudaSetDevice(c->device));
-  launch_save(c->d, istep, c->st);
-  if (int rc = tracer_save(c)) return rc;
+  if (int rc = save_all(c, istep)) return rc;
   c->trap_solves = 0;
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
@@ -1310,25 +1336,29 @@ static int step_impl(Ctx* c, int n, si3d_step_stats* st) {
     rc = fd_impl(c, 1, leapfrog_only, st);
     if (rc) return rc;
     if (leapfrog_only) {
-      rc = stage(c, ST_SAVE, 2, [&] { launch_save(c->d, 1, c->st); });
-      if (!rc) rc = tracer_save(c);
+      int rs = 0;
+      rc = stage(c, ST_SAVE, 2, [&] { rs = save_all(c, 1); });
+      if (!rc) rc = rs;
       if (rc) return rc;
       goto done;
     }
-    rc = stage(c, ST_SETTRAP, 3, [&] { launch_settrap(c->d, c->st); });
+    rc = stage(c, ST_SETTRAP, 3, [&] { settrap_all(c); });
     if (rc) return rc;
   }
   for (int it = 1; it <= niter1; ++it) {
     rc = fd_impl(c, 2, it == niter1, st);
     if (rc) return rc;
     if (it < niter1) {
-      rc = stage(c, ST_SETTRAP2, 3, [&] { launch_settrap2(c->d, c->st); });
+      rc = stage(c, ST_SETTRAP2, 3, [&] { settrap2_all(c); });
       if (rc) return rc;
     }
     if (it > 20) break;
   }
-  rc = stage(c, ST_SAVE, 2, [&] { launch_save(c->d, 2, c->st); });
-  if (!rc) rc = tracer_save(c);
+  {
+    int rs = 0;
+    rc = stage(c, ST_SAVE, 2, [&] { rs = save_all(c, 2); });
+    if (!rc) rc = rs;
+  }
   if (rc) return rc;
 done:
   CK(cudaGetLastError());

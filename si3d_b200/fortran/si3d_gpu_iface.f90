@@ -27,7 +27,7 @@
       INTEGER(C_INT) :: pcg_itmax
       REAL(C_DOUBLE) :: srelpr
       INTEGER(C_INT) :: ordering, x0_mode, precision
-      INTEGER(C_INT) :: ntr
+      INTEGER(C_INT) :: ntr, iturb
    END TYPE si3d_params_t
 
    TYPE, BIND(C) :: si3d_step_stats_t

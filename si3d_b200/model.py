@@ -12,7 +12,7 @@ from . import native
 from .native import SolverOpts, StepStats, check
 
 FIELDS_3D = ("uh uhp uhpp up upp hu hup hupp agx arx vh vhp vhpp vp vpp hv hvp hvpp agy ary h hp hpp sal salp salpp "
-             "rhop Av Dv wp HeatSource Bth2 Bth3 Bth4").split()
+             "rhop Av Dv wp HeatSource Bth2 Bth3 Bth4 q2 q2p q2pp q2l q2lp q2lpp u v").split()
 FIELDS_2D = "s sp spp eagx earx eagy eary sx sy dd qq rr uair vair cdw".split()
 IFIELDS = ("k1z", "k1u", "k1v")
 

@@ -43,7 +43,7 @@ class Params(C.Structure):
                 ("iadv", C.c_int), ("itrmom", C.c_int), ("ihd", C.c_int), ("ibc", C.c_int), ("isal", C.c_int),
                 ("itrap", C.c_int), ("niter", C.c_int), ("ismooth", C.c_int), ("pcg_test", C.c_int),
                 ("pcg_tol", C.c_double), ("pcg_itmax", C.c_int), ("srelpr", C.c_double), ("ordering", C.c_int),
-                ("x0_mode", C.c_int), ("precision", C.c_int), ("ntr", C.c_int)]
+                ("x0_mode", C.c_int), ("precision", C.c_int), ("ntr", C.c_int), ("iturb", C.c_int)]
 
 
 class StepStats(C.Structure):
@@ -123,7 +123,7 @@ HOST_SYMBOLS = {
 }
 
 STAGES = ("momentum_x", "momentum_y", "matcon", "pcg_setup", "pcg_iter", "pcg_finish", "slayer_h", "vel",
-          "scalar", "vel2", "settrap", "settrap2", "save", "learn", "tracer")
+          "scalar", "vel2", "settrap", "settrap2", "save", "learn", "tracer", "turbulence")
 
 _gpu = None
 _host = None

@@ -58,6 +58,7 @@ class Basin:
     niter: int = 2
     ibc: int = 1                 # baroclinic pressure term on/off
     ntr: int = 0                 # non-active (conservative) tracers, ecomod = 0
+    iturb: int = 0               # 0 constant eddy coefficients, 1 Mellor-Yamada 2.5
     # binary outputs: H-planes every iop steps from itspfh (outh), tracers every iotr steps (outz),
     # the 3-D ptrack file every ipxml steps from itspf (outp); 0 = off
     iop: int = 0
@@ -169,7 +170,7 @@ def write_inp(b: Basin, path: str) -> None:
                      ("zeta0", 0.0), ("idt", b.dt), ("ibathf", 0)]:
         L.append(_rec(lab, float(val) if lab != "ibathf" else val))
     L += [sep, "Parameters controlling solution algorithm", sep]
-    for lab, val in [("itrap", 1), ("niter", b.niter), ("smooth", 0), ("beta", 0.05), ("iturb", 0),
+    for lab, val in [("itrap", 1), ("niter", b.niter), ("smooth", 0), ("beta", 0.05), ("iturb", b.iturb),
                      ("az0", b.Av0), ("dz0", b.Dv0), ("iadv", 1), ("itrmom", 1), ("ihd", 1), ("ax0", b.Ax0),
                      ("ay0", b.Ay0), ("f", b.f), ("theta", 1.0), ("ibc", b.ibc), ("isal", 1), ("itrsch", 4),
                      ("cd", b.cd), ("ifsbc", 0), ("dtsbc", 3600.0), ("icw", 0), ("cw", b.cw), ("ws", b.wa),
@@ -278,11 +279,12 @@ def write_run(b: Basin, run_dir: str) -> str:
 
 
 def make(name: str, run_dir: str, nsteps: Optional[int] = None, seed_offset: int = 0, ntr: int = 0,
-         outputs: Optional[dict] = None) -> Basin:
+         outputs: Optional[dict] = None, iturb: int = 0) -> Basin:
     """Write workload `name` into run_dir; `outputs` sets the output records (iop, itspfh, planes,
     ipxml, itspf, iotr, itspftr)."""
     b = config(name, nsteps, seed_offset)
     b.ntr = ntr
+    b.iturb = iturb
     for k, v in (outputs or {}).items():
         setattr(b, k, v)
     write_run(b, run_dir)

@@ -62,6 +62,19 @@ def tracer_dirs(tmp_path_factory):
 
 
 @pytest.fixture(scope="session")
+def turb_dirs(tmp_path_factory):
+    """The small runs with the Mellor-Yamada 2.5 closure (iturb = 1)."""
+    from si3d_b200 import synth
+    base = tmp_path_factory.mktemp("turb_runs")
+    out = {}
+    for name in ("t0", "t1", "c0"):
+        d = str(base / name)
+        synth.make(name, d, iturb=1)
+        out[name] = d
+    return out
+
+
+@pytest.fixture(scope="session")
 def run_dirs(tmp_path_factory):
     """Small reference-format runs shared by the tests."""
     from si3d_b200 import synth
