@@ -45,6 +45,9 @@ MG_ITER_STREAMS = 15
 # written.
 TRACER_SHARED_STREAMS = 16
 TRACER_STREAMS_PER_TRACER = 2
+# The Mellor-Yamada 2.5 closure of one fd call, per wet 3-D cell: hp, rhop, up, vp, q2p, q2pp,
+# q2lp, q2lpp, Av, Dv read, Av, Dv, q2, q2l written.
+STAGE_STREAMS_TURB = 14
 
 WORKLOAD_DESC = {
     "c2": "c2: 2000x1000 cells x 60 layers, seeded random bathymetry and wind stress, dt 30 s, itrap=1 niter=2, "
@@ -119,12 +122,12 @@ def traffic_table():
     return {}
 
 
-def workload_dir(name: str, rank: int, ntr: int = 0) -> str:
+def workload_dir(name: str, rank: int, ntr: int = 0, iturb: int = 0) -> str:
     from si3d_b200 import synth
-    d = os.path.join(tempfile.gettempdir(), f"si3d_bench_{name}_tr{ntr}_r{rank}")
+    d = os.path.join(tempfile.gettempdir(), f"si3d_bench_{name}_tr{ntr}_t{iturb}_r{rank}")
     marker = os.path.join(d, ".complete")
     if not os.path.exists(marker):
-        synth.make(name, d, ntr=ntr)
+        synth.make(name, d, ntr=ntr, iturb=iturb)
         open(marker, "w").close()
     return d
 
@@ -148,7 +151,7 @@ def counts(run_dir: str):
     return lm, n3
 
 
-def cpu_sample(name: str, threads: int, steps: int = 0, warmup: int = 0, ntr: int = 0) -> dict:
+def cpu_sample(name: str, threads: int, steps: int = 0, warmup: int = 0, ntr: int = 0, iturb: int = 0) -> dict:
     """The CPU restatement of the reference timed on a window of the workload (same layers,
     bathymetry and forcing generators), extrapolated linearly in wet 3-D cells.  The column stages
     run on `threads` host threads; the zeta solve is serial, as the reference runs it on thread 0.
@@ -164,11 +167,12 @@ def cpu_sample(name: str, threads: int, steps: int = 0, warmup: int = 0, ntr: in
     x0, y0 = (full.nx - wx) // 2, (full.ny - wy) // 2
     sub.nx, sub.ny = wx, wy
     sub.ntr = ntr
+    sub.iturb = iturb
     sub.depth = full.depth[x0:x0 + wx, y0:y0 + wy].copy()
     if full.uair is not None:
         sub.uair = full.uair[x0:x0 + wx, y0:y0 + wy].copy()
         sub.vair = full.vair[x0:x0 + wx, y0:y0 + wy].copy()
-    d = os.path.join(tempfile.gettempdir(), f"si3d_cpu_window_{name}_tr{ntr}")
+    d = os.path.join(tempfile.gettempdir(), f"si3d_cpu_window_{name}_tr{ntr}_t{iturb}")
     synth.write_run(sub, d)
     os.environ["SI3D_ORACLE_THREADS"] = str(threads)   # read once, at the oracle's first column loop
     pyoracle.build()
@@ -276,6 +280,8 @@ def main() -> int:
     ap.add_argument("--itmax", type=int, default=2000)
     ap.add_argument("--ntr", type=int, default=0,
                     help="conservative tracers carried by the workload (0..30; the headline workload has none)")
+    ap.add_argument("--iturb", type=int, default=0, choices=[0, 1],
+                    help="1: the Mellor-Yamada 2.5 closure instead of constant eddy coefficients")
     ap.add_argument("--forms", default="",
                     help="comma-separated subset of plain_fp64,mixed_ir,mixed_last,learned_fp64,learned_mixed (the last one "
                          "is the headline); default: plain_fp64,mixed_ir,mixed_last and learned_mixed when trained "
@@ -289,14 +295,14 @@ def main() -> int:
         if rank != 0:
             return 0
         threads = os.cpu_count() or 1
-        lm_full, n3_full = counts(workload_dir(args.workload, 0, args.ntr))
-        smp = cpu_sample(args.workload, threads, steps=args.steps, warmup=args.warmup, ntr=args.ntr)
+        lm_full, n3_full = counts(workload_dir(args.workload, 0, args.ntr, args.iturb))
+        smp = cpu_sample(args.workload, threads, steps=args.steps, warmup=args.warmup, ntr=args.ntr, iturb=args.iturb)
         v = smp["window_s_per_step"] * n3_full / smp["n3"]
         line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "s/timestep", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD_DESC.get(args.workload, args.workload), "form": "plain_fp64",
-                           "ntr": args.ntr,
+                           "ntr": args.ntr, "iturb": args.iturb,
                            "lm": lm_full, "n3": n3_full, "parallelism": "replicas x1",
                            "l2": "host run; no GPU caches involved"},
                 "cpu_baseline": {"value": v, "unit": "s/timestep", "cores": threads, "kind": "port",
@@ -326,7 +332,7 @@ def main() -> int:
     sbuild.build_all()
     if args.workload == "c3":
         return bench_ensemble(args, ws, rank, device, pg)
-    run_dir = workload_dir(args.workload, rank, args.ntr)
+    run_dir = workload_dir(args.workload, rank, args.ntr, args.iturb)
     lm, n3 = counts(run_dir)
     peak, peak_kind = measured_peaks()
     g = native.gpu()
@@ -379,6 +385,13 @@ def main() -> int:
                                    "ms_per_tracer": ms / calls / args.ntr, "algorithmic_bytes_per_call": alg,
                                    "achieved": alg / (ms / calls * 1e-3) / 1e9, "peak": peak, "unit": "GB/s",
                                    "frac": alg / (ms / calls * 1e-3) / 1e9 / peak, "peak_kind": peak_kind}
+        if "turbulence" in stage_ms:
+            ms, calls = stage_ms["turbulence"]
+            alg = 8 * n3 * STAGE_STREAMS_TURB
+            out["turbulence_stage"] = {"ms_per_call": ms / calls, "calls_per_step": calls / 2,
+                                       "algorithmic_bytes_per_call": alg, "achieved": alg / (ms / calls * 1e-3) / 1e9,
+                                       "peak": peak, "unit": "GB/s", "frac": alg / (ms / calls * 1e-3) / 1e9 / peak,
+                                       "peak_kind": peak_kind}
         dominant = max(stage_ms, key=lambda k: stage_ms[k][0])
         if dominant == "tracer":
             ts = out["tracer_stage"]
@@ -447,7 +460,7 @@ def main() -> int:
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        smp = cpu_sample(args.workload, threads, ntr=args.ntr)
+        smp = cpu_sample(args.workload, threads, ntr=args.ntr, iturb=args.iturb)
         v = smp["window_s_per_step"] * n3 / smp["n3"]
         cpu = {"value": v, "unit": "s/timestep", "cores": threads, "kind": "port",
                "sample": f"{smp['steps']} steps of a {smp['window']} window (plain FP64, red-black MIC-PCG at 1e-12), "
@@ -466,7 +479,7 @@ def main() -> int:
                       "mg_mixed": "f64 (fp32 multigrid inner solves)",
                       "learned_mg": "f64 (fp32 multigrid inner solves, bf16 guess net)"}[head_form], "data": "synthetic",
             "config": {"workload": WORKLOAD_DESC.get(args.workload, args.workload),
-                       "form": head_form, "ntr": args.ntr, "lm": lm, "n3": n3, "parallelism": f"replicas x{ws}",
+                       "form": head_form, "ntr": args.ntr, "iturb": args.iturb, "lm": lm, "n3": n3, "parallelism": f"replicas x{ws}",
                        "l2": "state (~25 GB) far larger than L2; no flush needed"},
             "pcg_iters_per_step": head["pcg_iters_per_step"], "pcg_s_per_step": head["pcg_s_per_step"],
             "speedup_vs_plain_fp64": plain["s_per_step"] / head["s_per_step"],
