@@ -55,3 +55,31 @@ def test_closure_runs_match_oracle(turb_dirs, oracle_lib, native_libs, name):
             assert _rel(o.get(f), g.get(f)) <= tol, f
     finally:
         g.close()
+
+
+def test_closure_with_tracers_and_outputs(tmp_path, oracle_lib, native_libs):
+    """Every addition at once on t1: the closure feeds Dv to temperature and tracer diffusion and Av
+    to momentum, two tracers, and the plane, tracer and ptrack files; 12 steps against the oracle."""
+    import os
+    import shutil
+    from si3d_b200 import synth
+    from si3d_b200.model import GpuRun
+    from test_outputs_oracle import read_records
+    out = dict(iop=4, planes=(3, 99), ipxml=6, iotr=4)
+    dg, do = str(tmp_path / "gpu"), str(tmp_path / "oracle")
+    synth.make("t1", dg, ntr=2, iturb=1, outputs=out)
+    shutil.copytree(dg, do)
+    g = GpuRun(dg, pcg_itmax=2000)
+    o = oracle_lib.OracleRun(do, ordering=1, pcg_itmax=2000)
+    try:
+        g.run(12)
+        o.run(12)
+        assert np.abs(o.get("s") - g.get("s")).max() <= 1e-9
+        for f, tol in (("uh", 1e-8), ("sal", 1e-10), ("tracer1", 1e-9), ("tracer2", 1e-9), ("q2", 1e-8), ("Dv", 1e-8)):
+            assert _rel(o.get(f), g.get(f)) <= tol, f
+        for name in ("si3d_3D", "tracer_1", "tracer_2", "plane_3", "plane_99"):
+            rg, ro = read_records(os.path.join(dg, name)), read_records(os.path.join(do, name))
+            assert [len(r) for r in rg] == [len(r) for r in ro] and rg[:3] == ro[:3], name
+    finally:
+        g.close()
+        o.close()
