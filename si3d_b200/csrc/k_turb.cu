@@ -101,6 +101,18 @@ __global__ void k_turb_column(Dev d, TurbConst T, double* __restrict__ sxl, doub
     // dcoeff(k1s) = Sq 0.5 (xl(k1s) + xl(k1s + 1)) sqrt(0.5 (q2p(k1s) + q2p(k1s + 1))), xl(k1s) = 0
     dco_prev = Sq * 0.50 * (0.0 + sxl[IX(d, k1s + 1, l)]) *
                sqrt(0.50 * (q2p[IX(d, k1s, l)] + q2p[IX(d, k1s + 1, l)]));
+    // the interior layers' inputs, loaded one layer ahead of the arithmetic that uses them
+    struct In { double hpk, hpu, xl, xln, qp, qpn, SP, BP, x1, x2, zb; };
+    auto load = [&](int k) -> In {
+      const int ik = IX(d, k, l);
+      In v;
+      v.hpk = hp[ik]; v.hpu = hp[ik - P]; v.xl = sxl[ik]; v.xln = (k < kms) ? sxl[ik + P] : 0.0;
+      v.qp = q2p[ik]; v.qpn = q2p[ik + P]; v.SP = ssp[ik]; v.BP = sbp[ik];
+      if (eq == 0) { v.x1 = q2pp[ik]; v.x2 = 0.0; v.zb = 0.0; }
+      else { v.x1 = q2lp[ik]; v.x2 = q2lpp[ik]; v.zb = szb[ik]; }
+      return v;
+    };
+    In nxt = load(k1s + 1);
     for (int k = k1s; k <= kms + 1; ++k) {
       const int ik = IX(d, k, l);
       double a1 = 0.0, a2 = r3, a3 = 0.0, ds;
@@ -109,26 +121,26 @@ __global__ void k_turb_column(Dev d, TurbConst T, double* __restrict__ sxl, doub
       } else if (k == kms + 1) {
         ds = eq == 0 ? 3. * T.b1_23 * ustar_b / twodt1 : 0.0;
       } else {
-        const double hpk = hp[ik], hpu = hp[ik - P];
-        const double xl = sxl[ik], qp = q2p[ik];
-        const double xln = (k < kms) ? sxl[ik + P] : 0.0;
-        const double dco = Sq * 0.50 * (xl + xln) * sqrt(0.50 * (qp + q2p[ik + P]));
+        const In v = nxt;
+        if (k + 1 <= kms) nxt = load(k + 1);
+        const double hpk = v.hpk, hpu = v.hpu, xl = v.xl, qp = v.qp;
+        const double dco = Sq * 0.50 * (xl + v.xln) * sqrt(0.50 * (qp + v.qpn));
         a3 = -dco / (hpk * 0.50 * (hpk + hpu));
         a1 = -dco_prev / (hpu * 0.50 * (hpk + hpu));
         dco_prev = dco;
         zt = zt + hpu;   // distance from the surface to the top of layer k
-        const double SP = ssp[ik], BP = sbp[ik];
+        const double SP = v.SP, BP = v.BP;
         if (eq == 0) {
           a2 = r3 - a1 - a3 + 2. * (sqrt(qp) / (B_1 * xl));
-          ds = 4. * qp / twodt1 - q2pp[ik] / twodt1;
+          ds = 4. * qp / twodt1 - v.x1 / twodt1;
           if (BP >= 0.0) ds = ds + 2. * (SP + BP);
           else { ds = ds + 2. * (SP); a2 = a2 - BP * 2. / qp; }
         } else {
-          const double wa = xl / (kKappaS * szb[ik]), wb = xl / (kKappaS * zt);
+          const double wa = xl / (kKappaS * v.zb), wb = xl / (kKappaS * zt);
           a2 = r3 - a1 - a3 + sqrt(qp) / (B_1 * xl) * (1. + E_2 * (wa * wa) + E_3 * (wb * wb));
           if (BP >= 0) ds = xl * (E_1 * SP + E_1 * BP);
           else { ds = xl * (E_1 * SP); a2 = a2 - E_1 * BP / qp; }
-          ds = ds + 4 * q2lp[ik] / twodt1 - q2lpp[ik] / twodt1;
+          ds = ds + 4 * v.x1 / twodt1 - v.x2 / twodt1;
         }
       }
       if (k == k1s) {
@@ -145,9 +157,13 @@ __global__ void k_turb_column(Dev d, TurbConst T, double* __restrict__ sxl, doub
     const double qmin = eq == 0 ? kQ2Min : kQ2lMin;
     double x = f_prev;
     out[IX(d, kms + 1, l)] = fmax(qmin, x);
+    // backward sweep, the next layer's factor and forward value loaded ahead
+    double en = se[IX(d, kms, l)], fn = out[IX(d, kms, l)];
     for (int k = kms; k >= k1s; --k) {
       const int ik = IX(d, k, l);
-      x = se[ik] * x + out[ik];
+      const double e = en, fv = fn;
+      if (k - 1 >= k1s) { en = se[ik - P]; fn = out[ik - P]; }
+      x = e * x + fv;
       out[ik] = fmax(qmin, x);
     }
     const double top = out[IX(d, k1s, l)];
