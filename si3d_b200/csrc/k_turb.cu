@@ -7,8 +7,9 @@
 // of time n+1 from q2 and q2l of time n (a column's production reads only its own coefficients, so
 // they are replaced as soon as they are used), then the two tridiagonal systems for q2 and q2l over
 // the layers k1s .. kms + 1 (the same off-diagonals), solved as tridT does (divisions, not
-// reciprocals).  Per-layer quantities the sweeps reuse (limited length scale, production terms,
-// distance from the bottom, elimination factors) go to four scratch fields.
+// reciprocals), each sweep loading its next layer before the current layer's arithmetic.
+// Per-layer quantities the sweeps reuse (limited length scale, production terms, distance from the
+// bottom, elimination factors) go to four scratch fields.
 #include "kernels.h"
 
 namespace si3d {
