@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(32 * CLN) k_tracer_flux(Dev d, const double* _
   if (l > d.g.lm) return;
   const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
   if (k1s + (int)threadIdx.y > kms) return;
-  const int P = d.g.P, km1 = d.g.km1;
+  const int P = d.g.P;
   const int lE = NB(d.g.lEC, l), lW = NB(d.g.lWC, l), lN = NB(d.g.lNC, l), lS = NB(d.g.lSC, l);
   const int lEE = NB(d.g.lEC, lE), lNN = NB(d.g.lNC, lN);
   const int dEo = lE - l, dWo = lW - l, dNo = lN - l, dSo = lS - l, dEEo = lEE - l, dNNo = lNN - l;
