@@ -115,3 +115,53 @@ def test_calendar_rolls_over_days_and_months(tmp_path, oracle_lib):
     stamps = [frame(r, 5 if k else 8)[0] for k, r in enumerate(read_records(os.path.join(d, "si3d_3D"))[2:])]
     assert [s[1:] for s in stamps] == [(2024, 1, 31, 2398.0), (2024, 1, 31, 2400.0), (2024, 2, 1, 1.0),
                                        (2024, 2, 1, 3.0)]
+
+
+def test_calendar_rolls_over_the_year(tmp_path, oracle_lib):
+    """31 December 23.98 h with 60 s steps: the second step is 1 January of the next year."""
+    from si3d_b200 import synth
+    d = str(tmp_path / "year")
+    synth.make("t0", d, outputs=dict(ipxml=1))
+    p = os.path.join(d, "si3d_inp.txt")
+    lines = open(p).read().splitlines()
+    for lab, val in (("month", 12), ("day", 31), ("hour", 2398)):
+        i = next(i for i, ln in enumerate(lines) if ln.startswith(f" {lab:<12}!"))
+        lines[i] = synth._rec(lab, val)
+    open(p, "w").write("\n".join(lines) + "\n")
+    o = oracle_lib.OracleRun(d, ordering=1, pcg_itmax=2000)
+    o.run(2)
+    stamps = [frame(r, 5 if k else 8)[0][1:] for k, r in enumerate(read_records(os.path.join(d, "si3d_3D"))[2:])]
+    assert stamps == [(2024, 12, 31, 2398.0), (2024, 12, 31, 2400.0), (2025, 1, 1, 1.0)]
+
+
+def test_later_first_frame_and_interval(tmp_path, oracle_lib):
+    """ptrack frames every 2 steps from step 4 (itspf = 4), after the initial frame; the header's
+    frame count is (nts - itspf) / ipxml."""
+    from si3d_b200 import synth
+    d = str(tmp_path / "later")
+    synth.make("t0", d, outputs=dict(ipxml=2, itspf=4))
+    o = oracle_lib.OracleRun(d, ordering=1, pcg_itmax=2000)
+    o.run(7)
+    recs = read_records(os.path.join(d, "si3d_3D"))
+    assert struct.unpack("<i", recs[0])[0] == (o.nts - 4) // 2
+    assert [frame(r, 5 if k else 8)[0][0] for k, r in enumerate(recs[2:])] == [0, 4, 6]
+
+
+def test_turbulence_variables_in_ptrack_output_are_refused(tmp_path, oracle_lib, native_libs):
+    """iTurbVars = 1 asks outp for the turbulence fields, which only a closure provides."""
+    import ctypes as C
+    from si3d_b200 import synth
+    d = str(tmp_path / "tv")
+    synth.make("t0", d, outputs=dict(ipxml=1))
+    p = os.path.join(d, "si3d_inp.txt")
+    lines = open(p).read().splitlines()
+    i = lines.index(synth._rec("iTurbVars", 0))
+    lines[i] = synth._rec("iTurbVars", 1)
+    open(p, "w").write("\n".join(lines) + "\n")
+    with pytest.raises(RuntimeError, match="turbulence"):
+        oracle_lib.OracleRun(d)
+    h = native_libs.host()
+    hm = C.c_int(-1)
+    err = C.create_string_buffer(256)
+    assert h.si3d_host_open(d.encode(), None, C.byref(hm), err, 256) == -101
+    assert b"turbulence" in err.value
