@@ -73,3 +73,25 @@ def test_host_reads_the_closure(turb_dirs, native_libs):
     err = C.create_string_buffer(256)
     assert h.si3d_host_open(turb_dirs["t0"].encode(), None, C.byref(hm), err, 256) == 0, err.value
     h.si3d_host_close(hm.value)
+
+
+def test_closure_keeps_a_lake_at_rest_quiet(tmp_path, oracle_lib):
+    """No wind, uniform temperature: the friction velocities vanish, so both boundary rows sit at
+    q2_min; the flow stays below a micrometre per second as without the closure, q2 never rises
+    above its initial maximum, and the closure keeps every eddy coefficient finite."""
+    import dataclasses
+    from si3d_b200 import synth
+    b = dataclasses.replace(synth.config("c0", nsteps=30), wa=0.0, t_top=15.0, t_bottom=15.0, iturb=1)
+    d = str(tmp_path / "rest_turb")
+    synth.write_run(b, d)
+    o = oracle_lib.OracleRun(d, ordering=1, pcg_itmax=2000)
+    q0 = o.get("q2").max()
+    o.run(10)
+    assert np.abs(o.get("s")).max() < 1e-6
+    assert np.abs(o.get("uh")).max() < 1e-4
+    q2 = o.get("q2")[:, :o.lm]
+    assert q2.max() <= q0 * (1 + 1e-12)
+    k1z, kmz = o.geti("k1z")[:o.lm], o.geti("kmz")[:o.lm]
+    c = np.arange(o.lm)
+    assert np.all(q2[k1z - 1, c] == 2e-6)
+    assert np.isfinite(o.get("Av")).all() and np.isfinite(o.get("Dv")).all()
