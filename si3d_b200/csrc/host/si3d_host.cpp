@@ -146,7 +146,8 @@ bool read_parameters(HostModel& M, const std::string& dir) {
   gi(M.itrap); gi(M.niter); gi(M.ismooth); g(M.beta); gi(M.iturb); g(M.Av0); g(M.Dv0); gi(M.iadv); gi(M.itrmom);
   gi(M.ihd); g(M.Ax0); g(M.Ay0); g(M.f); g(M.theta); gi(M.ibc); gi(M.isal); gi(M.itrsca); g(M.cd); gi(M.ifsurfbc);
   g(M.dtsurfbc); gi(M.icw); g(M.cw); g(M.wa); g(M.phi); gi(dummy); gi(dummy);
-  R.skip(3); gi(dummy); gi(dummy); R.skip(2);    // ipt, nnodes, node lists
+  int nnodes = 0;
+  R.skip(3); gi(dummy); gi(nnodes); R.skip(2);   // ipt, nnodes, node lists
   R.skip(3); gi(M.iop); gi(M.itspfh); gi(M.n_planes);
   {   // planes '(14X,20I)'
     const std::string rec = R.take();
@@ -175,6 +176,10 @@ bool read_parameters(HostModel& M, const std::string& dir) {
     M.err = "si3d_inp.txt selects an option outside the semi-implicit core (open boundaries, point "
             "sources, heat budget, turbulence closure, Smagorinsky, smoothing, non-centred advection or "
             "variable layers)";
+    return false;
+  }
+  if (nnodes > 0 || M.ipxml < 0) {
+    M.err = "si3d_inp.txt: the time-series (outt, nnodes > 0) and XML (outs, ipxml < 0) writers are not built";
     return false;
   }
   if (M.ipxml > 0 && M.iTurbVars != 0) {

@@ -135,3 +135,15 @@ def test_tracer_columns_missing_from_profile(native_libs, oracle_lib, run_dirs, 
     native_libs.host().si3d_host_close(hm)
     o = oracle_lib.OracleRun(d)
     assert o.ntr == 2 and not o.get("tracer2").any()
+
+
+@pytest.mark.parametrize("label,value", [("nnodes", 2), ("ipxml", -1)])
+def test_unbuilt_writers_are_refused(native_libs, oracle_lib, run_dirs, tmp_path, label, value):
+    """Time series at nodes (outt) and the XML output (outs) are not built: a run that asks for them
+    is refused instead of running without its files."""
+    d = _copy(run_dirs["t0"], str(tmp_path / f"w_{label}"))
+    _set_records(os.path.join(d, "si3d_inp.txt"), [(label, value)])
+    rc, _, err = _open(native_libs, d)
+    assert rc == -101 and "not built" in err
+    with pytest.raises(RuntimeError, match="not restated"):
+        oracle_lib.OracleRun(d)
