@@ -28,6 +28,8 @@ def main(argv=None) -> int:
     ap.add_argument("--itmax", type=int, default=2000)
     ap.add_argument("--device", type=int, default=0)
     ap.add_argument("--ntr", type=int, default=0, help="conservative tracers added to a synthetic workload")
+    ap.add_argument("--iturb", type=int, default=0, choices=[0, 1],
+                    help="1: a synthetic workload with the Mellor-Yamada 2.5 closure")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the launch shapes of the column stages on the live state first")
     args = ap.parse_args(argv)
@@ -37,10 +39,10 @@ def main(argv=None) -> int:
     build.build_all()
     run_dir = args.run_dir
     if run_dir is None:
-        run_dir = os.path.join(tempfile.gettempdir(), f"si3d_bench_{args.workload}_tr{args.ntr}_r0")
+        run_dir = os.path.join(tempfile.gettempdir(), f"si3d_bench_{args.workload}_tr{args.ntr}_t{args.iturb}_r0")
         marker = os.path.join(run_dir, ".complete")
         if not os.path.exists(marker):
-            synth.make(args.workload, run_dir, ntr=args.ntr)
+            synth.make(args.workload, run_dir, ntr=args.ntr, iturb=args.iturb)
             open(marker, "w").close()
     prec = {"fp64": native.SI3D_FP64, "mixed": native.SI3D_MIXED_IR, "mg": native.SI3D_MIXED_MG}[args.precision]
     run = GpuRun(run_dir, device=args.device, pcg_itmax=args.itmax, precision=prec, autotune=args.autotune)
