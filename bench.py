@@ -151,44 +151,44 @@ def counts(run_dir: str):
     return lm, n3
 
 
-def cpu_sample(name: str, threads: int, steps: int = 0, warmup: int = 0, ntr: int = 0, iturb: int = 0) -> dict:
-    """The CPU restatement of the reference timed on a window of the workload (same layers,
-    bathymetry and forcing generators), extrapolated linearly in wet 3-D cells.  The column stages
-    run on `threads` host threads; the zeta solve is serial, as the reference runs it on thread 0.
-    (Linear extrapolation understates the solve at full size, whose iteration count grows with the
-    domain.)  With `steps`, exactly `warmup` untimed and `steps` timed window steps; otherwise up to
-    20 steps or 10 s."""
-    from si3d_b200 import synth
+def physical_cores() -> int:
+    """Physical cores among the CPUs this process may run on (one thread per core, hyper-threads
+    not counted)."""
+    seen = set()
+    for c in sorted(os.sched_getaffinity(0)):
+        base = f"/sys/devices/system/cpu/cpu{c}/topology/"
+        try:
+            with open(base + "physical_package_id") as f1, open(base + "core_id") as f2:
+                seen.add((f1.read().strip(), f2.read().strip()))
+        except OSError:
+            seen.add(("cpu", c))
+    return max(1, len(seen))
+
+
+def cpu_port_run(name: str, threads: int, steps: int, warmup: int, ntr: int = 0, iturb: int = 0) -> dict:
+    """The CPU restatement of the reference run on the full workload: `warmup` untimed steps, then
+    `steps` timed steps.  Natural-order MIC-CG (the reference's ordering), stopping test 5 at 1e-12;
+    the column stages on `threads` host threads, the zeta solve serial as the reference runs it on
+    OpenMP thread 0 (si3d_procedures.f90:1975-2028).  Only the oracle's library is loaded."""
+    import numpy as np
     from oracle import pyoracle
-    full = synth.config(name)
-    sub = synth.config(name)
-    # central window of the basin, 1/25 of the cells
-    wx, wy = max(full.nx // 5, 16), max(full.ny // 5, 16)
-    x0, y0 = (full.nx - wx) // 2, (full.ny - wy) // 2
-    sub.nx, sub.ny = wx, wy
-    sub.ntr = ntr
-    sub.iturb = iturb
-    sub.depth = full.depth[x0:x0 + wx, y0:y0 + wy].copy()
-    if full.uair is not None:
-        sub.uair = full.uair[x0:x0 + wx, y0:y0 + wy].copy()
-        sub.vair = full.vair[x0:x0 + wx, y0:y0 + wy].copy()
-    d = os.path.join(tempfile.gettempdir(), f"si3d_cpu_window_{name}_tr{ntr}_t{iturb}")
-    synth.write_run(sub, d)
     os.environ["SI3D_ORACLE_THREADS"] = str(threads)   # read once, at the oracle's first column loop
     pyoracle.build()
-    o = pyoracle.OracleRun(d, ordering=1, pcg_itmax=2000)
-    o.run(1 + max(warmup, 0))    # first step: trapezoidal start
-    t0 = time.perf_counter()
-    nsteps = 0
-    while True:
-        o.run(1)
-        nsteps += 1
-        if (steps > 0 and nsteps >= steps) or (steps <= 0 and (time.perf_counter() - t0 > 10.0 or nsteps >= 20)):
-            break
-    dt = (time.perf_counter() - t0) / nsteps
-    lm_w, n3_w = counts(d)
-    return {"window_s_per_step": dt, "window": f"{wx}x{wy} cells of {name}", "lm": lm_w, "n3": n3_w,
-            "steps": nsteps, "iters_per_step": sum(s["iters"] for s in o.solves()[-3 * nsteps:]) / nsteps}
+    d = workload_dir(name, 0, ntr, iturb)
+    o = pyoracle.OracleRun(d, ordering=0, pcg_itmax=2000)
+    try:
+        kmz = o.geti("kmz")
+        lm, n3 = o.lm, int((kmz[:o.lm] - 1).sum())
+        o.run(max(warmup, 0))
+        n0 = len(o.solves())
+        t0 = time.perf_counter()
+        o.run(steps)
+        dt = (time.perf_counter() - t0) / steps
+        sv = o.solves()[n0:]
+        return {"s_per_step": dt, "lm": lm, "n3": n3, "steps": steps, "warmup": warmup,
+                "iters_per_step": sum(s["iters"] for s in sv) / steps}
+    finally:
+        o.close()
 
 
 def step_roofline(form: dict, lm: int, n3: int, peak: float, peak_kind: str) -> dict:
@@ -294,21 +294,22 @@ def main() -> int:
     if args.impl == "reference":
         if rank != 0:
             return 0
-        threads = os.cpu_count() or 1
-        lm_full, n3_full = counts(workload_dir(args.workload, 0, args.ntr, args.iturb))
-        smp = cpu_sample(args.workload, threads, steps=args.steps, warmup=args.warmup, ntr=args.ntr, iturb=args.iturb)
-        v = smp["window_s_per_step"] * n3_full / smp["n3"]
+        threads = physical_cores()
+        smp = cpu_port_run(args.workload, threads, args.steps, args.warmup, ntr=args.ntr, iturb=args.iturb)
+        v = smp["s_per_step"]
         line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "s/timestep", "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {"workload": WORKLOAD_DESC.get(args.workload, args.workload), "form": "plain_fp64",
                            "ntr": args.ntr, "iturb": args.iturb,
-                           "lm": lm_full, "n3": n3_full, "parallelism": "replicas x1",
+                           "lm": smp["lm"], "n3": smp["n3"], "parallelism": "replicas x1",
                            "l2": "host run; no GPU caches involved"},
+                "pcg_iters_per_step": smp["iters_per_step"],
                 "cpu_baseline": {"value": v, "unit": "s/timestep", "cores": threads, "kind": "port",
-                                 "sample": f"{smp['steps']} steps of a {smp['window']} window, extrapolated by wet "
-                                           f"3-D cells ({smp['n3']} -> {n3_full}); column stages on {threads} threads, "
-                                           f"the zeta solve serial as in the reference"},
+                                 "sample": f"the full workload, {smp['warmup']} untimed and {smp['steps']} timed "
+                                           f"steps; natural-order MIC-CG (the reference's ordering) at 1e-12; column "
+                                           f"stages on {threads} threads (one per physical core), the zeta solve "
+                                           f"serial as in the reference"},
                 "e2e": {"value": v, "unit": "s/timestep", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         return 0
@@ -459,13 +460,13 @@ def main() -> int:
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        threads = os.cpu_count() or 1
-        smp = cpu_sample(args.workload, threads, ntr=args.ntr, iturb=args.iturb)
-        v = smp["window_s_per_step"] * n3 / smp["n3"]
+        threads = physical_cores()
+        smp = cpu_port_run(args.workload, threads, steps=2, warmup=1, ntr=args.ntr, iturb=args.iturb)
+        v = smp["s_per_step"]
         cpu = {"value": v, "unit": "s/timestep", "cores": threads, "kind": "port",
-               "sample": f"{smp['steps']} steps of a {smp['window']} window (plain FP64, red-black MIC-PCG at 1e-12), "
-                         f"extrapolated by wet 3-D cells ({smp['n3']} -> {n3}); column stages on {threads} threads, "
-                         f"the zeta solve serial as in the reference"}
+               "sample": f"the full workload, 1 untimed and 2 timed steps (plain FP64, natural-order MIC-CG at 1e-12, "
+                         f"{smp['iters_per_step']:.1f} CG iterations per step); column stages on {threads} threads "
+                         f"(one per physical core), the zeta solve serial as in the reference"}
 
     if rank == 0:
         plain = res.get("plain_fp64", head)

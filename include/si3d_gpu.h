@@ -219,10 +219,12 @@ int si3d_gpu_counters(int handle, long long* launches, double* stage_ms, long lo
  * buffers in layer-major order (element k of system s at k*nsys + s); the sweep's scratch is a
  * fixed array inside the library, so n*nsys must not exceed SI3D_NOALLOC_MAX_ELEMS (larger
  * problems return SI3D_ECAPACITY without touching the GPU).  The library image keeps that 8 MiB
- * array on every GPU that loads it until the process exits.  The first call on a device looks the
- * array's address up (make it before any stream capture).  All calls share the array, so calls
- * whose kernels overlap on one GPU race.  Work is queued on `stream` (a cudaStream_t, NULL = the
- * default stream) and the call returns after that stream has finished it. */
+ * array on every GPU that loads it until the process exits.  Every call looks the array's address
+ * up in the current context.  All calls share the array, so calls whose kernels overlap on one GPU
+ * race: serialise them, for example on one stream.  Work is queued on `stream` (a cudaStream_t,
+ * NULL = the default stream) and the call returns after that stream has finished it, so the call
+ * cannot be made on a stream that is capturing a CUDA graph.  A CUDA error already pending when
+ * the call starts is reported as SI3D_ECUDA (and left pending) without launching anything. */
 #define SI3D_NOALLOC_MAX_ELEMS (1 << 20)
 int si3d_gpu_column_tridiag_noalloc(int n, int nsys, const double* a, const double* b, const double* c,
                                    const double* g, const double* r, double* ag, double* ar, void* stream);
@@ -239,6 +241,13 @@ int si3d_gpu_set_tune(int handle, const int* choice);
 
 /* Wait for the handle's stream. */
 int si3d_gpu_sync(int handle);
+/* Test hook for the bounded device waits (no counterpart in the reference).  The next cooperative
+ * zeta-solve launch of this handle (FP64 or FP32 MIC loop, or the multigrid solve) waits at each
+ * grid barrier for `absent_blocks` blocks beyond its grid - blocks that do not exist - and gives up
+ * after `polls` polls (1 .. 2^26) instead of the built-in limit.  That solve then ends with
+ * SI3D_ETIMEOUT through the call that ran it, and the handle stays usable.  Applies once.
+ * SI3D_EDIMS for out-of-range arguments or a handle whose steps are being captured in a graph. */
+int si3d_gpu_test_wait_limit(int handle, long long polls, int absent_blocks);
 /* Human-readable text for an error code. */
 const char* si3d_gpu_strerror(int code);
 /* Free the device state of a handle. */

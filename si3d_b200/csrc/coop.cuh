@@ -1,9 +1,9 @@
 // Helpers of the cooperative (grid-barrier) kernels: block sums in a fixed order, every-block
 // reduction of block partials, and a counting grid barrier with a bounded wait.
 //
-// Every barrier wait is bounded: after kSpinLimit polls a block records SI3D_ETIMEOUT as the
-// solve's ier, raises the barrier's abort flag and returns false; the other blocks see the flag at
-// their next wait and return too, so a kernel built on it always ends.
+// Every barrier wait is bounded: after kSpinLimit polls (or the barrier record's own limit) a block
+// records SI3D_ETIMEOUT as the solve's ier, raises the barrier's abort flag and returns false; the
+// other blocks see the flag at their next wait and return too, so a kernel built on it always ends.
 #pragma once
 #include "../../include/si3d_gpu.h"
 #include "kernels.h"
@@ -64,17 +64,21 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, int* s_f
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
+    // zero in every solve; a test sets them to make the wait run out
+    const unsigned int absent = __ldcg(&bar->absent);
+    const unsigned long long lim = __ldcg(&bar->limit);
+    const long long limit = lim ? (long long)lim : kSpinLimit;
     const unsigned int gen = ld_acquire(&bar->gen);
     __threadfence();
     const unsigned int arrived = atomicAdd(&bar->count, 1u);
-    if (arrived == gridDim.x - 1) {
+    if (arrived == gridDim.x - 1 + absent) {
       atomicExch(&bar->count, 0u);
       __threadfence();
       atomicAdd(&bar->gen, 1u);
     } else {
       long long spins = 0;
       while (ld_acquire(&bar->gen) == gen) {
-        if (++spins > kSpinLimit || ld_acquire(&bar->abort) != 0u) { ok = 0; break; }
+        if (++spins > limit || ld_acquire(&bar->abort) != 0u) { ok = 0; break; }
         __nanosleep(32);
       }
     }

@@ -466,8 +466,12 @@ void mg_setup(const Dev& d, const MgDev& M, int x0_mode, const double* dz, const
   }
 }
 
-int mg_solve(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st) {
-  if (cudaMemsetAsync(bar, 0, sizeof(GridBar), st) != cudaSuccess) return -1;
+int mg_solve(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st, const GridBar* init) {
+  if (init) {
+    if (cudaMemcpyAsync(bar, init, sizeof(GridBar), cudaMemcpyHostToDevice, st) != cudaSuccess) return -1;
+  } else if (cudaMemsetAsync(bar, 0, sizeof(GridBar), st) != cudaSuccess) {
+    return -1;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nblocks);
   cfg.blockDim = dim3(MQ);

@@ -357,8 +357,12 @@ __global__ void __launch_bounds__(PQB, 1) k_pcg_loop(PcgDevT<T> P, GridBar* bar)
 // Cooperative launch (all blocks co-resident) through cudaLaunchKernelEx, which stream capture
 // records as a cooperative kernel node.
 template <typename T>
-int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st) {
-  if (cudaMemsetAsync(bar, 0, sizeof(GridBar), st) != cudaSuccess) return -1;
+int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st, const GridBar* init) {
+  if (init) {
+    if (cudaMemcpyAsync(bar, init, sizeof(GridBar), cudaMemcpyHostToDevice, st) != cudaSuccess) return -1;
+  } else if (cudaMemsetAsync(bar, 0, sizeof(GridBar), st) != cudaSuccess) {
+    return -1;
+  }
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(nblocks);
   cfg.blockDim = dim3(PQB);
@@ -394,12 +398,12 @@ int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32) {
   return std::max(1, std::min(sms * std::max(per_sm, 1), need));
 }
 
-int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st) {
-  return launch_loop<double>(P, bar, nblocks, test2, st);
+int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st, const GridBar* init) {
+  return launch_loop<double>(P, bar, nblocks, test2, st, init);
 }
 
-int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st) {
-  return launch_loop<float>(F, bar, nblocks, false, st);
+int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st, const GridBar* init) {
+  return launch_loop<float>(F, bar, nblocks, false, st, init);
 }
 
 }  // namespace si3d

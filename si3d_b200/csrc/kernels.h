@@ -75,12 +75,18 @@ void ir_correct(const PcgDev& P, const PcgDevF& F, cudaStream_t st);
 
 // Whole solve in one cooperative launch (k_pcg_persistent.cu).  The barrier state is reset by
 // every launch.
+// Grid barrier record, zeroed before every cooperative launch.  `absent` (blocks the barrier waits
+// for beyond the grid) and `limit` (polls before a wait gives up; 0 = the built-in limit) are zero in
+// every solve; a test sets them through si3d_gpu_test_wait_limit to make a wait run out.
 struct GridBar {
-  unsigned int count, gen, abort, pad;
+  unsigned int count, gen, abort, absent;
+  unsigned long long limit, pad;
 };
 int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32);
-int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st);   // test2: stopping test 2
-int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st);
+// `init` (host memory, optional) replaces the zeroed barrier record of this launch
+int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st,
+             const GridBar* init = nullptr);   // test2: stopping test 2
+int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st, const GridBar* init = nullptr);
 
 void launch_slayer_h(const Dev& d, cudaStream_t st);
 void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cudaStream_t st);

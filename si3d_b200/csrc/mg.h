@@ -64,7 +64,7 @@ size_t mg_level_elems(int rows, int cols);   // floats of one array of a rows x 
 int mg_loop_blocks(int device, int cells0, int max_per_sm);
 // the FP64 system, level 0 and the coarser levels from matcon's sx, sy, qq and the initial guess
 void mg_setup(const Dev& d, const MgDev& M, int x0_mode, const double* dz, const double* hist, cudaStream_t st);
-int mg_solve(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st);     // the cooperative solve
+int mg_solve(const MgDev& M, GridBar* bar, int nblocks, cudaStream_t st, const GridBar* init = nullptr);     // the cooperative solve
 void mg_finish(const Dev& d, const MgDev& M, double* hist, cudaStream_t st);  // s(l) = u (and hist)
 
 }  // namespace si3d

@@ -8,14 +8,13 @@
 //
 // The array is a file-scope __device__ variable: every GPU that loads the library holds its
 // 8 MiB until the process exits.  Host code cannot use the name of the array as a device address,
-// so the first call on each device looks the address up with cudaGetSymbolAddress while that
-// device is current and caches it; make that first call before any stream capture.  Every call
-// shares the one array: the forward sweep writes each scratch element before the backward sweep
-// reads it, so nothing has to be cleared between calls, but two calls whose kernels overlap on
-// the same GPU race on it.
+// so every call looks the address up with cudaGetSymbolAddress in the context that is current at
+// that moment (a cached address could belong to another context of the same device, or to a module
+// image that a device reset has since replaced); the lookup is cheap next to the synchronisation
+// that ends the call.  Every call shares the one array: the forward sweep writes each scratch
+// element before the backward sweep reads it, so nothing has to be cleared between calls, but two
+// calls whose kernels overlap on the same GPU race on it.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "../../include/si3d_gpu.h"
 #include "kernels.h"
@@ -24,25 +23,6 @@ namespace {
 
 static __device__ __align__(256) double g_trid_scratch[SI3D_NOALLOC_MAX_ELEMS];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-double* g_scratch_addr[kMaxDevices] = {nullptr};
-
-// Device address of the scratch array on the current device (looked up once per device).
-int scratch_address(double** out) {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return SI3D_ENODEV;
-  if (dev < 0 || dev >= kMaxDevices) return SI3D_ENODEV;
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    if (cudaGetSymbolAddress(&p, g_trid_scratch) != cudaSuccess || !p) return SI3D_ECUDA;
-    g_scratch_addr[dev] = static_cast<double*>(p);
-  }
-  *out = g_scratch_addr[dev];
-  return 0;
-}
-
 }  // namespace
 
 extern "C" int si3d_gpu_column_tridiag_noalloc(int n, int nsys, const double* a, const double* b, const double* c,
@@ -50,12 +30,14 @@ extern "C" int si3d_gpu_column_tridiag_noalloc(int n, int nsys, const double* a,
                                                void* stream) {
   if (n < 1 || nsys < 1 || !a || !b || !c || !g || !r || !ag || !ar) return SI3D_EDIMS;
   if ((long long)n * (long long)nsys > (long long)SI3D_NOALLOC_MAX_ELEMS) return SI3D_ECAPACITY;
-  double* scratch = nullptr;
-  const int rc = scratch_address(&scratch);
-  if (rc) return rc;
+  // An error left pending by the caller's earlier work is reported, not cleared, and nothing is
+  // launched on top of it.
+  if (cudaPeekAtLastError() != cudaSuccess) return SI3D_ECUDA;
+  void* scratch = nullptr;
+  if (cudaGetSymbolAddress(&scratch, g_trid_scratch) != cudaSuccess || !scratch) return SI3D_ECUDA;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
-  si3d::launch_column_tridiag(n, nsys, a, b, c, g, r, ag, ar, scratch, st);
-  if (cudaGetLastError() != cudaSuccess) return SI3D_ECUDA;
+  si3d::launch_column_tridiag(n, nsys, a, b, c, g, r, ag, ar, static_cast<double*>(scratch), st);
+  if (cudaPeekAtLastError() != cudaSuccess) return SI3D_ECUDA;
   if (cudaStreamSynchronize(st) != cudaSuccess) return SI3D_ECUDA;
   return 0;
 }

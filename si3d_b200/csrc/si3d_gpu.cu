@@ -96,6 +96,9 @@ struct Ctx {
   bool persistent = true;
   int loop_blocks = 0, loop_blocks_f = 0;   // FP64 / FP32 grids of the cooperative solve
   GridBar* bar = nullptr;
+  // si3d_gpu_test_wait_limit: barrier record for the next cooperative solve launch only
+  GridBar bar_test{};
+  bool bar_test_armed = false;
   bool log_solves = false;   // SI3D_LOG_SOLVES=1: per-solve iteration counts on stderr
   int cur_istep = 1;         // istep of the fd call in progress (1 = leapfrog, 2 = trapezoidal)
   // solve slot within a step (0 = leapfrog, 1.. = trapezoidal iterations, clamped to kHistSlots - 1)
@@ -183,6 +186,13 @@ struct Ctx {
 
 std::mutex g_mu;
 std::vector<Ctx*> g_ctx;
+
+// The barrier record armed by si3d_gpu_test_wait_limit, once (nullptr: the zeroed record).
+const GridBar* take_bar_test(Ctx* c) {
+  if (!c->bar_test_armed) return nullptr;
+  c->bar_test_armed = false;
+  return &c->bar_test;
+}
 
 Ctx* get(int h) {
   std::lock_guard<std::mutex> lk(g_mu);
@@ -639,8 +649,9 @@ int refine(Ctx* c, int* total_inner) {
     CK(cudaMemcpyAsync(c->pcgf.sc, c->h_scf, sizeof(PcgScal), cudaMemcpyHostToDevice, c->st));
     int rci = iterate(c, c->pcgf.sc, c->h_scf, p.pcg_itmax, c->last_inner,
                       [&](int par) { pcg_iteration_f(c->pcgf, par, c->st); },
-                      [&] { return pcg_loop_f(c->pcgf, c->bar, c->loop_blocks_f, c->st); });
+                      [&] { return pcg_loop_f(c->pcgf, c->bar, c->loop_blocks_f, c->st, take_bar_test(c)); });
     if (rci) return rci;
+    if (c->h_scf->ier == SI3D_ETIMEOUT) return SI3D_ETIMEOUT;
     const int its = c->h_scf->in;
     if (c->log_solves) std::fprintf(stderr, "si3d: inner FP32 MIC solve %d: %d iterations\n", outer + 1, its);
     inner_total += its;
@@ -667,7 +678,7 @@ int solve_mg(Ctx* c, const PcgScal& init, int x0, double* hist, int ier, int* it
   int rc = stage(c, ST_PCG_SETUP, c->mg.nlev, [&] { mg_setup(c->d, c->mg, x0, c->dz, hist, c->st); });
   if (rc) return rc;
   if (c->prof) CK(cudaEventRecord(c->pe0, c->st));
-  if (mg_solve(c->mg, c->bar, c->mg_blocks, c->st) != 0) return cuda_fail(cudaGetLastError(), "mg_solve", __LINE__);
+  if (mg_solve(c->mg, c->bar, c->mg_blocks, c->st, take_bar_test(c)) != 0) return cuda_fail(cudaGetLastError(), "mg_solve", __LINE__);
   c->launches += 1;
   CK(cudaMemcpyAsync(c->h_sc, c->mg.sc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
@@ -767,7 +778,9 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
     // run iterations in batches; every kernel returns at once after convergence
     int rci = iterate(c, c->pcg.sc, c->h_sc, p.pcg_itmax, c->last_iters,
                       [&](int par) { pcg_iteration(c->pcg, par, c->st); },
-                      [&] { return pcg_loop(c->pcg, c->bar, c->loop_blocks, c->prm.pcg_test == 2, c->st); });
+                      [&] {
+                        return pcg_loop(c->pcg, c->bar, c->loop_blocks, c->prm.pcg_test == 2, c->st, take_bar_test(c));
+                      });
     if (rci) return rci;
     total_iters = c->h_sc->in;
     c->last_iters = std::max(total_iters, 1);
@@ -1780,6 +1793,18 @@ int si3d_gpu_counters(int h, long long* launches, double* stage_ms, long long* s
     if (stage_n) stage_n[i] = c->prof_n[i];
   }
   return ST_COUNT;
+}
+
+int si3d_gpu_test_wait_limit(int h, long long polls, int absent_blocks) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (polls < 1 || polls > (1LL << 26) || absent_blocks < 0 || absent_blocks > 1024) return SI3D_EDIMS;
+  if (!c->persistent || c->graph_mode) return SI3D_EDIMS;
+  c->bar_test = GridBar{};
+  c->bar_test.absent = (unsigned int)absent_blocks;
+  c->bar_test.limit = (unsigned long long)polls;
+  c->bar_test_armed = true;
+  return 0;
 }
 
 int si3d_gpu_sync(int h) {

@@ -4,7 +4,8 @@ The reference ships no golden data for its semi-implicit core, so these fixtures
 own outputs on small seeded inputs: they pin the oracle against accidental change (CPU tests) and
 let the GPU tests check the CUDA path against stored numbers without running the oracle.
 
-  python tests/golden/make_golden.py
+  python tests/golden/make_golden.py        # the small fixtures (seconds)
+  python tests/golden/make_golden.py c1     # the 1000-step c1 fixture (about an hour on 6 threads)
 """
 import dataclasses
 import os
@@ -53,8 +54,45 @@ def pcg_fixture():
     return dict(coef=coef, jcoef=jcoef, rhs=b, x=x, iters=np.int32(info["iters"]), stptst=info["stptst"])
 
 
+C1_STEPS = 1000
+C1_SAMPLE_COLUMNS = 2048
+C1_SAMPLE_SEED = 1000
+
+
+def c1_fixture(steps: int = C1_STEPS, threads: int = 6):
+    """The 1000 x 500 x 40 workload (seeded random bathymetry and wind stress, dt = 30 s) run for
+    `steps` steps by the oracle with the reference's own solver settings apart from the tolerance:
+    natural-order MIC-CG, stopping test 5 at 1e-12.  Stored: zeta on every wet column, uh, vh and
+    sal at every layer of a seeded sample of wet columns, the per-solve iteration counts and
+    stopping values, and max |zeta| after every step (the run's stability record)."""
+    os.environ.setdefault("SI3D_ORACLE_THREADS", str(threads))
+    d = os.path.join(tempfile.mkdtemp(), "c1")
+    b = synth.make("c1", d)
+    o = pyoracle.OracleRun(d, ordering=0, pcg_itmax=2000)
+    zmax = np.empty(steps)
+    for n in range(steps):
+        o.run(1)
+        zmax[n] = np.abs(o.get("s")[:o.lm]).max()
+    cols = np.sort(np.random.default_rng(C1_SAMPLE_SEED).choice(o.lm, C1_SAMPLE_COLUMNS, replace=False))
+    out = {"s": o.get("s")[:o.lm].copy(), "columns": cols.astype(np.int32)}
+    for f in ("uh", "vh", "sal"):
+        out[f] = o.get(f)[:, cols].copy()
+        out[f + "_scale"] = np.float64(np.abs(o.get(f)[:, :o.lm]).max())
+    sv = o.solves()
+    out["iters"] = np.array([s["iters"] for s in sv], dtype=np.int32)
+    out["ier"] = np.array([s["ier"] for s in sv], dtype=np.int32)
+    out["stptst"] = np.array([s["stptst"] for s in sv])
+    out["zeta_max"] = zmax
+    out["steps"] = np.int32(steps)
+    out["seeds"] = np.array([b.seeds["bathymetry"], b.seeds["wind"]], dtype=np.int64)
+    return out
+
+
 def main():
     pyoracle.build()
+    if sys.argv[1:] == ["c1"]:
+        np.savez_compressed(os.path.join(HERE, f"c1_oracle_{C1_STEPS}steps.npz"), **c1_fixture())
+        return
     np.savez_compressed(os.path.join(HERE, f"t0_oracle_{STEPS}steps.npz"), **run_fixture("t0"))
     np.savez_compressed(os.path.join(HERE, f"t1_oracle_{STEPS}steps.npz"), **run_fixture("t1", fields_3d=()))
     np.savez_compressed(os.path.join(HERE, "pcg_48x32.npz"), **pcg_fixture())

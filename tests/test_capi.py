@@ -22,7 +22,8 @@ def test_headers_declare_the_boundary():
     gpu = _declared(os.path.join(ROOT, "include", "si3d_gpu.h"))
     host = _declared(os.path.join(ROOT, "include", "si3d_host.h"))
     for name in ("si3d_gpu_init", "si3d_gpu_fd", "si3d_gpu_settrap", "si3d_gpu_settrap2", "si3d_gpu_save",
-                 "si3d_gpu_solve_zeta", "si3d_gpu_column_tridiag", "si3d_gpu_strerror", "si3d_gpu_finalize"):
+                 "si3d_gpu_solve_zeta", "si3d_gpu_column_tridiag", "si3d_gpu_column_tridiag_noalloc",
+                 "si3d_gpu_strerror", "si3d_gpu_finalize"):
         assert name in gpu
     assert "si3d_host_open" in host and "si3d_host_run" in host
 

@@ -26,6 +26,17 @@ def _system(rng, n, nsys):
     return a, b, c, g, r
 
 
+def _banded(a, b, c, rhs, s):
+    """System s solved by LAPACK's banded solver (an independent check of both entry points)."""
+    from scipy.linalg import solve_banded
+    n = a.shape[0]
+    ab = np.zeros((3, n))
+    ab[0, 1:] = c[:-1, s]
+    ab[1] = b[:, s]
+    ab[2, :-1] = a[1:, s]
+    return solve_banded((1, 1), ab, rhs[:, s])
+
+
 def test_noalloc_matches_allocating_entry(native_libs):
     import torch
 
@@ -34,10 +45,14 @@ def test_noalloc_matches_allocating_entry(native_libs):
 
     lib = native.gpu()
     rng = np.random.default_rng(20261203)
-    # two calls in a row with different shapes: the second reuses the scratch the first filled
-    for n, nsys in ((62, 9000), (41, 16384)):
+    # three calls in a row with different shapes: each reuses the scratch the one before filled; the
+    # last fills the array exactly (n * nsys == SI3D_NOALLOC_MAX_ELEMS)
+    for n, nsys in ((62, 9000), (41, 16384), (64, 16384)):
         a, b, c, g, r = _system(rng, n, nsys)
         ag_ref, ar_ref = column_tridiag(a, b, c, g, r)
+        for s in rng.choice(nsys, 16, replace=False):
+            np.testing.assert_allclose(ag_ref[:, s], _banded(a, b, c, g, s), rtol=1e-12, atol=1e-14)
+            np.testing.assert_allclose(ar_ref[:, s], _banded(a, b, c, r, s), rtol=1e-12, atol=1e-14)
         # caller-owned device buffers, layer-major: element k of system s at k*nsys + s
         dev = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (a, b, c, g, r)]
         ag = torch.empty((n, nsys), dtype=torch.float64, device="cuda")
