@@ -164,19 +164,22 @@ def pcg(coef, jcoef, rhs, x0, *, pcg_test=5, tol=1e-12, itmax=200, ordering=0, s
 
 def trid(a, b, c, g, r):
     n = len(a)
+    # every array handed to the library is bound to a name, so it outlives the call
     aa = np.asfortranarray(np.stack([a, b, c]), dtype=np.float64)
+    gc = np.ascontiguousarray(g, dtype=np.float64)
+    rc = np.ascontiguousarray(r, dtype=np.float64)
     ag = np.empty(n)
     ar = np.empty(n)
-    lib().orc_trid(n, _p(aa), _p(np.ascontiguousarray(g, dtype=np.float64)), _p(np.ascontiguousarray(r, dtype=np.float64)),
-                   _p(ag), _p(ar))
+    lib().orc_trid(n, _p(aa), _p(gc), _p(rc), _p(ag), _p(ar))
     return ag, ar
 
 
 def trid1(a, b, c, d):
     n = len(a)
     aa = np.asfortranarray(np.stack([a, b, c]), dtype=np.float64)
+    dc = np.ascontiguousarray(d, dtype=np.float64)
     x = np.empty(n)
-    lib().orc_trid1(n, _p(aa), _p(np.ascontiguousarray(d, dtype=np.float64)), _p(x))
+    lib().orc_trid1(n, _p(aa), _p(dc), _p(x))
     return x
 
 

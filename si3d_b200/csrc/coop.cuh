@@ -12,7 +12,7 @@ namespace si3d {
 namespace coop {
 
 constexpr int QB = 256;                       // threads per block
-constexpr long long kSpinLimit = 1LL << 26;   // polls (>= 32 ns each) before a wait gives up: > 2 s
+constexpr long long kSpinLimit = 1LL << 23;   // polls (an L2 round trip each) before a wait gives up: > 2 s
 
 __device__ __forceinline__ unsigned int ld_acquire(const unsigned int* p) {
   unsigned int v;
@@ -58,9 +58,28 @@ __device__ __forceinline__ void all_partials(const double* part, int n, int stri
   bsum<NV, BS>(v, sh);
 }
 
-// Counting grid barrier with a bounded wait.  Returns false (in every thread of the block) once
-// any block has given up.
-__device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, int* s_flag) {
+// Per-block state of the grid barrier, in shared memory: the outcome of the last wait and the
+// number of barriers this block has passed.  Zero `epoch` (thread 0) before the first barrier.
+struct BarSt {
+  int ok;
+  unsigned int epoch;
+};
+
+__device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ void red_release_add(unsigned long long* p, unsigned long long v) {
+  asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// Grid barrier on a monotonic arrival counter: barrier e (1, 2, ...) of the launch is passed once
+// the counter reaches e * (blocks + absent).  An arrival is one release-add (no round trip, no
+// reset); the wait polls with acquire loads.  Bounded: returns false (in every thread of the block)
+// once this block gave up or any block has.
+__device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, BarSt* st) {
   __syncthreads();
   if (threadIdx.x == 0) {
     int ok = 1;
@@ -68,29 +87,23 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, int* s_f
     const unsigned int absent = __ldcg(&bar->absent);
     const unsigned long long lim = __ldcg(&bar->limit);
     const long long limit = lim ? (long long)lim : kSpinLimit;
-    const unsigned int gen = ld_acquire(&bar->gen);
+    const unsigned int e = ++st->epoch;
+    const unsigned long long target = (unsigned long long)e * (gridDim.x + absent);
     __threadfence();
-    const unsigned int arrived = atomicAdd(&bar->count, 1u);
-    if (arrived == gridDim.x - 1 + absent) {
-      atomicExch(&bar->count, 0u);
-      __threadfence();
-      atomicAdd(&bar->gen, 1u);
-    } else {
-      long long spins = 0;
-      while (ld_acquire(&bar->gen) == gen) {
-        if (++spins > limit || ld_acquire(&bar->abort) != 0u) { ok = 0; break; }
-        __nanosleep(32);
-      }
+    red_release_add(&bar->count, 1ull);
+    long long spins = 0;
+    while (ld_acquire64(&bar->count) < target) {
+      if (++spins > limit || ((spins & 15) == 0 && ld_acquire(&bar->abort) != 0u)) { ok = 0; break; }
     }
     if (!ok && atomicExch(&bar->abort, 1u) == 0u) {
       sc->ier = SI3D_ETIMEOUT;
       sc->done = 1;
     }
     __threadfence();
-    *s_flag = ok;
+    st->ok = ok;
   }
   __syncthreads();
-  return *s_flag != 0;
+  return st->ok != 0;
 }
 
 }  // namespace coop

@@ -207,7 +207,7 @@ __device__ __forceinline__ void restrict_residual(const MgLevel& F, const MgLeve
 // FP32 MG-PCG on level 0 from e = 0 (M.u) with right-hand side r (level 0's b), until
 // ||r|| < bnorm * zeta or itmax iterations.  Returns false when a barrier gave up (the caller returns
 // at once); otherwise its = the iterations taken and ier = 0, 1 (itmax) or -6 / -7 (breakdown).
-__device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* bar, PcgScal* SC, int* s_flag,
+__device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* bar, PcgScal* SC, BarSt* s_flag,
                        double* sh, double zeta, double bnorm, int itmax, int& its, int& ier) {
   const int nb = gridDim.x, stride = nb * MQ, g0 = blockIdx.x * MQ + threadIdx.x;
   double* const rr_part = M.part;
@@ -362,8 +362,9 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
 // ---------------------------------------------------------------- the whole solve
 __global__ void __launch_bounds__(MQ, 1) k_mg_solve(MgDev M, GridBar* bar) {
   __shared__ double sh[(MQ / 32) * 2 + 2];
-  __shared__ int s_flag;
+  __shared__ BarSt s_flag;
   __shared__ MgLevel s_lv[kMgMaxLevels];
+  if (threadIdx.x == 0) s_flag.epoch = 0;
   const int nlev = M.nlev;
   if (threadIdx.x < nlev) s_lv[threadIdx.x] = M.lv[threadIdx.x];
   __syncthreads();

@@ -162,7 +162,8 @@ __device__ __noinline__ void lz_chgcon(PcgScal* S, double* tri, int ip, double a
 template <typename T, bool TEST2>
 __global__ void __launch_bounds__(PQB, 1) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
   __shared__ double sh[(PQB / 32) * 4 + 4];
-  __shared__ int s_flag;
+  __shared__ BarSt s_flag;
+  if (threadIdx.x == 0) s_flag.epoch = 0;
   const PcgColorT<T> &R = P.R, &B = P.B;
   PcgScal* SC = P.sc;
   const int nb = gridDim.x;

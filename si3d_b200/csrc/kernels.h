@@ -79,7 +79,8 @@ void ir_correct(const PcgDev& P, const PcgDevF& F, cudaStream_t st);
 // for beyond the grid) and `limit` (polls before a wait gives up; 0 = the built-in limit) are zero in
 // every solve; a test sets them through si3d_gpu_test_wait_limit to make a wait run out.
 struct GridBar {
-  unsigned int count, gen, abort, absent;
+  unsigned long long count;        // arrivals since the launch (never reset within it)
+  unsigned int abort, absent;
   unsigned long long limit, pad;
 };
 int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32);

@@ -230,7 +230,7 @@ def iterations(run_dir: str, steps: int, *, params: Optional[np.ndarray], x0_mod
     run = GpuRun(run_dir, device=device, pcg_itmax=2000, x0_mode=x0_mode, precision=precision)
     try:
         if params is not None:
-            native.check(native.gpu().si3d_learn_set_params(run.gh, C.c_void_p(np.ascontiguousarray(params).ctypes.data)))
+            run.set_net(params)
         st = run.run(warmup + steps)[warmup:]
         its = [s.iters[i] for s in st for i in range(s.nsolves)]
         return dict(iters=its, iters_per_step=sum(its) / steps, max_relres=max(s.relres[i] for s in st
