@@ -19,6 +19,7 @@ namespace {
 
 
 constexpr int TB = 128;
+constexpr int BK_TRIP = 2;   // layers a lane handles per trip of the bookkeeping passes
 
 __device__ __forceinline__ bool ewet(const Dev& d, int l) { return NB(d.g.lEC, l) != d.g.lm1; }
 __device__ __forceinline__ bool nwet(const Dev& d, int l) { return NB(d.g.lNC, l) != d.g.lm1; }
@@ -488,37 +489,35 @@ __global__ void __launch_bounds__(32 * CLN) k_vel2(Dev d) {
 }
 
 // ------------------------------------------------------------- settrap / settrap2 / save
-// zeta at n+1/2 (settrap: rotate n -> n-1 first; settrap2: recompute only)
+// zeta at n+1/2 (settrap: spp <- sp first; settrap2: recompute only)
 __global__ void k_half_zeta(Dev d, int rotate) {
-  double* __restrict__ f_hp = d.f.hp;
-  double* __restrict__ f_hpp = d.f.hpp;
-  double* __restrict__ f_hup = d.f.hup;
-  double* __restrict__ f_hupp = d.f.hupp;
-  double* __restrict__ f_hvp = d.f.hvp;
-  double* __restrict__ f_hvpp = d.f.hvpp;
   const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
   if (l > d.g.lm) return;
-  if (rotate) {
-    d.s.spp[l - 1] = d.s.sp[l - 1];
-    const int zL = zlim(d, l), uL = ulim(d, l), vL = vlim(d, l);
-    #pragma unroll 4
-    for (int k = 1; k <= zL; ++k) f_hpp[IX(d, k, l)] = f_hp[IX(d, k, l)];
-    #pragma unroll 4
-    for (int k = 1; k <= uL; ++k) f_hupp[IX(d, k, l)] = f_hup[IX(d, k, l)];
-    #pragma unroll 4
-    for (int k = 1; k <= vL; ++k) f_hvpp[IX(d, k, l)] = f_hvp[IX(d, k, l)];
-  }
+  if (rotate) d.s.spp[l - 1] = d.s.sp[l - 1];
   d.s.sp[l - 1] = 0.5 * (d.s.s[l - 1] + d.s.spp[l - 1]);
 }
 
+// Bookkeeping kernels are cell-parallel: block = 32 consecutive columns x CLN layer lanes, a lane
+// taking layers k0 + lane, k0 + lane + CLN, ...  Every routine of a call (the pp rotation, the
+// thicknesses, the scalar with its density, both velocities) is one pass over the layers in which a
+// cell's loads are all issued before any of its arithmetic, and a lane handles BK_TRIP layers per
+// trip, so a trip costs one memory round trip for all of them.  The expressions are the
+// reference's, so the state is bit-identical to the per-routine loops.
+
+// Values of one cell (k, l) that settrap / settrap2 read.
+struct HalfIn {
+  double hp, hup, hvp, sal, salq, uh, uhq, up, vh, vhq, vp;   // q: salp/uhp/vhp (rotate) or the pp level
+};
+
 // settrap / settrap2 body after the zeta update (layer_hp2, TopLayerIndexp2, scalars at n+1/2 with
-// densty_s, velocities at n+1/2), cell-parallel: block = 32 columns x CLN layer lanes.  The first wet
-// layer of each column (TopLayerIndexp2) is the minimum over the lanes, reduced in shared memory;
-// the surface corrections at the new k1u/k1v run after a block barrier, once every layer's average
-// is in place.
-template <int CLN>
-__global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
+// densty_s, velocities at n+1/2) with settrap's rotation n -> n-1 of h, s, u, v (ROT).  The first
+// wet layer of each column (TopLayerIndexp2) is the minimum over the lanes, reduced in shared
+// memory; the surface corrections at the new k1u/k1v run after a block barrier, once every layer's
+// average is in place.
+template <int CLN, bool ROT>
+__global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d) {
   double* __restrict__ f_hp = d.f.hp;
+  double* __restrict__ f_hpp = d.f.hpp;
   double* __restrict__ f_hu = d.f.hu;
   double* __restrict__ f_hup = d.f.hup;
   double* __restrict__ f_hupp = d.f.hupp;
@@ -544,47 +543,74 @@ __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
   const int l = blockIdx.x * 32 + cx + 1;
   const bool act = l <= d.g.lm;
   const int k1 = d.g.k1, km1 = d.g.km1;
-  int kms = 0, kmx = 0, kmy = 0;
   bool ew = false, nw = false;
   int fz = km1, fu = km1, fv = km1;
   if (act) {
-    kms = NB(d.g.kmz, l);
-    const double spl = d.s.sp[l - 1];
-    const double hhs = d.g.hhs[l - 1];
-    #pragma unroll 4
-    for (int k = k1 + ty; k <= kms; k += CLN) {
-      double v = fmin(zl(d, k + 1), hhs) - fmax(zl(d, k), -spl);
-      if (v <= HMIN) v = ZERO;
-      f_hp[IX(d, k, l)] = v;
-      if (v > ZERO && k < fz) fz = k;
-    }
+    const int kms = NB(d.g.kmz, l);
     ew = ewet(d, l);
-    if (ew) {
-      const int lE = NB(d.g.lEC, l);
-      kmx = min(kms, NB(d.g.kmz, lE));
-      const double sm = fmax(spl, d.s.sp[lE - 1]);
-      const double hhu = d.g.hhu[l - 1];
-      #pragma unroll 4
-      for (int k = k1 + ty; k <= kmx; k += CLN) {
-        double v = fmin(zl(d, k + 1), hhu) - fmax(zl(d, k), -sm);
-        if (v <= HMIN) v = ZERO;
-        f_hup[IX(d, k, l)] = v;
-        if (v > ZERO && k < fu) fu = k;
-      }
-    }
     nw = nwet(d, l);
-    if (nw) {
-      const int lN = NB(d.g.lNC, l);
-      kmy = min(kms, NB(d.g.kmz, lN));
-      const double sm = fmax(spl, d.s.sp[lN - 1]);
-      const double hhv = d.g.hhv[l - 1];
-      #pragma unroll 4
-      for (int k = k1 + ty; k <= kmy; k += CLN) {
-        double v = fmin(zl(d, k + 1), hhv) - fmax(zl(d, k), -sm);
-        if (v <= HMIN) v = ZERO;
-        f_hvp[IX(d, k, l)] = v;
-        if (v > ZERO && k < fv) fv = k;
+    const int lE = NB(d.g.lEC, l), lN = NB(d.g.lNC, l);
+    const int kmx = ew ? min(kms, NB(d.g.kmz, lE)) : 0;
+    const int kmy = nw ? min(kms, NB(d.g.kmz, lN)) : 0;
+    const double spl = d.s.sp[l - 1];
+    const double hhs = d.g.hhs[l - 1], hhu = d.g.hhu[l - 1], hhv = d.g.hhv[l - 1];
+    const double smx = fmax(spl, d.s.sp[lE - 1]), smy = fmax(spl, d.s.sp[lN - 1]);
+    // settrap also rotates hp, hup, hvp over levels 1 .. kmz + 1 (1 .. kmx, 1 .. kmy)
+    const int kb = ROT ? 1 : k1, ke = ROT ? kms + 1 : kms;
+    auto load = [&](int k, HalfIn& v) {
+      const int ik = IX(d, min(k, ke), l);   // clamped: every address is inside the column
+      v.hp = f_hp[ik]; v.hup = f_hup[ik]; v.hvp = f_hvp[ik];
+      v.sal = f_sal[ik]; v.salq = ROT ? f_salp[ik] : f_salpp[ik];
+      v.uh = f_uh[ik]; v.uhq = ROT ? f_uhp[ik] : f_uhpp[ik]; v.up = f_up[ik];
+      v.vh = f_vh[ik]; v.vhq = ROT ? f_vhp[ik] : f_vhpp[ik]; v.vp = f_vp[ik];
+    };
+    auto apply = [&](int k, const HalfIn& v) {
+      if (k > ke) return;
+      const int ik = IX(d, k, l);
+      const bool zin = k >= k1 && k <= kms;
+      const bool uin = ew && k >= k1 && k <= kmx;
+      const bool vin = nw && k >= k1 && k <= kmy;
+      if (ROT) {
+        f_hpp[ik] = v.hp;
+        if (ew && k <= kmx) f_hupp[ik] = v.hup;
+        if (nw && k <= kmy) f_hvpp[ik] = v.hvp;
       }
+      if (zin) {
+        double h = fmin(zl(d, k + 1), hhs) - fmax(zl(d, k), -spl);
+        if (h <= HMIN) h = ZERO;
+        f_hp[ik] = h;
+        if (h > ZERO && k < fz) fz = k;
+        // scalar at n+1/2 (salpp <- salp first in settrap)
+        if (ROT) f_salpp[ik] = v.salq;
+        const double sp = (v.sal + v.salq) / 2.;
+        f_salp[ik] = sp;
+        f_rhop[ik] = densty_s(sp, 0.00004, zmid(d, k, h)) - 1000.;
+      }
+      if (uin) {
+        double h = fmin(zl(d, k + 1), hhu) - fmax(zl(d, k), -smx);
+        if (h <= HMIN) h = ZERO;
+        f_hup[ik] = h;
+        if (h > ZERO && k < fu) fu = k;
+        if (ROT) { f_uhpp[ik] = v.uhq; f_upp[ik] = v.up; }
+        if (h > ZERO) { const double a = 0.5 * (v.uh + v.uhq); f_uhp[ik] = a; f_up[ik] = a / h; }
+        else { f_uhp[ik] = 0.0; f_up[ik] = 0.0; }
+      }
+      if (vin) {
+        double h = fmin(zl(d, k + 1), hhv) - fmax(zl(d, k), -smy);
+        if (h <= HMIN) h = ZERO;
+        f_hvp[ik] = h;
+        if (h > ZERO && k < fv) fv = k;
+        if (ROT) { f_vhpp[ik] = v.vhq; f_vpp[ik] = v.vp; }
+        if (h > ZERO) { const double a = 0.5 * (v.vh + v.vhq); f_vhp[ik] = a; f_vp[ik] = a / h; }
+        else { f_vhp[ik] = 0.0; f_vp[ik] = 0.0; }
+      }
+    };
+    for (int k = kb + ty; k <= ke; k += BK_TRIP * CLN) {
+      HalfIn v[BK_TRIP];
+#pragma unroll
+      for (int t = 0; t < BK_TRIP; ++t) load(k + t * CLN, v[t]);
+#pragma unroll
+      for (int t = 0; t < BK_TRIP; ++t) apply(k + t * CLN, v[t]);
     }
   }
   s_first[0][ty][cx] = fz; s_first[1][ty][cx] = fu; s_first[2][ty][cx] = fv;
@@ -597,38 +623,6 @@ __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
     }
     d.s.k1z[l - 1] = kz; d.s.k1u[l - 1] = ku; d.s.k1v[l - 1] = kv;
   }
-  if (act) {
-    #pragma unroll 4
-    for (int k = k1 + ty; k <= kms; k += CLN) {
-      const int ik = IX(d, k, l);
-      const double z = zmid(d, k, f_hp[ik]);
-      if (rotate) f_salpp[ik] = f_salp[ik];
-      const double sp = (f_sal[ik] + f_salpp[ik]) / 2.;
-      f_salp[ik] = sp;
-      f_rhop[ik] = densty_s(sp, 0.00004, z) - 1000.;
-    }
-    if (ew) {
-      #pragma unroll 4
-      for (int k = k1 + ty; k <= kmx; k += CLN) {
-        const int ik = IX(d, k, l);
-        if (rotate) { f_uhpp[ik] = f_uhp[ik]; f_upp[ik] = f_up[ik]; }
-        const double hup = f_hup[ik];
-        if (hup > ZERO) { const double v = 0.5 * (f_uh[ik] + f_uhpp[ik]); f_uhp[ik] = v; f_up[ik] = v / hup; }
-        else { f_uhp[ik] = 0.0; f_up[ik] = 0.0; }
-      }
-    }
-    if (nw) {
-      #pragma unroll 4
-      for (int k = k1 + ty; k <= kmy; k += CLN) {
-        const int ik = IX(d, k, l);
-        if (rotate) { f_vhpp[ik] = f_vhp[ik]; f_vpp[ik] = f_vp[ik]; }
-        const double hvp = f_hvp[ik];
-        if (hvp > ZERO) { const double v = 0.5 * (f_vh[ik] + f_vhpp[ik]); f_vhp[ik] = v; f_vp[ik] = v / hvp; }
-        else { f_vhp[ik] = 0.0; f_vp[ik] = 0.0; }
-      }
-    }
-  }
-  __syncthreads();
   if (!act || ty != 0) return;
   // surface corrections at the first wet face layer (:3503-3516 / :4033-4046)
   if (ew) {
@@ -657,10 +651,16 @@ __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d, int rotate) {
   }
 }
 
-// save (istep = 2 after a trapezoidal step, 1 after a leapfrog step), cell-parallel like
-// k_half_level; the new first wet layers are reduced over the lanes in shared memory.
-template <int CLN>
-__global__ void __launch_bounds__(32 * CLN) k_save(Dev d, int istep) {
+// Values of one cell (k, l) that save reads.
+struct SaveIn {
+  double h, hp, hu, hup, hv, hvp, sal, salp, uh, uhp, up, vh, vhp, vp;
+};
+
+// save (istep = 2 after a trapezoidal step, 1 after a leapfrog step, which also rotates n -> n-1):
+// one pass over levels 1 .. kmz + 1 like k_half_level; the new first wet layers are reduced over
+// the lanes in shared memory.
+template <int CLN, bool ROT>
+__global__ void __launch_bounds__(32 * CLN) k_save(Dev d) {
   double* __restrict__ f_h = d.f.h;
   double* __restrict__ f_hp = d.f.hp;
   double* __restrict__ f_hpp = d.f.hpp;
@@ -690,39 +690,60 @@ __global__ void __launch_bounds__(32 * CLN) k_save(Dev d, int istep) {
   const bool act = l <= d.g.lm;
   const int k1 = d.g.k1, km1 = d.g.km1;
   int fz = km1, fu = km1, fv = km1;
-  int zL = 0, uL = 0, vL = 0, kms = 0;
   if (act) {
     if (ty == 0) {
-      if (istep == 1) d.s.spp[l - 1] = d.s.sp[l - 1];
+      if (ROT) d.s.spp[l - 1] = d.s.sp[l - 1];
       d.s.sp[l - 1] = d.s.s[l - 1];
     }
-    zL = zlim(d, l); uL = ulim(d, l); vL = vlim(d, l);
-    kms = NB(d.g.kmz, l);
-    const int kmx = ewet(d, l) ? min(kms, NB(d.g.kmz, NB(d.g.lEC, l))) : 0;
-    const int kmy = nwet(d, l) ? min(kms, NB(d.g.kmz, NB(d.g.lNC, l))) : 0;
-    #pragma unroll 4
-    for (int k = 1 + ty; k <= zL; k += CLN) {
+    const int kms = NB(d.g.kmz, l);
+    const int zL = zlim(d, l), uL = ulim(d, l), vL = vlim(d, l);
+    const int ksal = min(d.g.km, zL);
+    auto load = [&](int k, SaveIn& v) {
+      const int ik = IX(d, min(k, zL), l);   // clamped: every address is inside the column
+      v.h = f_h[ik]; v.hp = f_hp[ik]; v.hu = f_hu[ik]; v.hup = f_hup[ik]; v.hv = f_hv[ik]; v.hvp = f_hvp[ik];
+      v.sal = f_sal[ik]; v.salp = f_salp[ik];
+      v.uh = f_uh[ik]; v.uhp = f_uhp[ik]; v.up = f_up[ik];
+      v.vh = f_vh[ik]; v.vhp = f_vhp[ik]; v.vp = f_vp[ik];
+    };
+    auto apply = [&](int k, const SaveIn& v) {
+      if (k > zL) return;
       const int ik = IX(d, k, l);
-      if (istep == 1) f_hpp[ik] = f_hp[ik];
-      const double v = f_h[ik];
-      f_hp[ik] = v;
-      if (k >= k1 && k <= kms && v > ZERO && k < fz) fz = k;
-    }
-    #pragma unroll 4
-    for (int k = 1 + ty; k <= uL; k += CLN) {
-      const int ik = IX(d, k, l);
-      if (istep == 1) f_hupp[ik] = f_hup[ik];
-      const double v = f_hu[ik];
-      f_hup[ik] = v;
-      if (k >= k1 && k <= kmx && v > ZERO && k < fu) fu = k;
-    }
-    #pragma unroll 4
-    for (int k = 1 + ty; k <= vL; k += CLN) {
-      const int ik = IX(d, k, l);
-      if (istep == 1) f_hvpp[ik] = f_hvp[ik];
-      const double v = f_hv[ik];
-      f_hvp[ik] = v;
-      if (k >= k1 && k <= kmy && v > ZERO && k < fv) fv = k;
+      if (ROT) f_hpp[ik] = v.hp;
+      f_hp[ik] = v.h;
+      if (k >= k1 && k <= kms && v.h > ZERO && k < fz) fz = k;
+      if (k <= uL) {
+        if (ROT) f_hupp[ik] = v.hup;
+        f_hup[ik] = v.hu;
+        if (k >= k1 && v.hu > ZERO && k < fu) fu = k;
+      }
+      if (k <= vL) {
+        if (ROT) f_hvpp[ik] = v.hvp;
+        f_hvp[ik] = v.hv;
+        if (k >= k1 && v.hv > ZERO && k < fv) fv = k;
+      }
+      if (k >= k1 && k <= ksal) {
+        const double z = zmid(d, k, v.h);
+        if (ROT) f_salpp[ik] = v.salp;
+        f_salp[ik] = v.sal;
+        f_rhop[ik] = densty_s(v.sal, 0.00004, z) - 1000.;
+      }
+      if (k >= k1 && k <= uL) {
+        if (ROT) { f_uhpp[ik] = v.uhp; f_upp[ik] = v.up; }
+        if (v.hu > ZERO) { f_uhp[ik] = v.uh; f_up[ik] = v.uh / v.hu; }
+        else { f_uhp[ik] = 0.0; f_up[ik] = 0.0; }
+      }
+      if (k >= k1 && k <= vL) {
+        if (ROT) { f_vhpp[ik] = v.vhp; f_vpp[ik] = v.vp; }
+        if (v.hv > ZERO) { f_vhp[ik] = v.vh; f_vp[ik] = v.vh / v.hv; }
+        else { f_vhp[ik] = 0.0; f_vp[ik] = 0.0; }
+      }
+    };
+    for (int k = 1 + ty; k <= zL; k += BK_TRIP * CLN) {
+      SaveIn v[BK_TRIP];
+#pragma unroll
+      for (int t = 0; t < BK_TRIP; ++t) load(k + t * CLN, v[t]);
+#pragma unroll
+      for (int t = 0; t < BK_TRIP; ++t) apply(k + t * CLN, v[t]);
     }
   }
   s_first[0][ty][cx] = fz; s_first[1][ty][cx] = fu; s_first[2][ty][cx] = fv;
@@ -734,31 +755,6 @@ __global__ void __launch_bounds__(32 * CLN) k_save(Dev d, int istep) {
       kz = min(kz, s_first[0][q][cx]); ku = min(ku, s_first[1][q][cx]); kv = min(kv, s_first[2][q][cx]);
     }
     d.s.k1z[l - 1] = kz; d.s.k1u[l - 1] = ku; d.s.k1v[l - 1] = kv;
-  }
-  if (!act) return;
-  #pragma unroll 4
-  for (int k = k1 + ty; k <= min(d.g.km, zL); k += CLN) {
-    const int ik = IX(d, k, l);
-    const double z = zmid(d, k, f_hp[ik]);
-    if (istep == 1) f_salpp[ik] = f_salp[ik];
-    f_salp[ik] = f_sal[ik];
-    f_rhop[ik] = densty_s(f_salp[ik], 0.00004, z) - 1000.;
-  }
-  #pragma unroll 4
-  for (int k = k1 + ty; k <= uL; k += CLN) {
-    const int ik = IX(d, k, l);
-    if (istep == 1) { f_uhpp[ik] = f_uhp[ik]; f_upp[ik] = f_up[ik]; }
-    const double hup = f_hup[ik];
-    if (hup > ZERO) { const double v = f_uh[ik]; f_uhp[ik] = v; f_up[ik] = v / hup; }
-    else { f_uhp[ik] = 0.0; f_up[ik] = 0.0; }
-  }
-  #pragma unroll 4
-  for (int k = k1 + ty; k <= vL; k += CLN) {
-    const int ik = IX(d, k, l);
-    if (istep == 1) { f_vhpp[ik] = f_vhp[ik]; f_vpp[ik] = f_vp[ik]; }
-    const double hvp = f_hvp[ik];
-    if (hvp > ZERO) { const double v = f_vh[ik]; f_vhp[ik] = v; f_vp[ik] = v / hvp; }
-    else { f_vhp[ik] = 0.0; f_vp[ik] = 0.0; }
   }
 }
 
@@ -835,18 +831,19 @@ void launch_vel2(const Dev& d, cudaStream_t st) {
 
 void launch_settrap(const Dev& d, cudaStream_t st) {
   k_half_zeta<<<grid_of(d.g.lm), TB, 0, st>>>(d, 1);
-  k_half_level<BK_LANES><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d, 1);
+  k_half_level<BK_LANES, true><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
   k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
 }
 
 void launch_settrap2(const Dev& d, cudaStream_t st) {
   k_half_zeta<<<grid_of(d.g.lm), TB, 0, st>>>(d, 0);
-  k_half_level<BK_LANES><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d, 0);
+  k_half_level<BK_LANES, false><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
   k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
 }
 
 void launch_save(const Dev& d, int istep, cudaStream_t st) {
-  k_save<BK_LANES><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d, istep);
+  if (istep == 1) k_save<BK_LANES, true><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
+  else k_save<BK_LANES, false><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
   k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
 }
 
