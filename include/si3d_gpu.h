@@ -49,7 +49,12 @@ extern "C" {
                              a project addition with no counterpart in the reference */
 
 /* zeta-solve orderings */
-#define SI3D_ORDER_REDBLACK 1   /* NSPCG iperm=1 red-black MIC (the GPU form) */
+#define SI3D_ORDER_REDBLACK 1   /* NSPCG iperm=1 red-black MIC (the GPU form; 0 means the same) */
+#define SI3D_ORDER_NATURAL 2    /* the reference's own natural-order MIC (mic1, nspcg.f:21759-21805,
+                                   :22875-22922, :22729-22777): its triangular sweeps are recurrences
+                                   along l, run level by level by one thread block, so it is meant for
+                                   small systems (iterate-level comparison with the reference's
+                                   algorithm); plain FP64 only, not with SI3D_X0_HIST or ensembles */
 
 /* initial guess for the zeta solve */
 #define SI3D_X0_PREV 0      /* sp, as the reference (si3d_procedures.f90:1970) */
@@ -94,7 +99,7 @@ typedef struct si3d_params {
   double pcg_tol;
   int pcg_itmax;
   double srelpr;
-  int ordering;            /* SI3D_ORDER_REDBLACK */
+  int ordering;            /* SI3D_ORDER_REDBLACK or SI3D_ORDER_NATURAL */
   int x0_mode;             /* SI3D_X0_* */
   int precision;           /* SI3D_FP64, SI3D_MIXED_IR or SI3D_MIXED_MG */
   int ntr;                 /* non-active tracers, 0..30 (ntrmax, si3d_types.f90:291); conservative
@@ -164,9 +169,11 @@ int si3d_gpu_set_warmstart(int handle, const double* dzeta, int on_device);
  * host Purdue arrays: coef (lm x 5, column-major: diagonal, W, S, N, E), jcoef (1-based,
  * 0 = no entry), rhs (lm), zeta (lm; in: x0, out: solution).  The matrix must have the
  * 5-point structure SolverSparse builds (jcoef columns = l, lWC, lSC, lNC, lEC).
+ * ordering: SI3D_ORDER_REDBLACK (0 or 1) or SI3D_ORDER_NATURAL (NSPCG's default numbering, the
+ * reference's; precision SI3D_FP64 only).
  * Outputs: iterations, final stopping-test value, emin/emax estimates. */
 int si3d_gpu_solve_zeta(int lm, const double* coeffA, const int* jcoefA, const double* rhs, double* zeta,
-                        int pcg_test, double pcg_tol, int pcg_itmax, double srelpr, int precision,
+                        int pcg_test, double pcg_tol, int pcg_itmax, double srelpr, int precision, int ordering,
                         int* iters, double* stptst, double* emin, double* emax);
 
 /* Batched tridiagonal solves with two right-hand sides sharing one factorisation, as trid

@@ -25,7 +25,8 @@ typedef struct si3d_solver_opts {
   int pcg_itmax;
   double srelpr;
   int x0_mode;       /* SI3D_X0_* */
-  int precision;     /* SI3D_FP64 / SI3D_MIXED_IR */
+  int precision;     /* SI3D_FP64 / SI3D_MIXED_IR / SI3D_MIXED_MG */
+  int ordering;      /* SI3D_ORDER_REDBLACK (0 or 1) or SI3D_ORDER_NATURAL */
 } si3d_solver_opts;
 
 /* Read the input files of a run directory and build grid + initial state on the host.

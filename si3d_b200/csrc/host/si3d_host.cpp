@@ -654,7 +654,8 @@ int si3d_host_attach_gpu(int h, int device, int* gpu_handle) {
   p.iadv = M->iadv; p.itrmom = M->itrmom; p.ihd = M->ihd; p.ibc = M->ibc; p.isal = M->isal; p.itrap = M->itrap;
   p.niter = M->niter; p.ismooth = M->ismooth;
   p.pcg_test = M->opt.pcg_test; p.pcg_tol = M->opt.pcg_tol; p.pcg_itmax = M->opt.pcg_itmax; p.srelpr = M->opt.srelpr;
-  p.ordering = SI3D_ORDER_REDBLACK; p.x0_mode = M->opt.x0_mode; p.precision = M->opt.precision;
+  p.ordering = M->opt.ordering == SI3D_ORDER_NATURAL ? SI3D_ORDER_NATURAL : SI3D_ORDER_REDBLACK;
+  p.x0_mode = M->opt.x0_mode; p.precision = M->opt.precision;
   p.ntr = M->ntr;
   p.iturb = M->iturb;
   int gh = -1;

@@ -379,6 +379,260 @@ int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, bool test2, cuda
   return e == cudaSuccess ? 0 : -1;
 }
 
+// ---------------------------------------------------------------- natural-order MIC-CG
+// One block runs the whole solve of the reference's own ordering (nspcg.f: icfp :20724-20850 with
+// property A, icsp/icfstp/icbsp :21759-21805, :22875-22922, :22729-22777, mult1 :23919-23947, itcg
+// :8967-9092, pstops :25956-26100), row by row in the operation order of those routines.  The
+// sweeps' recurrences along l run level by level (a level's rows in parallel, a block barrier
+// between levels); dot products are block sums in a fixed order.
+constexpr int NQB = 1024;
+
+__device__ __forceinline__ double nat_coef(const NatDev& N, int i, int code) {
+  switch (code) {
+    case 0: return N.cW[i];
+    case 1: return N.cS[i];
+    case 2: return N.cN[i];
+    case 3: return N.cE[i];
+    default: return 0.0;   // an absent neighbour: adjust made it the row itself with coefficient 0
+  }
+}
+__device__ __forceinline__ int nat_col(const int4& nb, int i, int code) {
+  switch (code) {
+    case 0: return nb.x;
+    case 1: return nb.y;
+    case 2: return nb.z;
+    case 3: return nb.w;
+    default: return i;
+  }
+}
+
+// (A x)_i in mult1's order: the diagonal, then the off-diagonal columns as move1 left them.
+__device__ __forceinline__ double nat_row_apply(const NatDev& N, const double* x, int i) {
+  const int4 nb = N.nbr[i];
+  const int ord = N.order[i];
+  double y = N.cd[i] * x[i];
+#pragma unroll
+  for (int sl = 0; sl < 4; ++sl) {
+    const int c = (ord >> (3 * sl)) & 7;
+    y = y + nat_coef(N, i, c) * x[nat_col(nb, i, c)];
+  }
+  return y;
+}
+
+// Lower neighbours of row i in ascending row order (the order in which their pushes reach row i
+// in icfp and icfstp), with their codes; returns how many.
+__device__ __forceinline__ int nat_lower(const NatDev& N, int i, int4 nb, int (&rows)[4], int (&codes)[4]) {
+  const int cand[4] = {nb.x, nb.y, nb.z, nb.w};
+  int m = 0;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    if (cand[c] < i) {   // absent neighbours are n > i
+      int j = m++;
+      while (j > 0 && rows[j - 1] > cand[c]) { rows[j] = rows[j - 1]; codes[j] = codes[j - 1]; --j; }
+      rows[j] = cand[c];
+      codes[j] = c;
+    }
+  }
+  return m;
+}
+
+template <bool TEST2>
+__global__ void __launch_bounds__(NQB, 1) k_pcg_natural(NatDev N) {
+  __shared__ double sh[(NQB / 32) * 3 + 3];
+  PcgScal* SC = N.sc;
+  const int n = N.n, tid = threadIdx.x;
+  // ---- icfp: MIC pivots, property A, omega = 1 (a row's pivot after its lower neighbours')
+  for (int L = 0; L < N.nlev; ++L) {
+    for (int q = N.lvl_off[L] + tid; q < N.lvl_off[L + 1]; q += NQB) {
+      const int i = N.lvl_row[q];
+      int rows[4], codes[4];
+      const int m = nat_lower(N, i, N.nbr[i], rows, codes);
+      double dd = N.cd[i];
+      for (int t = 0; t < m; ++t) {
+        const int k = rows[t];
+        const int ok = N.order[k];
+        double wk = 0.0;   // row sum of k's upper columns (icfp's wksp)
+        for (int sl = 0; sl < N.nt; ++sl) wk = wk + nat_coef(N, k, (ok >> (3 * sl)) & 7);
+        const double c = nat_coef(N, i, codes[t]);   // = A(k, i) (the matrix is symmetric)
+        const double term = c / N.piv[k];
+        dd = dd - term * (1.0 * wk - (1.0 - 1.0) * c);
+      }
+      N.piv[i] = dd;
+    }
+    __syncthreads();
+  }
+  int zero = 0, neg = 0;
+  for (int i = tid; i < n; i += NQB) {
+    const double pv = N.piv[i];
+    if (pv == 0.0) zero = 1;
+    const double di = 1.0 / pv;
+    N.dinv[i] = di;
+    if (di < 0.0) neg = 1;
+  }
+  zero = __syncthreads_or(zero);
+  neg = __syncthreads_or(neg);
+  if (zero) {
+    if (tid == 0) { SC->negpiv = 2; SC->in = 0; SC->done = 1; }
+    return;
+  }
+  // ---- cgw: r = b - A u, ||b|| (nmcalc)
+  {
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int i = tid; i < n; i += NQB) {
+      N.r[i] = N.b[i] - nat_row_apply(N, N.u, i);
+      v[0] += N.b[i] * N.b[i];
+    }
+    bsum<3, NQB>(v, sh);
+    if (tid == 0) SC->bnorm = fmax(sqrt(v[0]), SC->srelpr);
+  }
+  __syncthreads();
+  const double zeta = SC->zeta, srelpr = SC->srelpr, bnorm = SC->bnorm, tiny = 500.0 * srelpr;
+  const int itmax = SC->itmax, hist_cap = SC->hist_cap;
+  double alpha = 0.0, beta = 0.0, alphao = 0.0, rzdot = 0.0, dkm1 = 0.0, udnm = 1.0, stptst = 0.0;
+  bool q1 = false;
+  int in = 0, ier = 0;
+  bool first = true;
+  for (;;) {
+    if (!first)
+      for (int i = tid; i < n; i += NQB) N.r[i] = N.r[i] - alpha * N.q[i];
+    first = false;
+    __syncthreads();
+    // ---- z = M^-1 r (icsp): forward sweep level by level, z /= d, backward sweep in reverse
+    for (int L = 0; L < N.nlev; ++L) {
+      for (int q = N.lvl_off[L] + tid; q < N.lvl_off[L + 1]; q += NQB) {
+        const int i = N.lvl_row[q];
+        int rows[4], codes[4];
+        const int m = nat_lower(N, i, N.nbr[i], rows, codes);
+        double t = N.r[i];
+        for (int j = 0; j < m; ++j) t = t - nat_coef(N, i, codes[j]) * N.z[rows[j]];
+        N.z[i] = t * N.dinv[i];
+      }
+      __syncthreads();
+    }
+    for (int i = tid; i < n; i += NQB) N.z[i] = N.z[i] / N.dinv[i];
+    __syncthreads();
+    for (int L = N.nlev - 1; L >= 0; --L) {
+      for (int q = N.lvl_off[L] + tid; q < N.lvl_off[L + 1]; q += NQB) {
+        const int i = N.lvl_row[q];
+        const int4 nb = N.nbr[i];
+        const int ord = N.order[i];
+        double sum = N.z[i];
+        for (int sl = 0; sl < N.nt; ++sl) {
+          const int c = (ord >> (3 * sl)) & 7;
+          sum = sum - nat_coef(N, i, c) * N.z[nat_col(nb, i, c)];
+        }
+        N.z[i] = sum * N.dinv[i];
+      }
+      __syncthreads();
+    }
+    // ---- (r, z); pstops
+    double v[3] = {0.0, 0.0, 0.0};
+    for (int i = tid; i < n; i += NQB) {
+      const double ri = N.r[i], zi = N.z[i];
+      v[0] += ri * zi;
+      v[1] += ri * ri;
+      v[2] += zi * zi;
+    }
+    bsum<3, NQB>(v, sh);
+    dkm1 = rzdot;
+    rzdot = v[0];
+    if (!(rzdot > 0.0)) { ier = -7; break; }
+    bool halt = false;
+    if (TEST2) {
+      if (in < 1) {
+        q1 = false;
+        udnm = 1.0;
+        stptst = sqrt(rzdot);
+        if (stptst < tiny) halt = true;
+      } else {
+        if (!q1 && !((in > 5) && (in % 5 != 0))) {
+          const double uold = udnm;
+          double w[1] = {0.0};
+          for (int i = tid; i < n; i += NQB) w[0] += N.u[i] * N.u[i];
+          bsum<1, NQB>(w, sh);
+          udnm = sqrt(w[0]);
+          if (udnm < tiny) udnm = 1.0;
+          if ((in > 5) && (fabs(udnm - uold) < udnm * zeta)) q1 = true;
+        }
+        double eminl = __ldcg(&SC->emin);   // chgcon's latest estimate (written by thread 0)
+        if (eminl < tiny) eminl = tiny;
+        const double tl = sqrt(v[2]), tr = udnm * eminl;
+        stptst = tl / tr;
+        if (tl < tr * zeta) halt = true;
+      }
+    } else {
+      const double tl = sqrt(v[1]);
+      stptst = tl / bnorm;
+      if (tl < bnorm * zeta) halt = true;
+    }
+    if (halt) break;
+    if (!(in < itmax)) { ier = 1; break; }
+    if (in != 0) beta = rzdot / dkm1;
+    for (int i = tid; i < n; i += NQB) N.p[i] = N.z[i] + beta * N.p[i];
+    __syncthreads();
+    double w[1] = {0.0};
+    for (int i = tid; i < n; i += NQB) {
+      const double qi = nat_row_apply(N, N.p, i);
+      N.q[i] = qi;
+      w[0] += N.p[i] * qi;
+    }
+    bsum<1, NQB>(w, sh);
+    alphao = alpha;
+    alpha = rzdot / w[0];
+    if (!(w[0] > 0.0)) { ier = -6; break; }
+    if (tid == 0 && in < hist_cap) { N.hist_alpha[in] = alpha; N.hist_beta[in] = beta; }
+    if (TEST2) {
+      if (tid == 0 && (SC->maxadp || SC->minadp)) lz_chgcon(SC, N.tri, in, alpha, beta, alphao);
+      __syncthreads();
+    }
+    for (int i = tid; i < n; i += NQB) N.u[i] = N.u[i] + alpha * N.p[i];
+    ++in;
+  }
+  if (tid == 0) {
+    SC->alpha = alpha; SC->beta = beta; SC->rzdot = rzdot; SC->udnm = udnm; SC->in = in; SC->stptst = stptst;
+    if (ier) SC->ier = ier;
+    else if (SC->chg_ier) SC->ier = SC->chg_ier;
+    SC->negpiv = neg ? 1 : 0;
+    SC->done = 1;
+  }
+}
+
+// Rows of the natural system from matcon's sx, sy, qq, as SolverSparse assembles coeffA
+// (si3d_procedures.f90:1950-1967), and the initial guess (x0 modes of the red-black gather).
+__global__ void k_nat_gather(Dev d, NatDev N, int x0_mode, const double* __restrict__ dz) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > N.n) return;
+  if (i == N.n) {   // the zero slot of absent neighbours
+    N.u[i] = N.r[i] = N.z[i] = N.p[i] = N.q[i] = N.b[i] = 0.0;
+    N.cd[i] = N.cW[i] = N.cS[i] = N.cN[i] = N.cE[i] = 0.0;
+    return;
+  }
+  const int l = i + 1, lm1 = d.g.lm1;
+  const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l), lN = NB(d.g.lNC, l), lE = NB(d.g.lEC, l);
+  const double sxi = d.s.sx[l - 1], syi = d.s.sy[l - 1];
+  const double sxW = lW != lm1 ? d.s.sx[lW - 1] : 0.0, syS = lS != lm1 ? d.s.sy[lS - 1] : 0.0;
+  N.cd[i] = 1 + sxi + sxW + syi + syS;
+  N.cW[i] = lW != lm1 ? -sxW : 0.0;
+  N.cS[i] = lS != lm1 ? -syS : 0.0;
+  N.cN[i] = lN != lm1 ? -syi : 0.0;
+  N.cE[i] = lE != lm1 ? -sxi : 0.0;
+  N.b[i] = d.s.qq[l - 1];
+  double x0;
+  switch (x0_mode) {
+    case 1: x0 = 0.0; break;
+    case 3: x0 = d.s.s[l - 1]; break;
+    default: x0 = d.s.sp[l - 1]; if (x0_mode == 2 && dz) x0 = x0 + dz[l - 1];
+  }
+  N.u[i] = x0;
+  N.z[i] = 0.0; N.p[i] = 0.0; N.q[i] = 0.0;
+}
+
+__global__ void k_nat_scatter(Dev d, NatDev N) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= N.n) return;
+  d.s.s[i] = N.u[i];
+}
+
 }  // namespace
 
 int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32) {
@@ -405,6 +659,24 @@ int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, bool test2, cudaStream_
 
 int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st, const GridBar* init) {
   return launch_loop<float>(F, bar, nblocks, false, st, init);
+}
+
+}  // namespace si3d
+
+namespace si3d {
+
+void nat_setup(const Dev& d, const NatDev& N, int x0_mode, const double* dz, cudaStream_t st) {
+  k_nat_gather<<<(N.n + 1 + 255) / 256, 256, 0, st>>>(d, N, x0_mode, dz);
+}
+
+int nat_solve(const NatDev& N, bool test2, cudaStream_t st) {
+  if (test2) k_pcg_natural<true><<<1, NQB, 0, st>>>(N);
+  else k_pcg_natural<false><<<1, NQB, 0, st>>>(N);
+  return cudaPeekAtLastError() == cudaSuccess ? 0 : -1;
+}
+
+void nat_finish(const Dev& d, const NatDev& N, cudaStream_t st) {
+  k_nat_scatter<<<(N.n + 255) / 256, 256, 0, st>>>(d, N);
 }
 
 }  // namespace si3d

@@ -84,6 +84,32 @@ struct GridBar {
   unsigned long long limit, pad;
 };
 int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32);
+
+// Natural-order MIC-CG (the reference's own ordering, SI3D_ORDER_NATURAL), k_pcg_persistent.cu.
+// The unknowns are the wet columns in l order.  Each row keeps its four neighbours and their
+// coefficients; `order` packs, 3 bits per slot, the codes (0 W, 1 S, 2 N, 3 E, 4 none) of the row's
+// off-diagonal columns in the order NSPCG's move1 leaves them (upper columns first), which fixes
+// the order of the sums in the SpMV and the backward sweep.  The triangular sweeps of the
+// preconditioner are recurrences along l; they run level by level (a row's level is one more than
+// its lower neighbours'), the rows of a level in parallel.
+struct NatDev {
+  int n = 0, nlev = 0, nt = 0;   // rows, levels, upper columns per row (move1's nt)
+  const int* lvl_off = nullptr;   // [nlev + 1]
+  const int* lvl_row = nullptr;   // [n] rows (0-based) by ascending level
+  const int* lrow = nullptr;      // [n] 1-based column index l of each row (= row + 1)
+  const int4* nbr = nullptr;      // [n] W, S, N, E rows (n = none)
+  const int* order = nullptr;     // [n] move1 column order, packed
+  double *cd = nullptr, *cW = nullptr, *cS = nullptr, *cN = nullptr, *cE = nullptr;   // [n + 1]
+  double *b = nullptr, *u = nullptr, *r = nullptr, *z = nullptr, *p = nullptr, *q = nullptr;
+  double *piv = nullptr, *dinv = nullptr;
+  PcgScal* sc = nullptr;
+  double *hist_alpha = nullptr, *hist_beta = nullptr, *tri = nullptr;
+};
+// rows and x0 from matcon's sx, sy, qq (x0 modes as the red-black gather); the solve (one block);
+// zeta back to the columns
+void nat_setup(const Dev& d, const NatDev& N, int x0_mode, const double* dz, cudaStream_t st);
+int nat_solve(const NatDev& N, bool test2, cudaStream_t st);
+void nat_finish(const Dev& d, const NatDev& N, cudaStream_t st);
 // `init` (host memory, optional) replaces the zeroed barrier record of this launch
 int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st,
              const GridBar* init = nullptr);   // test2: stopping test 2

@@ -84,6 +84,8 @@ struct Ctx {
   // red-black zeta system
   PcgDev pcg{};
   PcgDevF pcgf{};            // FP32 inner system of iterative refinement
+  NatDev nat{};              // natural-order system (ordering SI3D_ORDER_NATURAL)
+  bool natural = false;
   MgDev mg{};                // aggregation hierarchy of the MG inner solves (precision SI3D_MIXED_MG)
   int mg_blocks = 0;
   PcgScal* h_scf = nullptr;  // pinned
@@ -405,6 +407,95 @@ int build_mg(Ctx* c, const si3d_grid* g) {
   return rc;
 }
 
+// The natural-order system of ordering SI3D_ORDER_NATURAL: rows are the wet columns in l order.
+// Lower neighbours must precede a row and upper ones follow it (the reference's i-outer, j-inner
+// numbering guarantees it).  Per row: the level of the triangular sweeps (one more than its lower
+// neighbours') and the order in which NSPCG's move1 (nspcg.f:23287-23380) leaves the row's
+// off-diagonal columns - upper columns first - which fixes the order of every row sum.
+int build_natural(Ctx* c, const si3d_grid* g) {
+  const int lm = g->lm, lm1 = lm + 1;
+  NatDev& N = c->nat;
+  N.n = lm;
+  std::vector<int4> nb(lm);
+  std::vector<int> level(lm, 0), order(lm, 0);
+  int nt = 0, nbm = 0, nlev = 0;
+  for (int i = 0; i < lm; ++i) {
+    auto row = [&](const int* m) { const int v = m[i]; return v == lm1 ? lm : v - 1; };
+    nb[i] = make_int4(row(g->lWC), row(g->lSC), row(g->lNC), row(g->lEC));
+    const int cand[4] = {nb[i].x, nb[i].y, nb[i].z, nb[i].w};
+    int up = 0, lo = 0, lev = 0;
+    for (int m : cand) {
+      if (m == lm) continue;
+      if (m == i) return SI3D_EDIMS;
+      if (m < i) { ++lo; lev = std::max(lev, level[m] + 1); }
+      else ++up;
+    }
+    // the reference's numbering: W and S precede the row, N and E follow it
+    if ((nb[i].x != lm && nb[i].x > i) || (nb[i].y != lm && nb[i].y > i) || (nb[i].z != lm && nb[i].z < i) ||
+        (nb[i].w != lm && nb[i].w < i))
+      return SI3D_EDIMS;
+    level[i] = lev;
+    nlev = std::max(nlev, lev + 1);
+    nt = std::max(nt, up);
+    nbm = std::max(nbm, lo);
+  }
+  N.nt = nt;
+  N.nlev = nlev;
+  // move1 on each row's column indices (absent neighbours are the row itself after adjust)
+  for (int i = 0; i < lm; ++i) {
+    const int cand[4] = {nb[i].x, nb[i].y, nb[i].z, nb[i].w};
+    int J[6], code[6];
+    J[1] = i; code[1] = 4;
+    for (int q = 0; q < 4; ++q) { J[q + 2] = cand[q] == lm ? i : cand[q]; code[q + 2] = cand[q] == lm ? 4 : q; }
+    const int maxnz = 5, nt2 = nt + 1, nb1 = nt2 + 1;
+    if (nt * nbm != 0) {
+      int jbc = nt2;
+      for (int jtc = 2; jtc <= nt2; ++jtc) {
+        if (J[jtc] >= i) continue;
+        do { ++jbc; } while (jbc <= maxnz && J[jbc] < i);
+        if (jbc > maxnz) return SI3D_EDIMS;
+        std::swap(J[jtc], J[jbc]);
+        std::swap(code[jtc], code[jbc]);
+      }
+      int jtc = 1;
+      for (jbc = nb1; jbc <= maxnz; ++jbc) {
+        if (J[jbc] <= i) continue;
+        do { ++jtc; } while (jtc <= maxnz && J[jtc] > i);
+        if (jtc > maxnz) return SI3D_EDIMS;
+        std::swap(J[jtc], J[jbc]);
+        std::swap(code[jtc], code[jbc]);
+      }
+    }
+    int packed = 0;
+    for (int q = 0; q < 4; ++q) packed |= code[q + 2] << (3 * q);
+    order[i] = packed;
+  }
+  std::vector<int> off(nlev + 1, 0), rows(lm);
+  for (int i = 0; i < lm; ++i) off[level[i] + 1]++;
+  for (int L = 0; L < nlev; ++L) off[L + 1] += off[L];
+  std::vector<int> fill(off.begin(), off.end() - 1);
+  for (int i = 0; i < lm; ++i) rows[fill[level[i]]++] = i;
+  int rc = 0;
+  int *d_off = nullptr, *d_rows = nullptr, *d_order = nullptr;
+  int4* d_nb = nullptr;
+  rc |= c->alloc(&d_off, nlev + 1);
+  rc |= c->alloc(&d_rows, lm);
+  rc |= c->alloc(&d_order, lm);
+  rc |= c->alloc(&d_nb, lm);
+  for (double** q : {&N.cd, &N.cW, &N.cS, &N.cN, &N.cE, &N.b, &N.u, &N.r, &N.z, &N.p, &N.q, &N.piv, &N.dinv})
+    rc |= c->alloc(q, (size_t)lm + 1);
+  if (rc) return rc;
+  CK(cudaMemcpy(d_off, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_rows, rows.data(), rows.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(d_nb, nb.data(), nb.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  N.lvl_off = d_off; N.lvl_row = d_rows; N.order = d_order; N.nbr = d_nb;
+  // scalars, alpha/beta record and Lanczos tridiagonal shared with the red-black system
+  N.sc = c->pcg.sc; N.hist_alpha = c->pcg.hist_alpha; N.hist_beta = c->pcg.hist_beta; N.tri = c->pcg.tri;
+  c->natural = true;
+  return 0;
+}
+
 int build_pcg(Ctx* c, const si3d_grid* g) {
   const int lm = g->lm, lm1 = lm + 1;
   std::vector<int> col;
@@ -492,6 +583,7 @@ int build_pcg(Ctx* c, const si3d_grid* g) {
   F.hist_alpha = P.hist_alpha; F.hist_beta = P.hist_beta; F.tri = nullptr;
   CK(cudaMallocHost(&c->h_scf, sizeof(PcgScal)));
   if (c->prm.precision == SI3D_MIXED_MG) return build_mg(c, g);
+  if (c->prm.ordering == SI3D_ORDER_NATURAL) return build_natural(c, g);
   return 0;
 }
 
@@ -709,6 +801,37 @@ int solve_mg(Ctx* c, const PcgScal& init, int x0, double* hist, int ier, int* it
 }
 
 // One zeta solve on the device (SolverSparse's call of nspcg, si3d_procedures.f90:1986-2003).
+// The zeta solve with the reference's own ordering: natural-order MIC-CG in one single-block launch.
+int solve_natural(Ctx* c, int x0, int ier, int* iters, double* relres, int* ier_out) {
+  int rc = stage(c, ST_PCG_SETUP, 1, [&] { nat_setup(c->d, c->nat, x0, c->dz, c->st); });
+  if (rc) return rc;
+  if (c->prof) CK(cudaEventRecord(c->pe0, c->st));
+  if (nat_solve(c->nat, c->prm.pcg_test == 2, c->st) != 0) return cuda_fail(cudaGetLastError(), "nat_solve", __LINE__);
+  c->launches += 1;
+  CK(cudaMemcpyAsync(c->h_sc, c->nat.sc, sizeof(PcgScal), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const PcgScal& S = *c->h_sc;
+  if (!S.done) return SI3D_ETIMEOUT;
+  if (c->prof) {
+    CK(cudaEventRecord(c->pe1, c->st));
+    CK(cudaEventSynchronize(c->pe1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->pe0, c->pe1);
+    c->prof_ms[ST_PCG_ITER] += ms;
+    c->prof_n[ST_PCG_ITER] += S.in;
+  }
+  if (c->log_solves) std::fprintf(stderr, "si3d: natural-order solve: %d iterations\n", S.in);
+  rc = stage(c, ST_PCG_FINISH, 1, [&] { nat_finish(c->d, c->nat, c->st); });
+  if (rc) return rc;
+  if (S.negpiv & 2) ier = -12;
+  else if (S.ier != 0) ier = S.ier;
+  else if ((S.negpiv & 1) && ier == 0) ier = 5;
+  *iters = S.in;
+  *relres = S.stptst;
+  *ier_out = ier;
+  return 0;
+}
+
 int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   const si3d_params& p = c->prm;
   PcgScal init{};
@@ -723,7 +846,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   init.hist_cap = p.pcg_itmax + 1;
   if (c->graph_mode) {
     // the scalars are set by a kernel (a host copy would capture a host buffer that later solves reuse)
-    if (p.precision != SI3D_FP64 || !c->persistent || c->rec_buf) return SI3D_EDIMS;
+    if (p.precision != SI3D_FP64 || !c->persistent || c->rec_buf || c->natural) return SI3D_EDIMS;
     pcg_init_scalars(c->pcg.sc, init, c->st);
     c->launches += 1;
   } else {
@@ -754,6 +877,7 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   const bool use_hist = p.x0_mode == SI3D_X0_HIST;
   double* hist = use_hist ? c->hist + (size_t)c->hist_slot * (c->pcg.R.n + c->pcg.B.n + 2) : nullptr;
   if (p.precision == SI3D_MIXED_MG) return solve_mg(c, init, x0, hist, ier, iters, relres, ier_out);
+  if (c->natural) return solve_natural(c, x0, ier, iters, relres, ier_out);
   int rc0 = stage(c, ST_PCG_SETUP, 7, [&] { pcg_setup(c->d, c->pcg, x0, c->dz, hist, &c->pcg.sc->negpiv, c->st); });
   if (rc0) return rc0;
   if (c->graph_mode) {
@@ -889,6 +1013,11 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
   if (prm->itrmom != 1 || prm->ihd > 1 || prm->pcg_itmax < 1 || (prm->pcg_test != 5 && prm->pcg_test != 2))
     return SI3D_EDIMS;
   if (prm->x0_mode < SI3D_X0_PREV || prm->x0_mode > SI3D_X0_HIST) return SI3D_EDIMS;
+  // 0 is taken as the default red-black ordering; the natural ordering is the plain FP64 solve only
+  if (prm->ordering != 0 && prm->ordering != SI3D_ORDER_REDBLACK && prm->ordering != SI3D_ORDER_NATURAL)
+    return SI3D_EDIMS;
+  if (prm->ordering == SI3D_ORDER_NATURAL && (prm->precision != SI3D_FP64 || prm->x0_mode == SI3D_X0_HIST))
+    return SI3D_EDIMS;
   if (prm->ntr < 0 || prm->ntr > 30) return SI3D_EDIMS;   // ntrmax (si3d_types.f90:291)
   if (prm->iturb != 0 && prm->iturb != 1) return SI3D_EDIMS;
   // every kernel indexes neighbours through the maps and layers down to kmz + 1: both are checked
@@ -1530,7 +1659,7 @@ int si3d_ens_create(const int* handles, int n, int* ens) {
     Ctx* c = get(handles[i]);
     if (!c) return SI3D_EHANDLE;
     if (i == 0) E->device = c->device;
-    if (c->device != E->device || c->prm.precision != SI3D_FP64 || !c->persistent) return SI3D_EDIMS;
+    if (c->device != E->device || c->prm.precision != SI3D_FP64 || !c->persistent || c->natural) return SI3D_EDIMS;
     for (int j = 0; j < i; ++j)
       if (handles[j] == handles[i]) return SI3D_EDIMS;
     E->hs.push_back(handles[i]);
@@ -1816,11 +1945,12 @@ int si3d_gpu_sync(int h) {
 }
 
 int si3d_gpu_solve_zeta(int lm, const double* coef, const int* jcoef, const double* rhs, double* zeta, int pcg_test,
-                        double pcg_tol, int pcg_itmax, double srelpr, int precision, int* iters, double* stptst,
-                        double* emin, double* emax) {
+                        double pcg_tol, int pcg_itmax, double srelpr, int precision, int ordering, int* iters,
+                        double* stptst, double* emin, double* emax) {
   if (lm < 1 || !coef || !jcoef || !rhs || !zeta || pcg_itmax < 1 || (pcg_test != 5 && pcg_test != 2))
     return SI3D_EDIMS;
   if (precision != SI3D_FP64 && precision != SI3D_MIXED_IR) return SI3D_EDIMS;
+  if (ordering != 0 && ordering != SI3D_ORDER_REDBLACK && ordering != SI3D_ORDER_NATURAL) return SI3D_EDIMS;
   // Recover the grid graph and sx/sy from the SolverSparse structure:
   // coef = [rr, -sx(lW), -sy(lS), -sy(l), -sx(l)], jcoef = [l, lWC, lSC, lNC, lEC] (0 = dry).
   const int lm1 = lm + 1;
@@ -1852,7 +1982,8 @@ int si3d_gpu_solve_zeta(int lm, const double* coef, const int* jcoef, const doub
   si3d_params prm{};
   prm.dt = 1; prm.dx = 1; prm.dy = 1; prm.theta = 1; prm.itrmom = 1; prm.ihd = 1;
   prm.pcg_test = pcg_test; prm.pcg_tol = pcg_tol; prm.pcg_itmax = pcg_itmax; prm.srelpr = srelpr;
-  prm.ordering = SI3D_ORDER_REDBLACK; prm.x0_mode = SI3D_X0_PREV; prm.precision = precision;
+  prm.ordering = ordering == SI3D_ORDER_NATURAL ? SI3D_ORDER_NATURAL : SI3D_ORDER_REDBLACK;
+  prm.x0_mode = SI3D_X0_PREV; prm.precision = precision;
   int hdl = -1;
   int rc = si3d_gpu_init(&g, &prm, 0, &hdl);
   if (rc) return rc;

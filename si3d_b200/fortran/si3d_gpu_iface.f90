@@ -109,10 +109,10 @@
       END FUNCTION
 
       INTEGER(C_INT) FUNCTION si3d_gpu_solve_zeta(lm, coeffA, jcoefA, rhs, zeta, pcg_test, pcg_tol, pcg_itmax, &
-                                                  srelpr, precision, iters, stptst, emin, emax)            &
+                                                  srelpr, precision, ordering, iters, stptst, emin, emax)  &
                                                   BIND(C, NAME="si3d_gpu_solve_zeta")
          IMPORT :: C_INT, C_DOUBLE
-         INTEGER(C_INT), VALUE         :: lm, pcg_test, pcg_itmax, precision
+         INTEGER(C_INT), VALUE         :: lm, pcg_test, pcg_itmax, precision, ordering
          REAL(C_DOUBLE), VALUE         :: pcg_tol, srelpr
          REAL(C_DOUBLE), INTENT(IN)    :: coeffA(*), rhs(*)
          INTEGER(C_INT), INTENT(IN)    :: jcoefA(*)

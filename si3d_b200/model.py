@@ -22,10 +22,10 @@ class GpuRun:
 
     def __init__(self, run_dir: str, *, device: int = 0, pcg_test: int = 5, pcg_tol: float = 1e-12,
                  pcg_itmax: int = 200, srelpr: float = 2.220446049250313e-16, x0_mode: int = native.SI3D_X0_PREV,
-                 precision: int = native.SI3D_FP64, autotune: bool = False):
+                 precision: int = native.SI3D_FP64, autotune: bool = False, ordering: int = native.SI3D_ORDER_REDBLACK):
         self.h = native.host()
         self.g = native.gpu()
-        opts = SolverOpts(pcg_test, pcg_tol, pcg_itmax, srelpr, x0_mode, precision)
+        opts = SolverOpts(pcg_test, pcg_tol, pcg_itmax, srelpr, x0_mode, precision, ordering)
         hm = C.c_int(-1)
         err = C.create_string_buffer(512)
         rc = self.h.si3d_host_open(run_dir.encode(), C.byref(opts), C.byref(hm), err, 512)
@@ -141,7 +141,7 @@ class GpuRun:
 
 def solve_zeta(coef: np.ndarray, jcoef: np.ndarray, rhs: np.ndarray, x0: np.ndarray, *, pcg_test: int = 5,
                tol: float = 1e-12, itmax: int = 200, srelpr: float = 2.220446049250313e-16,
-               precision: int = native.SI3D_FP64):
+               precision: int = native.SI3D_FP64, ordering: int = native.SI3D_ORDER_REDBLACK):
     """Standalone replacement of the reference's nspcg(mic1, cg, ...) call on Purdue arrays."""
     g = native.gpu()
     lm = rhs.shape[0]
@@ -152,7 +152,7 @@ def solve_zeta(coef: np.ndarray, jcoef: np.ndarray, rhs: np.ndarray, x0: np.ndar
     it = C.c_int(0)
     st, e0, e1 = C.c_double(0), C.c_double(0), C.c_double(0)
     rc = g.si3d_gpu_solve_zeta(lm, native.ptr(c), native.ptr(j), native.ptr(b), native.ptr(x), pcg_test, tol, itmax,
-                               srelpr, precision, C.byref(it), C.byref(st), C.byref(e0), C.byref(e1))
+                               srelpr, precision, ordering, C.byref(it), C.byref(st), C.byref(e0), C.byref(e1))
     check(rc)
     return x, dict(iters=it.value, stptst=st.value, emin=e0.value, emax=e1.value, ier=rc)
 

@@ -16,6 +16,7 @@ SI3D_FP64 = 0
 SI3D_MIXED_IR = 1
 SI3D_MIXED_MG = 2
 SI3D_ORDER_REDBLACK = 1
+SI3D_ORDER_NATURAL = 2
 SI3D_X0_PREV, SI3D_X0_ZERO, SI3D_X0_LEARNED, SI3D_X0_LAST, SI3D_X0_HIST = 0, 1, 2, 3, 4
 
 
@@ -53,7 +54,7 @@ class StepStats(C.Structure):
 
 class SolverOpts(C.Structure):
     _fields_ = [("pcg_test", C.c_int), ("pcg_tol", C.c_double), ("pcg_itmax", C.c_int), ("srelpr", C.c_double),
-                ("x0_mode", C.c_int), ("precision", C.c_int)]
+                ("x0_mode", C.c_int), ("precision", C.c_int), ("ordering", C.c_int)]
 
 
 GPU_SYMBOLS = {
@@ -71,7 +72,7 @@ GPU_SYMBOLS = {
     "si3d_gpu_step": (C.c_int, [C.c_int, C.c_int, C.POINTER(StepStats)]),
     "si3d_gpu_set_warmstart": (C.c_int, [C.c_int, C.c_void_p, C.c_int]),
     "si3d_gpu_solve_zeta": (C.c_int, [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
-                                      C.c_int, C.c_double, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
+                                      C.c_int, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double),
                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "si3d_gpu_column_tridiag": (C.c_int, [C.c_int, C.c_int] + [C.c_void_p] * 7),
     "si3d_gpu_column_tridiag_noalloc": (C.c_int, [C.c_int, C.c_int] + [C.c_void_p] * 8),

@@ -97,6 +97,12 @@ def test_bad_arguments_are_rejected(native_libs):
     grid.k1 = 2
     prm.itrmom = 2                                  # only itrmom = 1 is on the path
     assert g.si3d_gpu_init(C.byref(grid), C.byref(prm), 0, C.byref(h)) == -101
+    prm.itrmom = 1
+    prm.ordering = 3                                # red-black (0, 1) or natural (2)
+    assert g.si3d_gpu_init(C.byref(grid), C.byref(prm), 0, C.byref(h)) == -101
+    prm.ordering, prm.precision = 2, 1              # the natural ordering is the plain FP64 solve
+    assert g.si3d_gpu_init(C.byref(grid), C.byref(prm), 0, C.byref(h)) == -101
+    prm.ordering, prm.precision = 1, 0
     assert g.si3d_gpu_fd(12345, 1, 1, 0, None) == -102
     assert g.si3d_gpu_sync(-1) == -102
 
