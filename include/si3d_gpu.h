@@ -246,6 +246,22 @@ int si3d_gpu_autotune(int handle, int reps, int* choice);
 /* Apply a launch-shape choice (e.g. a cached autotuner result). */
 int si3d_gpu_set_tune(int handle, const int* choice);
 
+/* Open boundaries with a specified water-surface elevation (the reference's itype = 1), replacing
+ * the boundary set-up of openbc0 (si3d_boundaryconditions.f90:23-897) and the per-stage
+ * adjustments openbcUVH (:900), MODexmom4openBCX/Y (:1801, :2370), MODqqddrr4openBC (:1508),
+ * MODvel4openBC (:2941) and openbcSCA (:3157), which the library then applies inside si3d_gpu_fd,
+ * si3d_gpu_settrap, si3d_gpu_settrap2 and si3d_gpu_save.  Per boundary nn (0-based arrays of nopen):
+ * side iside (1 W, 2 N, 3 E, 4 S), itype (must be 1), the cell range isbc/jsbc/iebc/jebc in the
+ * reference's 1-based (i, j); every boundary cell must be wet with a dry cell outside it and a wet
+ * one inside.  The series (elevation wse and temperature temp, [nopen][npts] row-major) hold one
+ * value every dtsec seconds from t = 0 and are interpolated as parab does (si3d_utils.f90:895)
+ * at the step's time n * dt; a step past their end returns SI3D_EDIMS.  The host sets sp of the
+ * boundary cells to the first value at t = 0, as openbc0 does.  Not with SI3D_MIXED_IR, tracers or
+ * ensembles (SI3D_EDIMS). */
+int si3d_gpu_set_open_boundaries(int handle, int nopen, const int* iside, const int* itype, const int* isbc,
+                                 const int* jsbc, const int* iebc, const int* jebc, double dtsec, int npts,
+                                 const double* wse, const double* temp);
+
 /* Wait for the handle's stream. */
 int si3d_gpu_sync(int handle);
 /* Test hook for the bounded device waits (no counterpart in the reference).  The next cooperative

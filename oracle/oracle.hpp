@@ -69,6 +69,14 @@ struct Inp {
   std::vector<int> p_out;   // output planes (si3d_utils.f90:80-83)
 };
 
+// One open boundary (si3d_utils.f90:124-140): side (1 W, 2 N, 3 E, 4 S), type (1 = water-surface
+// elevation specified, the only type restated), the cell range, and the series read from its
+// openbcNN.txt file (openbc0, si3d_boundaryconditions.f90:55-91): wse and the scalar (temperature).
+struct OpenBC {
+  int iside = 0, itype = 0, isbc = 0, jsbc = 0, iebc = 0, jebc = 0;
+  std::vector<double> wse, sal;
+};
+
 // Calendar of compute_date (si3d_utils.f90:3546-3674); REAL variables as double.
 struct Date {
   int iyr = 0, imon = 0, iday = 0, ihr = 0, iyrp = 0, imonp = 0, idayp = 0, ihrp = 0;
@@ -131,6 +139,10 @@ struct Model {
   Date date;
   std::shared_ptr<FILE> f_ptrack;
   std::vector<std::shared_ptr<FILE>> f_tracer, f_plane;
+  // open boundaries (nopen > 0): records, series spacing dtsecOpenBC (s), hours of the current step
+  std::vector<OpenBC> obc;
+  double dtsec_obc = 0;
+  double thrs = 0;
   // per-column wind override (harness overlay; surfbc CASE 0 otherwise)
   bool wind_override = false;
   std::vector<real> uair_ovr, vair_ovr;  // l-indexed (1..lm)
@@ -144,6 +156,15 @@ struct Model {
 
 // I/O and setup
 bool read_inputs(Model& m, const std::string& dir);  // input + ZGridDimensions + bathy + init
+// open boundaries (oracle_obc.cpp)
+bool read_openbc_files(Model& m, const std::string& dir);   // the openbcNN.txt series
+bool openbc0(Model& m);                                      // checks and sp at t = 0
+bool openbc_uvh(Model& m);                                   // s on the boundary cells at thrs
+void mod_exmom_openbc(Model& m, int ieq);                    // ex of the faces at the boundaries
+void mod_qq_openbc(Model& m);                                // qq and sx/sy of the zeta system
+void mod_vel_openbc(Model& m);                               // vh/uh and wp of the boundary cells
+void openbc_sca(Model& m);                                   // temperature of the boundary cells
+double parab(double frstpt, double x, const std::vector<double>& fx, double dx);
 void compute_date(Model& m, double itime_sec);
 // Mellor-Yamada 2.5 (oracle_turb.cpp)
 void init_turbulence(Model& m);

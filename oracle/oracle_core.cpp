@@ -248,6 +248,7 @@ void exmom(Model& m, int ieq, ExCoef& C) {
       }
     });
   }
+  if (!m.obc.empty()) mod_exmom_openbc(m, ieq);   // MODexmom4openBCX/Y (:957, :1165)
 }
 
 // bclnc_km (si3d_procedures.f90:1633-1746); eps = EPSILON(0.0) of the working precision.
@@ -428,6 +429,7 @@ void matcon(Model& m) {
     m.qq(l) = m.spp(l) - dtdx1 * (m.eagx(l) - m.eagx(lW)) - dtdy1 * (m.eagy(l) - m.eagy(lS)) - m.dd(l);
     m.rr(l) = 1 + m.sx(l) + m.sx(lW) + m.sy(l) + m.sy(lS);
   });
+  if (!m.obc.empty()) mod_qq_openbc(m);   // MODqqddrr4openBC (:1859), after rr
 }
 
 // slayer_h (si3d_procedures.f90:2070-2175)
@@ -532,6 +534,7 @@ void continuity(Model& m, int ist) {
         m.wp(k1s, l) = m.wp(k1s, l) - (m.uhp(k, l) - m.uhp(k, lW)) / m.dx - (m.vhp(k, l) - m.vhp(k, lS)) / m.dy;
     }
   });
+  if (!m.obc.empty()) mod_vel_openbc(m);   // MODvel4openBC (:2821)
 }
 
 // vel (si3d_procedures.f90:2430-2567)
@@ -1033,6 +1036,7 @@ void save(Model& m, int istep) {
 // fd (si3d_procedures.f90:382-575) for the hot-path configuration.
 bool fd(Model& m, ExCoef& C) {
   m.tz = 1.0 / m.istep;
+  if (!m.obc.empty() && !openbc_uvh(m)) return false;   // :423
   surfbc(m);
   exmom(m, 1, C);
   matmom(m, 1);
@@ -1040,8 +1044,13 @@ bool fd(Model& m, ExCoef& C) {
   matmom(m, 2);
   matcon(m);
   if (!solver_sparse(m)) return false;
+  if (!m.obc.empty() && !openbc_uvh(m)) return false;   // :482
   vel(m);
-  if (m.in.isal != 0) { exsal(m); imsal(m); }
+  if (m.in.isal != 0) {
+    exsal(m);
+    imsal(m);
+    if (!m.obc.empty()) openbc_sca(m);   // :515
+  }
   if (m.in.ntr > 0 && m.in.niter > 0 && m.lastiter == 1) tracers(m);
   vel2(m);
   if (m.in.ismooth >= 1 && m.istep == 1) { m.err = "ismooth>=1 is not on the hot path"; return false; }
@@ -1061,7 +1070,7 @@ bool run_stage(Model& m, const std::string& stage, int istep) {
   else if (stage == "matcon") matcon(m);
   else if (stage == "solve") return solver_sparse(m);
   else if (stage == "vel") vel(m);
-  else if (stage == "scalar") { exsal(m); imsal(m); }
+  else if (stage == "scalar") { exsal(m); imsal(m); if (!m.obc.empty()) openbc_sca(m); }
   else if (stage == "tracer") tracers(m);
   else if (stage == "turbulence") { if (m.in.iturb == 1) update_mixing(m, istep); }
   else if (stage == "vel2") vel2(m);
@@ -1079,6 +1088,7 @@ bool run_steps(Model& m, int nsteps) {
   C.haxpp.init(m.km1, m.lm1); C.haypp.init(m.km1, m.lm1); C.th.init(m.km1, m.lm1); C.th1.init(m.km1, m.lm1);
   for (int s = 0; s < nsteps; ++s) {
     m.n += 1;
+    m.thrs = (double)m.n * m.in.idt / 3600.;   // its = its + idt, thrs = its / 3600. (si3d.f90:326-327)
     compute_date(m, m.in.idt);   // si3d.f90:333
     int niter1 = m.in.niter;
     m.lastiter = 0;

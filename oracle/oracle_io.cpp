@@ -70,6 +70,22 @@ bool rec_i(Lines& L, int& v) {
   return true;
 }
 
+// '(14X,20I)' record: n integers after column 14, separated by blanks or commas.
+bool rec_ints(Lines& L, int n, std::vector<int>& out) {
+  const std::string rec = field(L.next(), 14, 1000);
+  out.clear();
+  size_t i = 0;
+  while ((int)out.size() < n) {
+    while (i < rec.size() && (rec[i] == ' ' || rec[i] == ',' || rec[i] == '\t')) ++i;
+    size_t j = i;
+    while (j < rec.size() && (std::isdigit((unsigned char)rec[j]) || rec[j] == '-')) ++j;
+    if (j == i) return false;
+    out.push_back(std::atoi(rec.substr(i, j - i).c_str()));
+    i = j;
+  }
+  return true;
+}
+
 }  // namespace
 
 // si3d_utils.f90:21-315 (records read in the order the reference reads them)
@@ -115,9 +131,24 @@ static bool read_inp(Model& m, const std::string& dir) {
   L.skip(3); ok &= rec_i(L, p.ipxml); ok &= rec_i(L, p.itspf); ok &= rec_i(L, p.iTurbVars);
   if (p.ipxml > 0 && p.iTurbVars != 0) { m.err = "turbulence variables in the 3-D output need iturb > 0"; return false; }
   if (p.nnodes > 0 || p.ipxml < 0) { m.err = "the time-series (outt) and XML (outs) writers are not restated"; return false; }
-  L.skip(3); ok &= rec_i(L, p.nopen);                                 // :125-145
-  if (p.nopen != 0) { m.err = "open boundaries (nopen>0) are outside the hot path"; return false; }
-  L.skip(7);
+  L.skip(3); ok &= rec_i(L, p.nopen);                                 // :124-145
+  if (p.nopen > 0) {
+    // dtsecopenbc, then iside, itype, isbc, jsbc, iebc, jebc, nopen values each
+    ok &= rec_g(L, m.dtsec_obc);
+    std::vector<int> v[6];
+    for (int r = 0; r < 6; ++r) ok &= rec_ints(L, p.nopen, v[r]);
+    if (!ok) { m.err = "si3d_inp.txt: bad open-boundary records"; return false; }
+    m.obc.assign(p.nopen, OpenBC{});
+    for (int nn = 0; nn < p.nopen; ++nn) {
+      OpenBC& b = m.obc[nn];
+      b.iside = v[0][nn]; b.itype = v[1][nn]; b.isbc = v[2][nn]; b.jsbc = v[3][nn]; b.iebc = v[4][nn]; b.jebc = v[5][nn];
+      if (b.itype != 1) { m.err = "only water-surface-elevation open boundaries (itype = 1) are restated"; return false; }
+      if (b.iside < 1 || b.iside > 4) { m.err = "open boundary side must be 1..4"; return false; }
+    }
+    if (!(m.dtsec_obc > 0)) { m.err = "dtsecopenbc must be positive"; return false; }
+  } else {
+    L.skip(7);
+  }
   L.skip(3); ok &= rec_i(L, p.nxNBO);                                 // ioNBTOGGLE=1 block
   if (p.nxNBO != 0) { m.err = "nested-boundary output (nxNBO>0) is not supported"; return false; }
   L.skip(7);
@@ -128,6 +159,7 @@ static bool read_inp(Model& m, const std::string& dir) {
     if (p.ntr > 30) { m.err = "ntr > ntrmax = 30 (si3d_types.f90:291)"; return false; }
     // srcsnk00 (si3d_ecomod.f90:24-34): conservative tracers; the other models are not restated
     if (p.ecomod != 0) { m.err = "only conservative tracers (ecomod=0) are restated"; return false; }
+    if (p.nopen > 0) { m.err = "tracers at open boundaries (openbcTracer) are not restated"; return false; }
   } else {
     L.skip(5);
   }
@@ -380,6 +412,7 @@ bool read_inputs(Model& m, const std::string& dir) {
   if (!read_init_profile(m, dir, prof)) return false;
   if (!read_wind_override(m, dir)) return false;
   init_state(m, prof);
+  if (!m.obc.empty() && (!read_openbc_files(m, dir) || !openbc0(m))) return false;   // si3d.f90:64
   return write_outputs(m, 0);   // initial frames (si3d.f90:89-100)
 }
 

@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "_lib")
 
 CUDA_SOURCES = ["si3d_gpu.cu", "k_momentum.cu", "k_zeta.cu", "k_pcg_persistent.cu", "k_transport.cu", "k_learn.cu",
-                "noalloc.cu", "k_mg.cu", "k_tracer.cu", "k_output.cu", "k_turb.cu"]
+                "noalloc.cu", "k_mg.cu", "k_tracer.cu", "k_output.cu", "k_turb.cu", "k_openbc.cu"]
 CUDA_DEPS = CUDA_SOURCES + ["common.cuh", "coop.cuh", "kernels.h", "learn.h", "mg.h"]
 HOST_SOURCES = [os.path.join("host", "si3d_host.cpp")]
 

@@ -44,6 +44,21 @@ struct Records {
 };
 
 // Value of a fixed-width numeric field (blanks ignored, empty = 0, D exponents allowed).
+// Integers of a '(14X,20I)' record (separated by blanks or commas); false when fewer than n.
+bool int_list(const std::string& rec, int n, std::vector<int>& out) {
+  out.clear();
+  size_t i = 14;
+  while ((int)out.size() < n) {
+    while (i < rec.size() && (rec[i] == ' ' || rec[i] == ',' || rec[i] == '\t')) ++i;
+    size_t j = i;
+    while (j < rec.size() && (std::isdigit((unsigned char)rec[j]) || rec[j] == '-')) ++j;
+    if (j == i) return false;
+    out.push_back(std::atoi(rec.substr(i, j - i).c_str()));
+    i = j;
+  }
+  return true;
+}
+
 bool numeric(const std::string& row, size_t col, size_t width, double& v) {
   std::string t;
   for (size_t i = col; i < std::min(row.size(), col + width); ++i) {
@@ -75,6 +90,11 @@ struct HostModel {
   std::vector<double> s0, hp0, hup0, hvp0, salp0, Av0f, Dv0f, uair, vair, cdw;
   std::vector<double> tracer0;   // ntr fields of (km1, lm1), column-major
   std::vector<double> q2l0;      // iturb = 1: initial q2l (InitializeTurbulenceModel CASE(1))
+  // open boundaries (si3d_utils.f90:124-140 and the openbcNN.txt series, openbc0 :55-91)
+  double obc_dtsec = 0;
+  std::vector<int> ob_side, ob_type, ob_is, ob_js, ob_ie, ob_je;
+  int ob_npts = 0;
+  std::vector<double> ob_wse, ob_tmp;   // [nopen][ob_npts]
   // outputs (si3d_utils.f90:72-121, :172-181) and the date of compute_date (:3546-3674)
   int iyr0 = 0, imon0 = 0, iday0 = 0, ihr0 = 0;
   int iop = 0, itspfh = 0, n_planes = 0, ipxml = 0, itspf = 0, iTurbVars = 0, iotr = 0, itspftr = 0;
@@ -164,18 +184,27 @@ bool read_parameters(HostModel& M, const std::string& dir) {
   }
   R.skip(3); gi(M.iox);
   R.skip(3); gi(M.ipxml); gi(M.itspf); gi(M.iTurbVars);
-  R.skip(3); gi(M.nopen); R.skip(7);
+  R.skip(3); gi(M.nopen);
+  if (M.nopen > 0) {
+    g(M.obc_dtsec);
+    for (std::vector<int>* v : {&M.ob_side, &M.ob_type, &M.ob_is, &M.ob_js, &M.ob_ie, &M.ob_je})
+      if (!int_list(R.take(), M.nopen, *v)) { M.err = "si3d_inp.txt: bad open-boundary record"; return false; }
+    for (int t : M.ob_type)
+      if (t != 1) { M.err = "si3d_inp.txt: only water-surface-elevation open boundaries (itype = 1) are built"; return false; }
+  } else {
+    R.skip(7);
+  }
   R.skip(3); gi(M.nxNBO); R.skip(7);
   R.skip(3); gi(M.ntr);                          // tracer block (si3d_utils.f90:172-190)
   if (M.ntr > 0) { gi(M.ecomod); gi(M.iotr); gi(M.itspftr); gi(dummy); gi(dummy); }   // ipwq nswq unused
   else R.skip(5);
   R.skip(3); gi(M.iopss);
   if (!ok) { M.err = "si3d_inp.txt: unreadable record"; return false; }
-  if (M.iox || M.nopen || M.nxNBO || M.iopss || M.ifsurfbc || (M.iturb != 0 && M.iturb != 1) || M.ihd > 1 || M.ibathyf < 0 ||
+  if (M.nopen > 0 && M.ntr > 0) { M.err = "si3d_inp.txt: tracers at open boundaries (openbcTracer) are not built"; return false; }
+  if (M.iox || M.nxNBO || M.iopss || M.ifsurfbc || (M.iturb != 0 && M.iturb != 1) || M.ihd > 1 || M.ibathyf < 0 ||
       M.ismooth || M.itrmom != 1) {
-    M.err = "si3d_inp.txt selects an option outside the semi-implicit core (open boundaries, point "
-            "sources, heat budget, turbulence closure, Smagorinsky, smoothing, non-centred advection or "
-            "variable layers)";
+    M.err = "si3d_inp.txt selects an option outside the semi-implicit core (point sources, heat budget, "
+            "turbulence closure, Smagorinsky, smoothing, non-centred advection or variable layers)";
     return false;
   }
   if (nnodes > 0 || M.ipxml < 0) {
@@ -592,13 +621,46 @@ int write_outputs(HostModel& M, int n) {
 
 extern "C" {
 
+// The series of each open boundary: openbcNN.txt with five header records, the record count in
+// '(10X,I7)', then '(10X,(ntr+2)G11.2)' records of which the first two values (elevation,
+// temperature) are used (openbc0, si3d_boundaryconditions.f90:55-91).
+bool read_openbc(HostModel& M, const std::string& dir) {
+  std::vector<std::vector<double>> w(M.nopen), t(M.nopen);
+  int npts = -1;
+  for (int nn = 1; nn <= M.nopen; ++nn) {
+    char name[32];
+    std::snprintf(name, sizeof name, "openbc%02d.txt", nn);
+    Records R;
+    if (!R.load(dir + "/" + name)) { M.err = std::string("cannot open ") + name; return false; }
+    R.skip(5);
+    double np = 0;
+    if (!numeric(R.take(), 10, 7, np) || np < 3) { M.err = std::string(name) + ": bad record count"; return false; }
+    for (int j = 0; j < (int)np; ++j) {
+      if (!R.more()) { M.err = std::string(name) + ": truncated"; return false; }
+      const std::string row = R.take();
+      double a = 0, b = 0;
+      if (!numeric(row, 10, 11, a) || !numeric(row, 21, 11, b)) { M.err = std::string(name) + ": bad value"; return false; }
+      w[nn - 1].push_back(a);
+      t[nn - 1].push_back(b);
+    }
+    npts = npts < 0 ? (int)np : std::min(npts, (int)np);
+  }
+  M.ob_npts = npts;
+  for (int nn = 0; nn < M.nopen; ++nn) {
+    M.ob_wse.insert(M.ob_wse.end(), w[nn].begin(), w[nn].begin() + npts);
+    M.ob_tmp.insert(M.ob_tmp.end(), t[nn].begin(), t[nn].begin() + npts);
+  }
+  return true;
+}
+
 int si3d_host_open(const char* run_dir, const si3d_solver_opts* opts, int* hm, char* err, int errlen) {
   auto M = std::make_unique<HostModel>();
   if (opts) M->opt = *opts;
   else { M->opt.pcg_test = 5; M->opt.pcg_tol = 1e-12; M->opt.pcg_itmax = 200; M->opt.srelpr = 2.220446049250313e-16; }
   const std::string dir = run_dir ? run_dir : ".";
   std::vector<double> prof;
-  bool ok = read_parameters(*M, dir) && read_bathymetry(*M, dir) && read_profile(*M, dir, prof) && read_wind(*M, dir);
+  bool ok = read_parameters(*M, dir) && read_bathymetry(*M, dir) && read_profile(*M, dir, prof) && read_wind(*M, dir) &&
+            (M->nopen == 0 || read_openbc(*M, dir));
   if (!ok) {
     if (err && errlen > 0) { std::strncpy(err, M->err.c_str(), errlen - 1); err[errlen - 1] = 0; }
     return SI3D_EDIMS;
@@ -664,6 +726,24 @@ int si3d_host_attach_gpu(int h, int device, int* gpu_handle) {
   // initial fields (init: s = sp = spp; hpp = hp = h; k1 indices; sal = salp = salpp; Av/Dv)
   const char* same_s[] = {"s", "sp", "spp"};
   for (const char* nm : same_s) if ((rc = si3d_gpu_set_field(gh, nm, M->s0.data()))) return rc;
+  if (M->nopen > 0) {
+    // openbc0 (si3d.f90:64, after init): the boundary cells' sp takes the series' first value
+    std::vector<double> sp0 = M->s0;
+    for (int nn = 0; nn < M->nopen; ++nn) {
+      const bool x = M->ob_side[nn] == 1 || M->ob_side[nn] == 3;
+      const int a = x ? M->ob_js[nn] : M->ob_is[nn], e = x ? M->ob_je[nn] : M->ob_ie[nn];
+      for (int q = a; q <= e; ++q) {
+        const int i = x ? M->ob_is[nn] : q, j = x ? q : M->ob_js[nn];
+        if (i < 1 || j < 1 || i > M->im1 || j > M->jm1 || !M->W(i, j)) return SI3D_EDIMS;
+        sp0[M->L(i, j) - 1] = M->ob_wse[(size_t)nn * M->ob_npts];
+      }
+    }
+    if ((rc = si3d_gpu_set_field(gh, "sp", sp0.data()))) return rc;
+    if ((rc = si3d_gpu_set_open_boundaries(gh, M->nopen, M->ob_side.data(), M->ob_type.data(), M->ob_is.data(),
+                                           M->ob_js.data(), M->ob_ie.data(), M->ob_je.data(), M->obc_dtsec,
+                                           M->ob_npts, M->ob_wse.data(), M->ob_tmp.data())))
+      return rc;
+  }
   const char* same_h[] = {"h", "hp", "hpp"};
   for (const char* nm : same_h) if ((rc = si3d_gpu_set_field(gh, nm, M->hp0.data()))) return rc;
   const char* same_hu[] = {"hu", "hup", "hupp"};

@@ -70,7 +70,7 @@ __global__ void k_mg_setup(Dev d, MgDev M, int x0_mode, const double* __restrict
   const double sxi = d.s.sx[l - 1], syi = d.s.sy[l - 1];
   const double sxW = (lW != lm1) ? d.s.sx[lW - 1] : 0.0;
   const double syS = (lS != lm1) ? d.s.sy[lS - 1] : 0.0;
-  const double diag = 1 + sxi + sxW + syi + syS;
+  const double diag = d.s.rr[l - 1];   // matcon's 1 + sx + sx(W) + sy + sy(S), before any face cut
   const double fN = (lN != lm1) ? syi : 0.0;   // face to (i, j + 1): the next column
   const double fE = (lE != lm1) ? sxi : 0.0;   // face to (i + 1, j): the next row
   M.fc64[o] = fN;

@@ -338,13 +338,16 @@ int momentum_init(int km1) {
 }
 
 template <int IEQ>
-void launch_dir(const Dev& d, const FaceMeta* cols, int ncols, const Tune& tu, cudaStream_t st) {
+void launch_dir(const Dev& d, const FaceMeta* cols, int ncols, const Tune& tu, cudaStream_t st, const ObcDev* obc,
+                int nobc) {
   const int g1 = (ncols + CW - 1) / CW;
   switch (tu.mom_cl) {
     case 2: k_mom_cells<IEQ, 2><<<g1, dim3(CW, 2), 0, st>>>(d, cols, ncols); break;
     case 4: k_mom_cells<IEQ, 4><<<g1, dim3(CW, 4), 0, st>>>(d, cols, ncols); break;
     default: k_mom_cells<IEQ, 8><<<g1, dim3(CW, 8), 0, st>>>(d, cols, ncols); break;
   }
+  // open boundaries: MODexmom4openBCX/Y replace the explicit term of their face columns
+  for (int b = 0; b < nobc; ++b) obc_exmom(d, obc[b], IEQ, st);
   switch (tu.mom_nt) {
     case 64: k_mom_columns<IEQ, 64><<<(ncols + 63) / 64, 64, 0, st>>>(d, cols, ncols); break;
     case 256: k_mom_columns<IEQ, 256><<<(ncols + 255) / 256, 256, 0, st>>>(d, cols, ncols); break;
@@ -352,10 +355,11 @@ void launch_dir(const Dev& d, const FaceMeta* cols, int ncols, const Tune& tu, c
   }
 }
 
-void launch_momentum(const Dev& d, int ieq, const FaceMeta* cols, int ncols, const Tune& tu, cudaStream_t st) {
+void launch_momentum(const Dev& d, int ieq, const FaceMeta* cols, int ncols, const Tune& tu, cudaStream_t st,
+                     const ObcDev* obc, int nobc) {
   if (ncols <= 0) return;
-  if (ieq == 1) launch_dir<1>(d, cols, ncols, tu, st);
-  else launch_dir<2>(d, cols, ncols, tu, st);
+  if (ieq == 1) launch_dir<1>(d, cols, ncols, tu, st, obc, nobc);
+  else launch_dir<2>(d, cols, ncols, tu, st, obc, nobc);
 }
 
 }  // namespace si3d

@@ -159,7 +159,7 @@ __device__ __noinline__ void lz_chgcon(PcgScal* S, double* tri, int ip, double a
 
 // TEST2: stopping test 2 with chgcon's adaptive emin (test 5 otherwise); a separate instantiation keeps
 // the test-5 loop free of the eigenvalue code.
-template <typename T, bool TEST2>
+template <typename T, bool TEST2, bool DIAG>
 __global__ void __launch_bounds__(PQB, 1) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
   __shared__ double sh[(PQB / 32) * 4 + 4];
   __shared__ BarSt s_flag;
@@ -321,7 +321,7 @@ __global__ void __launch_bounds__(PQB, 1) k_pcg_loop(PcgDevT<T> P, GridBar* bar)
         const T pN = O.z[q4.z] + bt * Op[q4.z];
         const T pE = O.z[q4.w] + bt * Op[q4.w];
         const T sxW = O.sx[q4.x], syS = O.sy[q4.y];
-        const T diag = (T)1 + C.sx[i] + sxW + C.sy[i] + syS;
+        const T diag = DIAG ? C.diag[i] : (T)1 + C.sx[i] + sxW + C.sy[i] + syS;
         T y = diag * pi;
         y = y + (-sxW) * pW;
         y = y + (-syS) * pS;
@@ -374,8 +374,11 @@ int launch_loop(const PcgDevT<T>& P, GridBar* bar, int nblocks, bool test2, cuda
   attr[0].val.cooperative = 1;
   cfg.attrs = attr;
   cfg.numAttrs = 1;
-  const cudaError_t e = test2 ? cudaLaunchKernelEx(&cfg, k_pcg_loop<T, true>, P, bar)
-                              : cudaLaunchKernelEx(&cfg, k_pcg_loop<T, false>, P, bar);
+  cudaError_t e;
+  if (P.diag_stored) e = test2 ? cudaLaunchKernelEx(&cfg, k_pcg_loop<T, true, true>, P, bar)
+                               : cudaLaunchKernelEx(&cfg, k_pcg_loop<T, false, true>, P, bar);
+  else e = test2 ? cudaLaunchKernelEx(&cfg, k_pcg_loop<T, true, false>, P, bar)
+                 : cudaLaunchKernelEx(&cfg, k_pcg_loop<T, false, false>, P, bar);
   return e == cudaSuccess ? 0 : -1;
 }
 
@@ -611,7 +614,7 @@ __global__ void k_nat_gather(Dev d, NatDev N, int x0_mode, const double* __restr
   const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l), lN = NB(d.g.lNC, l), lE = NB(d.g.lEC, l);
   const double sxi = d.s.sx[l - 1], syi = d.s.sy[l - 1];
   const double sxW = lW != lm1 ? d.s.sx[lW - 1] : 0.0, syS = lS != lm1 ? d.s.sy[lS - 1] : 0.0;
-  N.cd[i] = 1 + sxi + sxW + syi + syS;
+  N.cd[i] = d.s.rr[l - 1];   // 1 + sx + sx(W) + sy + sy(S), formed before open boundaries cut faces
   N.cW[i] = lW != lm1 ? -sxW : 0.0;
   N.cS[i] = lS != lm1 ? -syS : 0.0;
   N.cN[i] = lN != lm1 ? -syi : 0.0;
@@ -640,11 +643,14 @@ int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   int occ2 = 0;
   if (fp32) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<float, false>, PQB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<float, false, false>, PQB, 0);
     occ2 = occ;
   } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<double, false>, PQB, 0);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_pcg_loop<double, true>, PQB, 0);
+    int occ3 = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop<double, false, false>, PQB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k_pcg_loop<double, true, true>, PQB, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ3, k_pcg_loop<double, true, false>, PQB, 0);
+    occ2 = std::min(occ2, occ3);
   }
   occ = std::min(occ, occ2);
   int per_sm = occ;

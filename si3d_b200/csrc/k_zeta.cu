@@ -126,13 +126,15 @@ __global__ void k_pcg_gather(Dev d, PcgDev P, int color, int x0_mode, const doub
   if (i == C.n) {  // the permanent zero slot
     C.sx[i] = 0.0; C.sy[i] = 0.0; C.u[i] = 0.0; C.r[i] = 0.0; C.z[i] = 0.0; C.p[i] = 0.0; C.p2[i] = 0.0;
     C.q[i] = 0.0;
-    C.rhs[i] = 0.0; C.dinv[i] = 0.0;
+    C.rhs[i] = 0.0; C.dinv[i] = 0.0; C.diag[i] = 0.0;
     return;
   }
   const int l = C.l[i];
   C.sx[i] = d.s.sx[l - 1];
   C.sy[i] = d.s.sy[l - 1];
   C.rhs[i] = d.s.qq[l - 1];
+  // matcon's rr: 1 + sx + sx(W) + sy + sy(S), formed before open boundaries cut their faces
+  C.diag[i] = d.s.rr[l - 1];
   // x0: sp (the reference), zero, sp + learned increment, s (the latest accepted solution),
   // or s + this solve's correction one step earlier
   double x0;
@@ -152,11 +154,10 @@ __global__ void k_pcg_factor_red(PcgDev P) {
   const PcgColor &R = P.R, &B = P.B;
   if (i >= R.n) return;
   const int4 nb = R.nbr[i];
-  const double diag = 1 + R.sx[i] + B.sx[nb.x] + R.sy[i] + B.sy[nb.y];
+  const double diag = R.diag[i];
   R.dinv[i] = 1.0 / diag;
   // row sum of the upper triangle T (icfp wksp, nspcg.f:20786-20789), columns W, S, N, E
   const double tW = -B.sx[nb.x], tS = -B.sy[nb.y], tN = -R.sy[i], tE = -R.sx[i];
-  R.diag[i] = diag;
   R.rs[i] = (((0.0 + tW) + tS) + tN) + tE;
 }
 
@@ -167,7 +168,7 @@ __global__ void k_pcg_factor_black(PcgDev P, int* __restrict__ negpiv) {
   const PcgColor &R = P.R, &B = P.B;
   if (j >= B.n) return;
   const int4 nb = B.nbr[j];
-  double dj = 1 + B.sx[j] + R.sx[nb.x] + B.sy[j] + R.sy[nb.y];
+  double dj = B.diag[j];
   const double omega = 1.0;
   const int ks[4] = {nb.x, nb.y, nb.z, nb.w};
   const double t[4] = {-R.sx[nb.x], -R.sy[nb.y], -B.sy[j], -B.sx[j]};
@@ -190,7 +191,7 @@ __global__ void k_pcg_resid0(PcgDev P, int color) {
   const PcgColor& O = color ? P.R : P.B;
   if (i >= C.n) return;
   const int4 nb = C.nbr[i];
-  const double diag = 1 + C.sx[i] + O.sx[nb.x] + C.sy[i] + O.sy[nb.y];
+  const double diag = C.diag[i];
   double y = diag * C.u[i];
   y = y + (-O.sx[nb.x]) * O.u[nb.x];
   y = y + (-O.sy[nb.y]) * O.u[nb.y];
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(PB) k_pcg_red_solve(PcgDevT<T> P, int par, int
 // nodes, the rest black).  The other colour's new p is formed on the fly from its z and old p,
 // with the same expression, so both colours see identical values; p is double-buffered.
 // Then (p,q), alpha and the iteration count (itcg :9064-9086).
-template <typename T>
+template <typename T, bool DIAG>
 __global__ void __launch_bounds__(PB) k_pcg_apply(PcgDevT<T> P, int par, int nblk_red) {
   __shared__ double sh[32];
   if (P.sc->done) return;
@@ -385,7 +386,7 @@ __global__ void __launch_bounds__(PB) k_pcg_apply(PcgDevT<T> P, int par, int nbl
       const T pN = O.z[nb.z] + beta * Op[nb.z];
       const T pE = O.z[nb.w] + beta * Op[nb.w];
       const T sxW = O.sx[nb.x], syS = O.sy[nb.y];
-      const T diag = (T)1 + C.sx[i] + sxW + C.sy[i] + syS;
+      const T diag = DIAG ? C.diag[i] : (T)1 + C.sx[i] + sxW + C.sy[i] + syS;
       T y = diag * pi;
       y = y + (-sxW) * pW;
       y = y + (-syS) * pS;
@@ -440,7 +441,8 @@ void pcg_iteration(const PcgDev& P, int par, cudaStream_t st) {
   const int gB = std::max((nB + PB * NPT - 1) / (PB * NPT), 1), gR = std::max((nR + PB * NPT - 1) / (PB * NPT), 1);
   k_pcg_black_solve<double><<<gB, PB, 0, st>>>(P, par);
   k_pcg_red_solve<double><<<gR, PB, 0, st>>>(P, par, gB);
-  k_pcg_apply<double><<<gR + gB, PB, 0, st>>>(P, par, gR);
+  if (P.diag_stored) k_pcg_apply<double, true><<<gR + gB, PB, 0, st>>>(P, par, gR);
+  else k_pcg_apply<double, false><<<gR + gB, PB, 0, st>>>(P, par, gR);
 }
 
 void pcg_iteration_f(const PcgDevF& F, int par, cudaStream_t st) {
@@ -448,7 +450,7 @@ void pcg_iteration_f(const PcgDevF& F, int par, cudaStream_t st) {
   const int gB = std::max((nB + PB * NPT - 1) / (PB * NPT), 1), gR = std::max((nR + PB * NPT - 1) / (PB * NPT), 1);
   k_pcg_black_solve<float><<<gB, PB, 0, st>>>(F, par);
   k_pcg_red_solve<float><<<gR, PB, 0, st>>>(F, par, gB);
-  k_pcg_apply<float><<<gR + gB, PB, 0, st>>>(F, par, gR);
+  k_pcg_apply<float, false><<<gR + gB, PB, 0, st>>>(F, par, gR);
 }
 
 __global__ void k_pcg_init(PcgScal* sc, PcgScal init) { *sc = init; }

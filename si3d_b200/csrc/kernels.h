@@ -33,6 +33,9 @@ struct PcgDevT {
   int part_n;
   double *hist_alpha, *hist_beta;
   double* tri;   // Lanczos tridiagonal of chgcon, 2 x (itmax + 2), column-major (test 2)
+  // the iteration reads the gathered diagonal (matcon's rr) instead of forming it from sx and sy:
+  // set for handles with open boundaries, whose cut faces leave rr larger than that sum
+  bool diag_stored = false;
 };
 using PcgDev = PcgDevT<double>;
 using PcgDevF = PcgDevT<float>;
@@ -54,7 +57,11 @@ struct FaceMeta {
 };
 
 int momentum_init(int km1);
-void launch_momentum(const Dev& d, int ieq, const FaceMeta* meta, int ncols, const Tune& tu, cudaStream_t st);
+struct ObcDev;
+// `obc` (nobc boundaries): open boundaries whose face columns' explicit term is recomputed between
+// the cell and the column kernels
+void launch_momentum(const Dev& d, int ieq, const FaceMeta* meta, int ncols, const Tune& tu, cudaStream_t st,
+                     const ObcDev* obc = nullptr, int nobc = 0);
 void launch_matcon(const Dev& d, cudaStream_t st);
 
 void pcg_setup(const Dev& d, const PcgDev& P, int x0_mode, const double* dz, const double* hist, int* negpiv,
@@ -105,6 +112,23 @@ struct NatDev {
   PcgScal* sc = nullptr;
   double *hist_alpha = nullptr, *hist_beta = nullptr, *tri = nullptr;
 };
+// One open boundary with a specified water-surface elevation (k_openbc.cu).  side: 1 W, 2 N, 3 E,
+// 4 S.  Per boundary cell (1-based column indices): the cell, its interior neighbour, the column
+// whose sx (W, E) or sy (N, S) couples the two; per boundary row, the face column whose momentum
+// the reference recomputes (`mom`, nface entries).
+struct ObcDev {
+  int side = 0, n = 0, nface = 0;
+  const int* cells = nullptr;
+  const int* inner = nullptr;
+  const int* face = nullptr;
+  const int* mom = nullptr;
+};
+void obc_set_s(const Dev& d, const ObcDev& B, double v, cudaStream_t st);
+void obc_exmom(const Dev& d, const ObcDev& B, int ieq, cudaStream_t st);
+void obc_qq(const Dev& d, const ObcDev& B, cudaStream_t st);
+void obc_vel(const Dev& d, const ObcDev& B, cudaStream_t st);
+void obc_sca(const Dev& d, const ObcDev& B, double salbc, cudaStream_t st);
+
 // rows and x0 from matcon's sx, sy, qq (x0 modes as the red-black gather); the solve (one block);
 // zeta back to the columns
 void nat_setup(const Dev& d, const NatDev& N, int x0_mode, const double* dz, cudaStream_t st);

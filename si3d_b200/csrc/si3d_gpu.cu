@@ -86,6 +86,13 @@ struct Ctx {
   PcgDevF pcgf{};            // FP32 inner system of iterative refinement
   NatDev nat{};              // natural-order system (ordering SI3D_ORDER_NATURAL)
   bool natural = false;
+  // host copies of the grid maps (1-based, lm entries) for set-ups that need (i, j) lookups
+  std::vector<int> h_l2i, h_l2j, h_lEC, h_lWC, h_lNC, h_lSC;
+  // open boundaries (si3d_gpu_set_open_boundaries): device cell lists, the series (host), their
+  // spacing in seconds, and the time of the step in progress in hours (thrs of si3d.f90:327)
+  std::vector<ObcDev> obc;
+  std::vector<std::vector<double>> obc_wse, obc_tmp;
+  double obc_dtsec = 0, thrs = 0;
   MgDev mg{};                // aggregation hierarchy of the MG inner solves (precision SI3D_MIXED_MG)
   int mg_blocks = 0;
   PcgScal* h_scf = nullptr;  // pinned
@@ -293,16 +300,20 @@ int tracer_save(Ctx* c) {
 
 // settrap / settrap2 / save with the turbulence time levels (si3d_procedures.f90:3612, :4085,
 // :3769, :3924) and save's tracer hand-over.
+void obc_continuity(Ctx* c);
 void settrap_all(Ctx* c) {
   launch_settrap(c->d, c->st);
+  obc_continuity(c);
   if (c->prm.iturb == 1) launch_turb_half(c->d, 1, c->st);
 }
 void settrap2_all(Ctx* c) {
   launch_settrap2(c->d, c->st);
+  obc_continuity(c);
   if (c->prm.iturb == 1) launch_turb_half(c->d, 2, c->st);
 }
 int save_all(Ctx* c, int istep) {
   launch_save(c->d, istep, c->st);
+  obc_continuity(c);
   if (c->prm.iturb == 1) launch_turb_save(c->d, istep, c->st);
   return tracer_save(c);
 }
@@ -936,16 +947,70 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   return 0;
 }
 
+// Parabolic interpolation in a boundary series of spacing dx hours from time 0 (the reference's
+// parab, si3d_utils.f90:895-920); NaN past the series' end.
+double series_at(const std::vector<double>& fx, double x, double dx) {
+  int m = (int)(x / dx);
+  const double om = m;
+  double theta = (x - om * dx) / dx;
+  if (m == 0) { m = 2; theta = theta - 1.0; }
+  else m = m + 1;
+  if (m + 1 > (int)fx.size() || m < 2) return std::nan("");
+  auto f = [&](int i) { return fx[(size_t)(i - 1)]; };
+  return f(m) + 0.5 * theta * (f(m + 1) - f(m - 1) + theta * (f(m + 1) + f(m - 1) - 2.0 * f(m)));
+}
+
+// openbcUVH CASE(1): zeta of the boundary cells at the current time.
+int obc_uvh(Ctx* c) {
+  for (size_t b = 0; b < c->obc.size(); ++b) {
+    const double v = series_at(c->obc_wse[b], c->thrs, c->obc_dtsec / 3600.);
+    if (std::isnan(v)) return SI3D_EDIMS;   // the series ends before the run does
+    obc_set_s(c->d, c->obc[b], v, c->st);
+  }
+  return 0;
+}
+
+// Stages with the open-boundary adjustments that follow their kernels.
+void momentum_stage(Ctx* c, int ieq) {
+  if (ieq == 1) launch_momentum(c->d, 1, c->mce, c->nce, c->tune, c->st, c->obc.data(), (int)c->obc.size());
+  else launch_momentum(c->d, 2, c->mcn, c->ncn, c->tune, c->st, c->obc.data(), (int)c->obc.size());
+}
+void matcon_stage(Ctx* c) {
+  launch_matcon(c->d, c->st);
+  for (const ObcDev& b : c->obc) obc_qq(c->d, b, c->st);   // MODqqddrr4openBC (:1859)
+}
+void obc_continuity(Ctx* c) {
+  for (const ObcDev& b : c->obc) obc_vel(c->d, b, c->st);   // MODvel4openBC (:2821)
+}
+void vel_stage(Ctx* c) {
+  launch_vel(c->d, c->ce, c->nce, c->cn, c->ncn, c->st);
+  obc_continuity(c);
+}
+int scalar_stage(Ctx* c) {
+  launch_exsal_imsal(c->d, c->tune, c->st);
+  for (size_t b = 0; b < c->obc.size(); ++b) {   // openbcSCA (:515)
+    const double v = series_at(c->obc_tmp[b], c->thrs, c->obc_dtsec / 3600.);
+    if (std::isnan(v)) return SI3D_EDIMS;
+    obc_sca(c->d, c->obc[b], v, c->st);
+  }
+  return 0;
+}
+int obc_launches(const Ctx* c) { return (int)c->obc.size(); }
+
 int fd_impl(Ctx* c, int istep, bool lastiter, si3d_step_stats* st) {
   Dev& d = c->d;
   d.tz = 1.0 / istep;
   c->cur_istep = istep;
   if (istep == 1) c->trap_solves = 0;
   c->hist_slot = istep == 1 ? 0 : std::min(++c->trap_solves, kHistSlots - 1);
+  // openbcUVH (:423)
+  int rc = obc_uvh(c);
+  if (rc) return rc;
+  c->launches += obc_launches(c);
   // surfbc CASE(0) is a constant per-column wind set by the host (uair/vair/cdw fields)
-  int rc = stage(c, ST_MOMX, 2, [&] { launch_momentum(d, 1, c->mce, c->nce, c->tune, c->st); });
-  if (!rc) rc = stage(c, ST_MOMY, 2, [&] { launch_momentum(d, 2, c->mcn, c->ncn, c->tune, c->st); });
-  if (!rc) rc = stage(c, ST_MATCON, 1, [&] { launch_matcon(d, c->st); });
+  rc = stage(c, ST_MOMX, 2 + obc_launches(c), [&] { momentum_stage(c, 1); });
+  if (!rc) rc = stage(c, ST_MOMY, 2 + obc_launches(c), [&] { momentum_stage(c, 2); });
+  if (!rc) rc = stage(c, ST_MATCON, 1 + 2 * obc_launches(c), [&] { matcon_stage(c); });
   if (rc) return rc;
   if (st) CK(cudaEventRecord(c->evp0, c->st));
   int iters = 0, ier = 0;
@@ -962,8 +1027,14 @@ int fd_impl(Ctx* c, int istep, bool lastiter, si3d_step_stats* st) {
   }
   if (ier < 0) return ier;
   rc = stage(c, ST_SLAYER, 1, [&] { launch_slayer_h(d, c->st); });
-  if (!rc) rc = stage(c, ST_VEL, 3, [&] { launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st); });
-  if (!rc && c->prm.isal != 0) rc = stage(c, ST_SCALAR, 3, [&] { launch_exsal_imsal(d, c->tune, c->st); });
+  if (!rc) rc = obc_uvh(c);   // openbcUVH after the solve (:482)
+  if (!rc) c->launches += obc_launches(c);
+  if (!rc) rc = stage(c, ST_VEL, 3 + obc_launches(c), [&] { vel_stage(c); });
+  if (!rc && c->prm.isal != 0) {
+    int rs = 0;
+    rc = stage(c, ST_SCALAR, 3 + obc_launches(c), [&] { rs = scalar_stage(c); });
+    if (!rc) rc = rs;
+  }
   if (!rc && c->prm.ntr > 0 && c->prm.niter > 0 && lastiter)
     rc = stage(c, ST_TRACER, 2 * ((c->prm.ntr + kTracerFluxGroup - 1) / kTracerFluxGroup) + 1, [&] { tracer_stage(c); });
   if (!rc) rc = stage(c, ST_VEL2, 1, [&] { launch_vel2(d, c->st); });
@@ -1064,6 +1135,9 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
     if (!rc) cudaMemcpy(p, v.data(), P * sizeof(double), cudaMemcpyHostToDevice);
     return p;
   };
+  c->h_l2i.assign(g->l2i, g->l2i + lm); c->h_l2j.assign(g->l2j, g->l2j + lm);
+  c->h_lEC.assign(g->lEC, g->lEC + lm); c->h_lWC.assign(g->lWC, g->lWC + lm);
+  c->h_lNC.assign(g->lNC, g->lNC + lm); c->h_lSC.assign(g->lSC, g->lSC + lm);
   d.g.lEC = up_int(g->lEC, lm, lm1);
   d.g.lWC = up_int(g->lWC, lm, lm1);
   d.g.lNC = up_int(g->lNC, lm, lm1);
@@ -1368,9 +1442,9 @@ int si3d_learn_recorded(int h) {
 }
 
 int si3d_gpu_fd(int h, int n, int istep, int lastiter, si3d_step_stats* st) {
-  (void)n;
   Ctx* c = get(h);
   if (!c) return SI3D_EHANDLE;
+  c->thrs = (double)n * c->prm.dt / 3600.;   // its = n idt, thrs = its / 3600. (si3d.f90:326-327)
   if (istep != 1 && istep != 2) return SI3D_EDIMS;
   CK(cudaSetDevice(c->device));
   if (st) { std::memset(st, 0, sizeof(*st)); CK(cudaEventRecord(c->ev0, c->st)); }
@@ -1406,8 +1480,8 @@ int si3d_gpu_stage(int h, const char* stage, int istep, si3d_step_stats* st) {
   const std::string s = stage;
   Dev& d = c->d;
   d.tz = 1.0 / istep;
-  if (s == "momentum") { launch_momentum(d, 1, c->mce, c->nce, c->tune, c->st); launch_momentum(d, 2, c->mcn, c->ncn, c->tune, c->st); }
-  else if (s == "matcon") launch_matcon(d, c->st);
+  if (s == "momentum") { momentum_stage(c, 1); momentum_stage(c, 2); }
+  else if (s == "matcon") matcon_stage(c);
   else if (s == "solve") {
     int it = 0, ier = 0;
     double rr = 0;
@@ -1416,8 +1490,8 @@ int si3d_gpu_stage(int h, const char* stage, int istep, si3d_step_stats* st) {
     if (st) { st->nsolves = 1; st->iters[0] = it; st->relres[0] = rr; st->ier[0] = ier; st->total_iters = it; }
     if (ier < 0) return ier;
     launch_slayer_h(d, c->st);
-  } else if (s == "vel") launch_vel(d, c->ce, c->nce, c->cn, c->ncn, c->st);
-  else if (s == "scalar") launch_exsal_imsal(d, c->tune, c->st);
+  } else if (s == "vel") vel_stage(c);
+  else if (s == "scalar") { if (int rc = scalar_stage(c)) return rc; }
   else if (s == "tracer") { if (c->prm.ntr > 0) tracer_stage(c); }
   else if (s == "turbulence") { if (c->prm.iturb == 1) launch_turbulence(d, c->turb_scr, c->st); }
   else if (s == "vel2") launch_vel2(d, c->st);
@@ -1467,6 +1541,7 @@ int si3d_gpu_save(int h, int istep) {
 // trapezoidal fd/settrap2 iterations, save.  Enqueues only; the caller synchronises.
 static int step_impl(Ctx* c, int n, si3d_step_stats* st) {
   c->trap_solves = 0;
+  c->thrs = (double)n * c->prm.dt / 3600.;   // its = n idt, thrs = its / 3600. (si3d.f90:326-327)
   if (st) { std::memset(st, 0, sizeof(*st)); CK(cudaEventRecord(c->ev0, c->st)); }
   const si3d_params& p = c->prm;
   int niter1 = p.niter;
@@ -1533,8 +1608,8 @@ static int time_stage(Ctx* c, int which, int reps, float* best) {
   Dev& d = c->d;
   auto run = [&] {
     if (which == 0) {
-      launch_momentum(d, 1, c->mce, c->nce, c->tune, c->st);
-      launch_momentum(d, 2, c->mcn, c->ncn, c->tune, c->st);
+      momentum_stage(c, 1);
+      momentum_stage(c, 2);
     } else {
       launch_exsal_imsal(d, c->tune, c->st);
     }
@@ -1659,7 +1734,8 @@ int si3d_ens_create(const int* handles, int n, int* ens) {
     Ctx* c = get(handles[i]);
     if (!c) return SI3D_EHANDLE;
     if (i == 0) E->device = c->device;
-    if (c->device != E->device || c->prm.precision != SI3D_FP64 || !c->persistent || c->natural) return SI3D_EDIMS;
+    if (c->device != E->device || c->prm.precision != SI3D_FP64 || !c->persistent || c->natural || !c->obc.empty())
+      return SI3D_EDIMS;
     for (int j = 0; j < i; ++j)
       if (handles[j] == handles[i]) return SI3D_EDIMS;
     E->hs.push_back(handles[i]);
@@ -1924,6 +2000,71 @@ int si3d_gpu_counters(int h, long long* launches, double* stage_ms, long long* s
   return ST_COUNT;
 }
 
+int si3d_gpu_set_open_boundaries(int h, int nopen, const int* iside, const int* itype, const int* isbc,
+                                 const int* jsbc, const int* iebc, const int* jebc, double dtsec, int npts,
+                                 const double* wse, const double* temp) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (nopen < 0) return SI3D_EDIMS;
+  if (nopen > 0 && (!iside || !itype || !isbc || !jsbc || !iebc || !jebc || !wse || !temp || npts < 3 || !(dtsec > 0)))
+    return SI3D_EDIMS;
+  // tracers at open boundaries (openbcTracer) and the FP32 MIC inner solves are not built for them
+  if (nopen > 0 && (c->prm.precision == SI3D_MIXED_IR || c->prm.ntr > 0 || c->graph_mode)) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  const int im1 = c->im1, jm1 = c->jm1, lm1 = c->lm1;
+  std::vector<int> ij((size_t)im1 * jm1, 0);
+  for (int l = 1; l <= c->lm; ++l) ij[(size_t)(c->h_l2i[l - 1] - 1) * jm1 + (c->h_l2j[l - 1] - 1)] = l;
+  auto cell = [&](int i, int j) { return (i < 1 || j < 1 || i > im1 || j > jm1) ? 0 : ij[(size_t)(i - 1) * jm1 + (j - 1)]; };
+  std::vector<ObcDev> obc;
+  std::vector<std::vector<int>> keep;
+  for (int nn = 0; nn < nopen; ++nn) {
+    const int side = iside[nn];
+    if (itype[nn] != 1 || side < 1 || side > 4) return SI3D_EDIMS;   // water-surface elevation only
+    std::vector<int> cells, inner, face, mom;
+    const bool x = side == 1 || side == 3;
+    const int a = x ? jsbc[nn] : isbc[nn], e = x ? jebc[nn] : iebc[nn];
+    if (e < a) return SI3D_EDIMS;
+    for (int q = a; q <= e; ++q) {
+      const int i = x ? isbc[nn] : q, j = x ? q : jsbc[nn];
+      const int lb = cell(i, j);
+      const int outer = side == 1 ? cell(i - 1, j) : side == 2 ? cell(i, j + 1) : side == 3 ? cell(i + 1, j) : cell(i, j - 1);
+      if (!lb || outer) return SI3D_EDIMS;   // a wet cell with a dry cell outside it (openbc0's checks)
+      const int li = side == 1 ? c->h_lEC[lb - 1] : side == 2 ? c->h_lSC[lb - 1] : side == 3 ? c->h_lWC[lb - 1] : c->h_lNC[lb - 1];
+      if (li == lm1) return SI3D_EDIMS;     // the interior neighbour must be wet
+      cells.push_back(lb);
+      inner.push_back(li);
+      face.push_back((side == 1 || side == 4) ? lb : li);
+      mom.push_back((side == 1 || side == 4) ? lb : li);
+    }
+    ObcDev B;
+    B.side = side;
+    B.n = B.nface = (int)cells.size();
+    int *dc = nullptr, *di = nullptr, *df = nullptr, *dm = nullptr;
+    int rc = c->alloc(&dc, cells.size());
+    rc |= c->alloc(&di, cells.size());
+    rc |= c->alloc(&df, cells.size());
+    rc |= c->alloc(&dm, cells.size());
+    if (rc) return rc;
+    CK(cudaMemcpy(dc, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(di, inner.data(), inner.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(df, face.data(), face.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(dm, mom.data(), mom.size() * sizeof(int), cudaMemcpyHostToDevice));
+    B.cells = dc; B.inner = di; B.face = df; B.mom = dm;
+    obc.push_back(B);
+  }
+  c->obc = obc;
+  c->obc_wse.assign(nopen, {});
+  c->obc_tmp.assign(nopen, {});
+  for (int nn = 0; nn < nopen; ++nn) {
+    c->obc_wse[nn].assign(wse + (size_t)nn * npts, wse + (size_t)(nn + 1) * npts);
+    c->obc_tmp[nn].assign(temp + (size_t)nn * npts, temp + (size_t)(nn + 1) * npts);
+  }
+  c->obc_dtsec = dtsec;
+  // the cut faces leave matcon's rr above 1 + sx + sx(W) + sy + sy(S): the iteration reads rr
+  c->pcg.diag_stored = nopen > 0;
+  return 0;
+}
+
 int si3d_gpu_test_wait_limit(int h, long long polls, int absent_blocks) {
   Ctx* c = get(h);
   if (!c) return SI3D_EHANDLE;
@@ -1965,13 +2106,19 @@ int si3d_gpu_solve_zeta(int lm, const double* coef, const int* jcoef, const doub
     qq[m] = rhs[m];
     sp[m] = zeta[m];
   }
+  // the diagonal is the caller's (SolverSparse's rr); when it differs from 1 + the face sum (open
+  // boundaries cut faces after rr is formed) the iteration reads it instead of forming it
+  std::vector<double> rrv(lm1, 1.0);
+  bool diag_is_sum = true;
   for (int m = 0; m < lm; ++m) {
     const double sxw = W[m] == lm1 ? 0.0 : sx[W[m] - 1], sys = S[m] == lm1 ? 0.0 : sy[S[m] - 1];
     if (-coef[(size_t)1 * lm + m] != sxw || -coef[(size_t)2 * lm + m] != sys) return SI3D_EDIMS;
-    if (coef[m] != 1 + sx[m] + sxw + sy[m] + sys) return SI3D_EDIMS;
+    rrv[m] = coef[m];
+    if (coef[m] != 1 + sx[m] + sxw + sy[m] + sys) diag_is_sum = false;
     if (E[m] != lm1 && W[E[m] - 1] != m + 1) return SI3D_EDIMS;
     if (N[m] != lm1 && S[N[m] - 1] != m + 1) return SI3D_EDIMS;
   }
+  if (!diag_is_sum && precision == SI3D_MIXED_IR) return SI3D_EDIMS;   // the FP32 inner rows form it
   si3d_grid g{};
   std::vector<int> kmz(lm1, 2), l2(lm, 1);   // one layer (k1 = 2) per column; the sentinel at km1
   kmz[lm] = 3;
@@ -1992,6 +2139,8 @@ int si3d_gpu_solve_zeta(int lm, const double* coef, const int* jcoef, const doub
   double rr = 0;
   rc = si3d_gpu_set_field(hdl, "sx", sx.data());
   if (!rc) rc = si3d_gpu_set_field(hdl, "sy", sy.data());
+  if (!rc) rc = si3d_gpu_set_field(hdl, "rr", rrv.data());
+  c->pcg.diag_stored = !diag_is_sum;
   if (!rc) rc = si3d_gpu_set_field(hdl, "qq", qq.data());
   if (!rc) rc = si3d_gpu_set_field(hdl, "sp", sp.data());
   if (!rc) rc = solve(c, &it, &rr, &ier);

@@ -121,6 +121,18 @@
          REAL(C_DOUBLE), INTENT(OUT)   :: stptst, emin, emax
       END FUNCTION
 
+      ! open boundaries with a specified water-surface elevation (openbc0 and the stage adjustments
+      ! of si3d_boundaryconditions.f90), the series varsOpenBC(nn,1,:) and (nn,2,:) as wse, temp
+      INTEGER(C_INT) FUNCTION si3d_gpu_set_open_boundaries(handle, nopen, iside, itype, isbc, jsbc, iebc,  &
+                                                           jebc, dtsec, npts, wse, temp)                 &
+                                                           BIND(C, NAME="si3d_gpu_set_open_boundaries")
+         IMPORT :: C_INT, C_DOUBLE
+         INTEGER(C_INT), VALUE      :: handle, nopen, npts
+         INTEGER(C_INT), INTENT(IN) :: iside(*), itype(*), isbc(*), jsbc(*), iebc(*), jebc(*)
+         REAL(C_DOUBLE), VALUE      :: dtsec
+         REAL(C_DOUBLE), INTENT(IN) :: wse(*), temp(*)
+      END FUNCTION
+
       SUBROUTINE si3d_gpu_finalize(handle) BIND(C, NAME="si3d_gpu_finalize")
          IMPORT :: C_INT
          INTEGER(C_INT), VALUE :: handle

@@ -87,6 +87,8 @@ GPU_SYMBOLS = {
     "si3d_gpu_host_free": (C.c_int, [C.c_void_p]),
     "si3d_gpu_sync": (C.c_int, [C.c_int]),
     "si3d_gpu_test_wait_limit": (C.c_int, [C.c_int, C.c_longlong, C.c_int]),
+    "si3d_gpu_set_open_boundaries": (C.c_int, [C.c_int, C.c_int] + [C.c_void_p] * 6 + [C.c_double, C.c_int,
+                                                                                       C.c_void_p, C.c_void_p]),
     "si3d_gpu_strerror": (C.c_char_p, [C.c_int]),
     "si3d_gpu_finalize": (None, [C.c_int]),
     "si3d_gpu_autotune": (C.c_int, [C.c_int, C.c_int, C.c_void_p]),

@@ -69,6 +69,13 @@ class Basin:
     iotr: int = 0
     itspftr: int = 0
     seeds: dict = dataclasses.field(default_factory=dict)
+    # open boundaries with a specified water-surface elevation (itype 1): (iside, isbc, jsbc, iebc,
+    # jebc) each, 1-based grid indices (the real cells are 2 .. nx + 1, 2 .. ny + 1), and the series
+    # written to openbcNN.txt every obc_dtsec seconds: elevation (m) and temperature (deg C)
+    obc: tuple = ()
+    obc_dtsec: float = 600.0
+    obc_wse: tuple = ()
+    obc_temp: tuple = ()
 
     @property
     def zl(self) -> float:
@@ -144,6 +151,29 @@ def config(name: str, nsteps: Optional[int] = None, seed_offset: int = 0) -> Bas
         u = wind_speed_for_stress(tau)
         return Basin(name, nx, ny, dx, dx, depth, nl, ddz, 30.0, nsteps or steps, dzmin=0.1,
                      uair=u, vair=np.zeros_like(u), seeds={"bathymetry": sb, "wind": sw})
+    if name in ("t2", "t3"):
+        # open-boundary basins: a channel forced by a tide through its west end (t2), and a basin
+        # with open east, north and south sides (t3); smooth bottom 3-9 m, 10 layers of 1 m
+        nx, ny = (40, 16) if name == "t2" else (32, 24)
+        x = (np.arange(nx) + 0.5) / nx
+        y = (np.arange(ny) + 0.5) / ny
+        depth = 6.0 + 2.5 * np.cos(2.0 * math.pi * x)[:, None] * np.sin(math.pi * y)[None, :] - 0.5 * x[:, None]
+        depth = np.round(depth * 10.0) / 10.0
+        if name == "t2":
+            obc = ((1, 2, 2, 2, ny + 1),)
+        else:
+            obc = ((3, nx + 1, 4, nx + 1, ny - 3), (2, 6, ny + 1, nx - 5, ny + 1), (4, 6, 2, nx - 5, 2))
+        dts = 600.0
+        npts = 40
+        t = np.arange(npts) * dts
+        wse, temp = [], []
+        for q in range(len(obc)):
+            amp, period = 0.05 + 0.02 * q, 7200.0 + 1800.0 * q
+            wse.append(tuple(np.round(amp * np.sin(2.0 * math.pi * t / period), 6)))
+            temp.append(tuple(np.round(15.0 + 1.0 * np.cos(2.0 * math.pi * t / 5400.0) + q, 5)))
+        return Basin(name, nx, ny, 100.0, 100.0, depth, 10, 1.0, 60.0, nsteps or 30, dzmin=0.05,
+                     wa=float(wind_speed_for_stress(0.05)), phi=270.0, obc=obc, obc_dtsec=dts,
+                     obc_wse=tuple(wse), obc_temp=tuple(temp))
     if name == "t0":  # tiny bowl
         nx, ny, dx = 24, 16, 100.0
         return Basin("t0", nx, ny, dx, dx, bowl_bathymetry(nx, ny, dx, dx, hmax=8.0), 8, 1.0, 60.0,
@@ -183,8 +213,14 @@ def write_inp(b: Basin, path: str) -> None:
     L += [sep, "Output specifications for X-section files", sep, _rec("ixt", 0)]
     L += [sep, "Output specifications for 3D space files", sep, _rec("ipxml", b.ipxml), _rec("itspf", b.itspf),
           _rec("iTurbVars", 0)]
-    L += [sep, "Open boundary conditions specifications", sep, _rec("nopen", 0), _rec("dtopenbc", 360.0)]
-    L += [_rec(x, 0) for x in ("iside", "itype", "isbc", "jsbc", "iebc", "jebc")]
+    L += [sep, "Open boundary conditions specifications", sep, _rec("nopen", len(b.obc))]
+    if b.obc:
+        L += [_rec("dtopenbc", float(b.obc_dtsec))]
+        cols = list(zip(*[(ob[0], 1, ob[1], ob[2], ob[3], ob[4]) for ob in b.obc]))
+        L += [_rec(x, " ".join(str(v) for v in c)) for x, c in zip(("iside", "itype", "isbc", "jsbc", "iebc", "jebc"), cols)]
+    else:
+        L += [_rec("dtopenbc", 360.0)]
+        L += [_rec(x, 0) for x in ("iside", "itype", "isbc", "jsbc", "iebc", "jebc")]
     L += [sep, "Open boundary conditions for nesting procedures", sep, _rec("nxBDO", 0)]
     L += [_rec(x, 0) for x in ("iob", "xxb", "iside", "isbc", "jsbc", "iebc", "jebc")]
     L += [sep, "Specification for tracer simulation", sep, _rec("ntr", b.ntr)]
@@ -265,8 +301,21 @@ def write_wind(b: Basin, path: str) -> None:
         fh.write(np.ascontiguousarray(v, dtype="<f8").tobytes())
 
 
+def write_openbc(b: Basin, run_dir: str) -> None:
+    """openbcNN.txt per open boundary (openbc0, si3d_boundaryconditions.f90:55-91): five header
+    records, the record count in '(10X,I7)', then one record '(10X,(ntr+2)G11.2)' per time."""
+    for nn, (wse, temp) in enumerate(zip(b.obc_wse, b.obc_temp), start=1):
+        lines = [f"Open boundary {nn} of {b.name}", "water-surface elevation (m), temperature (deg C)",
+                 f"every {b.obc_dtsec:g} s from t = 0", "synthetic", "-" * 40, f"{'npts':<10}{len(wse):7d}"]
+        for w, t in zip(wse, temp):
+            lines.append(f"{'':10}{w:11.6f}{t:11.5f}")
+        with open(os.path.join(run_dir, f"openbc{nn:02d}.txt"), "w") as fh:
+            fh.write("\n".join(lines) + "\n")
+
+
 def write_run(b: Basin, run_dir: str) -> str:
     os.makedirs(run_dir, exist_ok=True)
+    write_openbc(b, run_dir)
     write_inp(b, os.path.join(run_dir, "si3d_inp.txt"))
     write_bathy(b, os.path.join(run_dir, "si3d_bathy"))
     write_init(b, os.path.join(run_dir, "si3d_init.txt"))

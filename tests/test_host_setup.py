@@ -71,10 +71,11 @@ def test_truncated_profile(native_libs, run_dirs, tmp_path):
     assert rc == -101 and "si3d_init.txt" in err
 
 
-@pytest.mark.parametrize("label,value", [("nopen", 1), ("iturb", 2), ("iturb", -1)])
+@pytest.mark.parametrize("label,value", [("iturb", 2), ("iturb", -1)])
 def test_options_outside_the_core_are_refused(native_libs, run_dirs, tmp_path, label, value):
-    """Open boundaries, the k-kl closure (iturb >= 2) and GOTM (iturb = -1) are not built; a run
-    that selects them is refused rather than silently run without them."""
+    """The k-kl closure (iturb >= 2) and GOTM (iturb = -1) are not built; a run that selects them is
+    refused rather than silently run without them (open boundaries other than itype 1: see
+    test_openbc_oracle.py)."""
     d = _copy(run_dirs["t0"], str(tmp_path / f"opt_{label}_{value}"))
     p = os.path.join(d, "si3d_inp.txt")
     lines = open(p).read().splitlines()
