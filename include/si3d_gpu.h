@@ -133,6 +133,11 @@ int si3d_gpu_init(const si3d_grid* grid, const si3d_params* params, int device, 
  * Fortran module arrays of si3d_types.f90:117-164. */
 int si3d_gpu_set_field(int handle, const char* name, const double* host);
 int si3d_gpu_get_field(int handle, const char* name, double* host);
+/* The same copies for a host whose arrays are default REAL (4 bytes), as the reference is built
+ * (si3d_types.f90:26-27, no -r8 in its makefile): values are widened to FP64 on the device, and
+ * rounded to the nearest float on the way back.  Same names, layout and errors as above. */
+int si3d_gpu_set_field_f32(int handle, const char* name, const float* host);
+int si3d_gpu_get_field_f32(int handle, const char* name, float* host);
 /* Integer column arrays k1z k1u k1v (lm1 entries). */
 int si3d_gpu_set_ifield(int handle, const char* name, const int* host);
 int si3d_gpu_get_ifield(int handle, const char* name, int* host);

@@ -142,6 +142,7 @@ struct Ctx {
   int* d_stats_ii = nullptr;     // [24][2]
   double* d_stats_rr = nullptr;  // [24]
   double* staging = nullptr;  // device staging for transposes (km1 * lm1)
+  float* staging_f = nullptr; // FP32 staging of the single-precision field copies (allocated on first use)
   // non-active tracers: two pools of ntr layer-major fields; tr_buf[tr_cur] holds tracer, the other
   // tracerpp.  save makes tracerpp = tracer by swapping the pools; after it the tracer pool is not
   // read (tr_alias: "tracer" reads resolve to tracerpp) until the next ImTracer rewrites every
@@ -1345,6 +1346,83 @@ int si3d_gpu_get_field(int h, const char* name, double* host) {
     return 0;
   }
   return SI3D_ENAME;
+}
+
+// Single-precision copies: the reference as shipped keeps its module arrays in default REAL (4 bytes,
+// si3d_types.f90:26).  The values cross the bus as floats and are widened (or rounded to nearest)
+// on the device.
+namespace {
+__global__ void k_f32_to_f64(const float* __restrict__ s, double* __restrict__ d, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) d[i] = (double)s[i];
+}
+__global__ void k_f64_to_f32(const double* __restrict__ s, float* __restrict__ d, long long n) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) d[i] = (float)s[i];
+}
+int staging_f(Ctx* c) {
+  if (!c->staging_f) return c->alloc(&c->staging_f, (size_t)c->km1 * c->lm1);
+  return 0;
+}
+}  // namespace
+
+int si3d_gpu_set_field_f32(int h, const char* name, const float* host) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (!name || !host) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  bool pp = false;
+  const int nt = tracer_name(c, name, &pp);
+  if (nt < 0) return SI3D_ENAME;
+  const bool is3 = nt > 0 || f3ptr(c, name);
+  if (!is3 && !f2ptr(c, name)) return SI3D_ENAME;
+  if (int rc = staging_f(c)) return rc;
+  const long long n = is3 ? (long long)c->km1 * c->lm1 : c->lm1;
+  CK(cudaMemcpyAsync(c->staging_f, host, sizeof(float) * n, cudaMemcpyHostToDevice, c->st));
+  if (is3) {
+    double* dst = nullptr;
+    if (nt > 0) {
+      if (int rc = tracer_materialise(c)) return rc;
+      c->tr_synced = false;
+      dst = tracer_pool(c, pp) + (nt - 1) * c->tr_stride;
+    } else {
+      dst = f3ptr(c, name);
+    }
+    k_f32_to_f64<<<(unsigned)((n + 255) / 256), 256, 0, c->st>>>(c->staging_f, c->staging, n);
+    dim3 b(32, 8), gr((c->lm1 + 31) / 32, (c->km1 + 31) / 32);
+    k_colmajor_to_layer<<<gr, b, 0, c->st>>>(c->staging, dst, c->km1, c->lm1, c->P);
+  } else {
+    k_f32_to_f64<<<(unsigned)((n + 255) / 256), 256, 0, c->st>>>(c->staging_f, f2ptr(c, name), n);
+  }
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int si3d_gpu_get_field_f32(int h, const char* name, float* host) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (!name || !host) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  bool pp = false;
+  const int nt = tracer_name(c, name, &pp);
+  if (nt < 0) return SI3D_ENAME;
+  const double* src3 = nt > 0 ? tracer_pool(c, pp || c->tr_alias) + (nt - 1) * c->tr_stride : f3ptr(c, name);
+  const double* src2 = src3 ? nullptr : f2ptr(c, name);
+  if (!src3 && !src2) return SI3D_ENAME;
+  if (int rc = staging_f(c)) return rc;
+  const long long n = src3 ? (long long)c->km1 * c->lm1 : c->lm1;
+  if (src3) {
+    dim3 b(32, 8), gr((c->lm1 + 31) / 32, (c->km1 + 31) / 32);
+    k_layer_to_colmajor<<<gr, b, 0, c->st>>>(src3, c->staging, c->km1, c->lm1, c->P);
+    k_f64_to_f32<<<(unsigned)((n + 255) / 256), 256, 0, c->st>>>(c->staging, c->staging_f, n);
+  } else {
+    k_f64_to_f32<<<(unsigned)((n + 255) / 256), 256, 0, c->st>>>(src2, c->staging_f, n);
+  }
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, c->staging_f, sizeof(float) * n, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
 }
 
 int si3d_gpu_set_ifield(int h, const char* name, const int* host) {

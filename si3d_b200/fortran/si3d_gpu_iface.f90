@@ -62,6 +62,21 @@
          REAL(C_DOUBLE), INTENT(OUT)        :: host(*)
       END FUNCTION
 
+      ! the same for the reference's default-REAL (4-byte) module arrays, without -r8
+      INTEGER(C_INT) FUNCTION si3d_gpu_set_field_f32(handle, name, host) BIND(C, NAME="si3d_gpu_set_field_f32")
+         IMPORT :: C_INT, C_CHAR, C_FLOAT
+         INTEGER(C_INT), VALUE              :: handle
+         CHARACTER(KIND=C_CHAR), INTENT(IN) :: name(*)
+         REAL(C_FLOAT), INTENT(IN)          :: host(*)
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_get_field_f32(handle, name, host) BIND(C, NAME="si3d_gpu_get_field_f32")
+         IMPORT :: C_INT, C_CHAR, C_FLOAT
+         INTEGER(C_INT), VALUE              :: handle
+         CHARACTER(KIND=C_CHAR), INTENT(IN) :: name(*)
+         REAL(C_FLOAT), INTENT(OUT)         :: host(*)
+      END FUNCTION
+
       INTEGER(C_INT) FUNCTION si3d_gpu_set_ifield(handle, name, host) BIND(C, NAME="si3d_gpu_set_ifield")
          IMPORT :: C_INT, C_CHAR
          INTEGER(C_INT), VALUE              :: handle

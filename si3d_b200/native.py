@@ -61,6 +61,8 @@ GPU_SYMBOLS = {
     "si3d_gpu_init": (C.c_int, [C.POINTER(Grid), C.POINTER(Params), C.c_int, C.POINTER(C.c_int)]),
     "si3d_gpu_set_field": (C.c_int, [C.c_int, C.c_char_p, C.c_void_p]),
     "si3d_gpu_get_field": (C.c_int, [C.c_int, C.c_char_p, C.c_void_p]),
+    "si3d_gpu_set_field_f32": (C.c_int, [C.c_int, C.c_char_p, C.c_void_p]),
+    "si3d_gpu_get_field_f32": (C.c_int, [C.c_int, C.c_char_p, C.c_void_p]),
     "si3d_gpu_set_ifield": (C.c_int, [C.c_int, C.c_char_p, C.c_void_p]),
     "si3d_gpu_get_ifield": (C.c_int, [C.c_int, C.c_char_p, C.c_void_p]),
     "si3d_gpu_density": (C.c_int, [C.c_int]),

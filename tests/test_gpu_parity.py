@@ -226,3 +226,28 @@ def test_column_tridiag_matches_oracle_trid(native_libs, oracle_lib):
         ag_o, ar_o = oracle_lib.trid(a[:, s], b[:, s], c[:, s], g[:, s], r[:, s])
         np.testing.assert_allclose(ag[:, s], ag_o, rtol=1e-13, atol=1e-15)
         np.testing.assert_allclose(ar[:, s], ar_o, rtol=1e-13, atol=1e-15)
+
+
+def test_single_precision_field_copies(native_libs, run_dirs):
+    """si3d_gpu_set_field_f32 / get_field_f32, the boundary for the reference as shipped (default
+    REAL of 4 bytes): floats widen exactly on the way in and round to nearest on the way out, for
+    3-D and 2-D fields alike."""
+    import ctypes as C
+
+    from si3d_b200 import native
+    from si3d_b200.model import GpuRun
+    g = native.gpu()
+    run = GpuRun(run_dirs["t1"], pcg_itmax=2000)
+    try:
+        run.run(2)
+        for name, shape in (("uh", (run.km1, run.lm1)), ("s", (run.lm1,))):
+            ref = run.get(name)
+            out = np.empty(shape, dtype=np.float32, order="F")
+            assert g.si3d_gpu_get_field_f32(run.gh, name.encode(), C.c_void_p(out.ctypes.data)) == 0
+            np.testing.assert_array_equal(out, ref.astype(np.float32))
+            vals = np.asfortranarray((np.random.default_rng(7).standard_normal(shape)).astype(np.float32))
+            assert g.si3d_gpu_set_field_f32(run.gh, name.encode(), C.c_void_p(vals.ctypes.data)) == 0
+            np.testing.assert_array_equal(run.get(name), vals.astype(np.float64))
+        assert g.si3d_gpu_set_field_f32(run.gh, b"nosuch", C.c_void_p(out.ctypes.data)) == -103
+    finally:
+        run.close()
