@@ -137,6 +137,7 @@ struct Model {
   // binary output files (outp, outz, outh) written into the run directory, and the date stamp
   std::string dir;
   Date date;
+  bool space_written = false;   // outs' first_entry
   std::shared_ptr<FILE> f_ptrack;
   std::vector<std::shared_ptr<FILE>> f_tracer, f_plane;
   // open boundaries (nopen > 0): records, series spacing dtsecOpenBC (s), hours of the current step

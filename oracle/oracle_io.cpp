@@ -130,7 +130,7 @@ static bool read_inp(Model& m, const std::string& dir) {
   if (p.iox != 0) { m.err = "si3d_inp.txt: cross-section output (iox/=0) is not supported"; return false; }
   L.skip(3); ok &= rec_i(L, p.ipxml); ok &= rec_i(L, p.itspf); ok &= rec_i(L, p.iTurbVars);
   if (p.ipxml > 0 && p.iTurbVars != 0) { m.err = "turbulence variables in the 3-D output need iturb > 0"; return false; }
-  if (p.nnodes > 0 || p.ipxml < 0) { m.err = "the time-series (outt) and XML (outs) writers are not restated"; return false; }
+  if (p.nnodes > 0) { m.err = "the time-series writer (outt) is not restated"; return false; }
   L.skip(3); ok &= rec_i(L, p.nopen);                                 // :124-145
   if (p.nopen > 0) {
     // dtsecopenbc, then iside, itype, isbc, jsbc, iebc, jebc, nopen values each

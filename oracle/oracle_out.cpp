@@ -199,9 +199,86 @@ bool outh(Model& m, int n) {
 }  // namespace
 
 // The output calls of the time loop (si3d.f90:430-438; the initial ones :89-100 with n = 0).
+// outs (si3d_utils.f90:2605-2760), ipxml < 0: the Gr viewer's XML header on the first call, the two
+// binary space files opened (and left empty: outs_bin, :2763, has no caller).  runNumber, the
+// wall-clock date_and_time, is written as 12 zeros here; a comparison skips that line.
+static bool outs(Model& m) {
+  if (m.space_written) return true;
+  const Inp& p = m.in;
+  FILE* f = std::fopen((m.dir + "/spacefile.xml").c_str(), "w");
+  if (!f) { m.err = "Error opening spacefile.xml"; return false; }
+  for (const char* b : {"/spacefile2d.bin", "/spacefile3d.bin"}) {
+    FILE* g = std::fopen((m.dir + b).c_str(), "wb");
+    if (!g) { std::fclose(f); m.err = "Error opening space file"; return false; }
+    std::fclose(g);
+  }
+  auto ch = [](long v) { return std::string("\"") + std::to_string(v) + "\""; };   // int_to_char(v, 0)
+  const int im = m.im, jm = m.jm;
+  std::fprintf(f, "<?xml version=\"1.0\"?>\n");
+  std::fprintf(f, " \n");
+  std::fprintf(f, "<!-- Si3D Output for Gr -->\n");
+  std::fprintf(f, "<!-- xml header file for binary spacefiles -->\n");
+  // FORMAT 1 (:2651-2655)
+  std::fprintf(f, "<!-- Run Parameters:  dt =%5.2f s  dz =%5.2f m  im =%5d  jm =%5d\n", p.idt, m.ddz, im, jm);
+  std::fprintf(f, "     itrsca =%2d  itrap =%2d  cd = %7.4f  ismooth =%2d  beta =%6.3f  niter =%2d\n", p.itrsca,
+               p.itrap, p.cd, p.ismooth, p.beta, p.niter);
+  std::fprintf(f, "     itrmom =%2d  f =%7.4f  wa =%8.1f -->\n", p.itrmom, p.f, p.wa);
+  std::fprintf(f, " \n");
+  std::fprintf(f, "<gov.usgs.gr>\n");
+  std::fprintf(f, "   <obj class=\"gov.usgs.sfhydro.si3d.Si3dOutput\"\n");
+  std::string title = p.title;
+  while (!title.empty() && title.back() == ' ') title.pop_back();
+  std::fprintf(f, "        runTitle=\"%s\"\n", title.c_str());
+  std::fprintf(f, "        runNumber=\"000000000000\"\n");
+  const long idt2 = (long)p.ipxml * (long)p.idt;
+  const Date keep = m.date;
+  if (p.itspf == 0) {
+    compute_date(m, 0.0);
+  } else {
+    long itspf1 = (p.itspf / idt2) * idt2;
+    if (p.itspf % idt2 != 0) itspf1 = itspf1 + idt2;
+    compute_date(m, (double)itspf1);
+  }
+  const int ihr2 = (int)(m.date.isec / 3600);
+  int isec2 = (int)(m.date.isec - ihr2 * 3600);
+  const int imin2 = isec2 / 60;
+  isec2 = isec2 - imin2 * 60;
+  std::fprintf(f, "        startTime=\"%4d/%02d/%02d %02d:%02d:%02d\" timeStepInSeconds=%s>\n", m.date.iyr, m.date.imon,
+               m.date.iday, ihr2, imin2, isec2, ch(idt2).c_str());
+  m.date = keep;   // compute_date(0.0) returns the calendar to the start of the run
+  std::fprintf(f, " \n");
+  const char* blocks[2][3] = {{"2-D x-y Variables", "spacefile2d.bin", "2-D Variables"},
+                              {"3-D Variables", "spacefile3d.bin", "3-D Variables"}};
+  for (int b = 0; b < 2; ++b) {
+    std::fprintf(f, "      <obj class=\"gov.usgs.gr.GrObjectContainer\" title=\"%s\">\n", blocks[b][0]);
+    std::fprintf(f, "         <dataseries class=\"gov.usgs.gr.data.RafDataSeries\"\n");
+    std::fprintf(f, "            file=\"%s\"\n", blocks[b][1]);
+    std::fprintf(f, "            title=\"%s\" numDimensions=%s>\n", blocks[b][2], ch(b == 0 ? 1 : 4).c_str());
+    if (b == 0) {
+      std::fprintf(f, "            <dim num=\"0\" title=\"Zeta\" units=\"meters\" unitScale=\"0.0001\"/>\n");
+    } else {
+      std::fprintf(f, "            <dim num=\"0\" title=\"u\" units=\"m/s\" unitScale=\"0.0001\"/>\n");
+      std::fprintf(f, "            <dim num=\"1\" title=\"v\" units=\"m/s\" unitScale=\"0.0001\"/>\n");
+      std::fprintf(f, "            <dim num=\"2\" title=\"w\" units=\"m/s\" unitScale=\"0.00001\"/>\n");
+      std::fprintf(f, "            <dim num=\"3\" title=\"dz\" units=\"m**2/s\" unitScale=\"0.0001\"/>\n");
+    }
+    std::fprintf(f, " \n");
+    std::fprintf(f, "         </dataseries>\n");
+    std::fprintf(f, "      </obj>\n");
+    if (b == 0) std::fprintf(f, " \n");
+  }
+  std::fprintf(f, "   </obj>\n");
+  std::fprintf(f, "</gov.usgs.gr>\n");
+  std::fprintf(f, " \n");
+  std::fclose(f);
+  m.space_written = true;
+  return true;
+}
+
 bool write_outputs(Model& m, int n) {
   const Inp& p = m.in;
   const int apxml = std::abs(p.ipxml);
+  if (p.ipxml < 0 && !outs(m)) return false;   // called at n = 0 and every step; writes once
   if (p.iop > 0 && (n == 0 || (n >= p.itspfh && n % std::max(p.iop, 1) == 0)) && !outh(m, n)) return false;
   if (p.iotr > 0 && (n == 0 || n % std::max(p.iotr, 1) == 0) && !outz(m, n)) return false;
   if (p.ipxml > 0 && (n == 0 || (n >= p.itspf && n % std::max(apxml, 1) == 0)) && !outp(m, n)) return false;

@@ -13,6 +13,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <ctime>
 #include <fstream>
 #include <condition_variable>
 #include <deque>
@@ -104,7 +105,8 @@ struct HostModel {
     double isec = 0, isecp = 0, isec0 = 0;
     int month[12] = {31, 28, 31, 30, 31, 30, 31, 31, 30, 31, 30, 31};
   } date;
-  std::string dir;
+  std::string dir, title;
+  bool space_written = false;   // outs writes its header once (first_entry)
   std::shared_ptr<FILE> f_ptrack;
   std::vector<std::shared_ptr<FILE>> f_tracer, f_plane;
   // frame writer: the main thread packs frames into page-locked buffers (asynchronous copies); a
@@ -157,7 +159,7 @@ bool read_parameters(HostModel& M, const std::string& dir) {
   auto g = [&](double& v) { ok = ok && numeric(R.take(), 14, 20, v); };
   auto gi = [&](int& v) { double x = 0; ok = ok && numeric(R.take(), 14, 20, x); v = (int)std::lround(x); };
   int dummy = 0;
-  R.skip(2);                                     // title block
+  R.skip(1); M.title = R.take();                 // title block '(/(A))'
   R.skip(3); gi(M.iyr0); gi(M.imon0); gi(M.iday0); gi(M.ihr0);
   R.skip(3);
   g(M.xl); g(M.yl); g(M.zl); g(M.tl); g(M.idx); g(M.idy); g(M.idz); g(M.dzmin); g(M.datadj); g(M.zetainit);
@@ -207,8 +209,8 @@ bool read_parameters(HostModel& M, const std::string& dir) {
             "turbulence closure, Smagorinsky, smoothing, non-centred advection or variable layers)";
     return false;
   }
-  if (nnodes > 0 || M.ipxml < 0) {
-    M.err = "si3d_inp.txt: the time-series (outt, nnodes > 0) and XML (outs, ipxml < 0) writers are not built";
+  if (nnodes > 0) {
+    M.err = "si3d_inp.txt: the time-series writer (outt, nnodes > 0) is not built";
     return false;
   }
   if (M.ipxml > 0 && M.iTurbVars != 0) {
@@ -573,6 +575,74 @@ int frame_record(HostModel& M, const std::shared_ptr<FILE>& f, int n, int kind, 
 
 // The output calls of the time loop (si3d.f90:430-438; with n = 0 the initial ones, :89-100):
 // outh (planes), outz (tracers), outp (ptrack file).  Files go to the run directory.
+// outs (si3d_utils.f90:2605-2760) with ipxml < 0: on its first call the XML header of the Gr viewer's
+// binary space files, and the two binary files opened empty.  The reference writes nothing more: its
+// frame writer outs_bin (:2763) is not called anywhere, so the binary files stay empty.  runNumber
+// is the wall-clock date and time (date_and_time), as in the reference.
+int write_space_xml(HostModel& M) {
+  FILE* f = std::fopen((M.dir + "/spacefile.xml").c_str(), "w");
+  if (!f) { M.err = "output: cannot open spacefile.xml"; return SI3D_EDIMS; }
+  for (const char* b : {"spacefile2d.bin", "spacefile3d.bin"}) {
+    FILE* g = std::fopen((M.dir + "/" + b).c_str(), "wb");
+    if (!g) { std::fclose(f); M.err = std::string("output: cannot open ") + b; return SI3D_EDIMS; }
+    std::fclose(g);
+  }
+  // int_to_char(v, 0): the value left-justified between quotes
+  auto quoted = [](long long v) { return "\"" + std::to_string(v) + "\""; };
+  std::fprintf(f, "<?xml version=\"1.0\"?>\n \n<!-- Si3D Output for Gr -->\n");
+  std::fprintf(f, "<!-- xml header file for binary spacefiles -->\n");
+  std::fprintf(f, "<!-- Run Parameters:  dt =%5.2f s  dz =%5.2f m  im =%5d  jm =%5d\n", M.idt, M.idz, M.im, M.jm);
+  std::fprintf(f, "     itrsca =%2d  itrap =%2d  cd = %7.4f  ismooth =%2d  beta =%6.3f  niter =%2d\n", M.itrsca, M.itrap,
+               M.cd, M.ismooth, M.beta, M.niter);
+  std::fprintf(f, "     itrmom =%2d  f =%7.4f  wa =%8.1f -->\n \n", M.itrmom, M.f, M.wa);
+  std::fprintf(f, "<gov.usgs.gr>\n   <obj class=\"gov.usgs.sfhydro.si3d.Si3dOutput\"\n");
+  std::string title = M.title;
+  while (!title.empty() && title.back() == ' ') title.pop_back();
+  std::fprintf(f, "        runTitle=\"%s\"\n", title.c_str());
+  std::time_t now = std::time(nullptr);
+  std::tm lt{};
+  localtime_r(&now, &lt);
+  std::fprintf(f, "        runNumber=\"%04d%02d%02d%02d%02d\"\n", lt.tm_year + 1900, lt.tm_mon + 1, lt.tm_mday, lt.tm_hour,
+               lt.tm_min);
+  // start of the output: itspf rounded up to a multiple of ipxml * idt (idt2 < 0 for ipxml < 0)
+  const long long idt2 = (long long)M.ipxml * (long long)M.idt;
+  HostModel::Date saved = M.date;
+  if (M.itspf == 0) {
+    compute_date(M, 0.0);
+  } else {
+    long long itspf1 = (M.itspf / idt2) * idt2;
+    if (M.itspf % idt2 != 0) itspf1 += idt2;
+    compute_date(M, (double)itspf1);
+  }
+  const int ihr2 = (int)(M.date.isec / 3600);
+  int isec2 = (int)(M.date.isec - ihr2 * 3600);
+  const int imin2 = isec2 / 60;
+  isec2 = isec2 - imin2 * 60;
+  std::fprintf(f, "        startTime=\"%4d/%02d/%02d %02d:%02d:%02d\" timeStepInSeconds=%s>\n", M.date.iyr, M.date.imon,
+               M.date.iday, ihr2, imin2, isec2, quoted(idt2).c_str());
+  M.date = saved;
+  compute_date(M, 0.0);   // reset to the start of the run, as outs does
+  M.date = saved;
+  std::fprintf(f, " \n      <obj class=\"gov.usgs.gr.GrObjectContainer\" title=\"2-D x-y Variables\">\n");
+  std::fprintf(f, "         <dataseries class=\"gov.usgs.gr.data.RafDataSeries\"\n");
+  std::fprintf(f, "            file=\"spacefile2d.bin\"\n");
+  std::fprintf(f, "            title=\"2-D Variables\" numDimensions=%s>\n", quoted(1).c_str());
+  std::fprintf(f, "            <dim num=\"0\" title=\"Zeta\" units=\"meters\" unitScale=\"0.0001\"/>\n \n");
+  std::fprintf(f, "         </dataseries>\n      </obj>\n \n");
+  std::fprintf(f, "      <obj class=\"gov.usgs.gr.GrObjectContainer\" title=\"3-D Variables\">\n");
+  std::fprintf(f, "         <dataseries class=\"gov.usgs.gr.data.RafDataSeries\"\n");
+  std::fprintf(f, "            file=\"spacefile3d.bin\"\n");
+  std::fprintf(f, "            title=\"3-D Variables\" numDimensions=%s>\n", quoted(4).c_str());
+  std::fprintf(f, "            <dim num=\"0\" title=\"u\" units=\"m/s\" unitScale=\"0.0001\"/>\n");
+  std::fprintf(f, "            <dim num=\"1\" title=\"v\" units=\"m/s\" unitScale=\"0.0001\"/>\n");
+  std::fprintf(f, "            <dim num=\"2\" title=\"w\" units=\"m/s\" unitScale=\"0.00001\"/>\n");
+  std::fprintf(f, "            <dim num=\"3\" title=\"dz\" units=\"m**2/s\" unitScale=\"0.0001\"/>\n \n");
+  std::fprintf(f, "         </dataseries>\n      </obj>\n   </obj>\n</gov.usgs.gr>\n \n");
+  std::fclose(f);
+  M.space_written = true;
+  return 0;
+}
+
 int write_outputs(HostModel& M, int n) {
   int rc = 0;
   const int apxml = std::abs(M.ipxml);
@@ -606,6 +676,8 @@ int write_outputs(HostModel& M, int n) {
     for (int t = 1; t <= M.ntr; ++t)
       if ((rc = frame_record(M, M.f_tracer[t - 1], n, SI3D_OUT_TRACER, t))) return rc;
   }
+  // outs, called at n = 0 and every step (MOD(n, MAX(ipxml, 1)) with ipxml < 0), writes once
+  if (M.ipxml < 0 && !M.space_written && (rc = write_space_xml(M))) return rc;
   if (M.ipxml > 0 && (n == 0 || (n >= M.itspf && n % std::max(apxml, 1) == 0))) {
     if (n == 0) {
       M.f_ptrack = open_output(M, "si3d_3D");

@@ -102,3 +102,32 @@ def test_output_files_match_the_oracle(tmp_path, oracle_lib, native_libs):
             assert a[:20] == b[:20], f"{name}: time stamp"
             x, y = np.frombuffer(a[20:], dtype="<f4"), np.frombuffer(b[20:], dtype="<f4")
             np.testing.assert_allclose(x, y, rtol=1e-6, atol=1e-7 * max(np.abs(y).max(), 1e-30), err_msg=name)
+
+
+def test_space_xml_matches_oracle(native_libs, oracle_lib, tmp_path):
+    """The host's outs (ipxml < 0) writes the same XML header as the oracle's, line for line except
+    runNumber (the wall-clock date), and the same two empty binary space files."""
+    import os
+
+    from si3d_b200 import synth
+    from si3d_b200.model import GpuRun
+    dg, do = str(tmp_path / "gpu"), str(tmp_path / "orc")
+    for d in (dg, do):
+        synth.make("t1", d, outputs={"ipxml": -1, "itspf": 0})
+    g = GpuRun(dg, pcg_itmax=2000)
+    try:
+        g.run(3)
+    finally:
+        g.close()
+    o = oracle_lib.OracleRun(do, ordering=1, pcg_itmax=2000)
+    o.run(3)
+    a = open(os.path.join(dg, "spacefile.xml")).read().split("\n")
+    b = open(os.path.join(do, "spacefile.xml")).read().split("\n")
+    assert len(a) == len(b)
+    for x, y in zip(a, b):
+        if "runNumber=" in y:
+            assert x.startswith('        runNumber="') and len(x) == len(y)
+        else:
+            assert x == y
+    for f in ("spacefile2d.bin", "spacefile3d.bin"):
+        assert os.path.getsize(os.path.join(dg, f)) == 0

@@ -138,10 +138,10 @@ def test_tracer_columns_missing_from_profile(native_libs, oracle_lib, run_dirs, 
     assert o.ntr == 2 and not o.get("tracer2").any()
 
 
-@pytest.mark.parametrize("label,value", [("nnodes", 2), ("ipxml", -1)])
+@pytest.mark.parametrize("label,value", [("nnodes", 2)])
 def test_unbuilt_writers_are_refused(native_libs, oracle_lib, run_dirs, tmp_path, label, value):
-    """Time series at nodes (outt) and the XML output (outs) are not built: a run that asks for them
-    is refused instead of running without its files."""
+    """Time series at nodes (outt) are not built: a run that asks for them is refused instead of
+    running without its files."""
     d = _copy(run_dirs["t0"], str(tmp_path / f"w_{label}"))
     _set_records(os.path.join(d, "si3d_inp.txt"), [(label, value)])
     rc, _, err = _open(native_libs, d)

@@ -165,3 +165,28 @@ def test_turbulence_variables_in_ptrack_output_are_refused(tmp_path, oracle_lib,
     err = C.create_string_buffer(256)
     assert h.si3d_host_open(d.encode(), None, C.byref(hm), err, 256) == -101
     assert b"turbulence" in err.value
+
+
+def test_space_xml_header(oracle_lib, tmp_path):
+    """outs with ipxml < 0 (si3d_utils.f90:2605-2760): the Gr header on the first call only, the
+    run parameters in FORMAT 1, the start time of the output and its time step (ipxml * idt, signed
+    as the reference computes it), and the two binary space files left empty (outs_bin has no
+    caller in the reference)."""
+    import os
+
+    from si3d_b200 import synth
+    d = str(tmp_path / "xml")
+    synth.make("t0", d, outputs={"ipxml": -1, "itspf": 0})
+    o = oracle_lib.OracleRun(d, ordering=1, pcg_itmax=2000)
+    o.run(3)
+    lines = open(os.path.join(d, "spacefile.xml")).read().split("\n")
+    assert lines[0] == '<?xml version="1.0"?>' and lines[1] == " "
+    assert lines[4] == "<!-- Run Parameters:  dt =60.00 s  dz = 1.00 m  im =   25  jm =   17"
+    assert lines[5] == "     itrsca = 4  itrap = 1  cd =  0.0025  ismooth = 0  beta = 0.050  niter = 2"
+    assert lines[6] == "     itrmom = 1  f = 0.0001  wa =     8.0 -->"
+    assert lines[10] == '        runTitle="SYNTHETIC t0 24x16x8"'
+    assert lines[12] == '        startTime="2024/01/01 00:00:00" timeStepInSeconds="-60">'
+    assert 'numDimensions="1">' in lines[17] and 'numDimensions="4">' in lines[26]
+    assert lines[-3:] == ["</gov.usgs.gr>", " ", ""]
+    for b in ("spacefile2d.bin", "spacefile3d.bin"):
+        assert os.path.getsize(os.path.join(d, b)) == 0
