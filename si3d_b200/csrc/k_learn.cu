@@ -222,6 +222,179 @@ __global__ void __launch_bounds__(128) k_conv32(const bf16* __restrict__ Xin, co
   }
 }
 
+// ------------------------------------------------------------------ 32 -> 32 conv, tcgen05 (forward)
+// The same convolution on the fifth-generation tensor cores: tcgen05.mma with FP32 accumulators in
+// tensor memory (TMEM), issued by one thread, operands read by the tensor core from shared memory
+// through matrix descriptors.
+//
+// A block takes TC_R output rows x 128 pixels.  Its input tile (TC_R + 2 rows x 130 pixels, 32
+// bf16 channels) is stored as 16-byte channel chunks, sA[row][chunk][pixel][8 channels], so the
+// A operand of tap (di, dj) for output row r - 128 pixels x 16 channels - is a plain K-major matrix
+// starting at row r + 1 + di, pixel 1 + dj: core matrices of 8 pixels x 16 bytes, 16 bytes
+// between pixels, 128 bytes between pixel groups, one chunk row (130 x 16 bytes) between K halves.
+// No im2col copies.  Weights sit as sB[tap][chunk][cout][8 cin] (core matrices of 8 output
+// channels x 16 bytes).  Per output row: 9 taps x 2 K-halves = 18 MMAs of M = 128, N = 32, K = 16
+// into its own 32 TMEM columns; one commit to an mbarrier; then each warp reads its 32 TMEM lanes
+// (its 32 pixels) with tcgen05.ld and applies bias, ReLU and the residual.
+constexpr int TC_R = 4;                        // output rows per block
+constexpr int TC_W = 128;                      // pixels per row (the MMA's M)
+constexpr int TC_WT = TC_W + 2;                // with halo
+constexpr int TC_CHUNK = TC_WT * 16;           // bytes of one chunk row (130 pixels x 16 B)
+constexpr int TC_ROWB = 4 * TC_CHUNK;          // bytes of one halo row (4 chunks)
+constexpr int TC_ABYTES = (TC_R + 2) * TC_ROWB;   // 49,920: the last descriptor ends at its last byte
+constexpr int TC_BBYTES = 9 * 4 * C * 16;          // 18,432
+constexpr int TC_SMEM = TC_ABYTES + TC_BBYTES;
+constexpr int TC_COLS = TC_R * C;              // TMEM columns (128)
+constexpr long long TC_WAIT_LIMIT = 1LL << 24; // mbarrier polls before giving up
+static_assert((TC_R + 2) * TC_ROWB <= TC_ABYTES, "A tile");
+static_assert(TC_COLS == 32 || TC_COLS == 64 || TC_COLS == 128 || TC_COLS == 256, "TMEM allocation");
+
+// Instruction descriptor of kind::f16: D FP32, A and B BF16, both K-major, N = 32, M = 128.
+constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(C >> 3) << 17) | ((uint32_t)(TC_W >> 4) << 24);
+
+// Shared-memory matrix descriptor, no swizzle: start address, the byte offsets between core
+// matrices along K (leading) and along M/N (stride), descriptor version 1.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+__global__ void __launch_bounds__(128) k_conv32_tc(const bf16* __restrict__ Xin, const bf16* __restrict__ Wk,
+                                                   const float* __restrict__ bias, int B, int H, int W,
+                                                   bf16* __restrict__ Xout, float* __restrict__ Y) {
+  extern __shared__ __align__(1024) unsigned char smem[];
+  unsigned char* sA = smem;
+  unsigned char* sB = smem + TC_ABYTES;
+  __shared__ uint32_t s_tmem;
+  __shared__ __align__(8) unsigned long long s_mbar;
+  __shared__ float s_bias[C];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const uint32_t aBase = (uint32_t)__cvta_generic_to_shared(sA);
+  const uint32_t bBase = (uint32_t)__cvta_generic_to_shared(sB);
+  const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mbar);
+  // weights -> sB[tap][chunk][cout][8]; bias; the A region's padding zeroed once
+  for (int r = tid; r < 9 * C * 4; r += 128) {
+    const int t = r / (C * 4), n = (r / 4) % C, kc = r % 4;
+    *reinterpret_cast<uint4*>(sB + (((t * 4 + kc) * C + n) * 16)) =
+        *reinterpret_cast<const uint4*>(&Wk[(t * C + n) * C + kc * 8]);
+  }
+  for (int r = tid; r < C; r += 128) s_bias[r] = bias[r];
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
+                 :: "r"((uint32_t)__cvta_generic_to_shared(&s_tmem)), "r"((uint32_t)TC_COLS) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(mbar) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+  const uint32_t tmem = s_tmem;
+  const int ntj = (W + TC_W - 1) / TC_W, nti = (H + TC_R - 1) / TC_R, ntiles = B * nti * ntj;
+  uint32_t phase = 0;
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+    const int b = tile / (nti * ntj), rem = tile - b * (nti * ntj);
+    const int i0 = (rem / ntj) * TC_R, j0 = (rem % ntj) * TC_W;
+    // the previous tile's TMEM reads and shared-memory reads are complete
+    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    // halo tile: (TC_R + 2) rows x 130 pixels x 4 chunks of 16 bytes, zero outside the image; every
+    // copy of a thread is issued before any is waited for (cp.async, zero-filled when the source
+    // size is 0)
+    for (int r = tid; r < (TC_R + 2) * TC_WT * 4; r += 128) {
+      const int c = r & 3, px = (r >> 2) % TC_WT, row = (r >> 2) / TC_WT;
+      const int gi = i0 + row - 1, gj = j0 + px - 1;
+      const bool in = gi >= 0 && gi < H && gj >= 0 && gj < W;
+      const bf16* src = in ? &Xin[(((size_t)b * H + gi) * W + gj) * C + c * 8] : Xin;
+      const uint32_t dst = aBase + (uint32_t)(row * TC_ROWB + c * TC_CHUNK + px * 16);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(dst), "l"(src), "r"(in ? 16 : 0) : "memory");
+    }
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+    // the tile's writes (made by this thread's copies) become visible to the tensor core's reads
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+    __syncthreads();
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      for (int r = 0; r < TC_R; ++r) {
+        for (int t = 0; t < 9; ++t) {
+          const int di = t / 3 - 1, dj = t % 3 - 1;
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            const uint32_t aAddr = aBase + (uint32_t)((r + 1 + di) * TC_ROWB + 2 * h * TC_CHUNK + (1 + dj) * 16);
+            const uint32_t bAddr = bBase + (uint32_t)(((t * 4 + 2 * h) * C) * 16);
+            const uint64_t ad = tc_desc(aAddr, TC_CHUNK, 128);
+            const uint64_t bd = tc_desc(bAddr, C * 16, 128);
+            const uint32_t acc = (t > 0 || h > 0) ? 1u : 0u;
+            asm volatile(
+                "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                :: "r"(tmem + (uint32_t)(r * C)), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc) : "memory");
+          }
+        }
+      }
+      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                   :: "r"(mbar) : "memory");
+    }
+    // wait for the MMAs (bounded: a wait that gives up poisons this tile's output with NaN)
+    bool done = false;
+    for (long long it = 0; it < TC_WAIT_LIMIT && !done; ++it) {
+      uint32_t ok;
+      asm volatile("{\n.reg .pred q;\nmbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\nselp.u32 %0, 1, 0, q;\n}\n"
+                   : "=r"(ok) : "r"(mbar), "r"(phase) : "memory");
+      done = ok != 0;
+    }
+    phase ^= 1u;
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    // epilogue: warp w reads TMEM lanes 32 w .. 32 w + 31 (pixels), 32 columns (channels) per row
+    const int px = warp * 32 + lane, gj = j0 + px;
+    for (int r = 0; r < TC_R; ++r) {
+      uint32_t v[C];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(r * C);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+          : "r"(taddr) : "memory");
+      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+      const int gi = i0 + r;
+      if (gi >= H || gj >= W) continue;
+      const size_t p = ((size_t)b * H + gi) * W + gj;
+      const unsigned char* xc = sA + (r + 1) * TC_ROWB + (px + 1) * 16;
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const uint4 xin = *reinterpret_cast<const uint4*>(xc + c * TC_CHUNK);
+        const __nv_bfloat162* x2 = reinterpret_cast<const __nv_bfloat162*>(&xin);
+        uint4 o;
+        uint32_t* o32 = reinterpret_cast<uint32_t*>(&o);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+          const int co = c * 8 + 2 * e;
+          float y0 = __uint_as_float(v[co]) + s_bias[co], y1 = __uint_as_float(v[co + 1]) + s_bias[co + 1];
+          if (!done) { y0 = __int_as_float(0x7fc00000); y1 = y0; }
+          if (Y) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
+          const float2 xf = __bfloat1622float2(x2[e]);
+          const __nv_bfloat162 ob = __floats2bfloat162_rn(xf.x + fmaxf(y0, 0.f), xf.y + fmaxf(y1, 0.f));
+          o32[e] = *reinterpret_cast<const uint32_t*>(&ob);
+        }
+        *reinterpret_cast<uint4*>(&Xout[p * C + c * 8]) = o;
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" :: "r"(tmem), "r"((uint32_t)TC_COLS)
+                 : "memory");
+  }
+}
+
 // ------------------------------------------------------------------ head: 32 -> 1, FP32 cores
 __global__ void __launch_bounds__(TP) k_head(const bf16* __restrict__ X, const float* __restrict__ w, int H, int W,
                                              float* __restrict__ out) {
@@ -563,6 +736,22 @@ int conv_blocks(int B, int H, int W) {
   return (int)std::max(1LL, std::min(ntiles, (long long)sms * std::max(occ, 1)));
 }
 
+// Persistent grid of the tcgen05 convolution (its dynamic shared memory enabled once per device).
+int conv_tc_blocks(int B, int H, int W) {
+  int dev = 0, sms = 1, occ = 1;
+  cudaGetDevice(&dev);
+  static bool attr_set[64] = {false};
+  if (dev >= 0 && dev < 64 && !attr_set[dev]) {
+    cudaFuncSetAttribute(k_conv32_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
+    cudaFuncSetAttribute(k_conv32_tc, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    attr_set[dev] = true;
+  }
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv32_tc, 128, TC_SMEM);
+  const long long ntiles = (long long)B * ((H + TC_R - 1) / TC_R) * ((W + TC_W - 1) / TC_W);
+  return (int)std::max(1LL, std::min(ntiles, (long long)sms * std::max(occ, 1)));
+}
+
 void forward(const Workspace& ws, const float* params, const float* feat, int B, int H, int W, float* out,
              cudaStream_t st) {
   const float* bias0 = params + OFF_BLK + 9 * C * C;
@@ -571,9 +760,9 @@ void forward(const Workspace& ws, const float* params, const float* feat, int B,
   for (int k = 0; k < SI3D_NET_BLOCKS; ++k) {
     const bf16* xin = ws.training ? ws.x[k] : ws.x[k & 1];
     bf16* xout = ws.training ? ws.x[k + 1] : ws.x[(k + 1) & 1];
-    k_conv32<CONV_FWD><<<conv_blocks<CONV_FWD>(B, H, W), 128, 0, st>>>(
+    k_conv32_tc<<<conv_tc_blocks(B, H, W), 128, TC_SMEM, st>>>(
         xin, ws.wfwd + (size_t)k * 9 * C * C, bias0 + (size_t)k * BLK_SZ, B, H, W, xout,
-        ws.training ? ws.y[k + 1] : nullptr, nullptr, nullptr);
+        ws.training ? ws.y[k + 1] : nullptr);
   }
   const bf16* xl = ws.training ? ws.x[SI3D_NET_BLOCKS] : ws.x[SI3D_NET_BLOCKS & 1];
   k_head<<<grid, TP, 0, st>>>(xl, ws.head, H, W, out);
