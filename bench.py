@@ -283,9 +283,9 @@ def main() -> int:
     ap.add_argument("--iturb", type=int, default=0, choices=[0, 1],
                     help="1: the Mellor-Yamada 2.5 closure instead of constant eddy coefficients")
     ap.add_argument("--forms", default="",
-                    help="comma-separated subset of plain_fp64,mixed_ir,mixed_last,learned_fp64,learned_mixed (the last one "
-                         "is the headline); default: plain_fp64,mixed_ir,mixed_last and learned_mixed when trained "
-                         "parameters exist")
+                    help="comma-separated subset of plain_fp64,mixed_ir,mixed_last,learned_fp64,learned_mixed,"
+                         "learned_mg,mg_mixed (the last one is the headline); default: plain_fp64,mixed_ir,mixed_last, "
+                         "learned_mixed and learned_mg when trained parameters exist, then mg_mixed")
     args = ap.parse_args()
     ws, rank, local = _dist()
     if args.warmup < 3:
@@ -443,9 +443,12 @@ def main() -> int:
              "learned_mixed": (native.SI3D_MIXED_IR, native.SI3D_X0_LEARNED, params),
              "mg_mixed": (native.SI3D_MIXED_MG, native.SI3D_X0_LAST, None),
              "learned_mg": (native.SI3D_MIXED_MG, native.SI3D_X0_LEARNED, params)}
+    # the last form is the headline: multigrid inner solves from the latest solution.  The learned
+    # guess is measured beside it (same solver, the network's guess for the leapfrog solve); on these
+    # basins it saves no multigrid iterations and costs the network's inference, so it is not the headline.
     names = args.forms.split(",") if args.forms else (
-        ["plain_fp64", "mixed_ir", "mixed_last", "mg_mixed"] +
-        (["learned_mixed", "learned_mg"] if params is not None else []))
+        ["plain_fp64", "mixed_ir", "mixed_last"] +
+        (["learned_mixed", "learned_mg"] if params is not None else []) + ["mg_mixed"])
     forms = [(f, *known[f]) for f in names]
     if any(f.startswith("learned") for f in names) and params is None:
         raise SystemExit("learned forms need " + learn.DEFAULT_PARAMS)

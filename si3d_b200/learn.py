@@ -241,6 +241,27 @@ def iterations(run_dir: str, steps: int, *, params: Optional[np.ndarray], x0_mod
         run.close()
 
 
+def time_forward(height: int, width: int, reps: int, params_path: str = DEFAULT_PARAMS) -> int:
+    """One inference of the network on a random (1, height, width, 4) feature image, 3 untimed and
+    `reps` timed, with CUDA events on the launching stream; prints the mean time per inference."""
+    import torch
+    from .build import build_all
+    build_all()
+    net = Net(1, height, width, load_params(params_path))
+    feat = torch.randn(1, height, width, 4, device=net.dev)
+    for _ in range(3):
+        net.forward(feat)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        net.forward(feat)
+    e1.record()
+    torch.cuda.synchronize()
+    print(json.dumps({"forward_ms": e0.elapsed_time(e1) / reps, "height": height, "width": width, "reps": reps}))
+    return 0
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(prog="python -m si3d_b200.learn")
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -255,7 +276,14 @@ def main(argv=None) -> int:
     e.add_argument("--workload", default="c2")
     e.add_argument("--steps", type=int, default=10)
     e.add_argument("--params", default=DEFAULT_PARAMS)
+    f = sub.add_parser("forward", help="time one network inference on a (height x width) image")
+    f.add_argument("--height", type=int, default=2002)
+    f.add_argument("--width", type=int, default=1002)
+    f.add_argument("--reps", type=int, default=20)
+    f.add_argument("--params", default=DEFAULT_PARAMS)
     args = ap.parse_args(argv)
+    if args.cmd == "forward":
+        return time_forward(args.height, args.width, args.reps, args.params)
     if args.cmd == "train":
         train(args.out, basins=args.basins, steps=args.steps, iters=args.iters, workload=args.workload, seed=args.seed)
         return 0
