@@ -243,8 +243,9 @@ int si3d_gpu_column_tridiag_noalloc(int n, int nsys, const double* a, const doub
 
 /* Autotuner (no reference counterpart): times every candidate launch shape of the momentum and
  * scalar-transport stages on this handle's current state and keeps the fastest - layer lanes per
- * column of the cell-parallel kernels (2, 4, 8) and threads per block of the column-sequential
- * kernels (64, 128, 256).  The fields those stages write are restored afterwards, so the state is
+ * column of the cell-parallel kernels (2, 4, 8; for momentum also 1, which selects the fused kernel
+ * that forms the explicit terms and runs the column sweep in one pass down each face column) and
+ * threads per block of the column-sequential kernels (64, 128, 256).  The fields those stages write are restored afterwards, so the state is
  * unchanged; shapes never change results.  `reps` timed launches per candidate; the choice
  * {mom_lanes, mom_threads, scalar_lanes, scalar_threads} is returned through `choice` (optional). */
 int si3d_gpu_autotune(int handle, int reps, int* choice);

@@ -330,16 +330,347 @@ __global__ void __launch_bounds__(NT, 768 / NT) k_mom_columns(Dev d, const FaceM
   else { d.s.eagy[l - 1] = sg; d.s.eary[l - 1] = sr; }
 }
 
+// ------------------------------------------------------------------ fused kernel
+// k_mom_fused (one thread per face column): the cell and the column work of a face column in one
+// pass down the column.  At layer k the thread forms the explicit term and the baroclinic increment
+// exactly as k_mom_cells does and feeds them straight into the forward sweep of k_mom_columns, so
+// neither goes through memory, and every input is read once.  The values that layer k needs and the
+// layer above it did not (32 FP64 loads: the layer's own cells and its neighbours, and layer k + 1
+// where the sweep or the vertical terms reach down) are copied by cp.async into this thread's slots
+// of a shared-memory ring, RD layers ahead; the values shared with the layer above (thickness,
+// velocity, wp, upp and Av of layer k, depth and density of layer k - 1 for the bottom-layer
+// interpolation) are carried in registers.  Same expressions in the same order as the split
+// kernels: the results are bit-identical to theirs.
+namespace fz {
+enum { HKP, HPL, HPO, A0, A1, A2, A3, B0, B1, B2, WDO, WDL, UVD, UVE, UVW, UVN, UVS, OWN, UPP1,
+       HPPL, HPPE, HPPN, HPPW, HPPS, PN, PS, PE, PW, RHO_O, RHO_L, AVO, AVL, NIN };
+}
+
+template <int NT, int RD>
+constexpr int fused_smem() { return RD * fz::NIN * NT * (int)sizeof(double); }
+
+template <int IEQ, int NT, int RD>
+__global__ void __launch_bounds__(NT) k_mom_fused(Dev d, const FaceMeta* __restrict__ meta, int ncols) {
+  extern __shared__ double ring[];   // [RD][NIN][NT]: a thread's slots are its own
+  const int t = blockIdx.x * NT + threadIdx.x;
+  if (t >= ncols) return;
+  const bool X = (IEQ == 1);
+  const int4 ma = __ldg(&meta[t].a), mb = __ldg(&meta[t].b);
+  const int l = ma.x, lE = ma.y, lW = ma.z, lN = ma.w, lS = mb.x, lX2 = mb.y, kmx = mb.z;
+  const int lO = X ? lE : lN;
+  const int* k1f = X ? d.s.k1u : d.s.k1v;
+  const int k1x = NB(k1f, l);
+  const int nw = kmx - k1x + 1;
+  if (nw < 1) return;
+  const int mW_last = mb.w, mS_last = __ldg(&meta[t].c.x);
+  const int mW_first = mW_last >= 0 ? NB(k1f, lW) : 0;
+  const int mS_first = mS_last >= 0 ? NB(k1f, lS) : 0;
+  const double* __restrict__ huv = X ? d.f.hup : d.f.hvp;
+  const double* __restrict__ huvpp = X ? d.f.hupp : d.f.hvpp;
+  const double* __restrict__ uvpp_h = X ? d.f.uhpp : d.f.vhpp;
+  const double* __restrict__ uvp = X ? d.f.up : d.f.vp;
+  const double* __restrict__ uvpp = X ? d.f.upp : d.f.vpp;
+  const double* __restrict__ vhp = d.f.vhp;
+  const double* __restrict__ uhp = d.f.uhp;
+  const double* __restrict__ wp = d.f.wp;
+  const double* __restrict__ hp3 = d.f.hp;
+  const double* __restrict__ rhop = d.f.rhop;
+  const double* __restrict__ Av = d.f.Av;
+  double* __restrict__ agA = X ? d.f.agx : d.f.agy;
+  double* __restrict__ arA = X ? d.f.arx : d.f.ary;
+  double* __restrict__ cc = d.scr;
+  const double twodt1 = d.p.twodt * d.tz, tz = d.tz, theta = d.p.theta;
+  const double gdt = X ? d.p.gdtdx : d.p.gdtdy;
+  const bool ihd = d.p.ihd == 1, ibc = d.p.ibc != 0;
+  const int P = d.g.P;
+  const int dE = lE - l, dW = lW - l, dN = lN - l, dS = lS - l, dX2 = lX2 - l, dO = lO - l;
+  const int tid = threadIdx.x;
+  auto sp = [&](int s, int i) { return &ring[(s * fz::NIN + i) * NT + tid]; };
+  auto issue = [&](int kk, int s) {   // the new inputs of layer kk into ring slot s
+    const int ikk = IX(d, kk, l);
+    cp_async8(sp(s, fz::HKP), &huv[ikk + P]);
+    cp_async8(sp(s, fz::HPL), &hp3[ikk]);
+    cp_async8(sp(s, fz::HPO), &hp3[ikk + dO]);
+    if (X) {
+      cp_async8(sp(s, fz::A0), &vhp[ikk + dE]);
+      cp_async8(sp(s, fz::A1), &vhp[ikk]);
+      cp_async8(sp(s, fz::A2), &vhp[ikk + dX2]);
+      cp_async8(sp(s, fz::A3), &vhp[ikk + dS]);
+      cp_async8(sp(s, fz::B0), &uhp[ikk + dE]);
+      cp_async8(sp(s, fz::B1), &uhp[ikk]);
+      cp_async8(sp(s, fz::B2), &uhp[ikk + dW]);
+    } else {
+      cp_async8(sp(s, fz::A0), &uhp[ikk + dN]);
+      cp_async8(sp(s, fz::A1), &uhp[ikk]);
+      cp_async8(sp(s, fz::A2), &uhp[ikk + dX2]);
+      cp_async8(sp(s, fz::A3), &uhp[ikk + dW]);
+      cp_async8(sp(s, fz::B0), &vhp[ikk + dN]);
+      cp_async8(sp(s, fz::B1), &vhp[ikk]);
+      cp_async8(sp(s, fz::B2), &vhp[ikk + dS]);
+    }
+    cp_async8(sp(s, fz::WDO), &wp[ikk + P + dO]);
+    cp_async8(sp(s, fz::WDL), &wp[ikk + P]);
+    cp_async8(sp(s, fz::UVD), &uvp[ikk + P]);
+    cp_async8(sp(s, fz::UVE), &uvp[ikk + dE]);
+    cp_async8(sp(s, fz::UVW), &uvp[ikk + dW]);
+    cp_async8(sp(s, fz::UVN), &uvp[ikk + dN]);
+    cp_async8(sp(s, fz::UVS), &uvp[ikk + dS]);
+    cp_async8(sp(s, fz::OWN), &uvpp_h[ikk]);
+    cp_async8(sp(s, fz::UPP1), &uvpp[ikk + P]);
+    if (ihd) {
+      cp_async8(sp(s, fz::HPPL), &huvpp[ikk]);
+      cp_async8(sp(s, fz::HPPE), &huvpp[ikk + dE]);
+      cp_async8(sp(s, fz::HPPN), &huvpp[ikk + dN]);
+      cp_async8(sp(s, fz::HPPW), &huvpp[ikk + dW]);
+      cp_async8(sp(s, fz::HPPS), &huvpp[ikk + dS]);
+      cp_async8(sp(s, fz::PN), &uvpp[ikk + dN]);
+      cp_async8(sp(s, fz::PS), &uvpp[ikk + dS]);
+      cp_async8(sp(s, fz::PE), &uvpp[ikk + dE]);
+      cp_async8(sp(s, fz::PW), &uvpp[ikk + dW]);
+    }
+    if (ibc) {
+      cp_async8(sp(s, fz::RHO_O), &rhop[ikk + dO]);
+      cp_async8(sp(s, fz::RHO_L), &rhop[ikk]);
+    }
+    cp_async8(sp(s, fz::AVO), &Av[ikk + P + dO]);
+    cp_async8(sp(s, fz::AVL), &Av[ikk + P]);
+  };
+#pragma unroll
+  for (int j = 0; j < RD; ++j) {   // one commit group per layer (empty past the bottom)
+    if (k1x + j <= kmx) issue(k1x + j, j);
+    cp_async_commit();
+  }
+  // column totals and surface / bottom terms while the first layers are in flight (as k_mom_columns)
+  double rsum = 0;
+#pragma unroll 4
+  for (int k = k1x; k <= kmx; ++k) rsum += 1000 + rhop[IX(d, k, l)];
+  const double rhopx = rsum / nw;
+  const double ws0 = rhopx * gdt * (d.s.spp[lO - 1] - d.s.spp[l - 1]);
+  double cwx;
+  {
+    const double ua = d.s.uair[l - 1], va = d.s.vair[l - 1];
+    if (X) {
+      const double usurf = d.f.up[IX(d, k1x, l)];
+      const double vsurf = (d.f.vp[IX(d, NB(d.s.k1v, l), l)] + d.f.vp[IX(d, NB(d.s.k1v, lS), lS)] +
+                            d.f.vp[IX(d, NB(d.s.k1v, lE), lE)] + d.f.vp[IX(d, NB(d.s.k1v, lX2), lX2)]) / 4.;
+      cwx = d.s.cdw[l - 1] * RHOAIR * sqrt((va - vsurf) * (va - vsurf) + (ua - usurf) * (ua - usurf));
+    } else {
+      const double vsurf = d.f.vp[IX(d, k1x, l)];
+      const double usurf = (d.f.up[IX(d, NB(d.s.k1u, l), l)] + d.f.up[IX(d, NB(d.s.k1u, lW), lW)] +
+                            d.f.up[IX(d, NB(d.s.k1u, lN), lN)] + d.f.up[IX(d, NB(d.s.k1u, lX2), lX2)]) / 4.;
+      cwx = d.s.cdw[l - 1] * RHOAIR * sqrt((ua - usurf) * (ua - usurf) + (va - vsurf) * (va - vsurf));
+    }
+  }
+  double taub;
+  {
+    const double hkb = huv[IX(d, kmx, l)];
+    double q;
+    if (X) q = 0.25 * (d.f.vhpp[IX(d, kmx, lE)] + d.f.vhpp[IX(d, kmx, l)] + d.f.vhpp[IX(d, kmx, lS)] +
+                       d.f.vhpp[IX(d, kmx, lX2)]);
+    else q = 0.25 * (d.f.uhpp[IX(d, kmx, lN)] + d.f.uhpp[IX(d, kmx, lX2)] + d.f.uhpp[IX(d, kmx, lW)] +
+                     d.f.uhpp[IX(d, kmx, l)]);
+    const double own = uvpp_h[IX(d, kmx, l)];
+    taub = d.p.cd * sqrt((own * own) + q * q) / (hkb * hkb);
+  }
+  const double taus_g = cwx / rhopx * (X ? d.s.uair[l - 1] : d.s.vair[l - 1]);
+  const double taus_a = cwx / rhopx / huv[IX(d, k1x, l)];
+  // carried values: layer k - 1 and k of the column, as the first iteration sees them
+  const int ik0 = IX(d, k1x, l);
+  double hkm = huv[ik0 - P], hk = huv[ik0];
+  double upm = uvpp[ik0 - P], upk = uvpp[ik0];
+  double uvU = uvp[ik0 - P], uc = uvp[ik0];
+  double avo = Av[ik0 + dO], avl = Av[ik0];
+  double wprev = 0.0;                                       // wp sum of layer k (the layer above's wD)
+  double hpl_prev = 0.0, hpo_prev = 0.0, ro_prev = 0.0, rl_prev = 0.0;
+  const double rrho = 1.0 / rhopx;
+  double rhk = 1.0 / hk, rhkm = 0.0, rkm = 0.0;
+  double bcl = 0, c1p = 0, d1p = 0, e1p = 0, hdr_prev = 0;
+  for (int k = k1x, s = 0; k <= kmx; ++k, s = (s + 1 == RD) ? 0 : s + 1) {
+    const int ik = IX(d, k, l);
+    cp_async_wait<RD - 1>();   // layer k's group has landed (this thread's own copies)
+    const double hkp = *sp(s, fz::HKP);
+    const double hpl = *sp(s, fz::HPL), hpo = *sp(s, fz::HPO);
+    // ---- explicit term (k_mom_cells)
+    double cor, uE, uW, vN, vS;
+    if (X) {
+      const double vE = *sp(s, fz::A0), vC = *sp(s, fz::A1), vX = *sp(s, fz::A2), vSS = *sp(s, fz::A3);
+      const double uEE = *sp(s, fz::B0), uC = *sp(s, fz::B1), uWW = *sp(s, fz::B2);
+      cor = 0.25 * d.p.f * (vE + vC + vX + vSS);
+      uE = uEE + uC;
+      uW = uC + uWW;
+      vN = vE + vC;
+      vS = vX + vSS;
+    } else {
+      const double uN = *sp(s, fz::A0), uC = *sp(s, fz::A1), uX = *sp(s, fz::A2), uWW = *sp(s, fz::A3);
+      const double vNN = *sp(s, fz::B0), vC = *sp(s, fz::B1), vSS = *sp(s, fz::B2);
+      cor = 0.25 * d.p.f * (uN + uC + uX + uWW);
+      uE = uN + uC;
+      uW = uX + uWW;
+      vN = vNN + vC;
+      vS = vC + vSS;
+    }
+    const double wDraw = *sp(s, fz::WDO) + *sp(s, fz::WDL);
+    double wU = wprev, wD = wDraw;
+    const double uvD = *sp(s, fz::UVD);
+    const double uvE = *sp(s, fz::UVE), uvW = *sp(s, fz::UVW), uvN = *sp(s, fz::UVN), uvS = *sp(s, fz::UVS);
+    const double own_pp = *sp(s, fz::OWN);
+    double hd = 0.0;
+    if (ihd) {
+      const double hppl = *sp(s, fz::HPPL), hppE = *sp(s, fz::HPPE), hppN = *sp(s, fz::HPPN);
+      const double hppW = *sp(s, fz::HPPW), hppS = *sp(s, fz::HPPS);
+      const double pc = upk, pN = *sp(s, fz::PN), pS = *sp(s, fz::PS), pE = *sp(s, fz::PE), pW = *sp(s, fz::PW);
+      const double ax_l = d.p.Ax0 * fmin(hppE, hppl);
+      const double ay_l = d.p.Ay0 * fmin(hppN, hppl);
+      const double ax_w = face_coef(d, d.p.Ax0, hppl, hppW, lW, mW_first, mW_last, k);
+      const double ay_s = face_coef(d, d.p.Ay0, hppl, hppS, lS, mS_first, mS_last, k);
+      hd = (ay_l * (pN - pc) - ay_s * (pc - pS)) / d.p.dydy + (ax_l * (pE - pc) - ax_w * (pc - pW)) / d.p.dxdx;
+    }
+    double ex;
+    if (hpl <= ZERO || hpo <= ZERO) {
+      ex = own_pp;
+    } else {
+      const double th_k = (k == k1x) ? 0.0 : hkm / (hkm + hk);
+      const double th1_k = (k == k1x) ? 0.0 : 1. - th_k;
+      const double th_kp = (k == kmx) ? 0.5 : hk / (hk + hkp);
+      const double th1_kp = (k == kmx) ? 0.5 : 1. - th_kp;
+      if (k == k1x) wU = 0.0;
+      if (k == kmx) wD = 0.0;
+      const double scE = uvE + uc, scW = uvW + uc;
+      const double scN = uvN + uc, scS = uvS + uc;
+      double adv = (uE * scE - uW * scW) / d.p.fourdx + (vN * scN - vS * scS) / d.p.fourdy;
+      adv = adv + (wU * (th_k * uc + th1_k * uvU) - wD * (th_kp * uvD + th1_kp * uc)) / 2.;
+      if (X) ex = own_pp - twodt1 * (adv * d.p.iadv - cor - hd);
+      else ex = own_pp - twodt1 * (adv * d.p.iadv + cor - hd);
+    }
+    // ---- baroclinic increment, bottom layer via bclnc_km (layer k - 1 carried)
+    double hdr = 0, ro = 0, rl = 0;
+    if (ibc) {
+      ro = *sp(s, fz::RHO_O);
+      rl = *sp(s, fz::RHO_L);
+      hdr = gdt * hk * (ro - rl);
+      if (k == kmx && kmx > k1x) {
+        const double eps = 2.220446049250313e-16;
+        const double hplus = hk + eps, hminus = hk - eps;
+        bool co, cw;
+        double rho_o, rho_w;
+        if (hpo > hplus || hpo < hminus) {
+          co = true;
+          const double dz1 = 0.5 * (hpo_prev + hpo);
+          const double dz2 = 0.5 * (hpo_prev + hk);
+          rho_o = ro_prev + (dz2 / dz1) * (ro - ro_prev);
+        } else { co = false; rho_o = ro; }
+        if (hpl > hplus || hpl < hminus) {
+          cw = true;
+          const double dz1 = 0.5 * (hpl_prev + hpl);
+          const double dz2 = 0.5 * (hpl_prev + hk);
+          rho_w = rl_prev + (dz2 / dz1) * (rl - rl_prev);
+        } else { cw = false; rho_w = rl; }
+        if (co || cw) hdr = gdt * hk * (rho_o - rho_w);
+      }
+    }
+    // ---- forward sweep (k_mom_columns)
+    const double upp1 = *sp(s, fz::UPP1);
+    const double avop = *sp(s, fz::AVO), avlp = *sp(s, fz::AVL);
+    const double rkp = 1.0 / (hk + hkp), rhkp = 1.0 / hkp;
+    const double Avk = (k > k1x) ? 0.5 * (avo + avl) : 0.0;
+    const double Avkp = (k < kmx) ? 0.5 * (avop + avlp) : 0.0;
+    double vdiff = 0.0;
+    if (nw >= 2) {
+      const double fk = (k > k1x) ? Avk * (upm - upk) * rkm : 0.0;
+      const double fkp = (k < kmx) ? Avkp * (upk - upp1) * rkp : 0.0;
+      vdiff = d.p.twodt * (fk - fkp) * 2. * (1. - theta);
+    }
+    double a1 = 0, a2, a3 = 0;
+    if (nw == 1) {
+      a2 = 1.0;
+    } else {
+      if (k < kmx) a3 = -twodt1 * Avkp * (rhkp * rkp) * 2. * theta;
+      if (k > k1x) a1 = -twodt1 * Avk * (rhkm * rkm) * 2. * theta;
+      a2 = 1.0 - (hkm * rhk) * a1 - (hkp * rhk) * a3;
+    }
+    if (ibc) {
+      if (k == k1x) bcl = hdr;
+      else if (X) { const double aaux = hdr_prev + hdr; bcl = bcl + aaux; }
+      else bcl = bcl + hdr_prev + hdr;
+    }
+    hdr_prev = hdr;
+    const double hh = hk * rrho;
+    const double vtz = vdiff * tz;
+    double gg = ex - hh * (bcl + ws0) * tz + vtz;
+    if (k == k1x) { gg = gg + taus_g * twodt1; a2 = a2 + taus_a * twodt1; }
+    if (k == kmx) a2 = a2 + taub * twodt1;
+    double c1v, d1v, e1v;
+    if (k == k1x) {
+      const double r = 1.0 / a2;
+      c1v = a3 * r; d1v = gg * r; e1v = hh * r;
+    } else {
+      const double r = 1.0 / (a2 - a1 * c1p);
+      c1v = a3 * r;
+      d1v = (gg - a1 * d1p) * r;
+      e1v = (hh - a1 * e1p) * r;
+    }
+    cc[ik] = c1v; agA[ik] = d1v; arA[ik] = e1v;
+    // refill the slot with layer k + RD (its values are consumed: the stores above depend on them)
+    if (k + RD <= kmx) issue(k + RD, s);
+    cp_async_commit();
+    c1p = c1v; d1p = d1v; e1p = e1v;
+    hkm = hk; hk = hkp;
+    upm = upk; upk = upp1;
+    avo = avop; avl = avlp;
+    rhkm = rhk; rhk = rhkp; rkm = rkp;
+    uvU = uc; uc = uvD;
+    wprev = wDraw;
+    hpl_prev = hpl; hpo_prev = hpo; ro_prev = ro; rl_prev = rl;
+  }
+  // back substitution, summing the depth totals on the way up
+  double d2 = d1p, e2 = e1p;
+  double sg = d2, sr = e2;
+#pragma unroll 4
+  for (int k = kmx - 1; k >= k1x; --k) {
+    const int ik = IX(d, k, l);
+    const double c = cc[ik];
+    d2 = agA[ik] - c * d2;
+    e2 = arA[ik] - c * e2;
+    agA[ik] = d2; arA[ik] = e2;
+    sg += d2; sr += e2;
+  }
+  if (X) { d.s.eagx[l - 1] = sg; d.s.earx[l - 1] = sr; }
+  else { d.s.eagy[l - 1] = sg; d.s.eary[l - 1] = sr; }
+}
+
+template <int IEQ, int NT, int RD>
+void launch_fused(const Dev& d, const FaceMeta* cols, int ncols, cudaStream_t st) {
+  k_mom_fused<IEQ, NT, RD><<<(ncols + NT - 1) / NT, NT, fused_smem<NT, RD>(), st>>>(d, cols, ncols);
+}
+
+template <int NT, int RD>
+int fused_attr() {
+  const int b = fused_smem<NT, RD>();
+  if (cudaFuncSetAttribute(k_mom_fused<1, NT, RD>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_mom_fused<2, NT, RD>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess)
+    return -1;
+  return 0;
+}
+
 }  // namespace
 
 int momentum_init(int km1) {
-  (void)km1;   // no per-handle launch attributes: both kernels use static resources only
+  (void)km1;   // the fused kernel's ring is sized by its threads, not by the column depth
+  if (fused_attr<64, 3>() || fused_attr<128, 2>() || fused_attr<256, 2>()) return -1;
   return 0;
 }
 
 template <int IEQ>
 void launch_dir(const Dev& d, const FaceMeta* cols, int ncols, const Tune& tu, cudaStream_t st, const ObcDev* obc,
                 int nobc) {
+  if (tu.mom_cl == 1 && nobc == 0) {   // one pass per column (open boundaries need the split kernels)
+    switch (tu.mom_nt) {
+      case 64: launch_fused<IEQ, 64, 3>(d, cols, ncols, st); break;
+      case 256: launch_fused<IEQ, 256, 2>(d, cols, ncols, st); break;
+      default: launch_fused<IEQ, 128, 2>(d, cols, ncols, st); break;
+    }
+    return;
+  }
   const int g1 = (ncols + CW - 1) / CW;
   switch (tu.mom_cl) {
     case 2: k_mom_cells<IEQ, 2><<<g1, dim3(CW, 2), 0, st>>>(d, cols, ncols); break;

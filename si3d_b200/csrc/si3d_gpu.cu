@@ -1747,7 +1747,7 @@ int si3d_gpu_autotune(int h, int reps, int* choice) {
     *knob = best_v;
   };
   Tune& tu = c->tune;
-  pick(0, &tu.mom_cl, {2, 4, 8});
+  pick(0, &tu.mom_cl, {1, 2, 4, 8});   // 1: the fused one-pass kernel
   pick(0, &tu.mom_nt, {64, 128, 256});
   if (c->prm.isal != 0) {
     pick(1, &tu.sal_cl, {2, 4, 8});
@@ -1773,7 +1773,8 @@ int si3d_gpu_set_tune(int h, const int* choice) {
   if (!c || !choice) return c ? SI3D_EDIMS : SI3D_EHANDLE;
   auto ok_cl = [](int v) { return v == 2 || v == 4 || v == 8; };
   auto ok_nt = [](int v) { return v == 64 || v == 128 || v == 256; };
-  if (!ok_cl(choice[0]) || !ok_nt(choice[1]) || !ok_cl(choice[2]) || !ok_nt(choice[3])) return SI3D_EDIMS;
+  if (!(choice[0] == 1 || ok_cl(choice[0])) || !ok_nt(choice[1]) || !ok_cl(choice[2]) || !ok_nt(choice[3]))
+    return SI3D_EDIMS;
   c->tune.mom_cl = choice[0]; c->tune.mom_nt = choice[1]; c->tune.sal_cl = choice[2]; c->tune.sal_nt = choice[3];
   return 0;
 }
