@@ -241,7 +241,7 @@ int si3d_gpu_counters(int handle, long long* launches, double* stage_ms, long lo
 int si3d_gpu_column_tridiag_noalloc(int n, int nsys, const double* a, const double* b, const double* c,
                                    const double* g, const double* r, double* ag, double* ar, void* stream);
 
-/* Autotuner (no reference counterpart): times every candidate launch shape of the momentum and
+/* Autotuner (no reference counterpart): times every pair of launch-shape knobs of the momentum and
  * scalar-transport stages on this handle's current state and keeps the fastest - layer lanes per
  * column of the cell-parallel kernels (2, 4, 8; for momentum also 1, which selects the fused kernel
  * that forms the explicit terms and runs the column sweep in one pass down each face column) and

@@ -40,6 +40,10 @@ struct Grid {
 struct Params {
   double dt, dx, dy, twodt, dtdx, dtdy, gdtdx, gdtdy, gdt2dx2, gdt2dy2, twodx, twody, fourdx, fourdy, dxdx,
       dydy;
+  // reciprocals of the grid constants: the momentum and scalar-transport kernels multiply by these
+  // where the reference divides (a product is a few instructions, an FP64 division a long dependent
+  // chain; the results differ from the quotients by at most an ulp)
+  double rfourdx, rfourdy, rdxdx, rdydy, rdx, rdy;
   double Av0, Dv0, Ax0, Ay0, f, theta, cd, cw;
   int iadv, itrmom, ihd, ibc, isal;
 };

@@ -15,10 +15,12 @@
 //   coefficients and boundary terms (wind and bottom stress) and the Thomas sweeps with two
 //   right-hand sides - reading the staged ex/increment back and writing the final ag/ar.  The c'
 //   coefficients of the forward sweep go to the Thomas scratch array.
-// The cell kernel evaluates the reference's expressions in its operation order.  The column kernel
-// shares reciprocals between the tridiagonal coefficients (three divisions a layer instead of ten)
-// and sums the depth totals during the back substitution (bottom to top), so ag, ar, eag and ear
-// agree with the reference's arithmetic to a few units in the last place.
+// The cell kernel evaluates the reference's expressions in its operation order, except that it
+// multiplies by the reciprocals of the grid constants (4 dx, 4 dy, dx^2, dy^2) where the reference
+// divides by them, and forms the interpolation weights hk / (hk + hkp) as hk * (1 / (hk + hkp)).  The column kernel shares reciprocals between the tridiagonal coefficients (three
+// divisions a layer instead of ten) and sums the depth totals during the back substitution (bottom
+// to top), so ag, ar, eag and ear agree with the reference's arithmetic to a few units in the last
+// place.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
@@ -118,21 +120,21 @@ __global__ void __launch_bounds__(CW * CL, 768 / (CW * CL)) k_mom_cells(Dev d, c
       const double ay_l = d.p.Ay0 * fmin(hppN, hppl);
       const double ax_w = face_coef(d, d.p.Ax0, hppl, hppW, lW, mW_first, mW_last, k);
       const double ay_s = face_coef(d, d.p.Ay0, hppl, hppS, lS, mS_first, mS_last, k);
-      hd = (ay_l * (pN - pc) - ay_s * (pc - pS)) / d.p.dydy + (ax_l * (pE - pc) - ax_w * (pc - pW)) / d.p.dxdx;
+      hd = (ay_l * (pN - pc) - ay_s * (pc - pS)) * d.p.rdydy + (ax_l * (pE - pc) - ax_w * (pc - pW)) * d.p.rdxdx;
     }
     double ex;
     if (hpl <= ZERO || hpo <= ZERO) {
       ex = own_pp;
     } else {
-      const double th_k = (k == k1x) ? 0.0 : hkm / (hkm + hk);
+      const double th_k = (k == k1x) ? 0.0 : hkm * (1.0 / (hkm + hk));
       const double th1_k = (k == k1x) ? 0.0 : 1. - th_k;
-      const double th_kp = (k == kmx) ? 0.5 : hk / (hk + hkp);
+      const double th_kp = (k == kmx) ? 0.5 : hk * (1.0 / (hk + hkp));
       const double th1_kp = (k == kmx) ? 0.5 : 1. - th_kp;
       if (k == k1x) wU = 0.0;
       if (k == kmx) wD = 0.0;
       const double scE = uvE + uc, scW = uvW + uc;
       const double scN = uvN + uc, scS = uvS + uc;
-      double adv = (uE * scE - uW * scW) / d.p.fourdx + (vN * scN - vS * scS) / d.p.fourdy;
+      double adv = (uE * scE - uW * scW) * d.p.rfourdx + (vN * scN - vS * scS) * d.p.rfourdy;
       adv = adv + (wU * (th_k * uc + th1_k * uvU) - wD * (th_kp * uvD + th1_kp * uc)) / 2.;
       if (X) ex = own_pp - twodt1 * (adv * d.p.iadv - cor - hd);
       else ex = own_pp - twodt1 * (adv * d.p.iadv + cor - hd);
@@ -349,8 +351,8 @@ enum { HKP, HPL, HPO, A0, A1, A2, A3, B0, B1, B2, WDO, WDL, UVD, UVE, UVW, UVN, 
 template <int NT, int RD>
 constexpr int fused_smem() { return RD * fz::NIN * NT * (int)sizeof(double); }
 
-template <int IEQ, int NT, int RD>
-__global__ void __launch_bounds__(NT) k_mom_fused(Dev d, const FaceMeta* __restrict__ meta, int ncols) {
+template <int IEQ, int NT, int RD, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_mom_fused(Dev d, const FaceMeta* __restrict__ meta, int ncols) {
   extern __shared__ double ring[];   // [RD][NIN][NT]: a thread's slots are its own
   const int t = blockIdx.x * NT + threadIdx.x;
   if (t >= ncols) return;
@@ -481,6 +483,7 @@ __global__ void __launch_bounds__(NT) k_mom_fused(Dev d, const FaceMeta* __restr
   double uvU = uvp[ik0 - P], uc = uvp[ik0];
   double avo = Av[ik0 + dO], avl = Av[ik0];
   double wprev = 0.0;                                       // wp sum of layer k (the layer above's wD)
+  double thq_prev = 0.0;                                    // hkm / (hkm + hk) of layer k
   double hpl_prev = 0.0, hpo_prev = 0.0, ro_prev = 0.0, rl_prev = 0.0;
   const double rrho = 1.0 / rhopx;
   double rhk = 1.0 / hk, rhkm = 0.0, rkm = 0.0;
@@ -523,21 +526,25 @@ __global__ void __launch_bounds__(NT) k_mom_fused(Dev d, const FaceMeta* __restr
       const double ay_l = d.p.Ay0 * fmin(hppN, hppl);
       const double ax_w = face_coef(d, d.p.Ax0, hppl, hppW, lW, mW_first, mW_last, k);
       const double ay_s = face_coef(d, d.p.Ay0, hppl, hppS, lS, mS_first, mS_last, k);
-      hd = (ay_l * (pN - pc) - ay_s * (pc - pS)) / d.p.dydy + (ax_l * (pE - pc) - ax_w * (pc - pW)) / d.p.dxdx;
+      hd = (ay_l * (pN - pc) - ay_s * (pc - pS)) * d.p.rdydy + (ax_l * (pE - pc) - ax_w * (pc - pW)) * d.p.rdxdx;
     }
+    // the interpolation weight hk / (hk + hkp), as the cell kernel forms it (a product with the
+    // reciprocal the sweep needs too); it is the next layer's hkm / (hkm + hk), so it is carried down
+    const double rkp = 1.0 / (hk + hkp);
+    const double thq = hk * rkp;
     double ex;
     if (hpl <= ZERO || hpo <= ZERO) {
       ex = own_pp;
     } else {
-      const double th_k = (k == k1x) ? 0.0 : hkm / (hkm + hk);
+      const double th_k = (k == k1x) ? 0.0 : thq_prev;
       const double th1_k = (k == k1x) ? 0.0 : 1. - th_k;
-      const double th_kp = (k == kmx) ? 0.5 : hk / (hk + hkp);
+      const double th_kp = (k == kmx) ? 0.5 : thq;
       const double th1_kp = (k == kmx) ? 0.5 : 1. - th_kp;
       if (k == k1x) wU = 0.0;
       if (k == kmx) wD = 0.0;
       const double scE = uvE + uc, scW = uvW + uc;
       const double scN = uvN + uc, scS = uvS + uc;
-      double adv = (uE * scE - uW * scW) / d.p.fourdx + (vN * scN - vS * scS) / d.p.fourdy;
+      double adv = (uE * scE - uW * scW) * d.p.rfourdx + (vN * scN - vS * scS) * d.p.rfourdy;
       adv = adv + (wU * (th_k * uc + th1_k * uvU) - wD * (th_kp * uvD + th1_kp * uc)) / 2.;
       if (X) ex = own_pp - twodt1 * (adv * d.p.iadv - cor - hd);
       else ex = own_pp - twodt1 * (adv * d.p.iadv + cor - hd);
@@ -571,7 +578,7 @@ __global__ void __launch_bounds__(NT) k_mom_fused(Dev d, const FaceMeta* __restr
     // ---- forward sweep (k_mom_columns)
     const double upp1 = *sp(s, fz::UPP1);
     const double avop = *sp(s, fz::AVO), avlp = *sp(s, fz::AVL);
-    const double rkp = 1.0 / (hk + hkp), rhkp = 1.0 / hkp;
+    const double rhkp = 1.0 / hkp;
     const double Avk = (k > k1x) ? 0.5 * (avo + avl) : 0.0;
     const double Avkp = (k < kmx) ? 0.5 * (avop + avlp) : 0.0;
     double vdiff = 0.0;
@@ -620,6 +627,7 @@ __global__ void __launch_bounds__(NT) k_mom_fused(Dev d, const FaceMeta* __restr
     rhkm = rhk; rhk = rhkp; rkm = rkp;
     uvU = uc; uc = uvD;
     wprev = wDraw;
+    thq_prev = thq;
     hpl_prev = hpl; hpo_prev = hpo; ro_prev = ro; rl_prev = rl;
   }
   // back substitution, summing the depth totals on the way up
@@ -638,16 +646,18 @@ __global__ void __launch_bounds__(NT) k_mom_fused(Dev d, const FaceMeta* __restr
   else { d.s.eagy[l - 1] = sg; d.s.eary[l - 1] = sr; }
 }
 
-template <int IEQ, int NT, int RD>
+// MINB: resident blocks per SM the register budget is sized for (the ring's shared memory allows
+// 7 blocks of 64 threads, 3 of 128, 1 of 256)
+template <int IEQ, int NT, int RD, int MINB>
 void launch_fused(const Dev& d, const FaceMeta* cols, int ncols, cudaStream_t st) {
-  k_mom_fused<IEQ, NT, RD><<<(ncols + NT - 1) / NT, NT, fused_smem<NT, RD>(), st>>>(d, cols, ncols);
+  k_mom_fused<IEQ, NT, RD, MINB><<<(ncols + NT - 1) / NT, NT, fused_smem<NT, RD>(), st>>>(d, cols, ncols);
 }
 
-template <int NT, int RD>
+template <int NT, int RD, int MINB>
 int fused_attr() {
   const int b = fused_smem<NT, RD>();
-  if (cudaFuncSetAttribute(k_mom_fused<1, NT, RD>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess ||
-      cudaFuncSetAttribute(k_mom_fused<2, NT, RD>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess)
+  if (cudaFuncSetAttribute(k_mom_fused<1, NT, RD, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess ||
+      cudaFuncSetAttribute(k_mom_fused<2, NT, RD, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) != cudaSuccess)
     return -1;
   return 0;
 }
@@ -656,7 +666,7 @@ int fused_attr() {
 
 int momentum_init(int km1) {
   (void)km1;   // the fused kernel's ring is sized by its threads, not by the column depth
-  if (fused_attr<64, 3>() || fused_attr<128, 2>() || fused_attr<256, 2>()) return -1;
+  if (fused_attr<64, 2, 7>() || fused_attr<128, 2, 3>() || fused_attr<256, 2, 1>()) return -1;
   return 0;
 }
 
@@ -665,9 +675,9 @@ void launch_dir(const Dev& d, const FaceMeta* cols, int ncols, const Tune& tu, c
                 int nobc) {
   if (tu.mom_cl == 1 && nobc == 0) {   // one pass per column (open boundaries need the split kernels)
     switch (tu.mom_nt) {
-      case 64: launch_fused<IEQ, 64, 3>(d, cols, ncols, st); break;
-      case 256: launch_fused<IEQ, 256, 2>(d, cols, ncols, st); break;
-      default: launch_fused<IEQ, 128, 2>(d, cols, ncols, st); break;
+      case 64: launch_fused<IEQ, 64, 2, 7>(d, cols, ncols, st); break;
+      case 256: launch_fused<IEQ, 256, 2, 1>(d, cols, ncols, st); break;
+      default: launch_fused<IEQ, 128, 2, 3>(d, cols, ncols, st); break;
     }
     return;
   }

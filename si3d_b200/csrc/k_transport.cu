@@ -210,7 +210,9 @@ __global__ void k_cont2(Dev d) {
 // persistent Bth2/Bth4/Bth3 fields.
 // Every value a layer may need is loaded before any test (all addresses are valid: neighbours are
 // real columns or the dry column lm1, and layer k - 2 is clamped to 1), so a layer costs one memory
-// round trip; the tests then only select among loaded values, in the reference's arithmetic.
+// round trip; the tests then only select among loaded values, in the reference's arithmetic (with
+// products by the reciprocals of dx and dy where the reference divides by them, here and in the
+// right-hand side below).
 template <int CLN>
 __global__ void __launch_bounds__(32 * CLN) k_exsal_flux(Dev d, const double* __restrict__ sp) {
   const int l = blockIdx.x * 32 + threadIdx.x + 1;
@@ -252,7 +254,7 @@ __global__ void __launch_bounds__(32 * CLN) k_exsal_flux(Dev d, const double* __
       const double s1 = (hW <= ZERO) ? s2 : sW;
       const double s4 = (hEE <= ZERO) ? s3 : sEE;
       const double C_f = superbee(s1, s2, s3, s4, vel, 0.0);
-      B2[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / d.p.dx * C_f) * (s3 - s2) / 2.;
+      B2[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 * d.p.rdx * C_f) * (s3 - s2) / 2.;
     } else B2[ik] = 0.0;
     // NS
     if (hv > ZERO) {
@@ -261,7 +263,7 @@ __global__ void __launch_bounds__(32 * CLN) k_exsal_flux(Dev d, const double* __
       const double s1 = (hS <= ZERO) ? s2 : sS;
       const double s4 = (hNN <= ZERO) ? s3 : sNN;
       const double C_f = superbee(s1, s2, s3, s4, vel, 0.0);
-      B4[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 / d.p.dy * C_f) * (s3 - s2) / 2.;
+      B4[ik] = vel / 2. * (s3 + s2) - ((1. - C_f) * fabs(vel) + vel * vel * twodt1 * d.p.rdy * C_f) * (s3 - s2) / 2.;
     } else B4[ik] = 0.0;
     // UD (hp(1, l) is never positive, so k-2 >= 1 whenever this branch is taken)
     if (hpu > ZERO) {
@@ -313,14 +315,14 @@ __global__ void __launch_bounds__(32 * CLN) k_exsal_rhs(Dev d) {
       sE = sp[ik + dE]; sW = sp[ik + dW]; sN = sp[ik + dN]; sS = sp[ik + dS];
       axl = hupp[ik]; axW = hupp[ik + dW]; ayl = hvpp[ik]; ayS = hvpp[ik + dS];
     }
-    double v = hc * spc / twodt1 - (b2 - b2W) / d.p.dx - (b4 - b4S) / d.p.dy - (b3 - b3D);
+    double v = hc * spc / twodt1 - (b2 - b2W) * d.p.rdx - (b4 - b4S) * d.p.rdy - (b3 - b3D);
     if (ihd) {
       const bool inl = k >= k1 && k <= kms;
       const double bxl = inl ? d.p.Ax0 * axl : 0.0;
       const double bxW = (lW != lm1 && k >= k1 && k <= kmW) ? d.p.Ax0 * axW : 0.0;
       const double byl = inl ? d.p.Ay0 * ayl : 0.0;
       const double byS = (lS != lm1 && k >= k1 && k <= kmS) ? d.p.Ay0 * ayS : 0.0;
-      const double hd = (bxl * (sE - spc) - bxW * (spc - sW)) / d.p.dxdx + (byl * (sN - spc) - byS * (spc - sS)) / d.p.dydy;
+      const double hd = (bxl * (sE - spc) - bxW * (spc - sW)) * d.p.rdxdx + (byl * (sN - spc) - byS * (spc - sS)) * d.p.rdydy;
       v = v + hd;
     }
     sal[ik] = v + hs;

@@ -1159,6 +1159,8 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
   p.gdtdx = G_GRAV * p.dtdx; p.gdtdy = G_GRAV * p.dtdy; p.gdt2dx2 = p.gdtdx * p.dtdx; p.gdt2dy2 = p.gdtdy * p.dtdy;
   p.twodx = 2. * p.dx; p.twody = 2. * p.dy; p.fourdx = 2. * p.twodx; p.fourdy = 2. * p.twody;
   p.dxdx = p.dx * p.dx; p.dydy = p.dy * p.dy;
+  p.rfourdx = 1.0 / p.fourdx; p.rfourdy = 1.0 / p.fourdy; p.rdxdx = 1.0 / p.dxdx; p.rdydy = 1.0 / p.dydy;
+  p.rdx = 1.0 / p.dx; p.rdy = 1.0 / p.dy;
   p.Av0 = prm->Av0; p.Dv0 = prm->Dv0; p.Ax0 = prm->Ax0; p.Ay0 = prm->Ay0; p.f = prm->f; p.theta = prm->theta;
   p.cd = prm->cd; p.cw = prm->cw;
   p.iadv = prm->iadv; p.itrmom = prm->itrmom; p.ihd = prm->ihd; p.ibc = prm->ibc; p.isal = prm->isal;
@@ -1734,25 +1736,25 @@ int si3d_gpu_autotune(int h, int reps, int* choice) {
     for (auto& k : keep) { CK(cudaMemcpy(host_copy.data() + o, k.first, k.second * sizeof(double), cudaMemcpyDeviceToHost)); o += k.second; }
   }
   int rc = 0;
-  auto pick = [&](int which, int* knob, std::initializer_list<int> cands) {
-    int best_v = *knob;
+  // every pair of the two knobs of a stage (the best lane count depends on the block size)
+  auto pick2 = [&](int which, int* cl, int* nt, std::initializer_list<int> cls) {
+    int best_cl = *cl, best_nt = *nt;
     float best_t = 1e30f;
-    for (int v : cands) {
-      if (rc) return;
-      *knob = v;
-      float t = 0;
-      rc = time_stage(c, which, reps, &t);
-      if (!rc && t < best_t) { best_t = t; best_v = v; }
-    }
-    *knob = best_v;
+    for (int a : cls)
+      for (int b : {64, 128, 256}) {
+        if (rc) return;
+        *cl = a;
+        *nt = b;
+        float t = 0;
+        rc = time_stage(c, which, reps, &t);
+        if (!rc && t < best_t) { best_t = t; best_cl = a; best_nt = b; }
+      }
+    *cl = best_cl;
+    *nt = best_nt;
   };
   Tune& tu = c->tune;
-  pick(0, &tu.mom_cl, {1, 2, 4, 8});   // 1: the fused one-pass kernel
-  pick(0, &tu.mom_nt, {64, 128, 256});
-  if (c->prm.isal != 0) {
-    pick(1, &tu.sal_cl, {2, 4, 8});
-    pick(1, &tu.sal_nt, {64, 128, 256});
-  }
+  pick2(0, &tu.mom_cl, &tu.mom_nt, {1, 2, 4, 8});   // lanes 1: the fused one-pass kernel
+  if (c->prm.isal != 0) pick2(1, &tu.sal_cl, &tu.sal_nt, {2, 4, 8});
   // restore the state the timing runs overwrote
   size_t o = 0;
   for (auto& k : keep) {
