@@ -46,29 +46,45 @@ struct FaceCol {
   int l, lE, lW, lN, lS, lO, kmx, k1x, lX2;
 };
 
-// ------------------------------------------------------------------ cell kernel
-template <int IEQ, int CL>
-__global__ void __launch_bounds__(CW * CL, 768 / (CW * CL)) k_mom_cells(Dev d, const FaceMeta* __restrict__ meta, int ncols) {
-  const int t = blockIdx.x * CW + threadIdx.x;
-  if (t >= ncols) return;
+// ------------------------------------------------------------------ cell terms
+// The per-thread description of one face column that the cell terms read.
+struct CellCol {
+  int l, lW, lS, lO, k1x, kmx, mW_first, mW_last, mS_first, mS_last;
+  int dE, dW, dN, dS, dX2, dO;
+};
+
+template <int IEQ>
+__device__ __forceinline__ CellCol cell_col(const Dev& d, const FaceMeta* __restrict__ meta, int t) {
   const bool X = (IEQ == 1);
   const int4 ma = __ldg(&meta[t].a), mb = __ldg(&meta[t].b);
-  const int l = ma.x, lE = ma.y, lW = ma.z, lN = ma.w, lS = mb.x, lX2 = mb.y, kmx = mb.z;
-  const int lO = X ? lE : lN;
+  const int l = ma.x, lE = ma.y, lW = ma.z, lN = ma.w, lS = mb.x, lX2 = mb.y;
+  CellCol C;
+  C.l = l; C.lW = lW; C.lS = lS; C.kmx = mb.z;
+  C.lO = X ? lE : lN;
   const int* k1f = X ? d.s.k1u : d.s.k1v;
-  const int k1x = NB(k1f, l);
-  if (k1x + (int)threadIdx.y > kmx) return;
+  C.k1x = NB(k1f, l);
   // west / south neighbouring faces' diffusion ranges (their first wet layers change per step)
-  const int mW_last = mb.w, mS_last = __ldg(&meta[t].c.x);
-  const int mW_first = mW_last >= 0 ? NB(k1f, lW) : 0;
-  const int mS_first = mS_last >= 0 ? NB(k1f, lS) : 0;
+  C.mW_last = mb.w;
+  C.mS_last = __ldg(&meta[t].c.x);
+  C.mW_first = C.mW_last >= 0 ? NB(k1f, lW) : 0;
+  C.mS_first = C.mS_last >= 0 ? NB(k1f, lS) : 0;
+  C.dE = lE - l; C.dW = lW - l; C.dN = lN - l; C.dS = lS - l; C.dX2 = lX2 - l; C.dO = C.lO - l;
+  return C;
+}
+
+// The explicit term ex(k) (advection, Coriolis, horizontal diffusion) and the baroclinic increment
+// of wet face layer k of column C, and the thickness of layer k + 1 (loaded for the weights anyway).
+template <int IEQ>
+__device__ __forceinline__ void mom_cell(const Dev& d, const CellCol& C, int k, double& ex_out, double& hdrho_out,
+                                         double& hkp_out) {
+  const bool X = (IEQ == 1);
+  const int l = C.l, lO = C.lO, k1x = C.k1x, kmx = C.kmx;
+  const int dE = C.dE, dW = C.dW, dN = C.dN, dS = C.dS, dX2 = C.dX2, dO = C.dO;
   const double* huv = X ? d.f.hup : d.f.hvp;
   const double* huvpp = X ? d.f.hupp : d.f.hvpp;
   const double* uvpp_h = X ? d.f.uhpp : d.f.vhpp;
   const double* uvp = X ? d.f.up : d.f.vp;
   const double* uvpp = X ? d.f.upp : d.f.vpp;
-  double* agA = X ? d.f.agx : d.f.agy;
-  double* arA = X ? d.f.arx : d.f.ary;
   const double twodt1 = d.p.twodt * d.tz;
   const double gdt = X ? d.p.gdtdx : d.p.gdtdy;
   const double* __restrict__ vhp = d.f.vhp;
@@ -76,96 +92,112 @@ __global__ void __launch_bounds__(CW * CL, 768 / (CW * CL)) k_mom_cells(Dev d, c
   const double* __restrict__ wp = d.f.wp;
   const double* __restrict__ hp3 = d.f.hp;
   const int P = d.g.P;
-  const int dE = lE - l, dW = lW - l, dN = lN - l, dS = lS - l, dX2 = lX2 - l, dO = lO - l;
-  for (int k = k1x + threadIdx.y; k <= kmx; k += CL) {
-    const int ik = IX(d, k, l);
-    // every input of the explicit term is loaded before the dry-cell test, so a layer costs one
-    // memory round trip; the arithmetic below is the reference's, term by term
-    const double hk = huv[ik];
-    const double hkm = huv[ik - P];
-    const double hkp = huv[ik + P];
-    const double hpl = hp3[ik], hpo = hp3[ik + dO];
-    double cor, uE, uW, vN, vS, wU, wD;
-    if (X) {
-      const double vE = vhp[ik + dE], vC = vhp[ik], vX = vhp[ik + dX2], vSS = vhp[ik + dS];
-      const double uEE = uhp[ik + dE], uC = uhp[ik], uWW = uhp[ik + dW];
-      cor = 0.25 * d.p.f * (vE + vC + vX + vSS);
-      uE = uEE + uC;
-      uW = uC + uWW;
-      vN = vE + vC;
-      vS = vX + vSS;
-      wU = wp[ik + dE] + wp[ik];
-      wD = wp[ik + P + dE] + wp[ik + P];
-    } else {
-      const double uN = uhp[ik + dN], uC = uhp[ik], uX = uhp[ik + dX2], uWW = uhp[ik + dW];
-      const double vNN = vhp[ik + dN], vC = vhp[ik], vSS = vhp[ik + dS];
-      cor = 0.25 * d.p.f * (uN + uC + uX + uWW);
-      uE = uN + uC;
-      uW = uX + uWW;
-      vN = vNN + vC;
-      vS = vC + vSS;
-      wU = wp[ik + dN] + wp[ik];
-      wD = wp[ik + P + dN] + wp[ik + P];
+  const int ik = IX(d, k, l);
+  // every input of the explicit term is loaded before the dry-cell test, so a layer costs one
+  // memory round trip; the arithmetic below is the reference's, term by term
+  const double hk = huv[ik];
+  const double hkm = huv[ik - P];
+  const double hkp = huv[ik + P];
+  const double hpl = hp3[ik], hpo = hp3[ik + dO];
+  double cor, uE, uW, vN, vS, wU, wD;
+  if (X) {
+    const double vE = vhp[ik + dE], vC = vhp[ik], vX = vhp[ik + dX2], vSS = vhp[ik + dS];
+    const double uEE = uhp[ik + dE], uC = uhp[ik], uWW = uhp[ik + dW];
+    cor = 0.25 * d.p.f * (vE + vC + vX + vSS);
+    uE = uEE + uC;
+    uW = uC + uWW;
+    vN = vE + vC;
+    vS = vX + vSS;
+    wU = wp[ik + dE] + wp[ik];
+    wD = wp[ik + P + dE] + wp[ik + P];
+  } else {
+    const double uN = uhp[ik + dN], uC = uhp[ik], uX = uhp[ik + dX2], uWW = uhp[ik + dW];
+    const double vNN = vhp[ik + dN], vC = vhp[ik], vSS = vhp[ik + dS];
+    cor = 0.25 * d.p.f * (uN + uC + uX + uWW);
+    uE = uN + uC;
+    uW = uX + uWW;
+    vN = vNN + vC;
+    vS = vC + vSS;
+    wU = wp[ik + dN] + wp[ik];
+    wD = wp[ik + P + dN] + wp[ik + P];
+  }
+  const double uc = uvp[ik];
+  const double uvE = uvp[ik + dE], uvW = uvp[ik + dW], uvN = uvp[ik + dN], uvS = uvp[ik + dS];
+  const double uvU = uvp[ik - P], uvD = uvp[ik + P];
+  const double own_pp = uvpp_h[ik];
+  double hd = 0.0;
+  if (d.p.ihd == 1) {
+    const double hppl = huvpp[ik], hppE = huvpp[ik + dE], hppN = huvpp[ik + dN];
+    const double hppW = huvpp[ik + dW], hppS = huvpp[ik + dS];
+    const double pc = uvpp[ik], pN = uvpp[ik + dN], pS = uvpp[ik + dS], pE = uvpp[ik + dE], pW = uvpp[ik + dW];
+    const double ax_l = d.p.Ax0 * fmin(hppE, hppl);
+    const double ay_l = d.p.Ay0 * fmin(hppN, hppl);
+    const double ax_w = face_coef(d, d.p.Ax0, hppl, hppW, C.lW, C.mW_first, C.mW_last, k);
+    const double ay_s = face_coef(d, d.p.Ay0, hppl, hppS, C.lS, C.mS_first, C.mS_last, k);
+    hd = (ay_l * (pN - pc) - ay_s * (pc - pS)) * d.p.rdydy + (ax_l * (pE - pc) - ax_w * (pc - pW)) * d.p.rdxdx;
+  }
+  double ex;
+  if (hpl <= ZERO || hpo <= ZERO) {
+    ex = own_pp;
+  } else {
+    const double th_k = (k == k1x) ? 0.0 : hkm * (1.0 / (hkm + hk));
+    const double th1_k = (k == k1x) ? 0.0 : 1. - th_k;
+    const double th_kp = (k == kmx) ? 0.5 : hk * (1.0 / (hk + hkp));
+    const double th1_kp = (k == kmx) ? 0.5 : 1. - th_kp;
+    if (k == k1x) wU = 0.0;
+    if (k == kmx) wD = 0.0;
+    const double scE = uvE + uc, scW = uvW + uc;
+    const double scN = uvN + uc, scS = uvS + uc;
+    double adv = (uE * scE - uW * scW) * d.p.rfourdx + (vN * scN - vS * scS) * d.p.rfourdy;
+    adv = adv + (wU * (th_k * uc + th1_k * uvU) - wD * (th_kp * uvD + th1_kp * uc)) / 2.;
+    if (X) ex = own_pp - twodt1 * (adv * d.p.iadv - cor - hd);
+    else ex = own_pp - twodt1 * (adv * d.p.iadv + cor - hd);
+  }
+  // ---- baroclinic increment (:1283-1301 / :1475-1491), bottom layer via bclnc_km
+  double hdrho = 0;
+  if (d.p.ibc != 0) {
+    hdrho = gdt * hk * (d.f.rhop[IX(d, k, lO)] - d.f.rhop[ik]);
+    if (k == kmx && kmx > k1x) {
+      const int kb = kmx;
+      const double eps = 2.220446049250313e-16;
+      const double hplus = hk + eps, hminus = hk - eps;
+      const double* rh = d.f.rhop;
+      const double* hp = d.f.hp;
+      bool co, cw;
+      double rho_o, rho_w;
+      if (hp[IX(d, kb, lO)] > hplus || hp[IX(d, kb, lO)] < hminus) {
+        co = true;
+        const double dz1 = 0.5 * (hp[IX(d, kb - 1, lO)] + hp[IX(d, kb, lO)]);
+        const double dz2 = 0.5 * (hp[IX(d, kb - 1, lO)] + hk);
+        rho_o = rh[IX(d, kb - 1, lO)] + (dz2 / dz1) * (rh[IX(d, kb, lO)] - rh[IX(d, kb - 1, lO)]);
+      } else { co = false; rho_o = rh[IX(d, kb, lO)]; }
+      if (hp[IX(d, kb, l)] > hplus || hp[IX(d, kb, l)] < hminus) {
+        cw = true;
+        const double dz1 = 0.5 * (hp[IX(d, kb - 1, l)] + hp[IX(d, kb, l)]);
+        const double dz2 = 0.5 * (hp[IX(d, kb - 1, l)] + hk);
+        rho_w = rh[IX(d, kb - 1, l)] + (dz2 / dz1) * (rh[IX(d, kb, l)] - rh[IX(d, kb - 1, l)]);
+      } else { cw = false; rho_w = rh[IX(d, kb, l)]; }
+      if (co || cw) hdrho = gdt * hk * (rho_o - rho_w);
     }
-    const double uc = uvp[ik];
-    const double uvE = uvp[ik + dE], uvW = uvp[ik + dW], uvN = uvp[ik + dN], uvS = uvp[ik + dS];
-    const double uvU = uvp[ik - P], uvD = uvp[ik + P];
-    const double own_pp = uvpp_h[ik];
-    double hd = 0.0;
-    if (d.p.ihd == 1) {
-      const double hppl = huvpp[ik], hppE = huvpp[ik + dE], hppN = huvpp[ik + dN];
-      const double hppW = huvpp[ik + dW], hppS = huvpp[ik + dS];
-      const double pc = uvpp[ik], pN = uvpp[ik + dN], pS = uvpp[ik + dS], pE = uvpp[ik + dE], pW = uvpp[ik + dW];
-      const double ax_l = d.p.Ax0 * fmin(hppE, hppl);
-      const double ay_l = d.p.Ay0 * fmin(hppN, hppl);
-      const double ax_w = face_coef(d, d.p.Ax0, hppl, hppW, lW, mW_first, mW_last, k);
-      const double ay_s = face_coef(d, d.p.Ay0, hppl, hppS, lS, mS_first, mS_last, k);
-      hd = (ay_l * (pN - pc) - ay_s * (pc - pS)) * d.p.rdydy + (ax_l * (pE - pc) - ax_w * (pc - pW)) * d.p.rdxdx;
-    }
-    double ex;
-    if (hpl <= ZERO || hpo <= ZERO) {
-      ex = own_pp;
-    } else {
-      const double th_k = (k == k1x) ? 0.0 : hkm * (1.0 / (hkm + hk));
-      const double th1_k = (k == k1x) ? 0.0 : 1. - th_k;
-      const double th_kp = (k == kmx) ? 0.5 : hk * (1.0 / (hk + hkp));
-      const double th1_kp = (k == kmx) ? 0.5 : 1. - th_kp;
-      if (k == k1x) wU = 0.0;
-      if (k == kmx) wD = 0.0;
-      const double scE = uvE + uc, scW = uvW + uc;
-      const double scN = uvN + uc, scS = uvS + uc;
-      double adv = (uE * scE - uW * scW) * d.p.rfourdx + (vN * scN - vS * scS) * d.p.rfourdy;
-      adv = adv + (wU * (th_k * uc + th1_k * uvU) - wD * (th_kp * uvD + th1_kp * uc)) / 2.;
-      if (X) ex = own_pp - twodt1 * (adv * d.p.iadv - cor - hd);
-      else ex = own_pp - twodt1 * (adv * d.p.iadv + cor - hd);
-    }
-    // ---- baroclinic increment (:1283-1301 / :1475-1491), bottom layer via bclnc_km
-    double hdrho = 0;
-    if (d.p.ibc != 0) {
-      hdrho = gdt * hk * (d.f.rhop[IX(d, k, lO)] - d.f.rhop[ik]);
-      if (k == kmx && kmx > k1x) {
-        const int kb = kmx;
-        const double eps = 2.220446049250313e-16;
-        const double hplus = hk + eps, hminus = hk - eps;
-        const double* rh = d.f.rhop;
-        const double* hp = d.f.hp;
-        bool co, cw;
-        double rho_o, rho_w;
-        if (hp[IX(d, kb, lO)] > hplus || hp[IX(d, kb, lO)] < hminus) {
-          co = true;
-          const double dz1 = 0.5 * (hp[IX(d, kb - 1, lO)] + hp[IX(d, kb, lO)]);
-          const double dz2 = 0.5 * (hp[IX(d, kb - 1, lO)] + hk);
-          rho_o = rh[IX(d, kb - 1, lO)] + (dz2 / dz1) * (rh[IX(d, kb, lO)] - rh[IX(d, kb - 1, lO)]);
-        } else { co = false; rho_o = rh[IX(d, kb, lO)]; }
-        if (hp[IX(d, kb, l)] > hplus || hp[IX(d, kb, l)] < hminus) {
-          cw = true;
-          const double dz1 = 0.5 * (hp[IX(d, kb - 1, l)] + hp[IX(d, kb, l)]);
-          const double dz2 = 0.5 * (hp[IX(d, kb - 1, l)] + hk);
-          rho_w = rh[IX(d, kb - 1, l)] + (dz2 / dz1) * (rh[IX(d, kb, l)] - rh[IX(d, kb - 1, l)]);
-        } else { cw = false; rho_w = rh[IX(d, kb, l)]; }
-        if (co || cw) hdrho = gdt * hk * (rho_o - rho_w);
-      }
-    }
+  }
+  ex_out = ex;
+  hdrho_out = hdrho;
+  hkp_out = hkp;
+}
+
+// ------------------------------------------------------------------ cell kernel
+template <int IEQ, int CL>
+__global__ void __launch_bounds__(CW * CL, 768 / (CW * CL)) k_mom_cells(Dev d, const FaceMeta* __restrict__ meta, int ncols) {
+  const int t = blockIdx.x * CW + threadIdx.x;
+  if (t >= ncols) return;
+  const CellCol C = cell_col<IEQ>(d, meta, t);
+  if (C.k1x + (int)threadIdx.y > C.kmx) return;
+  double* agA = (IEQ == 1) ? d.f.agx : d.f.agy;
+  double* arA = (IEQ == 1) ? d.f.arx : d.f.ary;
+  for (int k = C.k1x + threadIdx.y; k <= C.kmx; k += CL) {
+    double ex, hdrho, hkp;
+    mom_cell<IEQ>(d, C, k, ex, hdrho, hkp);
+    const int ik = IX(d, k, C.l);
     agA[ik] = ex;
     arA[ik] = hdrho;
   }

@@ -32,7 +32,13 @@ def main(argv=None) -> int:
                     help="1: a synthetic workload with the Mellor-Yamada 2.5 closure")
     ap.add_argument("--autotune", action="store_true",
                     help="pick the launch shapes of the column stages on the live state first")
+    ap.add_argument("--tune", default="",
+                    help="apply a launch-shape choice instead: momentum lanes (1 = the fused kernel, 2, 4, 8), "
+                         "momentum threads per block, scalar lanes, scalar threads (e.g. 1,128,2,64)")
     args = ap.parse_args(argv)
+    tune = tuple(int(v) for v in args.tune.split(",")) if args.tune else None
+    if tune is not None and len(tune) != 4:
+        ap.error("--tune takes four comma-separated integers")
 
     from . import build, native, synth
     from .model import GpuRun
@@ -47,6 +53,8 @@ def main(argv=None) -> int:
     prec = {"fp64": native.SI3D_FP64, "mixed": native.SI3D_MIXED_IR, "mg": native.SI3D_MIXED_MG}[args.precision]
     run = GpuRun(run_dir, device=args.device, pcg_itmax=args.itmax, precision=prec, autotune=args.autotune)
     try:
+        if tune is not None:
+            run.set_tune(tune)
         for _ in range(args.steps):
             (s,) = run.run(1)
             print(json.dumps({"step": len(run.stats), "iters": [s.iters[i] for i in range(min(s.nsolves, 24))],
