@@ -58,11 +58,15 @@ __device__ __forceinline__ void all_partials(const double* part, int n, int stri
   bsum<NV, BS>(v, sh);
 }
 
-// Per-block state of the grid barrier, in shared memory: the outcome of the last wait and the
-// number of barriers this block has passed.  Zero `epoch` (thread 0) before the first barrier.
+// Per-block state of the grid barrier, in shared memory: the outcome of the last wait, the
+// number of barriers this block has passed, and, read at the first barrier of the launch, the
+// arrivals a barrier waits for and the poll limit.  Zero `epoch` (thread 0) before the first
+// barrier.
 struct BarSt {
   int ok;
   unsigned int epoch;
+  unsigned int expect;
+  long long limit;
 };
 
 __device__ __forceinline__ unsigned long long ld_acquire64(const unsigned long long* p) {
@@ -77,19 +81,23 @@ __device__ __forceinline__ void red_release_add(unsigned long long* p, unsigned 
 
 // Grid barrier on a monotonic arrival counter: barrier e (1, 2, ...) of the launch is passed once
 // the counter reaches e * (blocks + absent).  An arrival is one release-add (no round trip, no
-// reset); the wait polls with acquire loads.  Bounded: returns false (in every thread of the block)
-// once this block gave up or any block has.
+// reset; the release orders the block's writes, which __syncthreads ordered before thread 0's
+// arrival, ahead of it); the wait polls with acquire loads, which order the block's later reads
+// after the other blocks' arrivals.  `absent` and `limit` (zero in every solve; a test sets them
+// to make the wait run out) are read once, at the first barrier, so a barrier costs one release
+// and the polls.  Bounded: returns false (in every thread of the block) once this block gave up
+// or any block has.
 __device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, BarSt* st) {
   __syncthreads();
   if (threadIdx.x == 0) {
+    if (st->epoch == 0) {
+      st->expect = gridDim.x + __ldcg(&bar->absent);
+      const unsigned long long lim = __ldcg(&bar->limit);
+      st->limit = lim ? (long long)lim : kSpinLimit;
+    }
     int ok = 1;
-    // zero in every solve; a test sets them to make the wait run out
-    const unsigned int absent = __ldcg(&bar->absent);
-    const unsigned long long lim = __ldcg(&bar->limit);
-    const long long limit = lim ? (long long)lim : kSpinLimit;
-    const unsigned int e = ++st->epoch;
-    const unsigned long long target = (unsigned long long)e * (gridDim.x + absent);
-    __threadfence();
+    const unsigned long long target = (unsigned long long)(++st->epoch) * st->expect;
+    const long long limit = st->limit;
     red_release_add(&bar->count, 1ull);
     long long spins = 0;
     while (ld_acquire64(&bar->count) < target) {
@@ -98,8 +106,8 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, BarSt* s
     if (!ok && atomicExch(&bar->abort, 1u) == 0u) {
       sc->ier = SI3D_ETIMEOUT;
       sc->done = 1;
+      __threadfence();
     }
-    __threadfence();
     st->ok = ok;
   }
   __syncthreads();
