@@ -19,6 +19,11 @@
 //           correction of their aggregate; red half-sweep; at level 0 both add to (r, z)
 //   PQ      beta, p = z + beta p and q = A p (neighbours' p formed on the fly), (p, q)
 // With L levels that is 4 L - 1 barriers an inner iteration.
+//
+// Every level pass walks groups of four consecutive cells of a row (one float4 of each array,
+// 16-byte aligned by the image layout, mg.h): a thread keeps several groups' loads in flight with a
+// quarter of the load instructions and index arithmetic of a cell-by-cell pass.  Frame and land
+// cells inside a group hold zero in every array and compute zero, so no cell is tested.
 #include <algorithm>
 
 #include "../../include/si3d_gpu.h"
@@ -38,10 +43,7 @@ FastDiv fast_div(int d) {
   return f;
 }
 
-size_t mg_level_elems(int rows, int cols) {
-  const int pitch = ((cols + 3 + 31) / 32) * 32;
-  return (size_t)(rows + 3) * (size_t)pitch;
-}
+size_t mg_level_elems(int rows, int cols) { return (size_t)(rows + 3) * (size_t)mg_pitch(cols); }
 
 namespace {
 
@@ -49,7 +51,10 @@ using namespace coop;
 
 constexpr int PB = 256;               // threads per block of the setup kernels
 constexpr float kFaceScale = 0.5f;    // coarse faces: half the sum of the crossing fine faces
-constexpr int UN = 4;                 // cells a thread keeps in flight in the level loops
+constexpr int UN = 4;                 // cells a thread keeps in flight in the cell-by-cell FP64 passes
+constexpr int CO = kMgColOff;
+constexpr int UG = 2;                 // groups of four cells a thread keeps in flight in the level-0 CG passes
+constexpr int UH = 2;                 // groups in flight in the half-sweeps
 constexpr int MQ = 512;               // threads per block of the cooperative solve (one block per SM)
 
 __device__ __forceinline__ int fdiv(const FastDiv& f, int x) {
@@ -108,13 +113,13 @@ __global__ void k_mg_coarsen(MgLevel F, MgLevel G) {
   if (t >= G.rows * G.cols) return;
   const int R = t / G.cols, Cc = t - R * G.cols;
   const int fp = F.pitch;
-  const int o00 = (2 * R + 1) * fp + 2 * Cc + 1, o01 = o00 + 1, o10 = o00 + fp, o11 = o10 + 1;
+  const int o00 = (2 * R + 1) * fp + 2 * Cc + CO, o01 = o00 + 1, o10 = o00 + fp, o11 = o10 + 1;
   const float mass = (F.mass[o00] + F.mass[o01]) + (F.mass[o10] + F.mass[o11]);
   const float fc = kFaceScale * (F.fc[o01] + F.fc[o11]);
   const float fr = kFaceScale * (F.fr[o10] + F.fr[o11]);
   const float fcW = kFaceScale * (F.fc[o00 - 1] + F.fc[o10 - 1]);
   const float frS = kFaceScale * (F.fr[o00 - fp] + F.fr[o01 - fp]);
-  const int O = (R + 1) * G.pitch + Cc + 1;
+  const int O = (R + 1) * G.pitch + Cc + CO;
   G.fc[O] = fc;
   G.fr[O] = fr;
   G.mass[O] = mass;
@@ -123,83 +128,153 @@ __global__ void k_mg_coarsen(MgLevel F, MgLevel G) {
 }
 
 // ---------------------------------------------------------------- V-cycle pieces
+__device__ __forceinline__ float4 ld4(const float* p, int o) { return *reinterpret_cast<const float4*>(p + o); }
+__device__ __forceinline__ float2 ld2(const float* p, int o) { return *reinterpret_cast<const float2*>(p + o); }
+__device__ __forceinline__ void st4(float* p, int o, float4 v) { *reinterpret_cast<float4*>(p + o) = v; }
+__device__ __forceinline__ void st2(float* p, int o, float2 v) { *reinterpret_cast<float2*>(p + o) = v; }
+__device__ __forceinline__ float sel(int j, float a0, float a1) { return j ? a1 : a0; }
+
+// Group t of a level: row r, group q, buffer offset of its first cell (column 4q).
+__device__ __forceinline__ int group_at(const MgLevel& L, int t, int& r, int& q) {
+  r = fdiv(L.div_q, t);
+  q = t - r * L.nq;
+  return (r + 1) * L.pitch + 4 * q + CO;
+}
+
 // Gauss-Seidel half-sweep over the cells of colour `col` ((r + c) & 1 == col) of level L:
 // z = dinv (b + sum of face * neighbour z).  PROLONG: each neighbour's value is its z plus the
 // correction of its aggregate in the coarser level G.  DOT: returns this thread's sum of b * z.
-template <bool PROLONG, bool DOT>
+// A group of four cells of row r holds two cells of the colour, at j0 = (r + col) & 1 and j0 + 2.
+template <bool PROLONG, bool DOT, int U>
 __device__ __forceinline__ double half_sweep(const MgLevel& L, const MgLevel& G, int col, int g0, int stride) {
   double rz = 0.0;
-  const int n = L.rows * L.hw, pt = L.pitch;
-  for (int h0 = g0; h0 < n; h0 += UN * stride) {
-    int o[UN];
-    bool ok[UN];
-    float s[UN], dv[UN], bb[UN];
+  const int n = L.rows * L.nq, pt = L.pitch;
+  for (int t0 = g0; t0 < n; t0 += U * stride) {
+    int x[U], jc[U];
+    bool ok[U];
+    float zv[U][2], bq[U][2];
 #pragma unroll
-    for (int k = 0; k < UN; ++k) {
-      const int h = h0 + k * stride;
-      int r = fdiv(L.div_hw, h);
-      int c = 2 * (h - r * L.hw) + ((r + col) & 1);
-      ok[k] = (h < n) && (c < L.cols);
-      if (!ok[k]) { r = 0; c = 0; }   // an interior cell, loaded and dropped
-      o[k] = (r + 1) * pt + c + 1;
-      float zw = L.z[o[k] - 1], ze = L.z[o[k] + 1], zs = L.z[o[k] - pt], zn = L.z[o[k] + pt];
+    for (int k = 0; k < U; ++k) {
+      const int t = t0 + k * stride;
+      ok[k] = t < n;
+      int r = 0, q = 0;
+      x[k] = ok[k] ? group_at(L, t, r, q) : pt + CO;   // an interior group, loaded and dropped
+      const int j = (r + col) & 1;
+      jc[k] = j;
+      const int o = x[k];
+      const float4 zm = ld4(L.z, o), zs = ld4(L.z, o - pt), zn = ld4(L.z, o + pt);
+      const float zw0 = L.z[o - 1], ze3 = L.z[o + 4];
+      const float4 bb = ld4(L.b, o), dv = ld4(L.dinv, o), fc = ld4(L.fc, o), fr = ld4(L.fr, o), fs = ld4(L.fr, o - pt);
+      const float fw0 = L.fc[o - 1];
+      // the two cells of the colour: column jj = j (m = 0) and j + 2 (m = 1)
+      // row values at columns -1 .. 4 of the group
+      const float zr[6] = {zw0, zm.x, zm.y, zm.z, zm.w, ze3};
+      const float fcr[5] = {fw0, fc.x, fc.y, fc.z, fc.w};   // fcr[c + 1] = face from column c to c + 1
+      const float zsv[4] = {zs.x, zs.y, zs.z, zs.w}, znv[4] = {zn.x, zn.y, zn.z, zn.w};
+      const float bv[4] = {bb.x, bb.y, bb.z, bb.w}, dvv[4] = {dv.x, dv.y, dv.z, dv.w};
+      const float frn[4] = {fr.x, fr.y, fr.z, fr.w}, frs[4] = {fs.x, fs.y, fs.z, fs.w};
+      float gW[2] = {0.f, 0.f}, gE[2] = {0.f, 0.f}, gS[2] = {0.f, 0.f}, gN[2] = {0.f, 0.f};
       if (PROLONG) {
+        // aggregates of the neighbours: row r >> 1 at coarse columns 2q - 1 .. 2q + 2, rows
+        // (r - 1) >> 1 and (r + 1) >> 1 at 2q, 2q + 1
         const int gp = G.pitch;
-        const int row = ((r >> 1) + 1) * gp;
-        zw += G.z[row + ((c - 1) >> 1) + 1];
-        ze += G.z[row + ((c + 1) >> 1) + 1];
-        zs += G.z[(((r - 1) >> 1) + 1) * gp + (c >> 1) + 1];
-        zn += G.z[(((r + 1) >> 1) + 1) * gp + (c >> 1) + 1];
+        const int gr = ((r >> 1) + 1) * gp + 2 * q + CO;
+        const float2 gm = ld2(G.z, gr);
+        const float gc[4] = {G.z[gr - 1], gm.x, gm.y, G.z[gr + 2]};   // coarse columns 2q - 1 .. 2q + 2
+        const float2 gs = ld2(G.z, (((r - 1) >> 1) + 1) * gp + 2 * q + CO);
+        const float2 gn = ld2(G.z, (((r + 1) >> 1) + 1) * gp + 2 * q + CO);
+        // cell jj = 2m + j: west neighbour's aggregate gc[((jj - 1) >> 1) + 1], east gc[((jj + 1) >> 1) + 1],
+        // south / north (jj >> 1) = m
+#pragma unroll
+        for (int m = 0; m < 2; ++m) {
+          gW[m] = sel(j, gc[m], gc[m + 1]);          // jj = 2m: column m ; jj = 2m + 1: column m + 1
+          gE[m] = sel(j, gc[m + 1], gc[m + 2]);
+          gS[m] = m ? gs.y : gs.x;
+          gN[m] = m ? gn.y : gn.x;
+        }
       }
-      bb[k] = L.b[o[k]];
-      s[k] = bb[k] + L.fc[o[k]] * ze + L.fc[o[k] - 1] * zw + L.fr[o[k]] * zn + L.fr[o[k] - pt] * zs;
-      dv[k] = L.dinv[o[k]];
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        // column jj = 2m + j, selected between the even (j = 0) and odd (j = 1) candidates
+        float zw = sel(j, zr[2 * m], zr[2 * m + 1]);
+        float ze = sel(j, zr[2 * m + 2], zr[2 * m + 3]);
+        float zs1 = sel(j, zsv[2 * m], zsv[2 * m + 1]);
+        float zn1 = sel(j, znv[2 * m], znv[2 * m + 1]);
+        if (PROLONG) { zw += gW[m]; ze += gE[m]; zs1 += gS[m]; zn1 += gN[m]; }
+        const float b1 = sel(j, bv[2 * m], bv[2 * m + 1]);
+        const float fce = sel(j, fcr[2 * m + 1], fcr[2 * m + 2]), fcw = sel(j, fcr[2 * m], fcr[2 * m + 1]);
+        const float fn = sel(j, frn[2 * m], frn[2 * m + 1]), fsv = sel(j, frs[2 * m], frs[2 * m + 1]);
+        const float s1 = b1 + fce * ze + fcw * zw + fn * zn1 + fsv * zs1;
+        zv[k][m] = sel(j, dvv[2 * m], dvv[2 * m + 1]) * s1;
+        bq[k][m] = b1;
+      }
     }
 #pragma unroll
-    for (int k = 0; k < UN; ++k) {
+    for (int k = 0; k < U; ++k) {
       if (!ok[k]) continue;
-      const float z = dv[k] * s[k];
-      L.z[o[k]] = z;
-      if (DOT) rz += (double)bb[k] * (double)z;
+#pragma unroll
+      for (int m = 0; m < 2; ++m) {
+        L.z[x[k] + 2 * m + jc[k]] = zv[k][m];
+        if (DOT) rz += (double)bq[k][m] * (double)zv[k][m];
+      }
     }
   }
   return rz;
 }
 
-// b of level G = the residual b - A z of level F summed over each 2 x 2 aggregate; the red cells of
-// G then take their first half-sweep from zero, z = dinv b.
+// b of level G = the residual b - A z of level F summed over each 2 x 2 aggregate; z of G = dinv b,
+// which is the first half-sweep from zero for its red cells (its black cells are swept before
+// they are read).  An item is one group of four columns in the two fine rows of a coarse row: the
+// coarse pair 2q, 2q + 1.
 __device__ __forceinline__ void restrict_residual(const MgLevel& F, const MgLevel& G, int g0, int stride) {
-  const int n = G.rows * G.cols, fp = F.pitch;
-  for (int t0 = g0; t0 < n; t0 += 2 * stride) {
-    float acc[2];
-    int O[2];
-    bool ok[2], red[2];
+  const int n = G.rows * F.nq, fp = F.pitch;
+  for (int t = g0; t < n; t += stride) {
+    const int R = fdiv(F.div_q, t);
+    const int q = t - R * F.nq;
+    const int x0 = (2 * R + 1) * fp + 4 * q + CO, x1 = x0 + fp;
+    const float4 zA = ld4(F.z, x0 - fp), z0 = ld4(F.z, x0), z1 = ld4(F.z, x1), zB = ld4(F.z, x1 + fp);
+    const float z0w = F.z[x0 - 1], z0e = F.z[x0 + 4], z1w = F.z[x1 - 1], z1e = F.z[x1 + 4];
+    const float4 b0 = ld4(F.b, x0), b1 = ld4(F.b, x1), m0 = ld4(F.mass, x0), m1 = ld4(F.mass, x1);
+    const float4 c0 = ld4(F.fc, x0), c1 = ld4(F.fc, x1);
+    const float c0w = F.fc[x0 - 1], c1w = F.fc[x1 - 1];
+    const float4 rA = ld4(F.fr, x0 - fp), r0 = ld4(F.fr, x0), r1 = ld4(F.fr, x1);
+    const int O = (R + 1) * G.pitch + 2 * q + CO;
+    const float2 dg = ld2(G.dinv, O);
+    float res[2][4];
+    {
+      const float zr[2][6] = {{z0w, z0.x, z0.y, z0.z, z0.w, z0e}, {z1w, z1.x, z1.y, z1.z, z1.w, z1e}};
+      const float zsv[2][4] = {{zA.x, zA.y, zA.z, zA.w}, {z0.x, z0.y, z0.z, z0.w}};
+      const float znv[2][4] = {{z1.x, z1.y, z1.z, z1.w}, {zB.x, zB.y, zB.z, zB.w}};
+      const float bv[2][4] = {{b0.x, b0.y, b0.z, b0.w}, {b1.x, b1.y, b1.z, b1.w}};
+      const float mv[2][4] = {{m0.x, m0.y, m0.z, m0.w}, {m1.x, m1.y, m1.z, m1.w}};
+      const float fcr[2][5] = {{c0w, c0.x, c0.y, c0.z, c0.w}, {c1w, c1.x, c1.y, c1.z, c1.w}};
+      const float frs[2][4] = {{rA.x, rA.y, rA.z, rA.w}, {r0.x, r0.y, r0.z, r0.w}};
+      const float frn[2][4] = {{r0.x, r0.y, r0.z, r0.w}, {r1.x, r1.y, r1.z, r1.w}};
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      const int t = t0 + k * stride;
-      ok[k] = t < n;
-      int R = ok[k] ? fdiv(G.div_cols, t) : 0;
-      int Cc = ok[k] ? t - R * G.cols : 0;
-      O[k] = (R + 1) * G.pitch + Cc + 1;
-      red[k] = ((R + Cc) & 1) == 0;
-      const int o00 = (2 * R + 1) * fp + 2 * Cc + 1;
-      float a = 0.f;
+      for (int h = 0; h < 2; ++h) {
 #pragma unroll
-      for (int ch = 0; ch < 4; ++ch) {
-        const int o = o00 + (ch >> 1) * fp + (ch & 1);
-        const float fcw = F.fc[o - 1], fce = F.fc[o], frs = F.fr[o - fp], frn = F.fr[o];
-        const float diag = F.mass[o] + fcw + fce + frs + frn;
-        const float az = diag * F.z[o] - fce * F.z[o + 1] - fcw * F.z[o - 1] - frn * F.z[o + fp] - frs * F.z[o - fp];
-        a += F.b[o] - az;
+        for (int jj = 0; jj < 4; ++jj) {
+          const float fcw = fcr[h][jj], fce = fcr[h][jj + 1], fs = frs[h][jj], fn = frn[h][jj];
+          const float diag = mv[h][jj] + fcw + fce + fs + fn;
+          const float az = diag * zr[h][jj + 1] - fce * zr[h][jj + 2] - fcw * zr[h][jj] - fn * znv[h][jj] -
+                           fs * zsv[h][jj];
+          res[h][jj] = bv[h][jj] - az;
+        }
       }
-      acc[k] = a;
     }
+    // aggregate (R, 2q + a): fine cells (2R, 2a), (2R, 2a + 1), (2R + 1, 2a), (2R + 1, 2a + 1), in that order
+    float acc[2];
 #pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      if (!ok[k]) continue;
-      G.b[O[k]] = acc[k];
-      if (red[k]) G.z[O[k]] = G.dinv[O[k]] * acc[k];
+    for (int a = 0; a < 2; ++a) {
+      float s1 = 0.f;
+      s1 += res[0][2 * a];
+      s1 += res[0][2 * a + 1];
+      s1 += res[1][2 * a];
+      s1 += res[1][2 * a + 1];
+      acc[a] = s1;
     }
+    st2(G.b, O, make_float2(acc[0], acc[1]));
+    st2(G.z, O, make_float2(dg.x * acc[0], dg.y * acc[1]));
   }
 }
 
@@ -217,40 +292,45 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
   int it = 0;
   ier = 0;
   const MgLevel& L0 = s_lv[0];
-  const int n0 = L0.rows * L0.cols, pt = L0.pitch;
+  const int n0q = L0.rows * L0.nq, pt = L0.pitch;
   for (;;) {
-    // ---- U: u += alpha p, r -= alpha q; (r, r); red half-sweep of level 0 from zero
+    // ---- U: u += alpha p, r -= alpha q; (r, r); z = dinv r, the red half-sweep of level 0 from zero
+    // (written for the black cells too: the black half-sweep replaces them before they are read)
     {
       const float a = (float)alpha;
       const float* __restrict__ pn = (it & 1) ? M.p1 : M.p0;
       double rr = 0.0;
-      for (int t0 = g0; t0 < n0; t0 += UN * stride) {
-        int o[UN];
-        bool ok[UN], red[UN];
-        float rv[UN], dv[UN], uv[UN], pv[UN], qv[UN];
+      for (int t0 = g0; t0 < n0q; t0 += UG * stride) {
+        int o[UG];
+        bool ok[UG];
+        float4 rv[UG], zv[UG], uv[UG];
 #pragma unroll
-        for (int k = 0; k < UN; ++k) {
+        for (int k = 0; k < UG; ++k) {
           const int t = t0 + k * stride;
-          ok[k] = t < n0;
-          const int r = ok[k] ? fdiv(L0.div_cols, t) : 0;
-          const int c = ok[k] ? t - r * L0.cols : 0;
-          o[k] = (r + 1) * pt + c + 1;
-          red[k] = ((r + c) & 1) == 0;
-          rv[k] = L0.b[o[k]];
-          dv[k] = L0.dinv[o[k]];
-          if (it > 0) { uv[k] = M.u[o[k]]; pv[k] = pn[o[k]]; qv[k] = M.q[o[k]]; }
+          ok[k] = t < n0q;
+          int r = 0, q = 0;
+          o[k] = ok[k] ? group_at(L0, t, r, q) : pt + CO;
+          rv[k] = ld4(L0.b, o[k]);
+          const float4 dv = ld4(L0.dinv, o[k]);
+          if (it > 0) {
+            const float4 u4 = ld4(M.u, o[k]), p4 = ld4(pn, o[k]), q4 = ld4(M.q, o[k]);
+            uv[k] = make_float4(u4.x + a * p4.x, u4.y + a * p4.y, u4.z + a * p4.z, u4.w + a * p4.w);
+            rv[k] = make_float4(rv[k].x - a * q4.x, rv[k].y - a * q4.y, rv[k].z - a * q4.z, rv[k].w - a * q4.w);
+          }
+          zv[k] = make_float4(dv.x * rv[k].x, dv.y * rv[k].y, dv.z * rv[k].z, dv.w * rv[k].w);
         }
 #pragma unroll
-        for (int k = 0; k < UN; ++k) {
+        for (int k = 0; k < UG; ++k) {
           if (!ok[k]) continue;
-          float r = rv[k];
           if (it > 0) {
-            M.u[o[k]] = uv[k] + a * pv[k];
-            r = r - a * qv[k];
-            L0.b[o[k]] = r;
+            st4(M.u, o[k], uv[k]);
+            st4(L0.b, o[k], rv[k]);
           }
-          rr += (double)r * (double)r;
-          if (red[k]) L0.z[o[k]] = dv[k] * r;
+          st4(L0.z, o[k], zv[k]);
+          rr += (double)rv[k].x * (double)rv[k].x;
+          rr += (double)rv[k].y * (double)rv[k].y;
+          rr += (double)rv[k].z * (double)rv[k].z;
+          rr += (double)rv[k].w * (double)rv[k].w;
         }
       }
       double w[1] = {rr};
@@ -267,7 +347,7 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
     }
     // ---- down: black half-sweep, restriction
     for (int k = 0; k < nlev - 1; ++k) {
-      half_sweep<false, false>(s_lv[k], s_lv[k], 1, g0, stride);
+      half_sweep<false, false, UH>(s_lv[k], s_lv[k], 1, g0, stride);
       if (!grid_barrier(bar, SC, s_flag)) return false;
       restrict_residual(s_lv[k], s_lv[k + 1], g0, stride);
       if (!grid_barrier(bar, SC, s_flag)) return false;
@@ -275,27 +355,27 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
     // ---- coarsest level: black, red (one block)
     if (blockIdx.x == 0) {
       const MgLevel& Lc = s_lv[nlev - 1];
-      half_sweep<false, false>(Lc, Lc, 1, threadIdx.x, MQ);
+      half_sweep<false, false, UH>(Lc, Lc, 1, threadIdx.x, MQ);
       __syncthreads();
-      half_sweep<false, false>(Lc, Lc, 0, threadIdx.x, MQ);
+      half_sweep<false, false, UH>(Lc, Lc, 0, threadIdx.x, MQ);
     }
     if (!grid_barrier(bar, SC, s_flag)) return false;
     // ---- up: black half-sweep with the coarse correction, red half-sweep; (r, z) at level 0
     for (int k = nlev - 2; k >= 0; --k) {
       if (k == 0) {
-        double w[1] = {half_sweep<true, true>(s_lv[0], s_lv[1], 1, g0, stride)};
+        double w[1] = {half_sweep<true, true, UH>(s_lv[0], s_lv[1], 1, g0, stride)};
         bsum<1, MQ>(w, sh);
         if (threadIdx.x == 0) rz_part[blockIdx.x] = w[0];
       } else {
-        half_sweep<true, false>(s_lv[k], s_lv[k + 1], 1, g0, stride);
+        half_sweep<true, false, UH>(s_lv[k], s_lv[k + 1], 1, g0, stride);
       }
       if (!grid_barrier(bar, SC, s_flag)) return false;
       if (k == 0) {
-        double w[1] = {half_sweep<false, true>(s_lv[0], s_lv[0], 0, g0, stride)};
+        double w[1] = {half_sweep<false, true, UH>(s_lv[0], s_lv[0], 0, g0, stride)};
         bsum<1, MQ>(w, sh);
         if (threadIdx.x == 0) rz_part[nb + blockIdx.x] = w[0];
       } else {
-        half_sweep<false, false>(s_lv[k], s_lv[k], 0, g0, stride);
+        half_sweep<false, false, UH>(s_lv[k], s_lv[k], 0, g0, stride);
       }
       if (!grid_barrier(bar, SC, s_flag)) return false;
     }
@@ -313,33 +393,55 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
       const float* __restrict__ po = (it & 1) ? M.p1 : M.p0;
       float* __restrict__ pw = (it & 1) ? M.p0 : M.p1;
       double pq = 0.0;
-      for (int t0 = g0; t0 < n0; t0 += UN * stride) {
-        int o[UN];
-        bool ok[UN];
-        float pc[UN], qv[UN];
+      for (int t0 = g0; t0 < n0q; t0 += UG * stride) {
+        int o[UG];
+        bool ok[UG];
+        float4 pc[UG], qv[UG];
 #pragma unroll
-        for (int k = 0; k < UN; ++k) {
+        for (int k = 0; k < UG; ++k) {
           const int t = t0 + k * stride;
-          ok[k] = t < n0;
-          const int r = ok[k] ? fdiv(L0.div_cols, t) : 0;
-          const int c = ok[k] ? t - r * L0.cols : 0;
-          const int x = (r + 1) * pt + c + 1;
+          ok[k] = t < n0q;
+          int r = 0, q = 0;
+          const int x = ok[k] ? group_at(L0, t, r, q) : pt + CO;
           o[k] = x;
-          float p0 = L0.z[x], pW = L0.z[x - 1], pE = L0.z[x + 1], pS = L0.z[x - pt], pN = L0.z[x + pt];
+          // p at columns -1 .. 4 of the row and at the four cells of the rows south and north
+          float4 zm = ld4(L0.z, x), zs = ld4(L0.z, x - pt), zn = ld4(L0.z, x + pt);
+          float zw = L0.z[x - 1], ze = L0.z[x + 4];
           if (!first) {
-            p0 += bt * po[x]; pW += bt * po[x - 1]; pE += bt * po[x + 1]; pS += bt * po[x - pt]; pN += bt * po[x + pt];
+            const float4 om = ld4(po, x), os = ld4(po, x - pt), on = ld4(po, x + pt);
+            const float ow = po[x - 1], oe = po[x + 4];
+            zm = make_float4(zm.x + bt * om.x, zm.y + bt * om.y, zm.z + bt * om.z, zm.w + bt * om.w);
+            zs = make_float4(zs.x + bt * os.x, zs.y + bt * os.y, zs.z + bt * os.z, zs.w + bt * os.w);
+            zn = make_float4(zn.x + bt * on.x, zn.y + bt * on.y, zn.z + bt * on.z, zn.w + bt * on.w);
+            zw = zw + bt * ow;
+            ze = ze + bt * oe;
           }
-          const float fcw = L0.fc[x - 1], fce = L0.fc[x], frs = L0.fr[x - pt], frn = L0.fr[x];
-          const float diag = L0.mass[x] + fcw + fce + frs + frn;
-          pc[k] = p0;
-          qv[k] = diag * p0 - fce * pE - fcw * pW - frn * pN - frs * pS;
+          const float4 fc = ld4(L0.fc, x), fr = ld4(L0.fr, x), fs = ld4(L0.fr, x - pt), ms = ld4(L0.mass, x);
+          const float fw0 = L0.fc[x - 1];
+          const float pr[6] = {zw, zm.x, zm.y, zm.z, zm.w, ze};
+          const float ps[4] = {zs.x, zs.y, zs.z, zs.w}, pn4[4] = {zn.x, zn.y, zn.z, zn.w};
+          const float fcr[5] = {fw0, fc.x, fc.y, fc.z, fc.w};
+          const float frn[4] = {fr.x, fr.y, fr.z, fr.w}, frs[4] = {fs.x, fs.y, fs.z, fs.w};
+          const float mv[4] = {ms.x, ms.y, ms.z, ms.w};
+          float qq[4];
+#pragma unroll
+          for (int jj = 0; jj < 4; ++jj) {
+            const float fcw = fcr[jj], fce = fcr[jj + 1];
+            const float diag = mv[jj] + fcw + fce + frs[jj] + frn[jj];
+            qq[jj] = diag * pr[jj + 1] - fce * pr[jj + 2] - fcw * pr[jj] - frn[jj] * pn4[jj] - frs[jj] * ps[jj];
+          }
+          pc[k] = zm;
+          qv[k] = make_float4(qq[0], qq[1], qq[2], qq[3]);
         }
 #pragma unroll
-        for (int k = 0; k < UN; ++k) {
+        for (int k = 0; k < UG; ++k) {
           if (!ok[k]) continue;
-          pw[o[k]] = pc[k];
-          M.q[o[k]] = qv[k];
-          pq += (double)pc[k] * (double)qv[k];
+          st4(pw, o[k], pc[k]);
+          st4(M.q, o[k], qv[k]);
+          pq += (double)pc[k].x * (double)qv[k].x;
+          pq += (double)pc[k].y * (double)qv[k].y;
+          pq += (double)pc[k].z * (double)qv[k].z;
+          pq += (double)pc[k].w * (double)qv[k].w;
         }
       }
       double w[1] = {pq};
@@ -382,7 +484,7 @@ __global__ void __launch_bounds__(MQ, 1) k_mg_solve(MgDev M, GridBar* bar) {
       // ---- u += e (FP64)
       for (int t = g0; t < n0; t += stride) {
         const int r = fdiv(L0.div_cols, t), c = t - r * L0.cols;
-        const int o = (r + 1) * pt + c + 1;
+        const int o = (r + 1) * pt + c + CO;
         M.u64[o] = M.u64[o] + (double)M.u[o];
       }
       if (!grid_barrier(bar, SC, &s_flag)) return;
@@ -400,7 +502,7 @@ __global__ void __launch_bounds__(MQ, 1) k_mg_solve(MgDev M, GridBar* bar) {
           ok[k] = t < n0;
           const int r = ok[k] ? fdiv(L0.div_cols, t) : 0;
           const int c = ok[k] ? t - r * L0.cols : 0;
-          const int x = (r + 1) * pt + c + 1;
+          const int x = (r + 1) * pt + c + CO;
           o[k] = x;
           double y = M.dg64[x] * M.u64[x];
           y = y + (-M.fr64[x - pt]) * M.u64[x - pt];

@@ -4,8 +4,12 @@
 // The zeta matrix is a mass term plus a graph Laplacian over the wet cells of the (im1, jm1)
 // grid: (A x)_l = m_l x_l + sum over the faces f of l of c_f (x_l - x_nbr).  Every level of the
 // hierarchy stores that form as an image: cell (r, c) of a rows x cols level at
-// (r + 1) * pitch + c + 1, with a zero frame (one ghost row/column before, two after) so that
-// stencils and 2 x 2 aggregates never test bounds.  Per cell: the mass, the face to the next
+// (r + 1) * pitch + c + kMgColOff, with a zero frame (one ghost row before and two after, four
+// ghost columns before and at least five after) so that stencils and 2 x 2 aggregates never test
+// bounds.  The offset of four columns puts every group of four cells 4q .. 4q + 3 of a row on a
+// 16-byte boundary (the level passes move them as one float4), and with it every aggregate pair of
+// the coarser level on an 8-byte boundary; a pass over whole groups also touches frame and land
+// cells, which hold zero in every array and stay zero.  Per cell: the mass, the face to the next
 // column (fc) and to the next row (fr), the inverse diagonal, the right-hand side b and the
 // iterate z.  Level 0 is the zeta system itself (row = i - 1, column = j - 1 of the wet column);
 // level k + 1 aggregates 2 x 2 cells of level k: masses add, the faces that cross between two
@@ -36,11 +40,18 @@ struct FastDiv {
   int p, d;
 };
 
+constexpr int kMgColOff = 4;   // buffer column of interior column 0
+
 struct MgLevel {
-  int rows, cols, pitch, hw;   // hw = (cols + 1) / 2 cells of one colour per row (at most)
-  FastDiv div_cols, div_hw;
+  int rows, cols, pitch, nq;   // nq = (cols + 3) / 4 groups of four cells per row
+  FastDiv div_cols, div_q;
   float *z, *b, *fc, *fr, *mass, *dinv;
 };
+
+// Floats per row of a level with `cols` columns: the four leading ghost columns, nq whole groups,
+// and at least five trailing ghost columns (the east neighbours of the last group and the
+// aggregate pairs the coarser level reads), rounded up to 32 floats.
+inline int mg_pitch(int cols) { return ((4 * ((cols + 3) / 4) + kMgColOff + 5 + 31) / 32) * 32; }
 
 constexpr int kMgMaxOuter = 40;      // FP64 refinement passes at most (then ier = 1)
 

@@ -374,10 +374,10 @@ int build_mg(Ctx* c, const si3d_grid* g) {
     MgLevel& L = M.lv[M.nlev++];
     L.rows = rows;
     L.cols = cols;
-    L.pitch = ((cols + 3 + 31) / 32) * 32;
-    L.hw = (cols + 1) / 2;
+    L.pitch = mg_pitch(cols);
+    L.nq = (cols + 3) / 4;
     L.div_cols = fast_div(cols);
-    L.div_hw = fast_div(L.hw);
+    L.div_q = fast_div(L.nq);
     const size_t ne = mg_level_elems(rows, cols);
     for (float** q : {&L.z, &L.b, &L.fc, &L.fr, &L.mass, &L.dinv}) rc |= c->alloc(q, ne);
     if (rc) return rc;
@@ -396,7 +396,7 @@ int build_mg(Ctx* c, const si3d_grid* g) {
   for (int l = 1; l <= lm; ++l) {
     const int i = g->l2i[l - 1] - 1, j = g->l2j[l - 1] - 1;
     if (i < 0 || i >= c->im1 || j < 0 || j >= c->jm1) return SI3D_EDIMS;
-    off[l] = (i + 1) * pitch + j + 1;
+    off[l] = (i + 1) * pitch + j + kMgColOff;
   }
   for (int l = 1; l <= lm; ++l) {
     const int e = g->lEC[l - 1], w = g->lWC[l - 1], n = g->lNC[l - 1], s = g->lSC[l - 1];
