@@ -13,12 +13,18 @@
 //           (red) half-sweep of level 0 from z = 0, which is z = dinv r;
 //           the stopping test on the inner residual right after its barrier
 //   down    per level k < L - 1: black half-sweep; residual summed over 2 x 2 aggregates into
-//           level k + 1's b, whose red cells get their first half-sweep z = dinv b
-//   coarse  black then red half-sweep of the coarsest level, by block 0 alone
+//           level k + 1's b, whose red cells get their first half-sweep z = dinv b.  On levels
+//           >= 2 the black half-sweep is not run as a phase: the restriction forms the black
+//           values it reads from their red neighbours (the same expression)
+//   coarse  black half-sweep of the coarsest level
 //   up      per level k = L - 2 .. 0: black half-sweep with the neighbours' values plus the coarse
-//           correction of their aggregate; red half-sweep; at level 0 both add to (r, z)
+//           correction of their aggregate; red half-sweep; at level 0 both add to (r, z).  The
+//           red half-sweeps of the coarsest level and of levels >= 2 are not run as phases: the
+//           black half-sweep of the next finer level forms each red aggregate it reads from that
+//           aggregate's black neighbours (the same expression, so the same values)
 //   PQ      beta, p = z + beta p and q = A p (neighbours' p formed on the fly), (p, q)
-// With L levels that is 4 L - 1 barriers an inner iteration.
+// With L >= 3 levels that is 2 L + 5 barriers an inner iteration (15 for the five levels of the
+// 2000 x 1000 system, where a V-cycle with every half-sweep a phase has 19).
 //
 // Every level pass walks groups of four consecutive cells of a row (one float4 of each array,
 // 16-byte aligned by the image layout, mg.h): a thread keeps several groups' loads in flight with a
@@ -51,10 +57,15 @@ using namespace coop;
 
 constexpr int PB = 256;               // threads per block of the setup kernels
 constexpr float kFaceScale = 0.5f;    // coarse faces: half the sum of the crossing fine faces
-constexpr int UN = 4;                 // cells a thread keeps in flight in the cell-by-cell FP64 passes
 constexpr int CO = kMgColOff;
 constexpr int UG = 2;                 // groups of four cells a thread keeps in flight in the level-0 CG passes
 constexpr int UH = 2;                 // groups in flight in the half-sweeps
+// Levels from kSweptFrom on (and the coarsest) skip their red half-sweep of the way up: the finer
+// level's black half-sweep forms the red values it reads from their black neighbours (swept_z).
+// Cheap on the small levels, it saves a grid barrier a level; on levels 0 and 1 the recomputation
+// costs more than the barrier.
+constexpr int kSweptFrom = 2;
+constexpr int kSpreadFrom = 2;   // levels whose items are dealt round robin (first_item_spread)
 constexpr int MQ = 512;               // threads per block of the cooperative solve (one block per SM)
 
 __device__ __forceinline__ int fdiv(const FastDiv& f, int x) {
@@ -141,11 +152,31 @@ __device__ __forceinline__ int group_at(const MgLevel& L, int t, int& r, int& q)
   return (r + 1) * L.pitch + 4 * q + CO;
 }
 
+// Gauss-Seidel value of cell (R, C) of level G from its neighbours' current z, dinv (b + sum of
+// face * neighbour z), in the half-sweep's operation order.  Every load is unconditional (the rows
+// are clamped into the frame), so a thread issues all of them at once; frame and land cells
+// (dinv = b = faces = 0) give zero.  R in [-1, rows + 1], C in [-1, 4 nq + 3].
+__device__ __forceinline__ float gs_value(const MgLevel& G, int R, int C) {
+  const int gp = G.pitch, o = (R + 1) * gp + C + CO;
+  const int oS = (max(R - 1, -1) + 1) * gp + C + CO, oN = (min(R + 1, G.rows + 1) + 1) * gp + C + CO;
+  const float s1 = G.b[o] + G.fc[o] * G.z[o + 1] + G.fc[o - 1] * G.z[o - 1] + G.fr[o] * G.z[oN] + G.fr[oS] * G.z[oS];
+  return G.dinv[o] * s1;
+}
+
+// z of cell (R, C) of level G as it stands after G's red half-sweep of the way up, when that sweep
+// was not run: red cells are formed from their black neighbours exactly as the sweep would form
+// them; black cells are read.
+__device__ __forceinline__ float swept_z(const MgLevel& G, int R, int C) {
+  const float v = gs_value(G, R, C), z = G.z[(R + 1) * G.pitch + C + CO];
+  return ((R + C) & 1) == 0 ? v : z;
+}
+
 // Gauss-Seidel half-sweep over the cells of colour `col` ((r + c) & 1 == col) of level L:
 // z = dinv (b + sum of face * neighbour z).  PROLONG: each neighbour's value is its z plus the
-// correction of its aggregate in the coarser level G.  DOT: returns this thread's sum of b * z.
+// correction of its aggregate in the coarser level G; with SWEPT, G's red half-sweep was not run and
+// the red aggregates are formed on the fly (swept_z).  DOT: returns this thread's sum of b * z.
 // A group of four cells of row r holds two cells of the colour, at j0 = (r + col) & 1 and j0 + 2.
-template <bool PROLONG, bool DOT, int U>
+template <bool PROLONG, bool DOT, int U, bool SWEPT = false>
 __device__ __forceinline__ double half_sweep(const MgLevel& L, const MgLevel& G, int col, int g0, int stride) {
   double rz = 0.0;
   const int n = L.rows * L.nq, pt = L.pitch;
@@ -177,12 +208,25 @@ __device__ __forceinline__ double half_sweep(const MgLevel& L, const MgLevel& G,
       if (PROLONG) {
         // aggregates of the neighbours: row r >> 1 at coarse columns 2q - 1 .. 2q + 2, rows
         // (r - 1) >> 1 and (r + 1) >> 1 at 2q, 2q + 1
-        const int gp = G.pitch;
-        const int gr = ((r >> 1) + 1) * gp + 2 * q + CO;
-        const float2 gm = ld2(G.z, gr);
-        const float gc[4] = {G.z[gr - 1], gm.x, gm.y, G.z[gr + 2]};   // coarse columns 2q - 1 .. 2q + 2
-        const float2 gs = ld2(G.z, (((r - 1) >> 1) + 1) * gp + 2 * q + CO);
-        const float2 gn = ld2(G.z, (((r + 1) >> 1) + 1) * gp + 2 * q + CO);
+        float gc[4];   // coarse columns 2q - 1 .. 2q + 2 of row r >> 1
+        float2 gs, gn;
+        if (SWEPT) {
+          // rows (r - 1) >> 1 and (r + 1) >> 1: one of them is row r >> 1 itself
+          const int g1 = r >> 1, go = (r & 1) ? g1 + 1 : g1 - 1;
+#pragma unroll
+          for (int i = 0; i < 4; ++i) gc[i] = swept_z(G, g1, 2 * q - 1 + i);
+          const float2 gm = make_float2(gc[1], gc[2]);
+          const float2 gx = make_float2(swept_z(G, go, 2 * q), swept_z(G, go, 2 * q + 1));
+          gs = (r & 1) ? gm : gx;
+          gn = (r & 1) ? gx : gm;
+        } else {
+          const int gp = G.pitch;
+          const int gr = ((r >> 1) + 1) * gp + 2 * q + CO;
+          const float2 gm = ld2(G.z, gr);
+          gc[0] = G.z[gr - 1]; gc[1] = gm.x; gc[2] = gm.y; gc[3] = G.z[gr + 2];
+          gs = ld2(G.z, (((r - 1) >> 1) + 1) * gp + 2 * q + CO);
+          gn = ld2(G.z, (((r + 1) >> 1) + 1) * gp + 2 * q + CO);
+        }
         // cell jj = 2m + j: west neighbour's aggregate gc[((jj - 1) >> 1) + 1], east gc[((jj + 1) >> 1) + 1],
         // south / north (jj >> 1) = m
 #pragma unroll
@@ -225,15 +269,35 @@ __device__ __forceinline__ double half_sweep(const MgLevel& L, const MgLevel& G,
 // b of level G = the residual b - A z of level F summed over each 2 x 2 aggregate; z of G = dinv b,
 // which is the first half-sweep from zero for its red cells (its black cells are swept before
 // they are read).  An item is one group of four columns in the two fine rows of a coarse row: the
-// coarse pair 2q, 2q + 1.
+// coarse pair 2q, 2q + 1.  BLK: F's black half-sweep of the way down was not run; the black values
+// the residuals read (ten of the twenty in the item's window) are formed here from their red
+// neighbours, as that half-sweep forms them (gs_value).
+template <bool BLK>
 __device__ __forceinline__ void restrict_residual(const MgLevel& F, const MgLevel& G, int g0, int stride) {
   const int n = G.rows * F.nq, fp = F.pitch;
   for (int t = g0; t < n; t += stride) {
     const int R = fdiv(F.div_q, t);
     const int q = t - R * F.nq;
     const int x0 = (2 * R + 1) * fp + 4 * q + CO, x1 = x0 + fp;
-    const float4 zA = ld4(F.z, x0 - fp), z0 = ld4(F.z, x0), z1 = ld4(F.z, x1), zB = ld4(F.z, x1 + fp);
-    const float z0w = F.z[x0 - 1], z0e = F.z[x0 + 4], z1w = F.z[x1 - 1], z1e = F.z[x1 + 4];
+    // z on fine rows 2R - 1 .. 2R + 2 (i) and columns 4q - 1 .. 4q + 4 (j); cell (i, j) is black when
+    // i + j is odd
+    float zw[4][6];
+    {
+      const float4 zA = ld4(F.z, x0 - fp), z0 = ld4(F.z, x0), z1 = ld4(F.z, x1), zB = ld4(F.z, x1 + fp);
+      const float z0w = F.z[x0 - 1], z0e = F.z[x0 + 4], z1w = F.z[x1 - 1], z1e = F.z[x1 + 4];
+      const float win[4][6] = {{0.f, zA.x, zA.y, zA.z, zA.w, 0.f},
+                               {z0w, z0.x, z0.y, z0.z, z0.w, z0e},
+                               {z1w, z1.x, z1.y, z1.z, z1.w, z1e},
+                               {0.f, zB.x, zB.y, zB.z, zB.w, 0.f}};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+#pragma unroll
+        for (int j = 0; j < 6; ++j) {
+          const bool used = (i == 1 || i == 2) || (j >= 1 && j <= 4);
+          zw[i][j] = (BLK && used && ((i + j) & 1)) ? gs_value(F, 2 * R - 1 + i, 4 * q - 1 + j) : win[i][j];
+        }
+      }
+    }
     const float4 b0 = ld4(F.b, x0), b1 = ld4(F.b, x1), m0 = ld4(F.mass, x0), m1 = ld4(F.mass, x1);
     const float4 c0 = ld4(F.fc, x0), c1 = ld4(F.fc, x1);
     const float c0w = F.fc[x0 - 1], c1w = F.fc[x1 - 1];
@@ -242,9 +306,6 @@ __device__ __forceinline__ void restrict_residual(const MgLevel& F, const MgLeve
     const float2 dg = ld2(G.dinv, O);
     float res[2][4];
     {
-      const float zr[2][6] = {{z0w, z0.x, z0.y, z0.z, z0.w, z0e}, {z1w, z1.x, z1.y, z1.z, z1.w, z1e}};
-      const float zsv[2][4] = {{zA.x, zA.y, zA.z, zA.w}, {z0.x, z0.y, z0.z, z0.w}};
-      const float znv[2][4] = {{z1.x, z1.y, z1.z, z1.w}, {zB.x, zB.y, zB.z, zB.w}};
       const float bv[2][4] = {{b0.x, b0.y, b0.z, b0.w}, {b1.x, b1.y, b1.z, b1.w}};
       const float mv[2][4] = {{m0.x, m0.y, m0.z, m0.w}, {m1.x, m1.y, m1.z, m1.w}};
       const float fcr[2][5] = {{c0w, c0.x, c0.y, c0.z, c0.w}, {c1w, c1.x, c1.y, c1.z, c1.w}};
@@ -256,8 +317,8 @@ __device__ __forceinline__ void restrict_residual(const MgLevel& F, const MgLeve
         for (int jj = 0; jj < 4; ++jj) {
           const float fcw = fcr[h][jj], fce = fcr[h][jj + 1], fs = frs[h][jj], fn = frn[h][jj];
           const float diag = mv[h][jj] + fcw + fce + fs + fn;
-          const float az = diag * zr[h][jj + 1] - fce * zr[h][jj + 2] - fcw * zr[h][jj] - fn * znv[h][jj] -
-                           fs * zsv[h][jj];
+          const float az = diag * zw[h + 1][jj + 1] - fce * zw[h + 1][jj + 2] - fcw * zw[h + 1][jj] -
+                           fn * zw[h + 2][jj + 1] - fs * zw[h][jj + 1];
           res[h][jj] = bv[h][jj] - az;
         }
       }
@@ -282,9 +343,20 @@ __device__ __forceinline__ void restrict_residual(const MgLevel& F, const MgLeve
 // FP32 MG-PCG on level 0 from e = 0 (M.u) with right-hand side r (level 0's b), until
 // ||r|| < bnorm * zeta or itmax iterations.  Returns false when a barrier gave up (the caller returns
 // at once); otherwise its = the iterations taken and ier = 0, 1 (itmax) or -6 / -7 (breakdown).
+// A thread's first item of a level pass.  On levels 0 and 1 a block takes MQ consecutive items
+// (b * MQ + thread, then + blocks * MQ), which keeps its accesses in few DRAM pages.  On the coarser
+// levels (a few thousand items) the items are dealt to the blocks in runs of 32 (one warp's worth,
+// so a warp's accesses stay coalesced), round robin, so that they spread over every SM instead of
+// filling the first blocks: thread (warp w, lane i) of block b takes (w * blocks + b) * 32 + i.
+__device__ __forceinline__ int first_item_dense() { return (int)blockIdx.x * MQ + (int)threadIdx.x; }
+__device__ __forceinline__ int first_item_spread() {
+  return ((int)(threadIdx.x >> 5) * (int)gridDim.x + (int)blockIdx.x) * 32 + (int)(threadIdx.x & 31);
+}
+
 __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* bar, PcgScal* SC, BarSt* s_flag,
                        double* sh, double zeta, double bnorm, int itmax, int& its, int& ier) {
-  const int nb = gridDim.x, stride = nb * MQ, g0 = blockIdx.x * MQ + threadIdx.x;
+  const int nb = gridDim.x, stride = nb * MQ, g0 = first_item_dense(), g0s = first_item_spread();
+  auto gk = [&](int k) { return k < kSpreadFrom ? g0 : g0s; };
   double* const rr_part = M.part;
   double* const rz_part = M.part + nb;
   double* const pq_part = M.part + 3 * nb;
@@ -345,37 +417,44 @@ __device__ bool mg_pcg(const MgDev& M, const MgLevel* s_lv, int nlev, GridBar* b
       if (tl < bnorm * zeta) break;
       if (it >= itmax) { ier = 1; break; }
     }
-    // ---- down: black half-sweep, restriction
+    // ---- down: black half-sweep, restriction (on levels >= kSweptFrom the restriction forms the
+    // black values it reads, and the black half-sweep is not run as a phase)
     for (int k = 0; k < nlev - 1; ++k) {
-      half_sweep<false, false, UH>(s_lv[k], s_lv[k], 1, g0, stride);
-      if (!grid_barrier(bar, SC, s_flag)) return false;
-      restrict_residual(s_lv[k], s_lv[k + 1], g0, stride);
-      if (!grid_barrier(bar, SC, s_flag)) return false;
-    }
-    // ---- coarsest level: black, red (one block)
-    if (blockIdx.x == 0) {
-      const MgLevel& Lc = s_lv[nlev - 1];
-      half_sweep<false, false, UH>(Lc, Lc, 1, threadIdx.x, MQ);
-      __syncthreads();
-      half_sweep<false, false, UH>(Lc, Lc, 0, threadIdx.x, MQ);
-    }
-    if (!grid_barrier(bar, SC, s_flag)) return false;
-    // ---- up: black half-sweep with the coarse correction, red half-sweep; (r, z) at level 0
-    for (int k = nlev - 2; k >= 0; --k) {
-      if (k == 0) {
-        double w[1] = {half_sweep<true, true, UH>(s_lv[0], s_lv[1], 1, g0, stride)};
-        bsum<1, MQ>(w, sh);
-        if (threadIdx.x == 0) rz_part[blockIdx.x] = w[0];
+      if (k >= kSweptFrom) {
+        restrict_residual<true>(s_lv[k], s_lv[k + 1], gk(k), stride);
       } else {
-        half_sweep<true, false, UH>(s_lv[k], s_lv[k + 1], 1, g0, stride);
+        half_sweep<false, false, UH>(s_lv[k], s_lv[k], 1, gk(k), stride);
+        if (!grid_barrier(bar, SC, s_flag)) return false;
+        restrict_residual<false>(s_lv[k], s_lv[k + 1], gk(k), stride);
       }
       if (!grid_barrier(bar, SC, s_flag)) return false;
+    }
+    // ---- coarsest level: black half-sweep (its red half-sweep is formed where it is read)
+    half_sweep<false, false, UH>(s_lv[nlev - 1], s_lv[nlev - 1], 1, gk(nlev - 1), stride);
+    if (!grid_barrier(bar, SC, s_flag)) return false;
+    // ---- up: black half-sweep with the coarse correction, red half-sweep; (r, z) at level 0.  The
+    // red half-sweeps of levels >= kSweptFrom (and of the coarsest) are not run: the black half-sweep
+    // of the next finer level forms the red aggregates it reads (swept_z), one barrier fewer each.
+    for (int k = nlev - 2; k >= 0; --k) {
+      const bool swept = k + 1 >= kSweptFrom || k + 1 == nlev - 1;
+      if (k == 0) {
+        double w[1] = {swept ? half_sweep<true, true, 1, true>(s_lv[0], s_lv[1], 1, g0, stride)
+                             : half_sweep<true, true, UH>(s_lv[0], s_lv[1], 1, g0, stride)};
+        bsum<1, MQ>(w, sh);
+        if (threadIdx.x == 0) rz_part[blockIdx.x] = w[0];
+      } else if (swept) {
+        half_sweep<true, false, 1, true>(s_lv[k], s_lv[k + 1], 1, gk(k), stride);
+      } else {
+        half_sweep<true, false, UH>(s_lv[k], s_lv[k + 1], 1, gk(k), stride);
+      }
+      if (!grid_barrier(bar, SC, s_flag)) return false;
+      if (k >= kSweptFrom) continue;
       if (k == 0) {
         double w[1] = {half_sweep<false, true, UH>(s_lv[0], s_lv[0], 0, g0, stride)};
         bsum<1, MQ>(w, sh);
         if (threadIdx.x == 0) rz_part[nb + blockIdx.x] = w[0];
       } else {
-        half_sweep<false, false, UH>(s_lv[k], s_lv[k], 0, g0, stride);
+        half_sweep<false, false, UH>(s_lv[k], s_lv[k], 0, gk(k), stride);
       }
       if (!grid_barrier(bar, SC, s_flag)) return false;
     }
@@ -471,7 +550,7 @@ __global__ void __launch_bounds__(MQ, 1) k_mg_solve(MgDev M, GridBar* bar) {
   if (threadIdx.x < nlev) s_lv[threadIdx.x] = M.lv[threadIdx.x];
   __syncthreads();
   PcgScal* SC = M.sc;
-  const int nb = gridDim.x, stride = nb * MQ, g0 = blockIdx.x * MQ + threadIdx.x;
+  const int nb = gridDim.x, stride = nb * MQ, g0 = first_item_dense();
   double* const res_part = M.part + 4 * nb;   // (r, r) [nb], (b, b) [nb] of the FP64 system
   const double zeta = SC->zeta, srelpr = SC->srelpr;
   const int itmax = SC->itmax;

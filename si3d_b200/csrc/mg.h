@@ -19,7 +19,7 @@
 //
 // The preconditioner is one symmetric V-cycle: red-black Gauss-Seidel (red then black) from a zero
 // guess on the way down, the residual summed over each aggregate, the coarsest level swept red,
-// black, red by one block, and on the way up the coarse correction enters through the black
+// black, red, and on the way up the coarse correction enters through the black
 // half-sweep (black then red), so the cycle is a symmetric positive-definite operator and plain CG
 // applies.
 #pragma once
@@ -28,7 +28,7 @@
 namespace si3d {
 
 constexpr int kMgMaxLevels = 10;
-constexpr int kMgCoarsest = 8192;   // cells of the coarsest level at most (one block sweeps it)
+constexpr int kMgCoarsest = 8192;   // cells of the coarsest level at most
 // Levels at least: each level divides the face-to-mass ratio of the operator by four, and the
 // coarsest level, swept once, must be mass-dominated; 4 coarsenings bring the ratio of the 50 m,
 // 30 s, 60 m deep workloads (about 210 at the leapfrog solve) below one.
