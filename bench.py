@@ -227,6 +227,7 @@ def bench_ensemble(args, ws: int, rank: int, device: int, pg) -> int:
     ens = ensemble.Ensemble(dirs, device=device, pcg_itmax=args.itmax, autotune=True)
     t_setup = time.perf_counter() - t_setup
     try:
+        ens.solve_mode(native.SI3D_ENS_SOLVE_MEMBERS if args.ens_solve == "members" else native.SI3D_ENS_SOLVE_BATCHED)
         ens.step(args.warmup)
         if pg is not None:
             pg.barrier()
@@ -251,7 +252,9 @@ def bench_ensemble(args, ws: int, rank: int, device: int, pg) -> int:
                                    "dt 30 s, FP64, zeta solve to 1e-12 (test 5)",
                        "members_run": len(chosen), "members_this_rank": len(mine),
                        "lm": int(sum(a for a, _ in lm)), "n3": int(sum(b for _, b in lm)),
-                       "device_gb": used / 1e9, "graph_nodes": ens.nodes(), "setup_s": t_setup},
+                       "device_gb": used / 1e9, "graph_nodes": ens.nodes(), "setup_s": t_setup,
+                       "zeta_solves": ("one cooperative launch for all members per solve, %d blocks" % ens.solve_blocks()
+                                       if ens.solve_blocks() > 0 else "one cooperative launch per member and solve")},
             "pcg_iters_per_step_mean_member": float(its.sum() / args.steps / max(len(chosen), 1)),
             "max_ier": int(ier.max()), "min_ier": int(ier.min()),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -282,6 +285,8 @@ def main() -> int:
                     help="conservative tracers carried by the workload (0..30; the headline workload has none)")
     ap.add_argument("--iturb", type=int, default=0, choices=[0, 1],
                     help="1: the Mellor-Yamada 2.5 closure instead of constant eddy coefficients")
+    ap.add_argument("--ens-solve", choices=["batched", "members"], default="batched",
+                    help="c3: each zeta solve of a step as one launch for all members (batched) or one per member")
     ap.add_argument("--forms", default="",
                     help="comma-separated subset of plain_fp64,mixed_ir,mixed_last,learned_fp64,learned_mixed,"
                          "learned_mg,mg_mixed (the last one is the headline); default: plain_fp64,mixed_ir,mixed_last, "

@@ -298,6 +298,23 @@ int si3d_ens_create(const int* handles, int n, int* ens);
 int si3d_ens_step(int ens, int n0, int nsteps, int* iters, int* ier, double* ms);
 /* Nodes of the captured step graph (0 before the first step n >= 2). */
 int si3d_ens_nodes(int ens);
+/* How the captured step runs the members' zeta solves (no counterpart in the reference).
+ * SI3D_ENS_SOLVE_BATCHED (the default): the members advance in lock step, and each of the step's
+ * zeta solves is ONE cooperative launch for all members, each basin iterating to its own
+ * convergence on its share of the SMs with its own barrier counter; it applies when every member
+ * uses stopping test 5, the same itrap and niter, and no open boundary, and there are no more
+ * members than co-resident blocks (otherwise the step falls back to the per-member form).
+ * SI3D_ENS_SOLVE_MEMBERS: one cooperative solve launch per member, on the member's own stream.
+ * A member that gets as many blocks in the batched launch as its own launch uses (the members'
+ * needs fit the GPU together) sums its dot products in the same order, and both forms give
+ * bit-identical states; when the members share fewer blocks, a basin's dot products are summed
+ * over fewer partials and its state agrees with the other form to rounding, each solve still
+ * iterating to the same tolerance.  Changing the mode re-captures at the next step. */
+#define SI3D_ENS_SOLVE_MEMBERS 0
+#define SI3D_ENS_SOLVE_BATCHED 1
+int si3d_ens_solve_mode(int ens, int mode);
+/* Blocks of the batched solve launch in the captured graph (0: per-member form, or not captured). */
+int si3d_ens_solve_blocks(int ens);
 void si3d_ens_destroy(int ens);
 
 #ifdef __cplusplus

@@ -80,18 +80,19 @@ __device__ __forceinline__ void red_release_add(unsigned long long* p, unsigned 
 }
 
 // Grid barrier on a monotonic arrival counter: barrier e (1, 2, ...) of the launch is passed once
-// the counter reaches e * (blocks + absent).  An arrival is one release-add (no round trip, no
+// the counter reaches e * (nblocks + absent), nblocks being the blocks that share this barrier
+// record (the whole grid, or one basin's share of an ensemble launch).  An arrival is one release-add (no round trip, no
 // reset; the release orders the block's writes, which __syncthreads ordered before thread 0's
 // arrival, ahead of it); the wait polls with acquire loads, which order the block's later reads
 // after the other blocks' arrivals.  `absent` and `limit` (zero in every solve; a test sets them
 // to make the wait run out) are read once, at the first barrier, so a barrier costs one release
 // and the polls.  Bounded: returns false (in every thread of the block) once this block gave up
 // or any block has.
-__device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, BarSt* st) {
+__device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, BarSt* st, unsigned int nblocks) {
   __syncthreads();
   if (threadIdx.x == 0) {
     if (st->epoch == 0) {
-      st->expect = gridDim.x + __ldcg(&bar->absent);
+      st->expect = nblocks + __ldcg(&bar->absent);
       const unsigned long long lim = __ldcg(&bar->limit);
       st->limit = lim ? (long long)lim : kSpinLimit;
     }
@@ -112,6 +113,10 @@ __device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, BarSt* s
   }
   __syncthreads();
   return st->ok != 0;
+}
+
+__device__ __forceinline__ bool grid_barrier(GridBar* bar, PcgScal* sc, BarSt* st) {
+  return grid_barrier(bar, sc, st, gridDim.x);
 }
 
 }  // namespace coop

@@ -158,17 +158,17 @@ __device__ __noinline__ void lz_chgcon(PcgScal* S, double* tri, int ip, double a
 }
 
 // TEST2: stopping test 2 with chgcon's adaptive emin (test 5 otherwise); a separate instantiation keeps
-// the test-5 loop free of the eigenvalue code.
+// the test-5 loop free of the eigenvalue code.  The loop of one system, run by the nb blocks that
+// share the barrier record `bar`, this block being block `bid` of them.
 template <typename T, bool TEST2, bool DIAG>
-__global__ void __launch_bounds__(PQB, 1) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
+__device__ __forceinline__ void pcg_loop_body(const PcgDevT<T>& P, GridBar* bar, int bid, int nb) {
   __shared__ double sh[(PQB / 32) * 4 + 4];
   __shared__ BarSt s_flag;
   if (threadIdx.x == 0) s_flag.epoch = 0;
   const PcgColorT<T> &R = P.R, &B = P.B;
   PcgScal* SC = P.sc;
-  const int nb = gridDim.x;
   const int stride = nb * PQB;
-  const int g0 = blockIdx.x * PQB + threadIdx.x;
+  const int g0 = bid * PQB + threadIdx.x;
   // partial sums: (r,r) in part0, (r,z) in part1, (u,u) in part2, (z,z) in part3, black blocks at
   // [0, nb) and red blocks at [nb, 2 nb); (p,q) at part0 + 2 nb.  The four arrays are equally
   // spaced (part_n apart in one allocation).
@@ -219,13 +219,13 @@ __global__ void __launch_bounds__(PQB, 1) k_pcg_loop(PcgDevT<T> P, GridBar* bar)
     if (t2) {
       bsum<4, PQB>(v, sh);
       if (threadIdx.x == 0)
-        for (int i = 0; i < 4; ++i) P.part0[i * pstride + blockIdx.x] = v[i];
+        for (int i = 0; i < 4; ++i) P.part0[i * pstride + bid] = v[i];
     } else {
       double w2[2] = {v[0], v[1]};
       bsum<2, PQB>(w2, sh);
-      if (threadIdx.x == 0) { P.part0[blockIdx.x] = w2[0]; P.part0[pstride + blockIdx.x] = w2[1]; }
+      if (threadIdx.x == 0) { P.part0[bid] = w2[0]; P.part0[pstride + bid] = w2[1]; }
     }
-    if (!grid_barrier(bar, SC, &s_flag)) return;
+    if (!grid_barrier(bar, SC, &s_flag, nb)) return;
     // ---- red nodes: u/r updates, red half of M^-1
     v[0] = v[1] = v[2] = v[3] = 0;
     q4n = (g0 < R.n) ? R.nbr[g0] : make_int4(0, 0, 0, 0);
@@ -251,13 +251,13 @@ __global__ void __launch_bounds__(PQB, 1) k_pcg_loop(PcgDevT<T> P, GridBar* bar)
     if (t2) {
       bsum<4, PQB>(v, sh);
       if (threadIdx.x == 0)
-        for (int i = 0; i < 4; ++i) P.part0[i * pstride + nb + blockIdx.x] = v[i];
+        for (int i = 0; i < 4; ++i) P.part0[i * pstride + nb + bid] = v[i];
     } else {
       double w2[2] = {v[0], v[1]};
       bsum<2, PQB>(w2, sh);
-      if (threadIdx.x == 0) { P.part0[nb + blockIdx.x] = w2[0]; P.part0[pstride + nb + blockIdx.x] = w2[1]; }
+      if (threadIdx.x == 0) { P.part0[nb + bid] = w2[0]; P.part0[pstride + nb + bid] = w2[1]; }
     }
-    if (!grid_barrier(bar, SC, &s_flag)) return;
+    if (!grid_barrier(bar, SC, &s_flag, nb)) return;
     // ---- every block: (r,r), (r,z) [, (u,u), (z,z)], the stopping test (pstops) and beta
     double rrt, rzt, uut = 0, zzt = 0;
     if (t2) {
@@ -333,26 +333,50 @@ __global__ void __launch_bounds__(PQB, 1) k_pcg_loop(PcgDevT<T> P, GridBar* bar)
       }
     }
     bsum<1, PQB>(pq, sh);
-    if (threadIdx.x == 0) pq_part[blockIdx.x] = pq[0];
-    if (!grid_barrier(bar, SC, &s_flag)) return;
+    if (threadIdx.x == 0) pq_part[bid] = pq[0];
+    if (!grid_barrier(bar, SC, &s_flag, nb)) return;
     double pap[1];
     all_partials<1, PQB>(pq_part, nb, 0, pap, sh);
     const double alpha_prev = alpha;
     alpha = rzdot / pap[0];
     if (!(pap[0] > 0.0)) { ier = -6; break; }
-    if (blockIdx.x == 0 && threadIdx.x == 0 && in < hist_cap) { P.hist_alpha[in] = alpha; P.hist_beta[in] = beta; }
-    if (TEST2 && blockIdx.x == 0 && threadIdx.x == 0 && P.tri && (SC->maxadp || SC->minadp))
+    if (bid == 0 && threadIdx.x == 0 && in < hist_cap) { P.hist_alpha[in] = alpha; P.hist_beta[in] = beta; }
+    if (TEST2 && bid == 0 && threadIdx.x == 0 && P.tri && (SC->maxadp || SC->minadp))
       lz_chgcon(SC, P.tri, in, alpha, beta, alpha_prev);
     in += 1;
     par ^= 1;
   }
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (bid == 0 && threadIdx.x == 0) {
     SC->alpha = alpha; SC->beta = beta; SC->rzdot = rzdot; SC->dkm1 = dkm1; SC->udnm = udnm; SC->q1 = q1;
     SC->in = in; SC->stptst = stptst;
     if (ier) SC->ier = ier;
     else if (SC->chg_ier) SC->ier = SC->chg_ier;
     SC->done = 1;
   }
+}
+
+template <typename T, bool TEST2, bool DIAG>
+__global__ void __launch_bounds__(PQB, 1) k_pcg_loop(PcgDevT<T> P, GridBar* bar) {
+  pcg_loop_body<T, TEST2, DIAG>(P, bar, blockIdx.x, gridDim.x);
+}
+
+// The FP64 loops of an ensemble's basins in one cooperative launch: basin m's system is solved by
+// blocks [first, first + nblk) of the grid with its own barrier record, so each basin iterates to
+// its own convergence and the launch ends when the last one has (stopping test 5, no stored
+// diagonal: the basins the ensemble form admits).
+__global__ void __launch_bounds__(PQB, 1) k_pcg_loop_ens(const PcgEnsItem* __restrict__ items, int nitems) {
+  __shared__ PcgEnsItem s_it;
+  __shared__ int s_m;
+  if (threadIdx.x == 0) {
+    int m = -1;
+    for (int i = 0; i < nitems && m < 0; ++i)
+      if ((int)blockIdx.x >= items[i].first && (int)blockIdx.x < items[i].first + items[i].nblk) m = i;
+    s_m = m;
+    if (m >= 0) s_it = items[m];
+  }
+  __syncthreads();
+  if (s_m < 0) return;
+  pcg_loop_body<double, false, false>(s_it.P, s_it.bar, (int)blockIdx.x - s_it.first, s_it.nblk);
 }
 
 // Cooperative launch (all blocks co-resident) through cudaLaunchKernelEx, which stream capture
@@ -661,6 +685,28 @@ int pcg_loop_blocks(int device, int nR, int nB, int max_per_sm, bool fp32) {
 
 int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st, const GridBar* init) {
   return launch_loop<double>(P, bar, nblocks, test2, st, init);
+}
+
+int pcg_loop_ens_blocks(int device) {
+  int sms = 0, occ = 0;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_pcg_loop_ens, PQB, 0);
+  return sms * std::max(occ, 0);
+}
+
+int pcg_loop_ens(const PcgEnsItem* items, int nitems, int nblocks, GridBar* bars, cudaStream_t st) {
+  if (cudaMemsetAsync(bars, 0, sizeof(GridBar) * (size_t)nitems, st) != cudaSuccess) return -1;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(nblocks);
+  cfg.blockDim = dim3(PQB);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k_pcg_loop_ens, items, nitems) == cudaSuccess ? 0 : -1;
 }
 
 int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st, const GridBar* init) {

@@ -135,6 +135,16 @@ void nat_setup(const Dev& d, const NatDev& N, int x0_mode, const double* dz, cud
 int nat_solve(const NatDev& N, bool test2, cudaStream_t st);
 void nat_finish(const Dev& d, const NatDev& N, cudaStream_t st);
 // `init` (host memory, optional) replaces the zeroed barrier record of this launch
+// One basin's share of an ensemble's batched FP64 solve (k_pcg_loop_ens): its system, its own
+// barrier record, and the blocks [first, first + nblk) of the launch that solve it.
+struct PcgEnsItem {
+  PcgDev P;
+  GridBar* bar;
+  int first, nblk;
+};
+int pcg_loop_ens_blocks(int device);   // co-resident blocks of the batched launch
+// the batched launch over nitems basins (items and bars in device memory; bars zeroed first)
+int pcg_loop_ens(const PcgEnsItem* items, int nitems, int nblocks, GridBar* bars, cudaStream_t st);
 int pcg_loop(const PcgDev& P, GridBar* bar, int nblocks, bool test2, cudaStream_t st,
              const GridBar* init = nullptr);   // test2: stopping test 2
 int pcg_loop_f(const PcgDevF& F, GridBar* bar, int nblocks, cudaStream_t st, const GridBar* init = nullptr);

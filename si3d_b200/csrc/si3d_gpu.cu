@@ -1,6 +1,7 @@
 // C-ABI implementation (include/si3d_gpu.h): handle management, device state, layout
 // transposes at the boundary, and the stage sequence of fd / settrap / settrap2 / save.
 #include <algorithm>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -139,6 +140,11 @@ struct Ctx {
   Tune tune;                     // launch shapes of the column stages (autotuned)
   bool graph_mode = false;
   int solve_slot = 0;
+  // batched ensemble capture: solve() stops after the set-up of its FP64 loop and leaves the loop
+  // to the ensemble's one launch, then solve_graph_post finishes it (hist and ier kept here)
+  bool ens_defer = false;
+  double* def_hist = nullptr;
+  int def_ier = 0;
   int* d_stats_ii = nullptr;     // [24][2]
   double* d_stats_rr = nullptr;  // [24]
   double* staging = nullptr;  // device staging for transposes (km1 * lm1)
@@ -844,6 +850,17 @@ int solve_natural(Ctx* c, int x0, int ier, int* iters, double* relres, int* ier_
   return 0;
 }
 
+// After the cooperative loop of a graph-mode FP64 solve: zeta back to the columns, and the solve's
+// statistics into its device slot.
+int solve_graph_post(Ctx* c, double* hist, int ier) {
+  const int rc = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, hist, c->st); });
+  if (rc) return rc;
+  pcg_record_stats(c->pcg.sc, ier, c->d_stats_ii, c->d_stats_rr, std::min(c->solve_slot, 23), c->st);
+  c->launches += 1;
+  c->solve_slot++;
+  return 0;
+}
+
 int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   const si3d_params& p = c->prm;
   PcgScal init{};
@@ -893,17 +910,17 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   int rc0 = stage(c, ST_PCG_SETUP, 7, [&] { pcg_setup(c->d, c->pcg, x0, c->dz, hist, &c->pcg.sc->negpiv, c->st); });
   if (rc0) return rc0;
   if (c->graph_mode) {
-    if (pcg_loop(c->pcg, c->bar, c->loop_blocks, c->prm.pcg_test == 2, c->st) != 0) return cuda_fail(cudaGetLastError(), "pcg_loop", __LINE__);
-    c->launches += 1;
-    rc0 = stage(c, ST_PCG_FINISH, 2, [&] { pcg_finish(c->d, c->pcg, hist, c->st); });
-    if (rc0) return rc0;
-    pcg_record_stats(c->pcg.sc, ier, c->d_stats_ii, c->d_stats_rr, std::min(c->solve_slot, 23), c->st);
-    c->launches += 1;
-    c->solve_slot++;
     *iters = 0;
     *relres = 0.0;
     *ier_out = 0;
-    return 0;
+    if (c->ens_defer) {   // the ensemble's batched launch runs the loop
+      c->def_hist = hist;
+      c->def_ier = ier;
+      return 0;
+    }
+    if (pcg_loop(c->pcg, c->bar, c->loop_blocks, c->prm.pcg_test == 2, c->st) != 0) return cuda_fail(cudaGetLastError(), "pcg_loop", __LINE__);
+    c->launches += 1;
+    return solve_graph_post(c, hist, ier);
   }
   if (c->prof) CK(cudaEventRecord(c->pe0, c->st));
   int total_iters = 0;
@@ -998,7 +1015,10 @@ int scalar_stage(Ctx* c) {
 }
 int obc_launches(const Ctx* c) { return (int)c->obc.size(); }
 
-int fd_impl(Ctx* c, int istep, bool lastiter, si3d_step_stats* st) {
+// One fd call is fd_pre, the zeta solve and fd_post (the batched ensemble capture runs the three
+// parts of all its members in lock step).
+// fd up to the zeta solve: time-level factor, openbcUVH, momentum, matcon.
+int fd_pre(Ctx* c, int istep) {
   Dev& d = c->d;
   d.tz = 1.0 / istep;
   c->cur_istep = istep;
@@ -1012,6 +1032,31 @@ int fd_impl(Ctx* c, int istep, bool lastiter, si3d_step_stats* st) {
   rc = stage(c, ST_MOMX, 2 + obc_launches(c), [&] { momentum_stage(c, 1); });
   if (!rc) rc = stage(c, ST_MOMY, 2 + obc_launches(c), [&] { momentum_stage(c, 2); });
   if (!rc) rc = stage(c, ST_MATCON, 1 + 2 * obc_launches(c), [&] { matcon_stage(c); });
+  return rc;
+}
+
+// fd after the zeta solve: surface layer, openbcUVH, velocities, scalar, tracers, wetting, mixing.
+int fd_post(Ctx* c, bool lastiter) {
+  Dev& d = c->d;
+  int rc = stage(c, ST_SLAYER, 1, [&] { launch_slayer_h(d, c->st); });
+  if (!rc) rc = obc_uvh(c);   // openbcUVH after the solve (:482)
+  if (!rc) c->launches += obc_launches(c);
+  if (!rc) rc = stage(c, ST_VEL, 3 + obc_launches(c), [&] { vel_stage(c); });
+  if (!rc && c->prm.isal != 0) {
+    int rs = 0;
+    rc = stage(c, ST_SCALAR, 3 + obc_launches(c), [&] { rs = scalar_stage(c); });
+    if (!rc) rc = rs;
+  }
+  if (!rc && c->prm.ntr > 0 && c->prm.niter > 0 && lastiter)
+    rc = stage(c, ST_TRACER, 2 * ((c->prm.ntr + kTracerFluxGroup - 1) / kTracerFluxGroup) + 1, [&] { tracer_stage(c); });
+  if (!rc) rc = stage(c, ST_VEL2, 1, [&] { launch_vel2(d, c->st); });
+  // UpdateMixingCoefficients (si3d_procedures.f90:571)
+  if (!rc && c->prm.iturb == 1) rc = stage(c, ST_TURB, 1, [&] { launch_turbulence(d, c->turb_scr, c->st); });
+  return rc;
+}
+
+int fd_impl(Ctx* c, int istep, bool lastiter, si3d_step_stats* st) {
+  int rc = fd_pre(c, istep);
   if (rc) return rc;
   if (st) CK(cudaEventRecord(c->evp0, c->st));
   int iters = 0, ier = 0;
@@ -1027,20 +1072,7 @@ int fd_impl(Ctx* c, int istep, bool lastiter, si3d_step_stats* st) {
     st->total_iters += iters;
   }
   if (ier < 0) return ier;
-  rc = stage(c, ST_SLAYER, 1, [&] { launch_slayer_h(d, c->st); });
-  if (!rc) rc = obc_uvh(c);   // openbcUVH after the solve (:482)
-  if (!rc) c->launches += obc_launches(c);
-  if (!rc) rc = stage(c, ST_VEL, 3 + obc_launches(c), [&] { vel_stage(c); });
-  if (!rc && c->prm.isal != 0) {
-    int rs = 0;
-    rc = stage(c, ST_SCALAR, 3 + obc_launches(c), [&] { rs = scalar_stage(c); });
-    if (!rc) rc = rs;
-  }
-  if (!rc && c->prm.ntr > 0 && c->prm.niter > 0 && lastiter)
-    rc = stage(c, ST_TRACER, 2 * ((c->prm.ntr + kTracerFluxGroup - 1) / kTracerFluxGroup) + 1, [&] { tracer_stage(c); });
-  if (!rc) rc = stage(c, ST_VEL2, 1, [&] { launch_vel2(d, c->st); });
-  // UpdateMixingCoefficients (si3d_procedures.f90:571)
-  if (!rc && c->prm.iturb == 1) rc = stage(c, ST_TURB, 1, [&] { launch_turbulence(d, c->turb_scr, c->st); });
+  rc = fd_post(c, lastiter);
   if (rc) return rc;
   if (st) {
     CK(cudaEventSynchronize(c->evp1));
@@ -1791,13 +1823,24 @@ struct Ens {
   cudaGraphExec_t exec = nullptr;
   size_t nodes = 0;
   std::vector<cudaEvent_t> joins;
-  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+  cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr, solved = nullptr;
+  // batched solves: every zeta solve of the step is one cooperative launch for all members
+  int mode = SI3D_ENS_SOLVE_BATCHED;   // requested; the per-member form when a member does not qualify
+  bool batched = false;                // the form of the captured graph
+  int loop_blocks = 0;                 // blocks of the batched launch
+  int slots = 0;                       // batched launches per step (zeta solves of a step)
+  std::vector<double> nodes_of;        // nodes of each member's larger colour
+  std::vector<int> caps;               // blocks of each member's own solve launch
+  PcgEnsItem* d_items = nullptr;       // [slots][members] shares of the batched launches
+  GridBar* d_bars = nullptr;
   ~Ens() {
     if (exec) cudaGraphExecDestroy(exec);
     if (graph) cudaGraphDestroy(graph);
     for (cudaEvent_t e : joins) cudaEventDestroy(e);
-    for (cudaEvent_t e : {fork, t0, t1}) if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {fork, t0, t1, solved}) if (e) cudaEventDestroy(e);
     if (master) cudaStreamDestroy(master);
+    if (d_items) cudaFree(d_items);
+    if (d_bars) cudaFree(d_bars);
   }
 };
 std::vector<Ens*> g_ens;
@@ -1824,11 +1867,196 @@ int si3d_ens_create(const int* handles, int n, int* ens) {
   CK(cudaSetDevice(E->device));
   CK(cudaStreamCreateWithFlags(&E->master, cudaStreamNonBlocking));
   for (cudaEvent_t* e : {&E->fork, &E->t0, &E->t1}) CK(cudaEventCreate(e));
+  CK(cudaEventCreateWithFlags(&E->solved, cudaEventDisableTiming));
   E->joins.resize(n);
   for (auto& e : E->joins) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
   std::lock_guard<std::mutex> lk(g_mu);
   g_ens.push_back(E.release());
   *ens = (int)g_ens.size() - 1;
+  return 0;
+}
+
+// Whether every member qualifies for the batched solves: stopping test 5, no stored diagonal, no
+// recording, the same time-stepping options, and no more members than co-resident blocks.  Fixes
+// the launch's grid (every co-resident block, or the sum of the members' own launch sizes if
+// smaller) and the solves a step has.
+static bool ens_batch_plan(Ens* E) {
+  const int m = (int)E->hs.size();
+  const si3d_params& p0 = get(E->hs[0])->prm;
+  E->nodes_of.assign(m, 0.0);
+  E->caps.assign(m, 1);
+  long long own = 0;
+  for (int i = 0; i < m; ++i) {
+    const Ctx* c = get(E->hs[i]);
+    if (c->prm.pcg_test != 5 || c->pcg.diag_stored || c->rec_buf || c->prm.itrap != p0.itrap ||
+        c->prm.niter != p0.niter || c->loop_blocks < 1)
+      return false;
+    E->nodes_of[i] = std::max(c->pcg.R.n, c->pcg.B.n);
+    E->caps[i] = c->loop_blocks;
+    own += c->loop_blocks;
+  }
+  const int nb = pcg_loop_ens_blocks(E->device);
+  if (nb < m) return false;
+  E->loop_blocks = (int)std::min<long long>(nb, own);
+  const bool leapfrog_only = p0.itrap == 0 || (2 % std::max(p0.itrap, 1)) != 0;
+  E->slots = leapfrog_only ? 1 : 1 + std::min(p0.niter, 21);
+  return true;
+}
+
+// The members' shares of one batched launch, for solves that took its[i] iterations (all 1 before
+// any step): one block each, then one more at a time to the member whose solve would take longest,
+// its[i] x (a fixed cost per iteration + its nodes per block x a streaming cost per node), up to the
+// blocks its own launch uses (its partial-sum arrays are sized for those).  Every block of the grid
+// is given out.
+static std::vector<int> ens_shares(const Ens* E, const std::vector<double>& its) {
+  constexpr double kIterUs = 5.0;      // three grid barriers and the partial sums of an iteration
+  constexpr double kNodeUs = 0.0066;   // both colours' streams of one node of the larger colour
+  const int m = (int)E->hs.size();
+  std::vector<int> b(m, 1);
+  int left = E->loop_blocks - m;
+  while (left > 0) {
+    int best = -1;
+    double bv = -1.0;
+    for (int i = 0; i < m; ++i) {
+      if (b[i] >= E->caps[i]) continue;
+      const double t = its[i] * (kIterUs + kNodeUs * E->nodes_of[i] / b[i]);
+      if (t > bv) { bv = t; best = i; }
+    }
+    if (best < 0) break;
+    ++b[best];
+    --left;
+  }
+  return b;
+}
+
+// Upload the shares of every solve slot of the step (its: [slot][member] iterations, or null for
+// the first plan).
+static int ens_upload_shares(Ens* E, const std::vector<std::vector<double>>* its) {
+  const int m = (int)E->hs.size();
+  std::vector<PcgEnsItem> items((size_t)m * E->slots);
+  for (int k = 0; k < E->slots; ++k) {
+    const std::vector<int> b = ens_shares(E, its ? (*its)[k] : std::vector<double>(m, 1.0));
+    int first = 0;
+    for (int i = 0; i < m; ++i) {
+      PcgEnsItem& it = items[(size_t)k * m + i];
+      it.P = get(E->hs[i])->pcg;
+      it.bar = E->d_bars + i;
+      it.first = first;
+      it.nblk = b[i];
+      first += b[i];
+    }
+  }
+  CK(cudaMemcpy(E->d_items, items.data(), sizeof(PcgEnsItem) * items.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+// Capture one step (n >= 2) with every zeta solve batched: the members advance in lock step on their
+// own streams up to each solve's set-up, join the master stream for one cooperative launch that
+// solves all of their systems (k_pcg_loop_ens, each member on its share of the blocks with its own
+// barrier record), and fork again for the rest of the fd call.  The stage sequence is step_impl's
+// for n >= 2.  The k-th launch reads its shares from slot k of the item array, which the steps
+// refresh from each solve's last iteration counts without capturing again.
+static int ens_capture_batched(Ens* E) {
+  const int m = (int)E->hs.size();
+  if (!E->d_items) {
+    CK(cudaMalloc(&E->d_bars, sizeof(GridBar) * (size_t)m));
+    CK(cudaMalloc(&E->d_items, sizeof(PcgEnsItem) * (size_t)m * E->slots));
+    const int rc = ens_upload_shares(E, nullptr);
+    if (rc) return rc;
+  }
+  int slot = 0;
+  std::vector<Ctx*> cs(m);
+  std::vector<char> prof(m);
+  CK(cudaStreamBeginCapture(E->master, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = cudaEventRecord(E->fork, E->master);
+  for (int i = 0; i < m; ++i) {
+    Ctx* c = cs[i] = get(E->hs[i]);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(c->st, E->fork, 0);
+    c->graph_mode = true;
+    c->ens_defer = true;
+    c->solve_slot = 0;
+    c->trap_solves = 0;
+    c->thrs = 2.0 * c->prm.dt / 3600.;
+    prof[i] = c->prof;
+    c->prof = false;
+  }
+  // one fd call of every member around one batched solve launch
+  auto fd_all = [&](int istep, bool last) -> int {
+    for (int i = 0; i < m; ++i) {
+      int it = 0, ie = 0;
+      double rr = 0.0;
+      int r = fd_pre(cs[i], istep);
+      if (!r) r = solve(cs[i], &it, &rr, &ie);
+      if (r) return r;
+      if (cudaEventRecord(E->joins[i], cs[i]->st) != cudaSuccess ||
+          cudaStreamWaitEvent(E->master, E->joins[i], 0) != cudaSuccess)
+        return cuda_fail(cudaGetLastError());
+    }
+    if (slot >= E->slots) return SI3D_EDIMS;
+    if (pcg_loop_ens(E->d_items + (size_t)slot * m, m, E->loop_blocks, E->d_bars, E->master) != 0)
+      return cuda_fail(cudaGetLastError(), "pcg_loop_ens", __LINE__);
+    ++slot;
+    cs[0]->launches += 1;
+    if (cudaEventRecord(E->solved, E->master) != cudaSuccess) return cuda_fail(cudaGetLastError());
+    for (int i = 0; i < m; ++i) {
+      if (cudaStreamWaitEvent(cs[i]->st, E->solved, 0) != cudaSuccess) return cuda_fail(cudaGetLastError());
+      int r = solve_graph_post(cs[i], cs[i]->def_hist, cs[i]->def_ier);
+      if (!r) r = fd_post(cs[i], last);
+      if (r) return r;
+    }
+    return 0;
+  };
+  auto each = [&](const std::function<int(Ctx*)>& f) -> int {
+    for (Ctx* c : cs) {
+      const int r = f(c);
+      if (r) return r;
+    }
+    return 0;
+  };
+  auto save = [](int istep) {
+    return [istep](Ctx* c) {
+      int rs = 0;
+      const int r = stage(c, ST_SAVE, 2, [&] { rs = save_all(c, istep); });
+      return r ? r : rs;
+    };
+  };
+  int rc = e == cudaSuccess ? 0 : cuda_fail(e);
+  if (!rc) {
+    const si3d_params& p = cs[0]->prm;
+    const bool leapfrog_only = p.itrap == 0 || (2 % std::max(p.itrap, 1)) != 0;
+    rc = fd_all(1, leapfrog_only);
+    if (!rc && leapfrog_only) {
+      rc = each(save(1));
+    } else if (!rc) {
+      rc = each([](Ctx* c) { return stage(c, ST_SETTRAP, 3, [&] { settrap_all(c); }); });
+      for (int it = 1; it <= p.niter && !rc; ++it) {
+        rc = fd_all(2, it == p.niter);
+        if (!rc && it < p.niter) rc = each([](Ctx* c) { return stage(c, ST_SETTRAP2, 3, [&] { settrap2_all(c); }); });
+        if (it > 20) break;
+      }
+      if (!rc) rc = each(save(2));
+    }
+    for (int i = 0; i < m && !rc; ++i) {
+      if (cudaEventRecord(E->joins[i], cs[i]->st) != cudaSuccess ||
+          cudaStreamWaitEvent(E->master, E->joins[i], 0) != cudaSuccess)
+        rc = cuda_fail(cudaGetLastError());
+    }
+  }
+  cudaGraph_t g = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(E->master, &g);
+  E->nsolves.assign(m, 0);
+  for (int i = 0; i < m; ++i) {
+    cs[i]->graph_mode = false;
+    cs[i]->ens_defer = false;
+    cs[i]->prof = prof[i] != 0;
+    E->nsolves[i] = std::min(cs[i]->solve_slot, 24);
+  }
+  if (rc) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e2 != cudaSuccess) return cuda_fail(e2);
+  E->graph = g;
+  E->batched = true;
+  CK(cudaGraphGetNodes(g, nullptr, &E->nodes));
+  CK(cudaGraphInstantiate(&E->exec, g, 0));
   return 0;
 }
 
@@ -1838,6 +2066,8 @@ static int ens_capture(Ens* E) {
   // a captured step replays fixed pointers, while the two tracer pools change roles at every save
   for (int h : E->hs)
     if (get(h)->prm.ntr > 0) return SI3D_EDIMS;
+  if (E->mode == SI3D_ENS_SOLVE_BATCHED && ens_batch_plan(E)) return ens_capture_batched(E);
+  E->batched = false;
   CK(cudaStreamBeginCapture(E->master, cudaStreamCaptureModeThreadLocal));
   int rc = 0;
   cudaError_t e = cudaEventRecord(E->fork, E->master);
@@ -1904,7 +2134,10 @@ int si3d_ens_step(int ens, int n0, int nsteps, int* iters, int* ier, double* ms)
       CK(cudaEventElapsedTime(&t, E->t0, E->t1));
       ms[s] = t;
     }
-    if (n > 1 && (iters || ier)) {
+    const bool batched = n > 1 && E->batched;
+    if (n > 1 && (iters || ier || batched)) {
+      // each solve slot's iteration counts weight the next step's shares of the batched launches
+      std::vector<std::vector<double>> its(batched ? E->slots : 0, std::vector<double>(m, 1.0));
       for (int i = 0; i < m; ++i) {
         Ctx* c = get(E->hs[i]);
         int buf[48];
@@ -1916,6 +2149,11 @@ int si3d_ens_step(int ens, int n0, int nsteps, int* iters, int* ier, double* ms)
         }
         for (int k = 0; k < E->nsolves[i]; ++k)
           if (buf[2 * k + 1] < 0) return buf[2 * k + 1];   // the reference stops on ier < 0
+        for (int k = 0; k < std::min(E->nsolves[i], (int)its.size()); ++k) its[k][i] = std::max(buf[2 * k], 1);
+      }
+      if (batched) {
+        const int rc = ens_upload_shares(E, &its);
+        if (rc) return rc;
       }
     }
   }
@@ -1926,6 +2164,27 @@ int si3d_ens_nodes(int ens) {
   Ens* E = get_ens(ens);
   if (!E) return SI3D_EHANDLE;
   return (int)E->nodes;
+}
+
+int si3d_ens_solve_mode(int ens, int mode) {
+  Ens* E = get_ens(ens);
+  if (!E) return SI3D_EHANDLE;
+  if (mode != SI3D_ENS_SOLVE_MEMBERS && mode != SI3D_ENS_SOLVE_BATCHED) return SI3D_EDIMS;
+  if (mode != E->mode) {   // the next step n >= 2 captures the graph again
+    CK(cudaSetDevice(E->device));
+    CK(cudaStreamSynchronize(E->master));
+    if (E->exec) { cudaGraphExecDestroy(E->exec); E->exec = nullptr; }
+    if (E->graph) { cudaGraphDestroy(E->graph); E->graph = nullptr; }
+    E->nodes = 0;
+    E->mode = mode;
+  }
+  return 0;
+}
+
+int si3d_ens_solve_blocks(int ens) {
+  Ens* E = get_ens(ens);
+  if (!E) return SI3D_EHANDLE;
+  return E->exec && E->batched ? E->loop_blocks : 0;
 }
 
 void si3d_ens_destroy(int ens) {

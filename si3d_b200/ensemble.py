@@ -89,6 +89,15 @@ class Ensemble:
     def nodes(self) -> int:
         return self.g.si3d_ens_nodes(self.e)
 
+    def solve_mode(self, mode: int) -> None:
+        """native.SI3D_ENS_SOLVE_BATCHED (default: each zeta solve of a step is one cooperative launch
+        for all members) or native.SI3D_ENS_SOLVE_MEMBERS (one launch per member)."""
+        check(self.g.si3d_ens_solve_mode(self.e, mode))
+
+    def solve_blocks(self) -> int:
+        """Blocks of the batched solve launch in the captured step (0: per-member form)."""
+        return self.g.si3d_ens_solve_blocks(self.e)
+
     def close(self) -> None:
         if getattr(self, "e", None) is not None:
             self.g.si3d_ens_destroy(self.e)

@@ -181,6 +181,11 @@
          REAL(C_DOUBLE), INTENT(OUT) :: ms(*)
       END FUNCTION
 
+      INTEGER(C_INT) FUNCTION si3d_ens_solve_mode(ens, mode) BIND(C, NAME="si3d_ens_solve_mode")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE :: ens, mode
+      END FUNCTION
+
       SUBROUTINE si3d_ens_destroy(ens) BIND(C, NAME="si3d_ens_destroy")
          IMPORT :: C_INT
          INTEGER(C_INT), VALUE :: ens

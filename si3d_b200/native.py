@@ -98,6 +98,8 @@ GPU_SYMBOLS = {
     "si3d_ens_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "si3d_ens_step": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "si3d_ens_nodes": (C.c_int, [C.c_int]),
+    "si3d_ens_solve_mode": (C.c_int, [C.c_int, C.c_int]),
+    "si3d_ens_solve_blocks": (C.c_int, [C.c_int]),
     "si3d_ens_destroy": (None, [C.c_int]),
     # learned initial guess (include/si3d_learn.h)
     "si3d_learn_set_params": (C.c_int, [C.c_int, C.c_void_p]),
@@ -114,6 +116,8 @@ GPU_SYMBOLS = {
     "si3d_net_sync": (C.c_int, []),
 }
 ENS_MAXSOLVES = 4
+SI3D_ENS_SOLVE_MEMBERS = 0
+SI3D_ENS_SOLVE_BATCHED = 1
 NET_NPARAM = 9 * 4 * 32 + 32 + 4 * (9 * 32 * 32 + 32) + 9 * 32 + 1
 NET_LOSS_FLOATS = 2 + 2 * 148
 

@@ -44,6 +44,67 @@ def test_ensemble_matches_members_run_alone(native_libs, small_members):
             run.close()
 
 
+def test_batched_and_member_solves_are_bit_identical(native_libs, small_members):
+    """Small members fit the batched launch with the blocks their own solve launches use, so the two
+    forms sum every dot product in the same order: fields and iteration counts agree bit for bit."""
+    from si3d_b200 import native
+    from si3d_b200.ensemble import Ensemble
+    out = {}
+    for mode in (native.SI3D_ENS_SOLVE_BATCHED, native.SI3D_ENS_SOLVE_MEMBERS):
+        ens = Ensemble(small_members)
+        try:
+            ens.solve_mode(mode)
+            iters, ier, _ = ens.step(5)
+            assert (ier == 0).all()
+            blocks = ens.solve_blocks()
+            assert (blocks > 0) == (mode == native.SI3D_ENS_SOLVE_BATCHED)
+            out[mode] = (iters, [(r.get("s").copy(), r.get("uh").copy(), r.get("sal").copy()) for r in ens.runs])
+        finally:
+            ens.close()
+    a, b = out[native.SI3D_ENS_SOLVE_BATCHED], out[native.SI3D_ENS_SOLVE_MEMBERS]
+    np.testing.assert_array_equal(a[0], b[0])
+    for fa, fb in zip(a[1], b[1]):
+        for x, y in zip(fa, fb):
+            np.testing.assert_array_equal(x, y)
+
+
+def test_batched_solve_shares_the_grid(native_libs, tmp_path):
+    """Members whose own solve launches would need more blocks than the GPU holds share the batched
+    launch's blocks: each basin still iterates to its own convergence at the same tolerance, and
+    agrees with the basin run alone to rounding (its dot products are summed over fewer blocks)."""
+    from si3d_b200 import ensemble, native
+    from si3d_b200.ensemble import Ensemble
+    from si3d_b200.model import GpuRun
+    ms = ensemble.basins(n=4, seed=23, size_min=(480, 380), size_max=(520, 420), layers=(8, 12))
+    dirs = ensemble.write(ms, str(tmp_path))
+    steps = 4
+    ens = Ensemble(dirs)
+    try:
+        ens.solve_mode(native.SI3D_ENS_SOLVE_BATCHED)
+        iters, ier, _ = ens.step(steps)
+        assert (ier == 0).all()
+        blocks = ens.solve_blocks()
+        # each member's own solve launch takes at least ceil((lm / 2) / 1024) blocks of 1024 threads
+        # (one node of the larger colour per thread): together more than the batched launch has
+        own = [-(-(r.lm // 2) // 1024) for r in ens.runs]
+        assert 0 < blocks < sum(own)
+        got = [(r.get("s").copy(), r.get("uh").copy()) for r in ens.runs]
+    finally:
+        ens.close()
+    for k, d in enumerate(dirs):
+        run = GpuRun(d, pcg_itmax=2000)
+        try:
+            st = run.run(steps)
+            s_ref, u_ref = run.get("s"), run.get("uh")
+            assert np.abs(got[k][0] - s_ref).max() <= 1e-10
+            assert np.abs(got[k][1] - u_ref).max() <= 1e-9 * max(np.abs(u_ref).max(), 1e-30)
+            for s in range(1, steps):
+                ref = [st[s].iters[i] for i in range(st[s].nsolves)]
+                assert all(abs(int(x) - y) <= 2 for x, y in zip(iters[s, k, :len(ref)], ref))
+        finally:
+            run.close()
+
+
 def test_graph_is_captured_once(native_libs, small_members):
     from si3d_b200.ensemble import Ensemble
     ens = Ensemble(small_members[:2])
