@@ -399,10 +399,10 @@ def main() -> int:
                                        "peak": peak, "unit": "GB/s", "frac": alg / (ms / calls * 1e-3) / 1e9 / peak,
                                        "peak_kind": peak_kind}
         dominant = max(stage_ms, key=lambda k: stage_ms[k][0])
-        if dominant == "tracer":
-            ts = out["tracer_stage"]
+        if dominant in ("tracer", "turbulence"):
+            ts = out["tracer_stage" if dominant == "tracer" else "turbulence_stage"]
             out["roofline"] = {"bound": "hbm", "achieved": ts["achieved"], "peak": peak, "unit": "GB/s",
-                               "frac": ts["frac"], "traffic": None, "kernel": "tracer",
+                               "frac": ts["frac"], "traffic": None, "kernel": dominant,
                                "algorithmic_bytes_per_call": ts["algorithmic_bytes_per_call"],
                                "ms_per_call": ts["ms_per_call"], "peak_kind": peak_kind}
         elif dominant in STAGE_STREAMS:

@@ -2,14 +2,18 @@
 // with SolveTKEandLengthScale (:301-551) and tridT (:554-612), and the time levels of q2 and q2l
 // (settrap_2EqTVars :727-771, settrap2_2EqTVars :775-816, save_2EqTvars :819-889).
 //
-// One thread per wet column walks its layers in FP64, in the reference's operation order: the
-// shear and buoyancy production from the eddy coefficients of time n, then the eddy coefficients
-// of time n+1 from q2 and q2l of time n (a column's production reads only its own coefficients, so
-// they are replaced as soon as they are used), then the two tridiagonal systems for q2 and q2l over
-// the layers k1s .. kms + 1 (the same off-diagonals), solved as tridT does (divisions, not
-// reciprocals), each sweep loading its next layer before the current layer's arithmetic.
-// Per-layer quantities the sweeps reuse (limited length scale, production terms, distance from the
-// bottom, elimination factors) go to four scratch fields.
+// Two kernels, in FP64 and in the reference's operation order.  k_turb_cells (block = 32
+// consecutive columns x CLN layer lanes) forms, cell by cell, the shear and buoyancy production from
+// the eddy coefficients of time n, then the eddy coefficients of time n+1 from q2 and q2l of time n
+// (a cell's production reads only its own coefficients, so they are replaced as soon as they are
+// used): independent cells, so thousands of loads are in flight.  k_turb_column (one thread per
+// wet column) then sums the distances from the bottom, applies the surface and out-of-column
+// limits to the coefficients and solves the two tridiagonal systems for q2 and q2l over the layers
+// k1s .. kms + 1 (the same off-diagonals) as tridT does (divisions, not reciprocals), both systems
+// in one forward and one backward pass, each pass loading its next layer before the current
+// layer's arithmetic.  Per-layer quantities the sweeps
+// reuse (limited length scale, production terms, distance from the bottom, elimination factors) go
+// to four scratch fields.
 #include "kernels.h"
 
 namespace si3d {
@@ -25,33 +29,24 @@ struct TurbConst {
   double t1, t2, t3, t4, t5, b1_23;
 };
 
-__global__ void k_turb_column(Dev d, TurbConst T, double* __restrict__ sxl, double* __restrict__ ssp,
-                              double* __restrict__ sbp, double* __restrict__ szb, double* __restrict__ se) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+template <int CLN>
+__global__ void __launch_bounds__(32 * CLN) k_turb_cells(Dev d, TurbConst T, double* __restrict__ sxl,
+                                                      double* __restrict__ ssp, double* __restrict__ sbp) {
+  const int l = blockIdx.x * 32 + threadIdx.x + 1;
   if (l > d.g.lm) return;
-  const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1], k1 = d.g.k1, km1 = d.g.km1, P = d.g.P;
+  const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1], P = d.g.P;
   if (kms - k1s + 1 <= 1) return;
   const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l), dW = lW - l, dS = lS - l;
-  const double twodt1 = d.p.twodt * d.tz;   // twodt / istep
   const double* __restrict__ hp = d.f.hp;
   const double* __restrict__ rhop = d.f.rhop;
   const double* __restrict__ up = d.f.up;
   const double* __restrict__ vp = d.f.vp;
   const double* __restrict__ q2p = d.f.q2p;
-  const double* __restrict__ q2pp = d.f.q2pp;
   const double* __restrict__ q2lp = d.f.q2lp;
-  const double* __restrict__ q2lpp = d.f.q2lpp;
-  double* __restrict__ q2 = d.f.q2;
-  double* __restrict__ q2l = d.f.q2l;
   double* __restrict__ Av = d.f.Av;
   double* __restrict__ Dv = d.f.Dv;
-  // ---- distances from the bottom (summed from the bottom up, as the reference does)
-  {
-    double z0 = 0.0;
-    for (int k = kms; k >= k1s + 1; --k) { z0 = z0 + hp[IX(d, k, l)]; szb[IX(d, k, l)] = z0; }
-  }
   // ---- production at time n, then the eddy coefficients (:253-277) in place of the old ones
-  for (int k = k1s + 1; k <= kms; ++k) {
+  for (int k = k1s + 1 + (int)threadIdx.y; k <= kms; k += CLN) {
     const int ik = IX(d, k, l);
     const double hpk = hp[ik], hpu = hp[ik - P];
     const double deltaz = 0.5 * (hpu + hpk);
@@ -77,6 +72,32 @@ __global__ void k_turb_column(Dev d, TurbConst T, double* __restrict__ sxl, doub
     Av[ik] = Rt * Sm + kAvMol;
     Dv[ik] = Rt * Sh + kDvMol;
   }
+}
+
+__global__ void k_turb_column(Dev d, TurbConst T, double* __restrict__ sxl, double* __restrict__ ssp,
+                              double* __restrict__ sbp, double* __restrict__ szb, double* __restrict__ se) {
+  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
+  if (l > d.g.lm) return;
+  const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1], k1 = d.g.k1, km1 = d.g.km1, P = d.g.P;
+  if (kms - k1s + 1 <= 1) return;
+  const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l), dW = lW - l, dS = lS - l;
+  const double twodt1 = d.p.twodt * d.tz;   // twodt / istep
+  const double* __restrict__ hp = d.f.hp;
+  const double* __restrict__ up = d.f.up;
+  const double* __restrict__ vp = d.f.vp;
+  const double* __restrict__ q2p = d.f.q2p;
+  const double* __restrict__ q2pp = d.f.q2pp;
+  const double* __restrict__ q2lp = d.f.q2lp;
+  const double* __restrict__ q2lpp = d.f.q2lpp;
+  double* __restrict__ q2 = d.f.q2;
+  double* __restrict__ q2l = d.f.q2l;
+  double* __restrict__ Av = d.f.Av;
+  double* __restrict__ Dv = d.f.Dv;
+  // ---- distances from the bottom (summed from the bottom up, as the reference does)
+  {
+    double z0 = 0.0;
+    for (int k = kms; k >= k1s + 1; --k) { z0 = z0 + hp[IX(d, k, l)]; szb[IX(d, k, l)] = z0; }
+  }
   if (hp[IX(d, k1s, l)] < 1.E-2) {
     const int ik = IX(d, k1s + 1, l);
     Av[ik] = fmax(Av[ik], 1.E-4);
@@ -93,34 +114,36 @@ __global__ void k_turb_column(Dev d, TurbConst T, double* __restrict__ sxl, doub
   const double du = d.s.uair[l - 1] - usurf, dv = d.s.vair[l - 1] - vsurf;
   const double ustar_s = d.s.cdw[l - 1] * kRhoAir * (du * du + dv * dv) / 1000.;
   const double r3 = 3. / twodt1;
-  // ---- the two systems over k1s .. kms + 1 (n = nw + 1 unknowns), tridT's forward sweep with the
-  // elimination factors in scratch and the forward values in place, then the backward sweep
-  for (int eq = 0; eq < 2; ++eq) {
-    double* __restrict__ out = eq == 0 ? q2 : q2l;
-    double e_prev = 0.0, f_prev = 0.0;
-    double dco_prev = 0.0, zt = 0.0;
+  // ---- the two systems over k1s .. kms + 1 (n = nw + 1 unknowns) in one pass: tridT's forward sweep
+  // of each, with the elimination factors in scratch (q2's in se, q2l's in ssp, whose value at a
+  // layer is dead once the layer is loaded) and the forward values in place, then both backward
+  // sweeps.  The systems share the off-diagonals and most inputs; each keeps its own arithmetic.
+  {
+    double e0 = 0.0, f0 = 0.0, e1 = 0.0, f1 = 0.0;
+    double zt = 0.0;
     // dcoeff(k1s) = Sq 0.5 (xl(k1s) + xl(k1s + 1)) sqrt(0.5 (q2p(k1s) + q2p(k1s + 1))), xl(k1s) = 0
-    dco_prev = Sq * 0.50 * (0.0 + sxl[IX(d, k1s + 1, l)]) *
-               sqrt(0.50 * (q2p[IX(d, k1s, l)] + q2p[IX(d, k1s + 1, l)]));
+    double dco_prev = Sq * 0.50 * (0.0 + sxl[IX(d, k1s + 1, l)]) *
+                      sqrt(0.50 * (q2p[IX(d, k1s, l)] + q2p[IX(d, k1s + 1, l)]));
     // the interior layers' inputs, loaded one layer ahead of the arithmetic that uses them
-    struct In { double hpk, hpu, xl, xln, qp, qpn, SP, BP, x1, x2, zb; };
+    struct In { double hpk, hpu, xl, xln, qp, qpn, SP, BP, q2o, q2lo, q2loo, zb; };
     auto load = [&](int k) -> In {
       const int ik = IX(d, k, l);
       In v;
       v.hpk = hp[ik]; v.hpu = hp[ik - P]; v.xl = sxl[ik]; v.xln = (k < kms) ? sxl[ik + P] : 0.0;
       v.qp = q2p[ik]; v.qpn = q2p[ik + P]; v.SP = ssp[ik]; v.BP = sbp[ik];
-      if (eq == 0) { v.x1 = q2pp[ik]; v.x2 = 0.0; v.zb = 0.0; }
-      else { v.x1 = q2lp[ik]; v.x2 = q2lpp[ik]; v.zb = szb[ik]; }
+      v.q2o = q2pp[ik]; v.q2lo = q2lp[ik]; v.q2loo = q2lpp[ik]; v.zb = szb[ik];
       return v;
     };
     In nxt = load(k1s + 1);
     for (int k = k1s; k <= kms + 1; ++k) {
       const int ik = IX(d, k, l);
-      double a1 = 0.0, a2 = r3, a3 = 0.0, ds;
+      double a1 = 0.0, a3 = 0.0, a20 = r3, a21 = r3, ds0, ds1;
       if (k == k1s) {
-        ds = eq == 0 ? 3. * T.b1_23 * ustar_s / twodt1 : 0.0;
+        ds0 = 3. * T.b1_23 * ustar_s / twodt1;
+        ds1 = 0.0;
       } else if (k == kms + 1) {
-        ds = eq == 0 ? 3. * T.b1_23 * ustar_b / twodt1 : 0.0;
+        ds0 = 3. * T.b1_23 * ustar_b / twodt1;
+        ds1 = 0.0;
       } else {
         const In v = nxt;
         if (k + 1 <= kms) nxt = load(k + 1);
@@ -131,44 +154,53 @@ __global__ void k_turb_column(Dev d, TurbConst T, double* __restrict__ sxl, doub
         dco_prev = dco;
         zt = zt + hpu;   // distance from the surface to the top of layer k
         const double SP = v.SP, BP = v.BP;
-        if (eq == 0) {
-          a2 = r3 - a1 - a3 + 2. * (sqrt(qp) / (B_1 * xl));
-          ds = 4. * qp / twodt1 - v.x1 / twodt1;
-          if (BP >= 0.0) ds = ds + 2. * (SP + BP);
-          else { ds = ds + 2. * (SP); a2 = a2 - BP * 2. / qp; }
-        } else {
-          const double wa = xl / (kKappaS * v.zb), wb = xl / (kKappaS * zt);
-          a2 = r3 - a1 - a3 + sqrt(qp) / (B_1 * xl) * (1. + E_2 * (wa * wa) + E_3 * (wb * wb));
-          if (BP >= 0) ds = xl * (E_1 * SP + E_1 * BP);
-          else { ds = xl * (E_1 * SP); a2 = a2 - E_1 * BP / qp; }
-          ds = ds + 4 * v.x1 / twodt1 - v.x2 / twodt1;
-        }
+        // q2
+        a20 = r3 - a1 - a3 + 2. * (sqrt(qp) / (B_1 * xl));
+        ds0 = 4. * qp / twodt1 - v.q2o / twodt1;
+        if (BP >= 0.0) ds0 = ds0 + 2. * (SP + BP);
+        else { ds0 = ds0 + 2. * (SP); a20 = a20 - BP * 2. / qp; }
+        // q2l
+        const double wa = xl / (kKappaS * v.zb), wb = xl / (kKappaS * zt);
+        a21 = r3 - a1 - a3 + sqrt(qp) / (B_1 * xl) * (1. + E_2 * (wa * wa) + E_3 * (wb * wb));
+        if (BP >= 0) ds1 = xl * (E_1 * SP + E_1 * BP);
+        else { ds1 = xl * (E_1 * SP); a21 = a21 - E_1 * BP / qp; }
+        ds1 = ds1 + 4 * v.q2lo / twodt1 - v.q2loo / twodt1;
       }
       if (k == k1s) {
-        e_prev = -a3 / a2;
-        f_prev = ds / a2;
+        e0 = -a3 / a20;
+        f0 = ds0 / a20;
+        e1 = -a3 / a21;
+        f1 = ds1 / a21;
       } else {
-        const double den = a2 + a1 * e_prev;
-        f_prev = (ds - a1 * f_prev) / den;
-        e_prev = -a3 / den;
+        const double den0 = a20 + a1 * e0;
+        f0 = (ds0 - a1 * f0) / den0;
+        e0 = -a3 / den0;
+        const double den1 = a21 + a1 * e1;
+        f1 = (ds1 - a1 * f1) / den1;
+        e1 = -a3 / den1;
       }
-      se[ik] = e_prev;
-      out[ik] = f_prev;
+      se[ik] = e0;
+      q2[ik] = f0;
+      ssp[ik] = e1;
+      q2l[ik] = f1;
     }
-    const double qmin = eq == 0 ? kQ2Min : kQ2lMin;
-    double x = f_prev;
-    out[IX(d, kms + 1, l)] = fmax(qmin, x);
-    // backward sweep, the next layer's factor and forward value loaded ahead
-    double en = se[IX(d, kms, l)], fn = out[IX(d, kms, l)];
+    double x0 = f0, x1 = f1;
+    q2[IX(d, kms + 1, l)] = fmax(kQ2Min, x0);
+    q2l[IX(d, kms + 1, l)] = fmax(kQ2lMin, x1);
+    // backward sweeps, the next layer's factors and forward values loaded ahead
+    double en0 = se[IX(d, kms, l)], fn0 = q2[IX(d, kms, l)];
+    double en1 = ssp[IX(d, kms, l)], fn1 = q2l[IX(d, kms, l)];
     for (int k = kms; k >= k1s; --k) {
       const int ik = IX(d, k, l);
-      const double e = en, fv = fn;
-      if (k - 1 >= k1s) { en = se[ik - P]; fn = out[ik - P]; }
-      x = e * x + fv;
-      out[ik] = fmax(qmin, x);
+      const double ea = en0, fa = fn0, eb = en1, fb = fn1;
+      if (k - 1 >= k1s) { en0 = se[ik - P]; fn0 = q2[ik - P]; en1 = ssp[ik - P]; fn1 = q2l[ik - P]; }
+      x0 = ea * x0 + fa;
+      q2[ik] = fmax(kQ2Min, x0);
+      x1 = eb * x1 + fb;
+      q2l[ik] = fmax(kQ2lMin, x1);
     }
-    const double top = out[IX(d, k1s, l)];
-    for (int k = k1; k <= k1s - 1; ++k) out[IX(d, k, l)] = top;
+    const double top0 = q2[IX(d, k1s, l)], top1 = q2l[IX(d, k1s, l)];
+    for (int k = k1; k <= k1s - 1; ++k) { q2[IX(d, k, l)] = top0; q2l[IX(d, k, l)] = top1; }
   }
 }
 
@@ -227,6 +259,7 @@ void launch_turbulence(const Dev& d, double* scr4, cudaStream_t st) {
   T.t5 = 9. * A_1 * A_2;
   T.b1_23 = pow(B_1, 2. / 3.);
   const long long n3 = (long long)d.g.km1 * d.g.P;
+  k_turb_cells<4><<<(d.g.lm + 31) / 32, dim3(32, 4), 0, st>>>(d, T, scr4, scr4 + n3, scr4 + 2 * n3);
   k_turb_column<<<(d.g.lm + 63) / 64, 64, 0, st>>>(d, T, scr4, scr4 + n3, scr4 + 2 * n3, scr4 + 3 * n3, d.scr);
 }
 

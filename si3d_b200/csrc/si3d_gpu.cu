@@ -1051,7 +1051,7 @@ int fd_post(Ctx* c, bool lastiter) {
     rc = stage(c, ST_TRACER, 2 * ((c->prm.ntr + kTracerFluxGroup - 1) / kTracerFluxGroup) + 1, [&] { tracer_stage(c); });
   if (!rc) rc = stage(c, ST_VEL2, 1, [&] { launch_vel2(d, c->st); });
   // UpdateMixingCoefficients (si3d_procedures.f90:571)
-  if (!rc && c->prm.iturb == 1) rc = stage(c, ST_TURB, 1, [&] { launch_turbulence(d, c->turb_scr, c->st); });
+  if (!rc && c->prm.iturb == 1) rc = stage(c, ST_TURB, 2, [&] { launch_turbulence(d, c->turb_scr, c->st); });
   return rc;
 }
 
