@@ -422,20 +422,36 @@ def main() -> int:
                                "peak_kind": peak_kind}
         if headline:
             # -------------------------------------------------------- end to end through the C ABI
-            # per step: upload the surface forcing (uair, vair, cdw) from pinned host memory,
-            # advance one step, read zeta back
-            forcing = {k: torch.from_numpy(run.get(k)).pin_memory() for k in ("uair", "vair", "cdw")}
-            zeta = torch.empty(run.lm1, dtype=torch.float64).pin_memory()
+            # per step: the surface forcing (uair, vair, cdw) from pinned host memory to the device,
+            # one step, zeta back to pinned host memory.  The copies are staged: step n + 1's
+            # forcing is copied while step n runs and step n's zeta while step n + 1 runs
+            # (si3d_gpu_stage_field / si3d_gpu_fetch_field); every copy is inside the timed region.
+            names = ("uair", "vair", "cdw")
+            forcing = [{k: torch.from_numpy(run.get(k)).pin_memory() for k in names} for _ in range(2)]
+            zeta = [torch.empty(run.lm1, dtype=torch.float64).pin_memory() for _ in range(2)]
+
+            def stage(n):
+                for k in names:
+                    native.check(g.si3d_gpu_stage_field(run.gh, k.encode(), C.c_void_p(forcing[n % 2][k].data_ptr())))
+                native.check(g.si3d_gpu_stage_commit(run.gh))
+
+            def e2e_loop(steps):
+                stage(0)
+                for n in range(steps):
+                    if n + 1 < steps:
+                        stage(n + 1)
+                    native.check(native.host().si3d_host_run(run.hm, 1, None))
+                    native.check(g.si3d_gpu_fetch_field(run.gh, b"s", C.c_void_p(zeta[n % 2].data_ptr())))
+                native.check(g.si3d_gpu_copies_wait(run.gh))
+
+            e2e_loop(2)   # warm-up: the staging and snapshot buffers are allocated on first use
             barrier()
             t_e2e = time.perf_counter()
-            for _ in range(args.steps):
-                for k, v in forcing.items():
-                    native.check(g.si3d_gpu_set_field(run.gh, k.encode(), C.c_void_p(v.data_ptr())))
-                native.check(native.host().si3d_host_run(run.hm, 1, None))
-                native.check(g.si3d_gpu_get_field(run.gh, b"s", C.c_void_p(zeta.data_ptr())))
+            e2e_loop(args.steps)
             barrier()
             out["e2e"] = {"value": reduce_max((time.perf_counter() - t_e2e) / args.steps), "unit": "s/timestep",
-                          "h2d_bytes_per_step": 3 * run.lm1 * 8, "d2h_bytes_per_step": run.lm1 * 8}
+                          "h2d_bytes_per_step": 3 * run.lm1 * 8, "d2h_bytes_per_step": run.lm1 * 8,
+                          "copies": "staged: step n + 1's forcing copied during step n, step n's zeta during step n + 1"}
         run.close()
         return out
 

@@ -277,6 +277,24 @@ int si3d_gpu_sync(int handle);
  * SI3D_ETIMEOUT through the call that ran it, and the handle stays usable.  Applies once.
  * SI3D_EDIMS for out-of-range arguments or a handle whose steps are being captured in a graph. */
 int si3d_gpu_test_wait_limit(int handle, long long polls, int absent_blocks);
+/* Staged inputs and asynchronous reads, for a host loop that overlaps its transfers with the time
+ * steps (no counterpart in the reference, whose fields live in host memory).  Work on 2-D fields
+ * (lm1 values, e.g. uair, vair, cdw, s) and PINNED host memory (si3d_gpu_host_alloc).
+ * si3d_gpu_stage_field queues a copy of the host values into a staging slot of the handle on a
+ * host-to-device copy stream and returns at once; si3d_gpu_stage_commit closes the group staged
+ * since the last commit.  Each si3d_gpu_step first takes the oldest committed group: it waits for
+ * the group's copies and moves the values into their fields before its first kernel, so a loop can
+ * stage step n + 1's inputs while step n runs.  Two groups at most may wait for a step
+ * (SI3D_EDIMS otherwise); the host buffer must stay unchanged until the copy has run
+ * (si3d_gpu_copies_wait).  si3d_gpu_fetch_field snapshots a 2-D field on the device after the work
+ * queued so far and copies the snapshot to the host buffer on a device-to-host copy stream,
+ * returning at once; the values are in the buffer after si3d_gpu_copies_wait, which waits for
+ * every staged and fetched copy of the handle. */
+int si3d_gpu_stage_field(int handle, const char* name, const double* host_pinned);
+int si3d_gpu_stage_commit(int handle);
+int si3d_gpu_fetch_field(int handle, const char* name, double* host_pinned);
+int si3d_gpu_copies_wait(int handle);
+
 /* Human-readable text for an error code. */
 const char* si3d_gpu_strerror(int code);
 /* Free the device state of a handle. */

@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -175,8 +176,24 @@ struct Ctx {
   std::map<int, std::pair<int*, int>> planes;
   std::vector<int> h_kmz;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr, evp0 = nullptr, evp1 = nullptr;
+  // staged inputs and asynchronous field reads (si3d_gpu_stage_field, si3d_gpu_fetch_field): copy
+  // streams for each direction, two staging slots used in turn, the committed groups oldest first
+  struct Staged {
+    std::map<std::string, double*> buf;
+    std::vector<std::pair<double*, double*>> moves;   // (field, staged values)
+    cudaEvent_t ready = nullptr, free = nullptr;
+  };
+  cudaStream_t ist = nullptr, fst = nullptr;
+  Staged stg[2];
+  int stg_fill = -1, stg_next = 0;
+  std::deque<int> stg_queue;
+  std::map<std::string, double*> snap;
+  cudaEvent_t snap_ready = nullptr, fetch_done = nullptr;
   ~Ctx() {
     if (st) cudaStreamSynchronize(st);
+    for (cudaStream_t x : {ist, fst}) if (x) { cudaStreamSynchronize(x); cudaStreamDestroy(x); }
+    for (cudaEvent_t e : {stg[0].ready, stg[0].free, stg[1].ready, stg[1].free, snap_ready, fetch_done})
+      if (e) cudaEventDestroy(e);
     for (void* p : allocs) cudaFree(p);
     if (h_sc) cudaFreeHost(h_sc);
     if (h_scf) cudaFreeHost(h_scf);
@@ -1701,10 +1718,107 @@ done:
   return 0;
 }
 
+// The oldest committed group of staged inputs into its fields, on the compute stream after the
+// group's copies; the slot is free again once these moves have run.
+static int take_staged(Ctx* c) {
+  if (c->stg_queue.empty()) return 0;
+  const int slot = c->stg_queue.front();
+  c->stg_queue.pop_front();
+  Ctx::Staged& S = c->stg[slot];
+  CK(cudaStreamWaitEvent(c->st, S.ready, 0));
+  for (const auto& mv : S.moves)
+    CK(cudaMemcpyAsync(mv.first, mv.second, sizeof(double) * c->lm1, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaEventRecord(S.free, c->st));
+  return 0;
+}
+
+static int copy_streams(Ctx* c) {
+  if (c->ist) return 0;
+  CK(cudaStreamCreateWithFlags(&c->ist, cudaStreamNonBlocking));
+  CK(cudaStreamCreateWithFlags(&c->fst, cudaStreamNonBlocking));
+  for (cudaEvent_t* e : {&c->stg[0].ready, &c->stg[0].free, &c->stg[1].ready, &c->stg[1].free, &c->snap_ready,
+                         &c->fetch_done})
+    CK(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  for (cudaEvent_t e : {c->stg[0].free, c->stg[1].free}) CK(cudaEventRecord(e, c->ist));
+  CK(cudaEventRecord(c->fetch_done, c->fst));
+  return 0;
+}
+
+int si3d_gpu_stage_field(int h, const char* name, const double* host) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (!name || !host) return SI3D_EDIMS;
+  double* field = f2ptr(c, name);
+  if (!field) return SI3D_ENAME;
+  CK(cudaSetDevice(c->device));
+  if (int rc = copy_streams(c)) return rc;
+  if (c->stg_fill < 0) {
+    if (c->stg_queue.size() >= 2) return SI3D_EDIMS;   // both slots hold groups no step has taken yet
+    const int slot = c->stg_next;
+    c->stg_next ^= 1;
+    c->stg_fill = slot;
+    c->stg[slot].moves.clear();
+    CK(cudaStreamWaitEvent(c->ist, c->stg[slot].free, 0));   // the slot's previous group has been moved
+  }
+  Ctx::Staged& S = c->stg[c->stg_fill];
+  double*& buf = S.buf[name];
+  if (!buf) {   // first use: the allocation's zero fill runs on the default stream, so wait for it
+    if (c->alloc(&buf, c->lm1)) return SI3D_ENOMEM;
+    CK(cudaDeviceSynchronize());
+  }
+  CK(cudaMemcpyAsync(buf, host, sizeof(double) * c->lm1, cudaMemcpyHostToDevice, c->ist));
+  S.moves.emplace_back(field, buf);
+  return 0;
+}
+
+int si3d_gpu_stage_commit(int h) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (c->stg_fill < 0) return SI3D_EDIMS;
+  CK(cudaSetDevice(c->device));
+  CK(cudaEventRecord(c->stg[c->stg_fill].ready, c->ist));
+  c->stg_queue.push_back(c->stg_fill);
+  c->stg_fill = -1;
+  return 0;
+}
+
+int si3d_gpu_fetch_field(int h, const char* name, double* host) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (!name || !host) return SI3D_EDIMS;
+  const double* field = f2ptr(c, name);
+  if (!field) return SI3D_ENAME;
+  CK(cudaSetDevice(c->device));
+  if (int rc = copy_streams(c)) return rc;
+  double*& snap = c->snap[name];
+  if (!snap) {
+    if (c->alloc(&snap, c->lm1)) return SI3D_ENOMEM;
+    CK(cudaDeviceSynchronize());
+  }
+  CK(cudaStreamWaitEvent(c->st, c->fetch_done, 0));   // the previous read has left the snapshots
+  CK(cudaMemcpyAsync(snap, field, sizeof(double) * c->lm1, cudaMemcpyDeviceToDevice, c->st));
+  CK(cudaEventRecord(c->snap_ready, c->st));
+  CK(cudaStreamWaitEvent(c->fst, c->snap_ready, 0));
+  CK(cudaMemcpyAsync(host, snap, sizeof(double) * c->lm1, cudaMemcpyDeviceToHost, c->fst));
+  CK(cudaEventRecord(c->fetch_done, c->fst));
+  return 0;
+}
+
+int si3d_gpu_copies_wait(int h) {
+  Ctx* c = get(h);
+  if (!c) return SI3D_EHANDLE;
+  if (!c->ist) return 0;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->ist));
+  CK(cudaStreamSynchronize(c->fst));
+  return 0;
+}
+
 int si3d_gpu_step(int h, int n, si3d_step_stats* st) {
   Ctx* c = get(h);
   if (!c) return SI3D_EHANDLE;
   CK(cudaSetDevice(c->device));
+  if (int rs = take_staged(c)) return rs;
   const int rc = step_impl(c, n, st);
   if (rc) return rc;
   CK(cudaStreamSynchronize(c->st));

@@ -62,6 +62,31 @@
          REAL(C_DOUBLE), INTENT(OUT)        :: host(*)
       END FUNCTION
 
+      ! staged inputs / asynchronous reads of 2-D fields through pinned buffers (si3d_gpu_host_alloc)
+      INTEGER(C_INT) FUNCTION si3d_gpu_stage_field(handle, name, host) BIND(C, NAME="si3d_gpu_stage_field")
+         IMPORT :: C_INT, C_CHAR, C_PTR
+         INTEGER(C_INT), VALUE              :: handle
+         CHARACTER(KIND=C_CHAR), INTENT(IN) :: name(*)
+         TYPE(C_PTR), VALUE                 :: host
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_stage_commit(handle) BIND(C, NAME="si3d_gpu_stage_commit")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE :: handle
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_fetch_field(handle, name, host) BIND(C, NAME="si3d_gpu_fetch_field")
+         IMPORT :: C_INT, C_CHAR, C_PTR
+         INTEGER(C_INT), VALUE              :: handle
+         CHARACTER(KIND=C_CHAR), INTENT(IN) :: name(*)
+         TYPE(C_PTR), VALUE                 :: host
+      END FUNCTION
+
+      INTEGER(C_INT) FUNCTION si3d_gpu_copies_wait(handle) BIND(C, NAME="si3d_gpu_copies_wait")
+         IMPORT :: C_INT
+         INTEGER(C_INT), VALUE :: handle
+      END FUNCTION
+
       ! the same for the reference's default-REAL (4-byte) module arrays, without -r8
       INTEGER(C_INT) FUNCTION si3d_gpu_set_field_f32(handle, name, host) BIND(C, NAME="si3d_gpu_set_field_f32")
          IMPORT :: C_INT, C_CHAR, C_FLOAT

@@ -98,6 +98,10 @@ GPU_SYMBOLS = {
     "si3d_ens_create": (C.c_int, [C.c_void_p, C.c_int, C.POINTER(C.c_int)]),
     "si3d_ens_step": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]),
     "si3d_ens_nodes": (C.c_int, [C.c_int]),
+    "si3d_gpu_stage_field": (C.c_int, [C.c_int, C.c_char_p, C.c_void_p]),
+    "si3d_gpu_stage_commit": (C.c_int, [C.c_int]),
+    "si3d_gpu_fetch_field": (C.c_int, [C.c_int, C.c_char_p, C.c_void_p]),
+    "si3d_gpu_copies_wait": (C.c_int, [C.c_int]),
     "si3d_ens_solve_mode": (C.c_int, [C.c_int, C.c_int]),
     "si3d_ens_solve_blocks": (C.c_int, [C.c_int]),
     "si3d_ens_destroy": (None, [C.c_int]),
