@@ -210,7 +210,10 @@ struct Ctx {
     cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
     if (e != cudaSuccess) { g_last_cuda = cudaGetErrorString(e); return SI3D_ENOMEM; }
     allocs.push_back(q);
+    // the zero fill runs on the legacy default stream, which the handle's non-blocking streams do
+    // not wait for: finish it before the buffer is handed out
     e = cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T));
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
     if (e != cudaSuccess) { g_last_cuda = cudaGetErrorString(e); return SI3D_ECUDA; }
     *p = static_cast<T*>(q);
     return 0;
@@ -1762,10 +1765,7 @@ int si3d_gpu_stage_field(int h, const char* name, const double* host) {
   }
   Ctx::Staged& S = c->stg[c->stg_fill];
   double*& buf = S.buf[name];
-  if (!buf) {   // first use: the allocation's zero fill runs on the default stream, so wait for it
-    if (c->alloc(&buf, c->lm1)) return SI3D_ENOMEM;
-    CK(cudaDeviceSynchronize());
-  }
+  if (!buf && c->alloc(&buf, c->lm1)) return SI3D_ENOMEM;
   CK(cudaMemcpyAsync(buf, host, sizeof(double) * c->lm1, cudaMemcpyHostToDevice, c->ist));
   S.moves.emplace_back(field, buf);
   return 0;
@@ -1791,10 +1791,7 @@ int si3d_gpu_fetch_field(int h, const char* name, double* host) {
   CK(cudaSetDevice(c->device));
   if (int rc = copy_streams(c)) return rc;
   double*& snap = c->snap[name];
-  if (!snap) {
-    if (c->alloc(&snap, c->lm1)) return SI3D_ENOMEM;
-    CK(cudaDeviceSynchronize());
-  }
+  if (!snap && c->alloc(&snap, c->lm1)) return SI3D_ENOMEM;
   CK(cudaStreamWaitEvent(c->st, c->fetch_done, 0));   // the previous read has left the snapshots
   CK(cudaMemcpyAsync(snap, field, sizeof(double) * c->lm1, cudaMemcpyDeviceToDevice, c->st));
   CK(cudaEventRecord(c->snap_ready, c->st));
