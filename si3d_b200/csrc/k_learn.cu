@@ -74,47 +74,65 @@ __global__ void k_prep(const float* __restrict__ prm, bf16* __restrict__ wfwd, b
 }
 
 // ------------------------------------------------------------------ stem: 4 -> 32, FP32 cores
+// A block takes 8 rows x 32 pixels; thread (ti, tj) computes pixels tj and tj + 16 of row ti, so each
+// weight it reads from shared memory serves two pixels, and a pixel's four input channels are one
+// 16-byte read.  Per output channel the products are accumulated in the order tap, input channel,
+// with the inputs rounded to BF16 first.
+constexpr int ST_W = 2 * TW;                   // pixels per row of a stem tile
+constexpr int ST_WT = ST_W + 2;                // with halo
 __global__ void __launch_bounds__(TP) k_stem(const float* __restrict__ feat, const float* __restrict__ w, int H, int W,
                                              bf16* __restrict__ X, float* __restrict__ Y) {
-  __shared__ float sF[HT * WT * 4];
+  __shared__ __align__(16) float sF[HT * ST_WT * 4];
   __shared__ __align__(16) float sW[9 * 4 * C + C];
-  const int b = blockIdx.z, i0 = blockIdx.y * TH, j0 = blockIdx.x * TW;
+  const int b = blockIdx.z, i0 = blockIdx.y * TH, j0 = blockIdx.x * ST_W;
   for (int r = threadIdx.x; r < 9 * 4 * C + C; r += TP) sW[r] = w[r];
-  for (int r = threadIdx.x; r < HT * WT; r += TP) {
-    const int gi = i0 + r / WT - 1, gj = j0 + r % WT - 1;
+  for (int r = threadIdx.x; r < HT * ST_WT; r += TP) {
+    const int gi = i0 + r / ST_WT - 1, gj = j0 + r % ST_WT - 1;
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
     if (gi >= 0 && gi < H && gj >= 0 && gj < W) v = *reinterpret_cast<const float4*>(feat + (((size_t)b * H + gi) * W + gj) * 4);
-    sF[r * 4 + 0] = bfr(v.x); sF[r * 4 + 1] = bfr(v.y); sF[r * 4 + 2] = bfr(v.z); sF[r * 4 + 3] = bfr(v.w);
+    *reinterpret_cast<float4*>(&sF[r * 4]) = make_float4(bfr(v.x), bfr(v.y), bfr(v.z), bfr(v.w));
   }
   __syncthreads();
   const int ti = threadIdx.x / TW, tj = threadIdx.x % TW;
-  const int gi = i0 + ti, gj = j0 + tj;
-  if (gi >= H || gj >= W) return;
-  float acc[C];
+  float acc[2][C];
 #pragma unroll
-  for (int co = 0; co < C; ++co) acc[co] = 0.f;
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int co = 0; co < C; ++co) acc[h][co] = 0.f;
   for (int t = 0; t < 9; ++t) {
-    const int pi = ti + 1 + t / 3 - 1, pj = tj + 1 + t % 3 - 1;
+    const int pi = ti + t / 3, pj = tj + t % 3;   // halo coordinates of the tap's input
+    const float4 va = *reinterpret_cast<const float4*>(&sF[(pi * ST_WT + pj) * 4]);
+    const float4 vb = *reinterpret_cast<const float4*>(&sF[(pi * ST_WT + pj + TW) * 4]);
+    const float xa[4] = {va.x, va.y, va.z, va.w}, xb[4] = {vb.x, vb.y, vb.z, vb.w};
 #pragma unroll
     for (int ci = 0; ci < 4; ++ci) {
-      const float v = sF[(pi * WT + pj) * 4 + ci];
       const float4* w4 = reinterpret_cast<const float4*>(&sW[(t * 4 + ci) * C]);
 #pragma unroll
       for (int q = 0; q < C / 4; ++q) {
-        const float4 w = w4[q];
-        acc[4 * q + 0] = __fmaf_rn(v, w.x, acc[4 * q + 0]);
-        acc[4 * q + 1] = __fmaf_rn(v, w.y, acc[4 * q + 1]);
-        acc[4 * q + 2] = __fmaf_rn(v, w.z, acc[4 * q + 2]);
-        acc[4 * q + 3] = __fmaf_rn(v, w.w, acc[4 * q + 3]);
+        const float4 wq = w4[q];
+        acc[0][4 * q + 0] = __fmaf_rn(xa[ci], wq.x, acc[0][4 * q + 0]);
+        acc[0][4 * q + 1] = __fmaf_rn(xa[ci], wq.y, acc[0][4 * q + 1]);
+        acc[0][4 * q + 2] = __fmaf_rn(xa[ci], wq.z, acc[0][4 * q + 2]);
+        acc[0][4 * q + 3] = __fmaf_rn(xa[ci], wq.w, acc[0][4 * q + 3]);
+        acc[1][4 * q + 0] = __fmaf_rn(xb[ci], wq.x, acc[1][4 * q + 0]);
+        acc[1][4 * q + 1] = __fmaf_rn(xb[ci], wq.y, acc[1][4 * q + 1]);
+        acc[1][4 * q + 2] = __fmaf_rn(xb[ci], wq.z, acc[1][4 * q + 2]);
+        acc[1][4 * q + 3] = __fmaf_rn(xb[ci], wq.w, acc[1][4 * q + 3]);
       }
     }
   }
-  const size_t p = ((size_t)b * H + gi) * W + gj;
+  const int gi = i0 + ti;
 #pragma unroll
-  for (int co = 0; co < C; co += 2) {
-    const float y0 = acc[co] + sW[9 * 4 * C + co], y1 = acc[co + 1] + sW[9 * 4 * C + co + 1];
-    if (Y) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
-    *reinterpret_cast<__nv_bfloat162*>(X + p * C + co) = __floats2bfloat162_rn(fmaxf(y0, 0.f), fmaxf(y1, 0.f));
+  for (int h = 0; h < 2; ++h) {
+    const int gj = j0 + tj + h * TW;
+    if (gi >= H || gj >= W) continue;
+    const size_t p = ((size_t)b * H + gi) * W + gj;
+#pragma unroll
+    for (int co = 0; co < C; co += 2) {
+      const float y0 = acc[h][co] + sW[9 * 4 * C + co], y1 = acc[h][co + 1] + sW[9 * 4 * C + co + 1];
+      if (Y) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
+      *reinterpret_cast<__nv_bfloat162*>(X + p * C + co) = __floats2bfloat162_rn(fmaxf(y0, 0.f), fmaxf(y1, 0.f));
+    }
   }
 }
 
@@ -747,7 +765,17 @@ int conv_tc_blocks(int B, int H, int W) {
     attr_set[dev] = true;
   }
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv32_tc, 128, TC_SMEM);
+  // the blocks whose shared memory fits one SM (each holds TC_COLS of the 512 TMEM columns), unless
+  // the occupancy query reports more; the blocks are independent, so a grid larger than what is
+  // resident only runs in waves
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv32_tc, 128, TC_SMEM) != cudaSuccess) {
+    cudaGetLastError();
+    occ = 1;
+  }
+  int smem = 0, rsv = 0;
+  cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  cudaDeviceGetAttribute(&rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+  occ = std::max(occ, std::min(smem / (TC_SMEM + rsv + 1024), 512 / TC_COLS));
   const long long ntiles = (long long)B * ((H + TC_R - 1) / TC_R) * ((W + TC_W - 1) / TC_W);
   return (int)std::max(1LL, std::min(ntiles, (long long)sms * std::max(occ, 1)));
 }
@@ -756,7 +784,8 @@ void forward(const Workspace& ws, const float* params, const float* feat, int B,
              cudaStream_t st) {
   const float* bias0 = params + OFF_BLK + 9 * C * C;
   const dim3 grid = tiles(B, H, W);
-  k_stem<<<grid, TP, 0, st>>>(feat, ws.stem, H, W, ws.x[0], ws.training ? ws.y[0] : nullptr);
+  k_stem<<<dim3((W + ST_W - 1) / ST_W, (H + TH - 1) / TH, B), TP, 0, st>>>(feat, ws.stem, H, W, ws.x[0],
+                                                                         ws.training ? ws.y[0] : nullptr);
   for (int k = 0; k < SI3D_NET_BLOCKS; ++k) {
     const bf16* xin = ws.training ? ws.x[k] : ws.x[k & 1];
     bf16* xout = ws.training ? ws.x[k + 1] : ws.x[(k + 1) & 1];
