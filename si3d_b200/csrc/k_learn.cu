@@ -9,7 +9,9 @@
 // (mma.sync m16n8k16); the same kernel with tap-flipped, channel-transposed weights gives the
 // data gradient.  The 4 -> 32 stem, the 32 -> 1 head and the weight gradients are small and run on
 // the FP32 cores, accumulating in a fixed order.
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 #include <stdint.h>
 
 #include <algorithm>
@@ -241,31 +243,43 @@ __global__ void __launch_bounds__(128) k_conv32(const bf16* __restrict__ Xin, co
 }
 
 // ------------------------------------------------------------------ 32 -> 32 conv, tcgen05 (forward)
-// The same convolution on the fifth-generation tensor cores: tcgen05.mma with FP32 accumulators in
-// tensor memory (TMEM), issued by one thread, operands read by the tensor core from shared memory
-// through matrix descriptors.
-//
-// A block takes TC_R output rows x 128 pixels.  Its input tile (TC_R + 2 rows x 130 pixels, 32
-// bf16 channels) is stored as 16-byte channel chunks, sA[row][chunk][pixel][8 channels], so the
-// A operand of tap (di, dj) for output row r - 128 pixels x 16 channels - is a plain K-major matrix
-// starting at row r + 1 + di, pixel 1 + dj: core matrices of 8 pixels x 16 bytes, 16 bytes
-// between pixels, 128 bytes between pixel groups, one chunk row (130 x 16 bytes) between K halves.
-// No im2col copies.  Weights sit as sB[tap][chunk][cout][8 cin] (core matrices of 8 output
-// channels x 16 bytes).  Per output row: 9 taps x 2 K-halves = 18 MMAs of M = 128, N = 32, K = 16
-// into its own 32 TMEM columns; one commit to an mbarrier; then each warp reads its 32 TMEM lanes
-// (its 32 pixels) with tcgen05.ld and applies bias, ReLU and the residual.
-constexpr int TC_R = 4;                        // output rows per block
+// The convolution on the fifth-generation tensor cores, as a pipeline in one persistent block per
+// SM that walks tiles of TC_R output rows x 128 pixels (tile blockIdx.x, + gridDim.x, ...):
+//   warp 0 (one lane)   loads each tile's halo (TC_R + 2 rows x 130 pixels x 32 bf16 channels) with
+//                       four TMA copies, one per 8-channel chunk, into a ring of TC_NS stages,
+//                       zero-filled outside the image;
+//   warp 1 (one lane)   issues per output row 9 taps x 2 K-halves = 18 tcgen05.mma (M = 128
+//                       pixels, N = 32, K = 16, BF16 in, FP32 accumulate) into that row's 32 columns
+//                       of one of two TMEM accumulators, then commits to the accumulator's "full"
+//                       barrier and to the stage's "empty" barrier;
+//   warps 2-5           read the accumulator (each warp its 32 TMEM lanes, i.e. pixels), add bias,
+//                       ReLU and the residual (from the same stage), store, and release the
+//                       accumulator and the stage.
+// So tile i + 1 loads and tile i multiplies while tile i - 1 is written.  The stage holds
+// [chunk][row][pixel][8 channels]: the A operand of tap (di, dj) for output row r is a K-major
+// no-swizzle matrix starting at row r + 1 + di, pixel 1 + dj (core matrices of 8 pixels x 16 bytes,
+// 128 bytes between pixel groups, one chunk between K halves) - no im2col.  Weights sit as
+// sB[tap][chunk][cout][8 cin].  Every mbarrier wait is bounded; a role whose wait gives up raises a
+// flag the others see, and the epilogue then writes NaN into the tiles it has not written, which
+// the solve rejects.
+constexpr int TC_R = 4;                        // output rows per tile
 constexpr int TC_W = 128;                      // pixels per row (the MMA's M)
 constexpr int TC_WT = TC_W + 2;                // with halo
-constexpr int TC_CHUNK = TC_WT * 16;           // bytes of one chunk row (130 pixels x 16 B)
-constexpr int TC_ROWB = 4 * TC_CHUNK;          // bytes of one halo row (4 chunks)
-constexpr int TC_ABYTES = (TC_R + 2) * TC_ROWB;   // 49,920: the last descriptor ends at its last byte
-constexpr int TC_BBYTES = 9 * 4 * C * 16;          // 18,432
-constexpr int TC_SMEM = TC_ABYTES + TC_BBYTES;
-constexpr int TC_COLS = TC_R * C;              // TMEM columns (128)
+constexpr int TC_CHUNK_TX = (TC_R + 2) * TC_WT * 16;   // bytes one chunk's TMA copy writes (12,480)
+constexpr int TC_CHUNK = (TC_CHUNK_TX + 127) / 128 * 128;   // chunk stride, 128-byte aligned (12,544)
+constexpr int TC_ROWB = TC_WT * 16;            // bytes of one halo row of a chunk
+constexpr int TC_STAGE = 4 * TC_CHUNK;         // one halo tile
+constexpr int TC_NS = 3;                       // halo tiles in flight
+constexpr int TC_BBYTES = 9 * 4 * C * 16;      // 18,432
+constexpr int TC_OSTRIDE = 80;                 // bytes per pixel of an epilogue warp's staging rows (64 + 16)
+constexpr int TC_OBYTES = 4 * 32 * TC_OSTRIDE; // four epilogue warps x 32 pixels
+constexpr int TC_SMEM = TC_NS * TC_STAGE + TC_BBYTES + TC_OBYTES + 1024;   // + alignment of the dynamic base
+constexpr int TC_ACC = TC_R * C;               // TMEM columns of one accumulator (128)
+constexpr int TC_COLS = 2 * TC_ACC;            // two accumulators
+constexpr int TC_THREADS = 192;
 constexpr long long TC_WAIT_LIMIT = 1LL << 24; // mbarrier polls before giving up
-static_assert((TC_R + 2) * TC_ROWB <= TC_ABYTES, "A tile");
-static_assert(TC_COLS == 32 || TC_COLS == 64 || TC_COLS == 128 || TC_COLS == 256, "TMEM allocation");
+static_assert(TC_COLS == 256, "TMEM allocation");
+static_assert(TC_STAGE % 1024 == 0 || TC_CHUNK % 128 == 0, "TMA destinations 128-byte aligned");
 
 // Instruction descriptor of kind::f16: D FP32, A and B BF16, both K-major, N = 32, M = 128.
 constexpr uint32_t TC_IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(C >> 3) << 17) | ((uint32_t)(TC_W >> 4) << 24);
@@ -277,136 +291,237 @@ __device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32
          ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-__global__ void __launch_bounds__(128) k_conv32_tc(const bf16* __restrict__ Xin, const bf16* __restrict__ Wk,
-                                                   const float* __restrict__ bias, int B, int H, int W,
-                                                   bf16* __restrict__ Xout, float* __restrict__ Y) {
-  extern __shared__ __align__(1024) unsigned char smem[];
-  unsigned char* sA = smem;
-  unsigned char* sB = smem + TC_ABYTES;
+// Bounded wait for the completion of phase `parity` of an mbarrier; gives up (raising *fail) after
+// TC_WAIT_LIMIT polls, or at once when another role has raised *fail.
+__device__ __forceinline__ bool tc_wait(uint32_t mbar, uint32_t parity, volatile int* fail, bool heed = true) {
+  for (long long it = 0; it < TC_WAIT_LIMIT; ++it) {
+    uint32_t ok;
+    asm volatile("{\n.reg .pred q;\nmbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\nselp.u32 %0, 1, 0, q;\n}\n"
+                 : "=r"(ok) : "r"(mbar), "r"(parity) : "memory");
+    if (ok) return true;
+    if (heed && (it & 63) == 0 && *fail) return false;
+  }
+  *fail = 1;
+  return false;
+}
+
+__device__ __forceinline__ void tc_arrive(uint32_t mbar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" :: "r"(mbar) : "memory");
+}
+
+__global__ void __launch_bounds__(TC_THREADS, 1) k_conv32_tc(const __grid_constant__ CUtensorMap xmap,
+                                                             const bf16* __restrict__ Wk,
+                                                             const float* __restrict__ bias, int B, int H, int W,
+                                                             bf16* __restrict__ Xout, float* __restrict__ Y) {
+  extern __shared__ unsigned char smem_raw[];
   __shared__ uint32_t s_tmem;
-  __shared__ __align__(8) unsigned long long s_mbar;
+  __shared__ __align__(8) unsigned long long s_bar[2 * TC_NS + 4];   // full[NS], empty[NS], tfull[2], tempty[2]
   __shared__ float s_bias[C];
+  __shared__ volatile int s_fail;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const uint32_t aBase = (uint32_t)__cvta_generic_to_shared(sA);
-  const uint32_t bBase = (uint32_t)__cvta_generic_to_shared(sB);
-  const uint32_t mbar = (uint32_t)__cvta_generic_to_shared(&s_mbar);
-  // weights -> sB[tap][chunk][cout][8]; bias; the A region's padding zeroed once
-  for (int r = tid; r < 9 * C * 4; r += 128) {
+  const uint32_t rawBase = (uint32_t)__cvta_generic_to_shared(smem_raw);
+  const uint32_t aBase = (rawBase + 1023u) & ~1023u;              // TC_NS stages of TC_STAGE bytes
+  const uint32_t bBase = aBase + TC_NS * TC_STAGE;
+  unsigned char* const sA = smem_raw + (aBase - rawBase);
+  unsigned char* const sB = smem_raw + (bBase - rawBase);
+  const uint32_t bar0 = (uint32_t)__cvta_generic_to_shared(&s_bar[0]);
+  auto full = [&](int st) { return bar0 + 8u * (uint32_t)st; };
+  auto empty = [&](int st) { return bar0 + 8u * (uint32_t)(TC_NS + st); };
+  auto tfull = [&](int a) { return bar0 + 8u * (uint32_t)(2 * TC_NS + a); };
+  auto tempty = [&](int a) { return bar0 + 8u * (uint32_t)(2 * TC_NS + 2 + a); };
+  // weights -> sB[tap][chunk][cout][8], bias; barriers; TMEM (warp 1)
+  for (int r = tid; r < 9 * C * 4; r += TC_THREADS) {
     const int t = r / (C * 4), n = (r / 4) % C, kc = r % 4;
     *reinterpret_cast<uint4*>(sB + (((t * 4 + kc) * C + n) * 16)) =
         *reinterpret_cast<const uint4*>(&Wk[(t * C + n) * C + kc * 8]);
   }
-  for (int r = tid; r < C; r += 128) s_bias[r] = bias[r];
-  if (warp == 0) {
+  for (int r = tid; r < C; r += TC_THREADS) s_bias[r] = bias[r];
+  if (tid == 0) {
+    s_fail = 0;
+    for (int st = 0; st < TC_NS; ++st) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(full(st)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 5;\n" :: "r"(empty(st)) : "memory");   // commit + 4 warps
+    }
+    for (int a = 0; a < 2; ++a) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(tfull(a)) : "memory");
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;\n" :: "r"(tempty(a)) : "memory");
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];\n" :: "l"(reinterpret_cast<uint64_t>(&xmap)) : "memory");
+  }
+  if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n"
                  :: "r"((uint32_t)__cvta_generic_to_shared(&s_tmem)), "r"((uint32_t)TC_COLS) : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
-  if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" :: "r"(mbar) : "memory");
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-  }
+  // the weights (generic-proxy writes) become visible to the tensor core's reads
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
   const uint32_t tmem = s_tmem;
   const int ntj = (W + TC_W - 1) / TC_W, nti = (H + TC_R - 1) / TC_R, ntiles = B * nti * ntj;
-  uint32_t phase = 0;
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-    const int b = tile / (nti * ntj), rem = tile - b * (nti * ntj);
-    const int i0 = (rem / ntj) * TC_R, j0 = (rem % ntj) * TC_W;
-    // the previous tile's TMEM reads and shared-memory reads are complete
-    asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    // halo tile: (TC_R + 2) rows x 130 pixels x 4 chunks of 16 bytes, zero outside the image; every
-    // copy of a thread is issued before any is waited for (cp.async, zero-filled when the source
-    // size is 0)
-    for (int r = tid; r < (TC_R + 2) * TC_WT * 4; r += 128) {
-      const int c = r & 3, px = (r >> 2) % TC_WT, row = (r >> 2) / TC_WT;
-      const int gi = i0 + row - 1, gj = j0 + px - 1;
-      const bool in = gi >= 0 && gi < H && gj >= 0 && gj < W;
-      const bf16* src = in ? &Xin[(((size_t)b * H + gi) * W + gj) * C + c * 8] : Xin;
-      const uint32_t dst = aBase + (uint32_t)(row * TC_ROWB + c * TC_CHUNK + px * 16);
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" :: "r"(dst), "l"(src), "r"(in ? 16 : 0) : "memory");
-    }
-    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
-    // the tile's writes (made by this thread's copies) become visible to the tensor core's reads
-    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    __syncthreads();
-    if (tid == 0) {
-      asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-      for (int r = 0; r < TC_R; ++r) {
-        for (int t = 0; t < 9; ++t) {
-          const int di = t / 3 - 1, dj = t % 3 - 1;
+  auto tile_origin = [&](int t, int& b, int& i0, int& j0) {
+    b = t / (nti * ntj);
+    const int rem = t - b * (nti * ntj);
+    i0 = (rem / ntj) * TC_R;
+    j0 = (rem % ntj) * TC_W;
+  };
+  if (warp == 0) {
+    // ---------------------------------------------------------------- producer
+    if (lane == 0) {
+      int issued = 0;
+      for (int i = 0, t = blockIdx.x; t < ntiles; ++i, t += gridDim.x) {
+        const int st = i % TC_NS;
+        if (i >= TC_NS && !tc_wait(empty(st), (uint32_t)((i / TC_NS - 1) & 1), &s_fail)) break;
+        issued = i + 1;
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n"
+                     :: "r"(full(st)), "r"((uint32_t)(4 * TC_CHUNK_TX)) : "memory");
+        int b, i0, j0;
+        tile_origin(t, b, i0, j0);
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
-            const uint32_t aAddr = aBase + (uint32_t)((r + 1 + di) * TC_ROWB + 2 * h * TC_CHUNK + (1 + dj) * 16);
-            const uint32_t bAddr = bBase + (uint32_t)(((t * 4 + 2 * h) * C) * 16);
-            const uint64_t ad = tc_desc(aAddr, TC_CHUNK, 128);
-            const uint64_t bd = tc_desc(bAddr, C * 16, 128);
-            const uint32_t acc = (t > 0 || h > 0) ? 1u : 0u;
-            asm volatile(
-                "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
-                :: "r"(tmem + (uint32_t)(r * C)), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc) : "memory");
-          }
+        for (int c = 0; c < 4; ++c) {
+          const uint32_t dst = aBase + (uint32_t)(st * TC_STAGE + c * TC_CHUNK);
+          asm volatile(
+              "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];\n"
+              :: "r"(dst), "l"(reinterpret_cast<uint64_t>(&xmap)), "r"(c * 8), "r"(j0 - 1), "r"(i0 - 1), "r"(b),
+                 "r"(full(st)) : "memory");
         }
       }
-      asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
-                   :: "r"(mbar) : "memory");
+      // after a failure, the copies still in flight land before the block leaves
+      if (s_fail)
+        for (int i = (issued > TC_NS ? issued - TC_NS : 0); i < issued; ++i)
+          tc_wait(full(i % TC_NS), (uint32_t)((i / TC_NS) & 1), &s_fail, false);
     }
-    // wait for the MMAs (bounded: a wait that gives up poisons this tile's output with NaN)
-    bool done = false;
-    for (long long it = 0; it < TC_WAIT_LIMIT && !done; ++it) {
-      uint32_t ok;
-      asm volatile("{\n.reg .pred q;\nmbarrier.try_wait.parity.shared::cta.b64 q, [%1], %2;\nselp.u32 %0, 1, 0, q;\n}\n"
-                   : "=r"(ok) : "r"(mbar), "r"(phase) : "memory");
-      done = ok != 0;
-    }
-    phase ^= 1u;
-    asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-    // epilogue: warp w reads TMEM lanes 32 w .. 32 w + 31 (pixels), 32 columns (channels) per row
-    const int px = warp * 32 + lane, gj = j0 + px;
-    for (int r = 0; r < TC_R; ++r) {
-      uint32_t v[C];
-      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(r * C);
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-          "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
-          : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-            "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
-            "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
-            "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
-          : "r"(taddr) : "memory");
-      asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-      const int gi = i0 + r;
-      if (gi >= H || gj >= W) continue;
-      const size_t p = ((size_t)b * H + gi) * W + gj;
-      const unsigned char* xc = sA + (r + 1) * TC_ROWB + (px + 1) * 16;
+  } else if (warp == 1) {
+    // ---------------------------------------------------------------- MMA issue
+    if (lane == 0) {
+      int issued = 0;
+      for (int i = 0, t = blockIdx.x; t < ntiles; ++i, t += gridDim.x) {
+        const int st = i % TC_NS, a = i & 1;
+        if (!tc_wait(full(st), (uint32_t)((i / TC_NS) & 1), &s_fail)) break;
+        if (i >= 2 && !tc_wait(tempty(a), (uint32_t)((i / 2 - 1) & 1), &s_fail)) break;
+        asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+        // descriptors of the stage's first A matrix and of the first B matrix; the other 71 differ only
+        // in their start address (the low 14 bits, address / 16), by compile-time offsets, so the
+        // fully unrolled issue is an add and an MMA each
+        const uint64_t ad0 = tc_desc(aBase + (uint32_t)(st * TC_STAGE), TC_CHUNK, 128);
+        const uint64_t bd0 = tc_desc(bBase, C * 16, 128);
+        const uint32_t d0 = tmem + (uint32_t)(a * TC_ACC);
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        const uint4 xin = *reinterpret_cast<const uint4*>(xc + c * TC_CHUNK);
-        const __nv_bfloat162* x2 = reinterpret_cast<const __nv_bfloat162*>(&xin);
-        uint4 o;
-        uint32_t* o32 = reinterpret_cast<uint32_t*>(&o);
+        for (int r = 0; r < TC_R; ++r) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          const int co = c * 8 + 2 * e;
-          float y0 = __uint_as_float(v[co]) + s_bias[co], y1 = __uint_as_float(v[co + 1]) + s_bias[co + 1];
-          if (!done) { y0 = __int_as_float(0x7fc00000); y1 = y0; }
-          if (Y) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
-          const float2 xf = __bfloat1622float2(x2[e]);
-          const __nv_bfloat162 ob = __floats2bfloat162_rn(xf.x + fmaxf(y0, 0.f), xf.y + fmaxf(y1, 0.f));
-          o32[e] = *reinterpret_cast<const uint32_t*>(&ob);
+          for (int tap = 0; tap < 9; ++tap) {
+            const int di = tap / 3 - 1, dj = tap % 3 - 1;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+              const uint64_t ad = ad0 + (uint64_t)((2 * h * TC_CHUNK + (r + 1 + di) * TC_ROWB + (1 + dj) * 16) >> 4);
+              const uint64_t bd = bd0 + (uint64_t)((((tap * 4 + 2 * h) * C) * 16) >> 4);
+              const uint32_t acc = (tap > 0 || h > 0) ? 1u : 0u;   // the row's first product starts it
+              asm volatile(
+                  "{\n.reg .pred p;\nsetp.ne.b32 p, %4, 0;\n"
+                  "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n"
+                  :: "r"(d0 + (uint32_t)(r * C)), "l"(ad), "l"(bd), "r"(TC_IDESC), "r"(acc) : "memory");
+            }
+          }
         }
-        *reinterpret_cast<uint4*>(&Xout[p * C + c * 8]) = o;
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                     :: "r"(tfull(a)) : "memory");
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n"
+                     :: "r"(empty(st)) : "memory");
+        ++issued;
+      }
+      // the last multiplications have finished before the accumulators are freed
+      if (issued > 0) tc_wait(tfull((issued - 1) & 1), (uint32_t)(((issued - 1) / 2) & 1), &s_fail);
+    }
+  } else {
+    // ---------------------------------------------------------------- epilogue (warps 2-5)
+    const int q = warp & 3;              // TMEM lanes 32 q .. 32 q + 31 = pixels of this warp
+    const int px = q * 32 + lane;
+    // staging rows of this warp's output: the stores to global memory go out as contiguous runs
+    unsigned char* const sO = sB + TC_BBYTES + (warp - 2) * 32 * TC_OSTRIDE;
+    bool ok = true;
+    for (int i = 0, t = blockIdx.x; t < ntiles; ++i, t += gridDim.x) {
+      const int st = i % TC_NS, a = i & 1;
+      int b, i0, j0;
+      tile_origin(t, b, i0, j0);
+      // one lane of the warp waits (the others would only compete with the tensor core for shared
+      // memory) for the accumulator and for the stage's halo tile, which is read below for the
+      // residual (its barrier is complete already: the stage cannot be refilled before this warp
+      // releases it); __syncwarp orders the other lanes' reads after the wait
+      if (lane == 0 && ok) {
+        ok = tc_wait(tfull(a), (uint32_t)((i / 2) & 1), &s_fail);
+        if (ok) ok = tc_wait(full(st), (uint32_t)((i / TC_NS) & 1), &s_fail);
+      }
+      ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;   // the TMEM reads below are warp-collective
+      __syncwarp();
+      if (ok) asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+      const int gj = j0 + px;
+      for (int r = 0; r < TC_R; ++r) {
+        uint32_t v[C];
+        if (ok) {
+          const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * TC_ACC + r * C);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+              "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+                "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+                "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+              : "r"(taddr) : "memory");
+          asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        } else {
+#pragma unroll
+          for (int k = 0; k < C; ++k) v[k] = 0u;
+        }
+        const int gi = i0 + r;
+        if (gi >= H) continue;   // warp-uniform: the whole row is outside the image
+        const bool inw = gj < W;
+        const size_t p = ((size_t)b * H + gi) * W + gj;
+        const unsigned char* xc = sA + st * TC_STAGE + (r + 1) * TC_ROWB + (px + 1) * 16;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          const uint4 xin = ok ? *reinterpret_cast<const uint4*>(xc + c * TC_CHUNK) : make_uint4(0u, 0u, 0u, 0u);
+          const __nv_bfloat162* x2 = reinterpret_cast<const __nv_bfloat162*>(&xin);
+          uint4 o;
+          uint32_t* o32 = reinterpret_cast<uint32_t*>(&o);
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const int co = c * 8 + 2 * e;
+            float y0 = __uint_as_float(v[co]) + s_bias[co], y1 = __uint_as_float(v[co + 1]) + s_bias[co + 1];
+            if (!ok) { y0 = __int_as_float(0x7fc00000); y1 = y0; }
+            if (Y && inw) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
+            const float2 xf = __bfloat1622float2(x2[e]);
+            const __nv_bfloat162 ob = __floats2bfloat162_rn(xf.x + fmaxf(y0, 0.f), xf.y + fmaxf(y1, 0.f));
+            o32[e] = *reinterpret_cast<const uint32_t*>(&ob);
+          }
+          *reinterpret_cast<uint4*>(sO + lane * TC_OSTRIDE + c * 16) = o;
+        }
+        // the warp's 32 pixels are 2 KB in a row of the output: written as four runs of 512 bytes,
+        // 16 bytes a lane (run k, lane l: pixel 8 k + l / 4, channels 8 (l % 4) ...)
+        __syncwarp();
+        const size_t p0 = ((size_t)b * H + gi) * W + (j0 + q * 32);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int byte = k * 512 + lane * 16, pl = byte >> 6, cc = (byte >> 4) & 3;
+          if (j0 + q * 32 + pl < W)
+            *reinterpret_cast<uint4*>(&Xout[(p0 + pl) * C + cc * 8]) =
+                *reinterpret_cast<const uint4*>(sO + pl * TC_OSTRIDE + cc * 16);
+        }
+        __syncwarp();
+      }
+      // this warp is done with the accumulator and the stage
+      asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+      __syncwarp();
+      if (ok && lane == 0) {
+        tc_arrive(tempty(a));
+        tc_arrive(empty(st));
       }
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
   __syncthreads();
-  if (warp == 0) {
+  if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" :: "r"(tmem), "r"((uint32_t)TC_COLS)
                  : "memory");
@@ -754,47 +869,69 @@ int conv_blocks(int B, int H, int W) {
   return (int)std::max(1LL, std::min(ntiles, (long long)sms * std::max(occ, 1)));
 }
 
-// Persistent grid of the tcgen05 convolution (its dynamic shared memory enabled once per device).
+// Persistent grid of the tcgen05 convolution: one block per SM (its shared memory takes most of
+// one), enabled once per device.
 int conv_tc_blocks(int B, int H, int W) {
-  int dev = 0, sms = 1, occ = 1;
+  int dev = 0, sms = 1;
   cudaGetDevice(&dev);
   static bool attr_set[64] = {false};
   if (dev >= 0 && dev < 64 && !attr_set[dev]) {
     cudaFuncSetAttribute(k_conv32_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM);
-    cudaFuncSetAttribute(k_conv32_tc, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     attr_set[dev] = true;
   }
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  // the blocks whose shared memory fits one SM (each holds TC_COLS of the 512 TMEM columns), unless
-  // the occupancy query reports more; the blocks are independent, so a grid larger than what is
-  // resident only runs in waves
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_conv32_tc, 128, TC_SMEM) != cudaSuccess) {
-    cudaGetLastError();
-    occ = 1;
-  }
-  int smem = 0, rsv = 0;
-  cudaDeviceGetAttribute(&smem, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
-  cudaDeviceGetAttribute(&rsv, cudaDevAttrReservedSharedMemoryPerBlock, dev);
-  occ = std::max(occ, std::min(smem / (TC_SMEM + rsv + 1024), 512 / TC_COLS));
   const long long ntiles = (long long)B * ((H + TC_R - 1) / TC_R) * ((W + TC_W - 1) / TC_W);
-  return (int)std::max(1LL, std::min(ntiles, (long long)sms * std::max(occ, 1)));
+  return (int)std::max(1LL, std::min(ntiles, (long long)sms));
 }
 
-void forward(const Workspace& ws, const float* params, const float* feat, int B, int H, int W, float* out,
-             cudaStream_t st) {
+// cuTensorMapEncodeTiled from the driver, looked up once.
+PFN_cuTensorMapEncodeTiled_v12000 encode_tiled() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  }
+  return fn;
+}
+
+// TMA map of a channels-last activation image [B][H][W][C] (bf16): boxes of 8 channels (16 bytes,
+// the innermost extent) x 130 pixels x (TC_R + 2) rows of one image; coordinates outside the image
+// read as zero.
+bool activation_map(CUtensorMap* m, const bf16* x, int B, int H, int W) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = encode_tiled();
+  if (!enc || (reinterpret_cast<uintptr_t>(x) & 15u) != 0) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)B};
+  const cuuint64_t strides[3] = {(cuuint64_t)C * sizeof(bf16), (cuuint64_t)W * C * sizeof(bf16),
+                                 (cuuint64_t)H * W * C * sizeof(bf16)};
+  const cuuint32_t box[4] = {8, (cuuint32_t)TC_WT, (cuuint32_t)(TC_R + 2), 1};
+  const cuuint32_t elem[4] = {1, 1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(x), dims, strides, box, elem,
+             CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+int forward(const Workspace& ws, const float* params, const float* feat, int B, int H, int W, float* out,
+            cudaStream_t st) {
   const float* bias0 = params + OFF_BLK + 9 * C * C;
   const dim3 grid = tiles(B, H, W);
+  CUtensorMap maps[SI3D_NET_BLOCKS];
+  for (int k = 0; k < SI3D_NET_BLOCKS; ++k)
+    if (!activation_map(&maps[k], ws.training ? ws.x[k] : ws.x[k & 1], B, H, W)) return SI3D_ECUDA;
   k_stem<<<dim3((W + ST_W - 1) / ST_W, (H + TH - 1) / TH, B), TP, 0, st>>>(feat, ws.stem, H, W, ws.x[0],
                                                                          ws.training ? ws.y[0] : nullptr);
+  const int nb = conv_tc_blocks(B, H, W);
   for (int k = 0; k < SI3D_NET_BLOCKS; ++k) {
-    const bf16* xin = ws.training ? ws.x[k] : ws.x[k & 1];
     bf16* xout = ws.training ? ws.x[k + 1] : ws.x[(k + 1) & 1];
-    k_conv32_tc<<<conv_tc_blocks(B, H, W), 128, TC_SMEM, st>>>(
-        xin, ws.wfwd + (size_t)k * 9 * C * C, bias0 + (size_t)k * BLK_SZ, B, H, W, xout,
-        ws.training ? ws.y[k + 1] : nullptr);
+    k_conv32_tc<<<nb, TC_THREADS, TC_SMEM, st>>>(maps[k], ws.wfwd + (size_t)k * 9 * C * C,
+                                                  bias0 + (size_t)k * BLK_SZ, B, H, W, xout,
+                                                  ws.training ? ws.y[k + 1] : nullptr);
   }
   const bf16* xl = ws.training ? ws.x[SI3D_NET_BLOCKS] : ws.x[SI3D_NET_BLOCKS & 1];
   k_head<<<grid, TP, 0, st>>>(xl, ws.head, H, W, out);
+  return 0;
 }
 
 void backward(const Workspace& ws, const float* feat, const float* gout, int B, int H, int W, float* grad,
@@ -857,7 +994,7 @@ int si3d_net_forward(const float* params, const float* feat, int B, int H, int W
   Workspace ws;
   if (!ws.carve(ws_ptr, ws_bytes, B, H, W, true)) return SI3D_EDIMS;
   si3d::learn::prepare(ws, params, 0);
-  si3d::learn::forward(ws, params, feat, B, H, W, out, 0);
+  if (int rc = si3d::learn::forward(ws, params, feat, B, H, W, out, 0)) return rc;
   return cudaGetLastError() == cudaSuccess ? SI3D_OK : SI3D_ECUDA;
 }
 

@@ -26,8 +26,9 @@ struct Workspace {
 };
 
 void prepare(const Workspace& ws, const float* params, cudaStream_t st);
-void forward(const Workspace& ws, const float* params, const float* feat, int B, int H, int W, float* out,
-             cudaStream_t st);
+// 0, or SI3D_ECUDA when the activations' TMA maps cannot be made (nothing is launched then)
+int forward(const Workspace& ws, const float* params, const float* feat, int B, int H, int W, float* out,
+            cudaStream_t st);
 void backward(const Workspace& ws, const float* feat, const float* gout, int B, int H, int W, float* grad,
               cudaStream_t st);
 

@@ -908,13 +908,15 @@ int solve(Ctx* c, int* iters, double* relres, int* ier_out) {
   const bool use_net = learned_step && c->net_loaded;
   if (use_net || c->rec_buf) {
     // features of this system; with the network loaded, the predicted increment into dz
+    int rf = 0;
     int rcl = stage(c, ST_LEARN, use_net ? 9 : 3, [&] {
       learn::features(c->d, c->pix, c->r0, c->fpart, c->sigma, c->feat, c->st);
       if (use_net) {
-        learn::forward(c->net_ws, c->net_params, c->feat, 1, c->im1, c->jm1, c->net_out, c->st);
-        learn::scatter(c->lm, c->pix, c->net_out, c->sigma, c->dz, c->st);
+        rf = learn::forward(c->net_ws, c->net_params, c->feat, 1, c->im1, c->jm1, c->net_out, c->st);
+        if (!rf) learn::scatter(c->lm, c->pix, c->net_out, c->sigma, c->dz, c->st);
       }
     });
+    if (!rcl) rcl = rf;
     if (rcl) return rcl;
     if (use_net) c->dz_set = true;
   }
