@@ -2,13 +2,13 @@
 // solver-side feature / scatter / record kernels.  Network shape and parameter layout are fixed by
 // include/si3d_learn.h.
 //
-// Tiling: every kernel works on 8 x 16 pixel tiles of a channels-last image with a one-pixel halo
-// staged in shared memory.  The four 32 -> 32 convolutions run on the tensor cores as an implicit
-// GEMM (M = 16 pixels of a tile row, N = 8 output channels, K = 16 input channels of one tap;
-// 9 taps x 2 channel halves = 18 K-steps), BF16 operands with FP32 accumulation
-// (mma.sync m16n8k16); the same kernel with tap-flipped, channel-transposed weights gives the
-// data gradient.  The 4 -> 32 stem, the 32 -> 1 head and the weight gradients are small and run on
-// the FP32 cores, accumulating in a fixed order.
+// Channels-last images with a one-pixel halo.  The four 32 -> 32 forward convolutions run on the
+// fifth-generation tensor cores (k_conv32_tc: TMA halo loads, tcgen05.mma into TMEM, a pipeline of
+// producer, MMA and epilogue warps; see there).  The data gradient for training is an implicit GEMM
+// on 8 x 16 pixel tiles with mma.sync m16n8k16 (M = 16 pixels of a tile row, N = 8 channels, K = 16
+// channels of one tap; 9 taps x 2 channel halves = 18 K-steps) with tap-flipped, channel-transposed
+// weights.  BF16 operands, FP32 accumulation.  The 4 -> 32 stem, the 32 -> 1 head and the weight
+// gradients are small and run on the FP32 cores, accumulating in a fixed order.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
