@@ -129,11 +129,20 @@ __global__ void __launch_bounds__(TP) k_stem(const float* __restrict__ feat, con
     const int gj = j0 + tj + h * TW;
     if (gi >= H || gj >= W) continue;
     const size_t p = ((size_t)b * H + gi) * W + gj;
+    // the pixel's 32 channels as four 16-byte stores
 #pragma unroll
-    for (int co = 0; co < C; co += 2) {
-      const float y0 = acc[h][co] + sW[9 * 4 * C + co], y1 = acc[h][co + 1] + sW[9 * 4 * C + co + 1];
-      if (Y) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
-      *reinterpret_cast<__nv_bfloat162*>(X + p * C + co) = __floats2bfloat162_rn(fmaxf(y0, 0.f), fmaxf(y1, 0.f));
+    for (int c4 = 0; c4 < C / 8; ++c4) {
+      uint4 o;
+      uint32_t* o32 = reinterpret_cast<uint32_t*>(&o);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const int co = c4 * 8 + 2 * e;
+        const float y0 = acc[h][co] + sW[9 * 4 * C + co], y1 = acc[h][co + 1] + sW[9 * 4 * C + co + 1];
+        if (Y) *reinterpret_cast<float2*>(Y + p * C + co) = make_float2(y0, y1);
+        const __nv_bfloat162 ob = __floats2bfloat162_rn(fmaxf(y0, 0.f), fmaxf(y1, 0.f));
+        o32[e] = *reinterpret_cast<const uint32_t*>(&ob);
+      }
+      *reinterpret_cast<uint4*>(X + p * C + c4 * 8) = o;
     }
   }
 }
