@@ -19,7 +19,7 @@ namespace {
 
 
 constexpr int TB = 128;
-constexpr int BK_TRIP = 2;   // layers a lane handles per trip of the bookkeeping passes
+constexpr int BK_TRIP = 1;   // layers a lane handles per trip of the bookkeeping passes
 
 __device__ __forceinline__ bool ewet(const Dev& d, int l) { return NB(d.g.lEC, l) != d.g.lm1; }
 __device__ __forceinline__ bool nwet(const Dev& d, int l) { return NB(d.g.lNC, l) != d.g.lm1; }
@@ -149,56 +149,68 @@ __global__ void __launch_bounds__(32 * CLN) k_vel_uv(Dev d, const int* __restric
   }
 }
 
-// continuity(1) and the surface-index update at the end of vel
-__global__ void k_cont1(Dev d) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (l > d.g.lm) return;
-  const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
-  const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l);
-  if (k1s <= kms) {
-    double* __restrict__ wp = d.f.wp;
-    const double* __restrict__ uh = d.f.uh;
-    const double* __restrict__ vh = d.f.vh;
-    const double* __restrict__ uhpp = d.f.uhpp;
-    const double* __restrict__ vhpp = d.f.vhpp;
-    for (int k = 1; k < k1s; ++k) wp[IX(d, k, l)] = 0.0;   // wp below kms is never non-zero
+// continuity(1) at the end of vel and continuity(2) after settrap, settrap2 and save
+// (si3d_procedures.f90:2653-2707): wp from the horizontal fluxes, summed from the column bottom up.
+// Block = 32 consecutive columns x CLN layer lanes.  The lanes form every layer's x and y flux
+// differences, divided by the grid constant as the reference divides, into shared memory (one
+// memory round trip per layer for all of them, every load of a layer issued first); then the first
+// warp runs the bottom-up sum of its 32 columns in the reference's order, w = (w - tx) - ty per
+// layer, so wp is bit-identical to the reference's one-thread loop.  CONT1: the fluxes are
+// uh + uhpp over 2 dx (2 dy), and k1z moves down one level where the top cell has dried.
+// Dynamic shared memory: two planes of (km1 + 1) levels x 32 columns.
+template <int CLN, bool CONT1>
+__global__ void __launch_bounds__(32 * CLN) k_cont(Dev d) {
+  extern __shared__ double s_term[];
+  const int cx = threadIdx.x, ty = threadIdx.y;
+  const int l = blockIdx.x * 32 + cx + 1;
+  const bool act = l <= d.g.lm;
+  const int kms = act ? NB(d.g.kmz, l) : 0, k1s = act ? d.s.k1z[l - 1] : 1;
+  const bool wet = act && k1s <= kms;
+  double* __restrict__ wp = d.f.wp;
+  double* s_x = s_term;
+  double* s_y = s_term + (d.g.km1 + 1) * 32;
+  if (wet) {
+    const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l);
+    for (int k = 1 + ty; k < k1s; k += CLN) wp[IX(d, k, l)] = 0.0;   // wp below kms is never non-zero
+    if (CONT1) {
+      const double* __restrict__ uh = d.f.uh;
+      const double* __restrict__ vh = d.f.vh;
+      const double* __restrict__ uhpp = d.f.uhpp;
+      const double* __restrict__ vhpp = d.f.vhpp;
+      for (int k = d.g.k1 + ty; k <= kms; k += CLN) {
+        const int ik = IX(d, k, l), iw = IX(d, k, lW), is = IX(d, k, lS);
+        const double a0 = uh[ik], a1 = uh[iw], a2 = uhpp[ik], a3 = uhpp[iw];
+        const double b0 = vh[ik], b1 = vh[is], b2 = vhpp[ik], b3 = vhpp[is];
+        s_x[k * 32 + cx] = (a0 - a1 + a2 - a3) / d.p.twodx;
+        s_y[k * 32 + cx] = (b0 - b1 + b2 - b3) / d.p.twody;
+      }
+    } else {
+      const double* __restrict__ uhp = d.f.uhp;
+      const double* __restrict__ vhp = d.f.vhp;
+      for (int k = d.g.k1 + ty; k <= kms; k += CLN) {
+        const int ik = IX(d, k, l);
+        const double a0 = uhp[ik], a1 = uhp[IX(d, k, lW)], b0 = vhp[ik], b1 = vhp[IX(d, k, lS)];
+        s_x[k * 32 + cx] = (a0 - a1) / d.p.dx;
+        s_y[k * 32 + cx] = (b0 - b1) / d.p.dy;
+      }
+    }
+  }
+  __syncthreads();
+  if (ty != 0 || !act) return;
+  if (wet) {
     double w = 0.0;
 #pragma unroll 4
-    for (int k = kms; k >= k1s; --k) {
-      w = w - (uh[IX(d, k, l)] - uh[IX(d, k, lW)] + uhpp[IX(d, k, l)] - uhpp[IX(d, k, lW)]) / d.p.twodx -
-          (vh[IX(d, k, l)] - vh[IX(d, k, lS)] + vhpp[IX(d, k, l)] - vhpp[IX(d, k, lS)]) / d.p.twody;
+    for (int k = kms; k > k1s; --k) {
+      w = w - s_x[k * 32 + cx] - s_y[k * 32 + cx];
       wp[IX(d, k, l)] = w;
     }
-    double ws = wp[IX(d, k1s, l)];
-    for (int k = d.g.k1; k <= k1s - 1; ++k)
-      ws = ws - (uh[IX(d, k, l)] - uh[IX(d, k, lW)] + uhpp[IX(d, k, l)] - uhpp[IX(d, k, lW)]) / d.p.twodx -
-           (vh[IX(d, k, l)] - vh[IX(d, k, lS)] + vhpp[IX(d, k, l)] - vhpp[IX(d, k, lS)]) / d.p.twody;
+    // level k1s: its own term, then the dry levels above it folded in (the reference stores the
+    // first sum and overwrites it with the second)
+    double ws = w - s_x[k1s * 32 + cx] - s_y[k1s * 32 + cx];
+    for (int k = d.g.k1; k <= k1s - 1; ++k) ws = ws - s_x[k * 32 + cx] - s_y[k * 32 + cx];
     wp[IX(d, k1s, l)] = ws;
   }
-  if (d.f.h[IX(d, k1s, l)] <= ZERO) d.s.k1z[l - 1] = min(k1s + 1, d.g.km1);
-}
-
-// continuity(2): wp from uhp/vhp
-__global__ void k_cont2(Dev d) {
-  const int l = blockIdx.x * blockDim.x + threadIdx.x + 1;
-  if (l > d.g.lm) return;
-  const int kms = NB(d.g.kmz, l), k1s = d.s.k1z[l - 1];
-  if (k1s > kms) return;
-  const int lW = NB(d.g.lWC, l), lS = NB(d.g.lSC, l);
-  double* __restrict__ wp = d.f.wp;
-  const double* __restrict__ uhp = d.f.uhp;
-  const double* __restrict__ vhp = d.f.vhp;
-  for (int k = 1; k < k1s; ++k) wp[IX(d, k, l)] = 0.0;   // wp below kms is never non-zero
-  double w = 0.0;
-#pragma unroll 4
-  for (int k = kms; k >= k1s; --k) {
-    w = w - (uhp[IX(d, k, l)] - uhp[IX(d, k, lW)]) / d.p.dx - (vhp[IX(d, k, l)] - vhp[IX(d, k, lS)]) / d.p.dy;
-    wp[IX(d, k, l)] = w;
-  }
-  double ws = wp[IX(d, k1s, l)];
-  for (int k = d.g.k1; k <= k1s - 1; ++k)
-    ws = ws - (uhp[IX(d, k, l)] - uhp[IX(d, k, lW)]) / d.p.dx - (vhp[IX(d, k, l)] - vhp[IX(d, k, lS)]) / d.p.dy;
-  wp[IX(d, k1s, l)] = ws;
+  if (CONT1 && d.f.h[IX(d, k1s, l)] <= ZERO) d.s.k1z[l - 1] = min(k1s + 1, d.g.km1);
 }
 
 // ------------------------------------------------------------- exsal fluxes
@@ -502,9 +514,36 @@ __global__ void k_half_zeta(Dev d, int rotate) {
 // Bookkeeping kernels are cell-parallel: block = 32 consecutive columns x CLN layer lanes, a lane
 // taking layers k0 + lane, k0 + lane + CLN, ...  Every routine of a call (the pp rotation, the
 // thicknesses, the scalar with its density, both velocities) is one pass over the layers in which a
-// cell's loads are all issued before any of its arithmetic, and a lane handles BK_TRIP layers per
-// trip, so a trip costs one memory round trip for all of them.  The expressions are the
-// reference's, so the state is bit-identical to the per-routine loops.
+// cell's loads are all issued before any of its arithmetic, one trip ahead (walk_layers).  The
+// expressions are the reference's, so the state is bit-identical to the per-routine loops.
+
+// The layer walk of a lane: layers k0, k0 + CLN, ... up to ke, BK_TRIP of them per trip.  `load`
+// fills one layer's inputs (its addresses clamped inside the column), `apply` does nothing above ke.
+// The next trip's loads are issued before this trip's arithmetic and stores, so a lane keeps a
+// memory round trip in flight while it evaluates the equation of state (measured at 2000x1000x60:
+// settrap 1.79 -> 1.67 ms against the same walk without the prefetch; two layers per trip with the
+// prefetch need 150 registers and are slower).
+template <int CLN, typename In, typename Load, typename Apply>
+__device__ __forceinline__ void walk_layers(int k0, int ke, Load& load, Apply& apply) {
+  constexpr int STEP = BK_TRIP * CLN;
+  if (k0 > ke) return;
+  In v[BK_TRIP];
+#pragma unroll
+  for (int t = 0; t < BK_TRIP; ++t) load(k0 + t * CLN, v[t]);
+  for (int k = k0;; k += STEP) {
+    const bool more = k + STEP <= ke;
+    In w[BK_TRIP];
+    if (more) {
+#pragma unroll
+      for (int t = 0; t < BK_TRIP; ++t) load(k + STEP + t * CLN, w[t]);
+    }
+#pragma unroll
+    for (int t = 0; t < BK_TRIP; ++t) apply(k + t * CLN, v[t]);
+    if (!more) break;
+#pragma unroll
+    for (int t = 0; t < BK_TRIP; ++t) v[t] = w[t];
+  }
+}
 
 // Values of one cell (k, l) that settrap / settrap2 read.
 struct HalfIn {
@@ -607,13 +646,7 @@ __global__ void __launch_bounds__(32 * CLN) k_half_level(Dev d) {
         else { f_vhp[ik] = 0.0; f_vp[ik] = 0.0; }
       }
     };
-    for (int k = kb + ty; k <= ke; k += BK_TRIP * CLN) {
-      HalfIn v[BK_TRIP];
-#pragma unroll
-      for (int t = 0; t < BK_TRIP; ++t) load(k + t * CLN, v[t]);
-#pragma unroll
-      for (int t = 0; t < BK_TRIP; ++t) apply(k + t * CLN, v[t]);
-    }
+    walk_layers<CLN, HalfIn>(kb + ty, ke, load, apply);
   }
   s_first[0][ty][cx] = fz; s_first[1][ty][cx] = fu; s_first[2][ty][cx] = fv;
   __syncthreads();
@@ -740,13 +773,7 @@ __global__ void __launch_bounds__(32 * CLN) k_save(Dev d) {
         else { f_vhp[ik] = 0.0; f_vp[ik] = 0.0; }
       }
     };
-    for (int k = 1 + ty; k <= zL; k += BK_TRIP * CLN) {
-      SaveIn v[BK_TRIP];
-#pragma unroll
-      for (int t = 0; t < BK_TRIP; ++t) load(k + t * CLN, v[t]);
-#pragma unroll
-      for (int t = 0; t < BK_TRIP; ++t) apply(k + t * CLN, v[t]);
-    }
+    walk_layers<CLN, SaveIn>(1 + ty, zL, load, apply);
   }
   s_first[0][ty][cx] = fz; s_first[1][ty][cx] = fu; s_first[2][ty][cx] = fv;
   __syncthreads();
@@ -800,7 +827,17 @@ __global__ void k_column_tridiag(int n, int nsys, const double* a, const double*
 
 static inline int grid_of(int n) { return (n + TB - 1) / TB; }
 
-constexpr int BK_LANES = 4;   // layer lanes of the cell-parallel bookkeeping and velocity kernels
+constexpr int BK_LANES = 4;   // layer lanes of the copy kernels (slayer_h, vel_uv, vel2)
+constexpr int HALF_LANES = 2;   // layer lanes of k_half_level and k_save
+constexpr int CONT_LANES = 8;   // layer lanes of the continuity kernels (4 and 16 measured slower)
+
+template <bool CONT1>
+static void launch_cont(const Dev& d, cudaStream_t st) {
+  const size_t smem = 2 * (size_t)(d.g.km1 + 1) * 32 * sizeof(double);
+  if (smem > 48 * 1024)
+    cudaFuncSetAttribute(k_cont<CONT_LANES, CONT1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  k_cont<CONT_LANES, CONT1><<<(d.g.lm + 31) / 32, dim3(32, CONT_LANES), smem, st>>>(d);
+}
 
 void launch_slayer_h(const Dev& d, cudaStream_t st) {
   k_slayer_h<BK_LANES><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
@@ -809,7 +846,7 @@ void launch_slayer_h(const Dev& d, cudaStream_t st) {
 void launch_vel(const Dev& d, const int* ce, int nce, const int* cn, int ncn, cudaStream_t st) {
   if (nce > 0) k_vel_uv<1, BK_LANES><<<(nce + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d, ce, nce);
   if (ncn > 0) k_vel_uv<2, BK_LANES><<<(ncn + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d, cn, ncn);
-  k_cont1<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+  launch_cont<true>(d, st);
 }
 
 void launch_exsal_imsal(const Dev& d, const Tune& tu, cudaStream_t st) {
@@ -833,20 +870,20 @@ void launch_vel2(const Dev& d, cudaStream_t st) {
 
 void launch_settrap(const Dev& d, cudaStream_t st) {
   k_half_zeta<<<grid_of(d.g.lm), TB, 0, st>>>(d, 1);
-  k_half_level<BK_LANES, true><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
-  k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+  k_half_level<HALF_LANES, true><<<(d.g.lm + 31) / 32, dim3(32, HALF_LANES), 0, st>>>(d);
+  launch_cont<false>(d, st);
 }
 
 void launch_settrap2(const Dev& d, cudaStream_t st) {
   k_half_zeta<<<grid_of(d.g.lm), TB, 0, st>>>(d, 0);
-  k_half_level<BK_LANES, false><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
-  k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+  k_half_level<HALF_LANES, false><<<(d.g.lm + 31) / 32, dim3(32, HALF_LANES), 0, st>>>(d);
+  launch_cont<false>(d, st);
 }
 
 void launch_save(const Dev& d, int istep, cudaStream_t st) {
-  if (istep == 1) k_save<BK_LANES, true><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
-  else k_save<BK_LANES, false><<<(d.g.lm + 31) / 32, dim3(32, BK_LANES), 0, st>>>(d);
-  k_cont2<<<grid_of(d.g.lm), TB, 0, st>>>(d);
+  if (istep == 1) k_save<HALF_LANES, true><<<(d.g.lm + 31) / 32, dim3(32, HALF_LANES), 0, st>>>(d);
+  else k_save<HALF_LANES, false><<<(d.g.lm + 31) / 32, dim3(32, HALF_LANES), 0, st>>>(d);
+  launch_cont<false>(d, st);
 }
 
 void launch_density_init(const Dev& d, cudaStream_t st) { k_density_init<<<grid_of(d.g.lm1), TB, 0, st>>>(d); }
