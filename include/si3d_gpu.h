@@ -73,7 +73,8 @@ extern "C" {
 /* Grid description produced by the host's `bathy` (si3d_utils.f90:595-892). */
 typedef struct si3d_grid {
   int im1, jm1;            /* (i,j) extents including the fictitious border */
-  int km1;                 /* number of levels incl. fictitious top and bottom layers */
+  int km1;                 /* number of levels incl. fictitious top and bottom layers (3 .. 448;
+                              si3d_gpu_init returns SI3D_EDIMS outside) */
   int k1;                  /* first real layer (2) */
   int lm;                  /* number of wet columns */
   const int* l2i;          /* [lm]   i of column l (1-based) */

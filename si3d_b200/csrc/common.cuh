@@ -11,7 +11,9 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#define SI3D_MAXK 512
+// Most levels per column (km1): the continuity kernels hold two planes of km1 + 1 levels x 32
+// columns of FP64 terms in shared memory, 229,888 bytes at 448 (227 KB per block at most).
+#define SI3D_MAXK 448
 
 namespace si3d {
 

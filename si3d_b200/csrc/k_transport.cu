@@ -831,12 +831,24 @@ constexpr int BK_LANES = 4;   // layer lanes of the copy kernels (slayer_h, vel_
 constexpr int HALF_LANES = 2;   // layer lanes of k_half_level and k_save
 constexpr int CONT_LANES = 8;   // layer lanes of the continuity kernels (4 and 16 measured slower)
 
+// Shared memory of a continuity block: two planes of km1 + 1 levels x 32 columns.
+static size_t cont_smem(int km1) { return 2 * (size_t)(km1 + 1) * 32 * sizeof(double); }
+
 template <bool CONT1>
 static void launch_cont(const Dev& d, cudaStream_t st) {
-  const size_t smem = 2 * (size_t)(d.g.km1 + 1) * 32 * sizeof(double);
-  if (smem > 48 * 1024)
-    cudaFuncSetAttribute(k_cont<CONT_LANES, CONT1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  k_cont<CONT_LANES, CONT1><<<(d.g.lm + 31) / 32, dim3(32, CONT_LANES), smem, st>>>(d);
+  k_cont<CONT_LANES, CONT1><<<(d.g.lm + 31) / 32, dim3(32, CONT_LANES), cont_smem(d.g.km1), st>>>(d);
+}
+
+// Columns deeper than 95 levels need more than the default 48 KB of dynamic shared memory in the
+// continuity kernels: the limit is raised once, to what SI3D_MAXK levels need, so handles of
+// different depths never lower it for one another.
+int transport_init(int km1) {
+  if (cont_smem(km1) <= 48 * 1024) return 0;
+  const int mx = (int)cont_smem(SI3D_MAXK);
+  if (cudaFuncSetAttribute(k_cont<CONT_LANES, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess ||
+      cudaFuncSetAttribute(k_cont<CONT_LANES, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx) != cudaSuccess)
+    return -1;
+  return 0;
 }
 
 void launch_slayer_h(const Dev& d, cudaStream_t st) {

@@ -57,6 +57,8 @@ struct FaceMeta {
 };
 
 int momentum_init(int km1);
+// Raises the continuity kernels' shared-memory limit for columns deeper than 95 levels.
+int transport_init(int km1);
 struct ObcDev;
 // `obc` (nobc boundaries): open boundaries whose face columns' explicit term is recomputed between
 // the cell and the column kernels

@@ -1261,6 +1261,7 @@ int si3d_gpu_init(const si3d_grid* g, const si3d_params* prm, int device, int* h
   rc |= c->alloc(&c->d_stats_ii, 48);
   rc |= c->alloc(&c->d_stats_rr, 24);
   if (!rc && momentum_init(km1) != 0) { g_last_cuda = "momentum kernel shared-memory attribute"; rc = SI3D_ECUDA; }
+  if (!rc && transport_init(km1) != 0) { g_last_cuda = "continuity kernel shared-memory attribute"; rc = SI3D_ECUDA; }
   // pixel (i - 1) * jm1 + (j - 1) of every wet column in the (im1, jm1) image of the learned
   // initial guess (only when the maps describe a real grid)
   c->im1 = std::max(g->im1, 1);
